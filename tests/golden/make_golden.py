@@ -1,0 +1,151 @@
+"""Generate the golden vectors that pin the oracle to the reference core.
+
+Run in a container that holds the reference sources (default
+``/root/reference/src``, or ``NPOM_REFERENCE_SRC``)::
+
+    python tests/golden/make_golden.py
+
+Writes ``tests/golden/*.npz``.  Every file records the reference's own CPU
+float32 outputs on seeded inputs; nothing here is needed at test time except
+the written fixtures.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import ref_harness as rh  # noqa: E402
+
+# Fields written by one internal step that the golden files keep.
+OUTPUT_FIELDS = (
+    "u", "ub", "v", "vb", "w", "t", "tb", "s", "sb", "rho", "q2", "q2b", "q2l", "q2lb",
+    "km", "kh", "kq", "l", "aam", "advx", "advy", "curv", "drhox", "drhoy",
+    "el", "elb", "elf", "et", "etb", "etf", "d", "dt", "ua", "uab", "uaf", "va", "vab", "vaf",
+    "utf", "utb", "vtf", "vtb", "egf", "egb", "adx2d", "ady2d", "drx2d", "dry2d", "aam2d",
+    "advua", "advva", "fluxua", "fluxva", "wubot", "wvbot", "tps", "wusurf", "wtsurf", "wssurf",
+)
+
+
+def perturbed_core(name, im, jm, seed):
+    """Production-configured reference core, clock at 1000 days (so the first
+    step runs the internal mode, as in the reference's own tests), spun up two
+    steps, then given seeded perturbations on every prognostic field."""
+    import torch
+    core = rh.build_reference_core(name, im, jm)
+    core.time = core.time0 = 1000.0
+    rh.advance(core, name, 2)
+    g = torch.Generator().manual_seed(seed)
+
+    def rn(shape):
+        return torch.randn(shape, generator=g, dtype=torch.float32)
+
+    def ru(shape):
+        return torch.rand(shape, generator=g, dtype=torch.float32)
+
+    fsm3, dum3, dvm3 = core.fsm[:, :, None], core.dum[:, :, None], core.dvm[:, :, None]
+    p3 = rn(core.t.shape)
+    core.t = core.t + 0.5 * p3 * fsm3
+    core.tb = core.tb + 0.45 * p3 * fsm3 + 0.05 * rn(core.t.shape) * fsm3
+    p3 = rn(core.s.shape)
+    core.s = core.s + 0.1 * p3 * fsm3
+    core.sb = core.sb + 0.1 * p3 * fsm3
+    for f, m in (("u", dum3), ("ub", dum3), ("v", dvm3), ("vb", dvm3)):
+        setattr(core, f, getattr(core, f) + 0.05 * rn(core.u.shape) * m)
+    for f, m in (("ua", core.dum), ("uab", core.dum), ("va", core.dvm), ("vab", core.dvm)):
+        setattr(core, f, getattr(core, f) + 0.02 * rn(core.ua.shape) * m)
+    for f in ("el", "elb", "et", "etb"):
+        setattr(core, f, getattr(core, f) + 0.05 * rn(core.el.shape) * core.fsm)
+    core.elf = core.el.clone()
+    core.etf = core.et.clone()
+    core.d = core.h + core.el
+    core.dt = core.h + core.et
+    for f in ("q2", "q2b", "q2l", "q2lb"):
+        cur = getattr(core, f)
+        setattr(core, f, cur * (1.0 + 0.5 * ru(cur.shape)) + 1e-6 * ru(cur.shape))
+    for f in ("km", "kh", "kq"):
+        cur = getattr(core, f)
+        setattr(core, f, cur * (1.0 + 0.3 * ru(cur.shape)))
+    core.aam = core.aam * (1.0 + 0.3 * ru(core.aam.shape))
+    core.wubot = core.wubot + 1e-5 * rn(core.el.shape) * core.dum
+    core.wvbot = core.wvbot + 1e-5 * rn(core.el.shape) * core.dvm
+    return core
+
+
+def make_step_golden(name, im, jm, seed, steps=(1, 3)):
+    import torch
+    core = perturbed_core(name, im, jm, seed)
+    arrays, scalars = rh.extract_state(core)
+    out = {f"in__{k}": v for k, v in arrays.items()}
+    for k, v in scalars.items():
+        out[f"scalar__{k}"] = np.asarray(v)
+    done = 0
+    for n in steps:
+        if hasattr(core, "_eta_solver_iteration_history"):
+            core._eta_solver_iteration_history = []
+        rh.advance(core, name, n - done)
+        done = n
+        a, _ = rh.extract_state(core)
+        for f in OUTPUT_FIELDS:
+            out[f"out{n}__{f}"] = a[f]
+        out[f"out{n}__scalar_time"] = np.asarray(float(core.time))
+        hist = getattr(core, "_eta_solver_iteration_history", None)
+        if hist is not None:
+            out[f"out{n}__cg_iters"] = np.asarray(hist, dtype=np.int32)
+    tag = "explicit" if name == "explicit" else "implicit"
+    path = os.path.join(HERE, f"step_{tag}_{im}x{jm}.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path))
+    _ = torch
+
+
+def make_proft_golden():
+    """Seeded column fixture of the reference's strict-vertical tests
+    (``tests/test_strict_vertical.py:11-21``, seed 817, 3x4 columns, kb=6)
+    passed through the reference ``TracersMixin.proft`` for nbc 1-4."""
+    import torch
+    from neuralpom.cores.implicit_p0_fixed.strict_vertical import _reference
+    out = {}
+    for dtype, tag in ((torch.float64, "f64"), (torch.float32, "f32")):
+        g = torch.Generator().manual_seed(817)
+        kb = 6
+
+        def rnd(shape):
+            return torch.rand(shape, generator=g, dtype=dtype)
+        shape = (3, 4)
+        inputs = [torch.linspace(0, -1, kb, dtype=dtype), 10 + rnd((*shape, kb)), rnd(shape) * 1e-5,
+                  rnd(shape) + 10, 100 + rnd(shape) * 20, rnd(shape) * .1,
+                  torch.full((kb,), 1 / (kb - 1), dtype=dtype), torch.full((kb,), 1 / (kb - 1), dtype=dtype),
+                  rnd(shape) * 1e-4, rnd((*shape, kb)) * 1e-3]
+        names = ("z", "f", "wfsurf", "fsurf", "h", "etf", "dz", "dzz", "swrad", "kh")
+        for n, v in zip(names, inputs):
+            out[f"{tag}__{n}"] = v.numpy()
+        for nbc in (1, 2, 3, 4):
+            res = _reference(inputs, (nbc, 1200., 2, 1e-6))
+            out[f"{tag}__nbc{nbc}__f"] = res[0].numpy()
+            out[f"{tag}__nbc{nbc}__dh"] = res[1].numpy()
+    path = os.path.join(HERE, "proft_strict_fixture.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path))
+
+
+def main():
+    src = rh.default_reference_path()
+    if src is None:
+        raise SystemExit("reference sources not found; set NPOM_REFERENCE_SRC")
+    rh.import_reference(src)
+    import torch
+    torch.set_num_threads(1)
+    make_proft_golden()
+    make_step_golden("explicit", 12, 10, seed=11)
+    make_step_golden("implicit_p0_fixed", 12, 10, seed=12)
+    make_step_golden("implicit_p0_fixed", 20, 18, seed=13, steps=(1,))
+
+
+if __name__ == "__main__":
+    main()
