@@ -1,0 +1,195 @@
+/*
+ * npom.h -- C ABI of the B200 (sm_100a) NeuralPOM physical time step.
+ *
+ * The library advances the state of one POM core (explicit mode-split or
+ * semi-implicit free surface) by whole internal steps, on one GPU, on the
+ * caller's CUDA stream.  All memory is owned by the caller: every field is a
+ * C-contiguous float32 device array laid out like the reference core's
+ * tensors -- 3-D fields (im, jm, kb) with the sigma level k fastest, 2-D
+ * fields (im, jm), 1-D fields (kb) -- and the workspace buffers are caller
+ * allocated too.  No entry point allocates or frees device memory.
+ *
+ * Reference interfaces replaced (paths relative to src/neuralpom/):
+ *   npom_step_explicit  <- cores/explicit/time_loop.py:20 TimeLoopMixin.run_time_loop
+ *   npom_step_implicit  <- cores/implicit_p0_fixed/time_loop.py:38 TimeLoopMixin.run_time_loop
+ *   npom_proft          <- cores/explicit/tracers.py:890 TracersMixin.proft
+ *                          (twin: cores/implicit_p0_fixed/strict_vertical.py:103 _reference)
+ *   npom_pcg_solve      <- cores/implicit_p0_fixed/core.py:775 POM2K_Core.solve_implicit_eta_cg
+ *   npom_run_phase      <- the individual operators of the two time loops
+ *                          (advct baroclinic.py:14, baropg momentum.py:543,
+ *                          advave baroclinic.py:262, vertvl baroclinic.py:930,
+ *                          advq tracers.py:14, profq tracers.py:158,
+ *                          advt1 tracers.py:433, dens momentum.py:467,
+ *                          advu/advv momentum.py:14/133, profu/profv
+ *                          momentum.py:250/359, bcond baroclinic.py:496 and
+ *                          implicit_p0_fixed/boundary/closed_basin.py:27)
+ *
+ * Error model: every entry point returns an npom_status; device-detected
+ * conditions (velocity above vmaxl, a barrier that timed out, PCG at
+ * max_iter) are OR-ed into a device status word that npom_status_read
+ * returns.
+ */
+#ifndef NPOM_H
+#define NPOM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* Fields: one device pointer per reference tensor attribute.          */
+/* ------------------------------------------------------------------ */
+#define NPOM_FIELD_LIST(X)                                                   \
+  /* static 2-D geometry */                                                  \
+  X(h) X(dx) X(dy) X(art) X(aru) X(arv) X(fsm) X(dum) X(dvm) X(cor) X(cbc)   \
+  X(north_e)                                                                 \
+  /* 1-D vertical grid (kb) */                                               \
+  X(z) X(zz) X(dz) X(dzz)                                                    \
+  /* open-boundary arrays of the explicit core (jm / im / (jm,kb) / (im,kb)) */\
+  X(ele) X(elw) X(eln) X(els) X(uabe) X(uabw) X(vabn) X(vabs)                \
+  X(tbe) X(sbe) X(tbw) X(sbw) X(tbn) X(sbn) X(tbs) X(sbs)                    \
+  /* 3-D state */                                                            \
+  X(u) X(ub) X(uf) X(v) X(vb) X(vf) X(w) X(t) X(tb) X(s) X(sb) X(rho)        \
+  X(rmean) X(tclim) X(sclim) X(q2) X(q2b) X(q2l) X(q2lb) X(km) X(kh) X(kq)   \
+  X(l) X(aam) X(advx) X(advy) X(drhox) X(drhoy) X(curv)                      \
+  /* 2-D state */                                                            \
+  X(el) X(elb) X(elf) X(et) X(etb) X(etf) X(d) X(dt) X(ua) X(uab) X(uaf)     \
+  X(va) X(vab) X(vaf) X(utf) X(utb) X(vtf) X(vtb) X(egf) X(egb) X(adx2d)     \
+  X(ady2d) X(drx2d) X(dry2d) X(aam2d) X(advua) X(advva) X(fluxua) X(fluxva)  \
+  X(wubot) X(wvbot) X(wusurf) X(wvsurf) X(wtsurf) X(wssurf) X(vfluxf)        \
+  X(vfluxb) X(swrad) X(e_atmos) X(tps) X(tsurf) X(ssurf)
+
+typedef enum npom_field {
+#define NPOM_X_ENUM(n) NPOM_F_##n,
+  NPOM_FIELD_LIST(NPOM_X_ENUM)
+#undef NPOM_X_ENUM
+  NPOM_NFIELDS
+} npom_field;
+
+/* Workspace buffers (caller-allocated device memory). */
+#define NPOM_WS_LIST(X)                                                      \
+  /* float32, im*jm each */                                                  \
+  X(us) X(vs) X(den_u) X(den_v) X(d_baro) X(rhs) X(x) X(r) X(p) X(zv) X(ap)  \
+  X(ce) X(cw) X(cn) X(cs) X(inv_art) X(diag)                                 \
+  /* float32: DST-I matrices (ni*ni, nj*nj), inverse eigenvalues and two     \
+     transform buffers (ni*nj each) of the spectral preconditioner */        \
+  X(sx) X(sy) X(inv_eigs) X(t1) X(t2)
+
+typedef enum npom_wsbuf {
+#define NPOM_X_ENUM(n) NPOM_W_##n,
+  NPOM_WS_LIST(NPOM_X_ENUM)
+#undef NPOM_X_ENUM
+  NPOM_NWS
+} npom_wsbuf;
+
+typedef struct npom_workspace {
+  float *buf[NPOM_NWS];
+  double *partials;        /* >= 4 * NPOM_MAX_COOP_BLOCKS doubles          */
+  unsigned int *sync;      /* >= 4 unsigned ints, zero before first use    */
+  unsigned int *status;    /* >= 1 unsigned int: OR of NPOM_ERR_* bits     */
+  int *cg_iters;           /* >= nsteps ints: PCG iterations of each step  */
+} npom_workspace;
+
+#define NPOM_MAX_COOP_BLOCKS 1024
+
+/* ------------------------------------------------------------------ */
+/* Scalar settings (the Python attributes of the reference BaseCore).  */
+/* ------------------------------------------------------------------ */
+typedef struct npom_params {
+  int32_t device;          /* CUDA device ordinal the pointers live on     */
+  int32_t im, jm, kb;
+  int32_t core;            /* NPOM_CORE_EXPLICIT / NPOM_CORE_IMPLICIT      */
+  int32_t isplit, ispadv, nbct, nbcs, ntp, mode, nadv;
+  int32_t eta_max_iter;
+  int32_t eta_precond;     /* NPOM_PRECOND_JACOBI / NPOM_PRECOND_SPECTRAL  */
+  int32_t wind_forcing;    /* implicit: rewrite wusurf/wvsurf every step   */
+  int32_t has_vmix;        /* clamp kh/km/kq to [0, vmix]                  */
+  int32_t lramp;
+  double dti, dte, dti2, dte2, ispi, isp2i;
+  double alpha, smoth, horcon, grav, umol, tprni, small, kappa, rhoref;
+  double tbias, sbias, vmaxl, hmax, rfe, rfw, rfn, rfs, aam_min, pi;
+  double eta_tol, eta_rel_tol, barotropic_shapiro, tracer_shapiro;
+  double velocity_shapiro, wind_tau0, vmix;
+  double period;           /* inertial period in days (ramp = time/period) */
+  double inverse_scale;    /* spectral preconditioner: 4 (ni+1)(nj+1)      */
+} npom_params;
+
+enum { NPOM_CORE_EXPLICIT = 0, NPOM_CORE_IMPLICIT = 1 };
+enum { NPOM_PRECOND_JACOBI = 0, NPOM_PRECOND_SPECTRAL = 1 };
+
+/* Return codes. */
+typedef enum npom_status {
+  NPOM_OK = 0,
+  NPOM_ERR_ARG = 1,        /* bad argument (null pointer, size, kb)        */
+  NPOM_ERR_CUDA = 2,       /* a CUDA runtime call failed                   */
+  NPOM_ERR_DEVICE = 3      /* the device status word is non-zero           */
+} npom_status;
+
+/* Device status bits. */
+#define NPOM_DEV_VMAX      0x1u  /* |vaf| > vmaxl in an external step     */
+#define NPOM_DEV_TIMEOUT   0x2u  /* a grid barrier wait ran out            */
+#define NPOM_DEV_PCG_MAXIT 0x4u  /* PCG reached eta_max_iter               */
+#define NPOM_DEV_NONFINITE 0x8u  /* a non-finite elevation was produced    */
+
+/* Per-call clock: the reference's time/time0/iint bookkeeping. */
+typedef struct npom_clock {
+  double time0;            /* clock at the start of the call (days)        */
+  int32_t first_iint;      /* iint of the first step (1 for a fresh call)  */
+  int32_t nsteps;
+} npom_clock;
+
+/* Library identity and layout checks (used by the host bindings). */
+int npom_abi_version(void);
+int npom_field_count(void);
+const char *npom_field_name(int index);
+int npom_ws_count(void);
+const char *npom_ws_name(int index);
+size_t npom_params_size(void);
+size_t npom_workspace_struct_size(void);
+
+/* Advance nsteps internal steps of the explicit mode-split core. */
+npom_status npom_step_explicit(const npom_params *p, float *const *fields,
+                               const npom_workspace *ws, const npom_clock *clk,
+                               void *stream);
+
+/* Advance nsteps internal steps of the semi-implicit free-surface core. */
+npom_status npom_step_implicit(const npom_params *p, float *const *fields,
+                               const npom_workspace *ws, const npom_clock *clk,
+                               void *stream);
+
+/* Run one named phase of a step on the current state (operator tests). */
+npom_status npom_run_phase(const npom_params *p, float *const *fields,
+                           const npom_workspace *ws, int phase, double ramp,
+                           void *stream);
+int npom_phase_count(void);
+const char *npom_phase_name(int index);
+
+/* Implicit vertical diffusion of ncol tracer columns of kb levels
+ * (kb <= 64), boundary type nbc 1-4, exactly like TracersMixin.proft:
+ * f_out may alias f_in; dh_out receives h + etf. */
+npom_status npom_proft(int ncol, int kb, const float *f_in, const float *wfsurf,
+                       const float *fsurf, int nbc, const float *h,
+                       const float *etf, double dti2, const float *dz,
+                       const float *dzz, const float *swrad, int ntp,
+                       const float *kh, double umol, const float *z,
+                       float *f_out, float *dh_out, void *stream);
+
+/* One PCG free-surface solve: fields[elf] holds the initial guess on entry
+ * and the solution on exit (before the Shapiro filter / boundary); rhs is
+ * read from ws->buf[NPOM_W_rhs].  Iterations go to ws->cg_iters[0]. */
+npom_status npom_pcg_solve(const npom_params *p, float *const *fields,
+                           const npom_workspace *ws, void *stream);
+
+/* Reads (and with clear != 0 zeroes) the device status word; blocks on
+ * the stream. */
+npom_status npom_status_read(const npom_workspace *ws, int clear,
+                             unsigned int *out_bits, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NPOM_H */

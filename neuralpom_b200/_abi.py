@@ -1,0 +1,162 @@
+"""ctypes mirror of ``include/npom.h`` and the loader of the CUDA library.
+
+The struct layouts and name lists here must match the header; the library
+exports its own field/workspace names and struct sizes so that a mismatch is
+caught at load time (``check_layout``).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+FIELD_NAMES = (
+    "h dx dy art aru arv fsm dum dvm cor cbc north_e "
+    "z zz dz dzz "
+    "ele elw eln els uabe uabw vabn vabs tbe sbe tbw sbw tbn sbn tbs sbs "
+    "u ub uf v vb vf w t tb s sb rho rmean tclim sclim q2 q2b q2l q2lb km kh kq l aam advx advy drhox drhoy curv "
+    "el elb elf et etb etf d dt ua uab uaf va vab vaf utf utb vtf vtb egf egb adx2d ady2d drx2d dry2d aam2d "
+    "advua advva fluxua fluxva wubot wvbot wusurf wvsurf wtsurf wssurf vfluxf vfluxb swrad e_atmos tps tsurf ssurf"
+).split()
+
+WS_NAMES = "us vs den_u den_v d_baro rhs x r p zv ap ce cw cn cs inv_art diag sx sy inv_eigs t1 t2".split()
+
+PHASES = ("A1_forcing_advct", "A2_baropg_smag_means", "A3_advave_predictor", "E_external",
+          "I5_corrector_filter", "B1_barotropic_fix", "B2A_vertvl", "B2B_advq", "B3_profq",
+          "B4_edges_bcond6", "B5_qfilter_advt1", "B6_proft", "B7_tsfilter_dens", "B8_advuv_profuv",
+          "B9_velfilter_shift")
+
+FIELDS_1D_K = ("z", "zz", "dz", "dzz")
+FIELDS_EDGE_J = ("ele", "elw", "uabe", "uabw")
+FIELDS_EDGE_I = ("eln", "els", "vabn", "vabs")
+FIELDS_EDGE_JK = ("tbe", "sbe", "tbw", "sbw")
+FIELDS_EDGE_IK = ("tbn", "sbn", "tbs", "sbs")
+FIELDS_3D = tuple("u ub uf v vb vf w t tb s sb rho rmean tclim sclim q2 q2b q2l q2lb km kh kq l aam advx advy "
+                  "drhox drhoy curv".split())
+
+CORE_EXPLICIT, CORE_IMPLICIT = 0, 1
+PRECOND_JACOBI, PRECOND_SPECTRAL = 0, 1
+DEV_VMAX, DEV_TIMEOUT, DEV_PCG_MAXIT, DEV_NONFINITE = 0x1, 0x2, 0x4, 0x8
+MAX_COOP_BLOCKS = 1024
+
+
+def field_shape(name, im, jm, kb):
+    if name in FIELDS_3D:
+        return (im, jm, kb)
+    if name in FIELDS_1D_K:
+        return (kb,)
+    if name in FIELDS_EDGE_J:
+        return (jm,)
+    if name in FIELDS_EDGE_I:
+        return (im,)
+    if name in FIELDS_EDGE_JK:
+        return (jm, kb)
+    if name in FIELDS_EDGE_IK:
+        return (im, kb)
+    return (im, jm)
+
+
+def ws_shape(name, im, jm):
+    ni, nj = im - 2, jm - 2
+    if name == "sx":
+        return (ni, ni)
+    if name == "sy":
+        return (nj, nj)
+    if name in ("inv_eigs", "t1", "t2"):
+        return (ni, nj)
+    return (im, jm)
+
+
+class NpomParams(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in (
+        "device", "im", "jm", "kb", "core", "isplit", "ispadv", "nbct", "nbcs", "ntp", "mode", "nadv",
+        "eta_max_iter", "eta_precond", "wind_forcing", "has_vmix", "lramp")] + [
+        (n, ctypes.c_double) for n in (
+            "dti", "dte", "dti2", "dte2", "ispi", "isp2i", "alpha", "smoth", "horcon", "grav", "umol", "tprni",
+            "small", "kappa", "rhoref", "tbias", "sbias", "vmaxl", "hmax", "rfe", "rfw", "rfn", "rfs", "aam_min",
+            "pi", "eta_tol", "eta_rel_tol", "barotropic_shapiro", "tracer_shapiro", "velocity_shapiro",
+            "wind_tau0", "vmix", "period", "inverse_scale")]
+
+
+class NpomWorkspace(ctypes.Structure):
+    _fields_ = [("buf", ctypes.c_void_p * len(WS_NAMES)), ("partials", ctypes.c_void_p),
+                ("sync", ctypes.c_void_p), ("status", ctypes.c_void_p), ("cg_iters", ctypes.c_void_p)]
+
+
+class NpomClock(ctypes.Structure):
+    _fields_ = [("time0", ctypes.c_double), ("first_iint", ctypes.c_int32), ("nsteps", ctypes.c_int32)]
+
+
+FieldArray = ctypes.c_void_p * len(FIELD_NAMES)
+
+STATUS_NAMES = {0: "NPOM_OK", 1: "NPOM_ERR_ARG", 2: "NPOM_ERR_CUDA", 3: "NPOM_ERR_DEVICE"}
+
+
+def library_path():
+    return os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libnpom_b200.so")
+
+
+_LIB = None
+
+
+def load_library():
+    """Load ``libnpom_b200.so`` and declare its signatures.  Raises if the
+    library has not been built -- there is no other implementation."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = library_path()
+    if not os.path.exists(path):
+        raise RuntimeError(f"neuralpom_b200 CUDA library missing at {path}; run `python -m neuralpom_b200.build`")
+    lib = ctypes.CDLL(path)
+    vp, i32, dbl = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    P = ctypes.POINTER
+    lib.npom_abi_version.restype = i32
+    lib.npom_field_count.restype = i32
+    lib.npom_field_name.restype = ctypes.c_char_p
+    lib.npom_field_name.argtypes = [i32]
+    lib.npom_ws_count.restype = i32
+    lib.npom_ws_name.restype = ctypes.c_char_p
+    lib.npom_ws_name.argtypes = [i32]
+    lib.npom_params_size.restype = ctypes.c_size_t
+    lib.npom_workspace_struct_size.restype = ctypes.c_size_t
+    lib.npom_phase_count.restype = i32
+    lib.npom_phase_name.restype = ctypes.c_char_p
+    lib.npom_phase_name.argtypes = [i32]
+    for name in ("npom_step_explicit", "npom_step_implicit"):
+        fn = getattr(lib, name)
+        fn.restype = i32
+        fn.argtypes = [P(NpomParams), P(FieldArray), P(NpomWorkspace), P(NpomClock), vp]
+    lib.npom_run_phase.restype = i32
+    lib.npom_run_phase.argtypes = [P(NpomParams), P(FieldArray), P(NpomWorkspace), i32, dbl, vp]
+    lib.npom_pcg_solve.restype = i32
+    lib.npom_pcg_solve.argtypes = [P(NpomParams), P(FieldArray), P(NpomWorkspace), vp]
+    lib.npom_proft.restype = i32
+    lib.npom_proft.argtypes = [i32, i32, vp, vp, vp, i32, vp, vp, dbl, vp, vp, vp, i32, vp, dbl, vp, vp, vp, vp]
+    lib.npom_status_read.restype = i32
+    lib.npom_status_read.argtypes = [P(NpomWorkspace), i32, P(ctypes.c_uint), vp]
+    check_layout(lib)
+    _LIB = lib
+    return lib
+
+
+def check_layout(lib):
+    """The library's field/workspace lists and struct sizes must match this
+    module's, or every pointer would land in the wrong slot."""
+    names = [lib.npom_field_name(i).decode() for i in range(lib.npom_field_count())]
+    if names != list(FIELD_NAMES):
+        raise RuntimeError("npom field list mismatch between include/npom.h and neuralpom_b200._abi")
+    ws = [lib.npom_ws_name(i).decode() for i in range(lib.npom_ws_count())]
+    if ws != list(WS_NAMES):
+        raise RuntimeError("npom workspace list mismatch")
+    if lib.npom_params_size() != ctypes.sizeof(NpomParams):
+        raise RuntimeError("npom_params size mismatch")
+    if lib.npom_workspace_struct_size() != ctypes.sizeof(NpomWorkspace):
+        raise RuntimeError("npom_workspace size mismatch")
+    phases = [lib.npom_phase_name(i).decode() for i in range(lib.npom_phase_count())]
+    if tuple(phases) != PHASES:
+        raise RuntimeError("npom phase list mismatch")
+
+
+def check(status, what):
+    if status != 0:
+        raise RuntimeError(f"{what} failed: {STATUS_NAMES.get(status, status)}")

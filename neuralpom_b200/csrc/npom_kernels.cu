@@ -1,0 +1,631 @@
+// npom_kernels.cu -- CUDA kernels for sm_100a and the C ABI of include/npom.h.
+//
+// A step is a fixed sequence of launches on the caller's stream:
+//
+//   A1  points   forcing + ADVCT                              (all cores)
+//   A2  columns  BAROPG + Smagorinsky + depth integrals
+//   A3  cells    rho round trip + ADVAVE + predictor (implicit)
+//   E   coop     explicit: fused 30-substep external mode (3 grid barriers
+//                per substep); implicit: fused PCG free-surface solve
+//   I5  cells    implicit corrector + Robert-Asselin + shifts
+//   B1..B9       internal mode (skipped on the very first step from rest)
+//
+// The cooperative kernels (PCG, external subcycle) keep every block resident
+// (cudaLaunchCooperativeKernel) and synchronise through a sense-counting
+// grid barrier whose waits are bounded in time: a wait that runs out sets
+// NPOM_DEV_TIMEOUT and the kernel returns instead of hanging.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "npom_phases_int.cuh"
+#include "npom_host.cuh"
+
+using namespace npom;
+
+namespace {
+
+constexpr int kThreads = 256;
+
+// ---------------------------------------------------------------------------
+// generic launch shapes
+// ---------------------------------------------------------------------------
+enum PointPhase { PP_A1 = 0, PP_B2B = 1, PP_B4 = 2, PP_B5 = 3, PP_B7 = 4 };
+enum ColPhase { CP_A2 = 0, CP_B1 = 1, CP_B2A = 2, CP_B3 = 3, CP_B6 = 4, CP_B8 = 5, CP_B9 = 6 };
+enum CellPhase { XP_A3 = 0, XP_I5 = 1, XP_COEF = 2 };
+
+template <int PH>
+__global__ void __launch_bounds__(kThreads) k_points(Ctx c) {
+  const size_t n = (size_t)c.im * c.jm * c.kb;
+  size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  int k = (int)(p % c.kb);
+  size_t col = p / c.kb;
+  int j = (int)(col % c.jm);
+  int i = (int)(col / c.jm);
+  if (PH == PP_A1) {
+    float ax, ay, cv;
+    advct_point(c, i, j, k, ax, ay, cv);
+    P3(advx, i, j, k) = ax;
+    P3(advy, i, j, k) = ay;
+    P3(curv, i, j, k) = cv;
+    if (k == 0) forcing_cell(c, i, j);
+  } else if (PH == PP_B2B) {
+    phase_b2b_point(c, i, j, k);
+  } else if (PH == PP_B4) {
+    phase_b4_point(c, i, j, k);
+  } else if (PH == PP_B5) {
+    phase_b5_point(c, i, j, k);
+  } else if (PH == PP_B7) {
+    phase_b7_point(c, i, j, k);
+  }
+}
+
+template <int PH>
+__global__ void __launch_bounds__(128) k_cols(Ctx c) {
+  const int n = c.im * c.jm;
+  int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= n) return;
+  int j = col % c.jm, i = col / c.jm;
+  if (PH == CP_A2) phase_a2_column(c, i, j);
+  else if (PH == CP_B1) phase_b1_column(c, i, j);
+  else if (PH == CP_B2A) phase_b2a_column(c, i, j);
+  else if (PH == CP_B3) phase_b3_column(c, i, j);
+  else if (PH == CP_B6) phase_b6_column(c, i, j);
+  else if (PH == CP_B8) phase_b8_column(c, i, j);
+  else if (PH == CP_B9) phase_b9_column(c, i, j);
+}
+
+template <int PH>
+__global__ void __launch_bounds__(kThreads) k_cells(Ctx c) {
+  const int n = c.im * c.jm;
+  int cell = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= n) return;
+  int j = cell % c.jm, i = cell / c.jm;
+  if (PH == XP_A3) {
+    phase_a3_cell(c, i, j);
+  } else if (PH == XP_I5) {
+    if (phase_i5_cell(c, i, j)) atomicOr(c.status, NPOM_DEV_VMAX);
+  } else if (PH == XP_COEF) {
+    elliptic_coeff_cell(c, i, j);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// bounded grid barrier (all blocks co-resident: cooperative launch)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s
+
+// sync[0] = arrival counter, sync[1] = generation.  Returns false after a
+// timeout (or once any block has timed out); the caller then returns.
+__device__ bool grid_barrier(const Ctx &c) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ok = 1;
+    volatile unsigned int *gen = c.sync + 1;
+    unsigned int my_gen = *gen;
+    __threadfence();
+    unsigned int arrived = atomicAdd(c.sync, 1u);
+    if (arrived == gridDim.x - 1) {
+      atomicExch(c.sync, 0u);
+      __threadfence();
+      atomicAdd(c.sync + 1, 1u);
+    } else {
+      unsigned long long t0 = globaltimer_ns();
+      unsigned int spins = 0;
+      while (*gen == my_gen) {
+        if ((++spins & 63u) == 0) {
+          if (*(volatile unsigned int *)c.status & NPOM_DEV_TIMEOUT) {
+            ok = 0;
+            break;
+          }
+          if (globaltimer_ns() - t0 > kBarrierTimeoutNs) {
+            atomicOr(c.status, NPOM_DEV_TIMEOUT);
+            ok = 0;
+            break;
+          }
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// block-wide FP64 sum of three values, result written to partials[slot*G+b]
+__device__ void block_sum3(const Ctx &c, double a0, double a1, double a2, int s0, int s1, int s2) {
+  __shared__ double red[3][kThreads / 32];
+  for (int off = 16; off > 0; off >>= 1) {
+    a0 += __shfl_down_sync(0xffffffffu, a0, off);
+    a1 += __shfl_down_sync(0xffffffffu, a1, off);
+    a2 += __shfl_down_sync(0xffffffffu, a2, off);
+  }
+  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+    red[0][w] = a0;
+    red[1][w] = a1;
+    red[2][w] = a2;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
+      t0 += red[0][q];
+      t1 += red[1][q];
+      t2 += red[2][q];
+    }
+    const int G = gridDim.x;
+    if (s0 >= 0) c.partials[s0 * G + blockIdx.x] = t0;
+    if (s1 >= 0) c.partials[s1 * G + blockIdx.x] = t1;
+    if (s2 >= 0) c.partials[s2 * G + blockIdx.x] = t2;
+  }
+  __syncthreads();
+}
+
+// sum of one partial slot over blocks, identical in every block
+__device__ double grid_total(const Ctx &c, int slot) {
+  __shared__ double tot;
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    const int G = gridDim.x;
+    for (int b = 0; b < G; ++b) t += __ldcg(c.partials + slot * G + b);
+    tot = t;
+  }
+  __syncthreads();
+  double r = tot;
+  __syncthreads();
+  return r;
+}
+
+// z = M^-1 r over the interior; returns after its own trailing barrier.
+// Accumulates r.z into *rz of this thread.
+__device__ bool precondition(const Ctx &c, double &rz) {
+  const int ni = c.im - 2, nj = c.jm - 2;
+  const size_t nint = (size_t)ni * nj;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  float *zv = c.W[NPOM_W_zv];
+  const float *r = c.W[NPOM_W_r];
+  rz = 0.0;
+  if (c.k.eta_precond == NPOM_PRECOND_SPECTRAL) {
+    float *t1 = c.W[NPOM_W_t1], *t2 = c.W[NPOM_W_t2];
+    for (size_t q = tid; q < nint; q += stride) {
+      int a = (int)(q / nj), b = (int)(q % nj);
+      t1[q] = dst_stage_i(c, r, true, a, b);
+    }
+    if (!grid_barrier(c)) return false;
+    for (size_t q = tid; q < nint; q += stride) {
+      int a = (int)(q / nj), b = (int)(q % nj);
+      t2[q] = dst_stage_j(c, t1, a, b) * ld(c.W[NPOM_W_inv_eigs] + q);
+    }
+    if (!grid_barrier(c)) return false;
+    for (size_t q = tid; q < nint; q += stride) {
+      int a = (int)(q / nj), b = (int)(q % nj);
+      t1[q] = dst_stage_i(c, t2, false, a, b);
+    }
+    if (!grid_barrier(c)) return false;
+    for (size_t q = tid; q < nint; q += stride) {
+      int a = (int)(q / nj), b = (int)(q % nj);
+      float zval = dst_stage_j(c, t1, a, b) / c.k.inverse_scale;
+      size_t o = NPOM_I2(c, a + 1, b + 1);
+      zv[o] = zval;
+      rz += (double)ld(r + o) * (double)zval;
+    }
+  } else {
+    for (size_t q = tid; q < nint; q += stride) {
+      int a = (int)(q / nj), b = (int)(q % nj);
+      size_t o = NPOM_I2(c, a + 1, b + 1);
+      float rv = ld(r + o);
+      float zval = rv / (ld(c.W[NPOM_W_diag] + o) + 1e-30f);
+      zv[o] = zval;
+      rz += (double)rv * (double)zval;
+    }
+  }
+  return true;
+}
+
+// Fused PCG free-surface solve (core.py:460-589, eager branch), followed by
+// the Shapiro filter and closed-basin bcond 1 (core.py:893-916) and
+// d = h + elf.  Iterations -> c.cg_iters[step].
+__global__ void __launch_bounds__(kThreads) k_pcg(Ctx c, int step, int with_rhs, int with_post) {
+  const int im = c.im, jm = c.jm, ni = im - 2, nj = jm - 2;
+  const size_t ncell = (size_t)im * jm, nint = (size_t)ni * nj;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  float *x = c.W[NPOM_W_x], *r = c.W[NPOM_W_r], *p = c.W[NPOM_W_p], *zv = c.W[NPOM_W_zv];
+  float *ap = c.W[NPOM_W_ap], *rhs = c.W[NPOM_W_rhs];
+  const float *elf = c.F[NPOM_F_elf];
+  // setup: rhs (+ stored transports), initial guess with zero ring, zeroed
+  // ring of every work vector
+  for (size_t q = tid; q < ncell; q += stride) {
+    int i = (int)(q / jm), j = (int)(q % jm);
+    if (with_rhs) {
+      rhs[q] = rhs_cell(c, i, j);
+      P2(fluxua, i, j) = rhs_fluxua(c, i, j);
+      P2(fluxva, i, j) = rhs_fluxva(c, i, j);
+    } else if (!interior(c, i, j)) {
+      rhs[q] = 0.0f;
+    }
+    bool in = interior(c, i, j);
+    x[q] = in ? ld(elf + q) : 0.0f;
+    if (!in) {
+      r[q] = 0.0f;
+      p[q] = 0.0f;
+      zv[q] = 0.0f;
+      ap[q] = 0.0f;
+    }
+  }
+  if (!grid_barrier(c)) return;
+  double rr = 0.0;
+  for (size_t q = tid; q < nint; q += stride) {
+    int i = (int)(q / nj) + 1, j = (int)(q % nj) + 1;
+    size_t o = NPOM_I2(c, i, j);
+    float a = elliptic_apply_cell(c, x, i, j);
+    float rv = ld(rhs + o) - a;
+    r[o] = rv;
+    rr += (double)rv * (double)rv;
+    if (c.k.eta_precond != NPOM_PRECOND_SPECTRAL) c.W[NPOM_W_diag][o] = jacobi_diag_cell(c, i, j);
+  }
+  block_sum3(c, rr, 0.0, 0.0, 1, -1, -1);
+  if (!grid_barrier(c)) return;
+  double rz;
+  if (!precondition(c, rz)) return;
+  block_sum3(c, rz, 0.0, 0.0, 2, -1, -1);
+  if (!grid_barrier(c)) return;
+  double rs0 = grid_total(c, 1);
+  double rho_old = grid_total(c, 2);
+  for (size_t q = tid; q < nint; q += stride) {
+    size_t o = NPOM_I2(c, (int)(q / nj) + 1, (int)(q % nj) + 1);
+    p[o] = ld(zv + o);
+  }
+  const double tol_sq = c.k.eta_tol * c.k.eta_tol;
+  const double rel_sq = c.k.eta_rel_tol * c.k.eta_rel_tol * (rs0 > 1e-30 ? rs0 : 1e-30);
+  int its = 0;
+  bool converged = false;
+  if (!grid_barrier(c)) return;
+  for (int it = 1; it <= c.k.eta_max_iter; ++it) {
+    double pap = 0.0;
+    for (size_t q = tid; q < nint; q += stride) {
+      int i = (int)(q / nj) + 1, j = (int)(q % nj) + 1;
+      size_t o = NPOM_I2(c, i, j);
+      float a = elliptic_apply_cell(c, p, i, j);
+      ap[o] = a;
+      pap += (double)ld(p + o) * (double)a;
+    }
+    block_sum3(c, pap, 0.0, 0.0, 0, -1, -1);
+    if (!grid_barrier(c)) return;
+    double denom = grid_total(c, 0);
+    float alpha = (float)(rho_old / (denom + 1e-30));
+    double rs = 0.0;
+    for (size_t q = tid; q < nint; q += stride) {
+      size_t o = NPOM_I2(c, (int)(q / nj) + 1, (int)(q % nj) + 1);
+      x[o] = ld(x + o) + alpha * ld(p + o);
+      float rv = ld(r + o) - alpha * ld(ap + o);
+      r[o] = rv;
+      rs += (double)rv * (double)rv;
+    }
+    block_sum3(c, rs, 0.0, 0.0, 1, -1, -1);
+    if (!grid_barrier(c)) return;
+    double rsn = grid_total(c, 1);
+    its = it;
+    if (rsn <= tol_sq || rsn <= rel_sq || rsn <= 1e-30) {
+      converged = true;
+      break;
+    }
+    if (!precondition(c, rz)) return;
+    block_sum3(c, rz, 0.0, 0.0, 2, -1, -1);
+    if (!grid_barrier(c)) return;
+    double rho_new = grid_total(c, 2);
+    float beta = (float)(rho_new / (rho_old + 1e-30));
+    for (size_t q = tid; q < nint; q += stride) {
+      size_t o = NPOM_I2(c, (int)(q / nj) + 1, (int)(q % nj) + 1);
+      p[o] = ld(p + o) * beta + ld(zv + o);
+    }
+    rho_old = rho_new;
+    if (!grid_barrier(c)) return;
+  }
+  if (tid == 0) {
+    c.cg_iters[step] = its;
+    if (!converged) atomicOr(c.status, NPOM_DEV_PCG_MAXIT);
+  }
+  if (!grid_barrier(c)) return;
+  if (!with_post) {
+    // raw solution into elf (the ring of x is zero)
+    for (size_t q = tid; q < ncell; q += stride) c.F[NPOM_F_elf][q] = ld(x + q);
+    return;
+  }
+  for (size_t q = tid; q < ncell; q += stride) {
+    int i = (int)(q / jm), j = (int)(q % jm);
+    float e = 0.0f;
+    if (interior(c, i, j)) {
+      float x0 = ld(x + q);
+      float sm = x0 + c.k.bshap_q * (ld(x + q + jm) + ld(x + q - jm) + ld(x + q + 1) + ld(x + q - 1) - 4.0f * x0);
+      float fsm = F2(fsm, i, j);
+      e = (sm * fsm) * fsm;
+      if (!(fabsf(e) <= 3.0e38f)) atomicOr(c.status, NPOM_DEV_NONFINITE);
+    }
+    c.F[NPOM_F_elf][q] = e;
+    c.F[NPOM_F_d][q] = F2(h, i, j) + e;
+  }
+}
+
+// Fused external mode of the explicit core: isplit substeps, three phases
+// each (explicit/time_loop.py:292-431).
+__global__ void __launch_bounds__(kThreads) k_subcycle(Ctx c) {
+  const size_t ncell = (size_t)c.im * c.jm;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int iext = 1; iext <= c.k.isplit; ++iext) {
+    bool adv = (iext % c.k.ispadv) == 0;
+    for (size_t q = tid; q < ncell; q += stride) ext_phase1_cell(c, (int)(q / c.jm), (int)(q % c.jm), adv);
+    if (!grid_barrier(c)) return;
+    bool exceed = false;
+    for (size_t q = tid; q < ncell; q += stride) exceed |= ext_phase2_cell(c, (int)(q / c.jm), (int)(q % c.jm), iext);
+    if (exceed) atomicOr(c.status, NPOM_DEV_VMAX);
+    if (!grid_barrier(c)) return;
+    for (size_t q = tid; q < ncell; q += stride) ext_phase3_cell(c, (int)(q / c.jm), (int)(q % c.jm), iext);
+    if (!grid_barrier(c)) return;
+  }
+}
+
+// PROFT over independent columns (TracersMixin.proft, any kb <= KMAX)
+__global__ void __launch_bounds__(128) k_proft(int ncol, int kb, const float *f_in, const float *wfsurf,
+                                               const float *fsurf, int nbc, const float *h, const float *etf,
+                                               float dti2, const float *dz, const float *dzz, const float *swrad,
+                                               int ntp, const float *kh, float umol, const float *z, float *f_out,
+                                               float *dh_out) {
+  int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= ncol) return;
+  ProftCol q;
+  q.f = f_in + (size_t)col * kb;
+  float tmp[KMAX];
+  q.out = tmp;
+  q.kh = kh + (size_t)col * kb;
+  q.dz = dz;
+  q.dzz = dzz;
+  q.z = z;
+  q.kb = kb;
+  q.nbc = nbc;
+  q.ntp = ntp;
+  q.dti2 = dti2;
+  q.umol = umol;
+  q.h = h[col];
+  q.etf = etf[col];
+  q.swrad = swrad[col];
+  q.wfsurf = wfsurf[col];
+  q.fsurf = fsurf[col];
+  float dh = proft_column(q);
+  for (int k = 0; k < kb; ++k) f_out[(size_t)col * kb + k] = tmp[k];
+  dh_out[col] = dh;
+}
+
+// ---------------------------------------------------------------------------
+// host helpers
+// ---------------------------------------------------------------------------
+bool check_args_dev(const npom_params *p, float *const *fields, const npom_workspace *ws) {
+  if (!check_args(p, fields, ws)) return false;
+  return cudaSetDevice(p->device) == cudaSuccess;
+}
+
+int blocks_for(size_t n, int threads) { return (int)((n + threads - 1) / threads); }
+
+cudaError_t coop_blocks(const void *fn, size_t work, int *out) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, 0);
+  if (e != cudaSuccess) return e;
+  int want = std::max(1, blocks_for(work, kThreads));
+  int cap = std::max(1, std::min(per_sm * sms, NPOM_MAX_COOP_BLOCKS));
+  *out = std::min(want, cap);
+  return cudaSuccess;
+}
+
+cudaError_t launch_coop(const void *fn, int blocks, void **args, cudaStream_t s) {
+  return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(kThreads), args, 0, s);
+}
+
+template <int PH>
+void launch_points(const Ctx &c, cudaStream_t s) {
+  size_t n = (size_t)c.im * c.jm * c.kb;
+  k_points<PH><<<blocks_for(n, kThreads), kThreads, 0, s>>>(c);
+}
+template <int PH>
+void launch_cols(const Ctx &c, cudaStream_t s) {
+  size_t n = (size_t)c.im * c.jm;
+  k_cols<PH><<<blocks_for(n, 128), 128, 0, s>>>(c);
+}
+template <int PH>
+void launch_cells(const Ctx &c, cudaStream_t s) {
+  size_t n = (size_t)c.im * c.jm;
+  k_cells<PH><<<blocks_for(n, kThreads), kThreads, 0, s>>>(c);
+}
+
+cudaError_t run_pcg(Ctx &c, int step, int with_rhs, int with_post, cudaStream_t s) {
+  int blocks = 0;
+  cudaError_t e = coop_blocks((const void *)k_pcg, (size_t)(c.im - 2) * (c.jm - 2), &blocks);
+  if (e != cudaSuccess) return e;
+  void *args[] = {&c, &step, &with_rhs, &with_post};
+  return launch_coop((const void *)k_pcg, blocks, args, s);
+}
+
+cudaError_t run_subcycle(Ctx &c, cudaStream_t s) {
+  int blocks = 0;
+  cudaError_t e = coop_blocks((const void *)k_subcycle, (size_t)c.im * c.jm, &blocks);
+  if (e != cudaSuccess) return e;
+  void *args[] = {&c};
+  return launch_coop((const void *)k_subcycle, blocks, args, s);
+}
+
+void internal_mode(const Ctx &c, cudaStream_t s) {
+  launch_cols<CP_B1>(c, s);
+  launch_cols<CP_B2A>(c, s);
+  launch_points<PP_B2B>(c, s);
+  launch_cols<CP_B3>(c, s);
+  launch_points<PP_B4>(c, s);
+  launch_points<PP_B5>(c, s);
+  launch_cols<CP_B6>(c, s);
+  launch_points<PP_B7>(c, s);
+  launch_cols<CP_B8>(c, s);
+}
+
+npom_status run_steps(const npom_params *p, float *const *fields, const npom_workspace *ws, const npom_clock *clk,
+                      void *stream, int core) {
+  if (!check_args_dev(p, fields, ws) || !clk || clk->nsteps < 0 || p->core != core) return NPOM_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  Ctx c = make_ctx(p, fields, ws);
+  // a barrier that timed out may leave its arrival counter non-zero
+  if (cudaMemsetAsync(ws->sync, 0, 2 * sizeof(unsigned int), s) != cudaSuccess) return NPOM_ERR_CUDA;
+  if (core == NPOM_CORE_IMPLICIT) {
+    launch_cells<XP_COEF>(c, s);
+  }
+  for (int n = 0; n < clk->nsteps; ++n) {
+    int iint = clk->first_iint + n;
+    double time = p->dti * iint * 1.0 / 86400.0 + clk->time0;
+    c.ramp = ramp_of(p, time);
+    c.do_internal = ((iint != 1 || clk->time0 != 0.0) && p->mode != 2) ? 1 : 0;
+    launch_points<PP_A1>(c, s);
+    launch_cols<CP_A2>(c, s);
+    launch_cells<XP_A3>(c, s);
+    cudaError_t e;
+    if (core == NPOM_CORE_IMPLICIT) {
+      e = run_pcg(c, n, 1, 1, s);
+      if (e != cudaSuccess) return NPOM_ERR_CUDA;
+      launch_cells<XP_I5>(c, s);
+    } else {
+      e = run_subcycle(c, s);
+      if (e != cudaSuccess) return NPOM_ERR_CUDA;
+    }
+    if (c.do_internal) internal_mode(c, s);
+    launch_cols<CP_B9>(c, s);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return NPOM_ERR_CUDA;
+  }
+  return NPOM_OK;
+}
+
+const char *kFieldNames[] = {
+#define NPOM_X_NAME(n) #n,
+    NPOM_FIELD_LIST(NPOM_X_NAME)
+#undef NPOM_X_NAME
+};
+const char *kWsNames[] = {
+#define NPOM_X_NAME(n) #n,
+    NPOM_WS_LIST(NPOM_X_NAME)
+#undef NPOM_X_NAME
+};
+const char *kPhaseNames[] = {"A1_forcing_advct", "A2_baropg_smag_means", "A3_advave_predictor", "E_external",
+                             "I5_corrector_filter", "B1_barotropic_fix",  "B2A_vertvl",          "B2B_advq",
+                             "B3_profq",            "B4_edges_bcond6",    "B5_qfilter_advt1",    "B6_proft",
+                             "B7_tsfilter_dens",    "B8_advuv_profuv",    "B9_velfilter_shift"};
+constexpr int kNumPhases = (int)(sizeof(kPhaseNames) / sizeof(kPhaseNames[0]));
+
+}  // namespace
+
+extern "C" {
+
+int npom_abi_version(void) { return 1; }
+int npom_field_count(void) { return NPOM_NFIELDS; }
+const char *npom_field_name(int index) { return (index >= 0 && index < NPOM_NFIELDS) ? kFieldNames[index] : nullptr; }
+int npom_ws_count(void) { return NPOM_NWS; }
+const char *npom_ws_name(int index) { return (index >= 0 && index < NPOM_NWS) ? kWsNames[index] : nullptr; }
+size_t npom_params_size(void) { return sizeof(npom_params); }
+size_t npom_workspace_struct_size(void) { return sizeof(npom_workspace); }
+int npom_phase_count(void) { return kNumPhases; }
+const char *npom_phase_name(int index) { return (index >= 0 && index < kNumPhases) ? kPhaseNames[index] : nullptr; }
+
+npom_status npom_step_explicit(const npom_params *p, float *const *fields, const npom_workspace *ws,
+                               const npom_clock *clk, void *stream) {
+  return run_steps(p, fields, ws, clk, stream, NPOM_CORE_EXPLICIT);
+}
+
+npom_status npom_step_implicit(const npom_params *p, float *const *fields, const npom_workspace *ws,
+                               const npom_clock *clk, void *stream) {
+  return run_steps(p, fields, ws, clk, stream, NPOM_CORE_IMPLICIT);
+}
+
+npom_status npom_run_phase(const npom_params *p, float *const *fields, const npom_workspace *ws, int phase,
+                           double ramp, void *stream) {
+  if (!check_args_dev(p, fields, ws) || phase < 0 || phase >= kNumPhases) return NPOM_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  Ctx c = make_ctx(p, fields, ws);
+  c.ramp = (float)ramp;
+  c.do_internal = 1;
+  cudaError_t e = cudaSuccess;
+  switch (phase) {
+    case 0: launch_points<PP_A1>(c, s); break;
+    case 1: launch_cols<CP_A2>(c, s); break;
+    case 2: launch_cells<XP_A3>(c, s); break;
+    case 3:
+      if (p->core == NPOM_CORE_IMPLICIT) {
+        launch_cells<XP_COEF>(c, s);
+        e = run_pcg(c, 0, 1, 1, s);
+      } else {
+        e = run_subcycle(c, s);
+      }
+      break;
+    case 4: launch_cells<XP_I5>(c, s); break;
+    case 5: launch_cols<CP_B1>(c, s); break;
+    case 6: launch_cols<CP_B2A>(c, s); break;
+    case 7: launch_points<PP_B2B>(c, s); break;
+    case 8: launch_cols<CP_B3>(c, s); break;
+    case 9: launch_points<PP_B4>(c, s); break;
+    case 10: launch_points<PP_B5>(c, s); break;
+    case 11: launch_cols<CP_B6>(c, s); break;
+    case 12: launch_points<PP_B7>(c, s); break;
+    case 13: launch_cols<CP_B8>(c, s); break;
+    case 14: launch_cols<CP_B9>(c, s); break;
+  }
+  if (e != cudaSuccess) return NPOM_ERR_CUDA;
+  return cudaGetLastError() == cudaSuccess ? NPOM_OK : NPOM_ERR_CUDA;
+}
+
+npom_status npom_proft(int ncol, int kb, const float *f_in, const float *wfsurf, const float *fsurf, int nbc,
+                       const float *h, const float *etf, double dti2, const float *dz, const float *dzz,
+                       const float *swrad, int ntp, const float *kh, double umol, const float *z, float *f_out,
+                       float *dh_out, void *stream) {
+  if (ncol < 0 || kb < 3 || kb > KMAX || nbc < 1 || nbc > 4 || ntp < 1 || ntp > 5) return NPOM_ERR_ARG;
+  if (ncol == 0) return NPOM_OK;
+  if (!f_in || !wfsurf || !fsurf || !h || !etf || !dz || !dzz || !swrad || !kh || !z || !f_out || !dh_out)
+    return NPOM_ERR_ARG;
+  k_proft<<<blocks_for((size_t)ncol, 128), 128, 0, (cudaStream_t)stream>>>(
+      ncol, kb, f_in, wfsurf, fsurf, nbc, h, etf, (float)dti2, dz, dzz, swrad, ntp, kh, (float)umol, z, f_out, dh_out);
+  return cudaGetLastError() == cudaSuccess ? NPOM_OK : NPOM_ERR_CUDA;
+}
+
+npom_status npom_pcg_solve(const npom_params *p, float *const *fields, const npom_workspace *ws, void *stream) {
+  if (!check_args_dev(p, fields, ws) || p->core != NPOM_CORE_IMPLICIT) return NPOM_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  Ctx c = make_ctx(p, fields, ws);
+  launch_cells<XP_COEF>(c, s);
+  cudaError_t e = run_pcg(c, 0, 0, 0, s);
+  if (e != cudaSuccess) return NPOM_ERR_CUDA;
+  return cudaGetLastError() == cudaSuccess ? NPOM_OK : NPOM_ERR_CUDA;
+}
+
+npom_status npom_status_read(const npom_workspace *ws, int clear, unsigned int *out_bits, void *stream) {
+  if (!ws || !ws->status || !out_bits) return NPOM_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned int bits = 0;
+  if (cudaMemcpyAsync(&bits, ws->status, sizeof(bits), cudaMemcpyDeviceToHost, s) != cudaSuccess) return NPOM_ERR_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return NPOM_ERR_CUDA;
+  if (clear && cudaMemsetAsync(ws->status, 0, sizeof(unsigned int), s) != cudaSuccess) return NPOM_ERR_CUDA;
+  *out_bits = bits;
+  return NPOM_OK;
+}
+
+}  // extern "C"

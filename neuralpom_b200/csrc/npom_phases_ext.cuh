@@ -1,0 +1,407 @@
+// npom_phases_ext.cuh -- external (2-D) mode of both cores.
+//
+//  * implicit: barotropic predictor, transport/RHS, elliptic operator and
+//    preconditioners of the PCG free-surface solve, corrector, time filter
+//    (implicit_p0_fixed/core.py:121-943, time_loop.py:243-387,
+//    boundary/closed_basin.py:27-98);
+//  * explicit: one external substep split into the phases of the fused
+//    subcycle kernel (explicit/time_loop.py:275-431, baroclinic.py:496-571).
+#pragma once
+
+#include "npom_phases_a.cuh"
+
+namespace npom {
+
+// ---------------------------------------------------------------------------
+// Phase A3 (2-D cell, both cores): rho round trip of BAROPG, ADVAVE,
+// adx2d/ady2d -= advua/advva, egf and provisional utf/vtf; implicit core
+// also stores d_baro and the predictor (u*, v*) with bcond 2.
+// ---------------------------------------------------------------------------
+NPOM_HD void phase_a3_cell(const Ctx &c, int i, int j) {
+  const int im = c.im, jm = c.jm;
+  // rho = (rho - rmean) + rmean (momentum.py:554,698)
+  for (int k = 0; k < c.kb; ++k) {
+    float rm = F3(rmean, i, j, k);
+    P3(rho, i, j, k) = (F3(rho, i, j, k) - rm) + rm;
+  }
+  AdvaveOut o = advave_cell(c, i, j);
+  P2(advua, i, j) = o.advua;
+  P2(advva, i, j) = o.advva;
+  if (o.write_flux) {
+    P2(fluxua, i, j) = o.fluxua;
+    P2(fluxva, i, j) = o.fluxva;
+  }
+  if (o.write_tps) P2(tps, i, j) = o.tps;
+  float adx = F2(adx2d, i, j) - o.advua;
+  float ady = F2(ady2d, i, j) - o.advva;
+  P2(adx2d, i, j) = adx;
+  P2(ady2d, i, j) = ady;
+  P2(egf, i, j) = F2(el, i, j) * c.k.ispi;
+  if (i >= 1) P2(utf, i, j) = F2(ua, i, j) * (F2(d, i, j) + F2(d, i - 1, j)) * c.k.isp2i;
+  if (j >= 1) P2(vtf, i, j) = F2(va, i, j) * (F2(d, i, j) + F2(d, i, j - 1)) * c.k.isp2i;
+  if (c.k.core != NPOM_CORE_IMPLICIT) return;
+
+  PW2(d_baro, i, j) = F2(h, i, j) + F2(elb, i, j);
+  // predictor (core.py:795-845) then closed-basin bcond 2 (closed_basin.py:261-272)
+  float us = 0.0f, vs = 0.0f, den_u = 0.0f, den_v = 0.0f;
+  if (interior(c, i, j)) {
+    const float g4 = c.k.quarter_g, al = c.k.alpha, a12 = c.k.one_m_2alpha;
+    float cor_u = 0.25f * (F2(cor, i, j) * F2(d, i, j) * (F2(va, i, j + 1) + F2(va, i, j)) +
+                           F2(cor, i - 1, j) * F2(d, i - 1, j) * (F2(va, i - 1, j + 1) + F2(va, i - 1, j)));
+    float cor_v = 0.25f * (F2(cor, i, j) * F2(d, i, j) * (F2(ua, i + 1, j) + F2(ua, i, j)) +
+                           F2(cor, i, j - 1) * F2(d, i, j - 1) * (F2(ua, i + 1, j - 1) + F2(ua, i, j - 1)));
+    float gu = g4 * (F2(dy, i, j) + F2(dy, i - 1, j)) * (F2(d, i, j) + F2(d, i - 1, j)) *
+               (a12 * (F2(el, i, j) - F2(el, i - 1, j)) + al * (F2(elb, i, j) - F2(elb, i - 1, j)) +
+                F2(e_atmos, i, j) - F2(e_atmos, i - 1, j));
+    float gv = g4 * (F2(dx, i, j) + F2(dx, i, j - 1)) * (F2(d, i, j) + F2(d, i, j - 1)) *
+               (a12 * (F2(el, i, j) - F2(el, i, j - 1)) + al * (F2(elb, i, j) - F2(elb, i, j - 1)) +
+                F2(e_atmos, i, j) - F2(e_atmos, i, j - 1));
+    float aru = F2(aru, i, j), arv = F2(arv, i, j);
+    float uprov = adx + o.advua - aru * cor_u + gu + F2(drx2d, i, j) - aru * (-F2(wusurf, i, j) + F2(wubot, i, j));
+    float vprov = ady + o.advva + arv * cor_v + gv + F2(dry2d, i, j) - arv * (-F2(wvsurf, i, j) + F2(wvbot, i, j));
+    den_u = (F2(h, i, j) + F2(el, i, j) + F2(h, i - 1, j) + F2(el, i - 1, j)) * aru;
+    float num_u = (F2(h, i, j) + F2(elb, i, j) + F2(h, i - 1, j) + F2(elb, i - 1, j)) * aru * F2(uab, i, j) -
+                  c.k.four_dti * uprov;
+    den_v = (F2(h, i, j) + F2(el, i, j) + F2(h, i, j - 1) + F2(el, i, j - 1)) * arv;
+    float num_v = (F2(h, i, j) + F2(elb, i, j) + F2(h, i, j - 1) + F2(elb, i, j - 1)) * arv * F2(vab, i, j) -
+                  c.k.four_dti * vprov;
+    us = (num_u / (den_u + 1e-20f)) * F2(dum, i, j);
+    vs = (num_v / (den_v + 1e-20f)) * F2(dvm, i, j);
+    us = us * F2(dum, i, j);
+    vs = vs * F2(dvm, i, j);
+  }
+  if (i == 0 || i == im - 1 || j == 0 || j == jm - 1) {
+    us = 0.0f;
+    vs = 0.0f;
+  }
+  PW2(us, i, j) = us;
+  PW2(vs, i, j) = vs;
+  PW2(den_u, i, j) = den_u;
+  PW2(den_v, i, j) = den_v;
+}
+
+// ---------------------------------------------------------------------------
+// Implicit free-surface solve pieces.
+// ---------------------------------------------------------------------------
+
+// Barotropic transports fed by the predictor (core.py:858-891): stored as
+// fluxua/fluxva (zero on row 0 / column 0).
+NPOM_HD float rhs_fluxua(const Ctx &c, int i, int j) {
+  if (i < 1 || j < 1) return 0.0f;
+  return 0.25f * (F2(d, i, j) + F2(d, i - 1, j)) * (F2(dy, i, j) + F2(dy, i - 1, j)) * W2(us, i, j);
+}
+NPOM_HD float rhs_fluxva(const Ctx &c, int i, int j) {
+  if (i < 1 || j < 1) return 0.0f;
+  return 0.25f * (F2(d, i, j) + F2(d, i, j - 1)) * (F2(dx, i, j) + F2(dx, i, j - 1)) * W2(vs, i, j);
+}
+
+// RHS of the elliptic problem with the Dirichlet ring zeroed
+// (core.py:879-880 and 480-485).
+NPOM_HD float rhs_cell(const Ctx &c, int i, int j) {
+  if (!interior(c, i, j)) return 0.0f;
+  float div = rhs_fluxua(c, i + 1, j) - rhs_fluxua(c, i, j) + rhs_fluxva(c, i, j + 1) - rhs_fluxva(c, i, j);
+  return F2(elb, i, j) - c.k.two_dti * (div / (F2(art, i, j) + 1e-20f) + F2(vfluxf, i, j));
+}
+
+// Geometry coefficients of the operator (core.py:129-185), stored in the
+// workspace once per core (they depend on the grid only).
+NPOM_HD void elliptic_coeff_cell(const Ctx &c, int i, int j) {
+  if (!interior(c, i, j)) {
+    PW2(ce, i, j) = 0.0f;
+    PW2(cw, i, j) = 0.0f;
+    PW2(cn, i, j) = 0.0f;
+    PW2(cs, i, j) = 0.0f;
+    PW2(inv_art, i, j) = 0.0f;
+    return;
+  }
+  float dx_e = 0.5f * (F2(dx, i + 1, j) + F2(dx, i, j));
+  float dx_w = 0.5f * (F2(dx, i, j) + F2(dx, i - 1, j));
+  float dy_e = 0.5f * (F2(dy, i + 1, j) + F2(dy, i, j));
+  float dy_w = 0.5f * (F2(dy, i, j) + F2(dy, i - 1, j));
+  float dy_n = 0.5f * (F2(dy, i, j + 1) + F2(dy, i, j));
+  float dy_s = 0.5f * (F2(dy, i, j) + F2(dy, i, j - 1));
+  float dx_n = 0.5f * (F2(dx, i, j + 1) + F2(dx, i, j));
+  float dx_s = 0.5f * (F2(dx, i, j) + F2(dx, i, j - 1));
+  PW2(ce, i, j) = dy_e / (dx_e + 1e-20f);
+  PW2(cw, i, j) = dy_w / (dx_w + 1e-20f);
+  PW2(cn, i, j) = dx_n / (dy_n + 1e-20f);
+  PW2(cs, i, j) = dx_s / (dy_s + 1e-20f);
+  PW2(inv_art, i, j) = 1.0f / (F2(art, i, j) + 1e-20f);
+}
+
+// out = eta - coeff * div(D grad eta) / art on the interior (core.py:591-639);
+// eta is a workspace or field vector with a zero Dirichlet ring.
+NPOM_HD float elliptic_apply_cell(const Ctx &c, const float *eta, int i, int j) {
+  const size_t o = NPOM_I2(c, i, j);
+  float e = ld(eta + o);
+  if (!interior(c, i, j)) return e;
+  const float *dd = c.F[NPOM_F_d];
+  const int jm = c.jm;
+  float d0 = ld(dd + o);
+  float he = 0.5f * (ld(dd + o + jm) + d0);
+  float hw = 0.5f * (d0 + ld(dd + o - jm));
+  float hn = 0.5f * (ld(dd + o + 1) + d0);
+  float hs = 0.5f * (d0 + ld(dd + o - 1));
+  float fe = he * (ld(eta + o + jm) - e) * W2(ce, i, j) * F2(dum, i + 1, j);
+  float fw = hw * (e - ld(eta + o - jm)) * W2(cw, i, j) * F2(dum, i, j);
+  float fn = hn * (ld(eta + o + 1) - e) * W2(cn, i, j) * F2(dvm, i, j + 1);
+  float fs = hs * (e - ld(eta + o - 1)) * W2(cs, i, j) * F2(dvm, i, j);
+  float div = (fe - fw + fn - fs) * W2(inv_art, i, j);
+  return e - c.k.implicit_coeff * div;
+}
+
+// Jacobi diagonal (core.py:677-700)
+NPOM_HD float jacobi_diag_cell(const Ctx &c, int i, int j) {
+  if (!interior(c, i, j)) return 1.0f;
+  float d0 = F2(d, i, j);
+  float he = 0.5f * (F2(d, i + 1, j) + d0);
+  float hw = 0.5f * (d0 + F2(d, i - 1, j));
+  float hn = 0.5f * (F2(d, i, j + 1) + d0);
+  float hs = 0.5f * (d0 + F2(d, i, j - 1));
+  return 1.0f + c.k.implicit_coeff * W2(inv_art, i, j) *
+                    (he * W2(ce, i, j) * F2(dum, i + 1, j) + hw * W2(cw, i, j) * F2(dum, i, j) +
+                     hn * W2(cn, i, j) * F2(dvm, i, j + 1) + hs * W2(cs, i, j) * F2(dvm, i, j));
+}
+
+// Spectral preconditioner stages (core.py:762-773): DST-I along i, along j,
+// scale by the inverse eigenvalues, DST-I along i, along j, / inverse_scale.
+// Index (a, b) runs over the ni x nj interior.
+NPOM_HD float dst_stage_i(const Ctx &c, const float *src, bool src_is_grid, int a, int b) {
+  const int ni = c.im - 2, nj = c.jm - 2;
+  const float *sx = c.W[NPOM_W_sx];
+  double acc = 0.0;
+  for (int m = 0; m < ni; ++m) {
+    float v = src_is_grid ? ld(src + NPOM_I2(c, m + 1, b + 1)) : ld(src + (size_t)m * nj + b);
+    acc += (double)ld(sx + (size_t)a * ni + m) * (double)v;
+  }
+  return (float)acc;
+}
+NPOM_HD float dst_stage_j(const Ctx &c, const float *src, int a, int b) {
+  const int nj = c.jm - 2;
+  const float *sy = c.W[NPOM_W_sy];
+  double acc = 0.0;
+  for (int m = 0; m < nj; ++m) acc += (double)ld(src + (size_t)a * nj + m) * (double)ld(sy + (size_t)m * nj + b);
+  return (float)acc;
+}
+
+// Corrector, closed-basin bcond 2, etf, Robert-Asselin filter, state shifts,
+// egf and endpoint transports (core.py:918-943, time_loop.py:309-387).
+// Returns true when |vaf| exceeds vmaxl at this cell.
+NPOM_HD bool phase_i5_cell(const Ctx &c, int i, int j) {
+  const int im = c.im, jm = c.jm;
+  const float elf0 = F2(elf, i, j);
+  float uaf = F2(uaf, i, j), vaf = F2(vaf, i, j);
+  if (interior(c, i, j)) {
+    const float g4 = c.k.quarter_g, al = c.k.alpha;
+    float h0 = F2(h, i, j);
+    float dnew = h0 + elf0;
+    float dnew_w = F2(h, i - 1, j) + F2(elf, i - 1, j);
+    float dnew_s = F2(h, i, j - 1) + F2(elf, i, j - 1);
+    float gu = g4 * (F2(dy, i, j) + F2(dy, i - 1, j)) * (dnew + dnew_w) * al * (elf0 - F2(elf, i - 1, j));
+    float gv = g4 * (F2(dx, i, j) + F2(dx, i, j - 1)) * (dnew + dnew_s) * al * (elf0 - F2(elf, i, j - 1));
+    float dfu = (h0 + elf0 + F2(h, i - 1, j) + F2(elf, i - 1, j)) * F2(aru, i, j);
+    float dfv = (h0 + elf0 + F2(h, i, j - 1) + F2(elf, i, j - 1)) * F2(arv, i, j);
+    uaf = (W2(us, i, j) * W2(den_u, i, j) - c.k.four_dti * gu) / (dfu + 1e-20f) * F2(dum, i, j);
+    vaf = (W2(vs, i, j) * W2(den_v, i, j) - c.k.four_dti * gv) / (dfv + 1e-20f) * F2(dvm, i, j);
+  }
+  uaf = uaf * F2(dum, i, j);
+  vaf = vaf * F2(dvm, i, j);
+  if (i == 0 || i == im - 1 || j == 0 || j == jm - 1) {
+    uaf = 0.0f;
+    vaf = 0.0f;
+  }
+  P2(uaf, i, j) = uaf;
+  P2(vaf, i, j) = vaf;
+  P2(etf, i, j) = elf0 * F2(fsm, i, j);
+  bool exceed = !(fabsf(vaf) <= c.k.vmaxl);
+  // Robert-Asselin filter and shifts (speculatively applied; a VMAX status
+  // aborts the step on the host)
+  const float hs = c.k.half_smoth;
+  float ua = F2(ua, i, j), va = F2(va, i, j), el = F2(el, i, j);
+  float uaf_f = ua + hs * (F2(uab, i, j) - 2.0f * ua + uaf);
+  float vaf_f = va + hs * (F2(vab, i, j) - 2.0f * va + vaf);
+  float el_f = el + hs * (F2(elb, i, j) - 2.0f * el + elf0);
+  P2(elb, i, j) = el_f;
+  P2(el, i, j) = elf0;
+  float dn = F2(h, i, j) + elf0;
+  P2(d, i, j) = dn;
+  P2(uab, i, j) = uaf_f;
+  P2(ua, i, j) = uaf;
+  P2(vab, i, j) = vaf_f;
+  P2(va, i, j) = vaf;
+  P2(egf, i, j) = (el_f + elf0) * 0.5f;
+  if (i >= 1) {
+    float dsum_new = dn + (F2(h, i - 1, j) + F2(elf, i - 1, j));
+    float dsum_baro = W2(d_baro, i, j) + W2(d_baro, i - 1, j);
+    P2(utf, i, j) = 0.25f * (uaf_f * dsum_baro + uaf * dsum_new);
+  }
+  if (j >= 1) {
+    float dsum_new = dn + (F2(h, i, j - 1) + F2(elf, i, j - 1));
+    float dsum_baro = W2(d_baro, i, j) + W2(d_baro, i, j - 1);
+    P2(vtf, i, j) = 0.25f * (vaf_f * dsum_baro + vaf * dsum_new);
+  }
+  return exceed;
+}
+
+// ---------------------------------------------------------------------------
+// Explicit external substep (explicit/time_loop.py:292-431).
+// ---------------------------------------------------------------------------
+
+// Interior elf before bcond 1 (time_loop.py:299-312)
+NPOM_HD float ext_elf_interior(const Ctx &c, int i, int j) {
+  auto fu = [&](int ii, int jj) {
+    return 0.25f * (F2(d, ii, jj) + F2(d, ii - 1, jj)) * (F2(dy, ii, jj) + F2(dy, ii - 1, jj)) * F2(ua, ii, jj);
+  };
+  auto fv = [&](int ii, int jj) {
+    return 0.25f * (F2(d, ii, jj) + F2(d, ii, jj - 1)) * (F2(dx, ii, jj) + F2(dx, ii, jj - 1)) * F2(va, ii, jj);
+  };
+  float div = fu(i + 1, j) - fu(i, j) + fv(i, j + 1) - fv(i, j);
+  float term = -(div / F2(art, i, j)) - F2(vfluxf, i, j);
+  return F2(elb, i, j) + c.k.dte2 * term;
+}
+
+// elf after the explicit bcond 1 (baroclinic.py:510-524): edges copy the
+// adjacent cell (rows first, then columns, so corners take the diagonal
+// interior value), then the whole field is masked by fsm.
+NPOM_HD float ext_elf_cell(const Ctx &c, int i, int j) {
+  int si = i, sj = j;
+  if (si == 0) si = 1;
+  if (si == c.im - 1) si = c.im - 2;
+  if (sj == 0) sj = 1;
+  if (sj == c.jm - 1) sj = c.jm - 2;
+  return ext_elf_interior(c, si, sj) * F2(fsm, i, j);
+}
+
+// Phase 1 of a substep: elf with bcond 1, and the stored fluxua/fluxva:
+// the transports (time_loop.py:299-305), or on ADVAVE substeps
+// (iext % ispadv == 0) the ADVAVE outputs that overwrite them.  ADVAVE reads
+// fluxua/fluxva only on row 0 / column 0, which no phase writes, so both
+// fit in one phase.
+NPOM_HD void ext_phase1_cell(const Ctx &c, int i, int j, bool do_advave) {
+  P2(elf, i, j) = ext_elf_cell(c, i, j);
+  if (do_advave) {
+    AdvaveOut o = advave_cell(c, i, j);
+    P2(advua, i, j) = o.advua;
+    P2(advva, i, j) = o.advva;
+    if (o.write_flux) {
+      P2(fluxua, i, j) = o.fluxua;
+      P2(fluxva, i, j) = o.fluxva;
+    }
+    if (o.write_tps) P2(tps, i, j) = o.tps;
+  } else if (i >= 1 && j >= 1) {
+    P2(fluxua, i, j) = 0.25f * (F2(d, i, j) + F2(d, i - 1, j)) * (F2(dy, i, j) + F2(dy, i - 1, j)) * F2(ua, i, j);
+    P2(fluxva, i, j) = 0.25f * (F2(d, i, j) + F2(d, i, j - 1)) * (F2(dx, i, j) + F2(dx, i, j - 1)) * F2(va, i, j);
+  }
+}
+
+// Phase 2: uaf/vaf with bcond 2 and the etf time filter
+// (time_loop.py:326-391).  Returns |vaf| > vmaxl.
+NPOM_HD bool ext_phase2_cell(const Ctx &c, int i, int j, int iext) {
+  const int im = c.im, jm = c.jm;
+  float uaf = F2(uaf, i, j), vaf = F2(vaf, i, j);
+  if (interior(c, i, j)) {
+    const float g4 = c.k.quarter_g, al = c.k.alpha, a12 = c.k.one_m_2alpha;
+    float d0 = F2(d, i, j);
+    float cor_u = 0.25f * (F2(cor, i, j) * d0 * (F2(va, i, j + 1) + F2(va, i, j)) +
+                           F2(cor, i - 1, j) * F2(d, i - 1, j) * (F2(va, i - 1, j + 1) + F2(va, i - 1, j)));
+    float gu = g4 * (F2(dy, i, j) + F2(dy, i - 1, j)) * (d0 + F2(d, i - 1, j)) *
+               (a12 * (F2(el, i, j) - F2(el, i - 1, j)) +
+                al * (F2(elb, i, j) - F2(elb, i - 1, j) + F2(elf, i, j) - F2(elf, i - 1, j)) + F2(e_atmos, i, j) -
+                F2(e_atmos, i - 1, j));
+    float aru = F2(aru, i, j), arv = F2(arv, i, j);
+    float up = F2(adx2d, i, j) + F2(advua, i, j) - aru * cor_u + gu + F2(drx2d, i, j) -
+               aru * (-F2(wusurf, i, j) + F2(wubot, i, j));
+    float den = (F2(h, i, j) + F2(elf, i, j) + F2(h, i - 1, j) + F2(elf, i - 1, j)) * aru;
+    float num = (F2(h, i, j) + F2(elb, i, j) + F2(h, i - 1, j) + F2(elb, i - 1, j)) * aru * F2(uab, i, j) -
+                c.k.four_dte * up;
+    uaf = num / (den + 1e-20f);
+    float cor_v = 0.25f * (F2(cor, i, j) * d0 * (F2(ua, i + 1, j) + F2(ua, i, j)) +
+                           F2(cor, i, j - 1) * F2(d, i, j - 1) * (F2(ua, i + 1, j - 1) + F2(ua, i, j - 1)));
+    float gv = g4 * (F2(dx, i, j) + F2(dx, i, j - 1)) * (d0 + F2(d, i, j - 1)) *
+               (a12 * (F2(el, i, j) - F2(el, i, j - 1)) +
+                al * (F2(elb, i, j) - F2(elb, i, j - 1) + F2(elf, i, j) - F2(elf, i, j - 1)) + F2(e_atmos, i, j) -
+                F2(e_atmos, i, j - 1));
+    float vp = F2(ady2d, i, j) + F2(advva, i, j) + arv * cor_v + gv + F2(dry2d, i, j) -
+               arv * (-F2(wvsurf, i, j) + F2(wvbot, i, j));
+    float denv = (F2(h, i, j) + F2(elf, i, j) + F2(h, i, j - 1) + F2(elf, i, j - 1)) * arv;
+    float numv = (F2(h, i, j) + F2(elb, i, j) + F2(h, i, j - 1) + F2(elb, i, j - 1)) * arv * F2(vab, i, j) -
+                 c.k.four_dte * vp;
+    vaf = numv / (denv + 1e-20f);
+  }
+  // bcond 2 (baroclinic.py:529-571): open-boundary (Flather) values, zero
+  // normal/tangential components on the ring, then masks.
+  const float ramp = c.ramp, g = c.k.grav;
+  auto rad = [&](float hh) { return sqrtf(fmaxf_t(g / fmaxf_t(hh, 1e-8f), 1e-8f)); };
+  if (j >= 1 && j <= jm - 2) {
+    if (i == im - 1) {
+      float te = c.k.rfe * rad(F2(h, im - 2, j)) * (F2(el, im - 2, j) - F1(ele, j));
+      uaf = (F1(uabe, j) + te) * ramp;
+      vaf = 0.0f;
+    }
+    if (i == 1 || i == 0) {
+      float tw = c.k.rfw * rad(F2(h, 1, j)) * (F2(el, 1, j) - F1(elw, j));
+      uaf = (F1(uabw, j) - tw) * ramp;
+    }
+    if (i == 0) vaf = 0.0f;
+  }
+  if (i >= 1 && i <= im - 2) {
+    if (j == jm - 1) {
+      float tn = c.k.rfn * rad(F2(h, i, jm - 2)) * (F2(el, i, jm - 2) - F1(eln, i));
+      vaf = (F1(vabn, i) + tn) * ramp;
+      uaf = 0.0f;
+    }
+    if (j == 1 || j == 0) {
+      float ts = c.k.rfs * rad(F2(h, i, 1)) * (F2(el, i, 1) - F1(els, i));
+      vaf = (F1(vabs, i) - ts) * ramp;
+    }
+    if (j == 0) uaf = 0.0f;
+  }
+  uaf = uaf * F2(dum, i, j);
+  vaf = vaf * F2(dvm, i, j);
+  P2(uaf, i, j) = uaf;
+  P2(vaf, i, j) = vaf;
+  // etf filter (time_loop.py:386-391)
+  const int isplit = c.k.isplit;
+  float elf0 = F2(elf, i, j);
+  if (iext == isplit - 2) {
+    P2(etf, i, j) = c.k.quarter_smoth * elf0;
+  } else if (iext == isplit - 1) {
+    P2(etf, i, j) = F2(etf, i, j) + c.k.etf_mid * elf0;
+  } else if (iext == isplit) {
+    P2(etf, i, j) = (F2(etf, i, j) + 0.5f * elf0) * F2(fsm, i, j);
+  }
+  return !(fabsf(vaf) <= c.k.vmaxl);
+}
+
+// Phase 3: Robert-Asselin filter, shifts, egf/utf/vtf accumulation
+// (time_loop.py:395-431).  Reads only this cell plus elf/h of the west and
+// south neighbours (d at the end of the substep is h + elf).
+NPOM_HD void ext_phase3_cell(const Ctx &c, int i, int j, int iext) {
+  const float hs = c.k.half_smoth;
+  float ua = F2(ua, i, j), va = F2(va, i, j), el = F2(el, i, j);
+  float uaf = F2(uaf, i, j), vaf = F2(vaf, i, j), elf0 = F2(elf, i, j);
+  float ua_f = ua + hs * (F2(uab, i, j) - 2.0f * ua + uaf);
+  float va_f = va + hs * (F2(vab, i, j) - 2.0f * va + vaf);
+  float el_f = el + hs * (F2(elb, i, j) - 2.0f * el + elf0);
+  P2(elb, i, j) = el_f;
+  P2(el, i, j) = elf0;
+  float dn = F2(h, i, j) + elf0;
+  P2(d, i, j) = dn;
+  P2(uab, i, j) = ua_f;
+  P2(ua, i, j) = uaf;
+  P2(vab, i, j) = va_f;
+  P2(va, i, j) = vaf;
+  if (iext != c.k.isplit) {
+    P2(egf, i, j) = F2(egf, i, j) + elf0 * c.k.ispi;
+    if (i >= 1) {
+      float ds = dn + (F2(h, i - 1, j) + F2(elf, i - 1, j));
+      P2(utf, i, j) = F2(utf, i, j) + uaf * ds * c.k.isp2i;
+    }
+    if (j >= 1) {
+      float ds = dn + (F2(h, i, j - 1) + F2(elf, i, j - 1));
+      P2(vtf, i, j) = F2(vtf, i, j) + vaf * ds * c.k.isp2i;
+    }
+  }
+}
+
+}  // namespace npom

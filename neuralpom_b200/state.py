@@ -1,0 +1,121 @@
+"""Scalar settings and solver caches of a core, shared by the torch host
+layer (``core.py``) and the tests.
+
+The scalar names are the reference core's Python attributes
+(``src/neuralpom/cores/explicit/base.py:37-120`` and
+``cores/implicit_p0_fixed/base.py``/``core.py:78-119``); the production
+values are pinned by ``src/neuralpom/v1/core_spec.py:22-47``.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import _abi
+
+# Attributes of BaseCore (explicit/base.py) before any case or spec override.
+BASE_SCALARS = dict(
+    small=1e-9, pi=math.atan(1.0) * 4.0, mode=3, nadv=1, nitera=2, sw=0.5, lramp=True, rhoref=1035.0,
+    hmax=2000.0, dte=30.0, isplit=30, grav=9.806, kappa=0.40, z0b=0.010, cbcmin=0.0025, cbcmax=1.0,
+    horcon=0.20, tprni=0.20, umol=2e-5, vmaxl=100.0, slmax=2.0, ntp=2, nbct=1, nbcs=1, ispadv=5,
+    tbias=0.0, sbias=0.0, rfe=0.0, rfw=0.0, rfn=0.0, rfs=0.0, ramp=0.0, aam_init=500.0,
+)
+EXPLICIT_DEFAULTS = dict(smoth=0.10, alpha=0.225)
+IMPLICIT_DEFAULTS = dict(smoth=0.15, alpha=0.333, aam_min=0.0, eta_solver_rel_tol=1e-5,
+                         eta_solver_preconditioner="spectral", eta_solver_max_iter=200,
+                         eta_solver_tol=1.0e-12, barotropic_shapiro=0.0, tracer_shapiro=0.0,
+                         velocity_shapiro=0.0)
+
+# core_spec.py:42-47 production settings (dti=600, dte=20, isplit=30)
+PRODUCTION = {
+    "explicit": dict(dte=20.0, isplit=30, alpha=0.225, smoth=0.10, horcon=0.05),
+    "implicit_p0_fixed": dict(dte=20.0, isplit=30, alpha=0.333, smoth=0.15, horcon=0.05,
+                              eta_solver_rel_tol=1e-5, eta_solver_preconditioner="spectral",
+                              barotropic_shapiro=0.0, tracer_shapiro=0.0, velocity_shapiro=0.0),
+}
+
+
+def derived_time(s):
+    """base.py:111-120 derived clock values."""
+    s["dti"] = s["dte"] * s["isplit"]
+    s["dte2"] = s["dte"] * 2.0
+    s["dti2"] = s["dti"] * 2.0
+    s["ispi"] = 1.0 / s["isplit"]
+    s["isp2i"] = 1.0 / (2.0 * s["isplit"])
+    return s
+
+
+def default_scalars(core):
+    s = dict(BASE_SCALARS)
+    s.update(EXPLICIT_DEFAULTS if core == "explicit" else IMPLICIT_DEFAULTS)
+    s.update(PRODUCTION[core])
+    return derived_time(s)
+
+
+def make_params(s, im, jm, kb, core, device=0):
+    """npom_params from a mapping (or object) of the reference scalars."""
+    get = (lambda k, d=None: s.get(k, d)) if isinstance(s, dict) else (lambda k, d=None: getattr(s, k, d))
+    p = _abi.NpomParams()
+    p.device = int(device)
+    p.im, p.jm, p.kb = int(im), int(jm), int(kb)
+    implicit = core != "explicit"
+    p.core = _abi.CORE_IMPLICIT if implicit else _abi.CORE_EXPLICIT
+    p.isplit = int(get("isplit"))
+    p.ispadv = int(get("ispadv", 5))
+    p.nbct, p.nbcs, p.ntp = int(get("nbct", 1)), int(get("nbcs", 1)), int(get("ntp", 2))
+    p.mode, p.nadv = int(get("mode", 3)), int(get("nadv", 1))
+    if p.nadv != 1:
+        raise ValueError("only the centred tracer advection (nadv=1) is implemented")
+    p.eta_max_iter = int(get("eta_solver_max_iter", 200) or 200)
+    pre = str(get("eta_solver_preconditioner", "spectral") or "spectral").strip().lower()
+    if implicit and pre not in ("spectral", "jacobi"):
+        raise ValueError(f"unknown eta preconditioner {pre!r}")
+    p.eta_precond = _abi.PRECOND_SPECTRAL if pre == "spectral" else _abi.PRECOND_JACOBI
+    p.wind_forcing = 1 if (implicit and get("wind_forcing", True)) else 0
+    vmix = get("vertical_mixing_max", None)
+    p.has_vmix = 1 if vmix is not None else 0
+    p.vmix = float(vmix) if vmix is not None else 0.0
+    p.lramp = 1 if get("lramp", True) else 0
+    for k in ("dti", "dte", "dti2", "dte2", "ispi", "isp2i", "alpha", "smoth", "horcon", "grav", "umol", "tprni",
+              "small", "kappa", "rhoref", "tbias", "sbias", "vmaxl", "hmax", "rfe", "rfw", "rfn", "rfs", "pi"):
+        setattr(p, k, float(get(k)))
+    p.aam_min = float(get("aam_min", 0.0) or 0.0)
+    p.eta_tol = float(get("eta_solver_tol", 1.0e-12))
+    p.eta_rel_tol = float(get("eta_solver_rel_tol", 1e-5))
+    p.barotropic_shapiro = float(get("barotropic_shapiro", 0.0) or 0.0)
+    p.tracer_shapiro = float(get("tracer_shapiro", 0.0) or 0.0)
+    p.velocity_shapiro = float(get("velocity_shapiro", 0.0) or 0.0)
+    if p.velocity_shapiro != 0.0:
+        raise ValueError("a non-zero internal-velocity Shapiro filter is not implemented (production uses 0)")
+    p.wind_tau0 = float(get("double_gyre_wind_stress_pa", 0.1) or 0.1)
+    period = get("period", 1.0)
+    p.period = float(np.asarray(period, dtype=np.float64))
+    p.inverse_scale = 4.0 * (im - 1) * (jm - 1)
+    return p
+
+
+def spectral_setup(dx, dy, h, dti, grav, alpha, dtype=np.float32):
+    """DST-I matrices and inverse eigenvalues of the spectral preconditioner
+    (``implicit_p0_fixed/core.py:730-760``; torch.median picks the lower
+    middle value)."""
+    im, jm = dx.shape
+    ni, nj = im - 2, jm - 2
+
+    def tmedian(a):
+        flat = np.sort(np.asarray(a, dtype=dtype).reshape(-1))
+        return flat[(flat.size - 1) // 2]
+
+    dx0, dy0, h0 = tmedian(dx[1:-1, 1:-1]), tmedian(dy[1:-1, 1:-1]), tmedian(h[1:-1, 1:-1])
+    coeff = 4.0 * (dti ** 2) * grav * alpha
+    kx = np.arange(1, ni + 1, dtype=dtype).reshape(-1, 1)
+    ky = np.arange(1, nj + 1, dtype=dtype).reshape(1, -1)
+    lam_x = 4.0 * np.square(np.sin(np.pi * kx / (2.0 * (ni + 1)))) / (dx0 * dx0 + 1e-30)
+    lam_y = 4.0 * np.square(np.sin(np.pi * ky / (2.0 * (nj + 1)))) / (dy0 * dy0 + 1e-30)
+    inv_eigs = (1.0 / (1.0 + coeff * h0 * (lam_x + lam_y))).astype(dtype)
+
+    def sine(n):
+        k = np.arange(1, n + 1, dtype=np.float64)
+        return (2.0 * np.sin(np.pi * np.outer(k, k) / (n + 1))).astype(dtype)
+
+    return sine(ni), sine(nj), np.ascontiguousarray(inv_eigs)

@@ -1,0 +1,238 @@
+// npom_emul.cu -- CPU emulation of the device phases, for tests only.
+//
+// Compiles the very same __host__ __device__ phase bodies as the CUDA
+// library (neuralpom_b200/csrc) for the host and runs each phase as a loop
+// over its points / columns / cells, in the order the kernels launch them.
+// The cooperative kernels (PCG, explicit subcycle) are restated with the
+// grid barriers replaced by the end of each loop.  This checks the index
+// logic of every phase against the oracle on a machine without a GPU; it is
+// not part of the product library and is never loaded by neuralpom_b200.
+#include <cmath>
+#include <cstring>
+
+#include "../../neuralpom_b200/csrc/npom_host.cuh"
+
+using namespace npom;
+
+namespace {
+
+template <class F>
+void each_point(const Ctx &c, F f) {
+  for (int i = 0; i < c.im; ++i)
+    for (int j = 0; j < c.jm; ++j)
+      for (int k = 0; k < c.kb; ++k) f(i, j, k);
+}
+template <class F>
+void each_cell(const Ctx &c, F f) {
+  for (int i = 0; i < c.im; ++i)
+    for (int j = 0; j < c.jm; ++j) f(i, j);
+}
+
+void a1(const Ctx &c) {
+  each_point(c, [&](int i, int j, int k) {
+    float ax, ay, cv;
+    advct_point(c, i, j, k, ax, ay, cv);
+    P3(advx, i, j, k) = ax;
+    P3(advy, i, j, k) = ay;
+    P3(curv, i, j, k) = cv;
+    if (k == 0) forcing_cell(c, i, j);
+  });
+}
+
+double dot_int(const Ctx &c, const float *a, const float *b) {
+  double s = 0.0;
+  for (int i = 1; i < c.im - 1; ++i)
+    for (int j = 1; j < c.jm - 1; ++j) {
+      size_t o = NPOM_I2(c, i, j);
+      s += (double)a[o] * (double)b[o];
+    }
+  return s;
+}
+
+void precondition(const Ctx &c) {
+  const int ni = c.im - 2, nj = c.jm - 2;
+  float *zv = c.W[NPOM_W_zv];
+  const float *r = c.W[NPOM_W_r];
+  if (c.k.eta_precond == NPOM_PRECOND_SPECTRAL) {
+    float *t1 = c.W[NPOM_W_t1], *t2 = c.W[NPOM_W_t2];
+    for (int a = 0; a < ni; ++a)
+      for (int b = 0; b < nj; ++b) t1[(size_t)a * nj + b] = dst_stage_i(c, r, true, a, b);
+    for (int a = 0; a < ni; ++a)
+      for (int b = 0; b < nj; ++b)
+        t2[(size_t)a * nj + b] = dst_stage_j(c, t1, a, b) * c.W[NPOM_W_inv_eigs][(size_t)a * nj + b];
+    for (int a = 0; a < ni; ++a)
+      for (int b = 0; b < nj; ++b) t1[(size_t)a * nj + b] = dst_stage_i(c, t2, false, a, b);
+    for (int a = 0; a < ni; ++a)
+      for (int b = 0; b < nj; ++b) zv[NPOM_I2(c, a + 1, b + 1)] = dst_stage_j(c, t1, a, b) / c.k.inverse_scale;
+  } else {
+    for (int i = 1; i < c.im - 1; ++i)
+      for (int j = 1; j < c.jm - 1; ++j) {
+        size_t o = NPOM_I2(c, i, j);
+        zv[o] = r[o] / (c.W[NPOM_W_diag][o] + 1e-30f);
+      }
+  }
+}
+
+void pcg(const Ctx &c, int step, int with_rhs, int with_post) {
+  const int im = c.im, jm = c.jm;
+  float *x = c.W[NPOM_W_x], *r = c.W[NPOM_W_r], *p = c.W[NPOM_W_p], *zv = c.W[NPOM_W_zv];
+  float *ap = c.W[NPOM_W_ap], *rhs = c.W[NPOM_W_rhs];
+  each_cell(c, [&](int i, int j) {
+    size_t q = NPOM_I2(c, i, j);
+    if (with_rhs) rhs[q] = rhs_cell(c, i, j);
+    else if (!interior(c, i, j)) rhs[q] = 0.0f;
+  });
+  if (with_rhs)
+    each_cell(c, [&](int i, int j) {
+      P2(fluxua, i, j) = rhs_fluxua(c, i, j);
+      P2(fluxva, i, j) = rhs_fluxva(c, i, j);
+    });
+  each_cell(c, [&](int i, int j) {
+    size_t q = NPOM_I2(c, i, j);
+    bool in = interior(c, i, j);
+    x[q] = in ? c.F[NPOM_F_elf][q] : 0.0f;
+    if (!in) r[q] = p[q] = zv[q] = ap[q] = 0.0f;
+  });
+  for (int i = 1; i < im - 1; ++i)
+    for (int j = 1; j < jm - 1; ++j) {
+      size_t o = NPOM_I2(c, i, j);
+      r[o] = rhs[o] - elliptic_apply_cell(c, x, i, j);
+      if (c.k.eta_precond != NPOM_PRECOND_SPECTRAL) c.W[NPOM_W_diag][o] = jacobi_diag_cell(c, i, j);
+    }
+  double rs0 = dot_int(c, r, r);
+  precondition(c);
+  double rho_old = dot_int(c, r, zv);
+  for (int i = 1; i < im - 1; ++i)
+    for (int j = 1; j < jm - 1; ++j) p[NPOM_I2(c, i, j)] = zv[NPOM_I2(c, i, j)];
+  const double tol_sq = c.k.eta_tol * c.k.eta_tol;
+  const double rel_sq = c.k.eta_rel_tol * c.k.eta_rel_tol * (rs0 > 1e-30 ? rs0 : 1e-30);
+  int its = 0;
+  bool conv = false;
+  for (int it = 1; it <= c.k.eta_max_iter; ++it) {
+    for (int i = 1; i < im - 1; ++i)
+      for (int j = 1; j < jm - 1; ++j) ap[NPOM_I2(c, i, j)] = elliptic_apply_cell(c, p, i, j);
+    double denom = dot_int(c, p, ap);
+    float alpha = (float)(rho_old / (denom + 1e-30));
+    for (int i = 1; i < im - 1; ++i)
+      for (int j = 1; j < jm - 1; ++j) {
+        size_t o = NPOM_I2(c, i, j);
+        x[o] = x[o] + alpha * p[o];
+        r[o] = r[o] - alpha * ap[o];
+      }
+    double rs = dot_int(c, r, r);
+    its = it;
+    if (rs <= tol_sq || rs <= rel_sq || rs <= 1e-30) {
+      conv = true;
+      break;
+    }
+    precondition(c);
+    double rho_new = dot_int(c, r, zv);
+    float beta = (float)(rho_new / (rho_old + 1e-30));
+    for (int i = 1; i < im - 1; ++i)
+      for (int j = 1; j < jm - 1; ++j) {
+        size_t o = NPOM_I2(c, i, j);
+        p[o] = p[o] * beta + zv[o];
+      }
+    rho_old = rho_new;
+  }
+  c.cg_iters[step] = its;
+  if (!conv) *c.status |= NPOM_DEV_PCG_MAXIT;
+  if (!with_post) {
+    each_cell(c, [&](int i, int j) { P2(elf, i, j) = x[NPOM_I2(c, i, j)]; });
+    return;
+  }
+  each_cell(c, [&](int i, int j) {
+    size_t q = NPOM_I2(c, i, j);
+    float e = 0.0f;
+    if (interior(c, i, j)) {
+      float x0 = x[q];
+      float sm = x0 + c.k.bshap_q * (x[q + jm] + x[q - jm] + x[q + 1] + x[q - 1] - 4.0f * x0);
+      float fsm = F2(fsm, i, j);
+      e = (sm * fsm) * fsm;
+    }
+    P2(elf, i, j) = e;
+    P2(d, i, j) = F2(h, i, j) + e;
+  });
+}
+
+void subcycle(const Ctx &c) {
+  for (int iext = 1; iext <= c.k.isplit; ++iext) {
+    bool adv = (iext % c.k.ispadv) == 0;
+    each_cell(c, [&](int i, int j) { ext_phase1_cell(c, i, j, adv); });
+    each_cell(c, [&](int i, int j) {
+      if (ext_phase2_cell(c, i, j, iext)) *c.status |= NPOM_DEV_VMAX;
+    });
+    each_cell(c, [&](int i, int j) { ext_phase3_cell(c, i, j, iext); });
+  }
+}
+
+void run_phase(const Ctx &c, const npom_params *p, int phase) {
+  switch (phase) {
+    case 0: a1(c); break;
+    case 1: each_cell(c, [&](int i, int j) { phase_a2_column(c, i, j); }); break;
+    case 2: each_cell(c, [&](int i, int j) { phase_a3_cell(c, i, j); }); break;
+    case 3:
+      if (p->core == NPOM_CORE_IMPLICIT) {
+        each_cell(c, [&](int i, int j) { elliptic_coeff_cell(c, i, j); });
+        pcg(c, 0, 1, 1);
+      } else {
+        subcycle(c);
+      }
+      break;
+    case 4:
+      each_cell(c, [&](int i, int j) {
+        if (phase_i5_cell(c, i, j)) *c.status |= NPOM_DEV_VMAX;
+      });
+      break;
+    case 5: each_cell(c, [&](int i, int j) { phase_b1_column(c, i, j); }); break;
+    case 6: each_cell(c, [&](int i, int j) { phase_b2a_column(c, i, j); }); break;
+    case 7: each_point(c, [&](int i, int j, int k) { phase_b2b_point(c, i, j, k); }); break;
+    case 8: each_cell(c, [&](int i, int j) { phase_b3_column(c, i, j); }); break;
+    case 9: each_point(c, [&](int i, int j, int k) { phase_b4_point(c, i, j, k); }); break;
+    case 10: each_point(c, [&](int i, int j, int k) { phase_b5_point(c, i, j, k); }); break;
+    case 11: each_cell(c, [&](int i, int j) { phase_b6_column(c, i, j); }); break;
+    case 12: each_point(c, [&](int i, int j, int k) { phase_b7_point(c, i, j, k); }); break;
+    case 13: each_cell(c, [&](int i, int j) { phase_b8_column(c, i, j); }); break;
+    case 14: each_cell(c, [&](int i, int j) { phase_b9_column(c, i, j); }); break;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int emul_run_phase(const npom_params *p, float *const *fields, const npom_workspace *ws, int phase, double ramp) {
+  if (!check_args(p, fields, ws)) return 1;
+  Ctx c = make_ctx(p, fields, ws);
+  c.ramp = (float)ramp;
+  c.do_internal = 1;
+  run_phase(c, p, phase);
+  return 0;
+}
+
+int emul_steps(const npom_params *p, float *const *fields, const npom_workspace *ws, const npom_clock *clk) {
+  if (!check_args(p, fields, ws) || !clk) return 1;
+  Ctx c = make_ctx(p, fields, ws);
+  if (p->core == NPOM_CORE_IMPLICIT) each_cell(c, [&](int i, int j) { elliptic_coeff_cell(c, i, j); });
+  for (int n = 0; n < clk->nsteps; ++n) {
+    int iint = clk->first_iint + n;
+    double time = p->dti * iint * 1.0 / 86400.0 + clk->time0;
+    c.ramp = ramp_of(p, time);
+    c.do_internal = ((iint != 1 || clk->time0 != 0.0) && p->mode != 2) ? 1 : 0;
+    run_phase(c, p, 0);
+    run_phase(c, p, 1);
+    run_phase(c, p, 2);
+    if (p->core == NPOM_CORE_IMPLICIT) {
+      pcg(c, n, 1, 1);
+      run_phase(c, p, 4);
+    } else {
+      subcycle(c);
+    }
+    if (c.do_internal)
+      for (int ph = 5; ph <= 13; ++ph) run_phase(c, p, ph);
+    run_phase(c, p, 14);
+  }
+  return 0;
+}
+
+}  // extern "C"
