@@ -1,0 +1,446 @@
+#!/usr/bin/env python
+"""Throughput of the NeuralPOM physical time step on B200.
+
+Workload: the semi-implicit free-surface core on the 90x82x16 closed basin
+with a Gaussian seamount (dx = 5 km, dtI = 300 s, PCG tolerance 1e-10, FP64
+dot products), synthetic seeded state.  One benchmark step = one simulated
+day (288 internal steps).  Metric: simulated days per second.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+With N > 1 (torchrun) every rank advances its own ensemble member (weak
+scaling, no collective on the data path); value = all members' simulated
+days / the slowest rank's time.  ``--impl reference`` times the reference's
+own PyTorch core on the host CPU (all cores) on the same configuration.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "simulated days/s (fwd, fwd+adjoint) at 90x82x16 vs ref torch core; % HBM peak"
+UNIT = "simulated days/s"
+GRID = (90, 82, 16)
+DTI = 300.0
+
+# Distinct arrays each phase reads / writes (3-D count, 2-D count): the
+# algorithmic-byte rule bytes = 4 * (sum of read numel + sum of written numel).
+PHASE_IO = {
+    "A1_forcing_advct": (5, 12, 3, 8),
+    "A2_baropg_smag_means": (6, 5, 3, 5),
+    "A3_advave_predictor": (2, 27, 1, 15),
+    "E_external": (0, 18, 0, 4),
+    "I5_corrector_filter": (0, 22, 0, 13),
+    "B1_barotropic_fix": (2, 6, 2, 0),
+    "B2A_vertvl": (3, 8, 1, 0),
+    "B2B_advq": (9, 11, 2, 0),
+    "B3_profq": (15, 8, 6, 0),
+    "B4_edges_bcond6": (2, 1, 2, 0),
+    "B5_qfilter_advt1": (17, 10, 10, 0),
+    "B6_proft": (3, 6, 2, 1),
+    "B7_tsfilter_dens": (6, 2, 5, 0),
+    "B8_advuv_profuv": (14, 17, 2, 3),
+    "B9_velfilter_shift": (6, 12, 6, 7),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
+    ap.add_argument("--internal-steps", type=int, default=288, help="internal steps per benchmark step")
+    ap.add_argument("--ref-internal-steps", type=int, default=6, help="reference arm: internal steps per sample")
+    ap.add_argument("--ref-device", default="cpu")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def workload(member=0):
+    from neuralpom_b200 import cases
+    A, Sc = cases.seamount(*GRID[:2], kb=GRID[2], dti=DTI)
+    if member:
+        # ensemble members: seeded temperature perturbation (0.2 degC)
+        g = np.random.default_rng(100 + member)
+        p = (0.2 * g.standard_normal(A["t"].shape) * A["fsm"][:, :, None]).astype(np.float32)
+        A["t"] = A["t"] + p
+        A["tb"] = A["tb"] + p
+    return A, dict(Sc)
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+            os.unlink(self.path)
+        except Exception:
+            return None
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows]
+        mx = [float(r[2]) for r in rows]
+        reasons = set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            for name, val in zip(names, r[5:9]):
+                if val.strip().lower() in ("active", "1"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def l2_flush(buf):
+    buf.add_(1.0)
+
+
+# ---------------------------------------------------------------------------
+# the B200 arm
+# ---------------------------------------------------------------------------
+
+def launches_of(core, nsteps, time0):
+    """Kernels one npom_step_* call enqueues (see npom_kernels.cu run_steps):
+    the operator coefficients once (implicit), then per internal step A1 A2
+    A3 + PCG + I5 (implicit) or A1 A2 A3 + subcycle (explicit), the nine
+    internal-mode kernels B1-B8 unless the step is the first from rest, and
+    B9."""
+    implicit = core.core_name != "explicit"
+    n = 1 if implicit else 0
+    for s in range(nsteps):
+        iint = 1 + s
+        n += (5 if implicit else 4) + 1
+        if (iint != 1 or time0 != 0.0) and core.mode != 2:
+            n += 9
+    return n
+
+
+def run_b200(args):
+    import torch
+    from neuralpom_b200 import _abi, build, resolve_core_class
+
+    ws_n, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if ws_n > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        pg = dist
+    build.build()
+    A, Sc = workload(member=rank)
+    core = resolve_core_class("implicit_p0_fixed").from_state(A, Sc, device=dev)
+    nin = args.internal_steps
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > L2
+
+    def day():
+        t0 = float(core.time)
+        core.launch_steps(nin, t0, 1, stream)
+        core.time = core.dti * nin / 86400.0 + t0
+        return t0
+
+    for _ in range(args.warmup):
+        day()
+    bits, _ = core.read_status(nin)
+    if bits & (_abi.DEV_TIMEOUT | _abi.DEV_VMAX | _abi.DEV_NONFINITE):
+        raise RuntimeError(f"device status 0x{bits:x} during warm-up")
+
+    launches = 0
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            l2_flush(flush)
+            ev[k][0].record(stream)
+            t0 = day()
+            ev[k][1].record(stream)
+            launches += launches_of(core, nin, t0)
+        torch.cuda.synchronize(dev)
+    if pg:
+        pg.barrier()
+    elapsed_ms = sum(a.elapsed_time(b) for a, b in ev)
+    bits, its = core.read_status(nin)
+    if bits & (_abi.DEV_TIMEOUT | _abi.DEV_VMAX | _abi.DEV_NONFINITE):
+        raise RuntimeError(f"device status 0x{bits:x} in the timed region")
+    t_max = elapsed_ms
+    if pg:
+        t = torch.tensor([elapsed_ms], device=dev, dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        t_max = float(t.item())
+    days_total = ws_n * args.steps * nin * core.dti / 86400.0
+    value = days_total / (t_max / 1000.0)
+
+    # dominant kernel, timed alone on the same stream (CUDA events)
+    roofline = dominant_kernel_roofline(core, stream, dev)
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = end_to_end(core, A, Sc, args, stream, dev, pg, ws_n)
+
+    cpu = None
+    if rank == 0 and ws_n == 1 and not args.no_cpu_baseline:
+        cpu = reference_cpu_sample(A, Sc, internal_steps=args.ref_internal_steps, warm=1, reps=2)
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws_n, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (FP64 PCG dot products)", "data": "synthetic",
+        "config": {"workload": "semi-implicit core, closed 90x82x16 seamount basin (dx=5 km), forward",
+                   "grid": list(GRID), "dti_s": DTI, "internal_steps_per_step": nin, "pcg_tol": 1e-10,
+                   "pcg_iterations_last_step": its[-1] if its else None,
+                   "members": ws_n, "parallelism": f"ensemble x{ws_n}" if ws_n > 1 else "single member",
+                   "l2": "flushed (256 MiB write) before every timed step"},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def dominant_kernel_roofline(core, stream, dev, reps=20):
+    """Time each phase of one internal step alone (CUDA events, after a
+    warm-up) and report the slowest one against the HBM roofline."""
+    import torch
+    from neuralpom_b200 import _abi
+    lib = _abi.load_library()
+    p = core.params()
+    fa = core._fields()
+    ws = core._workspace()
+    im, jm, kb = core.im, core.jm, core.kb
+    n3, n2 = im * jm * kb, im * jm
+    times = {}
+    snapshot = {n: getattr(core, n).clone() for n in _abi.FIELD_NAMES}
+    phases = [i for i, n in enumerate(_abi.PHASES) if n != "I5_corrector_filter" or core.core_name != "explicit"]
+    for ph in phases:
+        for n in _abi.FIELD_NAMES:
+            getattr(core, n).copy_(snapshot[n])
+        for _ in range(3):
+            _abi.check(lib.npom_run_phase(ctypes.byref(p), ctypes.byref(fa), ctypes.byref(ws["struct"]), ph, 1.0,
+                                          ctypes.c_void_p(stream.cuda_stream)), "phase")
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        a.record(stream)
+        for _ in range(reps):
+            _abi.check(lib.npom_run_phase(ctypes.byref(p), ctypes.byref(fa), ctypes.byref(ws["struct"]), ph, 1.0,
+                                          ctypes.c_void_p(stream.cuda_stream)), "phase")
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        times[_abi.PHASES[ph]] = a.elapsed_time(b) / reps
+    for n in _abi.FIELD_NAMES:
+        getattr(core, n).copy_(snapshot[n])
+    core.read_status(0)
+    name = max(times, key=times.get)
+    r3, r2, w3, w2 = PHASE_IO[name]
+    nbytes = 4 * ((r3 + w3) * n3 + (r2 + w2) * n2)
+    if name == "E_external" and core.core_name != "explicit":
+        ni, nj = im - 2, jm - 2
+        nbytes += 4 * (ni * ni + nj * nj + ni * nj)  # DST matrices and eigenvalues
+    sec = times[name] / 1000.0
+    achieved = nbytes / sec / 1e9
+    peak, src = measured_peaks()
+    return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": src, "traffic": None, "algorithmic_bytes": nbytes,
+            "launch_ms": times[name], "phase_ms": {k: round(v, 5) for k, v in times.items()}}
+
+
+def end_to_end(core, A, Sc, args, stream, dev, pg, ws_n):
+    """Same metric through the public drop-in API with the state in pinned
+    host memory: every step copies the full state host->device, advances one
+    simulated day, and reads the prognostic state back."""
+    import torch
+    from neuralpom_b200 import _abi
+    names = list(_abi.FIELD_NAMES)
+    host = {n: torch.from_numpy(np.ascontiguousarray(A[n] if n in A else np.zeros(
+        _abi.field_shape(n, *GRID), np.float32))).pin_memory() for n in names}
+    outs = ("u", "v", "t", "s", "el", "ua", "va", "q2", "q2l", "km", "kh", "w", "rho")
+    host_out = {n: torch.empty_like(host[n]).pin_memory() for n in outs}
+    h2d = sum(host[n].numel() * 4 for n in names)
+    d2h = sum(host_out[n].numel() * 4 for n in outs)
+    nin = args.internal_steps
+    steps = max(1, args.steps // 2)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize(dev)
+    a.record(stream)
+    for _ in range(steps):
+        for n in names:
+            getattr(core, n).copy_(host[n], non_blocking=True)
+        core.time = core.time0 = 1000.0
+        core.launch_steps(nin, 1000.0, 1, stream)
+        for n in outs:
+            host_out[n].copy_(getattr(core, n), non_blocking=True)
+    b.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = a.elapsed_time(b)
+    if pg:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    bits, _ = core.read_status(nin)
+    if bits & (_abi.DEV_TIMEOUT | _abi.DEV_VMAX | _abi.DEV_NONFINITE):
+        raise RuntimeError(f"device status 0x{bits:x} in the end-to-end region")
+    days = ws_n * steps * nin * core.dti / 86400.0
+    return {"value": days / (ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "steps": steps}
+
+
+# ---------------------------------------------------------------------------
+# the reference's own implementation
+# ---------------------------------------------------------------------------
+
+def reference_core(A, Sc, device="cpu"):
+    """Reference implicit core (baseline/_ref install, else the source tree)
+    loaded with this benchmark's state and clock."""
+    from oracle import ref_harness as rh
+    path = os.path.join(ROOT, "baseline", "_ref")
+    if not os.path.isdir(os.path.join(path, "neuralpom")):
+        path = rh.default_reference_path()
+    if path is None:
+        raise RuntimeError("reference package not installed (baseline/_ref missing)")
+    rh.import_reference(path)
+    import torch
+    from neuralpom.cores.implicit_p0_fixed import POM2K_Core
+    from neuralpom.hybrid import build_initialized_core
+    im, jm, kb = A["u"].shape
+    core = build_initialized_core(POM2K_Core, torch.device(device), im, jm, dte=Sc["dte"], isplit=Sc["isplit"])
+    core.prtd1 = core.prtd2 = 1e9
+    core.iprint = 10 ** 9
+    scal = {k: v for k, v in Sc.items() if k in (
+        "alpha", "smoth", "horcon", "eta_solver_rel_tol", "eta_solver_tol", "eta_solver_preconditioner",
+        "barotropic_shapiro", "tracer_shapiro", "velocity_shapiro", "double_gyre_wind_stress_pa", "hmax",
+        "time", "time0")}
+    scal["spatial_shapiro_enabled"] = False
+    rh.load_state(core, {k: v for k, v in A.items() if hasattr(core, k)}, scal)
+    return core, rh
+
+
+def reference_cpu_sample(A, Sc, internal_steps=6, warm=1, reps=2, device="cpu"):
+    import torch
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    core, rh = reference_core(A, Sc, device)
+    rh.advance(core, "implicit_p0_fixed", warm, device=device)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        rh.advance(core, "implicit_p0_fixed", internal_steps, device=device)
+    if device != "cpu":
+        torch.cuda.synchronize()
+    sec = time.perf_counter() - t0
+    days = reps * internal_steps * float(core.dti) / 86400.0
+    return {"value": days / sec, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"{reps} x {internal_steps} internal steps of the 90x82x16 seamount basin "
+                      f"(reference PyTorch core, {device}, after {warm} warm-up step)"}
+
+
+def run_reference(args):
+    ws_n, rank, local = dist_env()
+    if rank != 0:
+        return
+    A, Sc = workload(0)
+    import torch
+    dev = args.ref_device
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    core, rh = reference_core(A, Sc, dev)
+    n = args.ref_internal_steps
+    for _ in range(args.warmup):
+        rh.advance(core, "implicit_p0_fixed", n, device=dev)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        rh.advance(core, "implicit_p0_fixed", n, device=dev)
+    if dev != "cpu":
+        torch.cuda.synchronize()
+    sec = time.perf_counter() - t0
+    days = args.steps * n * float(core.dti) / 86400.0
+    value = days / sec
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0 if dev == "cpu" else 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sec / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "semi-implicit core, closed 90x82x16 seamount basin (dx=5 km), forward",
+                   "grid": list(GRID), "dti_s": DTI, "internal_steps_per_step": n, "device": dev},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{args.steps} x {n} internal steps, reference PyTorch core on {dev}"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,227 @@
+"""Drop-in POM cores whose physical time step runs on the B200 library.
+
+``ExplicitCore`` and ``ImplicitCore`` expose the attribute set of the
+reference ``POM2K_Core`` classes (``src/neuralpom/cores/explicit/core.py:17``,
+``cores/implicit_p0_fixed/core.py:62``): the same tensor names and shapes
+(``explicit/base.py:129-195``), the same scalar attributes, and the step
+function ``run_time_loop()`` that advances ``iend`` internal steps from
+``time0`` and leaves ``iint``/``time``/``ramp`` as the reference does
+(``explicit/time_loop.py:75-88``).  The arithmetic runs in
+``libnpom_b200.so`` (sm_100a) through the C ABI of ``include/npom.h``; there
+is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _abi, cases, state
+
+NUMERICS_VERSION = {
+    "explicit": "explicit-dg-v2-split-smag-v2align-closure",
+    "implicit_p0_fixed": "implicit-dg-v2-aligned-1e5-p0-barotropic-coupling-fixed",
+}
+MAX_STEPS_PER_CALL = 4096
+
+
+class B200Core:
+    """Common state container and C-ABI driver of both cores."""
+
+    core_name = None
+
+    def __init__(self, im, jm, problem_id=4, settings_overrides=None, case_name=None, device=None, kb=16):
+        if problem_id != 4:
+            raise ValueError(f"Only the Double-gyre problem_id=4 is supported; got {problem_id}.")
+        self.device = torch.device(device if device is not None else "cuda")
+        self.im, self.jm, self.kb = int(im), int(jm), int(kb)
+        self.iproblem = problem_id
+        self.case_name = case_name
+        for k, v in state.default_scalars(self.core_name).items():
+            setattr(self, k, v)
+        self._refresh_derived()
+        self.time = 0.0
+        self.time0 = 0.0
+        self.iint = 0
+        self.iend = 2
+        for n in _abi.FIELD_NAMES:
+            setattr(self, n, torch.zeros(_abi.field_shape(n, self.im, self.jm, self.kb), dtype=torch.float32,
+                                         device=self.device))
+        self.period = torch.ones((), dtype=torch.float32, device=self.device)
+        for k, v in dict(settings_overrides or {}).items():
+            setattr(self, k, v)
+        self._refresh_derived()
+        self._ws = None
+        self._ws_key = None
+        self._eta_solver_iteration_history = []
+
+    # -- reference-compatible helpers ------------------------------------
+    @property
+    def NUMERICS_VERSION(self):
+        return NUMERICS_VERSION[self.core_name]
+
+    def _refresh_derived(self):
+        self.imm1, self.imm2 = self.im - 1, self.im - 2
+        self.jmm1, self.jmm2 = self.jm - 1, self.jm - 2
+        self.kbm1, self.kbm2 = self.kb - 1, self.kb - 2
+        state.derived_time(self.__dict__)
+
+    def load_state(self, arrays, scalars=None):
+        """Overwrite tensors (and scalars) from numpy arrays / tensors."""
+        for k, v in (scalars or {}).items():
+            setattr(self, k, v)
+        self._refresh_derived()
+        for k, v in arrays.items():
+            t = torch.as_tensor(np.ascontiguousarray(v) if isinstance(v, np.ndarray) else v)
+            setattr(self, k, t.to(device=self.device, dtype=torch.float32).contiguous().clone())
+        self._ws_key = None
+        return self
+
+    @classmethod
+    def from_state(cls, arrays, scalars, device=None):
+        im, jm, kb = np.asarray(arrays["u"]).shape
+        core = cls(im, jm, device=device, kb=kb)
+        return core.load_state(arrays, scalars)
+
+    def run_initialization(self):
+        """The reference double gyre set-up (cases.py:30 + initialization.py:10)."""
+        arrays, scalars = cases.double_gyre(self.im, self.jm, self.core_name, self.kb)
+        self.load_state(arrays, scalars)
+
+    def state_arrays(self):
+        return {n: getattr(self, n).detach().cpu().numpy().copy() for n in _abi.FIELD_NAMES}
+
+    # -- workspace ---------------------------------------------------------
+    def _workspace(self):
+        geo = tuple((n, getattr(self, n).data_ptr(), getattr(self, n)._version) for n in ("dx", "dy", "h"))
+        key = (self.im, self.jm, self.kb, self.device, geo, float(self.dti), float(self.alpha))
+        if self._ws is not None and self._ws_key == key:
+            return self._ws
+        im, jm, dev = self.im, self.jm, self.device
+        if self._ws is None or self._ws["shape"] != (im, jm):
+            bufs = {n: torch.zeros(_abi.ws_shape(n, im, jm), dtype=torch.float32, device=dev) for n in _abi.WS_NAMES}
+            ws = {"shape": (im, jm), "bufs": bufs,
+                  "partials": torch.zeros(4 * _abi.MAX_COOP_BLOCKS, dtype=torch.float64, device=dev),
+                  # ctrl = [sync x4 | status | pad x3 | cg iterations ...]
+                  "ctrl": torch.zeros(8 + MAX_STEPS_PER_CALL, dtype=torch.int32, device=dev)}
+            s = _abi.NpomWorkspace()
+            for i, n in enumerate(_abi.WS_NAMES):
+                s.buf[i] = bufs[n].data_ptr()
+            base = ws["ctrl"].data_ptr()
+            s.partials = ws["partials"].data_ptr()
+            s.sync = base
+            s.status = base + 4 * 4
+            s.cg_iters = base + 8 * 4
+            ws["struct"] = s
+            self._ws = ws
+        if self.core_name != "explicit":
+            sx, sy, ie = state.spectral_setup(self.dx.detach().cpu().numpy(), self.dy.detach().cpu().numpy(),
+                                              self.h.detach().cpu().numpy(), float(self.dti), float(self.grav),
+                                              float(self.alpha))
+            b = self._ws["bufs"]
+            b["sx"].copy_(torch.from_numpy(sx))
+            b["sy"].copy_(torch.from_numpy(sy))
+            b["inv_eigs"].copy_(torch.from_numpy(ie))
+        self._ws_key = key
+        return self._ws
+
+    def _fields(self):
+        ptrs = []
+        for n in _abi.FIELD_NAMES:
+            t = getattr(self, n)
+            shp = _abi.field_shape(n, self.im, self.jm, self.kb)
+            if not torch.is_tensor(t):
+                raise TypeError(f"{n} must be a tensor")
+            if t.requires_grad:
+                raise NotImplementedError(
+                    f"{n} requires grad: the differentiable advance is not provided by the B200 core")
+            if (tuple(t.shape) != shp or t.dtype != torch.float32 or t.device != self.device
+                    or not t.is_contiguous()):
+                t = t.detach().to(device=self.device, dtype=torch.float32).reshape(shp).contiguous()
+                setattr(self, n, t)
+            ptrs.append(t.data_ptr())
+        return _abi.FieldArray(*ptrs)
+
+    def params(self):
+        return state.make_params(self, self.im, self.jm, self.kb, self.core_name,
+                                 self.device.index if self.device.index is not None else torch.cuda.current_device())
+
+    # -- the step ----------------------------------------------------------
+    def launch_steps(self, nsteps, time0, first_iint=1, stream=None):
+        """Enqueue ``nsteps`` internal steps on ``stream`` without waiting."""
+        lib = _abi.load_library()
+        if self.device.type != "cuda":
+            raise RuntimeError("the B200 core runs on CUDA devices only")
+        p = self.params()
+        fa = self._fields()
+        ws = self._workspace()
+        st = stream if stream is not None else torch.cuda.current_stream(self.device)
+        fn = lib.npom_step_explicit if self.core_name == "explicit" else lib.npom_step_implicit
+        done = 0
+        while done < nsteps:
+            n = min(MAX_STEPS_PER_CALL, nsteps - done)
+            clk = _abi.NpomClock(float(time0), int(first_iint + done), int(n))
+            _abi.check(fn(ctypes.byref(p), ctypes.byref(fa), ctypes.byref(ws["struct"]), ctypes.byref(clk),
+                          ctypes.c_void_p(st.cuda_stream)), "npom step")
+            done += n
+        return ws
+
+    def read_status(self, nsteps=0):
+        """(status bits, PCG iterations of the last call) -- one device sync."""
+        ws = self._ws
+        if ws is None:
+            return 0, []
+        n = min(int(nsteps), MAX_STEPS_PER_CALL)
+        ctrl = ws["ctrl"][4:8 + n].cpu()
+        bits = int(ctrl[0])
+        ws["ctrl"][4].zero_()
+        return bits, [int(v) for v in ctrl[4:4 + n]]
+
+    def run_time_loop(self):
+        """Advance ``iend`` internal steps from ``time0`` (reference
+        run_time_loop semantics); raises FloatingPointError when the
+        barotropic velocity exceeds vmaxl or the elevation is not finite."""
+        nsteps = int(self.iend)
+        if nsteps < 0:
+            raise ValueError("iend must be non-negative")
+        with torch.no_grad():
+            self.launch_steps(nsteps, float(self.time0))
+        bits, its = self.read_status(nsteps)
+        self.iint = nsteps
+        self.time = self.dti * nsteps * 1.0 / 86400.0 + self.time0
+        if self.lramp:
+            r = float(np.float32(self.time) / np.float32(float(self.period)))
+            self.ramp = 1.0 if r > 1.0 else r
+        else:
+            self.ramp = 1.0
+        if self.core_name != "explicit":
+            self._eta_solver_iteration_history.extend(its)
+        self._raise_for(bits)
+
+    def _raise_for(self, bits):
+        if bits & _abi.DEV_TIMEOUT:
+            raise RuntimeError("B200 step: a grid barrier timed out (device status 0x%x)" % bits)
+        if bits & (_abi.DEV_VMAX | _abi.DEV_NONFINITE):
+            raise FloatingPointError(
+                f"Barotropic velocity exceeds limit {self.vmaxl} or elevation not finite at time {self.time}")
+
+
+class ExplicitCore(B200Core):
+    """Explicit mode-split core (reference ``cores/explicit``)."""
+    core_name = "explicit"
+
+
+class ImplicitCore(B200Core):
+    """Semi-implicit free-surface core (reference ``cores/implicit_p0_fixed``)."""
+    core_name = "implicit_p0_fixed"
+
+
+CORE_REGISTRY = {"explicit": ExplicitCore, "implicit_p0_fixed": ImplicitCore}
+
+
+def resolve_core_class(name):
+    """Mirror of ``src/neuralpom/core_factory.py:resolve_core_class``."""
+    if name not in CORE_REGISTRY:
+        raise ValueError(f"Unsupported production core {name!r}; choose from {sorted(CORE_REGISTRY)}.")
+    return CORE_REGISTRY[name]

@@ -88,7 +88,8 @@ def make_params(s, im, jm, kb, core, device=0):
     p.velocity_shapiro = float(get("velocity_shapiro", 0.0) or 0.0)
     if p.velocity_shapiro != 0.0:
         raise ValueError("a non-zero internal-velocity Shapiro filter is not implemented (production uses 0)")
-    p.wind_tau0 = float(get("double_gyre_wind_stress_pa", 0.1) or 0.1)
+    tau0 = get("double_gyre_wind_stress_pa", None)
+    p.wind_tau0 = 0.1 if tau0 is None else float(tau0)
     period = get("period", 1.0)
     p.period = float(np.asarray(period, dtype=np.float64))
     p.inverse_scale = 4.0 * (im - 1) * (jm - 1)

@@ -1,0 +1,124 @@
+"""Parity of the B200 step with the reference (golden vectors) and with the
+oracle at the benchmark sizes, through the public drop-in API."""
+import numpy as np
+import pytest
+import torch
+
+from golden_io import load_step_golden, oracle_params, rel_err
+from oracle import pom_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+STEP_FILES = [("step_explicit_12x10.npz", "explicit"), ("step_implicit_12x10.npz", "implicit_p0_fixed"),
+              ("step_implicit_20x18.npz", "implicit_p0_fixed")]
+
+
+def _core(arrays, scalars, core):
+    from neuralpom_b200 import resolve_core_class
+    return resolve_core_class(core).from_state(arrays, scalars, device="cuda")
+
+
+@pytest.mark.parametrize("fname,core", STEP_FILES)
+def test_gpu_step_matches_reference_golden(fname, core):
+    from neuralpom_b200 import B200Physics
+    A, Sc, OUT = load_step_golden(fname)
+    c = _core(A, Sc, core)
+    phys = B200Physics(core_name=core)
+    done = 0
+    for n in sorted(OUT):
+        c._eta_solver_iteration_history = []
+        phys.advance(c, steps=n - done)
+        assert c.iint == n - done
+        done = n
+        # 1e-5 relative after one step; 1e-4 after three (rounding growth)
+        tol = 1e-5 if n == 1 else 1e-4
+        for f, ref in OUT[n].items():
+            if f.startswith("scalar") or f == "cg_iters":
+                continue
+            got = getattr(c, f).cpu().numpy()
+            assert rel_err(got, ref) < tol, (fname, n, f, rel_err(got, ref))
+        if "cg_iters" in OUT[n]:
+            assert c._eta_solver_iteration_history == [int(v) for v in OUT[n]["cg_iters"]]
+        assert abs(c.time - float(OUT[n]["scalar_time"])) < 1e-9
+
+
+def _oracle_pair(case, steps, core):
+    A, Sc = case
+    Sc = dict(Sc)
+    im, jm, kb = A["u"].shape
+    Sc.update(im=im, jm=jm, kb=kb)
+    c = _core(A, Sc, core)
+    S = {k: v.copy() for k, v in A.items()}
+    P = oracle_params(Sc, A, core)
+    from neuralpom_b200 import B200Physics
+    phys = B200Physics(core_name=core)
+    for _ in range(steps):
+        phys.advance(c, steps=1)
+        O.run(S, P, 1, core)
+    return c, S
+
+
+def test_gpu_seamount_90x82_matches_oracle():
+    """The semi-implicit benchmark basin at full size: the first step from
+    rest and three full steps (PCG tolerance 1e-10, FP64 dots)."""
+    from neuralpom_b200 import cases
+    c, S = _oracle_pair(cases.seamount(90, 82), 4, "implicit_p0_fixed")
+    for f in ("u", "v", "t", "s", "el", "q2", "km", "kh", "w", "rho", "ua", "va", "elf"):
+        got = getattr(c, f).cpu().numpy()
+        assert rel_err(got, S[f]) < 1e-3, (f, rel_err(got, S[f]))
+    for f in ("t", "s"):
+        assert rel_err(getattr(c, f).cpu().numpy(), S[f]) < 1e-5
+
+
+def test_gpu_explicit_basin_64x64_matches_oracle():
+    from neuralpom_b200 import cases
+    c, S = _oracle_pair(cases.noise_basin(64, 64), 3, "explicit")
+    for f in ("u", "v", "t", "s", "el", "q2", "km", "kh", "w", "rho", "ua", "va"):
+        got = getattr(c, f).cpu().numpy()
+        assert rel_err(got, S[f]) < 1e-4, (f, rel_err(got, S[f]))
+
+
+def _budgets(art, fsm, h, et, dz, t, s):
+    vol = art.astype(np.float64) * fsm * (h + et)
+    kbm1 = t.shape[2] - 1
+    lay_t = [(vol * dz[k] * t[:, :, k]).sum() for k in range(kbm1)]
+    lay_s = [(vol * dz[k] * s[:, :, k]).sum() for k in range(kbm1)]
+    return vol.sum(), np.array(lay_t), np.array(lay_s)
+
+
+def test_gpu_conservation_diagnostics_match_oracle():
+    """Volume and layer T/S budgets in FP64 (the reference's volume weights,
+    hybrid/sparse_coupling.py:18-20) agree with the oracle to rounding."""
+    from neuralpom_b200 import cases
+    c, S = _oracle_pair(cases.double_gyre(40, 36, "implicit_p0_fixed"), 3, "implicit_p0_fixed")
+    g = {n: getattr(c, n).cpu().numpy() for n in ("art", "fsm", "h", "et", "dz", "t", "s")}
+    bg = _budgets(g["art"], g["fsm"], g["h"], g["et"], g["dz"], g["t"], g["s"])
+    bo = _budgets(S["art"], S["fsm"], S["h"], S["et"], S["dz"], S["t"], S["s"])
+    assert abs(bg[0] - bo[0]) / abs(bo[0]) < 1e-9
+    np.testing.assert_allclose(bg[1], bo[1], rtol=1e-7)
+    np.testing.assert_allclose(bg[2], bo[2], rtol=1e-7)
+
+
+def test_gpu_run_twice_is_bitwise_deterministic():
+    from neuralpom_b200 import B200Physics, cases
+    A, Sc = cases.seamount(40, 36)
+    outs = []
+    for _ in range(2):
+        c = _core(A, Sc, "implicit_p0_fixed")
+        B200Physics(core_name="implicit_p0_fixed").advance(c, steps=3)
+        outs.append({f: getattr(c, f).cpu().numpy() for f in ("u", "v", "t", "el", "q2", "kh")})
+    for f in outs[0]:
+        assert np.array_equal(outs[0][f], outs[1][f]), f
+
+
+def test_gpu_vmax_raises_floating_point_error():
+    """A barotropic velocity beyond vmaxl is reported by the device status
+    word and raised on the host, like implicit time_loop.py:685-688."""
+    from neuralpom_b200 import B200Physics, cases
+    A, Sc = cases.double_gyre(20, 18, "implicit_p0_fixed")
+    c = _core(A, Sc, "implicit_p0_fixed")
+    c.vmaxl = 1e-12
+    c.time = c.time0 = 1000.0
+    with pytest.raises(FloatingPointError):
+        B200Physics(core_name="implicit_p0_fixed").advance(c, steps=1)
+    torch.cuda.synchronize()

@@ -1,0 +1,72 @@
+"""The oracle against the reference core's own outputs (golden vectors made
+by tests/golden/make_golden.py) and the reference tests' known answers."""
+import numpy as np
+import pytest
+
+from golden_io import golden_path, load_step_golden, oracle_params, rel_err
+from oracle import pom_oracle as O
+
+STEP_FILES = [("step_explicit_12x10.npz", "explicit"), ("step_implicit_12x10.npz", "implicit_p0_fixed"),
+              ("step_implicit_20x18.npz", "implicit_p0_fixed")]
+PROGNOSTIC = ("u", "v", "t", "s", "el", "q2", "q2l", "km", "kh", "w", "rho", "ua", "va", "elf", "etf")
+
+
+@pytest.mark.parametrize("fname,core", STEP_FILES)
+def test_oracle_matches_reference_steps(fname, core):
+    A, Sc, OUT = load_step_golden(fname)
+    S = {k: v.copy() for k, v in A.items()}
+    P = oracle_params(Sc, A, core)
+    done = 0
+    for n in sorted(OUT):
+        hist = O.run(S, P, n - done, core)
+        done = n
+        # one step: 1e-5 relative on every stored field (measured ~4e-7);
+        # three steps: 1e-4 (baroclinic gradient amplifies rounding)
+        tol = 1e-5 if n == 1 else 1e-4
+        for f, ref in OUT[n].items():
+            if f.startswith("scalar") or f == "cg_iters":
+                continue
+            assert rel_err(S[f], ref) < tol, (fname, n, f, rel_err(S[f], ref))
+        if "cg_iters" in OUT[n]:
+            assert hist == [int(v) for v in OUT[n]["cg_iters"]]
+        assert abs(P.time - float(OUT[n]["scalar_time"])) < 1e-9
+
+
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+@pytest.mark.parametrize("nbc", [1, 2, 3, 4])
+def test_oracle_proft_matches_reference_fixture(tag, nbc):
+    z = np.load(golden_path("proft_strict_fixture.npz"))
+    g = lambda n: z[f"{tag}__{n}"]  # noqa: E731
+    out, dh = O.proft(g("f"), g("wfsurf"), g("fsurf"), nbc, g("h"), g("etf"), 1200.0, g("dz"), g("dzz"),
+                      g("swrad"), 2, g("kh"), 1e-6, g("z"))
+    ref = z[f"{tag}__nbc{nbc}__f"]
+    # nbc 2/4 evaluate exp(), whose last bits differ between numpy and torch
+    tol = (1e-10 if nbc in (2, 4) else 1e-13) if tag == "f64" else 2e-6
+    assert rel_err(out, ref) < tol
+    assert np.array_equal(dh, z[f"{tag}__nbc{nbc}__dh"])
+    # the bottom ghost level is passed through untouched
+    assert np.array_equal(out[..., -1], g("f")[..., -1])
+
+
+def test_oracle_proft_uniform_column_known_answer():
+    """tests/test_strict_vertical.py:114-122: a column of 7 with no surface
+    flux stays 7; nbc 3/4 pin the surface value."""
+    z = np.load(golden_path("proft_strict_fixture.npz"))
+    g = lambda n: z[f"f64__{n}"]  # noqa: E731
+    f = np.full_like(g("f"), 7.0)
+    out, _ = O.proft(f, np.zeros_like(g("wfsurf")), g("fsurf"), 1, g("h"), g("etf"), 1200.0, g("dz"), g("dzz"),
+                     g("swrad"), 2, g("kh"), 1e-6, g("z"))
+    np.testing.assert_allclose(out, f, rtol=1e-15, atol=1e-15)
+    for nbc in (3, 4):
+        out, _ = O.proft(f, np.zeros_like(g("wfsurf")), g("fsurf"), nbc, g("h"), g("etf"), 1200.0, g("dz"),
+                         g("dzz"), g("swrad"), 2, g("kh"), 1e-6, g("z"))
+        assert np.array_equal(out[..., 0], g("fsurf"))
+
+
+def test_barotropic_endpoint_transport_identity():
+    """tests/test_fixed_core_runtime.py:41-50 known answer, in the oracle's
+    endpoint-transport form 0.25*(u*dsum + u*dsum) with dsum = 2d."""
+    v = np.array([0.2, -0.3], np.float32)
+    d = np.array([10.0, 20.0], np.float32)
+    got = 0.25 * (v * (2 * d) + v * (2 * d))
+    np.testing.assert_allclose(got, v * d)
