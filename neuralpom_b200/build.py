@@ -19,7 +19,8 @@ CSRC = os.path.join(PKG, "csrc")
 LIBDIR = os.path.join(PKG, "_lib")
 LIBNAME = "libnpom_b200.so"
 SOURCES = ["npom_kernels.cu"]
-HEADERS = ["npom_ctx.cuh", "npom_phases_a.cuh", "npom_phases_ext.cuh", "npom_phases_int.cuh"]
+HEADERS = ["npom_ctx.cuh", "npom_phases_a.cuh", "npom_phases_ext.cuh", "npom_phases_int.cuh", "npom_host.cuh",
+           "npom_pcg_cluster.cuh"]
 
 NVCC_FLAGS = [
     "-O3",

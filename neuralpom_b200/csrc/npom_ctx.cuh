@@ -21,15 +21,12 @@
 
 namespace npom {
 
-// Reads go through L2 (ld.global.cg) on the device: some buffers are written
-// by other thread blocks earlier in the same persistent kernel.
-NPOM_HD float ld(const float *p) {
-#if defined(__CUDA_ARCH__)
-  return __ldcg(p);
-#else
-  return *p;
-#endif
-}
+// Plain loads are L1-cached and coherent within a thread block, which is all
+// the one-phase kernels need (a phase never reads what another block writes
+// in the same launch).  The persistent cooperative kernels read values that
+// other blocks wrote before a grid barrier, so they load through L2
+// (ld.global.cg); Ctx::coh selects that path.
+NPOM_HD float ld(const float *p) { return *p; }
 
 // Scalars of the step, pre-folded the way the reference folds its Python
 // float constants (in double, rounded once to float when they meet a
@@ -58,20 +55,30 @@ struct Ctx {
   unsigned int *status;
   int *cg_iters;
   Consts k;
+  int coh;         // 1: loads bypass L1 (persistent cooperative kernels)
   float ramp;      // per step
   int do_internal; // per step: 0 on the first step from time0 == 0
 };
+
+NPOM_HD float ldc(const Ctx &c, const float *p) {
+#if defined(__CUDA_ARCH__)
+  return c.coh ? __ldcg(p) : *p;
+#else
+  (void)c;
+  return *p;
+#endif
+}
 
 // ---- indexing ----------------------------------------------------------
 #define NPOM_I2(c, i, j) ((size_t)(i) * (c).jm + (size_t)(j))
 #define NPOM_I3(c, i, j, k) (((size_t)(i) * (c).jm + (size_t)(j)) * (c).kb + (size_t)(k))
 
-#define F3(name, i, j, k) ::npom::ld(&c.F[NPOM_F_##name][NPOM_I3(c, i, j, k)])
-#define F2(name, i, j) ::npom::ld(&c.F[NPOM_F_##name][NPOM_I2(c, i, j)])
-#define F1(name, k) ::npom::ld(&c.F[NPOM_F_##name][(k)])
+#define F3(name, i, j, k) ::npom::ldc(c, &c.F[NPOM_F_##name][NPOM_I3(c, i, j, k)])
+#define F2(name, i, j) ::npom::ldc(c, &c.F[NPOM_F_##name][NPOM_I2(c, i, j)])
+#define F1(name, k) ::npom::ldc(c, &c.F[NPOM_F_##name][(k)])
 #define P3(name, i, j, k) (c.F[NPOM_F_##name][NPOM_I3(c, i, j, k)])
 #define P2(name, i, j) (c.F[NPOM_F_##name][NPOM_I2(c, i, j)])
-#define W2(name, i, j) ::npom::ld(&c.W[NPOM_W_##name][NPOM_I2(c, i, j)])
+#define W2(name, i, j) ::npom::ldc(c, &c.W[NPOM_W_##name][NPOM_I2(c, i, j)])
 #define PW2(name, i, j) (c.W[NPOM_W_##name][NPOM_I2(c, i, j)])
 
 NPOM_HD bool interior(const Ctx &c, int i, int j) {

@@ -20,9 +20,12 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
+#include <vector>
 
 #include "npom_phases_int.cuh"
 #include "npom_host.cuh"
+#include "npom_pcg_cluster.cuh"
 
 using namespace npom;
 
@@ -208,7 +211,7 @@ __device__ bool precondition(const Ctx &c, double &rz) {
     if (!grid_barrier(c)) return false;
     for (size_t q = tid; q < nint; q += stride) {
       int a = (int)(q / nj), b = (int)(q % nj);
-      t2[q] = dst_stage_j(c, t1, a, b) * ld(c.W[NPOM_W_inv_eigs] + q);
+      t2[q] = dst_stage_j(c, t1, a, b) * __ldcg(c.W[NPOM_W_inv_eigs] + q);
     }
     if (!grid_barrier(c)) return false;
     for (size_t q = tid; q < nint; q += stride) {
@@ -221,14 +224,14 @@ __device__ bool precondition(const Ctx &c, double &rz) {
       float zval = dst_stage_j(c, t1, a, b) / c.k.inverse_scale;
       size_t o = NPOM_I2(c, a + 1, b + 1);
       zv[o] = zval;
-      rz += (double)ld(r + o) * (double)zval;
+      rz += (double)__ldcg(r + o) * (double)zval;
     }
   } else {
     for (size_t q = tid; q < nint; q += stride) {
       int a = (int)(q / nj), b = (int)(q % nj);
       size_t o = NPOM_I2(c, a + 1, b + 1);
-      float rv = ld(r + o);
-      float zval = rv / (ld(c.W[NPOM_W_diag] + o) + 1e-30f);
+      float rv = __ldcg(r + o);
+      float zval = rv / (__ldcg(c.W[NPOM_W_diag] + o) + 1e-30f);
       zv[o] = zval;
       rz += (double)rv * (double)zval;
     }
@@ -238,8 +241,9 @@ __device__ bool precondition(const Ctx &c, double &rz) {
 
 // Fused PCG free-surface solve (core.py:460-589, eager branch), followed by
 // the Shapiro filter and closed-basin bcond 1 (core.py:893-916) and
-// d = h + elf.  Iterations -> c.cg_iters[step].
-__global__ void __launch_bounds__(kThreads) k_pcg(Ctx c, int step, int with_rhs, int with_post) {
+// d = h + elf.  Iterations -> c.cg_iters[c.sync[2]++] (one slot per solve
+// of the call).
+__global__ void __launch_bounds__(kThreads) k_pcg(Ctx c, int with_rhs, int with_post) {
   const int im = c.im, jm = c.jm, ni = im - 2, nj = jm - 2;
   const size_t ncell = (size_t)im * jm, nint = (size_t)ni * nj;
   const size_t stride = (size_t)gridDim.x * blockDim.x;
@@ -259,7 +263,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg(Ctx c, int step, int with_rhs,
       rhs[q] = 0.0f;
     }
     bool in = interior(c, i, j);
-    x[q] = in ? ld(elf + q) : 0.0f;
+    x[q] = in ? __ldcg(elf + q) : 0.0f;
     if (!in) {
       r[q] = 0.0f;
       p[q] = 0.0f;
@@ -273,7 +277,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg(Ctx c, int step, int with_rhs,
     int i = (int)(q / nj) + 1, j = (int)(q % nj) + 1;
     size_t o = NPOM_I2(c, i, j);
     float a = elliptic_apply_cell(c, x, i, j);
-    float rv = ld(rhs + o) - a;
+    float rv = __ldcg(rhs + o) - a;
     r[o] = rv;
     rr += (double)rv * (double)rv;
     if (c.k.eta_precond != NPOM_PRECOND_SPECTRAL) c.W[NPOM_W_diag][o] = jacobi_diag_cell(c, i, j);
@@ -288,7 +292,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg(Ctx c, int step, int with_rhs,
   double rho_old = grid_total(c, 2);
   for (size_t q = tid; q < nint; q += stride) {
     size_t o = NPOM_I2(c, (int)(q / nj) + 1, (int)(q % nj) + 1);
-    p[o] = ld(zv + o);
+    p[o] = __ldcg(zv + o);
   }
   const double tol_sq = c.k.eta_tol * c.k.eta_tol;
   const double rel_sq = c.k.eta_rel_tol * c.k.eta_rel_tol * (rs0 > 1e-30 ? rs0 : 1e-30);
@@ -302,7 +306,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg(Ctx c, int step, int with_rhs,
       size_t o = NPOM_I2(c, i, j);
       float a = elliptic_apply_cell(c, p, i, j);
       ap[o] = a;
-      pap += (double)ld(p + o) * (double)a;
+      pap += (double)__ldcg(p + o) * (double)a;
     }
     block_sum3(c, pap, 0.0, 0.0, 0, -1, -1);
     if (!grid_barrier(c)) return;
@@ -311,8 +315,8 @@ __global__ void __launch_bounds__(kThreads) k_pcg(Ctx c, int step, int with_rhs,
     double rs = 0.0;
     for (size_t q = tid; q < nint; q += stride) {
       size_t o = NPOM_I2(c, (int)(q / nj) + 1, (int)(q % nj) + 1);
-      x[o] = ld(x + o) + alpha * ld(p + o);
-      float rv = ld(r + o) - alpha * ld(ap + o);
+      x[o] = __ldcg(x + o) + alpha * __ldcg(p + o);
+      float rv = __ldcg(r + o) - alpha * __ldcg(ap + o);
       r[o] = rv;
       rs += (double)rv * (double)rv;
     }
@@ -331,27 +335,29 @@ __global__ void __launch_bounds__(kThreads) k_pcg(Ctx c, int step, int with_rhs,
     float beta = (float)(rho_new / (rho_old + 1e-30));
     for (size_t q = tid; q < nint; q += stride) {
       size_t o = NPOM_I2(c, (int)(q / nj) + 1, (int)(q % nj) + 1);
-      p[o] = ld(p + o) * beta + ld(zv + o);
+      p[o] = __ldcg(p + o) * beta + __ldcg(zv + o);
     }
     rho_old = rho_new;
     if (!grid_barrier(c)) return;
   }
   if (tid == 0) {
-    c.cg_iters[step] = its;
+    unsigned int slot = c.sync[2];
+    c.cg_iters[slot] = its;
+    c.sync[2] = slot + 1;
     if (!converged) atomicOr(c.status, NPOM_DEV_PCG_MAXIT);
   }
   if (!grid_barrier(c)) return;
   if (!with_post) {
     // raw solution into elf (the ring of x is zero)
-    for (size_t q = tid; q < ncell; q += stride) c.F[NPOM_F_elf][q] = ld(x + q);
+    for (size_t q = tid; q < ncell; q += stride) c.F[NPOM_F_elf][q] = __ldcg(x + q);
     return;
   }
   for (size_t q = tid; q < ncell; q += stride) {
     int i = (int)(q / jm), j = (int)(q % jm);
     float e = 0.0f;
     if (interior(c, i, j)) {
-      float x0 = ld(x + q);
-      float sm = x0 + c.k.bshap_q * (ld(x + q + jm) + ld(x + q - jm) + ld(x + q + 1) + ld(x + q - 1) - 4.0f * x0);
+      float x0 = __ldcg(x + q);
+      float sm = x0 + c.k.bshap_q * (__ldcg(x + q + jm) + __ldcg(x + q - jm) + __ldcg(x + q + 1) + __ldcg(x + q - 1) - 4.0f * x0);
       float fsm = F2(fsm, i, j);
       e = (sm * fsm) * fsm;
       if (!(fabsf(e) <= 3.0e38f)) atomicOr(c.status, NPOM_DEV_NONFINITE);
@@ -455,18 +461,83 @@ void launch_cells(const Ctx &c, cudaStream_t s) {
   k_cells<PH><<<blocks_for(n, kThreads), kThreads, 0, s>>>(c);
 }
 
-cudaError_t run_pcg(Ctx &c, int step, int with_rhs, int with_post, cudaStream_t s) {
-  int blocks = 0;
-  cudaError_t e = coop_blocks((const void *)k_pcg, (size_t)(c.im - 2) * (c.jm - 2), &blocks);
-  if (e != cudaSuccess) return e;
-  void *args[] = {&c, &step, &with_rhs, &with_post};
-  return launch_coop((const void *)k_pcg, blocks, args, s);
+// Cluster PCG when the interior fits in one cluster's shared memory (8 CTAs,
+// or 16 with the non-portable cluster size); NPOM_PCG=coop forces the
+// grid-barrier kernel.
+bool pcg_cluster_layout(const Ctx &c, ClusterLayout *out) {
+  const char *env = getenv("NPOM_PCG");
+  if (env && std::strcmp(env, "coop") == 0) return false;
+  int dev = 0, optin = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return false;
+  for (int nc : {8, 16}) {
+    ClusterLayout L = cluster_layout(c.im, c.jm, nc);
+    if (L.bytes() <= (size_t)optin) {
+      *out = L;
+      return true;
+    }
+  }
+  return false;
 }
 
-cudaError_t run_subcycle(Ctx &c, cudaStream_t s) {
-  int blocks = 0;
-  cudaError_t e = coop_blocks((const void *)k_subcycle, (size_t)c.im * c.jm, &blocks);
-  if (e != cudaSuccess) return e;
+// Kernel attributes are set once per device (not inside graph captures).
+bool ensure_cluster_attrs(const ClusterLayout &L) {
+  static int smem_set[64] = {0};
+  static bool nonportable[64] = {false};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
+  const void *fn = (const void *)k_pcg_cluster;
+  if ((int)L.bytes() > smem_set[dev]) {
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.bytes()) != cudaSuccess)
+      return false;
+    smem_set[dev] = (int)L.bytes();
+  }
+  if (L.nc > 8 && !nonportable[dev]) {
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) return false;
+    nonportable[dev] = true;
+  }
+  return true;
+}
+
+cudaError_t run_pcg_cluster(const Ctx &c, const ClusterLayout &L, int with_rhs, int with_post, cudaStream_t s) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(L.nc);
+  cfg.blockDim = dim3(kClusterThreads);
+  cfg.dynamicSmemBytes = L.bytes();
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = L.nc;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_pcg_cluster, c, L, with_rhs, with_post);
+}
+
+// Launch shape of the PCG for this grid, decided outside any capture.
+struct PcgPlan {
+  bool cluster;
+  ClusterLayout L;
+  int coop_blocks;
+};
+
+cudaError_t plan_pcg(const Ctx &c, PcgPlan *plan) {
+  plan->cluster = pcg_cluster_layout(c, &plan->L) && ensure_cluster_attrs(plan->L);
+  plan->coop_blocks = 0;
+  if (plan->cluster) return cudaSuccess;
+  return coop_blocks((const void *)k_pcg, (size_t)(c.im - 2) * (c.jm - 2), &plan->coop_blocks);
+}
+
+cudaError_t run_pcg(Ctx c, const PcgPlan &plan, int with_rhs, int with_post, cudaStream_t s) {
+  if (plan.cluster) return run_pcg_cluster(c, plan.L, with_rhs, with_post, s);
+  c.coh = 1;
+  void *args[] = {&c, &with_rhs, &with_post};
+  return launch_coop((const void *)k_pcg, plan.coop_blocks, args, s);
+}
+
+cudaError_t run_subcycle(Ctx c, int blocks, cudaStream_t s) {
+  c.coh = 1;
   void *args[] = {&c};
   return launch_coop((const void *)k_subcycle, blocks, args, s);
 }
@@ -483,39 +554,124 @@ void internal_mode(const Ctx &c, cudaStream_t s) {
   launch_cols<CP_B8>(c, s);
 }
 
+// Enqueue one internal step (all its kernels) on s.
+cudaError_t enqueue_step(const Ctx &c, int core, const PcgPlan &plan, int sub_blocks, cudaStream_t s) {
+  launch_points<PP_A1>(c, s);
+  launch_cols<CP_A2>(c, s);
+  launch_cells<XP_A3>(c, s);
+  cudaError_t e;
+  if (core == NPOM_CORE_IMPLICIT) {
+    e = run_pcg(c, plan, 1, 1, s);
+    if (e != cudaSuccess) return e;
+    launch_cells<XP_I5>(c, s);
+  } else {
+    e = run_subcycle(c, sub_blocks, s);
+    if (e != cudaSuccess) return e;
+  }
+  if (c.do_internal) internal_mode(c, s);
+  launch_cols<CP_B9>(c, s);
+  return cudaGetLastError();
+}
+
+// CUDA graphs of one internal step, keyed by the launch context (pointers,
+// settings, ramp, do_internal) and device.  Steps with ramp < 1 (the first
+// inertial period from rest) launch directly; every other step replays a
+// cached graph, which removes the host launch cost of the ~15 kernels.
+struct GraphEntry {
+  int device;
+  int core;
+  Ctx key;
+  cudaGraphExec_t exec;
+};
+
+std::mutex g_graph_mutex;
+std::vector<GraphEntry> g_graphs;
+cudaStream_t g_capture_stream[64] = {nullptr};
+bool g_capture_failed[64][2] = {};
+
+bool graphs_enabled() {
+  const char *env = getenv("NPOM_GRAPH");
+  return !(env && std::strcmp(env, "0") == 0);
+}
+
+cudaError_t launch_step_graph(const Ctx &c, int core, const PcgPlan &plan, int sub_blocks, cudaStream_t s,
+                              bool *launched) {
+  *launched = false;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= 64) return e;
+  std::lock_guard<std::mutex> lock(g_graph_mutex);
+  for (auto &g : g_graphs) {
+    if (g.device == dev && g.core == core && std::memcmp(&g.key, &c, sizeof(Ctx)) == 0) {
+      e = cudaGraphLaunch(g.exec, s);
+      *launched = (e == cudaSuccess);
+      return e;
+    }
+  }
+  if (g_capture_failed[dev][core]) return cudaSuccess;
+  if (!g_capture_stream[dev]) {
+    e = cudaStreamCreateWithFlags(&g_capture_stream[dev], cudaStreamNonBlocking);
+    if (e != cudaSuccess) return e;
+  }
+  cudaStream_t cs = g_capture_stream[dev];
+  e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return e;
+  cudaError_t le = enqueue_step(c, core, plan, sub_blocks, cs);
+  cudaGraph_t graph = nullptr;
+  e = cudaStreamEndCapture(cs, &graph);
+  if (le != cudaSuccess || e != cudaSuccess || !graph) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    g_capture_failed[dev][core] = true;
+    return cudaSuccess;  // not captured: the caller launches directly
+  }
+  cudaGraphExec_t exec = nullptr;
+  e = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    g_capture_failed[dev][core] = true;
+    return cudaSuccess;
+  }
+  if (g_graphs.size() >= 16) {
+    cudaGraphExecDestroy(g_graphs.front().exec);
+    g_graphs.erase(g_graphs.begin());
+  }
+  g_graphs.push_back(GraphEntry{dev, core, c, exec});
+  e = cudaGraphLaunch(exec, s);
+  *launched = (e == cudaSuccess);
+  return e;
+}
+
 npom_status run_steps(const npom_params *p, float *const *fields, const npom_workspace *ws, const npom_clock *clk,
                       void *stream, int core) {
   if (!check_args_dev(p, fields, ws) || !clk || clk->nsteps < 0 || p->core != core) return NPOM_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   Ctx c = make_ctx(p, fields, ws);
-  // a barrier that timed out may leave its arrival counter non-zero
-  if (cudaMemsetAsync(ws->sync, 0, 2 * sizeof(unsigned int), s) != cudaSuccess) return NPOM_ERR_CUDA;
+  // a barrier that timed out may leave its arrival counter non-zero;
+  // sync[2] counts the PCG solves of this call
+  if (cudaMemsetAsync(ws->sync, 0, 4 * sizeof(unsigned int), s) != cudaSuccess) return NPOM_ERR_CUDA;
+  PcgPlan plan{};
+  int sub_blocks = 0;
   if (core == NPOM_CORE_IMPLICIT) {
+    if (plan_pcg(c, &plan) != cudaSuccess) return NPOM_ERR_CUDA;
     launch_cells<XP_COEF>(c, s);
+  } else {
+    if (coop_blocks((const void *)k_subcycle, (size_t)c.im * c.jm, &sub_blocks) != cudaSuccess) return NPOM_ERR_CUDA;
   }
+  const bool graphs = graphs_enabled();
   for (int n = 0; n < clk->nsteps; ++n) {
     int iint = clk->first_iint + n;
     double time = p->dti * iint * 1.0 / 86400.0 + clk->time0;
     c.ramp = ramp_of(p, time);
     c.do_internal = ((iint != 1 || clk->time0 != 0.0) && p->mode != 2) ? 1 : 0;
-    launch_points<PP_A1>(c, s);
-    launch_cols<CP_A2>(c, s);
-    launch_cells<XP_A3>(c, s);
-    cudaError_t e;
-    if (core == NPOM_CORE_IMPLICIT) {
-      e = run_pcg(c, n, 1, 1, s);
-      if (e != cudaSuccess) return NPOM_ERR_CUDA;
-      launch_cells<XP_I5>(c, s);
-    } else {
-      e = run_subcycle(c, s);
-      if (e != cudaSuccess) return NPOM_ERR_CUDA;
+    bool done = false;
+    if (graphs && c.ramp == 1.0f) {
+      if (launch_step_graph(c, core, plan, sub_blocks, s, &done) != cudaSuccess) return NPOM_ERR_CUDA;
     }
-    if (c.do_internal) internal_mode(c, s);
-    launch_cols<CP_B9>(c, s);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return NPOM_ERR_CUDA;
+    if (!done && enqueue_step(c, core, plan, sub_blocks, s) != cudaSuccess) return NPOM_ERR_CUDA;
   }
-  return NPOM_OK;
+  return cudaGetLastError() == cudaSuccess ? NPOM_OK : NPOM_ERR_CUDA;
 }
 
 const char *kFieldNames[] = {
@@ -571,11 +727,18 @@ npom_status npom_run_phase(const npom_params *p, float *const *fields, const npo
     case 1: launch_cols<CP_A2>(c, s); break;
     case 2: launch_cells<XP_A3>(c, s); break;
     case 3:
+      if (cudaMemsetAsync(ws->sync, 0, 4 * sizeof(unsigned int), s) != cudaSuccess) return NPOM_ERR_CUDA;
       if (p->core == NPOM_CORE_IMPLICIT) {
-        launch_cells<XP_COEF>(c, s);
-        e = run_pcg(c, 0, 1, 1, s);
+        PcgPlan plan{};
+        e = plan_pcg(c, &plan);
+        if (e == cudaSuccess) {
+          launch_cells<XP_COEF>(c, s);
+          e = run_pcg(c, plan, 1, 1, s);
+        }
       } else {
-        e = run_subcycle(c, s);
+        int blocks = 0;
+        e = coop_blocks((const void *)k_subcycle, (size_t)c.im * c.jm, &blocks);
+        if (e == cudaSuccess) e = run_subcycle(c, blocks, s);
       }
       break;
     case 4: launch_cells<XP_I5>(c, s); break;
@@ -611,8 +774,12 @@ npom_status npom_pcg_solve(const npom_params *p, float *const *fields, const npo
   if (!check_args_dev(p, fields, ws) || p->core != NPOM_CORE_IMPLICIT) return NPOM_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   Ctx c = make_ctx(p, fields, ws);
+  if (cudaMemsetAsync(ws->sync, 0, 4 * sizeof(unsigned int), s) != cudaSuccess) return NPOM_ERR_CUDA;
+  PcgPlan plan{};
+  cudaError_t e = plan_pcg(c, &plan);
+  if (e != cudaSuccess) return NPOM_ERR_CUDA;
   launch_cells<XP_COEF>(c, s);
-  cudaError_t e = run_pcg(c, 0, 0, 0, s);
+  e = run_pcg(c, plan, 0, 0, s);
   if (e != cudaSuccess) return NPOM_ERR_CUDA;
   return cudaGetLastError() == cudaSuccess ? NPOM_OK : NPOM_ERR_CUDA;
 }

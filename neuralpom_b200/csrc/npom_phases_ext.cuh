@@ -133,19 +133,19 @@ NPOM_HD void elliptic_coeff_cell(const Ctx &c, int i, int j) {
 // eta is a workspace or field vector with a zero Dirichlet ring.
 NPOM_HD float elliptic_apply_cell(const Ctx &c, const float *eta, int i, int j) {
   const size_t o = NPOM_I2(c, i, j);
-  float e = ld(eta + o);
+  float e = ldc(c, eta + o);
   if (!interior(c, i, j)) return e;
   const float *dd = c.F[NPOM_F_d];
   const int jm = c.jm;
-  float d0 = ld(dd + o);
-  float he = 0.5f * (ld(dd + o + jm) + d0);
-  float hw = 0.5f * (d0 + ld(dd + o - jm));
-  float hn = 0.5f * (ld(dd + o + 1) + d0);
-  float hs = 0.5f * (d0 + ld(dd + o - 1));
-  float fe = he * (ld(eta + o + jm) - e) * W2(ce, i, j) * F2(dum, i + 1, j);
-  float fw = hw * (e - ld(eta + o - jm)) * W2(cw, i, j) * F2(dum, i, j);
-  float fn = hn * (ld(eta + o + 1) - e) * W2(cn, i, j) * F2(dvm, i, j + 1);
-  float fs = hs * (e - ld(eta + o - 1)) * W2(cs, i, j) * F2(dvm, i, j);
+  float d0 = ldc(c, dd + o);
+  float he = 0.5f * (ldc(c, dd + o + jm) + d0);
+  float hw = 0.5f * (d0 + ldc(c, dd + o - jm));
+  float hn = 0.5f * (ldc(c, dd + o + 1) + d0);
+  float hs = 0.5f * (d0 + ldc(c, dd + o - 1));
+  float fe = he * (ldc(c, eta + o + jm) - e) * W2(ce, i, j) * F2(dum, i + 1, j);
+  float fw = hw * (e - ldc(c, eta + o - jm)) * W2(cw, i, j) * F2(dum, i, j);
+  float fn = hn * (ldc(c, eta + o + 1) - e) * W2(cn, i, j) * F2(dvm, i, j + 1);
+  float fs = hs * (e - ldc(c, eta + o - 1)) * W2(cs, i, j) * F2(dvm, i, j);
   float div = (fe - fw + fn - fs) * W2(inv_art, i, j);
   return e - c.k.implicit_coeff * div;
 }
@@ -171,8 +171,8 @@ NPOM_HD float dst_stage_i(const Ctx &c, const float *src, bool src_is_grid, int 
   const float *sx = c.W[NPOM_W_sx];
   double acc = 0.0;
   for (int m = 0; m < ni; ++m) {
-    float v = src_is_grid ? ld(src + NPOM_I2(c, m + 1, b + 1)) : ld(src + (size_t)m * nj + b);
-    acc += (double)ld(sx + (size_t)a * ni + m) * (double)v;
+    float v = src_is_grid ? ldc(c, src + NPOM_I2(c, m + 1, b + 1)) : ldc(c, src + (size_t)m * nj + b);
+    acc += (double)ldc(c, sx + (size_t)a * ni + m) * (double)v;
   }
   return (float)acc;
 }
@@ -180,7 +180,7 @@ NPOM_HD float dst_stage_j(const Ctx &c, const float *src, int a, int b) {
   const int nj = c.jm - 2;
   const float *sy = c.W[NPOM_W_sy];
   double acc = 0.0;
-  for (int m = 0; m < nj; ++m) acc += (double)ld(src + (size_t)a * nj + m) * (double)ld(sy + (size_t)m * nj + b);
+  for (int m = 0; m < nj; ++m) acc += (double)ldc(c, src + (size_t)a * nj + m) * (double)ldc(c, sy + (size_t)m * nj + b);
   return (float)acc;
 }
 

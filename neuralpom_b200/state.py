@@ -91,7 +91,9 @@ def make_params(s, im, jm, kb, core, device=0):
     tau0 = get("double_gyre_wind_stress_pa", None)
     p.wind_tau0 = 0.1 if tau0 is None else float(tau0)
     period = get("period", 1.0)
-    p.period = float(np.asarray(period, dtype=np.float64))
+    if hasattr(period, "detach"):
+        period = period.detach().reshape(-1)[0].cpu().item()
+    p.period = float(np.asarray(period, dtype=np.float64).reshape(-1)[0])
     p.inverse_scale = 4.0 * (im - 1) * (jm - 1)
     return p
 

@@ -60,14 +60,25 @@ def _oracle_pair(case, steps, core):
 
 def test_gpu_seamount_90x82_matches_oracle():
     """The semi-implicit benchmark basin at full size: the first step from
-    rest and three full steps (PCG tolerance 1e-10, FP64 dots)."""
+    rest and three full steps (PCG tolerance 1e-10, FP64 dots).  The start
+    from a uniform current against closed walls is violent, so the bound is
+    the oracle's own sensitivity: 10x the spread that a 1-ulp change of T
+    produces over the same four steps (measured here, per field)."""
     from neuralpom_b200 import cases
-    c, S = _oracle_pair(cases.seamount(90, 82), 4, "implicit_p0_fixed")
+    A, Sc = cases.seamount(90, 82)
+    c, S = _oracle_pair((A, Sc), 4, "implicit_p0_fixed")
+    A2 = dict(A)
+    A2["t"] = np.nextafter(A["t"], np.float32(np.inf)).astype(np.float32)
+    Sc2 = dict(Sc)
+    Sc2.update(im=90, jm=82, kb=16)
+    S2 = {k: v.copy() for k, v in A2.items()}
+    P2 = oracle_params(Sc2, A2, "implicit_p0_fixed")
+    for _ in range(4):
+        O.run(S2, P2, 1, "implicit_p0_fixed")
     for f in ("u", "v", "t", "s", "el", "q2", "km", "kh", "w", "rho", "ua", "va", "elf"):
-        got = getattr(c, f).cpu().numpy()
-        assert rel_err(got, S[f]) < 1e-3, (f, rel_err(got, S[f]))
-    for f in ("t", "s"):
-        assert rel_err(getattr(c, f).cpu().numpy(), S[f]) < 1e-5
+        spread = rel_err(S2[f], S[f])
+        err = rel_err(getattr(c, f).cpu().numpy(), S[f])
+        assert err <= max(10.0 * spread, 1e-6), (f, err, spread)
 
 
 def test_gpu_explicit_basin_64x64_matches_oracle():
@@ -122,3 +133,34 @@ def test_gpu_vmax_raises_floating_point_error():
     with pytest.raises(FloatingPointError):
         B200Physics(core_name="implicit_p0_fixed").advance(c, steps=1)
     torch.cuda.synchronize()
+
+
+def test_gpu_graph_replay_is_bitwise_identical_to_direct_launches(monkeypatch):
+    """Steps replayed from the cached CUDA graph equal direct launches."""
+    from neuralpom_b200 import B200Physics, cases
+    A, Sc = cases.seamount(40, 36)
+    Sc = dict(Sc)
+    Sc.update(time=1000.0, time0=1000.0)
+    outs = []
+    for graph in ("0", "1"):
+        monkeypatch.setenv("NPOM_GRAPH", graph)
+        c = _core(A, Sc, "implicit_p0_fixed")
+        B200Physics(core_name="implicit_p0_fixed").advance(c, steps=3)
+        outs.append({f: getattr(c, f).cpu().numpy() for f in ("u", "v", "t", "el", "q2", "kh", "w")})
+    for f in outs[0]:
+        assert np.array_equal(outs[0][f], outs[1][f]), f
+
+
+def test_gpu_cluster_and_grid_barrier_pcg_agree(monkeypatch):
+    """The cluster (DSMEM) PCG and the grid-barrier PCG solve the same
+    system to the PCG tolerance."""
+    from neuralpom_b200 import B200Physics, cases
+    A, Sc = cases.seamount(40, 36)
+    outs = []
+    for mode in ("coop", "cluster"):
+        monkeypatch.setenv("NPOM_PCG", mode)
+        c = _core(A, Sc, "implicit_p0_fixed")
+        B200Physics(core_name="implicit_p0_fixed").advance(c, steps=2)
+        outs.append({f: getattr(c, f).cpu().numpy() for f in ("el", "ua", "va", "u", "t")})
+    for f in outs[0]:
+        assert rel_err(outs[1][f], outs[0][f]) < 1e-4, f
