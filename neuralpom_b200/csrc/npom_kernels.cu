@@ -26,6 +26,7 @@
 #include "npom_phases_int.cuh"
 #include "npom_host.cuh"
 #include "npom_pcg_cluster.cuh"
+#include "npom_lanes.cuh"
 
 using namespace npom;
 
@@ -80,6 +81,27 @@ __global__ void __launch_bounds__(128) k_cols(Ctx c) {
   else if (PH == CP_B6) phase_b6_column(c, i, j);
   else if (PH == CP_B8) phase_b8_column(c, i, j);
   else if (PH == CP_B9) phase_b9_column(c, i, j);
+}
+
+// One 16-lane segment per water column (kb == 16).  Threads past the last
+// column work on a copy of it and store nothing, so that every shuffle sees
+// all 32 lanes of its warp.
+template <int PH>
+__global__ void __launch_bounds__(kThreads) k_lanes(Ctx c) {
+  const int ncol = c.im * c.jm;
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  int col = p >> 4;
+  const int k = p & (KL - 1);
+  const bool st = col < ncol;
+  if (!st) col = ncol - 1;
+  const int j = col % c.jm, i = col / c.jm;
+  if (PH == CP_A2) lane_a2(c, i, j, k, st);
+  else if (PH == CP_B1) lane_b1(c, i, j, k, st);
+  else if (PH == CP_B2A) lane_b2a(c, i, j, k, st);
+  else if (PH == CP_B3) lane_b3(c, i, j, k, st);
+  else if (PH == CP_B6) lane_b6(c, i, j, k, st);
+  else if (PH == CP_B8) lane_b8(c, i, j, k, st);
+  else if (PH == CP_B9) lane_b9(c, i, j, k, st);
 }
 
 template <int PH>
@@ -450,10 +472,23 @@ void launch_points(const Ctx &c, cudaStream_t s) {
   size_t n = (size_t)c.im * c.jm * c.kb;
   k_points<PH><<<blocks_for(n, kThreads), kThreads, 0, s>>>(c);
 }
+// Column phases: with kb == 16 one 16-lane segment per column (lane = level,
+// npom_lanes.cuh); otherwise one thread per column.  NPOM_LANES=0 forces the
+// thread-per-column bodies.
+bool lanes_enabled(const Ctx &c) {
+  if (c.kb != KL) return false;
+  const char *env = getenv("NPOM_LANES");
+  return !(env && std::strcmp(env, "0") == 0);
+}
+
 template <int PH>
 void launch_cols(const Ctx &c, cudaStream_t s) {
   size_t n = (size_t)c.im * c.jm;
-  k_cols<PH><<<blocks_for(n, 128), 128, 0, s>>>(c);
+  if (lanes_enabled(c)) {
+    k_lanes<PH><<<blocks_for(n * KL, kThreads), kThreads, 0, s>>>(c);
+  } else {
+    k_cols<PH><<<blocks_for(n, 128), 128, 0, s>>>(c);
+  }
 }
 template <int PH>
 void launch_cells(const Ctx &c, cudaStream_t s) {

@@ -32,7 +32,7 @@ constexpr int kClusterThreads = 1024;
 struct ClusterLayout {
   int ni, nj, nc, rows, rp;  // interior size, CTAs, rows per CTA (rp: padded to 4)
   // float offsets in dynamic shared memory
-  int x, r, z, ap, rhs, p, he, hw, hn, hs, ce, cw, cn, cs, me, mw, mn, ms, iart, t1, cm, g, sxt, sy, ie;
+  int x, r, z, ap, rhs, p, he, hw, hn, hs, ce, cw, cn, cs, me, mw, mn, ms, iart, t1, cm, g, sxt, sy, ie, ks;
   int floats;
   size_t bytes() const { return (size_t)floats * sizeof(float) + 64 * sizeof(double); }
 };
@@ -76,52 +76,57 @@ inline ClusterLayout cluster_layout(int im, int jm, int nc) {
   L.sxt = take(L.ni * L.rp);  // Sx rows of the slab, transposed [m][row]
   L.sy = take(L.nj * L.nj);
   L.ie = take(rn);
+  L.ks = take(4 * kClusterThreads);  // split-K partials of the DST stages (float4 each)
   L.floats = o;
   return L;
 }
 
-// block-wide FP64 sum; the CTA's total is left in part[slot] (thread 0)
+// block-wide FP64 sum (fixed shuffle tree); the CTA's total is left in
+// part[slot] by warp 0
 __device__ __forceinline__ void cl_block_sum(double v, double *red, double *part, int slot) {
   for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (lane == 0) red[w] = v;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += red[q];
-    part[slot] = t;
+  if (w == 0) {
+    const int nw = (int)(blockDim.x >> 5);
+    double t = lane < nw ? red[lane] : 0.0;
+    for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
+    if (lane == 0) part[slot] = t;
   }
 }
 
-// after a cluster barrier: sum of part[slot] over the cluster, rank order
-__device__ __forceinline__ double cl_total(cgx::cluster_group &cl, double *part, int slot, int nc) {
-  double t = 0.0;
-  for (int q = 0; q < nc; ++q) t += *cl.map_shared_rank(part + slot, q);
-  return t;
+// after a cluster barrier: sum of part[slot] over the cluster.  Warp 0 reads
+// the nc partials in parallel and reduces them with the same shuffle tree in
+// every CTA, so all CTAs obtain bitwise the same total.
+__device__ __forceinline__ double cl_total(cgx::cluster_group &cl, double *part, int slot, int nc, double *bcast) {
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    double t = lane < nc ? *cl.map_shared_rank(part + slot, lane) : 0.0;
+    for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
+    if (lane == 0) bcast[slot] = t;
+  }
+  __syncthreads();
+  return bcast[slot];
 }
 
-// g <- all rows of the slab array at src_off (row length nj) of every CTA
+// g <- all rows of the slab array at src_off (row length nj) of every CTA:
+// the slab of CTA q is contiguous and lands at row q*rows of g
 __device__ __forceinline__ void cl_gather(cgx::cluster_group &cl, const ClusterLayout &L, float *sm, int src_off,
                                           float *g) {
   const int nj = L.nj;
-  if ((nj & 3) == 0) {
-    const int n4 = (L.ni * nj) >> 2, nj4 = nj >> 2;
-    float4 *g4 = reinterpret_cast<float4 *>(g);
-    for (int f = threadIdx.x; f < n4; f += blockDim.x) {
-      int a = f / nj4;
-      int q = a / L.rows;
-      int la = a - q * L.rows;
-      const float4 *remote = reinterpret_cast<const float4 *>(cl.map_shared_rank(sm + src_off, q));
-      g4[f] = remote[la * nj4 + (f - a * nj4)];
-    }
-  } else {
-    const int n = L.ni * nj;
-    for (int e = threadIdx.x; e < n; e += blockDim.x) {
-      int a = e / nj;
-      int q = a / L.rows;
-      int la = a - q * L.rows;
-      const float *remote = cl.map_shared_rank(sm + src_off, q);
-      g[e] = remote[la * nj + (e - a * nj)];
+  for (int q = 0; q < L.nc; ++q) {
+    const int nrq = min(L.rows, L.ni - q * L.rows);
+    if (nrq <= 0) break;
+    const float *remote = cl.map_shared_rank(sm + src_off, q);
+    float *dst = g + (size_t)q * L.rows * nj;
+    if ((nj & 3) == 0) {
+      const int n4 = (nrq * nj) >> 2;
+      const float4 *r4 = reinterpret_cast<const float4 *>(remote);
+      float4 *d4 = reinterpret_cast<float4 *>(dst);
+      for (int f = threadIdx.x; f < n4; f += blockDim.x) d4[f] = r4[f];
+    } else {
+      for (int e = threadIdx.x; e < nrq * nj; e += blockDim.x) dst[e] = remote[e];
     }
   }
 }
@@ -176,40 +181,70 @@ __device__ __forceinline__ double cl_spmv(const ClusterLayout &L, float *sm, flo
   return acc;
 }
 
-// DST along i for four slab rows: t1T[b][4g..4g+3] = sum_m Sx[row][m] g[m][b]
+// The two DST stages compute, for every output group (four slab rows x one
+// column), a length-K dot product.  The K range is split KS ways so that all
+// warps of the CTA work (KS * groups <= blockDim); the KS partial float4s are
+// then summed in split order.
+__device__ __forceinline__ int cl_splits(int ng) {
+  int ks = (int)blockDim.x / (ng > 0 ? ng : 1);
+  return ks < 1 ? 1 : (ks > 8 ? 8 : ks);
+}
+
+// DST along i: t1T[b][4g..4g+3] = sum_m Sx[row][m] g[m][b]
 __device__ __forceinline__ void cl_dst_i(const ClusterLayout &L, float *sm, int nr) {
-  const int nj = L.nj, rp = L.rp, groups = (nr + 3) >> 2;
+  const int nj = L.nj, rp = L.rp, groups = (nr + 3) >> 2, ng = groups * nj;
+  const int ks = cl_splits(ng), mlen = (L.ni + ks - 1) / ks;
   const float *g = sm + L.g, *sxt = sm + L.sxt;
-  float *t1 = sm + L.t1;
-  for (int t = threadIdx.x; t < groups * nj; t += blockDim.x) {
-    int grp = t / nj, b = t - grp * nj;
+  float4 *part = reinterpret_cast<float4 *>(sm + L.ks);
+  for (int t = threadIdx.x; t < ng * ks; t += blockDim.x) {
+    int s = t / ng, og = t - s * ng;
+    int grp = og / nj, b = og - grp * nj;
+    int m0 = s * mlen, m1 = min(L.ni, m0 + mlen);
     float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
     const float *sc = sxt + 4 * grp;
 #pragma unroll 4
-    for (int m = 0; m < L.ni; ++m) {
+    for (int m = m0; m < m1; ++m) {
       float gv = g[m * nj + b];
-      float4 s = *reinterpret_cast<const float4 *>(sc + m * rp);
-      a0 += s.x * gv;
-      a1 += s.y * gv;
-      a2 += s.z * gv;
-      a3 += s.w * gv;
+      float4 sv = *reinterpret_cast<const float4 *>(sc + m * rp);
+      a0 += sv.x * gv;
+      a1 += sv.y * gv;
+      a2 += sv.z * gv;
+      a3 += sv.w * gv;
     }
-    *reinterpret_cast<float4 *>(t1 + b * rp + 4 * grp) = make_float4(a0, a1, a2, a3);
+    part[t] = make_float4(a0, a1, a2, a3);
+  }
+  __syncthreads();
+  float *t1 = sm + L.t1;
+  for (int og = threadIdx.x; og < ng; og += blockDim.x) {
+    float4 v = part[og];
+    for (int s = 1; s < ks; ++s) {
+      float4 w = part[s * ng + og];
+      v.x += w.x;
+      v.y += w.y;
+      v.z += w.z;
+      v.w += w.w;
+    }
+    int grp = og / nj, b = og - grp * nj;
+    *reinterpret_cast<float4 *>(t1 + b * rp + 4 * grp) = v;
   }
 }
 
-// DST along j for four slab rows: out[row][l] = (sum_b t1T[b][row] Sy[b][l])
-// times scale[row][l] (the inverse eigenvalues) or divided by div
+// DST along j: out[row][l] = (sum_b t1T[b][row] Sy[b][l]) times scale[row][l]
+// (the inverse eigenvalues) or divided by div; accumulates r.out into rz
 __device__ __forceinline__ void cl_dst_j(const ClusterLayout &L, float *sm, int nr, float *out, const float *scale,
                                          float div, const float *r, double &rz) {
-  const int nj = L.nj, rp = L.rp, groups = (nr + 3) >> 2;
+  const int nj = L.nj, rp = L.rp, groups = (nr + 3) >> 2, ng = groups * nj;
+  const int ks = cl_splits(ng), blen = (nj + ks - 1) / ks;
   const float *t1 = sm + L.t1, *sy = sm + L.sy;
-  for (int t = threadIdx.x; t < groups * nj; t += blockDim.x) {
-    int grp = t / nj, l = t - grp * nj;
+  float4 *part = reinterpret_cast<float4 *>(sm + L.ks);
+  for (int t = threadIdx.x; t < ng * ks; t += blockDim.x) {
+    int s = t / ng, og = t - s * ng;
+    int grp = og / nj, l = og - grp * nj;
+    int b0 = s * blen, b1 = min(nj, b0 + blen);
     float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
     const float *tc = t1 + 4 * grp;
 #pragma unroll 4
-    for (int b = 0; b < nj; ++b) {
+    for (int b = b0; b < b1; ++b) {
       float syv = sy[b * nj + l];
       float4 tv = *reinterpret_cast<const float4 *>(tc + b * rp);
       a0 += tv.x * syv;
@@ -217,15 +252,28 @@ __device__ __forceinline__ void cl_dst_j(const ClusterLayout &L, float *sm, int 
       a2 += tv.z * syv;
       a3 += tv.w * syv;
     }
-    float acc[4] = {a0, a1, a2, a3};
+    part[t] = make_float4(a0, a1, a2, a3);
+  }
+  __syncthreads();
+  for (int og = threadIdx.x; og < ng; og += blockDim.x) {
+    float4 v = part[og];
+    for (int s = 1; s < ks; ++s) {
+      float4 w = part[s * ng + og];
+      v.x += w.x;
+      v.y += w.y;
+      v.z += w.z;
+      v.w += w.w;
+    }
+    int grp = og / nj, l = og - grp * nj;
+    float acc[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       int ra = 4 * grp + q;
       if (ra < nr) {
         int e = ra * nj + l;
-        float v = scale ? acc[q] * scale[e] : acc[q] / div;
-        out[e] = v;
-        if (r) rz += (double)r[e] * (double)v;
+        float val = scale ? acc[q] * scale[e] : acc[q] / div;
+        out[e] = val;
+        if (r) rz += (double)r[e] * (double)val;
       }
     }
   }
@@ -268,6 +316,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1)
   extern __shared__ __align__(16) float sm[];
   double *red = reinterpret_cast<double *>(sm + L.floats);  // 32 doubles
   double *part = red + 32;                                    // 8 slots
+  double *bcast = part + 8;                                   // 8 slots
   cgx::cluster_group cl = cgx::this_cluster();
   const int rank = (int)cl.block_rank();
   const int im = c.im, jm = c.jm, nj = L.nj;
@@ -349,12 +398,12 @@ __global__ void __launch_bounds__(kClusterThreads, 1)
   }
   cl_block_sum(rr, red, part, 0);
   cl.sync();  // r complete in every CTA
-  double rs0 = cl_total(cl, part, 0, L.nc);
+  double rs0 = cl_total(cl, part, 0, L.nc, bcast);
   double rz = cl_precondition(cl, L, sm, nr, c.k.inverse_scale, spectral);
   __syncthreads();
   cl_block_sum(rz, red, part, 1);
   cl.sync();
-  double rho_old = cl_total(cl, part, 1, L.nc);
+  double rho_old = cl_total(cl, part, 1, L.nc, bcast);
   for (int e = threadIdx.x; e < n; e += blockDim.x) sm[L.p + nj + e] = sm[L.z + e];
   const double tol_sq = c.k.eta_tol * c.k.eta_tol;
   const double rel_sq = c.k.eta_rel_tol * c.k.eta_rel_tol * (rs0 > 1e-30 ? rs0 : 1e-30);
@@ -367,7 +416,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1)
     double pap = cl_spmv(L, sm, coeff, nr, sm + L.ap, true);
     cl_block_sum(pap, red, part, 2);
     cl.sync();
-    double denom = cl_total(cl, part, 2, L.nc);
+    double denom = cl_total(cl, part, 2, L.nc, bcast);
     float alpha = (float)(rho_old / (denom + 1e-30));
     double rs = 0.0;
     for (int e = threadIdx.x; e < n; e += blockDim.x) {
@@ -379,7 +428,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1)
     }
     cl_block_sum(rs, red, part, 3);
     cl.sync();
-    double rsn = cl_total(cl, part, 3, L.nc);
+    double rsn = cl_total(cl, part, 3, L.nc, bcast);
     its = it;
     if (rsn <= tol_sq || rsn <= rel_sq || rsn <= 1e-30) {
       converged = true;
@@ -389,7 +438,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1)
     __syncthreads();
     cl_block_sum(rz, red, part, 4);
     cl.sync();
-    double rho_new = cl_total(cl, part, 4, L.nc);
+    double rho_new = cl_total(cl, part, 4, L.nc, bcast);
     float beta = (float)(rho_new / (rho_old + 1e-30));
     for (int e = threadIdx.x; e < n; e += blockDim.x) {
       float *pp = sm + L.p + nj + e;

@@ -164,3 +164,22 @@ def test_gpu_cluster_and_grid_barrier_pcg_agree(monkeypatch):
         outs.append({f: getattr(c, f).cpu().numpy() for f in ("el", "ua", "va", "u", "t")})
     for f in outs[0]:
         assert rel_err(outs[1][f], outs[0][f]) < 1e-4, f
+
+
+@pytest.mark.parametrize("core", ["implicit_p0_fixed", "explicit"])
+def test_gpu_lane_columns_equal_thread_columns(monkeypatch, core):
+    """The 16-lane column kernels (level per lane, shuffled recurrences)
+    compute bitwise the same step as the thread-per-column bodies."""
+    from neuralpom_b200 import B200Physics, cases
+    A, Sc = cases.double_gyre(30, 26, core)
+    Sc = dict(Sc)
+    Sc.update(time=1000.0, time0=1000.0)
+    outs = []
+    for lanes in ("0", "1"):
+        monkeypatch.setenv("NPOM_LANES", lanes)
+        c = _core(A, Sc, core)
+        B200Physics(core_name=core).advance(c, steps=2)
+        outs.append({f: getattr(c, f).cpu().numpy() for f in ("u", "v", "ub", "t", "s", "el", "q2", "q2l", "km",
+                                                              "kh", "kq", "l", "w", "rho", "aam", "drhox", "wubot")})
+    for f in outs[0]:
+        assert np.array_equal(outs[0][f], outs[1][f]), (f, rel_err(outs[1][f], outs[0][f]))
