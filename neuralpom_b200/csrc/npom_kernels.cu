@@ -498,16 +498,18 @@ void launch_cells(const Ctx &c, cudaStream_t s) {
 
 // Cluster PCG when the interior fits in one cluster's shared memory (8 CTAs,
 // or 16 with the non-portable cluster size); NPOM_PCG=coop forces the
-// grid-barrier kernel.
+// grid-barrier kernel, NPOM_PCG_CTAS=16 prefers the 16-CTA cluster.
 bool pcg_cluster_layout(const Ctx &c, ClusterLayout *out) {
   const char *env = getenv("NPOM_PCG");
   if (env && std::strcmp(env, "coop") == 0) return false;
   int dev = 0, optin = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return false;
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return false;
-  for (int nc : {8, 16}) {
+  const char *ctas = getenv("NPOM_PCG_CTAS");
+  const bool prefer16 = ctas && std::strcmp(ctas, "16") == 0;
+  for (int nc : {prefer16 ? 16 : 8, prefer16 ? 8 : 16}) {
     ClusterLayout L = cluster_layout(c.im, c.jm, nc);
-    if (L.bytes() <= (size_t)optin) {
+    if (L.fits && L.bytes() <= (size_t)optin) {
       *out = L;
       return true;
     }

@@ -1,22 +1,45 @@
 // npom_pcg_cluster.cuh -- the free-surface PCG solve on one thread-block
 // cluster (distributed shared memory), for grids whose interior fits in the
-// cluster's shared memory (90x82 needs ~140 KB per CTA with 8 CTAs).
+// cluster's shared memory (90x82 needs ~191 KB per CTA with 8 CTAs).
 //
 // The interior rows are split into NC slabs, one per CTA.  Every PCG vector,
-// the operator coefficients of the slab, its rows of the DST-I matrix Sx
-// (stored transposed), the whole Sy and the slab's inverse eigenvalues live
-// in shared memory for the whole solve.  Neighbour rows of p (the 5-point
-// stencil halo) and the full residual / spectral coefficients needed by the
-// i-direction DSTs are read from the other CTAs through DSMEM; reductions
-// combine per-CTA FP64 partials read the same way, in rank order, so every
-// CTA takes identical convergence decisions.  Cluster barriers separate the
-// phases: five per iteration.  The DST stages are register-blocked over four
-// rows of the slab (one shared-memory load of the data operand per four
-// fused products).
+// the operator coefficients of the slab, its rows of the DST-I matrix Sx,
+// the whole Sy and the slab's inverse eigenvalues live in shared memory for
+// the whole solve.
+//
+// Data moves between CTAs only by remote STORES issued by the producer (a
+// remote load stalls its warp for the DSMEM round trip; a store does not):
+//   * the residual r and the half-transformed coefficients cm are pushed,
+//     row by row as they are produced, into every CTA's full-grid copy (gr,
+//     gc), which the i-direction DST stages then read locally;
+//   * the first and last z rows of a slab are pushed into the neighbours' z
+//     halo (zh), from which each CTA advances its own copy of the p halo rows
+//     with the same expression the owner uses (p = p*beta + z), so the halo
+//     of p never has to be fetched;
+//   * every warp pushes its FP64 partial of a dot product into a slot of
+//     every CTA; after the cluster barrier each warp sums the NC x warps
+//     partials in a fixed order with a butterfly, so every warp of every CTA
+//     holds bitwise the same total and takes the same convergence decision.
+// The cluster barrier (release/acquire) that follows each producer phase is
+// what makes the pushed data visible; four per iteration.
 //
 // Arithmetic follows implicit_p0_fixed/core.py:460-589 (eager PCG) and
 // :591-639 (operator), :762-773 (spectral preconditioner, the DSTs as dense
-// sine-matrix products), :893-916 (Shapiro filter and bcond 1).
+// sine-matrix products), :893-916 (Shapiro filter and bcond 1).  The masks
+// dum/dvm of the operator are 0/1 and are folded into the metric ratios
+// (exact for 0/1 masks).
+//
+// The four DST stages are small dense products per CTA (slab rows <= 16,
+// K and N <= a few hundred) and run on the tensor cores as m16n8k8 TF32
+// MMAs in the 3xTF32 form: every FP32 operand x is split into a TF32 head
+// hi = rna(x) and a TF32 tail lo = rna(x - hi), and hi*hi + hi*lo + lo*hi
+// is accumulated in FP32 (the lo*lo term, 2^-22 relative, is dropped).  The
+// result is an FP32 product of FP32 accuracy, like the reference's dense
+// matmul; neither reproduces the other's blocking order bit for bit.  The
+// constant operands (the slab's Sx rows, Sy) are split once per solve and
+// kept in shared memory in fragment order, one 16-byte load per lane per
+// k-step; the i-stage writes its result directly in the A-fragment order of
+// the j-stage.
 #pragma once
 
 #include <cooperative_groups.h>
@@ -27,14 +50,20 @@ namespace npom {
 
 namespace cgx = cooperative_groups;
 
-constexpr int kClusterThreads = 1024;
+constexpr int kClusterThreads = 512;
+constexpr int kClusterWarps = kClusterThreads / 32;
+constexpr int kRedSlots = 4;  // pap, r.r, r.z, r0.r0
 
 struct ClusterLayout {
-  int ni, nj, nc, rows, rp;  // interior size, CTAs, rows per CTA (rp: padded to 4)
+  int ni, nj, nc, rows;  // interior size, CTAs, rows per CTA (<= 16: one MMA row tile)
+  int kti, nt;           // k-tiles of the i-stage (ceil(ni/8)); column tiles (ceil(nj/8)) = k-tiles of the j-stage
+  int gp;                // row pitch of gr/gc: >= 8*nt and 8 or 24 (mod 32), conflict-free B-fragment loads
   // float offsets in dynamic shared memory
-  int x, r, z, ap, rhs, p, he, hw, hn, hs, ce, cw, cn, cs, me, mw, mn, ms, iart, t1, cm, g, sxt, sy, ie, ks;
+  int x, r, z, ap, rhs, p, zh, h4, c4, iart, ie, gr, gc, sxf, syf, t1f;
   int floats;
-  size_t bytes() const { return (size_t)floats * sizeof(float) + 64 * sizeof(double); }
+  bool fits;  // rows <= 16 and one column tile per warp
+  size_t red_doubles() const { return (size_t)kRedSlots * nc * kClusterWarps; }
+  size_t bytes() const { return (size_t)floats * sizeof(float) + red_doubles() * sizeof(double); }
 };
 
 inline ClusterLayout cluster_layout(int im, int jm, int nc) {
@@ -43,7 +72,11 @@ inline ClusterLayout cluster_layout(int im, int jm, int nc) {
   L.nj = jm - 2;
   L.nc = nc;
   L.rows = (L.ni + nc - 1) / nc;
-  L.rp = (L.rows + 3) & ~3;
+  L.kti = (L.ni + 7) >> 3;
+  L.nt = (L.nj + 7) >> 3;
+  L.gp = 8 * L.nt;
+  while (L.gp % 32 != 8 && L.gp % 32 != 24) L.gp += 8;
+  L.fits = L.rows <= 16 && L.nt <= kClusterWarps;
   const int rn = L.rows * L.nj;
   int o = 0;
   auto take = [&](int n) {
@@ -57,81 +90,44 @@ inline ClusterLayout cluster_layout(int im, int jm, int nc) {
   L.ap = take(rn);
   L.rhs = take(rn);
   L.p = take((L.rows + 2) * L.nj);
-  L.he = take(rn);
-  L.hw = take(rn);
-  L.hn = take(rn);
-  L.hs = take(rn);
-  L.ce = take(rn);
-  L.cw = take(rn);
-  L.cn = take(rn);
-  L.cs = take(rn);
-  L.me = take(rn);
-  L.mw = take(rn);
-  L.mn = take(rn);
-  L.ms = take(rn);
+  L.zh = take(2 * L.nj);
+  L.h4 = take(4 * rn);  // (he, hw, hn, hs) per cell
+  L.c4 = take(4 * rn);  // metric ratios times the masks (ce, cw, cn, cs)
   L.iart = take(rn);
-  L.t1 = take(L.nj * L.rp);  // transposed [b][row]; Jacobi keeps its diagonal here
-  L.cm = take(rn);
-  L.g = take(L.ni * L.nj);
-  L.sxt = take(L.ni * L.rp);  // Sx rows of the slab, transposed [m][row]
-  L.sy = take(L.nj * L.nj);
-  L.ie = take(rn);
-  L.ks = take(4 * kClusterThreads);  // split-K partials of the DST stages (float4 each)
+  L.ie = take(rn);                         // inverse eigenvalues of the slab (Jacobi: the diagonal)
+  L.gr = take(8 * L.kti * L.gp);           // full residual, zero-padded rows/columns
+  L.gc = take(8 * L.kti * L.gp);           // full half-transformed field
+  L.sxf = take(L.kti * 32 * 8);            // Sx slab as A fragments: per k-tile 32 lanes x hi4, then 32 x lo4
+  L.syf = take(L.nt * L.nt * 32 * 4);      // Sy as B fragments: (hi x2, lo x2) per lane, k-tile, column tile
+  L.t1f = take(L.nt * 32 * 4);             // i-stage result as A fragments of the j-stage
   L.floats = o;
   return L;
 }
 
-// block-wide FP64 sum (fixed shuffle tree); the CTA's total is left in
-// part[slot] by warp 0
-__device__ __forceinline__ void cl_block_sum(double v, double *red, double *part, int slot) {
-  for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (lane == 0) red[w] = v;
-  __syncthreads();
-  if (w == 0) {
-    const int nw = (int)(blockDim.x >> 5);
-    double t = lane < nw ? red[lane] : 0.0;
-    for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
-    if (lane == 0) part[slot] = t;
+// Warp partial of a dot product, pushed into slot `slot` of every CTA.
+__device__ __forceinline__ void cl_push_partial(cgx::cluster_group &cl, double v, double *red, int slot, int nc,
+                                                int rank) {
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane < nc) {
+    double *dst = cl.map_shared_rank(red, lane);
+    dst[(slot * nc + rank) * kClusterWarps + w] = v;
   }
 }
 
-// after a cluster barrier: sum of part[slot] over the cluster.  Warp 0 reads
-// the nc partials in parallel and reduces them with the same shuffle tree in
-// every CTA, so all CTAs obtain bitwise the same total.
-__device__ __forceinline__ double cl_total(cgx::cluster_group &cl, double *part, int slot, int nc, double *bcast) {
-  if (threadIdx.x < 32) {
-    const int lane = threadIdx.x;
-    double t = lane < nc ? *cl.map_shared_rank(part + slot, lane) : 0.0;
-    for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
-    if (lane == 0) bcast[slot] = t;
-  }
-  __syncthreads();
-  return bcast[slot];
+// After the cluster barrier: the cluster total of slot `slot`, the same
+// bits in every warp of every CTA.
+__device__ __forceinline__ double cl_partial_total(const double *red, int slot, int nc) {
+  const int lane = threadIdx.x & 31;
+  double t = 0.0;
+  if (lane < kClusterWarps)
+    for (int q = 0; q < nc; ++q) t += red[(slot * nc + q) * kClusterWarps + lane];
+  for (int off = 16; off > 0; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
+  return t;
 }
 
-// g <- all rows of the slab array at src_off (row length nj) of every CTA:
-// the slab of CTA q is contiguous and lands at row q*rows of g
-__device__ __forceinline__ void cl_gather(cgx::cluster_group &cl, const ClusterLayout &L, float *sm, int src_off,
-                                          float *g) {
-  const int nj = L.nj;
-  for (int q = 0; q < L.nc; ++q) {
-    const int nrq = min(L.rows, L.ni - q * L.rows);
-    if (nrq <= 0) break;
-    const float *remote = cl.map_shared_rank(sm + src_off, q);
-    float *dst = g + (size_t)q * L.rows * nj;
-    if ((nj & 3) == 0) {
-      const int n4 = (nrq * nj) >> 2;
-      const float4 *r4 = reinterpret_cast<const float4 *>(remote);
-      float4 *d4 = reinterpret_cast<float4 *>(dst);
-      for (int f = threadIdx.x; f < n4; f += blockDim.x) d4[f] = r4[f];
-    } else {
-      for (int e = threadIdx.x; e < nrq * nj; e += blockDim.x) dst[e] = remote[e];
-    }
-  }
-}
-
-// fetch halo rows of p from the neighbouring CTAs (zero outside the domain)
+// fetch halo rows of p from the neighbouring CTAs (zero outside the domain);
+// used for the initial residual and the final filter only
 __device__ __forceinline__ void cl_halo(cgx::cluster_group &cl, const ClusterLayout &L, float *sm, int rank, int nr) {
   float *p = sm + L.p;
   for (int b = threadIdx.x; b < 2 * L.nj; b += blockDim.x) {
@@ -155,10 +151,13 @@ __device__ __forceinline__ void cl_halo(cgx::cluster_group &cl, const ClusterLay
   }
 }
 
-// ap = A p on the slab (p has its halo rows in place)
+// ap = A p on the slab (p has its halo rows in place); returns this thread's
+// share of p.Ap when asked
 __device__ __forceinline__ double cl_spmv(const ClusterLayout &L, float *sm, float coeff, int nr, float *out,
                                           bool dot_with_p) {
   const float *p = sm + L.p;
+  const float4 *h4 = reinterpret_cast<const float4 *>(sm + L.h4);
+  const float4 *c4 = reinterpret_cast<const float4 *>(sm + L.c4);
   double acc = 0.0;
   const int n = nr * L.nj;
   for (int e = threadIdx.x; e < n; e += blockDim.x) {
@@ -169,10 +168,11 @@ __device__ __forceinline__ double cl_spmv(const ClusterLayout &L, float *sm, flo
     float e_w = pr[b - L.nj];
     float e_n = (b + 1 < L.nj) ? pr[b + 1] : 0.0f;
     float e_s = (b > 0) ? pr[b - 1] : 0.0f;
-    float fe = sm[L.he + e] * (e_e - ev) * sm[L.ce + e] * sm[L.me + e];
-    float fw = sm[L.hw + e] * (ev - e_w) * sm[L.cw + e] * sm[L.mw + e];
-    float fn = sm[L.hn + e] * (e_n - ev) * sm[L.cn + e] * sm[L.mn + e];
-    float fs = sm[L.hs + e] * (ev - e_s) * sm[L.cs + e] * sm[L.ms + e];
+    float4 h = h4[e], cc = c4[e];
+    float fe = h.x * (e_e - ev) * cc.x;
+    float fw = h.y * (ev - e_w) * cc.y;
+    float fn = h.z * (e_n - ev) * cc.z;
+    float fs = h.w * (ev - e_s) * cc.w;
     float div = (fe - fw + fn - fs) * sm[L.iart + e];
     float a = ev - coeff * div;
     out[e] = a;
@@ -181,153 +181,179 @@ __device__ __forceinline__ double cl_spmv(const ClusterLayout &L, float *sm, flo
   return acc;
 }
 
-// The two DST stages compute, for every output group (four slab rows x one
-// column), a length-K dot product.  The K range is split KS ways so that all
-// warps of the CTA work (KS * groups <= blockDim); the KS partial float4s are
-// then summed in split order.
-__device__ __forceinline__ int cl_splits(int ng) {
-  int ks = (int)blockDim.x / (ng > 0 ? ng : 1);
-  return ks < 1 ? 1 : (ks > 8 ? 8 : ks);
-}
-
-// DST along i: t1T[b][4g..4g+3] = sum_m Sx[row][m] g[m][b]
-__device__ __forceinline__ void cl_dst_i(const ClusterLayout &L, float *sm, int nr) {
-  const int nj = L.nj, rp = L.rp, groups = (nr + 3) >> 2, ng = groups * nj;
-  const int ks = cl_splits(ng), mlen = (L.ni + ks - 1) / ks;
-  const float *g = sm + L.g, *sxt = sm + L.sxt;
-  float4 *part = reinterpret_cast<float4 *>(sm + L.ks);
-  for (int t = threadIdx.x; t < ng * ks; t += blockDim.x) {
-    int s = t / ng, og = t - s * ng;
-    int grp = og / nj, b = og - grp * nj;
-    int m0 = s * mlen, m1 = min(L.ni, m0 + mlen);
-    float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
-    const float *sc = sxt + 4 * grp;
-#pragma unroll 4
-    for (int m = m0; m < m1; ++m) {
-      float gv = g[m * nj + b];
-      float4 sv = *reinterpret_cast<const float4 *>(sc + m * rp);
-      a0 += sv.x * gv;
-      a1 += sv.y * gv;
-      a2 += sv.z * gv;
-      a3 += sv.w * gv;
+// push the slab rows held at src (pitch nj) into every CTA's full-grid copy
+// at dst (pitch gp), sixteen bytes per store when rows allow it
+__device__ __forceinline__ void cl_push_slab(cgx::cluster_group &cl, const ClusterLayout &L, float *sm, int src,
+                                             int dst, int a0, int nr) {
+  const int nj = L.nj;
+  if ((nj & 3) == 0) {
+    const int nj4 = nj >> 2;
+    for (int e4 = threadIdx.x; e4 < nr * nj4; e4 += blockDim.x) {
+      const int ra = e4 / nj4, b = 4 * (e4 - ra * nj4);
+      const float4 v = *reinterpret_cast<const float4 *>(sm + src + ra * nj + b);
+      const int at = (a0 + ra) * L.gp + b;
+      for (int q = 0; q < L.nc; ++q) *reinterpret_cast<float4 *>(cl.map_shared_rank(sm + dst, q) + at) = v;
     }
-    part[t] = make_float4(a0, a1, a2, a3);
-  }
-  __syncthreads();
-  float *t1 = sm + L.t1;
-  for (int og = threadIdx.x; og < ng; og += blockDim.x) {
-    float4 v = part[og];
-    for (int s = 1; s < ks; ++s) {
-      float4 w = part[s * ng + og];
-      v.x += w.x;
-      v.y += w.y;
-      v.z += w.z;
-      v.w += w.w;
+  } else {
+    for (int e = threadIdx.x; e < nr * nj; e += blockDim.x) {
+      const int ra = e / nj, b = e - ra * nj;
+      const float v = sm[src + e];
+      const int at = (a0 + ra) * L.gp + b;
+      for (int q = 0; q < L.nc; ++q) cl.map_shared_rank(sm + dst, q)[at] = v;
     }
-    int grp = og / nj, b = og - grp * nj;
-    *reinterpret_cast<float4 *>(t1 + b * rp + 4 * grp) = v;
   }
 }
 
-// DST along j: out[row][l] = (sum_b t1T[b][row] Sy[b][l]) times scale[row][l]
-// (the inverse eigenvalues) or divided by div; accumulates r.out into rz
-__device__ __forceinline__ void cl_dst_j(const ClusterLayout &L, float *sm, int nr, float *out, const float *scale,
-                                         float div, const float *r, double &rz) {
-  const int nj = L.nj, rp = L.rp, groups = (nr + 3) >> 2, ng = groups * nj;
-  const int ks = cl_splits(ng), blen = (nj + ks - 1) / ks;
-  const float *t1 = sm + L.t1, *sy = sm + L.sy;
-  float4 *part = reinterpret_cast<float4 *>(sm + L.ks);
-  for (int t = threadIdx.x; t < ng * ks; t += blockDim.x) {
-    int s = t / ng, og = t - s * ng;
-    int grp = og / nj, l = og - grp * nj;
-    int b0 = s * blen, b1 = min(nj, b0 + blen);
-    float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
-    const float *tc = t1 + 4 * grp;
-#pragma unroll 4
-    for (int b = b0; b < b1; ++b) {
-      float syv = sy[b * nj + l];
-      float4 tv = *reinterpret_cast<const float4 *>(tc + b * rp);
-      a0 += tv.x * syv;
-      a1 += tv.y * syv;
-      a2 += tv.z * syv;
-      a3 += tv.w * syv;
-    }
-    part[t] = make_float4(a0, a1, a2, a3);
+__device__ __forceinline__ unsigned tf32_rna(float x) {
+  unsigned r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+__device__ __forceinline__ void tf32_split(float x, unsigned &hi, unsigned &lo) {
+  hi = tf32_rna(x);
+  lo = tf32_rna(x - __uint_as_float(hi));
+}
+
+// d += a * b, m16n8k8, TF32 inputs, FP32 accumulators
+__device__ __forceinline__ void mma_tf32(float (&d)[4], unsigned a0, unsigned a1, unsigned a2, unsigned a3,
+                                         unsigned b0, unsigned b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// Fragment coordinates of lane: g = lane/4 (rows g and g+8 of A and C,
+// column g of B), t = lane%4 (k = t and t+4 of A and B, columns 2t and 2t+1
+// of C).
+
+// i-stage: T[r][n] = sum_m Sx[a0+r][m] G[m][n] for the slab rows r < 16 and
+// the column tile of this warp; T goes to t1f in the A-fragment order of
+// the j-stage (its k index is n).
+__device__ __forceinline__ void cl_dst_i(const ClusterLayout &L, float *sm, const float *G) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (w >= L.nt) return;
+  const int g = lane >> 2, t = lane & 3, n0 = 8 * w;
+  const float4 *af = reinterpret_cast<const float4 *>(sm + L.sxf);
+  float hh[4] = {0.f, 0.f, 0.f, 0.f}, hl[4] = {0.f, 0.f, 0.f, 0.f}, lh[4] = {0.f, 0.f, 0.f, 0.f};
+  const float *bcol = G + n0 + g;
+#pragma unroll 2
+  for (int kt = 0; kt < L.kti; ++kt) {
+    const float4 ah = af[(2 * kt) * 32 + lane], al = af[(2 * kt + 1) * 32 + lane];
+    unsigned bh0, bl0, bh1, bl1;
+    tf32_split(bcol[(8 * kt + t) * L.gp], bh0, bl0);
+    tf32_split(bcol[(8 * kt + t + 4) * L.gp], bh1, bl1);
+    const unsigned a0 = __float_as_uint(ah.x), a1 = __float_as_uint(ah.y), a2 = __float_as_uint(ah.z),
+                   a3 = __float_as_uint(ah.w);
+    mma_tf32(hh, a0, a1, a2, a3, bh0, bh1);
+    mma_tf32(hl, a0, a1, a2, a3, bl0, bl1);
+    mma_tf32(lh, __float_as_uint(al.x), __float_as_uint(al.y), __float_as_uint(al.z), __float_as_uint(al.w), bh0,
+             bh1);
   }
-  __syncthreads();
-  for (int og = threadIdx.x; og < ng; og += blockDim.x) {
-    float4 v = part[og];
-    for (int s = 1; s < ks; ++s) {
-      float4 w = part[s * ng + og];
-      v.x += w.x;
-      v.y += w.y;
-      v.z += w.z;
-      v.w += w.w;
-    }
-    int grp = og / nj, l = og - grp * nj;
-    float acc[4] = {v.x, v.y, v.z, v.w};
+  float *tf = sm + L.t1f;
+  // C element (row, col kk = 2t or 2t+1 of the tile) -> A fragment of k-tile w
+  // of the j-stage: lane 4*(row%8) + kk%4, slot (row>=8) + 2*(kk>=4)
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      int ra = 4 * grp + q;
-      if (ra < nr) {
-        int e = ra * nj + l;
-        float val = scale ? acc[q] * scale[e] : acc[q] / div;
-        out[e] = val;
-        if (r) rz += (double)r[e] * (double)val;
-      }
-    }
+  for (int q = 0; q < 4; ++q) {
+    const int row8 = q >> 1, kk = 2 * t + (q & 1);
+    const float v = (lh[q] + hl[q]) + hh[q];
+    tf[(w * 32 + 4 * g + (kk & 3)) * 4 + row8 + 2 * (kk >> 2)] = v;
   }
 }
 
-// z = M^-1 r: two cluster-wide gathers, one cluster barrier inside; returns
-// this thread's share of r.z.  Every CTA's r slab must be final on entry.
+// j-stage: C[r][l] = sum_b T[r][b] Sy[b][l] for the column tile of this
+// warp; epi(row, col, value) for the rows < nr and columns < nj
+template <class Epi>
+__device__ __forceinline__ void cl_dst_j(const ClusterLayout &L, float *sm, int nr, Epi &&epi) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (w >= L.nt) return;
+  const int g = lane >> 2, t = lane & 3;
+  const float4 *af = reinterpret_cast<const float4 *>(sm + L.t1f);
+  const float4 *bf = reinterpret_cast<const float4 *>(sm + L.syf);
+  float hh[4] = {0.f, 0.f, 0.f, 0.f}, hl[4] = {0.f, 0.f, 0.f, 0.f}, lh[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 2
+  for (int kt = 0; kt < L.nt; ++kt) {
+    const float4 av = af[kt * 32 + lane];
+    const float4 b = bf[(kt * L.nt + w) * 32 + lane];
+    unsigned ah0, al0, ah1, al1, ah2, al2, ah3, al3;
+    tf32_split(av.x, ah0, al0);
+    tf32_split(av.y, ah1, al1);
+    tf32_split(av.z, ah2, al2);
+    tf32_split(av.w, ah3, al3);
+    const unsigned bh0 = __float_as_uint(b.x), bh1 = __float_as_uint(b.y);
+    mma_tf32(hh, ah0, ah1, ah2, ah3, bh0, bh1);
+    mma_tf32(hl, ah0, ah1, ah2, ah3, __float_as_uint(b.z), __float_as_uint(b.w));
+    mma_tf32(lh, al0, al1, al2, al3, bh0, bh1);
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int row = g + 8 * (q >> 1), col = 8 * w + 2 * t + (q & 1);
+    if (row < nr && col < L.nj) epi(row, col, (lh[q] + hl[q]) + hh[q]);
+  }
+}
+
+// z = M^-1 r for the slab, with r already pushed into every CTA's gr (and
+// the cluster barrier after the push passed).  Pushes the half-transformed
+// field into gc (one cluster barrier inside), writes z, pushes the z rows
+// that neighbours keep as halo and returns this thread's share of r.z.
 __device__ __forceinline__ double cl_precondition(cgx::cluster_group &cl, const ClusterLayout &L, float *sm, int nr,
-                                                  float inverse_scale, bool spectral) {
-  const int n = nr * L.nj;
+                                                  int rank, int a0, float inverse_scale, bool spectral) {
+  const int nj = L.nj;
   float *z = sm + L.z;
   const float *r = sm + L.r;
+  const float *ie = sm + L.ie;
+  const bool up = rank > 0 && nr > 0;
+  const bool down = (rank + 1) < L.nc && (rank + 1) * L.rows < L.ni;
   double rz = 0.0;
+  auto finish = [&](int ra, int l, float zv) {
+    const int e = ra * nj + l;
+    z[e] = zv;
+    rz += (double)r[e] * (double)zv;
+    if (ra == 0 && up) cl.map_shared_rank(sm + L.zh, rank - 1)[nj + l] = zv;
+    if (ra == nr - 1 && down) cl.map_shared_rank(sm + L.zh, rank + 1)[l] = zv;
+  };
   if (!spectral) {
-    // Jacobi: the diagonal is kept in the t1 slab
-    for (int e = threadIdx.x; e < n; e += blockDim.x) {
-      float zv = r[e] / (sm[L.t1 + e] + 1e-30f);
-      z[e] = zv;
-      rz += (double)r[e] * (double)zv;
+    for (int e = threadIdx.x; e < nr * nj; e += blockDim.x) {
+      int ra = e / nj;
+      finish(ra, e - ra * nj, r[e] / (ie[e] + 1e-30f));
     }
     return rz;
   }
-  cl_gather(cl, L, sm, L.r, sm + L.g);
+  cl_dst_i(L, sm, sm + L.gr);
   __syncthreads();
-  cl_dst_i(L, sm, nr);
+  // DST along j times the inverse eigenvalues, pushed into every CTA's gc
+  // (staged in the ap slab, free until the next operator apply)
+  float *stage = sm + L.ap;
+  cl_dst_j(L, sm, nr, [&](int ra, int l, float acc) { stage[ra * nj + l] = acc * ie[ra * nj + l]; });
   __syncthreads();
-  double unused = 0.0;
-  cl_dst_j(L, sm, nr, sm + L.cm, sm + L.ie, 1.0f, nullptr, unused);
-  cl.sync();
-  cl_gather(cl, L, sm, L.cm, sm + L.g);
+  cl_push_slab(cl, L, sm, L.ap, L.gc, a0, nr);
+  cl.sync();  // gc complete in every CTA
+  cl_dst_i(L, sm, sm + L.gc);
   __syncthreads();
-  cl_dst_i(L, sm, nr);
-  __syncthreads();
-  cl_dst_j(L, sm, nr, z, nullptr, inverse_scale, r, rz);
+  // DST along j divided by the scale: z
+  cl_dst_j(L, sm, nr, [&](int ra, int l, float acc) { finish(ra, l, acc / inverse_scale); });
   return rz;
 }
 
 __global__ void __launch_bounds__(kClusterThreads, 1)
     k_pcg_cluster(Ctx c, ClusterLayout L, int with_rhs, int with_post) {
   extern __shared__ __align__(16) float sm[];
-  double *red = reinterpret_cast<double *>(sm + L.floats);  // 32 doubles
-  double *part = red + 32;                                    // 8 slots
-  double *bcast = part + 8;                                   // 8 slots
+  double *red = reinterpret_cast<double *>(sm + L.floats);
   cgx::cluster_group cl = cgx::this_cluster();
   const int rank = (int)cl.block_rank();
-  const int im = c.im, jm = c.jm, nj = L.nj;
+  const int im = c.im, jm = c.jm, nj = L.nj, nc = L.nc;
   const int a0 = rank * L.rows;
   const int nr = max(0, min(L.rows, L.ni - a0));
   const int n = nr * nj;
   const bool spectral = c.k.eta_precond == NPOM_PRECOND_SPECTRAL;
   const float coeff = c.k.implicit_coeff;
+  const bool has_up = rank > 0 && nr > 0;
+  const bool has_down = (rank + 1) < nc && (rank + 1) * L.rows < L.ni;
 
   // ---- set-up: stored transports (whole grid, strided over the cluster)
-  const int gt = rank * blockDim.x + threadIdx.x, gs = L.nc * blockDim.x;
+  const int gt = rank * blockDim.x + threadIdx.x, gs = nc * blockDim.x;
   if (with_rhs) {
     for (int q = gt; q < im * jm; q += gs) {
       int i = q / jm, j = q - i * jm;
@@ -337,15 +363,15 @@ __global__ void __launch_bounds__(kClusterThreads, 1)
   }
   // ---- slab: coefficients, rhs, initial guess, DST blocks
   const float *dd = c.F[NPOM_F_d];
+  float4 *h4 = reinterpret_cast<float4 *>(sm + L.h4);
+  float4 *c4 = reinterpret_cast<float4 *>(sm + L.c4);
   for (int e = threadIdx.x; e < n; e += blockDim.x) {
     int ra = e / nj, b = e - ra * nj;
     int i = a0 + ra + 1, j = b + 1;
     size_t o = NPOM_I2(c, i, j);
     float d0 = dd[o];
-    sm[L.he + e] = 0.5f * (dd[o + jm] + d0);
-    sm[L.hw + e] = 0.5f * (d0 + dd[o - jm]);
-    sm[L.hn + e] = 0.5f * (dd[o + 1] + d0);
-    sm[L.hs + e] = 0.5f * (d0 + dd[o - 1]);
+    h4[e] = make_float4(0.5f * (dd[o + jm] + d0), 0.5f * (d0 + dd[o - jm]), 0.5f * (dd[o + 1] + d0),
+                        0.5f * (d0 + dd[o - 1]));
     float dx_e = 0.5f * (F2(dx, i + 1, j) + F2(dx, i, j));
     float dx_w = 0.5f * (F2(dx, i, j) + F2(dx, i - 1, j));
     float dy_e = 0.5f * (F2(dy, i + 1, j) + F2(dy, i, j));
@@ -354,98 +380,158 @@ __global__ void __launch_bounds__(kClusterThreads, 1)
     float dy_s = 0.5f * (F2(dy, i, j) + F2(dy, i, j - 1));
     float dx_n = 0.5f * (F2(dx, i, j + 1) + F2(dx, i, j));
     float dx_s = 0.5f * (F2(dx, i, j) + F2(dx, i, j - 1));
-    sm[L.ce + e] = dy_e / (dx_e + 1e-20f);
-    sm[L.cw + e] = dy_w / (dx_w + 1e-20f);
-    sm[L.cn + e] = dx_n / (dy_n + 1e-20f);
-    sm[L.cs + e] = dx_s / (dy_s + 1e-20f);
-    sm[L.me + e] = F2(dum, i + 1, j);
-    sm[L.mw + e] = F2(dum, i, j);
-    sm[L.mn + e] = F2(dvm, i, j + 1);
-    sm[L.ms + e] = F2(dvm, i, j);
+    c4[e] = make_float4((dy_e / (dx_e + 1e-20f)) * F2(dum, i + 1, j), (dy_w / (dx_w + 1e-20f)) * F2(dum, i, j),
+                        (dx_n / (dy_n + 1e-20f)) * F2(dvm, i, j + 1), (dx_s / (dy_s + 1e-20f)) * F2(dvm, i, j));
     sm[L.iart + e] = 1.0f / (F2(art, i, j) + 1e-20f);
     sm[L.rhs + e] = with_rhs ? rhs_cell(c, i, j) : c.W[NPOM_W_rhs][o];
     sm[L.x + e] = F2(elf, i, j);
     if (spectral) sm[L.ie + e] = c.W[NPOM_W_inv_eigs][(size_t)(a0 + ra) * nj + b];
   }
+  for (int b = threadIdx.x; b < 2 * nj; b += blockDim.x) sm[L.zh + b] = 0.0f;
   if (spectral) {
-    // Sx rows of the slab, transposed, zero-padded to rp rows
-    for (int e = threadIdx.x; e < L.ni * L.rp; e += blockDim.x) {
-      int m = e / L.rp, q = e - m * L.rp;
-      sm[L.sxt + e] = (q < nr) ? c.W[NPOM_W_sx][(size_t)(a0 + q) * L.ni + m] : 0.0f;
+    const float *sx = c.W[NPOM_W_sx], *sy = c.W[NPOM_W_sy];
+    const int ni = L.ni;
+    // padding rows/columns of the full-grid copies stay zero
+    for (int e = threadIdx.x; e < 8 * L.kti * L.gp; e += blockDim.x) {
+      sm[L.gr + e] = 0.0f;
+      sm[L.gc + e] = 0.0f;
     }
-    for (int e = threadIdx.x; e < nj * nj; e += blockDim.x) sm[L.sy + e] = c.W[NPOM_W_sy][e];
+    // Sx rows of the slab as split A fragments (zero outside the slab)
+    for (int f = threadIdx.x; f < L.kti * 32; f += blockDim.x) {
+      const int kt = f >> 5, lane = f & 31, g = lane >> 2, t = lane & 3;
+      float v[4];
+      for (int q = 0; q < 4; ++q) {
+        const int row = g + 8 * (q & 1), m = 8 * kt + t + 4 * (q >> 1);
+        v[q] = (row < nr && m < ni) ? sx[(size_t)(a0 + row) * ni + m] : 0.0f;
+      }
+      unsigned hi[4], lo[4];
+      for (int q = 0; q < 4; ++q) tf32_split(v[q], hi[q], lo[q]);
+      float4 *dst = reinterpret_cast<float4 *>(sm + L.sxf) + (2 * kt) * 32 + lane;
+      dst[0] = make_float4(__uint_as_float(hi[0]), __uint_as_float(hi[1]), __uint_as_float(hi[2]), __uint_as_float(hi[3]));
+      dst[32] = make_float4(__uint_as_float(lo[0]), __uint_as_float(lo[1]), __uint_as_float(lo[2]), __uint_as_float(lo[3]));
+    }
+    // Sy as split B fragments
+    for (int f = threadIdx.x; f < L.nt * L.nt * 32; f += blockDim.x) {
+      const int lane = f & 31, tile = f >> 5, kt = tile / L.nt, ct = tile - kt * L.nt, g = lane >> 2, t = lane & 3;
+      const int col = 8 * ct + g, b0 = 8 * kt + t, b1 = b0 + 4;
+      const float v0 = (b0 < nj && col < nj) ? sy[(size_t)b0 * nj + col] : 0.0f;
+      const float v1 = (b1 < nj && col < nj) ? sy[(size_t)b1 * nj + col] : 0.0f;
+      unsigned h0, l0, h1, l1;
+      tf32_split(v0, h0, l0);
+      tf32_split(v1, h1, l1);
+      reinterpret_cast<float4 *>(sm + L.syf)[f] =
+          make_float4(__uint_as_float(h0), __uint_as_float(h1), __uint_as_float(l0), __uint_as_float(l1));
+    }
   }
   __syncthreads();
   if (!spectral) {
-    // Jacobi diagonal (core.py:677-700) into the t1 slab
-    for (int e = threadIdx.x; e < n; e += blockDim.x)
-      sm[L.t1 + e] = 1.0f + coeff * sm[L.iart + e] *
-                                (sm[L.he + e] * sm[L.ce + e] * sm[L.me + e] + sm[L.hw + e] * sm[L.cw + e] * sm[L.mw + e] +
-                                 sm[L.hn + e] * sm[L.cn + e] * sm[L.mn + e] + sm[L.hs + e] * sm[L.cs + e] * sm[L.ms + e]);
+    // Jacobi diagonal (core.py:677-700), kept where the eigenvalues would be
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+      float4 h = h4[e], cc = c4[e];
+      sm[L.ie + e] = 1.0f + coeff * sm[L.iart + e] * (h.x * cc.x + h.y * cc.y + h.z * cc.z + h.w * cc.w);
+    }
   }
   // r = rhs - A x  (x goes through the halo buffer)
   for (int e = threadIdx.x; e < n; e += blockDim.x) sm[L.p + nj + e] = sm[L.x + e];
-  cl.sync();
+  cl.sync();  // x slabs complete; zh zeroed everywhere before any push
   cl_halo(cl, L, sm, rank, nr);
   __syncthreads();
   cl_spmv(L, sm, coeff, nr, sm + L.ap, false);
-  __syncthreads();
   double rr = 0.0;
   for (int e = threadIdx.x; e < n; e += blockDim.x) {
     float rv = sm[L.rhs + e] - sm[L.ap + e];
     sm[L.r + e] = rv;
     rr += (double)rv * (double)rv;
   }
-  cl_block_sum(rr, red, part, 0);
-  cl.sync();  // r complete in every CTA
-  double rs0 = cl_total(cl, part, 0, L.nc, bcast);
-  double rz = cl_precondition(cl, L, sm, nr, c.k.inverse_scale, spectral);
   __syncthreads();
-  cl_block_sum(rz, red, part, 1);
-  cl.sync();
-  double rho_old = cl_total(cl, part, 1, L.nc, bcast);
-  for (int e = threadIdx.x; e < n; e += blockDim.x) sm[L.p + nj + e] = sm[L.z + e];
+  if (spectral) cl_push_slab(cl, L, sm, L.r, L.gr, a0, nr);
+  cl_push_partial(cl, rr, red, 3, nc, rank);
+  cl.sync();  // r pushed everywhere; neighbours' x halo reads done
+  const double rs0 = cl_partial_total(red, 3, nc);
+  double rz = cl_precondition(cl, L, sm, nr, rank, a0, c.k.inverse_scale, spectral);
+  cl_push_partial(cl, rz, red, 2, nc, rank);
+  cl.sync();  // z halo rows and r.z partials in place
+  double rho_old = cl_partial_total(red, 2, nc);
+  float *p = sm + L.p;
+  for (int e = threadIdx.x; e < n; e += blockDim.x) p[nj + e] = sm[L.z + e];
+  for (int b = threadIdx.x; b < nj; b += blockDim.x) {
+    p[b] = has_up ? sm[L.zh + b] : 0.0f;
+    p[(nr + 1) * nj + b] = has_down ? sm[L.zh + nj + b] : 0.0f;
+  }
   const double tol_sq = c.k.eta_tol * c.k.eta_tol;
   const double rel_sq = c.k.eta_rel_tol * c.k.eta_rel_tol * (rs0 > 1e-30 ? rs0 : 1e-30);
   int its = 0;
   bool converged = false;
-  cl.sync();  // p slabs complete
+  __syncthreads();  // p and its halo rows complete in this CTA
   for (int it = 1; it <= c.k.eta_max_iter; ++it) {
-    cl_halo(cl, L, sm, rank, nr);
-    __syncthreads();
     double pap = cl_spmv(L, sm, coeff, nr, sm + L.ap, true);
-    cl_block_sum(pap, red, part, 2);
+    cl_push_partial(cl, pap, red, 0, nc, rank);
     cl.sync();
-    double denom = cl_total(cl, part, 2, L.nc, bcast);
-    float alpha = (float)(rho_old / (denom + 1e-30));
+    const double denom = cl_partial_total(red, 0, nc);
+    const float alpha = (float)(rho_old / (denom + 1e-30));
     double rs = 0.0;
-    for (int e = threadIdx.x; e < n; e += blockDim.x) {
-      float pv = sm[L.p + nj + e];
-      sm[L.x + e] = sm[L.x + e] + alpha * pv;
-      float rv = sm[L.r + e] - alpha * sm[L.ap + e];
-      sm[L.r + e] = rv;
-      rs += (double)rv * (double)rv;
+    if ((nj & 3) == 0) {
+      // four cells per thread: the new r goes out to every CTA in one
+      // sixteen-byte store per destination
+      for (int e = 4 * threadIdx.x; e < n; e += 4 * blockDim.x) {
+        const float4 pv = *reinterpret_cast<const float4 *>(p + nj + e);
+        const float4 av = *reinterpret_cast<const float4 *>(sm + L.ap + e);
+        float4 xv = *reinterpret_cast<const float4 *>(sm + L.x + e);
+        float4 rv = *reinterpret_cast<const float4 *>(sm + L.r + e);
+        xv.x = xv.x + alpha * pv.x;
+        xv.y = xv.y + alpha * pv.y;
+        xv.z = xv.z + alpha * pv.z;
+        xv.w = xv.w + alpha * pv.w;
+        rv.x = rv.x - alpha * av.x;
+        rv.y = rv.y - alpha * av.y;
+        rv.z = rv.z - alpha * av.z;
+        rv.w = rv.w - alpha * av.w;
+        *reinterpret_cast<float4 *>(sm + L.x + e) = xv;
+        *reinterpret_cast<float4 *>(sm + L.r + e) = rv;
+        rs += (double)rv.x * (double)rv.x;
+        rs += (double)rv.y * (double)rv.y;
+        rs += (double)rv.z * (double)rv.z;
+        rs += (double)rv.w * (double)rv.w;
+        if (spectral) {
+          const int ra = e / nj, at = (a0 + ra) * L.gp + (e - ra * nj);
+          for (int q = 0; q < nc; ++q) *reinterpret_cast<float4 *>(cl.map_shared_rank(sm + L.gr, q) + at) = rv;
+        }
+      }
+    } else {
+      for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        float pv = p[nj + e];
+        sm[L.x + e] = sm[L.x + e] + alpha * pv;
+        float rv = sm[L.r + e] - alpha * sm[L.ap + e];
+        sm[L.r + e] = rv;
+        rs += (double)rv * (double)rv;
+      }
+      __syncthreads();
+      if (spectral) cl_push_slab(cl, L, sm, L.r, L.gr, a0, nr);
     }
-    cl_block_sum(rs, red, part, 3);
+    cl_push_partial(cl, rs, red, 1, nc, rank);
     cl.sync();
-    double rsn = cl_total(cl, part, 3, L.nc, bcast);
+    const double rsn = cl_partial_total(red, 1, nc);
     its = it;
     if (rsn <= tol_sq || rsn <= rel_sq || rsn <= 1e-30) {
       converged = true;
       break;
     }
-    rz = cl_precondition(cl, L, sm, nr, c.k.inverse_scale, spectral);
-    __syncthreads();
-    cl_block_sum(rz, red, part, 4);
+    rz = cl_precondition(cl, L, sm, nr, rank, a0, c.k.inverse_scale, spectral);
+    cl_push_partial(cl, rz, red, 2, nc, rank);
     cl.sync();
-    double rho_new = cl_total(cl, part, 4, L.nc, bcast);
-    float beta = (float)(rho_new / (rho_old + 1e-30));
+    const double rho_new = cl_partial_total(red, 2, nc);
+    const float beta = (float)(rho_new / (rho_old + 1e-30));
     for (int e = threadIdx.x; e < n; e += blockDim.x) {
-      float *pp = sm + L.p + nj + e;
+      float *pp = p + nj + e;
       *pp = *pp * beta + sm[L.z + e];
     }
+    // the halo rows follow the owner's own update p = p*beta + z
+    for (int b = threadIdx.x; b < nj; b += blockDim.x) {
+      if (has_up) p[b] = p[b] * beta + sm[L.zh + b];
+      if (has_down) p[(nr + 1) * nj + b] = p[(nr + 1) * nj + b] * beta + sm[L.zh + nj + b];
+    }
     rho_old = rho_new;
-    cl.sync();  // p slabs complete before the next halo fetch
+    __syncthreads();
   }
   if (rank == 0 && threadIdx.x == 0) {
     // one slot per step of the call: sync[2] counts the solves
@@ -455,14 +541,14 @@ __global__ void __launch_bounds__(kClusterThreads, 1)
     if (!converged) atomicOr(c.status, NPOM_DEV_PCG_MAXIT);
   }
   // ---- solution: Shapiro filter + closed-basin bcond 1, d = h + elf
-  for (int e = threadIdx.x; e < n; e += blockDim.x) sm[L.p + nj + e] = sm[L.x + e];
+  for (int e = threadIdx.x; e < n; e += blockDim.x) p[nj + e] = sm[L.x + e];
   cl.sync();
   cl_halo(cl, L, sm, rank, nr);
   __syncthreads();
   for (int e = threadIdx.x; e < n; e += blockDim.x) {
     int ra = e / nj, b = e - ra * nj;
     int i = a0 + ra + 1, j = b + 1;
-    const float *pr = sm + L.p + (ra + 1) * nj;
+    const float *pr = p + (ra + 1) * nj;
     float x0 = pr[b];
     float ev;
     if (with_post) {
