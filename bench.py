@@ -35,6 +35,11 @@ UNIT = "simulated days/s"
 GRID = (90, 82, 16)
 DTI = 300.0
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the
+# phase's kernel at 90x82x16, from the ncu capture summarised in
+# profiles/k_pcg_cluster_seamount_90x82x16.md
+NCU_DRAM_BYTES = {"E_external": 561152}
+
 # Distinct arrays each phase reads / writes (3-D count, 2-D count): the
 # algorithmic-byte rule bytes = 4 * (sum of read numel + sum of written numel).
 PHASE_IO = {
@@ -265,8 +270,12 @@ def run_b200(args):
 
 
 def dominant_kernel_roofline(core, stream, dev, reps=20):
-    """Time each phase of one internal step alone (CUDA events, after a
-    warm-up) and report the slowest one against the HBM roofline."""
+    """Time each phase of one internal step (CUDA events on the launching
+    stream around that phase alone) and report the slowest one against the
+    HBM roofline.  Every repetition restores the state at the start of the
+    step and runs the preceding phases untimed, so each phase -- the PCG in
+    particular, whose iteration count depends on its input -- sees the
+    input it has inside a step."""
     import torch
     from neuralpom_b200 import _abi
     lib = _abi.load_library()
@@ -278,36 +287,50 @@ def dominant_kernel_roofline(core, stream, dev, reps=20):
     times = {}
     snapshot = {n: getattr(core, n).clone() for n in _abi.FIELD_NAMES}
     phases = [i for i, n in enumerate(_abi.PHASES) if n != "I5_corrector_filter" or core.core_name != "explicit"]
+
+    def run(ph):
+        _abi.check(lib.npom_run_phase(ctypes.byref(p), ctypes.byref(fa), ctypes.byref(ws["struct"]), ph, 1.0,
+                                      ctypes.c_void_p(stream.cuda_stream)), "phase")
+
     for ph in phases:
-        for n in _abi.FIELD_NAMES:
-            getattr(core, n).copy_(snapshot[n])
-        for _ in range(3):
-            _abi.check(lib.npom_run_phase(ctypes.byref(p), ctypes.byref(fa), ctypes.byref(ws["struct"]), ph, 1.0,
-                                          ctypes.c_void_p(stream.cuda_stream)), "phase")
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps + 2)]
+        for k in range(reps + 2):
+            for n in _abi.FIELD_NAMES:
+                getattr(core, n).copy_(snapshot[n])
+            for q in phases:
+                if q == ph:
+                    break
+                run(q)
+            ev[k][0].record(stream)
+            run(ph)
+            ev[k][1].record(stream)
         torch.cuda.synchronize(dev)
-        a.record(stream)
-        for _ in range(reps):
-            _abi.check(lib.npom_run_phase(ctypes.byref(p), ctypes.byref(fa), ctypes.byref(ws["struct"]), ph, 1.0,
-                                          ctypes.c_void_p(stream.cuda_stream)), "phase")
-        b.record(stream)
-        torch.cuda.synchronize(dev)
-        times[_abi.PHASES[ph]] = a.elapsed_time(b) / reps
+        times[_abi.PHASES[ph]] = sum(a.elapsed_time(b) for a, b in ev[2:]) / reps
     for n in _abi.FIELD_NAMES:
         getattr(core, n).copy_(snapshot[n])
     core.read_status(0)
+    def phase_bytes(ph):
+        r3, r2, w3, w2 = PHASE_IO[ph]
+        nb = 4 * ((r3 + w3) * n3 + (r2 + w2) * n2)
+        if ph == "E_external" and core.core_name != "explicit":
+            ni, nj = im - 2, jm - 2
+            nb += 4 * (ni * ni + nj * nj + ni * nj)  # DST matrices and eigenvalues
+        return nb
+
     name = max(times, key=times.get)
-    r3, r2, w3, w2 = PHASE_IO[name]
-    nbytes = 4 * ((r3 + w3) * n3 + (r2 + w2) * n2)
-    if name == "E_external" and core.core_name != "explicit":
-        ni, nj = im - 2, jm - 2
-        nbytes += 4 * (ni * ni + nj * nj + ni * nj)  # DST matrices and eigenvalues
+    nbytes = phase_bytes(name)
     sec = times[name] / 1000.0
     achieved = nbytes / sec / 1e9
     peak, src = measured_peaks()
+    traffic = NCU_DRAM_BYTES.get(name) if (im, jm, kb) == GRID else None
+    step_bytes = sum(phase_bytes(ph) for ph in times)
+    step_ms = sum(times.values())
     return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_source": src, "traffic": None, "algorithmic_bytes": nbytes,
-            "launch_ms": times[name], "phase_ms": {k: round(v, 5) for k, v in times.items()}}
+            "frac": achieved / peak, "peak_source": src, "traffic": traffic, "algorithmic_bytes": nbytes,
+            "launch_ms": times[name], "phase_ms": {k: round(v, 5) for k, v in times.items()},
+            "step": {"algorithmic_bytes": step_bytes, "ms": step_ms,
+                     "achieved": step_bytes / (step_ms / 1000.0) / 1e9,
+                     "frac": step_bytes / (step_ms / 1000.0) / 1e9 / peak}}
 
 
 def end_to_end(core, A, Sc, args, stream, dev, pg, ws_n):
