@@ -183,6 +183,25 @@ npom_status npom_proft(int ncol, int kb, const float *f_in, const float *wfsurf,
 npom_status npom_pcg_solve(const npom_params *p, float *const *fields,
                            const npom_workspace *ws, void *stream);
 
+/* Backward of the free-surface solve x = A(d)^-1 rhs for the cotangent
+ * grad_x = dJ/dx (all arrays im*jm device float32):
+ *   grad_rhs = dJ/drhs = A^-T grad_x, solved as M A^-1 M^-1 with relative
+ *              cell areas, the right-hand side scaled by max|.| clamped to 1
+ *              and the absolute PCG tolerance by the same factor, from a
+ *              zero guess (ws->cg_iters[0] receives the iterations);
+ *   grad_d   = dJ/dd, the transposed depth stencil of the operator at the
+ *              forward solution x.
+ * d2d is the depth the forward solve used.  The scale is read back to the
+ * host once (one stream synchronisation), so the call is not capturable.
+ * Replaces cores/implicit_p0_fixed/core.py:24 _ImplicitEtaSolveFunction
+ * (backward :46-59, _solve_implicit_eta_adjoint :231-252,
+ * _apply_elliptic_operator_depth_adjoint :645-675).  A non-finite
+ * cotangent sets NPOM_DEV_NONFINITE and returns NPOM_ERR_DEVICE. */
+npom_status npom_pcg_adjoint(const npom_params *p, float *const *fields,
+                             const npom_workspace *ws, const float *grad_x,
+                             const float *x, const float *d2d, float *grad_rhs,
+                             float *grad_d, void *stream);
+
 /* Reads (and with clear != 0 zeroes) the device status word; blocks on
  * the stream. */
 npom_status npom_status_read(const npom_workspace *ws, int clear,

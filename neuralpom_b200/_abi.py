@@ -130,6 +130,8 @@ def load_library():
     lib.npom_run_phase.argtypes = [P(NpomParams), P(FieldArray), P(NpomWorkspace), i32, dbl, vp]
     lib.npom_pcg_solve.restype = i32
     lib.npom_pcg_solve.argtypes = [P(NpomParams), P(FieldArray), P(NpomWorkspace), vp]
+    lib.npom_pcg_adjoint.restype = i32
+    lib.npom_pcg_adjoint.argtypes = [P(NpomParams), P(FieldArray), P(NpomWorkspace), vp, vp, vp, vp, vp, vp]
     lib.npom_proft.restype = i32
     lib.npom_proft.argtypes = [i32, i32, vp, vp, vp, i32, vp, vp, dbl, vp, vp, vp, i32, vp, dbl, vp, vp, vp, vp]
     lib.npom_status_read.restype = i32

@@ -55,6 +55,7 @@ class B200Core:
         self._ws = None
         self._ws_key = None
         self._eta_solver_iteration_history = []
+        self._eta_adjoint_iteration_history = []
 
     # -- reference-compatible helpers ------------------------------------
     @property
@@ -212,9 +213,85 @@ class ExplicitCore(B200Core):
     core_name = "explicit"
 
 
+class _EtaSolveFunction(torch.autograd.Function):
+    """The free-surface solve as an autograd node, like the reference's
+    ``_ImplicitEtaSolveFunction`` (``implicit_p0_fixed/core.py:24-59``):
+    gradients flow to ``rhs`` and ``d_2d``; the backward is the CUDA adjoint
+    ``npom_pcg_adjoint``."""
+
+    @staticmethod
+    def forward(ctx, core, rhs, d_2d, max_iter, tol, initial_guess):
+        x = core._eta_solve(rhs, d_2d, max_iter, tol, initial_guess)
+        ctx.core = core
+        ctx.max_iter, ctx.tol = max_iter, tol
+        ctx.save_for_backward(x, d_2d)
+        return x
+
+    @staticmethod
+    def backward(ctx, grad_x):
+        x, d_2d = ctx.saved_tensors
+        lam, grad_d = ctx.core._eta_adjoint(grad_x, x, d_2d, ctx.max_iter, ctx.tol)
+        return None, lam, grad_d, None, None, None
+
+
 class ImplicitCore(B200Core):
     """Semi-implicit free-surface core (reference ``cores/implicit_p0_fixed``)."""
     core_name = "implicit_p0_fixed"
+
+    def solve_implicit_eta_cg(self, rhs, d_2d, max_iter=200, tol=1e-7, print_cg_residual=True, initial_guess=None):
+        """One free-surface solve A(d_2d) x = rhs on the device, drop-in for
+        ``implicit_p0_fixed/core.py:775``: warm start ``2 el - elb`` unless an
+        initial guess is given, Dirichlet ring, the core's relative tolerance
+        and preconditioner, iterations appended to
+        ``_eta_solver_iteration_history``.  Differentiable in ``rhs`` and
+        ``d_2d`` when either requires grad."""
+        if torch.is_grad_enabled() and (rhs.requires_grad or d_2d.requires_grad):
+            return _EtaSolveFunction.apply(self, rhs, d_2d, max_iter, tol, initial_guess)
+        return self._eta_solve(rhs, d_2d, max_iter, tol, initial_guess)
+
+    def _solver_call(self, max_iter, tol):
+        lib = _abi.load_library()
+        if self.device.type != "cuda":
+            raise RuntimeError("the B200 core runs on CUDA devices only")
+        p = self.params()
+        p.eta_max_iter = int(max_iter)
+        p.eta_tol = float(tol)
+        return lib, p, self._fields(), self._workspace(), torch.cuda.current_stream(self.device)
+
+    def _plane(self, t):
+        return t.detach().to(device=self.device, dtype=torch.float32).reshape(self.im, self.jm).contiguous()
+
+    def _eta_solve(self, rhs, d_2d, max_iter, tol, initial_guess):
+        lib, p, fa, ws, st = self._solver_call(max_iter, tol)
+        if initial_guess is not None:
+            x = self._plane(initial_guess).clone()
+        else:
+            x = self._plane(2.0 * self.el.detach() - self.elb.detach())
+        d = self._plane(d_2d)
+        ws["bufs"]["rhs"].copy_(self._plane(rhs))
+        fields = _abi.FieldArray(*fa)
+        fields[_abi.FIELD_NAMES.index("elf")] = x.data_ptr()
+        fields[_abi.FIELD_NAMES.index("d")] = d.data_ptr()
+        _abi.check(lib.npom_pcg_solve(ctypes.byref(p), ctypes.byref(fields), ctypes.byref(ws["struct"]),
+                                      ctypes.c_void_p(st.cuda_stream)), "npom_pcg_solve")
+        self._eta_solver_iteration_history.append(int(ws["ctrl"][8].item()))
+        return x
+
+    def _eta_adjoint(self, grad_x, x, d_2d, max_iter, tol):
+        lib, p, fa, ws, st = self._solver_call(max_iter, tol)
+        g, xs, d = self._plane(grad_x), self._plane(x), self._plane(d_2d)
+        lam = torch.empty_like(g)
+        grad_d = torch.empty_like(g)
+        status = lib.npom_pcg_adjoint(ctypes.byref(p), ctypes.byref(fa), ctypes.byref(ws["struct"]),
+                                      ctypes.c_void_p(g.data_ptr()), ctypes.c_void_p(xs.data_ptr()),
+                                      ctypes.c_void_p(d.data_ptr()), ctypes.c_void_p(lam.data_ptr()),
+                                      ctypes.c_void_p(grad_d.data_ptr()), ctypes.c_void_p(st.cuda_stream))
+        if status == 3:
+            ws["ctrl"][4].zero_()
+            raise FloatingPointError("free-surface adjoint: non-finite cotangent")
+        _abi.check(status, "npom_pcg_adjoint")
+        self._eta_adjoint_iteration_history.append(int(ws["ctrl"][8].item()))
+        return lam, grad_d
 
 
 CORE_REGISTRY = {"explicit": ExplicitCore, "implicit_p0_fixed": ImplicitCore}

@@ -727,7 +727,103 @@ const char *kPhaseNames[] = {"A1_forcing_advct", "A2_baropg_smag_means", "A3_adv
                              "B7_tsfilter_dens",    "B8_advuv_profuv",    "B9_velfilter_shift"};
 constexpr int kNumPhases = (int)(sizeof(kPhaseNames) / sizeof(kPhaseNames[0]));
 
+// ---------------------------------------------------------------------------
+// adjoint of the free-surface solve (implicit_p0_fixed/core.py:24-59 backward,
+// :231-252 _solve_implicit_eta_adjoint, :645-675 depth adjoint)
+// ---------------------------------------------------------------------------
+
+// relative cell area of the area-weighted transpose (1 on the ring)
+__device__ __forceinline__ float adj_area(const Ctx &c, int i, int j) {
+  return interior(c, i, j) ? F2(art, i, j) / F2(art, 1, 1) : 1.0f;
+}
+
+// rhs = g / area into the rhs workspace; max |rhs| as float bits (a
+// non-negative float orders like its bit pattern, NaN above infinity)
+__global__ void k_adj_prep(Ctx c, const float *g, unsigned int *maxbits) {
+  const size_t n = (size_t)c.im * c.jm;
+  unsigned int m = 0u;
+  for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(o / c.jm), j = (int)(o - (size_t)i * c.jm);
+    const float v = g[o] / adj_area(c, i, j);
+    c.W[NPOM_W_rhs][o] = v;
+    const float a = fabsf(v);
+    if (!(a <= 3.4028235e38f)) atomicOr(c.status, NPOM_DEV_NONFINITE);
+    m = max(m, __float_as_uint(a));
+  }
+  m = __reduce_max_sync(0xffffffffu, m);
+  if ((threadIdx.x & 31) == 0) atomicMax(maxbits, m);
+}
+
+// normalised rhs (rhs / scale) and a zero initial guess
+__global__ void k_adj_scale(Ctx c, float scale, float *x) {
+  const size_t n = (size_t)c.im * c.jm;
+  for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
+    c.W[NPOM_W_rhs][o] = c.W[NPOM_W_rhs][o] / scale;
+    x[o] = 0.0f;
+  }
+}
+
+// lambda at an interior cell, times coeff / art: the factor every face
+// term of the depth adjoint starts from
+__device__ __forceinline__ float adj_lam(const Ctx &c, const float *sol, float scale, int i, int j) {
+  const size_t o = NPOM_I2(c, i, j);
+  const float lam = (sol[o] * adj_area(c, i, j)) * scale;
+  return (lam * c.k.implicit_coeff) * W2(inv_art, i, j);
+}
+__device__ __forceinline__ float adj_east(const Ctx &c, const float *x, const float *sol, float scale, int i, int j) {
+  return (((0.5f * adj_lam(c, sol, scale, i, j)) * (x[NPOM_I2(c, i + 1, j)] - x[NPOM_I2(c, i, j)])) * W2(ce, i, j)) *
+         F2(dum, i + 1, j);
+}
+__device__ __forceinline__ float adj_west(const Ctx &c, const float *x, const float *sol, float scale, int i, int j) {
+  return (((0.5f * adj_lam(c, sol, scale, i, j)) * (x[NPOM_I2(c, i, j)] - x[NPOM_I2(c, i - 1, j)])) * W2(cw, i, j)) *
+         F2(dum, i, j);
+}
+__device__ __forceinline__ float adj_north(const Ctx &c, const float *x, const float *sol, float scale, int i, int j) {
+  return (((0.5f * adj_lam(c, sol, scale, i, j)) * (x[NPOM_I2(c, i, j + 1)] - x[NPOM_I2(c, i, j)])) * W2(cn, i, j)) *
+         F2(dvm, i, j + 1);
+}
+__device__ __forceinline__ float adj_south(const Ctx &c, const float *x, const float *sol, float scale, int i, int j) {
+  return (((0.5f * adj_lam(c, sol, scale, i, j)) * (x[NPOM_I2(c, i, j)] - x[NPOM_I2(c, i, j - 1)])) * W2(cs, i, j)) *
+         F2(dvm, i, j);
+}
+
+// grad_d = -(depth adjoint): the reference scatters eight face terms with
+// in-place adds in a fixed statement order; each cell gathers the same
+// terms in that order (east of i-1, east, west, west of i+1, north of j-1,
+// north, south, south of j+1)
+__global__ void k_adj_grad_d(Ctx c, const float *x, const float *sol, float scale, float *grad_d) {
+  const size_t n = (size_t)c.im * c.jm;
+  for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(o / c.jm), j = (int)(o - (size_t)i * c.jm);
+    float acc = 0.0f;
+    if (interior(c, i - 1, j)) acc = acc + -adj_east(c, x, sol, scale, i - 1, j);
+    if (interior(c, i, j)) {
+      acc = acc + -adj_east(c, x, sol, scale, i, j);
+      acc = acc + adj_west(c, x, sol, scale, i, j);
+    }
+    if (interior(c, i + 1, j)) acc = acc + adj_west(c, x, sol, scale, i + 1, j);
+    if (interior(c, i, j - 1)) acc = acc + -adj_north(c, x, sol, scale, i, j - 1);
+    if (interior(c, i, j)) {
+      acc = acc + -adj_north(c, x, sol, scale, i, j);
+      acc = acc + adj_south(c, x, sol, scale, i, j);
+    }
+    if (interior(c, i, j + 1)) acc = acc + adj_south(c, x, sol, scale, i, j + 1);
+    grad_d[o] = -acc;
+  }
+}
+
+// lambda = solution * area * scale, in place
+__global__ void k_adj_lambda(Ctx c, float scale, float *sol) {
+  const size_t n = (size_t)c.im * c.jm;
+  for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(o / c.jm), j = (int)(o - (size_t)i * c.jm);
+    sol[o] = (sol[o] * adj_area(c, i, j)) * scale;
+  }
+}
+
 }  // namespace
+
+
 
 extern "C" {
 
@@ -818,6 +914,41 @@ npom_status npom_pcg_solve(const npom_params *p, float *const *fields, const npo
   launch_cells<XP_COEF>(c, s);
   e = run_pcg(c, plan, 0, 0, s);
   if (e != cudaSuccess) return NPOM_ERR_CUDA;
+  return cudaGetLastError() == cudaSuccess ? NPOM_OK : NPOM_ERR_CUDA;
+}
+
+npom_status npom_pcg_adjoint(const npom_params *p, float *const *fields, const npom_workspace *ws,
+                             const float *grad_x, const float *x, const float *d2d, float *grad_rhs, float *grad_d,
+                             void *stream) {
+  if (!check_args_dev(p, fields, ws) || p->core != NPOM_CORE_IMPLICIT || !grad_x || !x || !d2d || !grad_rhs ||
+      !grad_d)
+    return NPOM_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  Ctx c = make_ctx(p, fields, ws);
+  c.F[NPOM_F_d] = const_cast<float *>(d2d);
+  const size_t n = (size_t)c.im * c.jm;
+  const int blocks = std::max(1, std::min(blocks_for(n, kThreads), 1024));
+  if (cudaMemsetAsync(ws->sync, 0, 4 * sizeof(unsigned int), s) != cudaSuccess) return NPOM_ERR_CUDA;
+  k_adj_prep<<<blocks, kThreads, 0, s>>>(c, grad_x, ws->sync + 3);
+  unsigned int bits = 0u, status = 0u;
+  if (cudaMemcpyAsync(&bits, ws->sync + 3, sizeof(bits), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaMemcpyAsync(&status, ws->status, sizeof(status), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return NPOM_ERR_CUDA;
+  if (status & NPOM_DEV_NONFINITE) return NPOM_ERR_DEVICE;
+  float amax = 0.0f;
+  std::memcpy(&amax, &bits, sizeof(amax));
+  const float scale = amax > 1.0f ? amax : 1.0f;  // clamp_min(1)
+  k_adj_scale<<<blocks, kThreads, 0, s>>>(c, scale, grad_rhs);
+  launch_cells<XP_COEF>(c, s);
+  Ctx ca = c;
+  ca.F[NPOM_F_elf] = grad_rhs;               // zero guess in, A^-1 (g/area/scale) out
+  ca.k.eta_tol = p->eta_tol / (double)scale;  // same stopping test as the forward
+  PcgPlan plan{};
+  if (plan_pcg(ca, &plan) != cudaSuccess) return NPOM_ERR_CUDA;
+  if (run_pcg(ca, plan, 0, 0, s) != cudaSuccess) return NPOM_ERR_CUDA;
+  k_adj_grad_d<<<blocks, kThreads, 0, s>>>(c, x, grad_rhs, scale, grad_d);
+  k_adj_lambda<<<blocks, kThreads, 0, s>>>(c, scale, grad_rhs);
   return cudaGetLastError() == cudaSuccess ? NPOM_OK : NPOM_ERR_CUDA;
 }
 

@@ -1246,6 +1246,50 @@ def pcg_solve(rhs, d, x0, S, P, C, SC, max_iter, tol, rel_tol, precond, dot_dtyp
     return x, its
 
 
+def eta_depth_adjoint(eta, lam_eta, d, C):
+    """d/dd of <lam_eta, A(d) eta> with the sign of the reference, i.e. the
+    array that ``_ImplicitEtaSolveFunction.backward`` negates.  Restates
+    ``implicit_p0_fixed/core.py:645-675``; the eight scatter-adds run in the
+    reference's statement order (their rounding depends on it)."""
+    im, jm = eta.shape
+    i, j = slice(1, im - 1), slice(1, jm - 1)
+    ip, imn, jp, jmn = slice(2, im), slice(0, im - 2), slice(2, jm), slice(0, jm - 2)
+    grad = np.zeros_like(d)
+    lam = lam_eta[i, j] * C["coeff"] * C["inv_art"]
+    east = 0.5 * lam * (eta[ip, j] - eta[i, j]) * C["ce"] * C["me"]
+    west = 0.5 * lam * (eta[i, j] - eta[imn, j]) * C["cw"] * C["mw"]
+    north = 0.5 * lam * (eta[i, jp] - eta[i, j]) * C["cn"] * C["mn"]
+    south = 0.5 * lam * (eta[i, j] - eta[i, jmn]) * C["cs"] * C["ms"]
+    grad[ip, j] += -east
+    grad[i, j] += -east
+    grad[i, j] += west
+    grad[imn, j] += west
+    grad[i, jp] += -north
+    grad[i, j] += -north
+    grad[i, j] += south
+    grad[i, jmn] += south
+    return grad
+
+
+def eta_adjoint(g, x, d, S, P, C, SC, max_iter, tol, rel_tol, precond, dot_dtype=np.float64):
+    """Backward of the free-surface solve x = A(d)^-1 rhs for the cotangent
+    g = dJ/dx.  Restates ``implicit_p0_fixed/core.py:24-59`` (the autograd
+    function) and ``:231-252`` (A^-T = M A^-1 M^-1 with relative cell
+    areas, the right-hand side scaled by max|rhs| clamped to 1 and the
+    absolute tolerance by the same factor, zero initial guess).  Returns
+    (dJ/drhs, dJ/dd, adjoint iterations)."""
+    dt_ = g.dtype
+    area = np.ones_like(g)
+    area[1:-1, 1:-1] = S["art"][1:-1, 1:-1] / S["art"][1, 1]
+    rhs = g / area
+    scale = np.asarray(max(np.max(np.abs(rhs)), dt_.type(1.0)), dtype=dt_)
+    nrhs = rhs / scale
+    sol, its = pcg_solve(nrhs, d, np.zeros_like(g), S, P, C, SC, max_iter, float(tol) / float(scale), rel_tol,
+                         precond, dot_dtype=dot_dtype)
+    lam = sol * area * scale
+    return lam, -eta_depth_adjoint(x, lam, d, C), its
+
+
 def barotropic_predictor(S, P):
     """Restates ``implicit_p0_fixed/core.py:795-845``; returns
     (u_star, v_star, denom_u, denom_v) before the velocity BC."""

@@ -3,7 +3,7 @@
 Run in a container that holds the reference sources (default
 ``/root/reference/src``, or ``NPOM_REFERENCE_SRC``)::
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [proft] [steps] [adjoint]
 
 Writes ``tests/golden/*.npz``.  Every file records the reference's own CPU
 float32 outputs on seeded inputs; nothing here is needed at test time except
@@ -134,18 +134,54 @@ def make_proft_golden():
     print("wrote", path, os.path.getsize(path))
 
 
-def main():
+def make_eta_adjoint_golden(im=20, jm=18, seed=21):
+    """Forward and backward of the reference's free-surface solve
+    (``POM2K_Core.solve_implicit_eta_cg`` under autograd, i.e.
+    ``_ImplicitEtaSolveFunction``, core.py:24-59 and 231-252) on a perturbed
+    production core: seeded rhs, depth and cotangent g; J = sum(g * x)."""
+    import torch
+    name = "implicit_p0_fixed"
+    core = perturbed_core(name, im, jm, seed)
+    arrays, scalars = rh.extract_state(core)
+    g = torch.Generator().manual_seed(seed + 1000)
+    fsm = core.fsm
+    rhs = (core.elb + 0.02 * torch.randn(core.el.shape, generator=g) * fsm).detach().requires_grad_(True)
+    d2d = (core.d * (1.0 + 0.05 * torch.rand(core.el.shape, generator=g))).detach().requires_grad_(True)
+    x0 = (2.0 * core.el - core.elb).detach()
+    cot = torch.randn(core.el.shape, generator=g) * fsm
+    tol = 1.0e-10
+    core._eta_solver_iteration_history = []
+    x = core.solve_implicit_eta_cg(rhs, d2d, max_iter=200, tol=tol, print_cg_residual=False, initial_guess=x0)
+    fwd_its = list(core._eta_solver_iteration_history)
+    (x * cot).sum().backward()
+    out = {f"in__{k}": v for k, v in arrays.items()}
+    for k, v in scalars.items():
+        out[f"scalar__{k}"] = np.asarray(v)
+    out.update({"adj__rhs": rhs.detach().numpy(), "adj__d2d": d2d.detach().numpy(), "adj__x0": x0.numpy(),
+                "adj__x": x.detach().numpy(), "adj__g": cot.numpy(), "adj__grad_rhs": rhs.grad.numpy(),
+                "adj__grad_d": d2d.grad.numpy(), "adj__tol": np.asarray(tol),
+                "adj__fwd_its": np.asarray(fwd_its, dtype=np.int32)})
+    path = os.path.join(HERE, f"eta_adjoint_{im}x{jm}.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path))
+
+
+def main(which=("proft", "steps", "adjoint")):
     src = rh.default_reference_path()
     if src is None:
         raise SystemExit("reference sources not found; set NPOM_REFERENCE_SRC")
     rh.import_reference(src)
     import torch
     torch.set_num_threads(1)
-    make_proft_golden()
-    make_step_golden("explicit", 12, 10, seed=11)
-    make_step_golden("implicit_p0_fixed", 12, 10, seed=12)
-    make_step_golden("implicit_p0_fixed", 20, 18, seed=13, steps=(1,))
+    if "proft" in which:
+        make_proft_golden()
+    if "steps" in which:
+        make_step_golden("explicit", 12, 10, seed=11)
+        make_step_golden("implicit_p0_fixed", 12, 10, seed=12)
+        make_step_golden("implicit_p0_fixed", 20, 18, seed=13, steps=(1,))
+    if "adjoint" in which:
+        make_eta_adjoint_golden()
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]) or ("proft", "steps", "adjoint"))

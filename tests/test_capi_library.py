@@ -46,6 +46,7 @@ def test_argument_errors_need_no_gpu(lib):
     assert lib.npom_proft(0, 6, None, None, None, 1, None, None, 1.0, None, None, None, 2, None, 1e-6, None, None,
                           None, None) == 0
     assert lib.npom_step_implicit(None, None, None, None, None) == 1
+    assert lib.npom_pcg_adjoint(None, None, None, None, None, None, None, None, None) == 1
 
 
 def test_library_is_sm100a(lib):

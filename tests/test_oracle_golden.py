@@ -70,3 +70,62 @@ def test_barotropic_endpoint_transport_identity():
     d = np.array([10.0, 20.0], np.float32)
     got = 0.25 * (v * (2 * d) + v * (2 * d))
     np.testing.assert_allclose(got, v * d)
+
+
+def _adjoint_case():
+    z = np.load(golden_path("eta_adjoint_20x18.npz"))
+    A = {k[4:]: z[k] for k in z.files if k.startswith("in__")}
+    Sc = {k[8:]: (z[k].item() if z[k].dtype.kind in "biuf" else str(z[k])) for k in z.files if k.startswith("scalar__")}
+    adj = {k[5:]: z[k] for k in z.files if k.startswith("adj__")}
+    P = oracle_params(Sc, A, "implicit_p0_fixed")
+    C = O.implicit_coefficients(A, P)
+    SC = O.spectral_cache(A, P, C) if P.eta_solver_preconditioner == "spectral" else None
+    return A, P, C, SC, adj
+
+
+def test_oracle_eta_solve_and_adjoint_match_reference_autograd():
+    """Forward solve and backward (dJ/drhs, dJ/dd) of the free-surface
+    solve against the reference's _ImplicitEtaSolveFunction run under
+    torch autograd (core.py:24-59, 231-252, 645-675)."""
+    A, P, C, SC, adj = _adjoint_case()
+    tol = float(adj["tol"])
+    x, its = O.pcg_solve(adj["rhs"], adj["d2d"], adj["x0"], A, P, C, SC, int(P.eta_solver_max_iter), tol,
+                         float(P.eta_solver_rel_tol), P.eta_solver_preconditioner)
+    assert its == int(adj["fwd_its"][0])
+    assert rel_err(x, adj["x"]) < 1e-5
+    lam, grad_d, _ = O.eta_adjoint(adj["g"], adj["x"], adj["d2d"], A, P, C, SC, int(P.eta_solver_max_iter), tol,
+                                   float(P.eta_solver_rel_tol), P.eta_solver_preconditioner)
+    assert rel_err(lam, adj["grad_rhs"]) < 1e-5, rel_err(lam, adj["grad_rhs"])
+    assert rel_err(grad_d, adj["grad_d"]) < 1e-4, rel_err(grad_d, adj["grad_d"])
+
+
+def test_oracle_eta_adjoint_matches_central_differences_fp64():
+    """The adjoint against central finite differences of J = <g, x(rhs, d)>
+    in FP64 along random unit directions (eps 1e-3 relative), with the
+    solve converged far below the difference step."""
+    A, P, C, SC, adj = _adjoint_case()
+    A = {k: (v.astype(np.float64) if v.dtype == np.float32 else v) for k, v in A.items()}
+    C = O.implicit_coefficients(A, P)
+    SC = O.spectral_cache(A, P, C) if SC is not None else None
+    rhs, d2d, g = (adj[k].astype(np.float64) for k in ("rhs", "d2d", "g"))
+    tol, rel = 1e-13, 1e-13
+
+    def solve(r, d):
+        return O.pcg_solve(r, d, np.zeros_like(r), A, P, C, SC, 400, tol, rel, P.eta_solver_preconditioner)[0]
+
+    x = solve(rhs, d2d)
+    lam, grad_d, _ = O.eta_adjoint(g, x, d2d, A, P, C, SC, 400, tol, rel, P.eta_solver_preconditioner)
+    rng = np.random.default_rng(3)
+    inner = np.zeros_like(rhs, dtype=bool)
+    inner[1:-1, 1:-1] = True
+    for _ in range(4):
+        v = rng.standard_normal(rhs.shape) * inner
+        v /= np.linalg.norm(v)
+        eps = 1e-3 * np.abs(rhs).max()
+        fd = (np.sum(g * solve(rhs + eps * v, d2d)) - np.sum(g * solve(rhs - eps * v, d2d))) / (2 * eps)
+        assert abs(fd - np.sum(lam * v)) <= 1e-6 * max(abs(fd), 1e-12) + 1e-12
+        w = rng.standard_normal(rhs.shape)
+        w /= np.linalg.norm(w)
+        eps = 1e-3 * np.abs(d2d).max()
+        fd = (np.sum(g * solve(rhs, d2d + eps * w)) - np.sum(g * solve(rhs, d2d - eps * w))) / (2 * eps)
+        assert abs(fd - np.sum(grad_d * w)) <= 1e-3 * max(abs(fd), 1e-12) + 1e-12
