@@ -160,6 +160,23 @@ def l2_flush(buf):
     buf.add_(1.0)
 
 
+def max_over_ranks(ms, pg=None, dev=None):
+    """The slowest rank's device time (ms): every rank contributes its own
+    CUDA-event total; an FP64 all-reduce MAX is the only collective."""
+    if pg is None:
+        return float(ms)
+    import torch
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_days_per_s(n_members, steps, internal_steps, dti, t_max_ms):
+    """Whole-job throughput: every member's simulated days over the slowest
+    rank's time (weak scaling: one member per rank)."""
+    return n_members * steps * internal_steps * dti / 86400.0 / (t_max_ms / 1000.0)
+
+
 # ---------------------------------------------------------------------------
 # the B200 arm
 # ---------------------------------------------------------------------------
@@ -231,13 +248,8 @@ def run_b200(args):
     bits, its = core.read_status(nin)
     if bits & (_abi.DEV_TIMEOUT | _abi.DEV_VMAX | _abi.DEV_NONFINITE):
         raise RuntimeError(f"device status 0x{bits:x} in the timed region")
-    t_max = elapsed_ms
-    if pg:
-        t = torch.tensor([elapsed_ms], device=dev, dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        t_max = float(t.item())
-    days_total = ws_n * args.steps * nin * core.dti / 86400.0
-    value = days_total / (t_max / 1000.0)
+    t_max = max_over_ranks(elapsed_ms, pg, dev)
+    value = aggregate_days_per_s(ws_n, args.steps, nin, core.dti, t_max)
 
     # dominant kernel, timed alone on the same stream (CUDA events)
     roofline = dominant_kernel_roofline(core, stream, dev)
