@@ -125,7 +125,8 @@ typedef enum npom_status {
   NPOM_OK = 0,
   NPOM_ERR_ARG = 1,        /* bad argument (null pointer, size, kb)        */
   NPOM_ERR_CUDA = 2,       /* a CUDA runtime call failed                   */
-  NPOM_ERR_DEVICE = 3      /* the device status word is non-zero           */
+  NPOM_ERR_DEVICE = 3,     /* the device status word is non-zero           */
+  NPOM_ERR_TOO_LARGE = 4   /* grid above NPOM_STATIC_MAX_CELLS (static)    */
 } npom_status;
 
 /* Device status bits. */
@@ -201,6 +202,39 @@ npom_status npom_pcg_adjoint(const npom_params *p, float *const *fields,
                              const npom_workspace *ws, const float *grad_x,
                              const float *x, const float *d2d, float *grad_rhs,
                              float *grad_d, void *stream);
+
+/* Largest im*jm that npom_pcg_solve_static accepts. */
+#define NPOM_STATIC_MAX_CELLS 32768
+
+/* No-allocation variant of npom_pcg_solve.  This entry point has no
+ * counterpart in the reference (whose solve allocates its work tensors
+ * with torch).  It is for callers that cannot allocate device memory: a
+ * host ocean model that owns only its state arrays and has no device
+ * allocator of its own, or a real-time loop that forbids allocation once
+ * it has started.  Same solve, same kernels and same result as
+ * npom_pcg_solve: fields[elf] holds the initial guess on entry and the
+ * solution on exit; rhs (im*jm) is read, not modified; sx (ni*ni),
+ * sy (nj*nj) and inv_eigs (ni*nj) are the spectral operator inputs
+ * (unused, may be null, with the Jacobi preconditioner).
+ *   - Scratch: one file-scope __device__ array of the library (~2 MB:
+ *     15 planes of NPOM_STATIC_MAX_CELLS floats, 4096 doubles, 8 words),
+ *     one copy per device.  Nothing is allocated or freed.
+ *   - Limit: im*jm > NPOM_STATIC_MAX_CELLS returns NPOM_ERR_TOO_LARGE.
+ *   - Zeroing: the caller zeroes nothing; the call clears the scratch's
+ *     control words itself, and the solve writes every other scratch word
+ *     before reading it.
+ *   - First call per device: looks up the scratch address with
+ *     cudaGetSymbolAddress (device p->device current); make it before any
+ *     stream capture.
+ *   - Concurrency: calls on one device share the scratch; overlapping
+ *     calls (other streams, other threads) race.  Serialise them.
+ *   - Outputs: iters_out and status_out (device int / unsigned int, may be
+ *     null) receive the iteration count and the device status bits.  */
+npom_status npom_pcg_solve_static(const npom_params *p, float *const *fields,
+                                  const float *rhs, const float *sx,
+                                  const float *sy, const float *inv_eigs,
+                                  int *iters_out, unsigned int *status_out,
+                                  void *stream);
 
 /* Reads (and with clear != 0 zeroes) the device status word; blocks on
  * the stream. */

@@ -88,7 +88,8 @@ class NpomClock(ctypes.Structure):
 
 FieldArray = ctypes.c_void_p * len(FIELD_NAMES)
 
-STATUS_NAMES = {0: "NPOM_OK", 1: "NPOM_ERR_ARG", 2: "NPOM_ERR_CUDA", 3: "NPOM_ERR_DEVICE"}
+STATUS_NAMES = {0: "NPOM_OK", 1: "NPOM_ERR_ARG", 2: "NPOM_ERR_CUDA", 3: "NPOM_ERR_DEVICE", 4: "NPOM_ERR_TOO_LARGE"}
+STATIC_MAX_CELLS = 32768
 
 
 def library_path():
@@ -131,6 +132,8 @@ def load_library():
     lib.npom_pcg_solve.restype = i32
     lib.npom_pcg_solve.argtypes = [P(NpomParams), P(FieldArray), P(NpomWorkspace), vp]
     lib.npom_pcg_adjoint.restype = i32
+    lib.npom_pcg_solve_static.restype = i32
+    lib.npom_pcg_solve_static.argtypes = [P(NpomParams), P(FieldArray), vp, vp, vp, vp, vp, vp, vp]
     lib.npom_pcg_adjoint.argtypes = [P(NpomParams), P(FieldArray), P(NpomWorkspace), vp, vp, vp, vp, vp, vp]
     lib.npom_proft.restype = i32
     lib.npom_proft.argtypes = [i32, i32, vp, vp, vp, i32, vp, vp, dbl, vp, vp, vp, i32, vp, dbl, vp, vp, vp, vp]

@@ -825,6 +825,46 @@ __global__ void k_adj_lambda(Ctx c, float scale, float *sol) {
 
 
 
+// ---------------------------------------------------------------------------
+// Scratch of npom_pcg_solve_static: the solve's work planes, FP64 partials
+// and control words in this module's own device memory (one copy per
+// device), for callers that cannot allocate device memory -- a host ocean
+// model that owns only its state arrays and has no device allocator of its
+// own (a Fortran or C POM driver linked against this library), or a
+// real-time loop that forbids allocation once it has started.  The
+// address is looked up once per device; calls on one device share the
+// scratch and must not overlap.
+// ---------------------------------------------------------------------------
+constexpr size_t kStaticCells = NPOM_STATIC_MAX_CELLS;
+constexpr int kStaticPlanes = 15;  // rhs x r p zv ap ce cw cn cs inv_art diag t1 t2 + one never touched
+constexpr size_t kStaticPlaneBytes = (size_t)kStaticPlanes * kStaticCells * sizeof(float);
+constexpr size_t kStaticPartialBytes = 4 * (size_t)NPOM_MAX_COOP_BLOCKS * sizeof(double);
+constexpr size_t kStaticCtrlWords = 8;  // barrier counter, generation, solve counter, spare, status, iterations, pad
+constexpr size_t kStaticBytes = kStaticPlaneBytes + kStaticPartialBytes + kStaticCtrlWords * sizeof(unsigned int);
+
+static __device__ __align__(256) unsigned char g_pcg_scratch[kStaticBytes];
+
+namespace {
+
+std::mutex g_static_mutex;
+unsigned char *g_static_addr[64] = {};
+
+// Device address of g_pcg_scratch on `dev`, which must be current.
+cudaError_t static_scratch(int dev, unsigned char **out) {
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_static_mutex);
+  if (!g_static_addr[dev]) {
+    unsigned char *ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress((void **)&ptr, g_pcg_scratch);
+    if (e != cudaSuccess) return e;
+    g_static_addr[dev] = ptr;
+  }
+  *out = g_static_addr[dev];
+  return cudaSuccess;
+}
+
+}  // namespace
+
 extern "C" {
 
 int npom_abi_version(void) { return 1; }
@@ -949,6 +989,56 @@ npom_status npom_pcg_adjoint(const npom_params *p, float *const *fields, const n
   if (run_pcg(ca, plan, 0, 0, s) != cudaSuccess) return NPOM_ERR_CUDA;
   k_adj_grad_d<<<blocks, kThreads, 0, s>>>(c, x, grad_rhs, scale, grad_d);
   k_adj_lambda<<<blocks, kThreads, 0, s>>>(c, scale, grad_rhs);
+  return cudaGetLastError() == cudaSuccess ? NPOM_OK : NPOM_ERR_CUDA;
+}
+
+npom_status npom_pcg_solve_static(const npom_params *p, float *const *fields, const float *rhs, const float *sx,
+                                  const float *sy, const float *inv_eigs, int *iters_out, unsigned int *status_out,
+                                  void *stream) {
+  if (!p || !fields || !rhs || p->core != NPOM_CORE_IMPLICIT || p->im < 3 || p->jm < 3) return NPOM_ERR_ARG;
+  if (p->eta_precond == NPOM_PRECOND_SPECTRAL && (!sx || !sy || !inv_eigs)) return NPOM_ERR_ARG;
+  const size_t ncell = (size_t)p->im * p->jm;
+  if (ncell > kStaticCells) return NPOM_ERR_TOO_LARGE;
+  if (cudaSetDevice(p->device) != cudaSuccess) return NPOM_ERR_CUDA;
+  unsigned char *base = nullptr;
+  if (static_scratch(p->device, &base) != cudaSuccess) return NPOM_ERR_CUDA;
+  // a workspace view: the inputs are read in place, everything the solve
+  // writes lands in the scratch
+  float *planes = reinterpret_cast<float *>(base);
+  int next = 0;
+  auto plane = [&]() { return planes + (size_t)(next++) * kStaticCells; };
+  npom_workspace ws;
+  for (int w : {NPOM_W_rhs, NPOM_W_x, NPOM_W_r, NPOM_W_p, NPOM_W_zv, NPOM_W_ap, NPOM_W_ce, NPOM_W_cw, NPOM_W_cn,
+                NPOM_W_cs, NPOM_W_inv_art, NPOM_W_diag, NPOM_W_t1, NPOM_W_t2})
+    ws.buf[w] = plane();
+  float *untouched = plane();  // predictor planes: the solve reads and writes none of them
+  for (int w : {NPOM_W_us, NPOM_W_vs, NPOM_W_den_u, NPOM_W_den_v, NPOM_W_d_baro}) ws.buf[w] = untouched;
+  ws.buf[NPOM_W_sx] = const_cast<float *>(sx ? sx : untouched);
+  ws.buf[NPOM_W_sy] = const_cast<float *>(sy ? sy : untouched);
+  ws.buf[NPOM_W_inv_eigs] = const_cast<float *>(inv_eigs ? inv_eigs : untouched);
+  ws.partials = reinterpret_cast<double *>(base + kStaticPlaneBytes);
+  unsigned int *ctrl = reinterpret_cast<unsigned int *>(base + kStaticPlaneBytes + kStaticPartialBytes);
+  ws.sync = ctrl;
+  ws.status = ctrl + 4;
+  ws.cg_iters = reinterpret_cast<int *>(ctrl + 5);
+  if (!check_args(p, fields, &ws)) return NPOM_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  // the control words (barrier counter, solve counter, status) must start
+  // at zero: cleared on every call; every other scratch word is written by
+  // the solve before it is read
+  if (cudaMemsetAsync(ctrl, 0, kStaticCtrlWords * sizeof(unsigned int), s) != cudaSuccess) return NPOM_ERR_CUDA;
+  if (cudaMemcpyAsync(ws.buf[NPOM_W_rhs], rhs, ncell * sizeof(float), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+    return NPOM_ERR_CUDA;
+  Ctx c = make_ctx(p, fields, &ws);
+  PcgPlan plan{};
+  if (plan_pcg(c, &plan) != cudaSuccess) return NPOM_ERR_CUDA;
+  launch_cells<XP_COEF>(c, s);
+  if (run_pcg(c, plan, 0, 0, s) != cudaSuccess) return NPOM_ERR_CUDA;
+  if (iters_out && cudaMemcpyAsync(iters_out, ws.cg_iters, sizeof(int), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+    return NPOM_ERR_CUDA;
+  if (status_out &&
+      cudaMemcpyAsync(status_out, ws.status, sizeof(unsigned int), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+    return NPOM_ERR_CUDA;
   return cudaGetLastError() == cudaSuccess ? NPOM_OK : NPOM_ERR_CUDA;
 }
 
