@@ -72,6 +72,7 @@ def parse():
     ap.add_argument("--ref-device", default="cpu")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference core on this GPU")
     return ap.parse_args()
 
 
@@ -258,6 +259,10 @@ def run_b200(args):
     if not args.no_e2e:
         e2e = end_to_end(core, A, Sc, args, stream, dev, pg, ws_n)
 
+    ref_gpu = None
+    if rank == 0 and ws_n == 1 and not args.no_ref_gpu:
+        ref_gpu = reference_gpu_sample(A, Sc, dev)
+
     cpu = None
     if rank == 0 and ws_n == 1 and not args.no_cpu_baseline:
         cpu = reference_cpu_sample(A, Sc, internal_steps=args.ref_internal_steps, warm=1, reps=2)
@@ -271,7 +276,7 @@ def run_b200(args):
                    "pcg_iterations_last_step": its[-1] if its else None,
                    "members": ws_n, "parallelism": f"ensemble x{ws_n}" if ws_n > 1 else "single member",
                    "l2": "flushed (256 MiB write) before every timed step"},
-        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+        "roofline": roofline, "cpu_baseline": cpu, "reference_gpu": ref_gpu, "e2e": e2e, "gpu_launches": launches,
         "clocks": clk.summary(),
     }
     if rank == 0:
@@ -433,6 +438,25 @@ def reference_cpu_sample(A, Sc, internal_steps=6, warm=1, reps=2, device="cpu"):
     return {"value": days / sec, "unit": UNIT, "cores": threads, "kind": "reference",
             "sample": f"{reps} x {internal_steps} internal steps of the 90x82x16 seamount basin "
                       f"(reference PyTorch core, {device}, after {warm} warm-up step)"}
+
+
+def reference_gpu_sample(A, Sc, device, internal_steps=12, warm=2, reps=2):
+    """The reference PyTorch core (eager mode, torch CG: the reference's
+    default SparsePhysics options) on this GPU, on the same basin: the
+    comparison the B200 core is built to beat on the same hardware."""
+    import torch
+    core, rh = reference_core(A, Sc, device)
+    rh.advance(core, "implicit_p0_fixed", warm, device=device)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        rh.advance(core, "implicit_p0_fixed", internal_steps, device=device)
+    torch.cuda.synchronize()
+    sec = time.perf_counter() - t0
+    days = reps * internal_steps * float(core.dti) / 86400.0
+    return {"value": days / sec, "unit": UNIT, "device": str(device),
+            "sample": f"{reps} x {internal_steps} internal steps of the 90x82x16 seamount basin (reference PyTorch "
+                      f"core, eager, torch CG, after {warm} warm-up steps; wall clock around synchronised calls)"}
 
 
 def run_reference(args):
