@@ -35,6 +35,19 @@ UNIT = "simulated days/s"
 GRID = (90, 82, 16)
 DTI = 300.0
 
+# Workloads: the headline (the semi-implicit seamount basin, one bench step =
+# one simulated day) and a roofline-only one whose state (~290 MB) exceeds
+# L2: the explicit core on the 354x322x16 coastal basin with its open
+# southern boundary, one bench step = 6 simulated hours.
+WORKLOADS = {
+    "seamount": {"grid": GRID, "core": "implicit_p0_fixed", "internal": 288,
+                 "desc": "semi-implicit core, closed 90x82x16 seamount basin (dx=5 km), forward"},
+    "coastal": {"grid": (354, 322, 16), "core": "explicit", "internal": 60, "horizon": 360,
+                "desc": "explicit core, 354x322x16 coastal basin (dx=500 m, open south boundary with Flather "
+                        "condition and M2 elevation 1 m updated every bench step), forward; one bench step = 1 "
+                        "simulated hour, restarted from the initial state every 6 h"},
+}
+
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the
 # phase's kernel at 90x82x16, from the ncu capture summarised in
 # profiles/k_pcg_cluster_seamount_90x82x16.md
@@ -47,6 +60,7 @@ PHASE_IO = {
     "A2_baropg_smag_means": (6, 5, 3, 5),
     "A3_advave_predictor": (2, 27, 1, 15),
     "E_external": (0, 18, 0, 4),
+    "E_external_explicit": (0, 33, 0, 19),
     "I5_corrector_filter": (0, 22, 0, 13),
     "B1_barotropic_fix": (2, 6, 2, 0),
     "B2A_vertvl": (3, 8, 1, 0),
@@ -67,7 +81,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
-    ap.add_argument("--internal-steps", type=int, default=288, help="internal steps per benchmark step")
+    ap.add_argument("--internal-steps", type=int, default=None,
+                    help="internal steps per benchmark step (default: one simulated day / 6 h, per workload)")
+    ap.add_argument("--workload", default="seamount", choices=sorted(WORKLOADS))
     ap.add_argument("--ref-internal-steps", type=int, default=6, help="reference arm: internal steps per sample")
     ap.add_argument("--ref-device", default="cpu")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -87,8 +103,14 @@ def dist_env():
     return ws, rank, local
 
 
-def workload(member=0):
+def workload(member=0, name="seamount"):
     from neuralpom_b200 import cases
+    if name == "coastal":
+        im, jm, kb = WORKLOADS[name]["grid"]
+        A, Sc = cases.coastal_tide(im, jm, kb=kb)
+        Sc = dict(Sc)
+        Sc.update(time=0.25, time0=0.25)   # internal mode from the first step
+        return A, Sc
     A, Sc = cases.seamount(*GRID[:2], kb=GRID[2], dti=DTI)
     if member:
         # ensemble members: seeded temperature perturbation (0.2 degC)
@@ -212,9 +234,13 @@ def run_b200(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
         pg = dist
     build.build()
-    A, Sc = workload(member=rank)
-    core = resolve_core_class("implicit_p0_fixed").from_state(A, Sc, device=dev)
-    nin = args.internal_steps
+    W = WORKLOADS[args.workload]
+    if args.workload != "seamount":
+        # roofline-only workload: no reference samples, no host round trip
+        args.no_e2e = args.no_ref_gpu = args.no_cpu_baseline = True
+    A, Sc = workload(member=rank, name=args.workload)
+    core = resolve_core_class(W["core"]).from_state(A, Sc, device=dev)
+    nin = args.internal_steps or W["internal"]
     stream = torch.cuda.current_stream(dev)
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > L2
 
@@ -224,7 +250,28 @@ def run_b200(args):
         core.time = core.dti * nin / 86400.0 + t0
         return t0
 
+    # coastal workload: the boundary tide between bench steps and a restart
+    # from the initial state at the 6 h horizon (the set-up's window), both
+    # outside the timed region
+    horizon = W.get("horizon")
+    snapshot = {n: getattr(core, n).clone() for n in _abi.FIELD_NAMES} if horizon else None
+    start_time = float(core.time)
+    done = [0]
+
+    def prepare():
+        if not horizon:
+            return
+        if done[0] + nin > horizon:
+            for n in _abi.FIELD_NAMES:
+                getattr(core, n).copy_(snapshot[n])
+            core.time = core.time0 = start_time
+            done[0] = 0
+        from neuralpom_b200 import cases
+        core.els.fill_(cases.tide_elevation(float(core.time) - start_time))
+        done[0] += nin
+
     for _ in range(args.warmup):
+        prepare()
         day()
     bits, _ = core.read_status(nin)
     if bits & (_abi.DEV_TIMEOUT | _abi.DEV_VMAX | _abi.DEV_NONFINITE):
@@ -238,6 +285,7 @@ def run_b200(args):
     with ClockSampler(local) as clk:
         for k in range(args.steps):
             l2_flush(flush)
+            prepare()
             ev[k][0].record(stream)
             t0 = day()
             ev[k][1].record(stream)
@@ -257,7 +305,7 @@ def run_b200(args):
 
     e2e = None
     if not args.no_e2e:
-        e2e = end_to_end(core, A, Sc, args, stream, dev, pg, ws_n)
+        e2e = end_to_end(core, A, Sc, args, stream, dev, pg, ws_n, nin)
 
     ref_gpu = None
     if rank == 0 and ws_n == 1 and not args.no_ref_gpu:
@@ -271,9 +319,10 @@ def run_b200(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws_n, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (FP64 PCG dot products)", "data": "synthetic",
-        "config": {"workload": "semi-implicit core, closed 90x82x16 seamount basin (dx=5 km), forward",
-                   "grid": list(GRID), "dti_s": DTI, "internal_steps_per_step": nin, "pcg_tol": 1e-10,
-                   "pcg_iterations_last_step": its[-1] if its else None,
+        "config": {"workload": W["desc"], "grid": list(W["grid"]), "dti_s": float(core.dti),
+                   "internal_steps_per_step": nin,
+                   "pcg_tol": 1e-10 if W["core"] != "explicit" else None,
+                   "pcg_iterations_last_step": (its[-1] if its else None) if W["core"] != "explicit" else None,
                    "members": ws_n, "parallelism": f"ensemble x{ws_n}" if ws_n > 1 else "single member",
                    "l2": "flushed (256 MiB write) before every timed step"},
         "roofline": roofline, "cpu_baseline": cpu, "reference_gpu": ref_gpu, "e2e": e2e, "gpu_launches": launches,
@@ -327,7 +376,8 @@ def dominant_kernel_roofline(core, stream, dev, reps=20):
         getattr(core, n).copy_(snapshot[n])
     core.read_status(0)
     def phase_bytes(ph):
-        r3, r2, w3, w2 = PHASE_IO[ph]
+        key = "E_external_explicit" if (ph == "E_external" and core.core_name == "explicit") else ph
+        r3, r2, w3, w2 = PHASE_IO[key]
         nb = 4 * ((r3 + w3) * n3 + (r2 + w2) * n2)
         if ph == "E_external" and core.core_name != "explicit":
             ni, nj = im - 2, jm - 2
@@ -345,12 +395,13 @@ def dominant_kernel_roofline(core, stream, dev, reps=20):
     return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": src, "traffic": traffic, "algorithmic_bytes": nbytes,
             "launch_ms": times[name], "phase_ms": {k: round(v, 5) for k, v in times.items()},
+            "phase_frac": {k: round(phase_bytes(k) / (v / 1000.0) / 1e9 / peak, 4) for k, v in times.items()},
             "step": {"algorithmic_bytes": step_bytes, "ms": step_ms,
                      "achieved": step_bytes / (step_ms / 1000.0) / 1e9,
                      "frac": step_bytes / (step_ms / 1000.0) / 1e9 / peak}}
 
 
-def end_to_end(core, A, Sc, args, stream, dev, pg, ws_n):
+def end_to_end(core, A, Sc, args, stream, dev, pg, ws_n, nin):
     """Same metric through the public drop-in API with the state in pinned
     host memory: every step copies the full state host->device, advances one
     simulated day, and reads the prognostic state back."""
@@ -363,7 +414,6 @@ def end_to_end(core, A, Sc, args, stream, dev, pg, ws_n):
     host_out = {n: torch.empty_like(host[n]).pin_memory() for n in outs}
     h2d = sum(host[n].numel() * 4 for n in names)
     d2h = sum(host_out[n].numel() * 4 for n in outs)
-    nin = args.internal_steps
     steps = max(1, args.steps // 2)
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if pg:

@@ -270,3 +270,53 @@ def noise_basin(im=64, jm=64, kb=16, dte=6.0, isplit=30, dx=20.0e3, seed=0, core
     if core != "explicit":
         s["wind_forcing"] = False
     return finish_initialization(A, s, core)
+
+
+def tide_elevation(time_days, amplitude=1.0, period_h=12.42):
+    """M2 boundary elevation a cos(2 pi t / T) at time t (days)."""
+    return float(amplitude * math.cos(2.0 * math.pi * time_days * 24.0 / period_h))
+
+
+def coastal_tide(im=354, jm=322, kb=16, dte=2.0, isplit=30, dx=500.0, seed=4, land_fraction=0.35,
+                 amplitude=1.0, lat=30.0):
+    """Coastal basin for the explicit core with one open boundary: dx = dy =
+    500 m; land where seeded Gaussian-filtered noise (sigma 12 cells) is
+    below its land_fraction quantile (h = 1, so fsm = 0); water depth 2 m at
+    the coast growing to 60 m with the distance from it; west, east and
+    north edges closed; the south edge open through the explicit core's
+    Flather condition (rfs = 1) with the M2 elevation els = amplitude at
+    t = 0 (``tide_elevation`` gives it at later times); T = 15 degC,
+    S = 31 psu + 1 psu per 10 m of depth, no wind, f-plane at ``lat``."""
+    from scipy.ndimage import distance_transform_edt
+    core = "explicit"
+    s = state.default_scalars(core)
+    s.update(dte=dte, isplit=isplit, hmax=60.0, rfs=1.0)
+    state.derived_time(s)
+    A = _zeros(im, jm, kb)
+    A["dx"][:] = dx
+    A["dy"][:] = dx
+    A["north_e"][:] = lat
+    A["cor"][:] = F32(2.0 * 7.2921e-5 * math.sin(math.radians(lat)))
+    n = _noise((im, jm), 12.0, seed)
+    land = n < np.quantile(n, land_fraction)
+    land[0, :] = True
+    land[-1, :] = True
+    land[:, -1] = True
+    land[:, 0] = land[:, 1]          # the open row continues the first interior row
+    water = ~land
+    dist = distance_transform_edt(water)
+    h = np.where(water, 2.0 + 58.0 * np.minimum(dist / max(float(dist[water].max()), 1.0), 1.0), 1.0)
+    A["h"] = h.astype(F32)
+    A["z"], A["zz"], A["dz"], A["dzz"] = sigma_levels(kb)
+    areas_masks(A)
+    depths = (A["z"][None, None, :] * A["h"][:, :, None]).astype(F32)
+    A["tb"][:] = F32(15.0)
+    A["sb"] = (F32(31.0) - F32(0.1) * depths).astype(F32)
+    A["tclim"] = A["tb"].copy()
+    A["sclim"] = A["sb"].copy()
+    A["rho"] = dens_np(A["tb"], A["sb"], A["h"], A["zz"], A["fsm"], s)
+    A["rmean"] = A["rho"].copy()
+    A["els"][:] = F32(amplitude)
+    A["tbs"] = A["tb"][:, 0, :].copy()
+    A["sbs"] = A["sb"][:, 0, :].copy()
+    return finish_initialization(A, s, core)

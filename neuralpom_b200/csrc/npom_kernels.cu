@@ -481,10 +481,16 @@ bool lanes_enabled(const Ctx &c) {
   return !(env && std::strcmp(env, "0") == 0);
 }
 
+// Columns from which PROFT runs one thread per column: its lane form issues
+// every step of the sequential sweeps for the whole segment (~70x the
+// instructions per column), which only pays while columns are too few to
+// fill the GPU.  Both forms compute bitwise the same values.
+constexpr size_t kProftThreadColumns = 16384;
+
 template <int PH>
 void launch_cols(const Ctx &c, cudaStream_t s) {
   size_t n = (size_t)c.im * c.jm;
-  if (lanes_enabled(c)) {
+  if (lanes_enabled(c) && !(PH == CP_B6 && n >= kProftThreadColumns)) {
     k_lanes<PH><<<blocks_for(n * KL, kThreads), kThreads, 0, s>>>(c);
   } else {
     k_cols<PH><<<blocks_for(n, 128), 128, 0, s>>>(c);

@@ -361,6 +361,15 @@ __device__ __forceinline__ void lane_b6(const Ctx &c, int i, int j, int k, bool 
   const float swrad = F2(swrad, i, j);
   float tf = lane_proft(c, k, F3(uf, i, j, k), khk, kh_next, F2(wtsurf, i, j), F2(tsurf, i, j), c.k.nbct, dh, swrad);
   float sf = lane_proft(c, k, F3(vf, i, j, k), khk, kh_next, F2(wssurf, i, j), F2(ssurf, i, j), c.k.nbcs, dh, swrad);
+  // explicit bcond 4 (upstream T/S at the edges) replaces levels
+  // 0..kbm1-1 of an edge column; each lane evaluates its own level
+  if (is_explicit(c) && k < KL - 1 && (i == 0 || i == c.im - 1 || j == 0 || j == c.jm - 1)) {
+    float ub, vb;
+    if (bcond4_explicit_level(c, i, j, k, ub, vb)) {
+      tf = ub;
+      sf = vb;
+    }
+  }
   if (!st) return;
   P3(uf, i, j, k) = tf;
   P3(vf, i, j, k) = sf;

@@ -506,6 +506,7 @@ NPOM_HD float proft_column(const ProftCol &q) {
 // upstream edge values (baroclinic.py:666-844).
 // ---------------------------------------------------------------------------
 NPOM_HD void bcond4_explicit_edge(const Ctx &c, int i, int j, float *ufc, float *vfc);
+NPOM_HD bool bcond4_explicit_level(const Ctx &c, int i, int j, int k, float &uo, float &vo);
 
 NPOM_HD void phase_b6_column(const Ctx &c, int i, int j) {
   const int kb = c.kb;
@@ -539,66 +540,77 @@ NPOM_HD void phase_b6_column(const Ctx &c, int i, int j) {
   if (is_explicit(c) && (i == 0 || i == c.im - 1 || j == 0 || j == c.jm - 1)) bcond4_explicit_edge(c, i, j, ufc, vfc);
 }
 
-NPOM_HD void bcond4_explicit_edge(const Ctx &c, int i, int j, float *ufc, float *vfc) {
+// Explicit bcond 4 at level k (< kbm1) of an edge column: upstream T/S on
+// the east, west, north and south edges, in the reference order
+// (explicit/baroclinic.py:666-846; later sides win at corners).  Returns
+// false when (i, j) lies on no edge; uo/vo are the new uf/vf values.
+NPOM_HD bool bcond4_explicit_level(const Ctx &c, int i, int j, int k, float &uo, float &vo) {
   const int im = c.im, jm = c.jm, kbm1 = c.kb - 1;
   const float dti = c.k.dti;
-  // East, west, north, south in the reference order; later sides win.
+  bool any = false;
   for (int side = 0; side < 4; ++side) {
-    int ie, ii, jx, jxi;  // edge cell and inner cell
+    int ie, ii;  // edge index and inner index along the normal
     bool xdir;
     if (side == 0) { if (i != im - 1) continue; ie = im - 1; ii = im - 2; xdir = true; }
     else if (side == 1) { if (i != 0) continue; ie = 0; ii = 1; xdir = true; }
     else if (side == 2) { if (j != jm - 1) continue; ie = jm - 1; ii = jm - 2; xdir = false; }
     else { if (j != 0) continue; ie = 0; ii = 1; xdir = false; }
-    (void)jx; (void)jxi;
-    for (int k = 0; k < kbm1; ++k) {
-      float u1;
-      float tc, sc, ti, si, te, se;
-      if (xdir) {
-        float vel = (side == 0) ? F3(u, im - 1, j, k) : F3(u, 1, j, k);
-        float dsum = (side == 0) ? (F2(dx, im - 1, j) + F2(dx, im - 2, j)) : (F2(dx, 0, j) + F2(dx, 1, j));
-        u1 = 2.0f * vel * dti / dsum;
-        tc = F3(t, ie, j, k); sc = F3(s, ie, j, k); ti = F3(t, ii, j, k); si = F3(s, ii, j, k);
-        size_t eo = (size_t)j * c.kb + k;
-        te = ::npom::ld((side == 0 ? c.F[NPOM_F_tbe] : c.F[NPOM_F_tbw]) + eo);
-        se = ::npom::ld((side == 0 ? c.F[NPOM_F_sbe] : c.F[NPOM_F_sbw]) + eo);
-      } else {
-        float vel = (side == 2) ? F3(v, i, jm - 1, k) : F3(v, i, 1, k);
-        float dsum = (side == 2) ? (F2(dy, i, jm - 1) + F2(dy, i, jm - 2)) : (F2(dy, i, 0) + F2(dy, i, 1));
-        u1 = 2.0f * vel * dti / dsum;
-        tc = F3(t, i, ie, k); sc = F3(s, i, ie, k); ti = F3(t, i, ii, k); si = F3(s, i, ii, k);
-        size_t eo = (size_t)i * c.kb + k;
-        te = ::npom::ld((side == 2 ? c.F[NPOM_F_tbn] : c.F[NPOM_F_tbs]) + eo);
-        se = ::npom::ld((side == 2 ? c.F[NPOM_F_sbn] : c.F[NPOM_F_sbs]) + eo);
-      }
-      bool east_like = (side == 0 || side == 2);
-      float uo, vo;
-      if (east_like) {
-        if (u1 <= 0.0f) { uo = tc - u1 * (te - tc); vo = sc - u1 * (se - sc); }
-        else { uo = tc - u1 * (tc - ti); vo = sc - u1 * (sc - si); }
-      } else {
-        if (u1 >= 0.0f) { uo = tc - u1 * (tc - te); vo = sc - u1 * (sc - se); }
-        else { uo = tc - u1 * (ti - tc); vo = sc - u1 * (si - sc); }
-      }
-      // vertical correction for outflow on 1 <= k <= kbm1-2
-      if (kbm1 > 2 && k >= 1 && k <= kbm1 - 2) {
-        bool outflow = east_like ? (u1 > 0.0f) : (u1 < 0.0f);
-        if (outflow) {
-          float wsum, dtv, tm, tp, sm, sp;
-          if (xdir) {
-            wsum = F3(w, ii, j, k) + F3(w, ii, j, k + 1);
-            dtv = F2(dt, ii, j);
-            tm = F3(t, ii, j, k - 1); tp = F3(t, ii, j, k + 1); sm = F3(s, ii, j, k - 1); sp = F3(s, ii, j, k + 1);
-          } else {
-            wsum = F3(w, i, ii, k) + F3(w, i, ii, k + 1);
-            dtv = F2(dt, i, ii);
-            tm = F3(t, i, ii, k - 1); tp = F3(t, i, ii, k + 1); sm = F3(s, i, ii, k - 1); sp = F3(s, i, ii, k + 1);
-          }
-          float wm = 0.5f * wsum * dti / ((F1(zz, k - 1) - F1(zz, k + 1)) * dtv);
-          uo = uo - wm * (tm - tp);
-          vo = vo - wm * (sm - sp);
+    any = true;
+    float u1;
+    float tc, sc, ti, si, te, se;
+    if (xdir) {
+      float vel = (side == 0) ? F3(u, im - 1, j, k) : F3(u, 1, j, k);
+      float dsum = (side == 0) ? (F2(dx, im - 1, j) + F2(dx, im - 2, j)) : (F2(dx, 0, j) + F2(dx, 1, j));
+      u1 = 2.0f * vel * dti / dsum;
+      tc = F3(t, ie, j, k); sc = F3(s, ie, j, k); ti = F3(t, ii, j, k); si = F3(s, ii, j, k);
+      size_t eo = (size_t)j * c.kb + k;
+      te = ::npom::ld((side == 0 ? c.F[NPOM_F_tbe] : c.F[NPOM_F_tbw]) + eo);
+      se = ::npom::ld((side == 0 ? c.F[NPOM_F_sbe] : c.F[NPOM_F_sbw]) + eo);
+    } else {
+      float vel = (side == 2) ? F3(v, i, jm - 1, k) : F3(v, i, 1, k);
+      float dsum = (side == 2) ? (F2(dy, i, jm - 1) + F2(dy, i, jm - 2)) : (F2(dy, i, 0) + F2(dy, i, 1));
+      u1 = 2.0f * vel * dti / dsum;
+      tc = F3(t, i, ie, k); sc = F3(s, i, ie, k); ti = F3(t, i, ii, k); si = F3(s, i, ii, k);
+      size_t eo = (size_t)i * c.kb + k;
+      te = ::npom::ld((side == 2 ? c.F[NPOM_F_tbn] : c.F[NPOM_F_tbs]) + eo);
+      se = ::npom::ld((side == 2 ? c.F[NPOM_F_sbn] : c.F[NPOM_F_sbs]) + eo);
+    }
+    bool east_like = (side == 0 || side == 2);
+    if (east_like) {
+      if (u1 <= 0.0f) { uo = tc - u1 * (te - tc); vo = sc - u1 * (se - sc); }
+      else { uo = tc - u1 * (tc - ti); vo = sc - u1 * (sc - si); }
+    } else {
+      if (u1 >= 0.0f) { uo = tc - u1 * (tc - te); vo = sc - u1 * (sc - se); }
+      else { uo = tc - u1 * (ti - tc); vo = sc - u1 * (si - sc); }
+    }
+    // vertical correction for outflow on 1 <= k <= kbm1-2
+    if (kbm1 > 2 && k >= 1 && k <= kbm1 - 2) {
+      bool outflow = east_like ? (u1 > 0.0f) : (u1 < 0.0f);
+      if (outflow) {
+        float wsum, dtv, tm, tp, sm, sp;
+        if (xdir) {
+          wsum = F3(w, ii, j, k) + F3(w, ii, j, k + 1);
+          dtv = F2(dt, ii, j);
+          tm = F3(t, ii, j, k - 1); tp = F3(t, ii, j, k + 1); sm = F3(s, ii, j, k - 1); sp = F3(s, ii, j, k + 1);
+        } else {
+          wsum = F3(w, i, ii, k) + F3(w, i, ii, k + 1);
+          dtv = F2(dt, i, ii);
+          tm = F3(t, i, ii, k - 1); tp = F3(t, i, ii, k + 1); sm = F3(s, i, ii, k - 1); sp = F3(s, i, ii, k + 1);
         }
+        float wm = 0.5f * wsum * dti / ((F1(zz, k - 1) - F1(zz, k + 1)) * dtv);
+        uo = uo - wm * (tm - tp);
+        vo = vo - wm * (sm - sp);
       }
+    }
+  }
+  return any;
+}
+
+NPOM_HD void bcond4_explicit_edge(const Ctx &c, int i, int j, float *ufc, float *vfc) {
+  const int kbm1 = c.kb - 1;
+  for (int k = 0; k < kbm1; ++k) {
+    float uo, vo;
+    if (bcond4_explicit_level(c, i, j, k, uo, vo)) {
       ufc[k] = uo;
       vfc[k] = vo;
     }

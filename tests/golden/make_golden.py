@@ -3,7 +3,7 @@
 Run in a container that holds the reference sources (default
 ``/root/reference/src``, or ``NPOM_REFERENCE_SRC``)::
 
-    python tests/golden/make_golden.py [proft] [steps] [adjoint]
+    python tests/golden/make_golden.py [proft] [steps] [adjoint] [coastal]
 
 Writes ``tests/golden/*.npz``.  Every file records the reference's own CPU
 float32 outputs on seeded inputs; nothing here is needed at test time except
@@ -77,9 +77,10 @@ def perturbed_core(name, im, jm, seed):
     return core
 
 
-def make_step_golden(name, im, jm, seed, steps=(1, 3)):
+def make_step_golden(name, im, jm, seed, steps=(1, 3), core=None, tag=None):
     import torch
-    core = perturbed_core(name, im, jm, seed)
+    if core is None:
+        core = perturbed_core(name, im, jm, seed)
     arrays, scalars = rh.extract_state(core)
     out = {f"in__{k}": v for k, v in arrays.items()}
     for k, v in scalars.items():
@@ -97,7 +98,7 @@ def make_step_golden(name, im, jm, seed, steps=(1, 3)):
         hist = getattr(core, "_eta_solver_iteration_history", None)
         if hist is not None:
             out[f"out{n}__cg_iters"] = np.asarray(hist, dtype=np.int32)
-    tag = "explicit" if name == "explicit" else "implicit"
+    tag = tag or ("explicit" if name == "explicit" else "implicit")
     path = os.path.join(HERE, f"step_{tag}_{im}x{jm}.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path))
@@ -134,6 +135,21 @@ def make_proft_golden():
     print("wrote", path, os.path.getsize(path))
 
 
+def make_coastal_golden(im=40, jm=34, seed=4):
+    """The explicit core with an open southern boundary (Flather, rfs = 1,
+    boundary elevation 1 m) on the coastal basin of
+    ``neuralpom_b200.cases.coastal_tide``, clock at 0.25 days so that the
+    first step runs the internal mode."""
+    sys.path.insert(0, ROOT)
+    from neuralpom_b200 import cases
+    A, Sc = cases.coastal_tide(im, jm, seed=seed)
+    Sc = dict(Sc)
+    Sc.update(time=0.25, time0=0.25)
+    core = rh.build_reference_core("explicit", im, jm)
+    rh.load_state(core, A, Sc)
+    make_step_golden("explicit", im, jm, seed, core=core, tag="coastal")
+
+
 def make_eta_adjoint_golden(im=20, jm=18, seed=21):
     """Forward and backward of the reference's free-surface solve
     (``POM2K_Core.solve_implicit_eta_cg`` under autograd, i.e.
@@ -166,7 +182,7 @@ def make_eta_adjoint_golden(im=20, jm=18, seed=21):
     print("wrote", path, os.path.getsize(path))
 
 
-def main(which=("proft", "steps", "adjoint")):
+def main(which=("proft", "steps", "adjoint", "coastal")):
     src = rh.default_reference_path()
     if src is None:
         raise SystemExit("reference sources not found; set NPOM_REFERENCE_SRC")
@@ -181,7 +197,9 @@ def main(which=("proft", "steps", "adjoint")):
         make_step_golden("implicit_p0_fixed", 20, 18, seed=13, steps=(1,))
     if "adjoint" in which:
         make_eta_adjoint_golden()
+    if "coastal" in which:
+        make_coastal_golden()
 
 
 if __name__ == "__main__":
-    main(tuple(sys.argv[1:]) or ("proft", "steps", "adjoint"))
+    main(tuple(sys.argv[1:]) or ("proft", "steps", "adjoint", "coastal"))

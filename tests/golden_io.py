@@ -50,3 +50,26 @@ def rel_err(a, b):
     b = np.asarray(b, dtype=np.float64)
     den = max(float(np.max(np.abs(b))), 1e-30)
     return float(np.max(np.abs(a - b))) / den
+
+
+# Fields of the coastal case that are small residuals of cancelling terms:
+# the pressure-gradient diagnostics (differences of nearly equal densities
+# in a weakly stratified 2-60 m basin) and w in the first steps after the
+# tide enters (divergence against d(eta)/dt).  Measured on the oracle, a
+# 1-ulp change of T moves the diagnostics by 0.85-1.7 % after three steps
+# and a 1-ulp change of the boundary elevation moves w by 1.0 % after one
+# step, so they are held to 2 %.
+ILL_CONDITIONED_COASTAL = ("w", "drhox", "drhoy", "drx2d", "dry2d")
+
+
+def step_field_error(got, ref, field, nsteps, golden):
+    """(error, bound) for one stored field of a step golden.  1e-5 relative
+    after one step, 1e-4 after three; w without its bottom level, whose exact
+    value is zero and whose computed value is cumsum rounding residue; the
+    ill-conditioned fields of the coastal case at 2 %."""
+    bound = 1e-5 if nsteps == 1 else 1e-4
+    if golden.startswith("step_coastal") and field in ILL_CONDITIONED_COASTAL:
+        bound = 2e-2
+    if field == "w":
+        return rel_err(got[..., :-1], ref[..., :-1]), bound
+    return rel_err(got, ref), bound
