@@ -11,8 +11,8 @@
 //   B1..B9       internal mode (skipped on the very first step from rest)
 //
 // The cooperative kernels (PCG, external subcycle) keep every block resident
-// (cudaLaunchCooperativeKernel) and synchronise through a sense-counting
-// grid barrier whose waits are bounded in time: a wait that runs out sets
+// (cudaLaunchCooperativeKernel) and synchronise through a counting grid
+// barrier whose waits are bounded in time: a wait that runs out sets
 // NPOM_DEV_TIMEOUT and the kernel returns instead of hanging.
 #include <cuda_runtime.h>
 
@@ -130,37 +130,35 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
 
 constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s
 
-// sync[0] = arrival counter, sync[1] = generation.  Returns false after a
-// timeout (or once any block has timed out); the caller then returns.
+// sync[0] counts arrivals and only grows during a launch (the host clears it
+// before every cooperative launch): barrier b of the launch is complete when
+// the count reaches (b + 1) * gridDim.x, so each block waits for the next
+// multiple of the grid size above its own arrival.  One atomic per block
+// and no reset inside the kernel keep each barrier at two serial L2 round
+// trips.  Returns false after a timeout (or once any block has timed out);
+// the caller then returns.
 __device__ bool grid_barrier(const Ctx &c) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     ok = 1;
-    volatile unsigned int *gen = c.sync + 1;
-    unsigned int my_gen = *gen;
     __threadfence();
-    unsigned int arrived = atomicAdd(c.sync, 1u);
-    if (arrived == gridDim.x - 1) {
-      atomicExch(c.sync, 0u);
-      __threadfence();
-      atomicAdd(c.sync + 1, 1u);
-    } else {
-      unsigned long long t0 = globaltimer_ns();
-      unsigned int spins = 0;
-      while (*gen == my_gen) {
-        if ((++spins & 63u) == 0) {
-          if (*(volatile unsigned int *)c.status & NPOM_DEV_TIMEOUT) {
-            ok = 0;
-            break;
-          }
-          if (globaltimer_ns() - t0 > kBarrierTimeoutNs) {
-            atomicOr(c.status, NPOM_DEV_TIMEOUT);
-            ok = 0;
-            break;
-          }
+    const unsigned int arrived = atomicAdd(c.sync, 1u);
+    const unsigned int target = (arrived / gridDim.x + 1u) * gridDim.x;
+    volatile unsigned int *count = c.sync;
+    unsigned long long t0 = globaltimer_ns();
+    unsigned int spins = 0;
+    while ((int)(*count - target) < 0) {
+      if ((++spins & 63u) == 0) {
+        if (*(volatile unsigned int *)c.status & NPOM_DEV_TIMEOUT) {
+          ok = 0;
+          break;
         }
-        __nanosleep(32);
+        if (globaltimer_ns() - t0 > kBarrierTimeoutNs) {
+          atomicOr(c.status, NPOM_DEV_TIMEOUT);
+          ok = 0;
+          break;
+        }
       }
     }
     __threadfence();
@@ -463,7 +461,11 @@ cudaError_t coop_blocks(const void *fn, size_t work, int *out) {
   return cudaSuccess;
 }
 
-cudaError_t launch_coop(const void *fn, int blocks, void **args, cudaStream_t s) {
+// Clears the barrier's arrival counter, then launches with every block
+// co-resident.
+cudaError_t launch_coop(const void *fn, int blocks, void **args, unsigned int *counter, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), s);
+  if (e != cudaSuccess) return e;
   return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(kThreads), args, 0, s);
 }
 
@@ -576,13 +578,13 @@ cudaError_t run_pcg(Ctx c, const PcgPlan &plan, int with_rhs, int with_post, cud
   if (plan.cluster) return run_pcg_cluster(c, plan.L, with_rhs, with_post, s);
   c.coh = 1;
   void *args[] = {&c, &with_rhs, &with_post};
-  return launch_coop((const void *)k_pcg, plan.coop_blocks, args, s);
+  return launch_coop((const void *)k_pcg, plan.coop_blocks, args, c.sync, s);
 }
 
 cudaError_t run_subcycle(Ctx c, int blocks, cudaStream_t s) {
   c.coh = 1;
   void *args[] = {&c};
-  return launch_coop((const void *)k_subcycle, blocks, args, s);
+  return launch_coop((const void *)k_subcycle, blocks, args, c.sync, s);
 }
 
 void internal_mode(const Ctx &c, cudaStream_t s) {
