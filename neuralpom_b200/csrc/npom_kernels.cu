@@ -119,6 +119,72 @@ __global__ void __launch_bounds__(kThreads) k_cells(Ctx c) {
   }
 }
 
+// A1 on large grids: every face flux of ADVCT computed once.  A block holds
+// kA1Cols output columns j (plus one halo column on each side) x 16 levels
+// and marches along i: the x-direction fluxes and the previous row's
+// curvature stay in registers, the y-direction fluxes and the curvature of
+// neighbouring columns pass through shared memory.  Each flux is the same
+// helper call, and the output expressions keep the point kernel's order,
+// so the results are bitwise those of k_points<PP_A1>.
+constexpr int kA1Cols = 16;
+constexpr int kA1Threads = 16 * (kA1Cols + 2);
+
+__global__ void __launch_bounds__(kA1Threads) k_a1_tiles(Ctx c, int ichunk) {
+  __shared__ float s_yu[kA1Cols + 2][16], s_yv[kA1Cols + 2][16], s_cv[kA1Cols + 2][16];
+  const int k = threadIdx.x & 15;
+  const int r = threadIdx.x >> 4;  // row r holds column j0 - 1 + r
+  const int j = blockIdx.x * kA1Cols - 1 + r;
+  const int i0 = blockIdx.y * ichunk, i1 = min(c.im, i0 + ichunk);
+  const bool jin = j >= 0 && j < c.jm;
+  const bool out_row = jin && r >= 1 && r <= kA1Cols;
+  const bool lev = k < c.kb - 1;
+  const int jc = jin ? j : 0;
+  // the values of row i0 - 1 that the first output row needs
+  float xu_prev = (jin && lev) ? advct_xflux_u(c, i0 - 1, jc, k) : 0.0f;
+  float xv_cur = (jin && lev) ? advct_xflux_v(c, i0, jc, k) : 0.0f;
+  float cv_prev = (jin && lev) ? advct_curv(c, i0 - 1, jc, k) : 0.0f;
+  for (int i = i0; i < i1; ++i) {
+    float xu = 0.0f, xv_next = 0.0f, yu = 0.0f, yv = 0.0f, cv = 0.0f;
+    if (jin && lev) {
+      xu = advct_xflux_u(c, i, jc, k);
+      if (i + 1 < c.im) xv_next = advct_xflux_v(c, i + 1, jc, k);
+      yu = advct_yflux_u(c, i, jc, k);
+      yv = advct_yflux_v(c, i, jc, k);
+      cv = advct_curv(c, i, jc, k);
+    }
+    s_yu[r][k] = yu;
+    s_yv[r][k] = yv;
+    s_cv[r][k] = cv;
+    __syncthreads();
+    if (out_row) {
+      float ax = 0.0f, ay = 0.0f, co = 0.0f;
+      if (lev && interior(c, i, j)) {
+        co = cv;
+        ax = xu - xu_prev + s_yu[r + 1][k] - yu;
+        if (i >= 2) {
+          float tc1 = cv * F2(dt, i, j) * (F3(v, i, j + 1, k) + F3(v, i, j, k));
+          float tc2 = cv_prev * F2(dt, i - 1, j) * (F3(v, i - 1, j + 1, k) + F3(v, i - 1, j, k));
+          ax -= F2(aru, i, j) * 0.25f * (tc1 + tc2);
+        }
+        ay = xv_next - xv_cur + yv - s_yv[r - 1][k];
+        if (j >= 2) {
+          float tc1 = cv * F2(dt, i, j) * (F3(u, i + 1, j, k) + F3(u, i, j, k));
+          float tc2 = s_cv[r - 1][k] * F2(dt, i, j - 1) * (F3(u, i + 1, j - 1, k) + F3(u, i, j - 1, k));
+          ay += F2(arv, i, j) * 0.25f * (tc1 + tc2);
+        }
+      }
+      P3(advx, i, j, k) = ax;
+      P3(advy, i, j, k) = ay;
+      P3(curv, i, j, k) = co;
+      if (k == 0) forcing_cell(c, i, j);
+    }
+    __syncthreads();
+    xu_prev = xu;
+    xv_cur = xv_next;
+    cv_prev = cv;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // bounded grid barrier (all blocks co-resident: cooperative launch)
 // ---------------------------------------------------------------------------
@@ -600,8 +666,33 @@ void internal_mode(const Ctx &c, cudaStream_t s) {
 }
 
 // Enqueue one internal step (all its kernels) on s.
+// A1 runs as flux-once tiles from kTileCells cells on (kb == 16; the point
+// kernel below that, where it has more threads in flight); NPOM_A1=tiles or
+// NPOM_A1=points forces either form.
+constexpr size_t kTileCells = 16384;
+
+void launch_a1(const Ctx &c, cudaStream_t s) {
+  const size_t ncell = (size_t)c.im * c.jm;
+  const char *env = getenv("NPOM_A1");
+  bool tiles = c.kb == 16 && ncell >= kTileCells;
+  if (env && c.kb == 16 && std::strcmp(env, "tiles") == 0) tiles = true;
+  if (env && std::strcmp(env, "points") == 0) tiles = false;
+  if (!tiles) {
+    launch_points<PP_A1>(c, s);
+    return;
+  }
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int strips = (c.jm + kA1Cols - 1) / kA1Cols;
+  // short marches, many blocks: ~16 blocks per SM (measured best at 354x322)
+  const int want = std::max(1, (16 * sms + strips - 1) / strips);
+  const int ichunk = std::max(2, (c.im + want - 1) / want);
+  const int chunks = (c.im + ichunk - 1) / ichunk;
+  k_a1_tiles<<<dim3(strips, chunks), kA1Threads, 0, s>>>(c, ichunk);
+}
+
 cudaError_t enqueue_step(const Ctx &c, int core, const PcgPlan &plan, int sub_blocks, cudaStream_t s) {
-  launch_points<PP_A1>(c, s);
+  launch_a1(c, s);
   launch_cols<CP_A2>(c, s);
   launch_cells<XP_A3>(c, s);
   cudaError_t e;
@@ -904,7 +995,7 @@ npom_status npom_run_phase(const npom_params *p, float *const *fields, const npo
   c.do_internal = 1;
   cudaError_t e = cudaSuccess;
   switch (phase) {
-    case 0: launch_points<PP_A1>(c, s); break;
+    case 0: launch_a1(c, s); break;
     case 1: launch_cols<CP_A2>(c, s); break;
     case 2: launch_cells<XP_A3>(c, s); break;
     case 3:

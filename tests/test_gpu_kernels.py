@@ -129,3 +129,32 @@ def test_pcg_solve_matches_oracle():
     # the solution satisfies the operator to the requested tolerance
     res = O.elliptic_apply(got, A["d"], C)[1:-1, 1:-1] - rhs[1:-1, 1:-1]
     assert np.linalg.norm(res) / np.linalg.norm(rhs[1:-1, 1:-1]) < 1e-4
+
+
+@pytest.mark.parametrize("case", ["gyre", "coastal"])
+def test_a1_flux_tiles_equal_point_kernel(monkeypatch, case):
+    """The flux-once tiled A1 kernel (large grids) writes bitwise what the
+    point kernel writes: advx, advy, curv and the surface forcing."""
+    from neuralpom_b200 import _abi, cases, resolve_core_class
+    if case == "gyre":
+        A, Sc = cases.double_gyre(37, 45, "explicit")
+    else:
+        A, Sc = cases.coastal_tide(60, 52)
+    Sc = dict(Sc)
+    Sc.update(time=0.25, time0=0.25)
+    lib = _lib()
+    stream = torch.cuda.current_stream()
+    outs = []
+    for form in ("points", "tiles"):
+        monkeypatch.setenv("NPOM_A1", form)
+        c = resolve_core_class("explicit").from_state(A, Sc, device="cuda")
+        # a developed state: two steps, then phase A1 alone
+        c.launch_steps(2, 0.25, 1, stream)
+        p, fa, ws = c.params(), c._fields(), c._workspace()
+        _abi.check(lib.npom_run_phase(ctypes.byref(p), ctypes.byref(fa), ctypes.byref(ws["struct"]), 0, 1.0,
+                                      ctypes.c_void_p(stream.cuda_stream)), "phase A1")
+        torch.cuda.synchronize()
+        outs.append({n: getattr(c, n).cpu().numpy() for n in ("advx", "advy", "curv", "wusurf", "wvsurf",
+                                                              "wtsurf", "wssurf", "u", "el")})
+    for n in outs[0]:
+        assert np.array_equal(outs[0][n], outs[1][n]), n
