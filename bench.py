@@ -88,6 +88,8 @@ def parse():
     ap.add_argument("--ref-device", default="cpu")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--members", type=int, default=8,
+                    help="ensemble members advanced concurrently on one GPU for the 'ensemble' key (1 = skip)")
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference core on this GPU")
     return ap.parse_args()
 
@@ -307,6 +309,10 @@ def run_b200(args):
     if not args.no_e2e:
         e2e = end_to_end(core, A, Sc, args, stream, dev, pg, ws_n, nin)
 
+    ens = None
+    if rank == 0 and ws_n == 1 and args.workload == "seamount" and args.members > 1:
+        ens = ensemble_sample(args, W, nin, dev, flush)
+
     ref_gpu = None
     if rank == 0 and ws_n == 1 and not args.no_ref_gpu:
         ref_gpu = reference_gpu_sample(A, Sc, dev)
@@ -325,7 +331,7 @@ def run_b200(args):
                    "pcg_iterations_last_step": (its[-1] if its else None) if W["core"] != "explicit" else None,
                    "members": ws_n, "parallelism": f"ensemble x{ws_n}" if ws_n > 1 else "single member",
                    "l2": "flushed (256 MiB write) before every timed step"},
-        "roofline": roofline, "cpu_baseline": cpu, "reference_gpu": ref_gpu, "e2e": e2e, "gpu_launches": launches,
+        "roofline": roofline, "cpu_baseline": cpu, "reference_gpu": ref_gpu, "ensemble": ens, "e2e": e2e, "gpu_launches": launches,
         "clocks": clk.summary(),
     }
     if rank == 0:
@@ -333,6 +339,61 @@ def run_b200(args):
     if pg:
         pg.barrier()
         pg.destroy_process_group()
+
+
+def ensemble_sample(args, W, nin, dev, flush):
+    """Members of an ensemble advanced together on one GPU: each seeded
+    member has its own core and its own stream, and every bench step
+    launches one simulated day of every member.  The step is latency bound
+    and the PCG cluster holds 8 of the SMs, so the members overlap; value =
+    all members' simulated days over the device time of the steps."""
+    import torch
+    from neuralpom_b200 import _abi, resolve_core_class
+    m = args.members
+    cores, streams = [], []
+    for member in range(m):
+        A, Sc = workload(member=member, name=args.workload)
+        cores.append(resolve_core_class(W["core"]).from_state(A, Sc, device=dev))
+        streams.append(torch.cuda.Stream(dev))
+    main = torch.cuda.current_stream(dev)
+
+    def day_all():
+        start = torch.cuda.Event()
+        start.record(main)
+        ends = []
+        for c, st in zip(cores, streams):
+            st.wait_event(start)
+            t0 = float(c.time)
+            c.launch_steps(nin, t0, 1, st)
+            c.time = c.dti * nin / 86400.0 + t0
+            e = torch.cuda.Event()
+            e.record(st)
+            ends.append(e)
+        for e in ends:
+            main.wait_event(e)
+
+    for _ in range(args.warmup):
+        day_all()
+    torch.cuda.synchronize(dev)
+    steps = max(2, args.steps // 2)
+    total = 0.0
+    for _ in range(steps):
+        l2_flush(flush)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(main)
+        day_all()
+        b.record(main)
+        torch.cuda.synchronize(dev)
+        total += a.elapsed_time(b)
+    for c in cores:
+        bits, _ = c.read_status(nin)
+        if bits & (_abi.DEV_TIMEOUT | _abi.DEV_VMAX | _abi.DEV_NONFINITE):
+            raise RuntimeError(f"device status 0x{bits:x} in the ensemble run")
+    value = aggregate_days_per_s(m, steps, nin, cores[0].dti, total)
+    return {"members": m, "value": value, "unit": UNIT, "ms_per_step": total / steps, "steps": steps,
+            "per_member": value / m,
+            "how": f"{m} seeded members (0.2 degC temperature perturbations), one core and one CUDA stream each, "
+                   "one simulated day of every member per step; device time with CUDA events around each step"}
 
 
 def dominant_kernel_roofline(core, stream, dev, reps=20):
