@@ -185,6 +185,62 @@ __global__ void __launch_bounds__(kA1Threads) k_a1_tiles(Ctx c, int ichunk) {
   }
 }
 
+// B5 on large grids: the ADVT1 face fluxes of T and S computed once per
+// face.  A block holds kB5Cols output columns (plus the column above) x 16
+// levels and marches along i; the x-face fluxes stay in registers, the
+// y-face fluxes of the column above pass through shared memory.  The output
+// expressions are those of phase_b5_point, so the results are bitwise equal.
+constexpr int kB5Cols = 16;
+constexpr int kB5Threads = 16 * (kB5Cols + 1);
+
+__global__ void __launch_bounds__(kB5Threads) k_b5_tiles(Ctx c, int ichunk) {
+  __shared__ float s_yt[kB5Cols + 1][16], s_ys[kB5Cols + 1][16];
+  const int k = threadIdx.x & 15;
+  const int r = threadIdx.x >> 4;  // row r holds column j0 + r
+  const int j = blockIdx.x * kB5Cols + r;
+  const int i0 = blockIdx.y * ichunk, i1 = min(c.im, i0 + ichunk);
+  const bool jin = j < c.jm;
+  const bool out_row = jin && r < kB5Cols;
+  const bool lev = k < c.kb - 1;
+  const int jc = jin ? j : 0;
+  const float *t = c.F[NPOM_F_t], *tb = c.F[NPOM_F_tb], *tcl = c.F[NPOM_F_tclim];
+  const float *sv = c.F[NPOM_F_s], *sb = c.F[NPOM_F_sb], *scl = c.F[NPOM_F_sclim];
+  // x-face fluxes at i0 (faces exist for 1 <= i <= im-1)
+  float xt = 0.0f, xs = 0.0f;
+  if (jin && lev && i0 >= 1) {
+    xt = advt1_xflux(c, t, tb, tcl, i0, jc, k);
+    xs = advt1_xflux(c, sv, sb, scl, i0, jc, k);
+  }
+  for (int i = i0; i < i1; ++i) {
+    float xt_n = 0.0f, xs_n = 0.0f, yt = 0.0f, ys = 0.0f;
+    if (jin && lev) {
+      if (i + 1 < c.im) {
+        xt_n = advt1_xflux(c, t, tb, tcl, i + 1, jc, k);
+        xs_n = advt1_xflux(c, sv, sb, scl, i + 1, jc, k);
+      }
+      if (jc >= 1) {
+        yt = advt1_yflux(c, t, tb, tcl, i, jc, k);
+        ys = advt1_yflux(c, sv, sb, scl, i, jc, k);
+      }
+    }
+    s_yt[r][k] = yt;
+    s_ys[r][k] = ys;
+    __syncthreads();
+    if (out_row) {
+      phase_b5_filter(c, i, j, k);
+      float tf_ = 0.0f, sf_ = 0.0f;
+      if (lev && interior(c, i, j)) {
+        tf_ = advt1_finish(c, t, tb, i, j, k, xt_n - xt + s_yt[r + 1][k] - yt);
+        sf_ = advt1_finish(c, sv, sb, i, j, k, xs_n - xs + s_ys[r + 1][k] - ys);
+      }
+      phase_b5_store(c, i, j, k, tf_, sf_);
+    }
+    __syncthreads();
+    xt = xt_n;
+    xs = xs_n;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // bounded grid barrier (all blocks co-resident: cooperative launch)
 // ---------------------------------------------------------------------------
@@ -653,13 +709,15 @@ cudaError_t run_subcycle(Ctx c, int blocks, cudaStream_t s) {
   return launch_coop((const void *)k_subcycle, blocks, args, c.sync, s);
 }
 
+void launch_b5(const Ctx &c, cudaStream_t s);
+
 void internal_mode(const Ctx &c, cudaStream_t s) {
   launch_cols<CP_B1>(c, s);
   launch_cols<CP_B2A>(c, s);
   launch_points<PP_B2B>(c, s);
   launch_cols<CP_B3>(c, s);
   launch_points<PP_B4>(c, s);
-  launch_points<PP_B5>(c, s);
+  launch_b5(c, s);
   launch_cols<CP_B6>(c, s);
   launch_points<PP_B7>(c, s);
   launch_cols<CP_B8>(c, s);
@@ -689,6 +747,27 @@ void launch_a1(const Ctx &c, cudaStream_t s) {
   const int ichunk = std::max(2, (c.im + want - 1) / want);
   const int chunks = (c.im + ichunk - 1) / ichunk;
   k_a1_tiles<<<dim3(strips, chunks), kA1Threads, 0, s>>>(c, ichunk);
+}
+
+// B5 the same way: flux-once tiles from kTileCells cells on (kb == 16, not
+// in mode 4); NPOM_B5=tiles or NPOM_B5=points forces either form.
+void launch_b5(const Ctx &c, cudaStream_t s) {
+  const size_t ncell = (size_t)c.im * c.jm;
+  const char *env = getenv("NPOM_B5");
+  bool tiles = c.kb == 16 && c.k.mode != 4 && ncell >= kTileCells;
+  if (env && c.kb == 16 && c.k.mode != 4 && std::strcmp(env, "tiles") == 0) tiles = true;
+  if (env && std::strcmp(env, "points") == 0) tiles = false;
+  if (!tiles) {
+    launch_points<PP_B5>(c, s);
+    return;
+  }
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int strips = (c.jm + kB5Cols - 1) / kB5Cols;
+  const int want = std::max(1, (16 * sms + strips - 1) / strips);
+  const int ichunk = std::max(2, (c.im + want - 1) / want);
+  const int chunks = (c.im + ichunk - 1) / ichunk;
+  k_b5_tiles<<<dim3(strips, chunks), kB5Threads, 0, s>>>(c, ichunk);
 }
 
 cudaError_t enqueue_step(const Ctx &c, int core, const PcgPlan &plan, int sub_blocks, cudaStream_t s) {
@@ -1019,7 +1098,7 @@ npom_status npom_run_phase(const npom_params *p, float *const *fields, const npo
     case 7: launch_points<PP_B2B>(c, s); break;
     case 8: launch_cols<CP_B3>(c, s); break;
     case 9: launch_points<PP_B4>(c, s); break;
-    case 10: launch_points<PP_B5>(c, s); break;
+    case 10: launch_b5(c, s); break;
     case 11: launch_cols<CP_B6>(c, s); break;
     case 12: launch_points<PP_B7>(c, s); break;
     case 13: launch_cols<CP_B8>(c, s); break;

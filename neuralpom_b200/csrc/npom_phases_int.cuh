@@ -345,37 +345,40 @@ NPOM_HD void phase_b4_point(const Ctx &c, int i, int j, int k) {
 // (time_loop.py:521-540), optional mixing clamp, then ADVT1 for T and S
 // (tracers.py:433-569) into uf/vf with the ghost-level copies of t/tb/s/sb.
 // ---------------------------------------------------------------------------
-NPOM_HD float advt1_point(const Ctx &c, const float *f, const float *fb, const float *fclim, int i, int j, int k) {
-  const int kb = c.kb, kbm1 = kb - 1;
-  if (!interior(c, i, j) || k >= kbm1) return 0.0f;
-  // ghost level of f/fb is only read at k = kb-1 (never, for k < kb-1)
-  auto xflux = [&](int ii) {
-    const size_t o = NPOM_I3(c, ii, j, k), om = NPOM_I3(c, ii - 1, j, k);
-    float xf = 0.25f * (F2(dt, ii, j) + F2(dt, ii - 1, j)) * (ld(f + o) + ld(f + om)) * F3(u, ii, j, k);
-    float aam_avg = 0.5f * (F3(aam, ii, j, k) + F3(aam, ii - 1, j, k));
-    float fa = ld(fb + o) - ld(fclim + o), fam = ld(fb + om) - ld(fclim + om);
-    xf -= aam_avg * (F2(h, ii, j) + F2(h, ii - 1, j)) * c.k.tprni * (fa - fam) * F2(dum, ii, j) /
-          (F2(dx, ii, j) + F2(dx, ii - 1, j));
-    xf *= 0.5f * (F2(dy, ii, j) + F2(dy, ii - 1, j));
-    return xf;
-  };
-  auto yflux = [&](int jj) {
-    const size_t o = NPOM_I3(c, i, jj, k), om = NPOM_I3(c, i, jj - 1, k);
-    float yf = 0.25f * (F2(dt, i, jj) + F2(dt, i, jj - 1)) * (ld(f + o) + ld(f + om)) * F3(v, i, jj, k);
-    float aam_avg = 0.5f * (F3(aam, i, jj, k) + F3(aam, i, jj - 1, k));
-    float fa = ld(fb + o) - ld(fclim + o), fam = ld(fb + om) - ld(fclim + om);
-    yf -= aam_avg * (F2(h, i, jj) + F2(h, i, jj - 1)) * c.k.tprni * (fa - fam) * F2(dvm, i, jj) /
-          (F2(dy, i, jj) + F2(dy, i, jj - 1));
-    yf *= 0.5f * (F2(dx, i, jj) + F2(dx, i, jj - 1));
-    return yf;
-  };
+// ADVT1 face fluxes of field f (tracers.py:433-569): x-face at (ii, j) for
+// ii >= 1 and y-face at (i, jj) for jj >= 1, level k < kb-1
+NPOM_HD float advt1_xflux(const Ctx &c, const float *f, const float *fb, const float *fclim, int ii, int j, int k) {
+  const size_t o = NPOM_I3(c, ii, j, k), om = NPOM_I3(c, ii - 1, j, k);
+  float xf = 0.25f * (F2(dt, ii, j) + F2(dt, ii - 1, j)) * (ld(f + o) + ld(f + om)) * F3(u, ii, j, k);
+  float aam_avg = 0.5f * (F3(aam, ii, j, k) + F3(aam, ii - 1, j, k));
+  float fa = ld(fb + o) - ld(fclim + o), fam = ld(fb + om) - ld(fclim + om);
+  xf -= aam_avg * (F2(h, ii, j) + F2(h, ii - 1, j)) * c.k.tprni * (fa - fam) * F2(dum, ii, j) /
+        (F2(dx, ii, j) + F2(dx, ii - 1, j));
+  xf *= 0.5f * (F2(dy, ii, j) + F2(dy, ii - 1, j));
+  return xf;
+}
+
+NPOM_HD float advt1_yflux(const Ctx &c, const float *f, const float *fb, const float *fclim, int i, int jj, int k) {
+  const size_t o = NPOM_I3(c, i, jj, k), om = NPOM_I3(c, i, jj - 1, k);
+  float yf = 0.25f * (F2(dt, i, jj) + F2(dt, i, jj - 1)) * (ld(f + o) + ld(f + om)) * F3(v, i, jj, k);
+  float aam_avg = 0.5f * (F3(aam, i, jj, k) + F3(aam, i, jj - 1, k));
+  float fa = ld(fb + o) - ld(fclim + o), fam = ld(fb + om) - ld(fclim + om);
+  yf -= aam_avg * (F2(h, i, jj) + F2(h, i, jj - 1)) * c.k.tprni * (fa - fam) * F2(dvm, i, jj) /
+        (F2(dy, i, jj) + F2(dy, i, jj - 1));
+  yf *= 0.5f * (F2(dx, i, jj) + F2(dx, i, jj - 1));
+  return yf;
+}
+
+// the ADVT1 forecast at an interior (i, j, k < kb-1) from its horizontal
+// flux divergence (the ghost level of f/fb is never read here)
+NPOM_HD float advt1_finish(const Ctx &c, const float *f, const float *fb, int i, int j, int k, float horiz) {
+  const int kbm1 = c.kb - 1;
   const float art = F2(art, i, j);
   auto zflux = [&](int kk) {
     if (kk == 0) return ld(f + NPOM_I3(c, i, j, 0)) * F3(w, i, j, 0) * art;
     if (kk >= kbm1) return 0.0f;
     return 0.5f * (ld(f + NPOM_I3(c, i, j, kk - 1)) + ld(f + NPOM_I3(c, i, j, kk))) * F3(w, i, j, kk) * art;
   };
-  float horiz = xflux(i + 1) - xflux(i) + yflux(j + 1) - yflux(j);
   float vert = (zflux(k) - zflux(k + 1)) / F1(dz, k);
   float ff = horiz + vert;
   float tb = (F2(h, i, j) + F2(etb, i, j)) * art;
@@ -383,8 +386,16 @@ NPOM_HD float advt1_point(const Ctx &c, const float *f, const float *fb, const f
   return (tb * ld(fb + NPOM_I3(c, i, j, k)) - c.k.dti2 * ff) / (tf + 1e-20f);
 }
 
-NPOM_HD void phase_b5_point(const Ctx &c, int i, int j, int k) {
-  const int kb = c.kb;
+NPOM_HD float advt1_point(const Ctx &c, const float *f, const float *fb, const float *fclim, int i, int j, int k) {
+  if (!interior(c, i, j) || k >= c.kb - 1) return 0.0f;
+  float horiz = advt1_xflux(c, f, fb, fclim, i + 1, j, k) - advt1_xflux(c, f, fb, fclim, i, j, k) +
+                advt1_yflux(c, f, fb, fclim, i, j + 1, k) - advt1_yflux(c, f, fb, fclim, i, j, k);
+  return advt1_finish(c, f, fb, i, j, k, horiz);
+}
+
+// B5 at one point, part 1: q2/q2l Robert-Asselin filter with the bcond 6
+// mask and the optional mixing clamp
+NPOM_HD void phase_b5_filter(const Ctx &c, int i, int j, int k) {
   const float fsm = F2(fsm, i, j);
   // bcond 6 mask (explicit adds 1e-10)
   float uf6 = F3(uf, i, j, k) * fsm;
@@ -406,11 +417,13 @@ NPOM_HD void phase_b5_point(const Ctx &c, int i, int j, int k) {
     P3(km, i, j, k) = fminf_t(fmaxf_t(F3(km, i, j, k), 0.0f), c.k.vmix);
     P3(kq, i, j, k) = fminf_t(fmaxf_t(F3(kq, i, j, k), 0.0f), c.k.vmix);
   }
-  if (c.k.mode == 4) return;
-  // ADVT1 forecasts; the ghost copy f[..., kb-1] = f[..., kb-2] is part of
-  // the stored t/tb/s/sb state (advt1 returns the modified copies)
-  float tf_ = advt1_point(c, c.F[NPOM_F_t], c.F[NPOM_F_tb], c.F[NPOM_F_tclim], i, j, k);
-  float sf_ = advt1_point(c, c.F[NPOM_F_s], c.F[NPOM_F_sb], c.F[NPOM_F_sclim], i, j, k);
+}
+
+// B5 part 2: store the ADVT1 forecasts; the ghost copy f[..., kb-1] =
+// f[..., kb-2] is part of the stored t/tb/s/sb state (advt1 returns the
+// modified copies)
+NPOM_HD void phase_b5_store(const Ctx &c, int i, int j, int k, float tf_, float sf_) {
+  const int kb = c.kb;
   P3(uf, i, j, k) = tf_;
   P3(vf, i, j, k) = sf_;
   if (k == kb - 1) {
@@ -419,6 +432,14 @@ NPOM_HD void phase_b5_point(const Ctx &c, int i, int j, int k) {
     P3(s, i, j, k) = F3(s, i, j, kb - 2);
     P3(sb, i, j, k) = F3(sb, i, j, kb - 2);
   }
+}
+
+NPOM_HD void phase_b5_point(const Ctx &c, int i, int j, int k) {
+  phase_b5_filter(c, i, j, k);
+  if (c.k.mode == 4) return;
+  float tf_ = advt1_point(c, c.F[NPOM_F_t], c.F[NPOM_F_tb], c.F[NPOM_F_tclim], i, j, k);
+  float sf_ = advt1_point(c, c.F[NPOM_F_s], c.F[NPOM_F_sb], c.F[NPOM_F_sclim], i, j, k);
+  phase_b5_store(c, i, j, k, tf_, sf_);
 }
 
 // ---------------------------------------------------------------------------

@@ -132,9 +132,13 @@ def test_pcg_solve_matches_oracle():
 
 
 @pytest.mark.parametrize("case", ["gyre", "coastal"])
-def test_a1_flux_tiles_equal_point_kernel(monkeypatch, case):
-    """The flux-once tiled A1 kernel (large grids) writes bitwise what the
-    point kernel writes: advx, advy, curv and the surface forcing."""
+@pytest.mark.parametrize("phase,env,fields", [
+    (0, "NPOM_A1", ("advx", "advy", "curv", "wusurf", "wvsurf", "wtsurf", "wssurf")),
+    (10, "NPOM_B5", ("uf", "vf", "q2", "q2b", "q2l", "q2lb", "t", "tb", "s", "sb"))])
+def test_flux_tiles_equal_point_kernel(monkeypatch, case, phase, env, fields):
+    """The flux-once tiled kernels of large grids (A1: forcing + ADVCT; B5:
+    q filter + ADVT1 of T and S) write bitwise what the point kernels
+    write."""
     from neuralpom_b200 import _abi, cases, resolve_core_class
     if case == "gyre":
         A, Sc = cases.double_gyre(37, 45, "explicit")
@@ -146,15 +150,14 @@ def test_a1_flux_tiles_equal_point_kernel(monkeypatch, case):
     stream = torch.cuda.current_stream()
     outs = []
     for form in ("points", "tiles"):
-        monkeypatch.setenv("NPOM_A1", form)
+        monkeypatch.setenv(env, form)
         c = resolve_core_class("explicit").from_state(A, Sc, device="cuda")
-        # a developed state: two steps, then phase A1 alone
+        # a developed state: two steps, then the phase alone
         c.launch_steps(2, 0.25, 1, stream)
         p, fa, ws = c.params(), c._fields(), c._workspace()
-        _abi.check(lib.npom_run_phase(ctypes.byref(p), ctypes.byref(fa), ctypes.byref(ws["struct"]), 0, 1.0,
-                                      ctypes.c_void_p(stream.cuda_stream)), "phase A1")
+        _abi.check(lib.npom_run_phase(ctypes.byref(p), ctypes.byref(fa), ctypes.byref(ws["struct"]), phase, 1.0,
+                                      ctypes.c_void_p(stream.cuda_stream)), "phase")
         torch.cuda.synchronize()
-        outs.append({n: getattr(c, n).cpu().numpy() for n in ("advx", "advy", "curv", "wusurf", "wvsurf",
-                                                              "wtsurf", "wssurf", "u", "el")})
+        outs.append({n: getattr(c, n).cpu().numpy() for n in fields + ("u", "el")})
     for n in outs[0]:
         assert np.array_equal(outs[0][n], outs[1][n]), n

@@ -195,3 +195,31 @@ def test_gpu_coastal_open_boundary_matches_oracle():
     for f in ("u", "v", "t", "s", "el", "q2", "km", "kh", "rho", "ua", "va", "elf", "w"):
         err, bound = step_field_error(getattr(c, f).cpu().numpy(), S[f], f, 3, "step_coastal")
         assert err < bound, (f, err)
+
+
+def test_gpu_explicit_double_gyre_48_steps_matches_oracle():
+    """The explicit basin of the 64x64x16 double-gyre set-up (dx = 20 km,
+    dtE = 6 s, isplit 30) from rest for the full 48 internal steps in one
+    call (graph replay after the first step): T and S within 1e-5, every
+    field within 10x the oracle's own spread under a 1-ulp change of T
+    (floor 1e-5)."""
+    from neuralpom_b200 import B200Physics, cases
+    A, Sc = cases.noise_basin(64, 64)
+    Sc = dict(Sc)
+    Sc.update(im=64, jm=64, kb=16)
+    c = _core(A, Sc, "explicit")
+    B200Physics(core_name="explicit").advance(c, steps=48)
+    runs = []
+    for perturb in (False, True):
+        A2 = dict(A)
+        if perturb:
+            A2["t"] = np.nextafter(A["t"], np.float32(np.inf)).astype(np.float32)
+        S = {k: v.copy() for k, v in A2.items()}
+        O.run(S, oracle_params(Sc, A2, "explicit"), 48, "explicit")
+        runs.append(S)
+    S, S2 = runs
+    for f in ("t", "s", "u", "v", "el", "q2", "kh", "km", "w", "rho", "ua", "va"):
+        spread = rel_err(S2[f], S[f])
+        bound = 1e-5 if f in ("t", "s") else max(10.0 * spread, 1e-5)
+        err = rel_err(getattr(c, f).cpu().numpy(), S[f])
+        assert err <= bound, (f, err, spread)
