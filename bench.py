@@ -42,6 +42,9 @@ DTI = 300.0
 WORKLOADS = {
     "seamount": {"grid": GRID, "core": "implicit_p0_fixed", "internal": 288,
                  "desc": "semi-implicit core, closed 90x82x16 seamount basin (dx=5 km), forward"},
+    "gyre": {"grid": (64, 64, 16), "core": "explicit", "internal": 480,
+             "desc": "explicit core, 64x64x16 double-gyre basin (dx=20 km, dtE=6 s, isplit=30, seeded "
+                     "bathymetry noise), forward; one bench step = one simulated day (480 internal steps)"},
     "coastal": {"grid": (354, 322, 16), "core": "explicit", "internal": 60, "horizon": 360,
                 "desc": "explicit core, 354x322x16 coastal basin (dx=500 m, open south boundary with Flather "
                         "condition and M2 elevation 1 m updated every bench step), forward; one bench step = 1 "
@@ -107,6 +110,9 @@ def dist_env():
 
 def workload(member=0, name="seamount"):
     from neuralpom_b200 import cases
+    if name == "gyre":
+        im, jm, kb = WORKLOADS[name]["grid"]
+        return cases.noise_basin(im, jm, kb=kb)
     if name == "coastal":
         im, jm, kb = WORKLOADS[name]["grid"]
         A, Sc = cases.coastal_tide(im, jm, kb=kb)
@@ -237,7 +243,7 @@ def run_b200(args):
         pg = dist
     build.build()
     W = WORKLOADS[args.workload]
-    if args.workload != "seamount":
+    if args.workload == "coastal":
         # roofline-only workload: no reference samples, no host round trip
         args.no_e2e = args.no_ref_gpu = args.no_cpu_baseline = True
     A, Sc = workload(member=rank, name=args.workload)
@@ -315,11 +321,12 @@ def run_b200(args):
 
     ref_gpu = None
     if rank == 0 and ws_n == 1 and not args.no_ref_gpu:
-        ref_gpu = reference_gpu_sample(A, Sc, dev)
+        ref_gpu = reference_gpu_sample(A, Sc, dev, core_name=W["core"])
 
     cpu = None
     if rank == 0 and ws_n == 1 and not args.no_cpu_baseline:
-        cpu = reference_cpu_sample(A, Sc, internal_steps=args.ref_internal_steps, warm=1, reps=2)
+        cpu = reference_cpu_sample(A, Sc, internal_steps=args.ref_internal_steps, warm=1, reps=2,
+                                   core_name=W["core"])
 
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws_n, "steps": args.steps,
@@ -470,7 +477,7 @@ def end_to_end(core, A, Sc, args, stream, dev, pg, ws_n, nin):
     from neuralpom_b200 import _abi
     names = list(_abi.FIELD_NAMES)
     host = {n: torch.from_numpy(np.ascontiguousarray(A[n] if n in A else np.zeros(
-        _abi.field_shape(n, *GRID), np.float32))).pin_memory() for n in names}
+        _abi.field_shape(n, core.im, core.jm, core.kb), np.float32))).pin_memory() for n in names}
     outs = ("u", "v", "t", "s", "el", "ua", "va", "q2", "q2l", "km", "kh", "w", "rho")
     host_out = {n: torch.empty_like(host[n]).pin_memory() for n in outs}
     h2d = sum(host[n].numel() * 4 for n in names)
@@ -507,9 +514,9 @@ def end_to_end(core, A, Sc, args, stream, dev, pg, ws_n, nin):
 # the reference's own implementation
 # ---------------------------------------------------------------------------
 
-def reference_core(A, Sc, device="cpu"):
-    """Reference implicit core (baseline/_ref install, else the source tree)
-    loaded with this benchmark's state and clock."""
+def reference_core(A, Sc, device="cpu", core_name="implicit_p0_fixed"):
+    """Reference core (baseline/_ref install, else the source tree) loaded
+    with this benchmark's state and clock."""
     from oracle import ref_harness as rh
     path = os.path.join(ROOT, "baseline", "_ref")
     if not os.path.isdir(os.path.join(path, "neuralpom")):
@@ -518,10 +525,11 @@ def reference_core(A, Sc, device="cpu"):
         raise RuntimeError("reference package not installed (baseline/_ref missing)")
     rh.import_reference(path)
     import torch
-    from neuralpom.cores.implicit_p0_fixed import POM2K_Core
+    from neuralpom.core_factory import resolve_core_class as ref_resolve
     from neuralpom.hybrid import build_initialized_core
     im, jm, kb = A["u"].shape
-    core = build_initialized_core(POM2K_Core, torch.device(device), im, jm, dte=Sc["dte"], isplit=Sc["isplit"])
+    core = build_initialized_core(ref_resolve(core_name), torch.device(device), im, jm, dte=Sc["dte"],
+                                  isplit=Sc["isplit"])
     core.prtd1 = core.prtd2 = 1e9
     core.iprint = 10 ** 9
     scal = {k: v for k, v in Sc.items() if k in (
@@ -533,41 +541,46 @@ def reference_core(A, Sc, device="cpu"):
     return core, rh
 
 
-def reference_cpu_sample(A, Sc, internal_steps=6, warm=1, reps=2, device="cpu"):
+def _basin_name(A):
+    im, jm, kb = A["u"].shape
+    return f"{im}x{jm}x{kb} basin"
+
+
+def reference_cpu_sample(A, Sc, internal_steps=6, warm=1, reps=2, device="cpu", core_name="implicit_p0_fixed"):
     import torch
     threads = os.cpu_count() or 1
     torch.set_num_threads(threads)
-    core, rh = reference_core(A, Sc, device)
-    rh.advance(core, "implicit_p0_fixed", warm, device=device)
+    core, rh = reference_core(A, Sc, device, core_name)
+    rh.advance(core, core_name, warm, device=device)
     t0 = time.perf_counter()
     for _ in range(reps):
-        rh.advance(core, "implicit_p0_fixed", internal_steps, device=device)
+        rh.advance(core, core_name, internal_steps, device=device)
     if device != "cpu":
         torch.cuda.synchronize()
     sec = time.perf_counter() - t0
     days = reps * internal_steps * float(core.dti) / 86400.0
     return {"value": days / sec, "unit": UNIT, "cores": threads, "kind": "reference",
-            "sample": f"{reps} x {internal_steps} internal steps of the 90x82x16 seamount basin "
-                      f"(reference PyTorch core, {device}, after {warm} warm-up step)"}
+            "sample": f"{reps} x {internal_steps} internal steps of the {_basin_name(A)} "
+                      f"(reference PyTorch core {core_name}, {device}, after {warm} warm-up step)"}
 
 
-def reference_gpu_sample(A, Sc, device, internal_steps=12, warm=2, reps=2):
+def reference_gpu_sample(A, Sc, device, internal_steps=12, warm=2, reps=2, core_name="implicit_p0_fixed"):
     """The reference PyTorch core (eager mode, torch CG: the reference's
     default SparsePhysics options) on this GPU, on the same basin: the
     comparison the B200 core is built to beat on the same hardware."""
     import torch
-    core, rh = reference_core(A, Sc, device)
-    rh.advance(core, "implicit_p0_fixed", warm, device=device)
+    core, rh = reference_core(A, Sc, device, core_name)
+    rh.advance(core, core_name, warm, device=device)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(reps):
-        rh.advance(core, "implicit_p0_fixed", internal_steps, device=device)
+        rh.advance(core, core_name, internal_steps, device=device)
     torch.cuda.synchronize()
     sec = time.perf_counter() - t0
     days = reps * internal_steps * float(core.dti) / 86400.0
     return {"value": days / sec, "unit": UNIT, "device": str(device),
-            "sample": f"{reps} x {internal_steps} internal steps of the 90x82x16 seamount basin (reference PyTorch "
-                      f"core, eager, torch CG, after {warm} warm-up steps; wall clock around synchronised calls)"}
+            "sample": f"{reps} x {internal_steps} internal steps of the {_basin_name(A)} (reference PyTorch core "
+                      f"{core_name}, eager, after {warm} warm-up steps; wall clock around synchronised calls)"}
 
 
 def run_reference(args):
