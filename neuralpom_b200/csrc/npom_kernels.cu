@@ -528,6 +528,33 @@ __global__ void __launch_bounds__(kThreads) k_subcycle(Ctx c) {
   }
 }
 
+// The same subcycle for grids of up to kSubClusterCells cells, on one
+// thread-block cluster of at most 16 CTAs: the three phases of a substep are
+// separated by the hardware cluster barrier (release/acquire at cluster
+// scope covers the global-memory state; loads bypass L1) instead of the
+// global-memory grid barrier, about a fifth of its latency.  Every CTA runs
+// the same loop, so every barrier is reached by all of them.
+constexpr int kSubClusterMax = 16;
+constexpr size_t kSubClusterCells = (size_t)kSubClusterMax * kThreads * 4;
+
+__global__ void __launch_bounds__(kThreads) k_subcycle_cluster(Ctx c) {
+  cgx::cluster_group cl = cgx::this_cluster();
+  const size_t ncell = (size_t)c.im * c.jm;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int iext = 1; iext <= c.k.isplit; ++iext) {
+    bool adv = (iext % c.k.ispadv) == 0;
+    for (size_t q = tid; q < ncell; q += stride) ext_phase1_cell(c, (int)(q / c.jm), (int)(q % c.jm), adv);
+    cl.sync();
+    bool exceed = false;
+    for (size_t q = tid; q < ncell; q += stride) exceed |= ext_phase2_cell(c, (int)(q / c.jm), (int)(q % c.jm), iext);
+    if (exceed) atomicOr(c.status, NPOM_DEV_VMAX);
+    cl.sync();
+    for (size_t q = tid; q < ncell; q += stride) ext_phase3_cell(c, (int)(q / c.jm), (int)(q % c.jm), iext);
+    cl.sync();
+  }
+}
+
 // PROFT over independent columns (TracersMixin.proft, any kb <= KMAX)
 __global__ void __launch_bounds__(128) k_proft(int ncol, int kb, const float *f_in, const float *wfsurf,
                                                const float *fsurf, int nbc, const float *h, const float *etf,
@@ -703,8 +730,64 @@ cudaError_t run_pcg(Ctx c, const PcgPlan &plan, int with_rhs, int with_post, cud
   return launch_coop((const void *)k_pcg, plan.coop_blocks, args, c.sync, s);
 }
 
+// Launch shape of the explicit subcycle, decided outside any capture:
+// > 0 grid-barrier blocks, < 0 the CTAs of one cluster.  NPOM_SUBCYCLE=grid
+// forces the grid-barrier form on small grids too.
+cudaError_t plan_subcycle(const Ctx &c, int *out) {
+  const size_t ncell = (size_t)c.im * c.jm;
+  const char *env = getenv("NPOM_SUBCYCLE");
+  const bool grid = env && std::strcmp(env, "grid") == 0;
+  if (!grid && ncell <= kSubClusterCells) {
+    static bool attr_set[64] = {false};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+      e = cudaFuncSetAttribute((const void *)k_subcycle_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+      if (e != cudaSuccess) return e;
+      attr_set[dev] = true;
+    }
+    int ctas = (int)std::min<size_t>(kSubClusterMax, (ncell + kThreads - 1) / kThreads);
+    ctas = std::max(1, ctas);
+    // a cluster of that size must fit on one GPC; halve it until one does
+    for (; ctas > 1; ctas /= 2) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(ctas);
+      cfg.blockDim = dim3(kThreads);
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = ctas;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      int nclusters = 0;
+      e = cudaOccupancyMaxActiveClusters(&nclusters, (const void *)k_subcycle_cluster, &cfg);
+      if (e == cudaSuccess && nclusters > 0) break;
+      cudaGetLastError();
+    }
+    *out = -ctas;
+    return cudaSuccess;
+  }
+  return coop_blocks((const void *)k_subcycle, ncell, out);
+}
+
 cudaError_t run_subcycle(Ctx c, int blocks, cudaStream_t s) {
   c.coh = 1;
+  if (blocks < 0) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(-blocks);
+    cfg.blockDim = dim3(kThreads);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = -blocks;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_subcycle_cluster, c);
+  }
   void *args[] = {&c};
   return launch_coop((const void *)k_subcycle, blocks, args, c.sync, s);
 }
@@ -795,6 +878,7 @@ cudaError_t enqueue_step(const Ctx &c, int core, const PcgPlan &plan, int sub_bl
 struct GraphEntry {
   int device;
   int core;
+  int sub_blocks;
   Ctx key;
   cudaGraphExec_t exec;
 };
@@ -817,7 +901,7 @@ cudaError_t launch_step_graph(const Ctx &c, int core, const PcgPlan &plan, int s
   if (e != cudaSuccess || dev < 0 || dev >= 64) return e;
   std::lock_guard<std::mutex> lock(g_graph_mutex);
   for (auto &g : g_graphs) {
-    if (g.device == dev && g.core == core && std::memcmp(&g.key, &c, sizeof(Ctx)) == 0) {
+    if (g.device == dev && g.core == core && g.sub_blocks == sub_blocks && std::memcmp(&g.key, &c, sizeof(Ctx)) == 0) {
       e = cudaGraphLaunch(g.exec, s);
       *launched = (e == cudaSuccess);
       return e;
@@ -852,7 +936,7 @@ cudaError_t launch_step_graph(const Ctx &c, int core, const PcgPlan &plan, int s
     cudaGraphExecDestroy(g_graphs.front().exec);
     g_graphs.erase(g_graphs.begin());
   }
-  g_graphs.push_back(GraphEntry{dev, core, c, exec});
+  g_graphs.push_back(GraphEntry{dev, core, sub_blocks, c, exec});
   e = cudaGraphLaunch(exec, s);
   *launched = (e == cudaSuccess);
   return e;
@@ -872,7 +956,7 @@ npom_status run_steps(const npom_params *p, float *const *fields, const npom_wor
     if (plan_pcg(c, &plan) != cudaSuccess) return NPOM_ERR_CUDA;
     launch_cells<XP_COEF>(c, s);
   } else {
-    if (coop_blocks((const void *)k_subcycle, (size_t)c.im * c.jm, &sub_blocks) != cudaSuccess) return NPOM_ERR_CUDA;
+    if (plan_subcycle(c, &sub_blocks) != cudaSuccess) return NPOM_ERR_CUDA;
   }
   const bool graphs = graphs_enabled();
   for (int n = 0; n < clk->nsteps; ++n) {
@@ -1088,7 +1172,7 @@ npom_status npom_run_phase(const npom_params *p, float *const *fields, const npo
         }
       } else {
         int blocks = 0;
-        e = coop_blocks((const void *)k_subcycle, (size_t)c.im * c.jm, &blocks);
+        e = plan_subcycle(c, &blocks);
         if (e == cudaSuccess) e = run_subcycle(c, blocks, s);
       }
       break;

@@ -161,3 +161,35 @@ def test_flux_tiles_equal_point_kernel(monkeypatch, case, phase, env, fields):
         outs.append({n: getattr(c, n).cpu().numpy() for n in fields + ("u", "el")})
     for n in outs[0]:
         assert np.array_equal(outs[0][n], outs[1][n]), n
+
+
+@pytest.mark.parametrize("case", ["gyre", "coastal"])
+def test_cluster_subcycle_equals_grid_subcycle(monkeypatch, case):
+    """On small grids the explicit external subcycle runs on one thread-block
+    cluster with the hardware cluster barrier; it writes bitwise what the
+    grid-barrier form writes, for the phase alone and over whole steps."""
+    from neuralpom_b200 import _abi, cases, resolve_core_class
+    if case == "gyre":
+        A, Sc = cases.double_gyre(37, 45, "explicit")
+    else:
+        A, Sc = cases.coastal_tide(60, 52)
+    Sc = dict(Sc)
+    Sc.update(time=0.25, time0=0.25)
+    lib = _lib()
+    stream = torch.cuda.current_stream()
+    names = ("el", "elb", "elf", "ua", "uab", "uaf", "va", "vab", "vaf", "egf", "utf", "vtf", "d", "etf")
+    outs = []
+    for form in ("grid", "cluster"):
+        monkeypatch.setenv("NPOM_SUBCYCLE", form)
+        c = resolve_core_class("explicit").from_state(A, Sc, device="cuda")
+        c.launch_steps(2, 0.25, 1, stream)
+        p, fa, ws = c.params(), c._fields(), c._workspace()
+        _abi.check(lib.npom_run_phase(ctypes.byref(p), ctypes.byref(fa), ctypes.byref(ws["struct"]), 3, 1.0,
+                                      ctypes.c_void_p(stream.cuda_stream)), "phase")
+        c.launch_steps(4, 0.25, 1, stream)
+        torch.cuda.synchronize()
+        bits, _ = c.read_status(1)
+        assert bits == 0
+        outs.append({n: getattr(c, n).cpu().numpy() for n in names + ("u", "v", "t")})
+    for n in outs[0]:
+        assert np.array_equal(outs[0][n], outs[1][n]), n
