@@ -236,6 +236,35 @@ npom_status npom_pcg_solve_static(const npom_params *p, float *const *fields,
                                   int *iters_out, unsigned int *status_out,
                                   void *stream);
 
+/* ------------------------------------------------------------------ */
+/* Adjoint of one explicit internal step (reverse mode).               */
+/* The reference differentiates its step with torch autograd           */
+/* (explicit/time_loop.py:20-709 under SparsePhysics.advance with      */
+/* differentiable=True, sparse_physics.py:91-149); this is the         */
+/* hand-written vector-Jacobian product of the same step.              */
+/* ------------------------------------------------------------------ */
+typedef struct npom_adjoint_ws {
+  float *lam[NPOM_NFIELDS];  /* one array per field, sized like it      */
+  float *save;               /* >= npom_adjoint_save_floats(p) floats   */
+  size_t save_floats;        /* capacity of save                        */
+} npom_adjoint_ws;
+
+/* Size of the per-step save area (floats) for these settings. */
+size_t npom_adjoint_save_floats(const npom_params *p);
+
+/* Differentiates the internal step clk->first_iint (clk->nsteps must be
+ * 1).  fields: the state at the START of that step (a checkpoint the
+ * caller kept); it is used as scratch and holds the start state again on
+ * return, apart from the zero surface-forcing fields.  grads[f]: on entry
+ * the cotangent of field f after the step, on exit the cotangent of f
+ * before it (vector-Jacobian product, accumulated in place).  Geometry,
+ * forcing and open-boundary arrays are constants.  Supported settings:
+ * explicit core, mode 3, nadv 1, nbct/nbcs 1 or 3; else NPOM_ERR_ARG. */
+npom_status npom_step_explicit_adjoint(const npom_params *p, float *const *fields,
+                                       const npom_workspace *ws,
+                                       const npom_clock *clk, float *const *grads,
+                                       const npom_adjoint_ws *aws, void *stream);
+
 /* Reads (and with clear != 0 zeroes) the device status word; blocks on
  * the stream. */
 npom_status npom_status_read(const npom_workspace *ws, int clear,

@@ -1,0 +1,181 @@
+// npom_adjoint_launch.cuh -- kernels and host driver of the explicit-core
+// step adjoint (included by npom_kernels.cu, which provides the forward
+// launchers).  One call differentiates one internal step: it recomputes the
+// step phase by phase from the checkpointed state, saving every field a
+// phase overwrites, then walks the phases backwards: restore the phase's
+// inputs, move the cotangents of what it wrote, run its adjoint.
+
+// Forward of one external-substep phase, one launch per phase (the fused
+// subcycle kernel computes the same values; this form leaves a point to
+// save the state between phases).
+__global__ void __launch_bounds__(kThreads) k_ext_fwd(Ctx c, int phase, int iext, int adv) {
+  const int n = c.im * c.jm;
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int i = q / c.jm, j = q % c.jm;
+  if (phase == AP_E1) ext_phase1_cell(c, i, j, adv != 0);
+  else if (phase == AP_E2) (void)ext_phase2_cell(c, i, j, iext);
+  else ext_phase3_cell(c, i, j, iext);
+}
+
+template <int PH>
+__global__ void __launch_bounds__(kThreads) k_adj_points(Ctx c, Adj a) {
+  const size_t n = (size_t)c.im * c.jm * c.kb;
+  size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int k = (int)(p % c.kb);
+  const size_t col = p / c.kb;
+  const int j = (int)(col % c.jm), i = (int)(col / c.jm);
+  if (PH == AP_A1) phase_a1_point_adj(c, a, i, j, k);
+  else if (PH == AP_B2B) phase_b2b_point_adj(c, a, i, j, k);
+  else if (PH == AP_B4) phase_b4_point_adj(c, a, i, j, k);
+  else if (PH == AP_B5) phase_b5_point_adj(c, a, i, j, k);
+  else if (PH == AP_B7) phase_b7_point_adj(c, a, i, j, k);
+}
+
+template <int PH>
+__global__ void __launch_bounds__(128) k_adj_cols(Ctx c, Adj a) {
+  const int n = c.im * c.jm;
+  int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= n) return;
+  const int j = col % c.jm, i = col / c.jm;
+  if (PH == AP_A2) phase_a2_column_adj(c, a, i, j);
+  else if (PH == AP_B1) phase_b1_column_adj(c, a, i, j);
+  else if (PH == AP_B2A) phase_b2a_column_adj(c, a, i, j);
+  else if (PH == AP_B3) phase_b3_column_adj(c, a, i, j);
+  else if (PH == AP_B6) phase_b6_column_adj(c, a, i, j);
+  else if (PH == AP_B8) phase_b8_column_adj(c, a, i, j);
+  else if (PH == AP_B9) phase_b9_column_adj(c, a, i, j);
+}
+
+__global__ void __launch_bounds__(kThreads) k_adj_cells(Ctx c, Adj a, int phase, int iext, int adv) {
+  const int n = c.im * c.jm;
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int i = q / c.jm, j = q % c.jm;
+  if (phase == AP_A3) phase_a3_cell_adj(c, a, i, j);
+  else if (phase == AP_E1) ext_phase1_cell_adj(c, a, i, j, adv != 0);
+  else if (phase == AP_E2) ext_phase2_cell_adj(c, a, i, j, iext);
+  else ext_phase3_cell_adj(c, a, i, j, iext);
+}
+
+// save[off_e ...] = F[fld_e] for every field e of a phase (blockIdx.y = e)
+__global__ void k_save_fields(Ctx c, AdjPhaseRec r, float *save) {
+  const int e = blockIdx.y;
+  if (e >= r.n) return;
+  const int f = r.fld[e];
+  const size_t n = adj_field_len(c, f);
+  const float *src = c.F[f];
+  float *dst = save + r.off[e];
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
+    dst[q] = src[q];
+}
+
+// F[fld_e] = save; and for moved fields L = G, G = 0
+__global__ void k_restore_move(Ctx c, Adj a, AdjPhaseRec r, const float *save) {
+  const int e = blockIdx.y;
+  if (e >= r.n) return;
+  const int f = r.fld[e];
+  const size_t n = adj_field_len(c, f);
+  const float *src = save + r.off[e];
+  float *dst = c.F[f];
+  const bool mv = r.move[e] != 0;
+  float *g = a.G[f], *l = a.L[f];
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    dst[q] = src[q];
+    if (mv) {
+      l[q] = g[q];
+      g[q] = 0.0f;
+    }
+  }
+}
+
+dim3 field_list_grid(const Ctx &c, const AdjPhaseRec &r) {
+  size_t n = 0;
+  for (int e = 0; e < r.n; ++e) n = std::max(n, adj_field_len(c, r.fld[e]));
+  const size_t blocks = std::min<size_t>((n + kThreads - 1) / kThreads, 4 * 148);
+  return dim3((unsigned)std::max<size_t>(blocks, 1), (unsigned)std::max(r.n, 1));
+}
+
+void launch_fwd_phase(const Ctx &c, const AdjPhaseRec &r, cudaStream_t s) {
+  switch (r.phase) {
+    case AP_A1: launch_a1(c, s); break;
+    case AP_A2: launch_cols<CP_A2>(c, s); break;
+    case AP_A3: launch_cells<XP_A3>(c, s); break;
+    case AP_E1:
+    case AP_E2:
+    case AP_E3: {
+      const int n = c.im * c.jm;
+      k_ext_fwd<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(c, r.phase, r.iext, r.adv);
+      break;
+    }
+    case AP_B1: launch_cols<CP_B1>(c, s); break;
+    case AP_B2A: launch_cols<CP_B2A>(c, s); break;
+    case AP_B2B: launch_points<PP_B2B>(c, s); break;
+    case AP_B3: launch_cols<CP_B3>(c, s); break;
+    case AP_B4: launch_points<PP_B4>(c, s); break;
+    case AP_B5: launch_b5(c, s); break;
+    case AP_B6: launch_cols<CP_B6>(c, s); break;
+    case AP_B7: launch_points<PP_B7>(c, s); break;
+    case AP_B8: launch_cols<CP_B8>(c, s); break;
+    case AP_B9: launch_cols<CP_B9>(c, s); break;
+  }
+}
+
+void launch_adj_phase(const Ctx &c, const Adj &a, const AdjPhaseRec &r, cudaStream_t s) {
+  const size_t np = (size_t)c.im * c.jm * c.kb;
+  const int ncol = c.im * c.jm;
+  const unsigned gp = (unsigned)((np + kThreads - 1) / kThreads), gx = (unsigned)((ncol + kThreads - 1) / kThreads);
+  const unsigned gc = (unsigned)((ncol + 127) / 128);
+  switch (r.phase) {
+    case AP_A1: k_adj_points<AP_A1><<<gp, kThreads, 0, s>>>(c, a); break;
+    case AP_A2: k_adj_cols<AP_A2><<<gc, 128, 0, s>>>(c, a); break;
+    case AP_A3:
+    case AP_E1:
+    case AP_E2:
+    case AP_E3: k_adj_cells<<<gx, kThreads, 0, s>>>(c, a, r.phase, r.iext, r.adv); break;
+    case AP_B1: k_adj_cols<AP_B1><<<gc, 128, 0, s>>>(c, a); break;
+    case AP_B2A: k_adj_cols<AP_B2A><<<gc, 128, 0, s>>>(c, a); break;
+    case AP_B2B: k_adj_points<AP_B2B><<<gp, kThreads, 0, s>>>(c, a); break;
+    case AP_B3: k_adj_cols<AP_B3><<<gc, 128, 0, s>>>(c, a); break;
+    case AP_B4: k_adj_points<AP_B4><<<gp, kThreads, 0, s>>>(c, a); break;
+    case AP_B5: k_adj_points<AP_B5><<<gp, kThreads, 0, s>>>(c, a); break;
+    case AP_B6: k_adj_cols<AP_B6><<<gc, 128, 0, s>>>(c, a); break;
+    case AP_B7: k_adj_points<AP_B7><<<gp, kThreads, 0, s>>>(c, a); break;
+    case AP_B8: k_adj_cols<AP_B8><<<gc, 128, 0, s>>>(c, a); break;
+    case AP_B9: k_adj_cols<AP_B9><<<gc, 128, 0, s>>>(c, a); break;
+  }
+}
+
+npom_status run_explicit_adjoint(const npom_params *p, float *const *fields, const npom_workspace *ws,
+                                 const npom_clock *clk, float *const *grads, const npom_adjoint_ws *aws,
+                                 cudaStream_t s) {
+  if (!check_args_dev(p, fields, ws) || !clk || clk->nsteps != 1 || !grads || !aws || !aws->save) return NPOM_ERR_ARG;
+  if (!adj_supported(p) || p->isplit > 4096) return NPOM_ERR_ARG;
+  for (int f = 0; f < NPOM_NFIELDS; ++f)
+    if (!grads[f] || !aws->lam[f]) return NPOM_ERR_ARG;
+  Ctx c = make_ctx(p, fields, ws);
+  c.coh = 0;
+  const int iint = clk->first_iint;
+  const double time = p->dti * iint * 1.0 / 86400.0 + clk->time0;
+  c.ramp = ramp_of(p, time);
+  c.do_internal = (iint != 1 || clk->time0 != 0.0) ? 1 : 0;
+  Adj a;
+  for (int f = 0; f < NPOM_NFIELDS; ++f) {
+    a.G[f] = grads[f];
+    a.L[f] = aws->lam[f];
+  }
+  std::vector<AdjPhaseRec> plan((size_t)(16 + 3 * p->isplit));
+  size_t need = 0;
+  const int np = adj_step_plan(c, plan.data(), (int)plan.size(), &need);
+  if (need > aws->save_floats) return NPOM_ERR_ARG;
+  for (int q = 0; q < np; ++q) {
+    k_save_fields<<<field_list_grid(c, plan[q]), kThreads, 0, s>>>(c, plan[q], aws->save);
+    launch_fwd_phase(c, plan[q], s);
+  }
+  for (int q = np - 1; q >= 0; --q) {
+    k_restore_move<<<field_list_grid(c, plan[q]), kThreads, 0, s>>>(c, a, plan[q], aws->save);
+    launch_adj_phase(c, a, plan[q], s);
+  }
+  return cudaGetLastError() == cudaSuccess ? NPOM_OK : NPOM_ERR_CUDA;
+}

@@ -27,6 +27,7 @@
 #include "npom_host.cuh"
 #include "npom_pcg_cluster.cuh"
 #include "npom_lanes.cuh"
+#include "npom_adjoint.cuh"
 
 using namespace npom;
 
@@ -871,6 +872,8 @@ cudaError_t enqueue_step(const Ctx &c, int core, const PcgPlan &plan, int sub_bl
   return cudaGetLastError();
 }
 
+#include "npom_adjoint_launch.cuh"
+
 // CUDA graphs of one internal step, keyed by the launch context (pointers,
 // settings, ramp, do_internal) and device.  Steps with ramp < 1 (the first
 // inertial period from rest) launch directly; every other step replays a
@@ -1147,6 +1150,28 @@ npom_status npom_step_explicit(const npom_params *p, float *const *fields, const
 npom_status npom_step_implicit(const npom_params *p, float *const *fields, const npom_workspace *ws,
                                const npom_clock *clk, void *stream) {
   return run_steps(p, fields, ws, clk, stream, NPOM_CORE_IMPLICIT);
+}
+
+size_t npom_adjoint_save_floats(const npom_params *p) {
+  if (!p || p->im < 3 || p->jm < 3 || p->kb < 3 || p->isplit < 1 || p->isplit > 4096 || p->ispadv < 1) return 0;
+  Ctx c;
+  std::memset(&c, 0, sizeof(c));
+  c.im = p->im;
+  c.jm = p->jm;
+  c.kb = p->kb;
+  c.k.isplit = p->isplit;
+  c.k.ispadv = p->ispadv;
+  c.do_internal = 1;
+  std::vector<AdjPhaseRec> plan((size_t)(16 + 3 * p->isplit));
+  size_t need = 0;
+  adj_step_plan(c, plan.data(), (int)plan.size(), &need);
+  return need;
+}
+
+npom_status npom_step_explicit_adjoint(const npom_params *p, float *const *fields, const npom_workspace *ws,
+                                       const npom_clock *clk, float *const *grads, const npom_adjoint_ws *aws,
+                                       void *stream) {
+  return run_explicit_adjoint(p, fields, ws, clk, grads, aws, (cudaStream_t)stream);
 }
 
 npom_status npom_run_phase(const npom_params *p, float *const *fields, const npom_workspace *ws, int phase,

@@ -10,7 +10,10 @@
 #include <cmath>
 #include <cstring>
 
+#include <vector>
+
 #include "../../neuralpom_b200/csrc/npom_host.cuh"
+#include "../../neuralpom_b200/csrc/npom_adjoint.cuh"
 
 using namespace npom;
 
@@ -197,9 +200,108 @@ void run_phase(const Ctx &c, const npom_params *p, int phase) {
   }
 }
 
+void fwd_plan_phase(const Ctx &c, const AdjPhaseRec &r) {
+  switch (r.phase) {
+    case AP_A1: a1(c); break;
+    case AP_A2: each_cell(c, [&](int i, int j) { phase_a2_column(c, i, j); }); break;
+    case AP_A3: each_cell(c, [&](int i, int j) { phase_a3_cell(c, i, j); }); break;
+    case AP_E1: each_cell(c, [&](int i, int j) { ext_phase1_cell(c, i, j, r.adv != 0); }); break;
+    case AP_E2: each_cell(c, [&](int i, int j) { (void)ext_phase2_cell(c, i, j, r.iext); }); break;
+    case AP_E3: each_cell(c, [&](int i, int j) { ext_phase3_cell(c, i, j, r.iext); }); break;
+    case AP_B1: each_cell(c, [&](int i, int j) { phase_b1_column(c, i, j); }); break;
+    case AP_B2A: each_cell(c, [&](int i, int j) { phase_b2a_column(c, i, j); }); break;
+    case AP_B2B: each_point(c, [&](int i, int j, int k) { phase_b2b_point(c, i, j, k); }); break;
+    case AP_B3: each_cell(c, [&](int i, int j) { phase_b3_column(c, i, j); }); break;
+    case AP_B4: each_point(c, [&](int i, int j, int k) { phase_b4_point(c, i, j, k); }); break;
+    case AP_B5: each_point(c, [&](int i, int j, int k) { phase_b5_point(c, i, j, k); }); break;
+    case AP_B6: each_cell(c, [&](int i, int j) { phase_b6_column(c, i, j); }); break;
+    case AP_B7: each_point(c, [&](int i, int j, int k) { phase_b7_point(c, i, j, k); }); break;
+    case AP_B8: each_cell(c, [&](int i, int j) { phase_b8_column(c, i, j); }); break;
+    case AP_B9: each_cell(c, [&](int i, int j) { phase_b9_column(c, i, j); }); break;
+  }
+}
+
+void adj_plan_phase(const Ctx &c, const Adj &a, const AdjPhaseRec &r) {
+  switch (r.phase) {
+    case AP_A1: each_point(c, [&](int i, int j, int k) { phase_a1_point_adj(c, a, i, j, k); }); break;
+    case AP_A2: each_cell(c, [&](int i, int j) { phase_a2_column_adj(c, a, i, j); }); break;
+    case AP_A3: each_cell(c, [&](int i, int j) { phase_a3_cell_adj(c, a, i, j); }); break;
+    case AP_E1: each_cell(c, [&](int i, int j) { ext_phase1_cell_adj(c, a, i, j, r.adv != 0); }); break;
+    case AP_E2: each_cell(c, [&](int i, int j) { ext_phase2_cell_adj(c, a, i, j, r.iext); }); break;
+    case AP_E3: each_cell(c, [&](int i, int j) { ext_phase3_cell_adj(c, a, i, j, r.iext); }); break;
+    case AP_B1: each_cell(c, [&](int i, int j) { phase_b1_column_adj(c, a, i, j); }); break;
+    case AP_B2A: each_cell(c, [&](int i, int j) { phase_b2a_column_adj(c, a, i, j); }); break;
+    case AP_B2B: each_point(c, [&](int i, int j, int k) { phase_b2b_point_adj(c, a, i, j, k); }); break;
+    case AP_B3: each_cell(c, [&](int i, int j) { phase_b3_column_adj(c, a, i, j); }); break;
+    case AP_B4: each_point(c, [&](int i, int j, int k) { phase_b4_point_adj(c, a, i, j, k); }); break;
+    case AP_B5: each_point(c, [&](int i, int j, int k) { phase_b5_point_adj(c, a, i, j, k); }); break;
+    case AP_B6: each_cell(c, [&](int i, int j) { phase_b6_column_adj(c, a, i, j); }); break;
+    case AP_B7: each_point(c, [&](int i, int j, int k) { phase_b7_point_adj(c, a, i, j, k); }); break;
+    case AP_B8: each_cell(c, [&](int i, int j) { phase_b8_column_adj(c, a, i, j); }); break;
+    case AP_B9: each_cell(c, [&](int i, int j) { phase_b9_column_adj(c, a, i, j); }); break;
+  }
+}
+
 }  // namespace
 
 extern "C" {
+
+// CPU emulation of npom_step_explicit_adjoint: same plan, same bodies.
+// stop_after >= 0 ends the reverse sweep after that many phases (tests of
+// single phases); -1 runs all of them.
+int emul_step_adjoint(const npom_params *p, float *const *fields, const npom_workspace *ws, const npom_clock *clk,
+                      float *const *grads, float *const *lam, float *save, size_t save_floats, int stop_after) {
+  if (!check_args(p, fields, ws) || !clk || clk->nsteps != 1 || !adj_supported(p)) return 1;
+  Ctx c = make_ctx(p, fields, ws);
+  const int iint = clk->first_iint;
+  const double time = p->dti * iint * 1.0 / 86400.0 + clk->time0;
+  c.ramp = ramp_of(p, time);
+  c.do_internal = (iint != 1 || clk->time0 != 0.0) ? 1 : 0;
+  Adj a;
+  for (int f = 0; f < NPOM_NFIELDS; ++f) {
+    a.G[f] = grads[f];
+    a.L[f] = lam[f];
+  }
+  std::vector<AdjPhaseRec> plan((size_t)(16 + 3 * p->isplit));
+  size_t need = 0;
+  const int np = adj_step_plan(c, plan.data(), (int)plan.size(), &need);
+  if (need > save_floats) return 2;
+  for (int q = 0; q < np; ++q) {
+    const AdjPhaseRec &r = plan[q];
+    for (int e = 0; e < r.n; ++e) std::memcpy(save + r.off[e], c.F[r.fld[e]], adj_field_len(c, r.fld[e]) * 4);
+    fwd_plan_phase(c, r);
+  }
+  int done = 0;
+  for (int q = np - 1; q >= 0; --q) {
+    if (stop_after >= 0 && done >= stop_after) break;
+    const AdjPhaseRec &r = plan[q];
+    for (int e = 0; e < r.n; ++e) {
+      const int f = r.fld[e];
+      const size_t n = adj_field_len(c, f);
+      std::memcpy(c.F[f], save + r.off[e], n * 4);
+      if (r.move[e]) {
+        std::memcpy(a.L[f], a.G[f], n * 4);
+        std::memset(a.G[f], 0, n * 4);
+      }
+    }
+    adj_plan_phase(c, a, r);
+    ++done;
+  }
+  return 0;
+}
+
+// the number of phases of one step and the save area they need
+int emul_adjoint_plan(const npom_params *p, int do_internal, size_t *save_floats) {
+  Ctx c;
+  std::memset(&c, 0, sizeof(c));
+  c.im = p->im;
+  c.jm = p->jm;
+  c.kb = p->kb;
+  c.k = make_consts(*p);
+  c.do_internal = do_internal;
+  std::vector<AdjPhaseRec> plan((size_t)(16 + 3 * p->isplit));
+  return adj_step_plan(c, plan.data(), (int)plan.size(), save_floats);
+}
 
 int emul_run_phase(const npom_params *p, float *const *fields, const npom_workspace *ws, int phase, double ramp) {
   if (!check_args(p, fields, ws)) return 1;

@@ -16,7 +16,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 SRC = os.path.join(ROOT, "tests", "emul", "npom_emul.cu")
 OUT = os.path.join(ROOT, "tests", "emul", "_build", "libnpom_emul.so")
 DEPS = [SRC] + [os.path.join(ROOT, "neuralpom_b200", "csrc", f) for f in
-                ("npom_ctx.cuh", "npom_phases_a.cuh", "npom_phases_ext.cuh", "npom_phases_int.cuh", "npom_host.cuh")]
+                ("npom_ctx.cuh", "npom_phases_a.cuh", "npom_phases_ext.cuh", "npom_phases_int.cuh", "npom_host.cuh",
+                 "npom_adjoint.cuh")]
 
 _LIB = None
 
@@ -42,6 +43,12 @@ def build_emul():
     lib.emul_run_phase.argtypes = [P(_abi.NpomParams), P(_abi.FieldArray), P(_abi.NpomWorkspace), ctypes.c_int,
                                    ctypes.c_double]
     lib.emul_steps.restype = ctypes.c_int
+    lib.emul_step_adjoint.restype = ctypes.c_int
+    lib.emul_step_adjoint.argtypes = [P(_abi.NpomParams), P(_abi.FieldArray), P(_abi.NpomWorkspace), P(_abi.NpomClock),
+                                      P(_abi.FieldArray), P(_abi.FieldArray), ctypes.c_void_p, ctypes.c_size_t,
+                                      ctypes.c_int]
+    lib.emul_adjoint_plan.restype = ctypes.c_int
+    lib.emul_adjoint_plan.argtypes = [P(_abi.NpomParams), ctypes.c_int, P(ctypes.c_size_t)]
     lib.emul_steps.argtypes = [P(_abi.NpomParams), P(_abi.FieldArray), P(_abi.NpomWorkspace), P(_abi.NpomClock)]
     _LIB = lib
     return lib
@@ -94,6 +101,28 @@ class EmulCore:
         assert rc == 0
         self.time = self.time + n * self.params.dti / 86400.0
         return list(self.cg_iters[:n])
+
+    def adjoint_step(self, grads, stop_after=-1):
+        """Vector-Jacobian product of one internal step from the current
+        state (which is restored afterwards): ``grads`` maps field names to
+        the cotangents after the step; returns the cotangents before it."""
+        from neuralpom_b200 import _abi
+        lib = build_emul()
+        need = ctypes.c_size_t(0)
+        lib.emul_adjoint_plan(ctypes.byref(self.params), 1, ctypes.byref(need))
+        save = np.zeros(max(int(need.value), 1), np.float32)
+        G = {n: np.zeros_like(self.F[n]) for n in _abi.FIELD_NAMES}
+        for n, g in grads.items():
+            G[n][...] = g
+        Lm = {n: np.zeros_like(self.F[n]) for n in _abi.FIELD_NAMES}
+        ga = _abi.FieldArray(*[G[n].ctypes.data for n in _abi.FIELD_NAMES])
+        la = _abi.FieldArray(*[Lm[n].ctypes.data for n in _abi.FIELD_NAMES])
+        clk = _abi.NpomClock(self.time, 1, 1)
+        rc = lib.emul_step_adjoint(ctypes.byref(self.params), ctypes.byref(self.fa), ctypes.byref(self.ws),
+                                   ctypes.byref(clk), ctypes.byref(ga), ctypes.byref(la), save.ctypes.data,
+                                   save.size, int(stop_after))
+        assert rc == 0, rc
+        return G
 
     def phase(self, ph, ramp=1.0):
         rc = build_emul().emul_run_phase(ctypes.byref(self.params), ctypes.byref(self.fa), ctypes.byref(self.ws),
