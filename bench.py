@@ -94,6 +94,7 @@ def parse():
     ap.add_argument("--members", type=int, default=8,
                     help="ensemble members advanced concurrently on one GPU for the 'ensemble' key (1 = skip)")
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference core on this GPU")
+    ap.add_argument("--no-fwd-adjoint", action="store_true", help="skip the forward+adjoint sample")
     return ap.parse_args()
 
 
@@ -328,6 +329,14 @@ def run_b200(args):
         cpu = reference_cpu_sample(A, Sc, internal_steps=args.ref_internal_steps, warm=1, reps=2,
                                    core_name=W["core"])
 
+    fa = None
+    if rank == 0 and ws_n == 1 and args.workload == "seamount" and not args.no_fwd_adjoint:
+        fa = fwd_adjoint_sample(args, dev)
+        if not args.no_ref_gpu:
+            fa["reference_gpu"] = reference_fwd_adjoint_sample(dev)
+        if not args.no_cpu_baseline:
+            fa["reference_cpu"] = reference_fwd_adjoint_sample("cpu", internal_steps=3)
+
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws_n, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -338,7 +347,8 @@ def run_b200(args):
                    "pcg_iterations_last_step": (its[-1] if its else None) if W["core"] != "explicit" else None,
                    "members": ws_n, "parallelism": f"ensemble x{ws_n}" if ws_n > 1 else "single member",
                    "l2": "flushed (256 MiB write) before every timed step"},
-        "roofline": roofline, "cpu_baseline": cpu, "reference_gpu": ref_gpu, "ensemble": ens, "e2e": e2e, "gpu_launches": launches,
+        "roofline": roofline, "cpu_baseline": cpu, "reference_gpu": ref_gpu, "ensemble": ens, "fwd_adjoint": fa, "e2e": e2e,
+        "gpu_launches": launches,
         "clocks": clk.summary(),
     }
     if rank == 0:
@@ -513,6 +523,162 @@ def end_to_end(core, A, Sc, args, stream, dev, pg, ws_n, nin):
 # ---------------------------------------------------------------------------
 # the reference's own implementation
 # ---------------------------------------------------------------------------
+
+# Forward+adjoint: the differentiation set-up of the Midtrain stage on the
+# explicit core (90x82x16 basin, dtI = 120 s, isplit = 20), three 1 h
+# intervals with an additive increment on T, S, u, v between them, loss =
+# MSE of u, v, T, S against a seeded target, gradient of every state field.
+FA_GRID = (90, 82, 16)
+FA_INTERVALS, FA_STEPS_PER_INTERVAL = 3, 30
+
+
+def midtrain_case(member=0):
+    """Seeded member: the explicit noise basin at 90x82x16 with the
+    dtE = 6 s, isplit = 20 clock; T/S perturbations from a Gaussian random
+    field (std 0.2 degC / 0.05 psu, correlation length 5 cells) and u/v
+    perturbations (std 0.05 m/s) on the wet faces; clock at 1 day."""
+    from scipy.ndimage import gaussian_filter
+    from neuralpom_b200 import cases
+    im, jm, kb = FA_GRID
+    A, Sc = cases.noise_basin(im, jm, kb=kb, dte=6.0, isplit=20, seed=member)
+    Sc = dict(Sc)
+    Sc.update(time=1.0, time0=1.0)
+    g = np.random.default_rng(100 + member)
+    shape = A["t"].shape
+
+    def grf(std):
+        n = gaussian_filter(g.standard_normal(shape), (5.0, 5.0, 0.0), mode="reflect")
+        return (n / n.std() * std).astype(np.float32)
+    fsm3 = A["fsm"][:, :, None]
+    pt, ps = grf(0.2) * fsm3, grf(0.05) * fsm3
+    pt[:, :, -1] = ps[:, :, -1] = 0.0
+    A["t"] = A["t"] + pt
+    A["tb"] = A["tb"] + pt
+    A["s"] = A["s"] + ps
+    A["sb"] = A["sb"] + ps
+    for f, m in (("u", "dum"), ("v", "dvm")):
+        p = (0.05 * g.standard_normal(shape) * A[m][:, :, None]).astype(np.float32)
+        p[:, :, -1] = 0.0
+        A[f] = A[f] + p
+        A[f + "b"] = A[f + "b"] + p
+    return A, Sc
+
+
+def _fa_targets(A, seed, dev=None):
+    g = np.random.default_rng(seed)
+    out = {}
+    for f, sd, m in (("t", 0.1, "fsm"), ("s", 0.02, "fsm"), ("u", 0.02, "dum"), ("v", 0.02, "dvm")):
+        out[f] = (A[f] + sd * g.standard_normal(A[f].shape) * A[m][:, :, None]).astype(np.float32)
+    incs = {}
+    for f, sd, m in (("t", 1e-3, "fsm"), ("s", 2e-4, "fsm"), ("u", 1e-4, "dum"), ("v", 1e-4, "dvm")):
+        incs[f] = (sd * g.standard_normal(A[f].shape) * A[m][:, :, None]).astype(np.float32)
+    return out, incs
+
+
+def fwd_adjoint_sample(args, dev, reps=3):
+    """Forward+adjoint through the drop-in API under torch autograd: every
+    state field a leaf, three differentiable run_time_loop() calls of 30
+    internal steps with the increment between them, the loss, backward().
+    Timed with CUDA events around forward and backward (checkpoint per
+    internal step, recomputation and the hand-written step adjoint)."""
+    import torch
+    from neuralpom_b200 import _abi, resolve_core_class
+    A, Sc = midtrain_case(0)
+    core = resolve_core_class("explicit").from_state(A, Sc, device=dev)
+    tgt, incs = _fa_targets(A, 7)
+    tgt = {f: torch.from_numpy(v).to(dev) for f, v in tgt.items()}
+    incs = {f: torch.from_numpy(v).to(dev) for f, v in incs.items()}
+    start = {f: getattr(core, f).detach().clone() for f in _abi.FIELD_NAMES}
+    dti = float(core.dti)
+    stream = torch.cuda.current_stream(dev)
+
+    def prepare():
+        for f in _abi.FIELD_NAMES:
+            setattr(core, f, start[f].clone())
+        leaves = []
+        for f in _abi.ADJ_STATE_FIELDS:
+            t = getattr(core, f).requires_grad_(True)
+            leaves.append(t)
+        return leaves
+
+    def fwd_bwd():
+        t0 = float(Sc["time"])
+        for k in range(FA_INTERVALS):
+            core.time0 = t0 + k * FA_STEPS_PER_INTERVAL * dti / 86400.0
+            core.iend = FA_STEPS_PER_INTERVAL
+            core.run_time_loop()
+            if k < FA_INTERVALS - 1:
+                for f, d in incs.items():
+                    setattr(core, f, getattr(core, f) + d)
+        loss = sum(((getattr(core, f) - tgt[f]) ** 2).mean() for f in tgt)
+        loss.backward()
+        return loss
+
+    for _ in range(max(args.warmup, 1)):
+        prepare()
+        fwd_bwd()
+    torch.cuda.synchronize(dev)
+    ms = []
+    for _ in range(reps):
+        leaves = prepare()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fwd_bwd()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms.append(e0.elapsed_time(e1))
+        assert all(t.grad is not None for t in leaves[:12])
+    nint = FA_INTERVALS * FA_STEPS_PER_INTERVAL
+    days = nint * dti / 86400.0
+    best = statistics.median(ms)
+    return {"value": days / (best / 1000.0), "unit": UNIT, "ms_per_sample": best,
+            "workload": f"explicit core, {FA_GRID[0]}x{FA_GRID[1]}x{FA_GRID[2]} noise basin (dtE=6 s, isplit=20, "
+                        f"dtI=120 s), T/S/u/v-perturbed member; {FA_INTERVALS} x 1 h intervals ({nint} internal "
+                        "steps) with an additive T/S/u/v increment between them, MSE(u,v,T,S) loss, backward to "
+                        "every state field; checkpoint per internal step, hand-written CUDA step adjoint",
+            "timing": f"median of {reps} samples, CUDA events around forward+backward (L2 not flushed: the "
+                      "90x82x16 state fits in L2)"}
+
+
+def reference_fwd_adjoint_sample(device, internal_steps=6):
+    """The reference explicit core under torch autograd
+    (SparsePhysics.advance(differentiable=True) + backward) on the same
+    member: ``internal_steps`` steps, wall clock."""
+    import torch
+    A, Sc = midtrain_case(0)
+    core, rh = reference_core(A, Sc, device, "explicit")
+    tgt, _ = _fa_targets(A, 7)
+    from neuralpom_b200 import _abi
+    names = [k for k in _abi.ADJ_STATE_FIELDS if torch.is_tensor(getattr(core, k, None))]
+
+    def once(n):
+        leaves = []
+        for k in names:
+            t = getattr(core, k).detach().clone().requires_grad_(True)
+            setattr(core, k, t)
+            leaves.append(t)
+        rh.advance(core, "explicit", n, differentiable=True, device=device)
+        loss = sum(((getattr(core, f) - torch.from_numpy(v).to(device)) ** 2).mean() for f, v in tgt.items())
+        loss.backward()
+        for k, v in list(vars(core).items()):
+            if torch.is_tensor(v):
+                setattr(core, k, v.detach())
+    once(1)
+    if device != "cpu":
+        torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    once(internal_steps)
+    if device != "cpu":
+        torch.cuda.synchronize()
+    sec = time.perf_counter() - t0
+    days = internal_steps * float(core.dti) / 86400.0
+    return {"value": days / sec, "unit": UNIT, "device": str(device),
+            "threads": (os.cpu_count() or 1) if device == "cpu" else None,
+            "sample": f"{internal_steps} internal steps forward+backward of the {_basin_name(A)} (reference "
+                      "explicit core, torch autograd through SparsePhysics.advance(differentiable=True), after a "
+                      "1-step warm-up; wall clock)"}
+
 
 def reference_core(A, Sc, device="cpu", core_name="implicit_p0_fixed"):
     """Reference core (baseline/_ref install, else the source tree) loaded

@@ -88,6 +88,22 @@ class NpomClock(ctypes.Structure):
 
 FieldArray = ctypes.c_void_p * len(FIELD_NAMES)
 
+
+class NpomAdjointWs(ctypes.Structure):
+    _fields_ = [("lam", ctypes.c_void_p * len(FIELD_NAMES)), ("save", ctypes.c_void_p),
+                ("save_floats", ctypes.c_size_t)]
+
+
+# State fields of the explicit core that carry a cotangent through a step:
+# everything the step reads or writes apart from geometry, forcing and
+# open-boundary arrays (explicit/base.py:129-195).
+ADJ_STATE_FIELDS = (
+    "u", "ub", "uf", "v", "vb", "vf", "w", "t", "tb", "s", "sb", "rho", "q2", "q2b", "q2l", "q2lb", "km", "kh",
+    "kq", "l", "aam", "advx", "advy", "drhox", "drhoy", "curv", "el", "elb", "elf", "et", "etb", "etf", "d", "dt",
+    "ua", "uab", "uaf", "va", "vab", "vaf", "utf", "utb", "vtf", "vtb", "egf", "egb", "adx2d", "ady2d", "drx2d",
+    "dry2d", "aam2d", "advua", "advva", "fluxua", "fluxva", "wubot", "wvbot", "tps",
+)
+
 STATUS_NAMES = {0: "NPOM_OK", 1: "NPOM_ERR_ARG", 2: "NPOM_ERR_CUDA", 3: "NPOM_ERR_DEVICE", 4: "NPOM_ERR_TOO_LARGE"}
 STATIC_MAX_CELLS = 32768
 
@@ -138,6 +154,11 @@ def load_library():
     lib.npom_proft.restype = i32
     lib.npom_proft.argtypes = [i32, i32, vp, vp, vp, i32, vp, vp, dbl, vp, vp, vp, i32, vp, dbl, vp, vp, vp, vp]
     lib.npom_status_read.restype = i32
+    lib.npom_adjoint_save_floats.restype = ctypes.c_size_t
+    lib.npom_adjoint_save_floats.argtypes = [P(NpomParams)]
+    lib.npom_step_explicit_adjoint.restype = i32
+    lib.npom_step_explicit_adjoint.argtypes = [P(NpomParams), P(FieldArray), P(NpomWorkspace), P(NpomClock),
+                                               P(FieldArray), P(NpomAdjointWs), vp]
     lib.npom_status_read.argtypes = [P(NpomWorkspace), i32, P(ctypes.c_uint), vp]
     check_layout(lib)
     _LIB = lib

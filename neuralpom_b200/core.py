@@ -182,13 +182,24 @@ class B200Core:
     def run_time_loop(self):
         """Advance ``iend`` internal steps from ``time0`` (reference
         run_time_loop semantics); raises FloatingPointError when the
-        barotropic velocity exceeds vmaxl or the elevation is not finite."""
+        barotropic velocity exceeds vmaxl or the elevation is not finite.
+        When grad mode is on and a state tensor requires grad, the advance
+        is one differentiable node (explicit core) whose backward is the
+        hand-written step adjoint; the state attributes are rebound to its
+        outputs, as the reference's autograd path rebinds them."""
         nsteps = int(self.iend)
         if nsteps < 0:
             raise ValueError("iend must be non-negative")
-        with torch.no_grad():
-            self.launch_steps(nsteps, float(self.time0))
-        bits, its = self.read_status(nsteps)
+        if self._differentiable_call():
+            outs = _ExplicitStepsFunction.apply(self, nsteps, float(self.time0),
+                                                *[getattr(self, f) for f in _abi.ADJ_STATE_FIELDS])
+            for f, o in zip(_abi.ADJ_STATE_FIELDS, outs):
+                setattr(self, f, o)
+            bits, its = self.read_status(nsteps)
+        else:
+            with torch.no_grad():
+                self.launch_steps(nsteps, float(self.time0))
+            bits, its = self.read_status(nsteps)
         self.iint = nsteps
         self.time = self.dti * nsteps * 1.0 / 86400.0 + self.time0
         if self.lramp:
@@ -199,6 +210,16 @@ class B200Core:
         if self.core_name != "explicit":
             self._eta_solver_iteration_history.extend(its)
         self._raise_for(bits)
+
+    def _differentiable_call(self):
+        if not torch.is_grad_enabled():
+            return False
+        needs = any(torch.is_tensor(getattr(self, f)) and getattr(self, f).requires_grad
+                    for f in _abi.FIELD_NAMES)
+        if needs and self.core_name != "explicit":
+            raise NotImplementedError("the differentiable step is provided for the explicit core; the implicit "
+                                      "core differentiates its free-surface solve (solve_implicit_eta_cg)")
+        return needs
 
     def _raise_for(self, bits):
         if bits & _abi.DEV_TIMEOUT:
@@ -211,6 +232,93 @@ class B200Core:
 class ExplicitCore(B200Core):
     """Explicit mode-split core (reference ``cores/explicit``)."""
     core_name = "explicit"
+
+
+class _StateBuffer:
+    """One flat float32 device buffer holding the given fields back to back,
+    with a view per field (a checkpoint of them is one copy)."""
+
+    def __init__(self, names, im, jm, kb, device):
+        self.names = tuple(names)
+        self.shapes = [_abi.field_shape(n, im, jm, kb) for n in self.names]
+        sizes = [int(np.prod(s)) for s in self.shapes]
+        self.flat = torch.zeros(sum(sizes), dtype=torch.float32, device=device)
+        self.views = {}
+        off = 0
+        for n, shp, sz in zip(self.names, self.shapes, sizes):
+            self.views[n] = self.flat[off:off + sz].view(shp)
+            off += sz
+
+
+class _ExplicitStepsFunction(torch.autograd.Function):
+    """``nsteps`` explicit internal steps as one autograd node: inputs and
+    outputs are the state fields ``_abi.ADJ_STATE_FIELDS``.  The forward
+    keeps one checkpoint of the state per step; the backward recomputes
+    each step from its checkpoint and runs ``npom_step_explicit_adjoint``
+    in reverse step order (per-internal-step checkpointing with
+    recomputation, like the reference's ``_checkpoint_chunk``,
+    sparse_physics.py:108-149, under torch autograd)."""
+
+    @staticmethod
+    def forward(ctx, core, nsteps, time0, *state):
+        dev = core.device
+        im, jm, kb = core.im, core.jm, core.kb
+        dyn = _StateBuffer(_abi.ADJ_STATE_FIELDS, im, jm, kb, dev)
+        for n, t in zip(_abi.ADJ_STATE_FIELDS, state):
+            dyn.views[n].copy_(t.detach().reshape(dyn.views[n].shape))
+            setattr(core, n, dyn.views[n])
+        ckpt = torch.empty((max(nsteps, 1), dyn.flat.numel()), dtype=torch.float32, device=dev)
+        for n in range(nsteps):
+            ckpt[n].copy_(dyn.flat)
+            core.launch_steps(1, time0, first_iint=n + 1)
+        ctx.core, ctx.nsteps, ctx.time0 = core, nsteps, time0
+        ctx.save_for_backward(ckpt)
+        outs = tuple(dyn.views[n].clone() for n in _abi.ADJ_STATE_FIELDS)
+        for n, o in zip(_abi.ADJ_STATE_FIELDS, outs):
+            setattr(core, n, o)
+        return outs
+
+    @staticmethod
+    def backward(ctx, *grads):
+        (ckpt,) = ctx.saved_tensors
+        core = ctx.core
+        lib = _abi.load_library()
+        dev = core.device
+        im, jm, kb = core.im, core.jm, core.kb
+        names = _abi.FIELD_NAMES
+        # the working state: every field, the dynamic ones reloaded from
+        # each step's checkpoint
+        work = _StateBuffer(_abi.ADJ_STATE_FIELDS + tuple(n for n in names if n not in _abi.ADJ_STATE_FIELDS),
+                            im, jm, kb, dev)
+        for n in names:
+            if n not in _abi.ADJ_STATE_FIELDS:
+                work.views[n].copy_(getattr(core, n).detach().reshape(work.views[n].shape))
+        ndyn = ckpt.shape[1]
+        G = _StateBuffer(names, im, jm, kb, dev)
+        Lm = _StateBuffer(names, im, jm, kb, dev)
+        for n, g in zip(_abi.ADJ_STATE_FIELDS, grads):
+            if g is not None:
+                G.views[n].copy_(g.reshape(G.views[n].shape))
+        p = core.params()
+        save = torch.empty(max(int(lib.npom_adjoint_save_floats(ctypes.byref(p))), 1), dtype=torch.float32,
+                           device=dev)
+        aws = _abi.NpomAdjointWs()
+        for i, n in enumerate(names):
+            aws.lam[i] = Lm.views[n].data_ptr()
+        aws.save = save.data_ptr()
+        aws.save_floats = save.numel()
+        fa = _abi.FieldArray(*[work.views[n].data_ptr() for n in names])
+        ga = _abi.FieldArray(*[G.views[n].data_ptr() for n in names])
+        ws = core._workspace()
+        st = torch.cuda.current_stream(dev)
+        for n in reversed(range(ctx.nsteps)):
+            work.flat[:ndyn].copy_(ckpt[n])
+            clk = _abi.NpomClock(float(ctx.time0), int(n + 1), 1)
+            _abi.check(lib.npom_step_explicit_adjoint(ctypes.byref(p), ctypes.byref(fa), ctypes.byref(ws["struct"]),
+                                                      ctypes.byref(clk), ctypes.byref(ga), ctypes.byref(aws),
+                                                      ctypes.c_void_p(st.cuda_stream)),
+                       "npom_step_explicit_adjoint")
+        return (None, None, None) + tuple(G.views[n].clone() for n in _abi.ADJ_STATE_FIELDS)
 
 
 class _EtaSolveFunction(torch.autograd.Function):

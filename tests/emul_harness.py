@@ -128,3 +128,21 @@ class EmulCore:
         rc = build_emul().emul_run_phase(ctypes.byref(self.params), ctypes.byref(self.fa), ctypes.byref(self.ws),
                                          ph, ramp)
         assert rc == 0
+
+
+def multi_step_adjoint(arrays, scalars, cot, nsteps):
+    """Reverse mode of ``nsteps`` emulated explicit steps with a checkpoint
+    per step: forward saving each step's start state, then the step
+    adjoints in reverse order.  Returns the cotangents of the start state."""
+    E = EmulCore(arrays, scalars, "explicit")
+    starts = []
+    for _ in range(nsteps):
+        starts.append(({n: v.copy() for n, v in E.F.items()}, E.time))
+        E.steps(1)
+    G = dict(cot)
+    for F0, t0 in reversed(starts):
+        for n, v in F0.items():
+            E.F[n][...] = v
+        E.time = t0
+        G = E.adjoint_step(G)
+    return G

@@ -3,7 +3,7 @@
 Run in a container that holds the reference sources (default
 ``/root/reference/src``, or ``NPOM_REFERENCE_SRC``)::
 
-    python tests/golden/make_golden.py [proft] [steps] [adjoint] [coastal]
+    python tests/golden/make_golden.py [proft] [steps] [adjoint] [coastal] [step_adjoint]
 
 Writes ``tests/golden/*.npz``.  Every file records the reference's own CPU
 float32 outputs on seeded inputs; nothing here is needed at test time except
@@ -182,7 +182,73 @@ def make_eta_adjoint_golden(im=20, jm=18, seed=21):
     print("wrote", path, os.path.getsize(path))
 
 
-def main(which=("proft", "steps", "adjoint", "coastal")):
+# State fields of the explicit core that carry a cotangent (everything the
+# step reads or writes apart from geometry, forcing and boundary arrays).
+ADJ_STATE_FIELDS = (
+    "u", "ub", "uf", "v", "vb", "vf", "w", "t", "tb", "s", "sb", "rho", "q2", "q2b", "q2l", "q2lb", "km", "kh",
+    "kq", "l", "aam", "advx", "advy", "drhox", "drhoy", "curv", "el", "elb", "elf", "et", "etb", "etf", "d", "dt",
+    "ua", "uab", "uaf", "va", "vab", "vaf", "utf", "utb", "vtf", "vtb", "egf", "egb", "adx2d", "ady2d", "drx2d",
+    "dry2d", "aam2d", "advua", "advva", "fluxua", "fluxva", "wubot", "wvbot", "tps",
+)
+ADJ_COT_FIELDS = ("u", "ub", "v", "vb", "t", "tb", "s", "sb", "el", "elb", "ua", "uab", "va", "vab", "q2", "q2l",
+                  "km", "kh", "et", "etb", "egb", "utb", "vtb", "wubot", "wvbot", "rho")
+
+
+def make_step_adjoint_golden(tag, core, steps=(1, 3), seed=0, cot_fields=ADJ_COT_FIELDS):
+    """Reverse mode of the reference's explicit step under torch autograd
+    (``SparsePhysics.advance(..., differentiable=True)``, sparse_physics.py:
+    91-149): seeded cotangents on ``cot_fields`` after ``n`` steps,
+    J = sum(cot * state), and dJ/d(start state) for every state field."""
+    import torch
+    arrays, scalars = rh.extract_state(core)
+    im, jm = arrays["u"].shape[:2]
+    out = {f"in__{k}": v for k, v in arrays.items()}
+    for k, v in scalars.items():
+        out[f"scalar__{k}"] = np.asarray(v)
+    g = torch.Generator().manual_seed(seed)
+    cot = {f: torch.randn(arrays[f].shape, generator=g, dtype=torch.float32) for f in cot_fields}
+    for f, v in cot.items():
+        out[f"cot__{f}"] = v.numpy()
+    for n in steps:
+        c2 = rh.build_reference_core("explicit", im, jm)
+        rh.load_state(c2, arrays, scalars)
+        leaves = {}
+        for f in ADJ_STATE_FIELDS:
+            leaves[f] = getattr(c2, f).detach().clone().requires_grad_(True)
+            setattr(c2, f, leaves[f])
+        rh.advance(c2, "explicit", n, differentiable=True)
+        loss = sum((getattr(c2, f) * cot[f]).sum() for f in cot_fields)
+        loss.backward()
+        for f in ADJ_STATE_FIELDS:
+            gr = leaves[f].grad
+            if gr is not None and bool(torch.any(gr != 0)):
+                out[f"grad{n}__{f}"] = gr.numpy()
+    path = os.path.join(HERE, f"step_adjoint_{tag}_{im}x{jm}.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path))
+
+
+def make_step_adjoint_goldens():
+    core = perturbed_core("explicit", 12, 10, 31)
+    core.time0 = float(core.time)
+    make_step_adjoint_golden("explicit", core, steps=(1, 3), seed=32)
+    core = perturbed_core("explicit", 12, 10, 33)
+    core.time = core.time0 = 0.0
+    make_step_adjoint_golden("rest", core, steps=(1, 2), seed=34)
+    sys.path.insert(0, ROOT)
+    from neuralpom_b200 import cases
+    A, Sc = cases.coastal_tide(16, 14, seed=4)
+    Sc = dict(Sc)
+    Sc.update(time=0.25, time0=0.25)
+    core = rh.build_reference_core("explicit", 16, 14)
+    rh.load_state(core, A, Sc)
+    rh.advance(core, "explicit", 3)
+    core.time0 = float(core.time)
+    make_step_adjoint_golden("coastal", core, steps=(1,), seed=35,
+                             cot_fields=("u", "v", "t", "s", "el", "ua", "va", "q2", "km"))
+
+
+def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint")):
     src = rh.default_reference_path()
     if src is None:
         raise SystemExit("reference sources not found; set NPOM_REFERENCE_SRC")
@@ -199,7 +265,9 @@ def main(which=("proft", "steps", "adjoint", "coastal")):
         make_eta_adjoint_golden()
     if "coastal" in which:
         make_coastal_golden()
+    if "step_adjoint" in which:
+        make_step_adjoint_goldens()
 
 
 if __name__ == "__main__":
-    main(tuple(sys.argv[1:]) or ("proft", "steps", "adjoint", "coastal"))
+    main(tuple(sys.argv[1:]) or ("proft", "steps", "adjoint", "coastal", "step_adjoint"))

@@ -73,3 +73,27 @@ def step_field_error(got, ref, field, nsteps, golden):
     if field == "w":
         return rel_err(got[..., :-1], ref[..., :-1]), bound
     return rel_err(got, ref), bound
+
+
+def load_adjoint_golden(name):
+    """(start state, scalars, cotangents, {nsteps: {field: gradient}}) of a
+    step_adjoint_*.npz file (the reference's torch-autograd gradients)."""
+    z = np.load(golden_path(name))
+    A = {k[4:]: z[k] for k in z.files if k.startswith("in__")}
+    Sc = {k[8:]: z[k].item() for k in z.files if k.startswith("scalar__")}
+    cot = {k[5:]: z[k] for k in z.files if k.startswith("cot__")}
+    grads = {}
+    for k in z.files:
+        if k.startswith("grad"):
+            n, f = k[4:].split("__")
+            grads.setdefault(int(n), {})[f] = z[k]
+    return A, Sc, cot, grads
+
+
+def grad_errors(got, ref):
+    """max|g - g_ref| / max|g_ref| per field of ``ref``."""
+    out = {}
+    for f, r in ref.items():
+        scale = float(np.abs(r).max())
+        out[f] = float(np.abs(np.asarray(got[f]) - r).max()) / (scale if scale > 0 else 1.0)
+    return out

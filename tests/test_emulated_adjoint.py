@@ -1,0 +1,89 @@
+"""The explicit step adjoint (the device reverse bodies of
+neuralpom_b200/csrc/npom_adjoint.cuh, run on the CPU by tests/emul) against
+the reference's own torch-autograd gradient of the same step(s)
+(``SparsePhysics.advance(differentiable=True)``, sparse_physics.py:91-149),
+recorded in tests/golden/step_adjoint_*.npz."""
+import numpy as np
+import pytest
+
+from golden_io import grad_errors, load_adjoint_golden
+
+emul = pytest.importorskip("emul_harness")
+
+
+def _has_nvcc():
+    import shutil
+    return shutil.which("nvcc") is not None
+
+
+pytestmark = pytest.mark.skipif(not _has_nvcc(), reason="nvcc needed to build the phase emulator")
+
+# tolerance on max|g - g_ref| / max|g_ref| per field: both are the exact
+# derivative of the same float32 step, evaluated in float32 with sums in
+# different orders (the worst field seen is kh of the coastal step, 3e-5)
+GRAD_TOL = 1e-4
+
+
+@pytest.mark.parametrize("fname", ["step_adjoint_explicit_12x10.npz", "step_adjoint_rest_12x10.npz",
+                                   "step_adjoint_coastal_16x14.npz"])
+def test_emulated_step_adjoint_matches_reference_autograd(fname):
+    A, Sc, cot, grads = load_adjoint_golden(fname)
+    for n, ref in sorted(grads.items()):
+        G = emul.multi_step_adjoint(A, Sc, cot, n)
+        errs = grad_errors(G, ref)
+        worst = max(errs, key=errs.get)
+        assert errs[worst] < GRAD_TOL, (fname, n, worst, errs[worst])
+        # every state field the reference differentiates is reached
+        for f in ref:
+            assert np.any(G[f] != 0), (fname, n, f)
+
+
+def test_emulated_step_adjoint_matches_float64_finite_differences():
+    """Three explicit steps of a developed double gyre, loss = MSE of u, v,
+    T, S against a seeded target: the emulated adjoint along 12 random unit
+    directions of (T, S, u, v) against central differences (eps = 1e-3) of
+    the float64 oracle.  Errors relative to the rms of the directional
+    derivatives (float32 and float64 Jacobians differ slightly): < 2e-3."""
+    from golden_io import oracle_params
+    from neuralpom_b200 import cases
+    from oracle import pom_oracle as O
+    A, Sc = cases.double_gyre(24, 20, "explicit")
+    Sc = dict(Sc)
+    Sc.update(time=0.5, time0=0.5)
+    im, jm, kb = A["u"].shape
+    Sc.update(im=im, jm=jm, kb=kb)
+    E = emul.EmulCore(A, Sc, "explicit")
+    E.steps(6)
+    start = {n: v.copy() for n, v in E.F.items()}
+    t0 = E.time
+    rng = np.random.default_rng(7)
+    masks = {"t": start["fsm"][:, :, None], "s": start["fsm"][:, :, None], "u": start["dum"][:, :, None],
+             "v": start["dvm"][:, :, None]}
+    masks = {f: np.broadcast_to(m, start[f].shape).astype(np.float64) for f, m in masks.items()}
+    scale = {"t": 1.0, "s": 0.1, "u": 0.01, "v": 0.01}
+    target = {f: start[f] + 0.1 * scale[f] * rng.standard_normal(start[f].shape) * masks[f] for f in masks}
+    E.steps(3)
+    cot = {f: (2 * (E.F[f].astype(np.float64) - target[f]) / E.F[f].size / scale[f] ** 2).astype(np.float32)
+           for f in target}
+    G = emul.multi_step_adjoint(start, dict(Sc, time=t0), cot, 3)
+    P0 = oracle_params(dict(Sc, time=t0, time0=t0), start, "explicit")
+
+    def run64(pert):
+        S = {n: v.astype(np.float64).copy() for n, v in start.items()}
+        for f, d in pert.items():
+            S[f] += d
+        P = P0.copy()
+        P.time = t0
+        O.run(S, P, 3, "explicit")
+        return sum(((S[f] - target[f]) ** 2).mean() / scale[f] ** 2 for f in target)
+
+    fds, ads = [], []
+    for _ in range(12):
+        dirs = {f: rng.standard_normal(start[f].shape) * masks[f] * scale[f] for f in target}
+        nrm = np.sqrt(sum((d ** 2).sum() for d in dirs.values()))
+        dirs = {f: d / nrm for f, d in dirs.items()}
+        fds.append((run64({f: 1e-3 * d for f, d in dirs.items()}) - run64({f: -1e-3 * d for f, d in dirs.items()}))
+                   / 2e-3)
+        ads.append(sum(float((G[f].astype(np.float64) * dirs[f]).sum()) for f in target))
+    fds, ads = np.array(fds), np.array(ads)
+    assert np.abs(fds - ads).max() / np.sqrt((ads ** 2).mean()) < 2e-3, (fds, ads)

@@ -1,0 +1,110 @@
+"""The explicit step under torch autograd through the drop-in API
+(``ExplicitCore.run_time_loop`` with state tensors that require grad; the
+backward is the CUDA step adjoint ``npom_step_explicit_adjoint``): against
+the reference's own autograd gradients (golden vectors) and against central
+finite differences of the CUDA forward."""
+import numpy as np
+import pytest
+import torch
+
+from golden_io import grad_errors, load_adjoint_golden
+
+pytestmark = pytest.mark.gpu
+
+GRAD_TOL = 1e-4  # relative to max|g_ref| per field, as for the CPU emulation
+
+
+def _core(A, Sc):
+    from neuralpom_b200 import resolve_core_class
+    return resolve_core_class("explicit").from_state(A, Sc, device="cuda")
+
+
+def _differentiable_advance(core, nsteps, time0):
+    """Leaves for every state field, ``nsteps`` steps, the leaves back."""
+    from neuralpom_b200 import _abi
+    leaves = {}
+    for f in _abi.ADJ_STATE_FIELDS:
+        leaves[f] = getattr(core, f).detach().clone().requires_grad_(True)
+        setattr(core, f, leaves[f])
+    core.time0 = time0
+    core.iend = nsteps
+    core.run_time_loop()
+    return leaves
+
+
+@pytest.mark.parametrize("fname", ["step_adjoint_explicit_12x10.npz", "step_adjoint_rest_12x10.npz",
+                                   "step_adjoint_coastal_16x14.npz"])
+def test_gpu_step_adjoint_matches_reference_autograd(fname):
+    A, Sc, cot, grads = load_adjoint_golden(fname)
+    for n, ref in sorted(grads.items()):
+        core = _core(A, Sc)
+        leaves = _differentiable_advance(core, n, float(Sc["time"]))
+        loss = sum((getattr(core, f) * torch.from_numpy(c).cuda()).sum() for f, c in cot.items())
+        loss.backward()
+        got = {f: (leaves[f].grad.cpu().numpy() if leaves[f].grad is not None else np.zeros_like(A[f]))
+               for f in ref}
+        errs = grad_errors(got, ref)
+        worst = max(errs, key=errs.get)
+        assert errs[worst] < GRAD_TOL, (fname, n, worst, errs[worst])
+
+
+def test_gpu_step_adjoint_matches_finite_differences():
+    """Midtrain-shaped check (three explicit steps of a developed double
+    gyre, loss = MSE of u, v, T, S against a seeded target): the CUDA
+    gradient with respect to the initial T, S, u, v along 16 random unit
+    directions against central differences (eps = 1e-3) of the float64
+    oracle step.  The float32 and float64 Jacobians differ slightly, so each
+    error is taken relative to the rms of the 16 directional derivatives:
+    bound 2e-3 (seen: below 1.5e-3), and the median error relative to its own
+    derivative below 1e-3."""
+    from neuralpom_b200 import cases
+    from golden_io import oracle_params
+    from oracle import pom_oracle as O
+    A, Sc = cases.double_gyre(24, 20, "explicit")
+    Sc = dict(Sc)
+    Sc.update(time=0.5, time0=0.5)
+    im, jm, kb = A["u"].shape
+    core = _core(A, Sc)
+    core.time0 = 0.5
+    core.iend = 6
+    with torch.no_grad():
+        core.run_time_loop()  # develop the state
+    t0 = float(core.time)
+    start = {f: getattr(core, f).detach().cpu().numpy().copy() for f in A}
+    rng = np.random.default_rng(7)
+    masks = {"t": start["fsm"][:, :, None], "s": start["fsm"][:, :, None], "u": start["dum"][:, :, None],
+             "v": start["dvm"][:, :, None]}
+    masks = {f: np.broadcast_to(m, start[f].shape).astype(np.float64) for f, m in masks.items()}
+    scale = {"t": 1.0, "s": 0.1, "u": 0.01, "v": 0.01}
+    target = {f: start[f] + 0.1 * scale[f] * rng.standard_normal(start[f].shape) * masks[f] for f in masks}
+
+    leaves = _differentiable_advance(core, 3, t0)
+    loss = sum(((getattr(core, f).double() - torch.from_numpy(target[f]).cuda()) ** 2).mean() / scale[f] ** 2
+               for f in target)
+    loss.backward()
+    grads = {f: leaves[f].grad.double().cpu().numpy() for f in target}
+
+    P0 = oracle_params(dict(Sc, im=im, jm=jm, kb=kb, time=t0, time0=t0), start, "explicit")
+
+    def run64(pert):
+        S = {n: v.astype(np.float64).copy() for n, v in start.items()}
+        for f, d in pert.items():
+            S[f] += d
+        P = P0.copy()
+        P.time = t0
+        O.run(S, P, 3, "explicit")
+        return sum(((S[f] - target[f]) ** 2).mean() / scale[f] ** 2 for f in target)
+
+    fds, ads = [], []
+    eps = 1e-3
+    for _ in range(16):
+        dirs = {f: rng.standard_normal(start[f].shape) * masks[f] * scale[f] for f in target}
+        nrm = np.sqrt(sum((d ** 2).sum() for d in dirs.values()))
+        dirs = {f: d / nrm for f, d in dirs.items()}
+        fds.append((run64({f: eps * d for f, d in dirs.items()}) - run64({f: -eps * d for f, d in dirs.items()}))
+                   / (2 * eps))
+        ads.append(sum(float((grads[f] * dirs[f]).sum()) for f in target))
+    fds, ads = np.array(fds), np.array(ads)
+    rms = float(np.sqrt((ads ** 2).mean()))
+    assert np.abs(fds - ads).max() / rms < 2e-3, (fds, ads)
+    assert np.median(np.abs(fds - ads) / np.maximum(np.abs(fds), np.abs(ads))) < 1e-3, (fds, ads)
