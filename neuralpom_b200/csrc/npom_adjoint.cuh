@@ -2079,6 +2079,40 @@ NPOM_HD size_t adj_field_len(const Ctx &c, int f) {
   return (f >= NPOM_F_u && f <= NPOM_F_curv) ? (size_t)c.im * c.jm * c.kb : (size_t)c.im * c.jm;
 }
 
+// The 2-D fields external-substep phase ph (1, 2, 3) of substep iext
+// overwrites, in save order; returns their number (at most 10).
+NPOM_HD int ext_phase_fields(int iext, int ph, int isplit, int ispadv, int *fld) {
+  int n = 0;
+  if (ph == 1) {
+    fld[n++] = NPOM_F_elf;
+    fld[n++] = NPOM_F_fluxua;
+    fld[n++] = NPOM_F_fluxva;
+    if ((iext % ispadv) == 0) {
+      fld[n++] = NPOM_F_advua;
+      fld[n++] = NPOM_F_advva;
+      fld[n++] = NPOM_F_tps;
+    }
+  } else if (ph == 2) {
+    fld[n++] = NPOM_F_uaf;
+    fld[n++] = NPOM_F_vaf;
+    if (iext >= isplit - 2) fld[n++] = NPOM_F_etf;
+  } else {
+    fld[n++] = NPOM_F_elb;
+    fld[n++] = NPOM_F_el;
+    fld[n++] = NPOM_F_d;
+    fld[n++] = NPOM_F_uab;
+    fld[n++] = NPOM_F_ua;
+    fld[n++] = NPOM_F_vab;
+    fld[n++] = NPOM_F_va;
+    if (iext != isplit) {
+      fld[n++] = NPOM_F_egf;
+      fld[n++] = NPOM_F_utf;
+      fld[n++] = NPOM_F_vtf;
+    }
+  }
+  return n;
+}
+
 // Fills out (capacity cap) and returns the number of phases; *save_floats
 // receives the size of the save area.
 inline int adj_step_plan(const Ctx &c, AdjPhaseRec *out, int cap, size_t *save_floats) {
@@ -2115,18 +2149,12 @@ inline int adj_step_plan(const Ctx &c, AdjPhaseRec *out, int cap, size_t *save_f
   const int isplit = c.k.isplit;
   for (int iext = 1; iext <= isplit; ++iext) {
     const int adv = (iext % c.k.ispadv) == 0;
-    r = begin(AP_E1, iext, adv);
-    for (int f : {NPOM_F_elf, NPOM_F_fluxua, NPOM_F_fluxva}) add(r, f, 1);
-    if (adv)
-      for (int f : {NPOM_F_advua, NPOM_F_advva, NPOM_F_tps}) add(r, f, 1);
-    r = begin(AP_E2, iext, adv);
-    add(r, NPOM_F_uaf, 1);
-    add(r, NPOM_F_vaf, 1);
-    if (iext >= isplit - 2) add(r, NPOM_F_etf, 1);
-    r = begin(AP_E3, iext, adv);
-    for (int f : {NPOM_F_elb, NPOM_F_el, NPOM_F_d, NPOM_F_uab, NPOM_F_ua, NPOM_F_vab, NPOM_F_va}) add(r, f, 1);
-    if (iext != isplit)
-      for (int f : {NPOM_F_egf, NPOM_F_utf, NPOM_F_vtf}) add(r, f, 1);
+    for (int ph = 1; ph <= 3; ++ph) {
+      r = begin(ph == 1 ? AP_E1 : (ph == 2 ? AP_E2 : AP_E3), iext, adv);
+      int fl[10];
+      const int nf = ext_phase_fields(iext, ph, isplit, c.k.ispadv, fl);
+      for (int e = 0; e < nf; ++e) add(r, fl[e], 1);
+    }
   }
   if (c.do_internal) {
     r = begin(AP_B1, 0, 0);

@@ -59,6 +59,100 @@ __global__ void __launch_bounds__(kThreads) k_adj_cells(Ctx c, Adj a, int phase,
   else ext_phase3_cell_adj(c, a, i, j, iext);
 }
 
+// The whole external subcycle of the recomputation on one thread-block
+// cluster (grids of up to kSubClusterCells cells): before each phase every
+// thread saves the values of the fields the phase overwrites at the cells it
+// computes (the same thread-to-cell map, so no barrier is needed between
+// save and compute), then computes the phase; the cluster barrier separates
+// the phases.  Loads go through L2 (Ctx::coh).  save + base is the first
+// external-phase record of the plan; records follow in plan order.
+template <int T>
+__global__ void __launch_bounds__(T, 1) k_adj_ext_forward(Ctx c, float *save) {
+  cgx::cluster_group cl = cgx::this_cluster();
+  const size_t ncell = (size_t)c.im * c.jm;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  float *out = save;
+  for (int iext = 1; iext <= c.k.isplit; ++iext) {
+    const bool adv = (iext % c.k.ispadv) == 0;
+    for (int ph = 1; ph <= 3; ++ph) {
+      int fl[10];
+      const int nf = ext_phase_fields(iext, ph, c.k.isplit, c.k.ispadv, fl);
+      for (int e = 0; e < nf; ++e) {
+        const float *src = c.F[fl[e]];
+        for (size_t q = tid; q < ncell; q += stride) out[(size_t)e * ncell + q] = __ldcg(src + q);
+      }
+      out += (size_t)nf * ncell;
+      for (size_t q = tid; q < ncell; q += stride) {
+        const int i = (int)(q / c.jm), j = (int)(q % c.jm);
+        if (ph == 1) ext_phase1_cell(c, i, j, adv);
+        else if (ph == 2) (void)ext_phase2_cell(c, i, j, iext);
+        else ext_phase3_cell(c, i, j, iext);
+      }
+      cl.sync();
+    }
+  }
+}
+
+// The reverse sweep of the external subcycle on one cluster: for each
+// phase from the last, restore its inputs and move the cotangents of what it
+// wrote (each thread its own cells), cluster barrier, the phase's adjoint
+// (scatters are atomics in L2; every other read goes through L2 or is of a
+// value the thread itself moved), cluster barrier.
+template <int T>
+__global__ void __launch_bounds__(T, 1) k_adj_ext_reverse(Ctx c, Adj a, const float *save_end) {
+  cgx::cluster_group cl = cgx::this_cluster();
+  const size_t ncell = (size_t)c.im * c.jm;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const float *in = save_end;
+  for (int iext = c.k.isplit; iext >= 1; --iext) {
+    const bool adv = (iext % c.k.ispadv) == 0;
+    for (int ph = 3; ph >= 1; --ph) {
+      int fl[10];
+      const int nf = ext_phase_fields(iext, ph, c.k.isplit, c.k.ispadv, fl);
+      in -= (size_t)nf * ncell;
+      for (int e = 0; e < nf; ++e) {
+        float *dst = c.F[fl[e]], *g = a.G[fl[e]], *l = a.L[fl[e]];
+        for (size_t q = tid; q < ncell; q += stride) {
+          dst[q] = in[(size_t)e * ncell + q];
+          l[q] = __ldcg(g + q);
+          g[q] = 0.0f;
+        }
+      }
+      cl.sync();
+      for (size_t q = tid; q < ncell; q += stride) {
+        const int i = (int)(q / c.jm), j = (int)(q % c.jm);
+        if (ph == 3) ext_phase3_cell_adj(c, a, i, j, iext);
+        else if (ph == 2) ext_phase2_cell_adj(c, a, i, j, iext);
+        else ext_phase1_cell_adj(c, a, i, j, adv);
+      }
+      cl.sync();
+    }
+  }
+}
+
+const void *const kAdjExtForward[3] = {(const void *)k_adj_ext_forward<256>, (const void *)k_adj_ext_forward<512>,
+                                       (const void *)k_adj_ext_forward<1024>};
+const void *const kAdjExtReverse[3] = {(const void *)k_adj_ext_reverse<256>, (const void *)k_adj_ext_reverse<512>,
+                                       (const void *)k_adj_ext_reverse<1024>};
+
+// Cluster shape of the fused external-subcycle adjoint kernels (0: use the
+// per-phase launches), decided outside any capture; NPOM_ADJ_EXT=phases
+// forces those.  Both kernels get the shape that fits both.
+int plan_adj_ext(const Ctx &c) {
+  const char *env = getenv("NPOM_ADJ_EXT");
+  if (env && std::strcmp(env, "phases") == 0) return 0;
+  const size_t ncell = (size_t)c.im * c.jm;
+  if (ncell > kSubClusterCells) return 0;
+  int f = 0, r = 0;
+  if (plan_cluster(kAdjExtForward, ncell, &f) != cudaSuccess || plan_cluster(kAdjExtReverse, ncell, &r) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return cluster_ctas(f) <= cluster_ctas(r) ? f : r;
+}
+
 // save[off_e ...] = F[fld_e] for every field e of a phase (blockIdx.y = e)
 __global__ void k_save_fields(Ctx c, AdjPhaseRec r, float *save) {
   const int e = blockIdx.y;
@@ -169,11 +263,42 @@ npom_status run_explicit_adjoint(const npom_params *p, float *const *fields, con
   size_t need = 0;
   const int np = adj_step_plan(c, plan.data(), (int)plan.size(), &need);
   if (need > aws->save_floats) return NPOM_ERR_ARG;
+  // the external-subcycle records sit together in the plan: [e0, e1)
+  int e0 = np, e1 = np;
+  for (int q = 0; q < np; ++q)
+    if (plan[q].phase == AP_E1 || plan[q].phase == AP_E2 || plan[q].phase == AP_E3) {
+      e0 = std::min(e0, q);
+      e1 = q + 1;
+    }
+  const int ext_shape = e0 < e1 ? plan_adj_ext(c) : 0;
+  const int ext_threads = ext_shape < 0 ? cluster_threads(ext_shape) : 0;
+  const int ext_t = ext_threads == 256 ? 0 : (ext_threads == 512 ? 1 : 2);
+  const int ext_ctas = ext_shape < 0 ? cluster_ctas(ext_shape) : 0;
+  Ctx cc = c;
+  cc.coh = 1;
+  float *ext_save = e0 < e1 ? aws->save + plan[e0].off[0] : nullptr;
+  const float *ext_end = e0 < e1 ? aws->save + plan[e1 - 1].off[plan[e1 - 1].n - 1] +
+                                       adj_field_len(c, plan[e1 - 1].fld[plan[e1 - 1].n - 1])
+                                 : nullptr;
   for (int q = 0; q < np; ++q) {
+    if (ext_ctas > 0 && q >= e0 && q < e1) {
+      if (q == e0) {
+        void *args[] = {&cc, &ext_save};
+        if (launch_cluster(kAdjExtForward[ext_t], ext_ctas, ext_threads, args, s) != cudaSuccess) return NPOM_ERR_CUDA;
+      }
+      continue;
+    }
     k_save_fields<<<field_list_grid(c, plan[q]), kThreads, 0, s>>>(c, plan[q], aws->save);
     launch_fwd_phase(c, plan[q], s);
   }
   for (int q = np - 1; q >= 0; --q) {
+    if (ext_ctas > 0 && q >= e0 && q < e1) {
+      if (q == e0) {
+        void *args[] = {&cc, &a, &ext_end};
+        if (launch_cluster(kAdjExtReverse[ext_t], ext_ctas, ext_threads, args, s) != cudaSuccess) return NPOM_ERR_CUDA;
+      }
+      continue;
+    }
     k_restore_move<<<field_list_grid(c, plan[q]), kThreads, 0, s>>>(c, a, plan[q], aws->save);
     launch_adj_phase(c, a, plan[q], s);
   }

@@ -530,15 +530,17 @@ __global__ void __launch_bounds__(kThreads) k_subcycle(Ctx c) {
 }
 
 // The same subcycle for grids of up to kSubClusterCells cells, on one
-// thread-block cluster of at most 16 CTAs: the three phases of a substep are
-// separated by the hardware cluster barrier (release/acquire at cluster
-// scope covers the global-memory state; loads bypass L1) instead of the
-// global-memory grid barrier, about a fifth of its latency.  Every CTA runs
-// the same loop, so every barrier is reached by all of them.
+// thread-block cluster of at most 16 CTAs of 256, 512 or 1024 threads (the
+// fewest that give every cell its own thread): the three phases of a
+// substep are separated by the hardware cluster barrier (release/acquire at
+// cluster scope covers the global-memory state; loads bypass L1) instead of
+// the global-memory grid barrier, about a fifth of its latency.  Every CTA
+// runs the same loop, so every barrier is reached by all of them.
 constexpr int kSubClusterMax = 16;
-constexpr size_t kSubClusterCells = (size_t)kSubClusterMax * kThreads * 4;
+constexpr size_t kSubClusterCells = (size_t)kSubClusterMax * 1024;
 
-__global__ void __launch_bounds__(kThreads) k_subcycle_cluster(Ctx c) {
+template <int T>
+__global__ void __launch_bounds__(T, 1) k_subcycle_cluster(Ctx c) {
   cgx::cluster_group cl = cgx::this_cluster();
   const size_t ncell = (size_t)c.im * c.jm;
   const size_t stride = (size_t)gridDim.x * blockDim.x;
@@ -555,6 +557,73 @@ __global__ void __launch_bounds__(kThreads) k_subcycle_cluster(Ctx c) {
     cl.sync();
   }
 }
+
+// A cluster launch shape, encoded as a negative int (positive values are
+// grid-barrier block counts): -(ctas * 4 + log2(threads / 256)).
+int encode_cluster(int ctas, int threads) { return -(ctas * 4 + (threads == 256 ? 0 : (threads == 512 ? 1 : 2))); }
+int cluster_ctas(int code) { return (-code) / 4; }
+int cluster_threads(int code) { return 256 << ((-code) % 4); }
+
+cudaError_t launch_cluster(const void *fn, int ctas, int threads, void **args, cudaStream_t s) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(ctas);
+  cfg.blockDim = dim3(threads);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = ctas;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
+// Shape of one cluster covering ncell cells with the kernel instance fn[t]
+// of 256 << t threads: the fewest threads per CTA that give each cell its
+// own thread, halving the CTA count while the cluster does not fit on a GPC.
+// Sets the non-portable cluster-size attribute once per kernel and device.
+cudaError_t plan_cluster(const void *const fn[3], size_t ncell, int *out) {
+  const int t = ncell <= 16 * 256 ? 0 : (ncell <= 16 * 512 ? 1 : 2);
+  const int threads = 256 << t;
+  static std::mutex mu;
+  static std::vector<std::pair<const void *, int>> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    bool seen = false;
+    for (auto &d : done) seen |= (d.first == fn[t] && d.second == dev);
+    if (!seen) {
+      e = cudaFuncSetAttribute(fn[t], cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+      if (e != cudaSuccess) return e;
+      done.emplace_back(fn[t], dev);
+    }
+  }
+  int ctas = (int)std::max<size_t>(1, std::min<size_t>(kSubClusterMax, (ncell + threads - 1) / threads));
+  for (; ctas > 1; ctas /= 2) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(ctas);
+    cfg.blockDim = dim3(threads);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = ctas;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    e = cudaOccupancyMaxActiveClusters(&nclusters, fn[t], &cfg);
+    if (e == cudaSuccess && nclusters > 0) break;
+    cudaGetLastError();
+  }
+  *out = encode_cluster(ctas, threads);
+  return cudaSuccess;
+}
+
+const void *const kSubcycleCluster[3] = {(const void *)k_subcycle_cluster<256>, (const void *)k_subcycle_cluster<512>,
+                                         (const void *)k_subcycle_cluster<1024>};
 
 // PROFT over independent columns (TracersMixin.proft, any kb <= KMAX)
 __global__ void __launch_bounds__(128) k_proft(int ncol, int kb, const float *f_in, const float *wfsurf,
@@ -732,64 +801,24 @@ cudaError_t run_pcg(Ctx c, const PcgPlan &plan, int with_rhs, int with_post, cud
 }
 
 // Launch shape of the explicit subcycle, decided outside any capture:
-// > 0 grid-barrier blocks, < 0 the CTAs of one cluster.  NPOM_SUBCYCLE=grid
-// forces the grid-barrier form on small grids too.
+// > 0 grid-barrier blocks, < 0 a cluster shape (encode_cluster).
+// NPOM_SUBCYCLE=grid forces the grid-barrier form on small grids too.
 cudaError_t plan_subcycle(const Ctx &c, int *out) {
   const size_t ncell = (size_t)c.im * c.jm;
   const char *env = getenv("NPOM_SUBCYCLE");
   const bool grid = env && std::strcmp(env, "grid") == 0;
-  if (!grid && ncell <= kSubClusterCells) {
-    static bool attr_set[64] = {false};
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-      e = cudaFuncSetAttribute((const void *)k_subcycle_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-      if (e != cudaSuccess) return e;
-      attr_set[dev] = true;
-    }
-    int ctas = (int)std::min<size_t>(kSubClusterMax, (ncell + kThreads - 1) / kThreads);
-    ctas = std::max(1, ctas);
-    // a cluster of that size must fit on one GPC; halve it until one does
-    for (; ctas > 1; ctas /= 2) {
-      cudaLaunchConfig_t cfg = {};
-      cfg.gridDim = dim3(ctas);
-      cfg.blockDim = dim3(kThreads);
-      cudaLaunchAttribute attr[1];
-      attr[0].id = cudaLaunchAttributeClusterDimension;
-      attr[0].val.clusterDim.x = ctas;
-      attr[0].val.clusterDim.y = 1;
-      attr[0].val.clusterDim.z = 1;
-      cfg.attrs = attr;
-      cfg.numAttrs = 1;
-      int nclusters = 0;
-      e = cudaOccupancyMaxActiveClusters(&nclusters, (const void *)k_subcycle_cluster, &cfg);
-      if (e == cudaSuccess && nclusters > 0) break;
-      cudaGetLastError();
-    }
-    *out = -ctas;
-    return cudaSuccess;
-  }
+  if (!grid && ncell <= kSubClusterCells) return plan_cluster(kSubcycleCluster, ncell, out);
   return coop_blocks((const void *)k_subcycle, ncell, out);
 }
 
 cudaError_t run_subcycle(Ctx c, int blocks, cudaStream_t s) {
   c.coh = 1;
-  if (blocks < 0) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(-blocks);
-    cfg.blockDim = dim3(kThreads);
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = -blocks;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_subcycle_cluster, c);
-  }
   void *args[] = {&c};
+  if (blocks < 0) {
+    const int threads = cluster_threads(blocks);
+    const int t = threads == 256 ? 0 : (threads == 512 ? 1 : 2);
+    return launch_cluster(kSubcycleCluster[t], cluster_ctas(blocks), threads, args, s);
+  }
   return launch_coop((const void *)k_subcycle, blocks, args, c.sync, s);
 }
 

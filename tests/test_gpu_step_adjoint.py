@@ -32,9 +32,13 @@ def _differentiable_advance(core, nsteps, time0):
     return leaves
 
 
+@pytest.mark.parametrize("ext", ["cluster", "phases"])
 @pytest.mark.parametrize("fname", ["step_adjoint_explicit_12x10.npz", "step_adjoint_rest_12x10.npz",
                                    "step_adjoint_coastal_16x14.npz"])
-def test_gpu_step_adjoint_matches_reference_autograd(fname):
+def test_gpu_step_adjoint_matches_reference_autograd(monkeypatch, fname, ext):
+    """Both forms of the external-subcycle adjoint: the two fused
+    thread-block-cluster kernels and one launch per substep phase."""
+    monkeypatch.setenv("NPOM_ADJ_EXT", ext)
     A, Sc, cot, grads = load_adjoint_golden(fname)
     for n, ref in sorted(grads.items()):
         core = _core(A, Sc)
