@@ -3,7 +3,10 @@
 
 ``advance(core, steps)`` resets the clock bookkeeping exactly like the
 reference's no-grad branch (``time0 = time``, ``iint = 0``, ``iend =
-steps``) and runs ``core.run_time_loop()`` on the B200 library.
+steps``) and runs ``core.run_time_loop()`` on the B200 library;
+``differentiable=True`` (explicit core) advances in chunks of
+``chunk_steps``, each one autograd node whose backward is the CUDA step
+adjoint, like the reference's checkpointed chunks.
 """
 from __future__ import annotations
 
@@ -33,7 +36,20 @@ class B200Physics:
         if not isinstance(core, B200Core) or core.core_name != self.core_name:
             raise TypeError(f"B200Physics({self.core_name!r}) requires the matching B200 core")
         if differentiable:
-            raise NotImplementedError("the differentiable advance is not provided by the B200 core")
+            # chunks of chunk_steps, each one autograd node with a checkpoint
+            # per internal step (sparse_physics.py:108-149)
+            if self.core_name != "explicit":
+                raise NotImplementedError("the differentiable advance is provided for the explicit core")
+            for start in range(0, steps, self.chunk_steps):
+                n = min(self.chunk_steps, steps - start)
+                core.time0 = float(core.time)
+                core.iint = 0
+                core.iend = n
+                with torch.enable_grad():
+                    core.run_time_loop()
+                if core.iint != n:
+                    raise RuntimeError("Physical core returned before the checkpoint chunk completed")
+            return
         core.time0 = float(core.time)
         core.iint = 0
         core.iend = steps

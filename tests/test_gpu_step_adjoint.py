@@ -112,3 +112,25 @@ def test_gpu_step_adjoint_matches_finite_differences():
     rms = float(np.sqrt((ads ** 2).mean()))
     assert np.abs(fds - ads).max() / rms < 2e-3, (fds, ads)
     assert np.median(np.abs(fds - ads) / np.maximum(np.abs(fds), np.abs(ads))) < 1e-3, (fds, ads)
+
+
+def test_gpu_physics_differentiable_advance_in_chunks():
+    """B200Physics.advance(differentiable=True) with chunk_steps = 2 over
+    three steps (a chunk of 2 and one of 1, the reference's
+    _checkpoint_chunk split) gives the reference's 3-step gradient."""
+    from neuralpom_b200 import B200Physics, _abi
+    A, Sc, cot, grads = load_adjoint_golden("step_adjoint_explicit_12x10.npz")
+    core = _core(A, Sc)
+    core.time = float(Sc["time"])
+    leaves = {}
+    for f in _abi.ADJ_STATE_FIELDS:
+        leaves[f] = getattr(core, f).detach().clone().requires_grad_(True)
+        setattr(core, f, leaves[f])
+    B200Physics("cuda", chunk_steps=2, core_name="explicit").advance(core, steps=3, differentiable=True)
+    assert core.iint == 1 and abs(core.time - (float(Sc["time"]) + 3 * core.dti / 86400.0)) < 1e-9
+    loss = sum((getattr(core, f) * torch.from_numpy(c).cuda()).sum() for f, c in cot.items())
+    loss.backward()
+    got = {f: leaves[f].grad.cpu().numpy() for f in grads[3]}
+    errs = grad_errors(got, grads[3])
+    worst = max(errs, key=errs.get)
+    assert errs[worst] < GRAD_TOL, (worst, errs[worst])
