@@ -329,13 +329,20 @@ def run_b200(args):
         cpu = reference_cpu_sample(A, Sc, internal_steps=args.ref_internal_steps, warm=1, reps=2,
                                    core_name=W["core"])
 
-    fa = None
+    fa = fam = None
     if rank == 0 and ws_n == 1 and args.workload == "seamount" and not args.no_fwd_adjoint:
-        fa = fwd_adjoint_sample(args, dev)
+        fa, A_dev, t_dev = seamount_fwd_adjoint(core, args, dev)
+        case = (A_dev, dict(Sc, time=t_dev, time0=t_dev))
         if not args.no_ref_gpu:
-            fa["reference_gpu"] = reference_fwd_adjoint_sample(dev)
+            fa["reference_gpu"] = reference_fwd_adjoint_sample(dev, case=case, core_name=W["core"], seed=11)
         if not args.no_cpu_baseline:
-            fa["reference_cpu"] = reference_fwd_adjoint_sample("cpu", internal_steps=3)
+            fa["reference_cpu"] = reference_fwd_adjoint_sample("cpu", internal_steps=3, case=case,
+                                                               core_name=W["core"], seed=11)
+        fam = fwd_adjoint_sample(args, dev)
+        if not args.no_ref_gpu:
+            fam["reference_gpu"] = reference_fwd_adjoint_sample(dev)
+        if not args.no_cpu_baseline:
+            fam["reference_cpu"] = reference_fwd_adjoint_sample("cpu", internal_steps=3)
 
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws_n, "steps": args.steps,
@@ -347,7 +354,7 @@ def run_b200(args):
                    "pcg_iterations_last_step": (its[-1] if its else None) if W["core"] != "explicit" else None,
                    "members": ws_n, "parallelism": f"ensemble x{ws_n}" if ws_n > 1 else "single member",
                    "l2": "flushed (256 MiB write) before every timed step"},
-        "roofline": roofline, "cpu_baseline": cpu, "reference_gpu": ref_gpu, "ensemble": ens, "fwd_adjoint": fa, "e2e": e2e,
+        "roofline": roofline, "cpu_baseline": cpu, "reference_gpu": ref_gpu, "ensemble": ens, "fwd_adjoint": fa, "fwd_adjoint_midtrain": fam, "e2e": e2e,
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
@@ -575,46 +582,34 @@ def _fa_targets(A, seed, dev=None):
     return out, incs
 
 
-def fwd_adjoint_sample(args, dev, reps=3):
-    """Forward+adjoint through the drop-in API under torch autograd: every
-    state field a leaf, three differentiable run_time_loop() calls of 30
-    internal steps with the increment between them, the loss, backward().
-    Timed with CUDA events around forward and backward (checkpoint per
-    internal step, recomputation and the hand-written step adjoint)."""
+def fwd_adjoint_timing(core, start, tgt, incs, intervals, steps_per_interval, t0, reps, warm, dev):
+    """Median CUDA-event time (ms) of forward+backward through the drop-in
+    API under torch autograd: every state field a leaf, ``intervals``
+    differentiable run_time_loop() calls of ``steps_per_interval`` internal
+    steps with the increments between them, MSE(u, v, T, S) loss,
+    backward()."""
     import torch
-    from neuralpom_b200 import _abi, resolve_core_class
-    A, Sc = midtrain_case(0)
-    core = resolve_core_class("explicit").from_state(A, Sc, device=dev)
-    tgt, incs = _fa_targets(A, 7)
-    tgt = {f: torch.from_numpy(v).to(dev) for f, v in tgt.items()}
-    incs = {f: torch.from_numpy(v).to(dev) for f, v in incs.items()}
-    start = {f: getattr(core, f).detach().clone() for f in _abi.FIELD_NAMES}
-    dti = float(core.dti)
+    from neuralpom_b200 import _abi
     stream = torch.cuda.current_stream(dev)
+    dti = float(core.dti)
 
     def prepare():
         for f in _abi.FIELD_NAMES:
             setattr(core, f, start[f].clone())
-        leaves = []
-        for f in _abi.ADJ_STATE_FIELDS:
-            t = getattr(core, f).requires_grad_(True)
-            leaves.append(t)
-        return leaves
+        return [getattr(core, f).requires_grad_(True) for f in _abi.ADJ_STATE_FIELDS]
 
     def fwd_bwd():
-        t0 = float(Sc["time"])
-        for k in range(FA_INTERVALS):
-            core.time0 = t0 + k * FA_STEPS_PER_INTERVAL * dti / 86400.0
-            core.iend = FA_STEPS_PER_INTERVAL
+        for k in range(intervals):
+            core.time0 = t0 + k * steps_per_interval * dti / 86400.0
+            core.iend = steps_per_interval
             core.run_time_loop()
-            if k < FA_INTERVALS - 1:
+            if k < intervals - 1:
                 for f, d in incs.items():
                     setattr(core, f, getattr(core, f) + d)
         loss = sum(((getattr(core, f) - tgt[f]) ** 2).mean() for f in tgt)
         loss.backward()
-        return loss
 
-    for _ in range(max(args.warmup, 1)):
+    for _ in range(max(warm, 1)):
         prepare()
         fwd_bwd()
     torch.cuda.synchronize(dev)
@@ -629,9 +624,54 @@ def fwd_adjoint_sample(args, dev, reps=3):
         torch.cuda.synchronize(dev)
         ms.append(e0.elapsed_time(e1))
         assert all(t.grad is not None for t in leaves[:12])
+    with torch.no_grad():
+        for f in _abi.FIELD_NAMES:
+            setattr(core, f, start[f].clone())
+    return statistics.median(ms)
+
+
+def seamount_fwd_adjoint(core, args, dev, nsteps=36, reps=3):
+    """Forward+adjoint on the headline workload: the semi-implicit core on
+    the 90x82x16 seamount basin from its state after the timed region,
+    ``nsteps`` internal steps (3 h), MSE(u, v, T, S) against a seeded
+    target, backward to every state field (the free-surface solve
+    differentiates through its CUDA adjoint)."""
+    import torch
+    from neuralpom_b200 import _abi
+    start = {f: getattr(core, f).detach().clone() for f in _abi.FIELD_NAMES}
+    A = {f: v.cpu().numpy() for f, v in start.items()}
+    tgt, _ = _fa_targets(A, 11)
+    tgt = {f: torch.from_numpy(v).to(dev) for f, v in tgt.items()}
+    t0 = float(core.time)
+    best = fwd_adjoint_timing(core, start, tgt, {}, 1, nsteps, t0, reps, args.warmup, dev)
+    days = nsteps * float(core.dti) / 86400.0
+    core.time = t0
+    return {"value": days / (best / 1000.0), "unit": UNIT, "ms_per_sample": best,
+            "workload": f"the headline workload (semi-implicit core, closed {GRID[0]}x{GRID[1]}x{GRID[2]} seamount "
+                        f"basin, dtI=300 s, PCG tolerance 1e-10) from its state after the timed region; {nsteps} "
+                        "internal steps forward under autograd, MSE(u,v,T,S) loss, backward to every state field; "
+                        "checkpoint per internal step, hand-written CUDA step adjoint with the free-surface "
+                        "solve's CUDA adjoint",
+            "timing": f"median of {reps} samples, CUDA events around forward+backward"}, A, t0
+
+
+def fwd_adjoint_sample(args, dev, reps=3):
+    """The Midtrain-shaped forward+adjoint: the explicit-core member of
+    ``midtrain_case``, three differentiable 1 h intervals with the
+    increment between them, MSE(u, v, T, S), backward (see
+    ``fwd_adjoint_timing``)."""
+    import torch
+    from neuralpom_b200 import _abi, resolve_core_class
+    A, Sc = midtrain_case(0)
+    core = resolve_core_class("explicit").from_state(A, Sc, device=dev)
+    tgt, incs = _fa_targets(A, 7)
+    tgt = {f: torch.from_numpy(v).to(dev) for f, v in tgt.items()}
+    incs = {f: torch.from_numpy(v).to(dev) for f, v in incs.items()}
+    start = {f: getattr(core, f).detach().clone() for f in _abi.FIELD_NAMES}
+    best = fwd_adjoint_timing(core, start, tgt, incs, FA_INTERVALS, FA_STEPS_PER_INTERVAL, float(Sc["time"]), reps,
+                              args.warmup, dev)
     nint = FA_INTERVALS * FA_STEPS_PER_INTERVAL
-    days = nint * dti / 86400.0
-    best = statistics.median(ms)
+    days = nint * float(core.dti) / 86400.0
     return {"value": days / (best / 1000.0), "unit": UNIT, "ms_per_sample": best,
             "workload": f"explicit core, {FA_GRID[0]}x{FA_GRID[1]}x{FA_GRID[2]} noise basin (dtE=6 s, isplit=20, "
                         f"dtI=120 s), T/S/u/v-perturbed member; {FA_INTERVALS} x 1 h intervals ({nint} internal "
@@ -641,14 +681,14 @@ def fwd_adjoint_sample(args, dev, reps=3):
                       "90x82x16 state fits in L2)"}
 
 
-def reference_fwd_adjoint_sample(device, internal_steps=6):
-    """The reference explicit core under torch autograd
+def reference_fwd_adjoint_sample(device, internal_steps=6, case=None, core_name="explicit", seed=7):
+    """The reference core under torch autograd
     (SparsePhysics.advance(differentiable=True) + backward) on the same
-    member: ``internal_steps`` steps, wall clock."""
+    state: ``internal_steps`` steps, wall clock."""
     import torch
-    A, Sc = midtrain_case(0)
-    core, rh = reference_core(A, Sc, device, "explicit")
-    tgt, _ = _fa_targets(A, 7)
+    A, Sc = case if case is not None else midtrain_case(0)
+    core, rh = reference_core(A, Sc, device, core_name)
+    tgt, _ = _fa_targets(A, seed)
     from neuralpom_b200 import _abi
     names = [k for k in _abi.ADJ_STATE_FIELDS if torch.is_tensor(getattr(core, k, None))]
 
@@ -658,7 +698,7 @@ def reference_fwd_adjoint_sample(device, internal_steps=6):
             t = getattr(core, k).detach().clone().requires_grad_(True)
             setattr(core, k, t)
             leaves.append(t)
-        rh.advance(core, "explicit", n, differentiable=True, device=device)
+        rh.advance(core, core_name, n, differentiable=True, device=device)
         loss = sum(((getattr(core, f) - torch.from_numpy(v).to(device)) ** 2).mean() for f, v in tgt.items())
         loss.backward()
         for k, v in list(vars(core).items()):
@@ -676,7 +716,7 @@ def reference_fwd_adjoint_sample(device, internal_steps=6):
     return {"value": days / sec, "unit": UNIT, "device": str(device),
             "threads": (os.cpu_count() or 1) if device == "cpu" else None,
             "sample": f"{internal_steps} internal steps forward+backward of the {_basin_name(A)} (reference "
-                      "explicit core, torch autograd through SparsePhysics.advance(differentiable=True), after a "
+                      f"{core_name} core, torch autograd through SparsePhysics.advance(differentiable=True), after a "
                       "1-step warm-up; wall clock)"}
 
 

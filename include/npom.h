@@ -259,8 +259,21 @@ size_t npom_adjoint_save_floats(const npom_params *p);
  * the cotangent of field f after the step, on exit the cotangent of f
  * before it (vector-Jacobian product, accumulated in place).  Geometry,
  * forcing and open-boundary arrays are constants.  Supported settings:
- * explicit core, mode 3, nadv 1, nbct/nbcs 1 or 3; else NPOM_ERR_ARG. */
+ * explicit core, mode 3, nadv 1, nbct/nbcs 1 or 3; else NPOM_ERR_ARG.
+ * The caller's save area also holds the step's scratch:
+ * npom_adjoint_save_floats includes it. */
 npom_status npom_step_explicit_adjoint(const npom_params *p, float *const *fields,
+                                       const npom_workspace *ws,
+                                       const npom_clock *clk, float *const *grads,
+                                       const npom_adjoint_ws *aws, void *stream);
+
+/* The same for the semi-implicit step (implicit_p0_fixed/time_loop.py:
+ * 38-688 under torch autograd; the free-surface solve differentiates as
+ * _ImplicitEtaSolveFunction, core.py:24-59).  Supported settings: mode 3,
+ * nadv 1, nbct/nbcs 1 or 3, zero barotropic and tracer Shapiro filters.
+ * Returns NPOM_ERR_DEVICE when the solve's cotangent is not finite; one
+ * host synchronisation per call (the adjoint solve's scale). */
+npom_status npom_step_implicit_adjoint(const npom_params *p, float *const *fields,
                                        const npom_workspace *ws,
                                        const npom_clock *clk, float *const *grads,
                                        const npom_adjoint_ws *aws, void *stream);

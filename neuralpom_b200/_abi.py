@@ -156,9 +156,10 @@ def load_library():
     lib.npom_status_read.restype = i32
     lib.npom_adjoint_save_floats.restype = ctypes.c_size_t
     lib.npom_adjoint_save_floats.argtypes = [P(NpomParams)]
-    lib.npom_step_explicit_adjoint.restype = i32
-    lib.npom_step_explicit_adjoint.argtypes = [P(NpomParams), P(FieldArray), P(NpomWorkspace), P(NpomClock),
-                                               P(FieldArray), P(NpomAdjointWs), vp]
+    for fn in (lib.npom_step_explicit_adjoint, lib.npom_step_implicit_adjoint):
+        fn.restype = i32
+        fn.argtypes = [P(NpomParams), P(FieldArray), P(NpomWorkspace), P(NpomClock), P(FieldArray),
+                       P(NpomAdjointWs), vp]
     lib.npom_status_read.argtypes = [P(NpomWorkspace), i32, P(ctypes.c_uint), vp]
     check_layout(lib)
     _LIB = lib

@@ -184,15 +184,15 @@ class B200Core:
         run_time_loop semantics); raises FloatingPointError when the
         barotropic velocity exceeds vmaxl or the elevation is not finite.
         When grad mode is on and a state tensor requires grad, the advance
-        is one differentiable node (explicit core) whose backward is the
-        hand-written step adjoint; the state attributes are rebound to its
-        outputs, as the reference's autograd path rebinds them."""
+        is one differentiable node whose backward is the hand-written step
+        adjoint; the state attributes are rebound to its outputs, as the
+        reference's autograd path rebinds them."""
         nsteps = int(self.iend)
         if nsteps < 0:
             raise ValueError("iend must be non-negative")
         if self._differentiable_call():
-            outs = _ExplicitStepsFunction.apply(self, nsteps, float(self.time0),
-                                                *[getattr(self, f) for f in _abi.ADJ_STATE_FIELDS])
+            outs = _StepsFunction.apply(self, nsteps, float(self.time0),
+                                        *[getattr(self, f) for f in _abi.ADJ_STATE_FIELDS])
             for f, o in zip(_abi.ADJ_STATE_FIELDS, outs):
                 setattr(self, f, o)
             bits, its = self.read_status(nsteps)
@@ -214,12 +214,7 @@ class B200Core:
     def _differentiable_call(self):
         if not torch.is_grad_enabled():
             return False
-        needs = any(torch.is_tensor(getattr(self, f)) and getattr(self, f).requires_grad
-                    for f in _abi.FIELD_NAMES)
-        if needs and self.core_name != "explicit":
-            raise NotImplementedError("the differentiable step is provided for the explicit core; the implicit "
-                                      "core differentiates its free-surface solve (solve_implicit_eta_cg)")
-        return needs
+        return any(torch.is_tensor(getattr(self, f)) and getattr(self, f).requires_grad for f in _abi.FIELD_NAMES)
 
     def _raise_for(self, bits):
         if bits & _abi.DEV_TIMEOUT:
@@ -250,14 +245,15 @@ class _StateBuffer:
             off += sz
 
 
-class _ExplicitStepsFunction(torch.autograd.Function):
-    """``nsteps`` explicit internal steps as one autograd node: inputs and
-    outputs are the state fields ``_abi.ADJ_STATE_FIELDS``.  The forward
-    keeps one checkpoint of the state per step; the backward recomputes
-    each step from its checkpoint and runs ``npom_step_explicit_adjoint``
-    in reverse step order (per-internal-step checkpointing with
-    recomputation, like the reference's ``_checkpoint_chunk``,
-    sparse_physics.py:108-149, under torch autograd)."""
+class _StepsFunction(torch.autograd.Function):
+    """``nsteps`` internal steps as one autograd node: inputs and outputs
+    are the state fields ``_abi.ADJ_STATE_FIELDS``.  The forward keeps one
+    checkpoint of the state per step; the backward recomputes each step
+    from its checkpoint and runs the step adjoint
+    (``npom_step_explicit_adjoint`` / ``npom_step_implicit_adjoint``) in
+    reverse step order (per-internal-step checkpointing with recomputation,
+    like the reference's ``_checkpoint_chunk``, sparse_physics.py:108-149,
+    under torch autograd)."""
 
     @staticmethod
     def forward(ctx, core, nsteps, time0, *state):
@@ -311,13 +307,16 @@ class _ExplicitStepsFunction(torch.autograd.Function):
         ga = _abi.FieldArray(*[G.views[n].data_ptr() for n in names])
         ws = core._workspace()
         st = torch.cuda.current_stream(dev)
+        fn = lib.npom_step_explicit_adjoint if core.core_name == "explicit" else lib.npom_step_implicit_adjoint
         for n in reversed(range(ctx.nsteps)):
             work.flat[:ndyn].copy_(ckpt[n])
             clk = _abi.NpomClock(float(ctx.time0), int(n + 1), 1)
-            _abi.check(lib.npom_step_explicit_adjoint(ctypes.byref(p), ctypes.byref(fa), ctypes.byref(ws["struct"]),
-                                                      ctypes.byref(clk), ctypes.byref(ga), ctypes.byref(aws),
-                                                      ctypes.c_void_p(st.cuda_stream)),
-                       "npom_step_explicit_adjoint")
+            status = fn(ctypes.byref(p), ctypes.byref(fa), ctypes.byref(ws["struct"]), ctypes.byref(clk),
+                        ctypes.byref(ga), ctypes.byref(aws), ctypes.c_void_p(st.cuda_stream))
+            if status == 3:
+                ws["ctrl"][4].zero_()
+                raise FloatingPointError("step adjoint: non-finite cotangent of the free-surface solve")
+            _abi.check(status, "step adjoint")
         return (None, None, None) + tuple(G.views[n].clone() for n in _abi.ADJ_STATE_FIELDS)
 
 

@@ -24,10 +24,24 @@
 
 namespace npom {
 
+// Workspace arrays that carry a cotangent inside an implicit step (written
+// by the predictor, read by the free-surface solve and the corrector): their
+// slots follow the fields in Adj.
+enum AdjWs { AW_us = 0, AW_vs, AW_den_u, AW_den_v, AW_d_baro, AW_COUNT };
+constexpr int kAdjSlots = NPOM_NFIELDS + AW_COUNT;
+
+NPOM_HD int aw_ws(int k) {
+  return k == AW_us ? NPOM_W_us
+                    : (k == AW_vs ? NPOM_W_vs : (k == AW_den_u ? NPOM_W_den_u : (k == AW_den_v ? NPOM_W_den_v : NPOM_W_d_baro)));
+}
+
 struct Adj {
-  float *G[NPOM_NFIELDS];
-  float *L[NPOM_NFIELDS];
+  float *G[kAdjSlots];
+  float *L[kAdjSlots];
 };
+
+// state array of a slot: a field or a workspace array
+NPOM_HD float *adj_fptr(const Ctx &c, int id) { return id < NPOM_NFIELDS ? c.F[id] : c.W[aw_ws(id - NPOM_NFIELDS)]; }
 
 NPOM_HD void aadd(float *p, float v) {
 #if defined(__CUDA_ARCH__)
@@ -45,6 +59,8 @@ NPOM_HD float sgnf(float x) { return x > 0.0f ? 1.0f : (x < 0.0f ? -1.0f : 0.0f)
 #define LA2(name, i, j) (a.L[NPOM_F_##name][NPOM_I2(c, i, j)])
 #define PASS3(name, i, j, k) GA3(name, i, j, k, LA3(name, i, j, k))
 #define PASS2(name, i, j) GA2(name, i, j, LA2(name, i, j))
+#define GAW(k, i, j, v) ::npom::aadd(&a.G[NPOM_NFIELDS + (k)][NPOM_I2(c, i, j)], (v))
+#define LAW(k, i, j) (a.L[NPOM_NFIELDS + (k)][NPOM_I2(c, i, j)])
 
 // ===========================================================================
 // A1: ADVCT (baroclinic.py:14-260) and the surface forcing
@@ -240,11 +256,22 @@ NPOM_HD void smag_level_adj(const Ctx &c, const Adj &a, int i, int j, int k, flo
       0.25f * (F3(u, i, j + 1, k) + F3(u, i + 1, j + 1, k) - F3(u, i, j - 1, k) - F3(u, i + 1, j - 1, k)) / dys;
   const float v_term =
       0.25f * (F3(v, i + 1, j, k) + F3(v, i + 1, j + 1, k) - F3(v, i - 1, j, k) - F3(v, i - 1, j + 1, k)) / dxs;
-  const float cc = (u_term + v_term) * c.k.sqrt_half;
-  const float mag = sqrtf(du_dx * du_dx + dv_dy * dv_dy + cc * cc);
-  if (!(mag > 0.0f)) return;  // the vector norm's gradient is zero at the origin
+  float mag, gsh;  // the norm and d(norm^2)/2 per unit of (u_term + v_term), times mag
+  if (is_explicit(c)) {
+    const float cc = (u_term + v_term) * c.k.sqrt_half;
+    mag = sqrtf(du_dx * du_dx + dv_dy * dv_dy + cc * cc);
+    gsh = cc * c.k.sqrt_half;
+  } else {
+    const float sh = u_term + v_term;
+    mag = sqrtf(du_dx * du_dx + dv_dy * dv_dy + 0.5f * (sh * sh));
+    gsh = 0.5f * sh;
+    if (c.k.aam_min > 0.0f && !(c.k.horcon * dxs * dys * mag >= c.k.aam_min)) return;  // clamped
+  }
+  // the norm's gradient is zero at the origin (explicit time_loop.py:8-14,
+  // implicit autograd.py:5-29)
+  if (!(mag > 0.0f)) return;
   const float lm = lam * c.k.horcon * dxs * dys / mag;
-  const float ldu = lm * du_dx / dxs, ldv = lm * dv_dy / dys, lcc = lm * cc * c.k.sqrt_half;
+  const float ldu = lm * du_dx / dxs, ldv = lm * dv_dy / dys, lcc = lm * gsh;
   GA3(u, i + 1, j, k, ldu);
   GA3(u, i, j, k, -ldu);
   GA3(v, i, j + 1, k, ldv);
@@ -505,6 +532,87 @@ NPOM_HD void advave_cell_adj(const Ctx &c, const Adj &a, int i, int j, float lua
   }
 }
 
+// The implicit barotropic predictor at an interior cell (core.py:795-845):
+// us/den_u (comp 0) or vs/den_v (comp 1).  The provisional forcing is
+// evaluated from the old adx2d, whose ADVAVE round trip (adx2d - advua +
+// advua) changes it by rounding only.
+NPOM_HD void a3_predictor_adj(const Ctx &c, const Adj &a, int i, int j, int comp) {
+  const float lus = LAW(comp == 0 ? AW_us : AW_vs, i, j), lden_in = LAW(comp == 0 ? AW_den_u : AW_den_v, i, j);
+  if (lus == 0.0f && lden_in == 0.0f) return;
+  const float g4 = c.k.quarter_g, al = c.k.alpha, a12 = c.k.one_m_2alpha;
+  const int oi = comp == 0 ? i - 1 : i, oj = comp == 0 ? j : j - 1;
+  const float ar = comp == 0 ? F2(aru, i, j) : F2(arv, i, j);
+  const float msk = comp == 0 ? F2(dum, i, j) : F2(dvm, i, j);
+  const float d0 = F2(d, i, j), dw = F2(d, oi, oj);
+  float s0, s1;
+  if (comp == 0) {
+    s0 = F2(va, i, j + 1) + F2(va, i, j);
+    s1 = F2(va, i - 1, j + 1) + F2(va, i - 1, j);
+  } else {
+    s0 = F2(ua, i + 1, j) + F2(ua, i, j);
+    s1 = F2(ua, i + 1, j - 1) + F2(ua, i, j - 1);
+  }
+  const float cor = 0.25f * (F2(cor, i, j) * d0 * s0 + F2(cor, oi, oj) * dw * s1);
+  const float G = g4 * (comp == 0 ? (F2(dy, i, j) + F2(dy, i - 1, j)) : (F2(dx, i, j) + F2(dx, i, j - 1)));
+  const float E = a12 * (F2(el, i, j) - F2(el, oi, oj)) + al * (F2(elb, i, j) - F2(elb, oi, oj)) + F2(e_atmos, i, j) -
+                  F2(e_atmos, oi, oj);
+  const float gu = G * (d0 + dw) * E;
+  float up;
+  if (comp == 0)
+    up = F2(adx2d, i, j) - ar * cor + gu + F2(drx2d, i, j) - ar * (-F2(wusurf, i, j) + F2(wubot, i, j));
+  else
+    up = F2(ady2d, i, j) + ar * cor + gu + F2(dry2d, i, j) - ar * (-F2(wvsurf, i, j) + F2(wvbot, i, j));
+  const float den = (F2(h, i, j) + F2(el, i, j) + F2(h, oi, oj) + F2(el, oi, oj)) * ar;
+  const float hb = F2(h, i, j) + F2(elb, i, j) + F2(h, oi, oj) + F2(elb, oi, oj);
+  const float ub = comp == 0 ? F2(uab, i, j) : F2(vab, i, j);
+  const float num = hb * ar * ub - c.k.four_dti * up;
+  const float dd = den + 1e-20f;
+  const float q = num / dd;
+  const float lq = lus * msk * msk;
+  const float lnum = lq / dd;
+  const float lden = lden_in - lq * q / dd;
+  GA2(el, i, j, lden * ar);
+  GA2(el, oi, oj, lden * ar);
+  const float tb = lnum * ar * ub;
+  GA2(elb, i, j, tb);
+  GA2(elb, oi, oj, tb);
+  if (comp == 0) GA2(uab, i, j, lnum * hb * ar);
+  else GA2(vab, i, j, lnum * hb * ar);
+  const float lup = -lnum * c.k.four_dti;
+  if (comp == 0) {
+    GA2(adx2d, i, j, lup);
+    GA2(drx2d, i, j, lup);
+    GA2(wubot, i, j, -lup * ar);
+  } else {
+    GA2(ady2d, i, j, lup);
+    GA2(dry2d, i, j, lup);
+    GA2(wvbot, i, j, -lup * ar);
+  }
+  const float lc = (comp == 0 ? -lup : lup) * ar * 0.25f;
+  GA2(d, i, j, lc * F2(cor, i, j) * s0);
+  GA2(d, oi, oj, lc * F2(cor, oi, oj) * s1);
+  const float q0 = lc * F2(cor, i, j) * d0, q1 = lc * F2(cor, oi, oj) * dw;
+  if (comp == 0) {
+    GA2(va, i, j + 1, q0);
+    GA2(va, i, j, q0);
+    GA2(va, i - 1, j + 1, q1);
+    GA2(va, i - 1, j, q1);
+  } else {
+    GA2(ua, i + 1, j, q0);
+    GA2(ua, i, j, q0);
+    GA2(ua, i + 1, j - 1, q1);
+    GA2(ua, i, j - 1, q1);
+  }
+  const float ld = lup * G * E;
+  GA2(d, i, j, ld);
+  GA2(d, oi, oj, ld);
+  const float lE = lup * G * (d0 + dw);
+  GA2(el, i, j, lE * a12);
+  GA2(el, oi, oj, -lE * a12);
+  GA2(elb, i, j, lE * al);
+  GA2(elb, oi, oj, -lE * al);
+}
+
 // A3 (explicit core): rho round trip (derivative one, rho is not moved),
 // ADVAVE, adx2d/ady2d -= advua/advva, egf, provisional utf/vtf
 NPOM_HD void phase_a3_cell_adj(const Ctx &c, const Adj &a, int i, int j) {
@@ -539,6 +647,11 @@ NPOM_HD void phase_a3_cell_adj(const Ctx &c, const Adj &a, int i, int j) {
     PASS2(fluxva, i, j);
     PASS2(tps, i, j);
   }
+  if (is_explicit(c)) return;
+  GA2(elb, i, j, LAW(AW_d_baro, i, j));
+  if (!interior(c, i, j)) return;  // us, vs, den_u, den_v are zero off the interior
+  a3_predictor_adj(c, a, i, j, 0);
+  a3_predictor_adj(c, a, i, j, 1);
 }
 
 // ===========================================================================
@@ -788,6 +901,197 @@ NPOM_HD void ext_phase3_cell_adj(const Ctx &c, const Adj &a, int i, int j, int i
 }
 
 // ===========================================================================
+// Implicit free surface (core.py:858-943, time_loop.py:269-387)
+// ===========================================================================
+
+// Shapiro filter (gamma 0) and masks of the solution: d(elf)/dx = fsm^2 on
+// the interior; d = h + elf there; ring values are constants
+NPOM_HD float imp_post_grad(const Ctx &c, const Adj &a, int i, int j) {
+  if (!interior(c, i, j)) return 0.0f;
+  const float f = F2(fsm, i, j);
+  return (LA2(elf, i, j) + LA2(d, i, j)) * f * f;
+}
+
+// one face transport fed by the predictor (rhs_fluxua / rhs_fluxva)
+NPOM_HD void imp_flux_adj(const Ctx &c, const Adj &a, int comp, int i, int j, float lam) {
+  if (lam == 0.0f || i < 1 || j < 1) return;
+  const int oi = comp == 0 ? i - 1 : i, oj = comp == 0 ? j : j - 1;
+  const float q = 0.25f * (comp == 0 ? (F2(dy, i, j) + F2(dy, i - 1, j)) : (F2(dx, i, j) + F2(dx, i, j - 1)));
+  const float sv = comp == 0 ? ld(c.W[NPOM_W_us] + NPOM_I2(c, i, j)) : ld(c.W[NPOM_W_vs] + NPOM_I2(c, i, j));
+  GAW(comp == 0 ? AW_us : AW_vs, i, j, lam * q * (F2(d, i, j) + F2(d, oi, oj)));
+  const float t = lam * q * sv;
+  GA2(d, i, j, t);
+  GA2(d, oi, oj, t);
+}
+
+// rhs and stored transports of one cell, given lambda = A^-T g (lam) and
+// the depth gradient of the solve (gd)
+NPOM_HD void imp_rhs_cell_adj(const Ctx &c, const Adj &a, int i, int j, const float *lam, const float *gd) {
+  const size_t o = NPOM_I2(c, i, j);
+  GA2(d, i, j, ld(gd + o));
+  imp_flux_adj(c, a, 0, i, j, LA2(fluxua, i, j));
+  imp_flux_adj(c, a, 1, i, j, LA2(fluxva, i, j));
+  if (!interior(c, i, j)) return;
+  const float l = ld(lam + o);
+  GA2(elb, i, j, l);
+  const float ldiv = -c.k.two_dti * l / (F2(art, i, j) + 1e-20f);
+  imp_flux_adj(c, a, 0, i + 1, j, ldiv);
+  imp_flux_adj(c, a, 0, i, j, -ldiv);
+  imp_flux_adj(c, a, 1, i, j + 1, ldiv);
+  imp_flux_adj(c, a, 1, i, j, -ldiv);
+}
+
+// The terms of the eta-solve adjoint (implicit_p0_fixed/core.py:231-252,
+// 645-675): relative cell area, and the face terms of the depth adjoint.
+NPOM_HD float adj_area(const Ctx &c, int i, int j) {
+  return interior(c, i, j) ? F2(art, i, j) / F2(art, 1, 1) : 1.0f;
+}
+NPOM_HD float adj_lam(const Ctx &c, const float *sol, float scale, int i, int j) {
+  const size_t o = NPOM_I2(c, i, j);
+  const float lam = (ld(sol + o) * adj_area(c, i, j)) * scale;
+  return (lam * c.k.implicit_coeff) * W2(inv_art, i, j);
+}
+NPOM_HD float adj_east(const Ctx &c, const float *x, const float *sol, float scale, int i, int j) {
+  return (((0.5f * adj_lam(c, sol, scale, i, j)) * (ld(x + NPOM_I2(c, i + 1, j)) - ld(x + NPOM_I2(c, i, j)))) *
+          W2(ce, i, j)) *
+         F2(dum, i + 1, j);
+}
+NPOM_HD float adj_west(const Ctx &c, const float *x, const float *sol, float scale, int i, int j) {
+  return (((0.5f * adj_lam(c, sol, scale, i, j)) * (ld(x + NPOM_I2(c, i, j)) - ld(x + NPOM_I2(c, i - 1, j)))) *
+          W2(cw, i, j)) *
+         F2(dum, i, j);
+}
+NPOM_HD float adj_north(const Ctx &c, const float *x, const float *sol, float scale, int i, int j) {
+  return (((0.5f * adj_lam(c, sol, scale, i, j)) * (ld(x + NPOM_I2(c, i, j + 1)) - ld(x + NPOM_I2(c, i, j)))) *
+          W2(cn, i, j)) *
+         F2(dvm, i, j + 1);
+}
+NPOM_HD float adj_south(const Ctx &c, const float *x, const float *sol, float scale, int i, int j) {
+  return (((0.5f * adj_lam(c, sol, scale, i, j)) * (ld(x + NPOM_I2(c, i, j)) - ld(x + NPOM_I2(c, i, j - 1)))) *
+          W2(cs, i, j)) *
+         F2(dvm, i, j);
+}
+// grad_d = -(depth adjoint): the reference scatters eight face terms with
+// in-place adds in a fixed statement order; each cell gathers the same
+// terms in that order (east of i-1, east, west, west of i+1, north of j-1,
+// north, south, south of j+1)
+NPOM_HD float adj_grad_d_cell(const Ctx &c, const float *x, const float *sol, float scale, int i, int j) {
+  float acc = 0.0f;
+  if (interior(c, i - 1, j)) acc = acc + -adj_east(c, x, sol, scale, i - 1, j);
+  if (interior(c, i, j)) {
+    acc = acc + -adj_east(c, x, sol, scale, i, j);
+    acc = acc + adj_west(c, x, sol, scale, i, j);
+  }
+  if (interior(c, i + 1, j)) acc = acc + adj_west(c, x, sol, scale, i + 1, j);
+  if (interior(c, i, j - 1)) acc = acc + -adj_north(c, x, sol, scale, i, j - 1);
+  if (interior(c, i, j)) {
+    acc = acc + -adj_north(c, x, sol, scale, i, j);
+    acc = acc + adj_south(c, x, sol, scale, i, j);
+  }
+  if (interior(c, i, j + 1)) acc = acc + adj_south(c, x, sol, scale, i, j + 1);
+  return -acc;
+}
+
+// I5: corrector with closed-basin bcond 2, etf, Robert-Asselin filter,
+// shifts, egf and endpoint transports (core.py:918-943,
+// time_loop.py:309-387)
+NPOM_HD void phase_i5_cell_adj(const Ctx &c, const Adj &a, int i, int j) {
+  const float hs = c.k.half_smoth, ohs = 1.0f - 2.0f * hs;
+  const bool inner = interior(c, i, j);
+  const float elf0 = F2(elf, i, j), dn = F2(h, i, j) + elf0;
+  const float dum = F2(dum, i, j), dvm = F2(dvm, i, j);
+  // forward values
+  float uaf = 0.0f, vaf = 0.0f, Nu = 0.0f, Nv = 0.0f, dfu = 0.0f, dfv = 0.0f;
+  float Gu = 0.0f, Gv = 0.0f, Su = 0.0f, Sv = 0.0f, Du = 0.0f, Dv = 0.0f;
+  const float g4 = c.k.quarter_g, al = c.k.alpha;
+  if (inner) {
+    const float h0 = F2(h, i, j);
+    Gu = g4 * (F2(dy, i, j) + F2(dy, i - 1, j));
+    Gv = g4 * (F2(dx, i, j) + F2(dx, i, j - 1));
+    Su = (h0 + elf0) + (F2(h, i - 1, j) + F2(elf, i - 1, j));
+    Sv = (h0 + elf0) + (F2(h, i, j - 1) + F2(elf, i, j - 1));
+    Du = elf0 - F2(elf, i - 1, j);
+    Dv = elf0 - F2(elf, i, j - 1);
+    const float gu = Gu * Su * al * Du, gv = Gv * Sv * al * Dv;
+    dfu = (h0 + elf0 + F2(h, i - 1, j) + F2(elf, i - 1, j)) * F2(aru, i, j) + 1e-20f;
+    dfv = (h0 + elf0 + F2(h, i, j - 1) + F2(elf, i, j - 1)) * F2(arv, i, j) + 1e-20f;
+    Nu = W2(us, i, j) * W2(den_u, i, j) - c.k.four_dti * gu;
+    Nv = W2(vs, i, j) * W2(den_v, i, j) - c.k.four_dti * gv;
+    uaf = (Nu / dfu * dum) * dum;
+    vaf = (Nv / dfv * dvm) * dvm;
+  }
+  const float ua = F2(ua, i, j), va = F2(va, i, j);
+  const float uaf_f = ua + hs * (F2(uab, i, j) - 2.0f * ua + uaf);
+  const float vaf_f = va + hs * (F2(vab, i, j) - 2.0f * va + vaf);
+  // cotangents of the outputs
+  float luaf = LA2(uaf, i, j) + LA2(ua, i, j), lvaf = LA2(vaf, i, j) + LA2(va, i, j);
+  float luaf_f = LA2(uab, i, j), lvaf_f = LA2(vab, i, j);
+  float lel_f = LA2(elb, i, j) + 0.5f * LA2(egf, i, j);
+  float lelf = LA2(etf, i, j) * F2(fsm, i, j) + LA2(el, i, j) + LA2(d, i, j) + 0.5f * LA2(egf, i, j);
+  if (i >= 1) {
+    const float lt = 0.25f * LA2(utf, i, j);
+    const float dsum_new = dn + (F2(h, i - 1, j) + F2(elf, i - 1, j));
+    const float dsum_baro = W2(d_baro, i, j) + W2(d_baro, i - 1, j);
+    luaf_f += lt * dsum_baro;
+    luaf += lt * dsum_new;
+    lelf += lt * uaf;
+    GA2(elf, i - 1, j, lt * uaf);
+    GAW(AW_d_baro, i, j, lt * uaf_f);
+    GAW(AW_d_baro, i - 1, j, lt * uaf_f);
+  } else {
+    PASS2(utf, i, j);
+  }
+  if (j >= 1) {
+    const float lt = 0.25f * LA2(vtf, i, j);
+    const float dsum_new = dn + (F2(h, i, j - 1) + F2(elf, i, j - 1));
+    const float dsum_baro = W2(d_baro, i, j) + W2(d_baro, i, j - 1);
+    lvaf_f += lt * dsum_baro;
+    lvaf += lt * dsum_new;
+    lelf += lt * vaf;
+    GA2(elf, i, j - 1, lt * vaf);
+    GAW(AW_d_baro, i, j, lt * vaf_f);
+    GAW(AW_d_baro, i, j - 1, lt * vaf_f);
+  } else {
+    PASS2(vtf, i, j);
+  }
+  // Robert-Asselin filters
+  GA2(ua, i, j, luaf_f * ohs);
+  GA2(uab, i, j, luaf_f * hs);
+  luaf += luaf_f * hs;
+  GA2(va, i, j, lvaf_f * ohs);
+  GA2(vab, i, j, lvaf_f * hs);
+  lvaf += lvaf_f * hs;
+  GA2(el, i, j, lel_f * ohs);
+  GA2(elb, i, j, lel_f * hs);
+  lelf += lel_f * hs;
+  // corrector (the ring is zero)
+  if (inner) {
+    for (int comp = 0; comp < 2; ++comp) {
+      const float m = comp == 0 ? dum : dvm;
+      const float lq = (comp == 0 ? luaf : lvaf) * m * m;
+      if (lq == 0.0f) continue;
+      const float df = comp == 0 ? dfu : dfv, N = comp == 0 ? Nu : Nv;
+      const float lN = lq / df, ldf = -lq * (N / df) / df;
+      if (comp == 0) {
+        GAW(AW_us, i, j, lN * W2(den_u, i, j));
+        GAW(AW_den_u, i, j, lN * W2(us, i, j));
+      } else {
+        GAW(AW_vs, i, j, lN * W2(den_v, i, j));
+        GAW(AW_den_v, i, j, lN * W2(vs, i, j));
+      }
+      const int oi = comp == 0 ? i - 1 : i, oj = comp == 0 ? j : j - 1;
+      const float ar = comp == 0 ? F2(aru, i, j) : F2(arv, i, j);
+      const float Gc = comp == 0 ? Gu : Gv, S = comp == 0 ? Su : Sv, D = comp == 0 ? Du : Dv;
+      const float lg = -lN * c.k.four_dti;
+      const float lS = lg * Gc * al * D, lD = lg * Gc * S * al;
+      lelf += lS + lD + ldf * ar;
+      GA2(elf, oi, oj, lS - lD + ldf * ar);
+    }
+  }
+  GA2(elf, i, j, lelf);
+}
+
+// ===========================================================================
 // B1: barotropic fix (time_loop.py:440-477)
 // ===========================================================================
 NPOM_HD void phase_b1_column_adj(const Ctx &c, const Adj &a, int i, int j) {
@@ -843,8 +1147,10 @@ NPOM_HD void vertvl_yflux_adj(const Ctx &c, const Adj &a, int i, int j, int k, f
 NPOM_HD void phase_b2a_column_adj(const Ctx &c, const Adj &a, int i, int j) {
   const int kb = c.kb, kbm1 = kb - 1;
   const float fsm = F2(fsm, i, j);
+  // bcond 5: explicit masks levels < kb-1, the closed basin every level
+  const int kend = is_explicit(c) ? kbm1 : kb;
   float lw[KMAX];
-  for (int k = 0; k < kb; ++k) lw[k] = LA3(w, i, j, k) * (k < kbm1 ? fsm : 1.0f);
+  for (int k = 0; k < kb; ++k) lw[k] = LA3(w, i, j, k) * (k < kend ? fsm : 1.0f);
   if (!interior(c, i, j)) {
     for (int k = 0; k < kb; ++k) GA3(w, i, j, k, lw[k]);
     return;
@@ -1061,7 +1367,8 @@ NPOM_HD void phase_b3_column_adj(const Ctx &c, const Adj &a, int i, int j) {
   gg2[0] = 0.0f;
   for (int k = 1; k < kbm1; ++k) {
     const float zk = F1(z, k);
-    wall0[k] = 1.0f / (fabsf(zk - z0) + 1e-20f) + 1.0f / (fabsf(zk - zb) + 1e-20f);
+    const float weps = is_explicit(c) ? 1e-20f : 1e-8f;
+    wall0[k] = 1.0f / (fabsf(zk - z0) + weps) + 1.0f / (fabsf(zk - zb) + weps);
     wallv[k] = wall0[k] * l[k] / (dh * kappa);
     const float dtefk = dtef[k] * (1.0f + e2 * (wallv[k] * wallv[k]));
     den2[k] = A[k] + C[k] * (1.0f - ee2[k - 1]) - (dti2 * dtefk + 1.0f);
@@ -1278,8 +1585,10 @@ NPOM_HD void phase_b4_point_adj(const Ctx &c, const Adj &a, int i, int j, int k)
   if (!edge) {
     PASS3(km, i, j, k);
     PASS3(kh, i, j, k);
-    PASS3(uf, i, j, k);
-    PASS3(vf, i, j, k);
+    if (is_explicit(c)) {
+      PASS3(uf, i, j, k);
+      PASS3(vf, i, j, k);
+    }
     return;
   }
   for (int comp = 0; comp < 2; ++comp) {
@@ -1298,6 +1607,7 @@ NPOM_HD void phase_b4_point_adj(const Ctx &c, const Adj &a, int i, int j, int k)
     }
     aadd(&a.G[fld][NPOM_I3(c, si, sj, k)], lam * f);
   }
+  if (!is_explicit(c)) return;  // uf/vf are not moved for the closed basin
   // bcond 6: the last side in the order east, west, north, south wins
   const float lu = LA3(uf, i, j, k), lv = LA3(vf, i, j, k);
   const float dti = c.k.dti, small = c.k.small;
@@ -1453,6 +1763,14 @@ NPOM_HD void phase_b5_point_adj(const Ctx &c, const Adj &a, int i, int j, int k)
   }
   advt1_point_adj(c, a, NPOM_F_t, NPOM_F_tb, NPOM_F_tclim, i, j, k, LA3(uf, i, j, k));
   advt1_point_adj(c, a, NPOM_F_s, NPOM_F_sb, NPOM_F_sclim, i, j, k, LA3(vf, i, j, k));
+  if (!is_explicit(c) && c.k.has_vmix) {
+    // clamp(x, 0, vmix): the gradient passes where 0 <= x <= vmix
+    const float vm = c.k.vmix;
+    const float kh = F3(kh, i, j, k), km = F3(km, i, j, k), kq = F3(kq, i, j, k);
+    GA3(kh, i, j, k, (kh >= 0.0f && kh <= vm) ? LA3(kh, i, j, k) : 0.0f);
+    GA3(km, i, j, k, (km >= 0.0f && km <= vm) ? LA3(km, i, j, k) : 0.0f);
+    GA3(kq, i, j, k, (kq >= 0.0f && kq <= vm) ? LA3(kq, i, j, k) : 0.0f);
+  }
   const float fsm = F2(fsm, i, j), hs = c.k.half_smoth, ohs = 1.0f - 2.0f * hs;
   const float lq2b = LA3(q2b, i, j, k), lq2lb = LA3(q2lb, i, j, k);
   GA3(q2, i, j, k, lq2b * ohs);
@@ -1650,7 +1968,7 @@ NPOM_HD void phase_b6_column_adj(const Ctx &c, const Adj &a, int i, int j) {
     lu[k] = LA3(uf, i, j, k);
     lv[k] = LA3(vf, i, j, k);
   }
-  if (i == 0 || i == c.im - 1 || j == 0 || j == c.jm - 1) {
+  if (is_explicit(c) && (i == 0 || i == c.im - 1 || j == 0 || j == c.jm - 1)) {
     for (int k = 0; k < kbm1; ++k) {
       bcond4_explicit_level_adj(c, a, i, j, k, lu[k], lv[k]);
       lu[k] = 0.0f;
@@ -1687,15 +2005,30 @@ NPOM_HD void dens_point_adj(const Ctx &c, float t, float s, int i, int j, int k,
   ds_ = f * (P2 + P3 * dS15 + 2.0f * 4.8314e-4f * sr + dQ * 1.34f);
 }
 
+// explicit: T/S = uf/vf * fsm; closed basin (Shapiro gamma 0): the edge
+// values copy the bcond 4 source cell, then T/S = value * fsm while the
+// filter sees the unmasked value
 NPOM_HD void phase_b7_point_adj(const Ctx &c, const Adj &a, int i, int j, int k) {
-  const int kb = c.kb;
+  const int im = c.im, jm = c.jm, kb = c.kb;
   const float fsm = F2(fsm, i, j), hs = c.k.half_smoth, ohs = 1.0f - 2.0f * hs;
+  int si = i, sj = j;
+  float fmask = fsm;  // d(ufv)/d(uf at the source): fsm for the explicit mask
+  if (!is_explicit(c)) {
+    fmask = 1.0f;
+    if (sj == 0) sj = 1;
+    if (sj == jm - 1) sj = jm - 2;
+    if (si == 0) si = 1;
+    if (si == im - 1) si = im - 2;
+  }
+  const float ufv = F3(uf, si, sj, k) * fmask, vfv = F3(vf, si, sj, k) * fmask;
+  // tn = ufv (explicit) or ufv * fsm (closed basin)
+  const float tmask = is_explicit(c) ? 1.0f : fsm;
   float lt = LA3(t, i, j, k), ls = LA3(s, i, j, k);
   if (k < kb - 1) {
     const float lr = LA3(rho, i, j, k);
     if (lr != 0.0f) {
       float dtn, dsn;
-      dens_point_adj(c, F3(uf, i, j, k) * fsm, F3(vf, i, j, k) * fsm, i, j, k, dtn, dsn);
+      dens_point_adj(c, ufv * tmask, vfv * tmask, i, j, k, dtn, dsn);
       lt += lr * dtn;
       ls += lr * dsn;
     }
@@ -1705,10 +2038,10 @@ NPOM_HD void phase_b7_point_adj(const Ctx &c, const Adj &a, int i, int j, int k)
   const float ltb = LA3(tb, i, j, k), lsb = LA3(sb, i, j, k);
   GA3(t, i, j, k, ltb * ohs);
   GA3(tb, i, j, k, ltb * hs);
-  GA3(uf, i, j, k, (ltb * hs + lt) * fsm);
+  GA3(uf, si, sj, k, (ltb * hs + lt * tmask) * fmask);
   GA3(s, i, j, k, lsb * ohs);
   GA3(sb, i, j, k, lsb * hs);
-  GA3(vf, i, j, k, (lsb * hs + ls) * fsm);
+  GA3(vf, si, sj, k, (lsb * hs + ls * tmask) * fmask);
 }
 
 // ===========================================================================
@@ -1994,7 +2327,7 @@ NPOM_HD void phase_b8_column_adj(const Ctx &c, const Adj &a, int i, int j) {
     luo[k] = LA3(uf, i, j, k);
     lvo[k] = LA3(vf, i, j, k);
   }
-  bcond3_explicit_edge_adj(c, a, i, j, luo, lvo);
+  if (is_explicit(c)) bcond3_explicit_edge_adj(c, a, i, j, luo, lvo);
   profuv_column_adj(c, a, 0, i, j, luo, LA2(wubot, i, j), 0.0f, lfin);
   if (inner)
     for (int k = 0; k < kb - 1; ++k) advu_point_adj(c, a, i, j, k, lfin[k]);
@@ -2010,8 +2343,12 @@ NPOM_HD void phase_b9_column_adj(const Ctx &c, const Adj &a, int i, int j) {
   const int kb = c.kb, kbm1 = kb - 1;
   if (c.do_internal) {
     const float hs = c.k.half_smoth;
+    const bool ring = (i == 0 || i == c.im - 1 || j == 0 || j == c.jm - 1);
     for (int comp = 0; comp < 2; ++comp) {
       const float mask = comp == 0 ? F2(dum, i, j) : F2(dvm, i, j);
+      // closed basin: the ring is zero and the filtered value is masked
+      const float fmask = (!is_explicit(c) && ring) ? 0.0f : mask;
+      const float bmask = is_explicit(c) ? 1.0f : mask;
       const int fa = comp == 0 ? NPOM_F_u : NPOM_F_v;
       const int fb = comp == 0 ? NPOM_F_ub : NPOM_F_vb;
       const int ff = comp == 0 ? NPOM_F_uf : NPOM_F_vf;
@@ -2021,7 +2358,7 @@ NPOM_HD void phase_b9_column_adj(const Ctx &c, const Adj &a, int i, int j) {
       for (int k = 0; k < kb; ++k) {
         lfnew[k] = a.L[fa][o + k] + a.L[ff][o + k];
         lterm[k] = 0.0f;
-        const float lfb = a.L[fb][o + k];
+        const float lfb = a.L[fb][o + k] * bmask;
         aadd(a.G[fa] + o + k, lfb);
         if (k < kbm1) {
           lterm[k] += hs * lfb;
@@ -2034,7 +2371,7 @@ NPOM_HD void phase_b9_column_adj(const Ctx &c, const Adj &a, int i, int j) {
         aadd(a.G[fb] + o + k, lterm[k]);
         aadd(a.G[fa] + o + k, -2.0f * lterm[k]);
       }
-      for (int k = 0; k < kb; ++k) aadd(a.G[ff] + o + k, lfnew[k] * mask);
+      for (int k = 0; k < kb; ++k) aadd(a.G[ff] + o + k, lfnew[k] * fmask);
     }
   }
   GA2(egf, i, j, LA2(egb, i, j));
@@ -2050,6 +2387,8 @@ NPOM_HD void phase_b9_column_adj(const Ctx &c, const Adj &a, int i, int j) {
 #undef LA2
 #undef PASS3
 #undef PASS2
+#undef GAW
+#undef LAW
 
 }  // namespace npom
 
@@ -2064,7 +2403,8 @@ NPOM_HD void phase_b9_column_adj(const Ctx &c, const Adj &a, int i, int j) {
 namespace npom {
 
 enum AdjPhase {
-  AP_A1 = 0, AP_A2, AP_A3, AP_E1, AP_E2, AP_E3, AP_B1, AP_B2A, AP_B2B, AP_B3, AP_B4, AP_B5, AP_B6, AP_B7, AP_B8, AP_B9
+  AP_A1 = 0, AP_A2, AP_A3, AP_E1, AP_E2, AP_E3, AP_B1, AP_B2A, AP_B2B, AP_B3, AP_B4, AP_B5, AP_B6, AP_B7, AP_B8, AP_B9,
+  AP_EI, AP_I5
 };
 constexpr int kAdjMaxFields = 16;
 
@@ -2146,7 +2486,17 @@ inline int adj_step_plan(const Ctx &c, AdjPhaseRec *out, int cap, size_t *save_f
   for (int f : {NPOM_F_advua, NPOM_F_advva, NPOM_F_fluxua, NPOM_F_fluxva, NPOM_F_tps, NPOM_F_adx2d, NPOM_F_ady2d,
                 NPOM_F_egf, NPOM_F_utf, NPOM_F_vtf})
     add(r, f, 1);
-  const int isplit = c.k.isplit;
+  const bool imp = c.k.core == NPOM_CORE_IMPLICIT;
+  if (imp) {
+    for (int w = 0; w < AW_COUNT; ++w) add(r, NPOM_NFIELDS + w, 1);
+    r = begin(AP_EI, 0, 0);
+    for (int f : {NPOM_F_fluxua, NPOM_F_fluxva, NPOM_F_elf, NPOM_F_d}) add(r, f, 1);
+    r = begin(AP_I5, 0, 0);
+    for (int f : {NPOM_F_uaf, NPOM_F_vaf, NPOM_F_etf, NPOM_F_elb, NPOM_F_el, NPOM_F_d, NPOM_F_uab, NPOM_F_ua,
+                  NPOM_F_vab, NPOM_F_va, NPOM_F_egf, NPOM_F_utf, NPOM_F_vtf})
+      add(r, f, 1);
+  }
+  const int isplit = imp ? 0 : c.k.isplit;
   for (int iext = 1; iext <= isplit; ++iext) {
     const int adv = (iext % c.k.ispadv) == 0;
     for (int ph = 1; ph <= 3; ++ph) {
@@ -2168,11 +2518,18 @@ inline int adj_step_plan(const Ctx &c, AdjPhaseRec *out, int cap, size_t *save_f
     r = begin(AP_B3, 0, 0);
     for (int f : {NPOM_F_l, NPOM_F_kq, NPOM_F_km, NPOM_F_kh, NPOM_F_uf, NPOM_F_vf}) add(r, f, 1);
     r = begin(AP_B4, 0, 0);
-    for (int f : {NPOM_F_km, NPOM_F_kh, NPOM_F_uf, NPOM_F_vf}) add(r, f, 1);
+    add(r, NPOM_F_km, 1);
+    add(r, NPOM_F_kh, 1);
+    if (!imp) {
+      add(r, NPOM_F_uf, 1);
+      add(r, NPOM_F_vf, 1);
+    }
     r = begin(AP_B5, 0, 0);
     for (int f : {NPOM_F_q2b, NPOM_F_q2, NPOM_F_q2lb, NPOM_F_q2l, NPOM_F_uf, NPOM_F_vf, NPOM_F_t, NPOM_F_tb,
                   NPOM_F_s, NPOM_F_sb})
       add(r, f, 1);
+    if (imp && c.k.has_vmix)
+      for (int f : {NPOM_F_kh, NPOM_F_km, NPOM_F_kq}) add(r, f, 1);
     r = begin(AP_B6, 0, 0);
     for (int f : {NPOM_F_uf, NPOM_F_vf, NPOM_F_tps}) add(r, f, 1);
     r = begin(AP_B7, 0, 0);
@@ -2188,11 +2545,13 @@ inline int adj_step_plan(const Ctx &c, AdjPhaseRec *out, int cap, size_t *save_f
   return np;
 }
 
-// Settings the adjoint covers: the explicit core in mode 3 with centred
-// tracer advection and surface flux (nbc 1) or value (nbc 3) conditions.
+// Settings the adjoint covers: mode 3 with centred tracer advection and
+// surface flux (nbc 1) or value (nbc 3) conditions; for the implicit core
+// the production Shapiro filters (gamma 0).
 inline bool adj_supported(const npom_params *p) {
-  return p->core == NPOM_CORE_EXPLICIT && p->mode == 3 && p->nadv == 1 && (p->nbct == 1 || p->nbct == 3) &&
-         (p->nbcs == 1 || p->nbcs == 3);
+  const bool base = p->mode == 3 && p->nadv == 1 && (p->nbct == 1 || p->nbct == 3) && (p->nbcs == 1 || p->nbcs == 3);
+  if (p->core == NPOM_CORE_EXPLICIT) return base;
+  return base && p->core == NPOM_CORE_IMPLICIT && p->barotropic_shapiro == 0.0 && p->tracer_shapiro == 0.0;
 }
 
 }  // namespace npom

@@ -54,6 +54,7 @@ __global__ void __launch_bounds__(kThreads) k_adj_cells(Ctx c, Adj a, int phase,
   if (q >= n) return;
   const int i = q / c.jm, j = q % c.jm;
   if (phase == AP_A3) phase_a3_cell_adj(c, a, i, j);
+  else if (phase == AP_I5) phase_i5_cell_adj(c, a, i, j);
   else if (phase == AP_E1) ext_phase1_cell_adj(c, a, i, j, adv != 0);
   else if (phase == AP_E2) ext_phase2_cell_adj(c, a, i, j, iext);
   else ext_phase3_cell_adj(c, a, i, j, iext);
@@ -153,13 +154,55 @@ int plan_adj_ext(const Ctx &c) {
   return cluster_ctas(f) <= cluster_ctas(r) ? f : r;
 }
 
+// Implicit free surface, forward: the solution x of the PCG (run without its
+// post step) is kept in xs; then the Shapiro filter (gamma 0) and masks of
+// the post step, d = h + elf, ring values -- the same arithmetic as
+// k_pcg_cluster's post step.
+__global__ void __launch_bounds__(kThreads) k_imp_post(Ctx c, const float *xs) {
+  const int n = c.im * c.jm;
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int i = q / c.jm, j = q % c.jm;
+  if (!interior(c, i, j)) {
+    P2(elf, i, j) = 0.0f;
+    P2(d, i, j) = F2(h, i, j);
+    return;
+  }
+  const int jm = c.jm;
+  const float x0 = xs[q];
+  const float xn = (j + 1 < jm - 1) ? xs[q + 1] : 0.0f;
+  const float xsv = (j - 1 > 0) ? xs[q - 1] : 0.0f;
+  const float xe = (i + 1 < c.im - 1) ? xs[q + jm] : 0.0f;
+  const float xw = (i - 1 > 0) ? xs[q - jm] : 0.0f;
+  const float smv = x0 + c.k.bshap_q * (xe + xw + xn + xsv - 4.0f * x0);
+  const float fsm = F2(fsm, i, j);
+  const float ev = (smv * fsm) * fsm;
+  if (!(fabsf(ev) <= 3.0e38f)) atomicOr(c.status, NPOM_DEV_NONFINITE);
+  P2(d, i, j) = F2(h, i, j) + ev;
+  P2(elf, i, j) = ev;
+}
+
+__global__ void __launch_bounds__(kThreads) k_imp_post_grad(Ctx c, Adj a, float *g) {
+  const int n = c.im * c.jm;
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  g[q] = imp_post_grad(c, a, q / c.jm, q % c.jm);
+}
+
+__global__ void __launch_bounds__(kThreads) k_imp_rhs_adj(Ctx c, Adj a, const float *lam, const float *gd) {
+  const int n = c.im * c.jm;
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  imp_rhs_cell_adj(c, a, q / c.jm, q % c.jm, lam, gd);
+}
+
 // save[off_e ...] = F[fld_e] for every field e of a phase (blockIdx.y = e)
 __global__ void k_save_fields(Ctx c, AdjPhaseRec r, float *save) {
   const int e = blockIdx.y;
   if (e >= r.n) return;
   const int f = r.fld[e];
   const size_t n = adj_field_len(c, f);
-  const float *src = c.F[f];
+  const float *src = adj_fptr(c, f);
   float *dst = save + r.off[e];
   for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
     dst[q] = src[q];
@@ -172,7 +215,7 @@ __global__ void k_restore_move(Ctx c, Adj a, AdjPhaseRec r, const float *save) {
   const int f = r.fld[e];
   const size_t n = adj_field_len(c, f);
   const float *src = save + r.off[e];
-  float *dst = c.F[f];
+  float *dst = adj_fptr(c, f);
   const bool mv = r.move[e] != 0;
   float *g = a.G[f], *l = a.L[f];
   for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
@@ -191,8 +234,26 @@ dim3 field_list_grid(const Ctx &c, const AdjPhaseRec &r) {
   return dim3((unsigned)std::max<size_t>(blocks, 1), (unsigned)std::max(r.n, 1));
 }
 
-void launch_fwd_phase(const Ctx &c, const AdjPhaseRec &r, cudaStream_t s) {
+// scratch planes of one step adjoint, after the plan's save records:
+// G and L of the workspace slots, the PCG solution, g, lambda, grad d
+constexpr int kAdjScratchPlanes = 2 * AW_COUNT + 4;
+
+struct ImpScratch {
+  float *xs, *g, *lam, *gd;
+};
+
+void launch_fwd_phase(const Ctx &c, const AdjPhaseRec &r, const PcgPlan &pplan, const ImpScratch &is,
+                      cudaStream_t s) {
+  const int ncell = c.im * c.jm;
+  const unsigned gx = (unsigned)((ncell + kThreads - 1) / kThreads);
   switch (r.phase) {
+    case AP_EI:
+      cudaMemsetAsync(c.sync, 0, 4 * sizeof(unsigned int), s);
+      run_pcg(c, pplan, 1, 0, s);
+      cudaMemcpyAsync(is.xs, c.F[NPOM_F_elf], (size_t)ncell * sizeof(float), cudaMemcpyDeviceToDevice, s);
+      k_imp_post<<<gx, kThreads, 0, s>>>(c, is.xs);
+      break;
+    case AP_I5: launch_cells<XP_I5>(c, s); break;
     case AP_A1: launch_a1(c, s); break;
     case AP_A2: launch_cols<CP_A2>(c, s); break;
     case AP_A3: launch_cells<XP_A3>(c, s); break;
@@ -216,12 +277,23 @@ void launch_fwd_phase(const Ctx &c, const AdjPhaseRec &r, cudaStream_t s) {
   }
 }
 
-void launch_adj_phase(const Ctx &c, const Adj &a, const AdjPhaseRec &r, cudaStream_t s) {
+npom_status launch_adj_phase(const npom_params *p, const npom_workspace *ws, const Ctx &c, const Adj &a,
+                             const AdjPhaseRec &r, const ImpScratch &is, cudaStream_t s) {
   const size_t np = (size_t)c.im * c.jm * c.kb;
   const int ncol = c.im * c.jm;
   const unsigned gp = (unsigned)((np + kThreads - 1) / kThreads), gx = (unsigned)((ncol + kThreads - 1) / kThreads);
   const unsigned gc = (unsigned)((ncol + 127) / 128);
   switch (r.phase) {
+    case AP_EI: {
+      // elf/d of the post step -> g = dJ/dx; the solve's adjoint gives
+      // lambda = A^-T g and dJ/dd; then the rhs and the transports
+      k_imp_post_grad<<<gx, kThreads, 0, s>>>(c, a, is.g);
+      const npom_status st = npom_pcg_adjoint(p, c.F, ws, is.g, is.xs, c.F[NPOM_F_d], is.lam, is.gd, (void *)s);
+      if (st != NPOM_OK) return st;
+      k_imp_rhs_adj<<<gx, kThreads, 0, s>>>(c, a, is.lam, is.gd);
+      break;
+    }
+    case AP_I5: k_adj_cells<<<gx, kThreads, 0, s>>>(c, a, r.phase, 0, 0); break;
     case AP_A1: k_adj_points<AP_A1><<<gp, kThreads, 0, s>>>(c, a); break;
     case AP_A2: k_adj_cols<AP_A2><<<gc, 128, 0, s>>>(c, a); break;
     case AP_A3:
@@ -239,13 +311,14 @@ void launch_adj_phase(const Ctx &c, const Adj &a, const AdjPhaseRec &r, cudaStre
     case AP_B8: k_adj_cols<AP_B8><<<gc, 128, 0, s>>>(c, a); break;
     case AP_B9: k_adj_cols<AP_B9><<<gc, 128, 0, s>>>(c, a); break;
   }
+  return NPOM_OK;
 }
 
-npom_status run_explicit_adjoint(const npom_params *p, float *const *fields, const npom_workspace *ws,
-                                 const npom_clock *clk, float *const *grads, const npom_adjoint_ws *aws,
-                                 cudaStream_t s) {
+npom_status run_step_adjoint(const npom_params *p, float *const *fields, const npom_workspace *ws,
+                             const npom_clock *clk, float *const *grads, const npom_adjoint_ws *aws, int core,
+                             cudaStream_t s) {
   if (!check_args_dev(p, fields, ws) || !clk || clk->nsteps != 1 || !grads || !aws || !aws->save) return NPOM_ERR_ARG;
-  if (!adj_supported(p) || p->isplit > 4096) return NPOM_ERR_ARG;
+  if (p->core != core || !adj_supported(p) || p->isplit > 4096) return NPOM_ERR_ARG;
   for (int f = 0; f < NPOM_NFIELDS; ++f)
     if (!grads[f] || !aws->lam[f]) return NPOM_ERR_ARG;
   Ctx c = make_ctx(p, fields, ws);
@@ -259,10 +332,28 @@ npom_status run_explicit_adjoint(const npom_params *p, float *const *fields, con
     a.G[f] = grads[f];
     a.L[f] = aws->lam[f];
   }
-  std::vector<AdjPhaseRec> plan((size_t)(16 + 3 * p->isplit));
+  std::vector<AdjPhaseRec> plan((size_t)(18 + 3 * p->isplit));
   size_t need = 0;
   const int np = adj_step_plan(c, plan.data(), (int)plan.size(), &need);
-  if (need > aws->save_floats) return NPOM_ERR_ARG;
+  const size_t ncell = (size_t)c.im * c.jm;
+  if (need + kAdjScratchPlanes * ncell > aws->save_floats) return NPOM_ERR_ARG;
+  float *scratch = aws->save + need;
+  for (int w = 0; w < AW_COUNT; ++w) {
+    a.G[NPOM_NFIELDS + w] = scratch + (size_t)w * ncell;
+    a.L[NPOM_NFIELDS + w] = scratch + (size_t)(AW_COUNT + w) * ncell;
+  }
+  ImpScratch is;
+  is.xs = scratch + (size_t)(2 * AW_COUNT) * ncell;
+  is.g = is.xs + ncell;
+  is.lam = is.g + ncell;
+  is.gd = is.lam + ncell;
+  // workspace cotangents live inside one step
+  if (cudaMemsetAsync(scratch, 0, (size_t)AW_COUNT * ncell * sizeof(float), s) != cudaSuccess) return NPOM_ERR_CUDA;
+  PcgPlan pplan{};
+  if (core == NPOM_CORE_IMPLICIT) {
+    if (plan_pcg(c, &pplan) != cudaSuccess) return NPOM_ERR_CUDA;
+    launch_cells<XP_COEF>(c, s);
+  }
   // the external-subcycle records sit together in the plan: [e0, e1)
   int e0 = np, e1 = np;
   for (int q = 0; q < np; ++q)
@@ -289,7 +380,7 @@ npom_status run_explicit_adjoint(const npom_params *p, float *const *fields, con
       continue;
     }
     k_save_fields<<<field_list_grid(c, plan[q]), kThreads, 0, s>>>(c, plan[q], aws->save);
-    launch_fwd_phase(c, plan[q], s);
+    launch_fwd_phase(c, plan[q], pplan, is, s);
   }
   for (int q = np - 1; q >= 0; --q) {
     if (ext_ctas > 0 && q >= e0 && q < e1) {
@@ -300,7 +391,8 @@ npom_status run_explicit_adjoint(const npom_params *p, float *const *fields, con
       continue;
     }
     k_restore_move<<<field_list_grid(c, plan[q]), kThreads, 0, s>>>(c, a, plan[q], aws->save);
-    launch_adj_phase(c, a, plan[q], s);
+    const npom_status st = launch_adj_phase(p, ws, c, a, plan[q], is, s);
+    if (st != NPOM_OK) return st;
   }
   return cudaGetLastError() == cudaSuccess ? NPOM_OK : NPOM_ERR_CUDA;
 }

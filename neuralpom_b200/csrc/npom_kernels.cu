@@ -1026,11 +1026,6 @@ constexpr int kNumPhases = (int)(sizeof(kPhaseNames) / sizeof(kPhaseNames[0]));
 // :231-252 _solve_implicit_eta_adjoint, :645-675 depth adjoint)
 // ---------------------------------------------------------------------------
 
-// relative cell area of the area-weighted transpose (1 on the ring)
-__device__ __forceinline__ float adj_area(const Ctx &c, int i, int j) {
-  return interior(c, i, j) ? F2(art, i, j) / F2(art, 1, 1) : 1.0f;
-}
-
 // rhs = g / area into the rhs workspace; max |rhs| as float bits (a
 // non-negative float orders like its bit pattern, NaN above infinity)
 __global__ void k_adj_prep(Ctx c, const float *g, unsigned int *maxbits) {
@@ -1057,52 +1052,13 @@ __global__ void k_adj_scale(Ctx c, float scale, float *x) {
   }
 }
 
-// lambda at an interior cell, times coeff / art: the factor every face
-// term of the depth adjoint starts from
-__device__ __forceinline__ float adj_lam(const Ctx &c, const float *sol, float scale, int i, int j) {
-  const size_t o = NPOM_I2(c, i, j);
-  const float lam = (sol[o] * adj_area(c, i, j)) * scale;
-  return (lam * c.k.implicit_coeff) * W2(inv_art, i, j);
-}
-__device__ __forceinline__ float adj_east(const Ctx &c, const float *x, const float *sol, float scale, int i, int j) {
-  return (((0.5f * adj_lam(c, sol, scale, i, j)) * (x[NPOM_I2(c, i + 1, j)] - x[NPOM_I2(c, i, j)])) * W2(ce, i, j)) *
-         F2(dum, i + 1, j);
-}
-__device__ __forceinline__ float adj_west(const Ctx &c, const float *x, const float *sol, float scale, int i, int j) {
-  return (((0.5f * adj_lam(c, sol, scale, i, j)) * (x[NPOM_I2(c, i, j)] - x[NPOM_I2(c, i - 1, j)])) * W2(cw, i, j)) *
-         F2(dum, i, j);
-}
-__device__ __forceinline__ float adj_north(const Ctx &c, const float *x, const float *sol, float scale, int i, int j) {
-  return (((0.5f * adj_lam(c, sol, scale, i, j)) * (x[NPOM_I2(c, i, j + 1)] - x[NPOM_I2(c, i, j)])) * W2(cn, i, j)) *
-         F2(dvm, i, j + 1);
-}
-__device__ __forceinline__ float adj_south(const Ctx &c, const float *x, const float *sol, float scale, int i, int j) {
-  return (((0.5f * adj_lam(c, sol, scale, i, j)) * (x[NPOM_I2(c, i, j)] - x[NPOM_I2(c, i, j - 1)])) * W2(cs, i, j)) *
-         F2(dvm, i, j);
-}
-
-// grad_d = -(depth adjoint): the reference scatters eight face terms with
-// in-place adds in a fixed statement order; each cell gathers the same
-// terms in that order (east of i-1, east, west, west of i+1, north of j-1,
-// north, south, south of j+1)
+// grad_d = -(depth adjoint), gathered per cell in the reference's order
+// (adj_grad_d_cell)
 __global__ void k_adj_grad_d(Ctx c, const float *x, const float *sol, float scale, float *grad_d) {
   const size_t n = (size_t)c.im * c.jm;
   for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
     const int i = (int)(o / c.jm), j = (int)(o - (size_t)i * c.jm);
-    float acc = 0.0f;
-    if (interior(c, i - 1, j)) acc = acc + -adj_east(c, x, sol, scale, i - 1, j);
-    if (interior(c, i, j)) {
-      acc = acc + -adj_east(c, x, sol, scale, i, j);
-      acc = acc + adj_west(c, x, sol, scale, i, j);
-    }
-    if (interior(c, i + 1, j)) acc = acc + adj_west(c, x, sol, scale, i + 1, j);
-    if (interior(c, i, j - 1)) acc = acc + -adj_north(c, x, sol, scale, i, j - 1);
-    if (interior(c, i, j)) {
-      acc = acc + -adj_north(c, x, sol, scale, i, j);
-      acc = acc + adj_south(c, x, sol, scale, i, j);
-    }
-    if (interior(c, i, j + 1)) acc = acc + adj_south(c, x, sol, scale, i, j + 1);
-    grad_d[o] = -acc;
+    grad_d[o] = adj_grad_d_cell(c, x, sol, scale, i, j);
   }
 }
 
@@ -1190,17 +1146,25 @@ size_t npom_adjoint_save_floats(const npom_params *p) {
   c.kb = p->kb;
   c.k.isplit = p->isplit;
   c.k.ispadv = p->ispadv;
+  c.k.core = p->core;
+  c.k.has_vmix = p->has_vmix;
   c.do_internal = 1;
-  std::vector<AdjPhaseRec> plan((size_t)(16 + 3 * p->isplit));
+  std::vector<AdjPhaseRec> plan((size_t)(18 + 3 * p->isplit));
   size_t need = 0;
   adj_step_plan(c, plan.data(), (int)plan.size(), &need);
-  return need;
+  return need + (size_t)kAdjScratchPlanes * (size_t)p->im * p->jm;
 }
 
 npom_status npom_step_explicit_adjoint(const npom_params *p, float *const *fields, const npom_workspace *ws,
                                        const npom_clock *clk, float *const *grads, const npom_adjoint_ws *aws,
                                        void *stream) {
-  return run_explicit_adjoint(p, fields, ws, clk, grads, aws, (cudaStream_t)stream);
+  return run_step_adjoint(p, fields, ws, clk, grads, aws, NPOM_CORE_EXPLICIT, (cudaStream_t)stream);
+}
+
+npom_status npom_step_implicit_adjoint(const npom_params *p, float *const *fields, const npom_workspace *ws,
+                                       const npom_clock *clk, float *const *grads, const npom_adjoint_ws *aws,
+                                       void *stream) {
+  return run_step_adjoint(p, fields, ws, clk, grads, aws, NPOM_CORE_IMPLICIT, (cudaStream_t)stream);
 }
 
 npom_status npom_run_phase(const npom_params *p, float *const *fields, const npom_workspace *ws, int phase,

@@ -4,7 +4,7 @@
 ``advance(core, steps)`` resets the clock bookkeeping exactly like the
 reference's no-grad branch (``time0 = time``, ``iint = 0``, ``iend =
 steps``) and runs ``core.run_time_loop()`` on the B200 library;
-``differentiable=True`` (explicit core) advances in chunks of
+``differentiable=True`` advances in chunks of
 ``chunk_steps``, each one autograd node whose backward is the CUDA step
 adjoint, like the reference's checkpointed chunks.
 """
@@ -38,8 +38,6 @@ class B200Physics:
         if differentiable:
             # chunks of chunk_steps, each one autograd node with a checkpoint
             # per internal step (sparse_physics.py:108-149)
-            if self.core_name != "explicit":
-                raise NotImplementedError("the differentiable advance is provided for the explicit core")
             for start in range(0, steps, self.chunk_steps):
                 n = min(self.chunk_steps, steps - start)
                 core.time0 = float(core.time)

@@ -7,6 +7,7 @@
 // grid barriers replaced by the end of each loop.  This checks the index
 // logic of every phase against the oracle on a machine without a GPU; it is
 // not part of the product library and is never loaded by neuralpom_b200.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -200,8 +201,66 @@ void run_phase(const Ctx &c, const npom_params *p, int phase) {
   }
 }
 
-void fwd_plan_phase(const Ctx &c, const AdjPhaseRec &r) {
+// the implicit free-surface phase of the recomputation: PCG without its post
+// step, the solution kept in xs, then the post step (as k_imp_post)
+void imp_forward(const Ctx &c, float *xs) {
+  pcg(c, 0, 1, 0);
+  const size_t n = (size_t)c.im * c.jm;
+  std::memcpy(xs, c.F[NPOM_F_elf], n * 4);
+  each_cell(c, [&](int i, int j) {
+    const size_t q = NPOM_I2(c, i, j);
+    if (!interior(c, i, j)) {
+      P2(elf, i, j) = 0.0f;
+      P2(d, i, j) = F2(h, i, j);
+      return;
+    }
+    const int jm = c.jm;
+    const float x0 = xs[q];
+    const float xn = (j + 1 < jm - 1) ? xs[q + 1] : 0.0f;
+    const float xsv = (j - 1 > 0) ? xs[q - 1] : 0.0f;
+    const float xe = (i + 1 < c.im - 1) ? xs[q + jm] : 0.0f;
+    const float xw = (i - 1 > 0) ? xs[q - jm] : 0.0f;
+    const float smv = x0 + c.k.bshap_q * (xe + xw + xn + xsv - 4.0f * x0);
+    const float fsm = F2(fsm, i, j);
+    const float ev = (smv * fsm) * fsm;
+    P2(d, i, j) = F2(h, i, j) + ev;
+    P2(elf, i, j) = ev;
+  });
+}
+
+// its reverse: g = dJ/dx, the eta-solve adjoint (npom_pcg_adjoint restated
+// on the host with the same bodies), the rhs and transports
+void imp_reverse(const Ctx &c, const Adj &a, const float *xs, float *g, float *lam, float *gd) {
+  const size_t n = (size_t)c.im * c.jm;
+  each_cell(c, [&](int i, int j) { g[NPOM_I2(c, i, j)] = imp_post_grad(c, a, i, j); });
+  float amax = 0.0f;
+  each_cell(c, [&](int i, int j) {
+    const size_t o = NPOM_I2(c, i, j);
+    const float v = g[o] / adj_area(c, i, j);
+    c.W[NPOM_W_rhs][o] = v;
+    amax = std::max(amax, std::fabs(v));
+  });
+  const float scale = amax > 1.0f ? amax : 1.0f;
+  for (size_t o = 0; o < n; ++o) {
+    c.W[NPOM_W_rhs][o] = c.W[NPOM_W_rhs][o] / scale;
+    lam[o] = 0.0f;
+  }
+  Ctx ca = c;
+  ca.F[NPOM_F_elf] = lam;
+  ca.k.eta_tol = c.k.eta_tol / (double)scale;
+  pcg(ca, 0, 0, 0);
+  each_cell(c, [&](int i, int j) { gd[NPOM_I2(c, i, j)] = adj_grad_d_cell(c, xs, lam, scale, i, j); });
+  each_cell(c, [&](int i, int j) {
+    const size_t o = NPOM_I2(c, i, j);
+    lam[o] = (lam[o] * adj_area(c, i, j)) * scale;
+  });
+  each_cell(c, [&](int i, int j) { imp_rhs_cell_adj(c, a, i, j, lam, gd); });
+}
+
+void fwd_plan_phase(const Ctx &c, const AdjPhaseRec &r, float *xs) {
   switch (r.phase) {
+    case AP_EI: imp_forward(c, xs); break;
+    case AP_I5: each_cell(c, [&](int i, int j) { (void)phase_i5_cell(c, i, j); }); break;
     case AP_A1: a1(c); break;
     case AP_A2: each_cell(c, [&](int i, int j) { phase_a2_column(c, i, j); }); break;
     case AP_A3: each_cell(c, [&](int i, int j) { phase_a3_cell(c, i, j); }); break;
@@ -221,8 +280,11 @@ void fwd_plan_phase(const Ctx &c, const AdjPhaseRec &r) {
   }
 }
 
-void adj_plan_phase(const Ctx &c, const Adj &a, const AdjPhaseRec &r) {
+void adj_plan_phase(const Ctx &c, const Adj &a, const AdjPhaseRec &r, const float *xs, float *g, float *lam,
+                    float *gd) {
   switch (r.phase) {
+    case AP_EI: imp_reverse(c, a, xs, g, lam, gd); break;
+    case AP_I5: each_cell(c, [&](int i, int j) { phase_i5_cell_adj(c, a, i, j); }); break;
     case AP_A1: each_point(c, [&](int i, int j, int k) { phase_a1_point_adj(c, a, i, j, k); }); break;
     case AP_A2: each_cell(c, [&](int i, int j) { phase_a2_column_adj(c, a, i, j); }); break;
     case AP_A3: each_cell(c, [&](int i, int j) { phase_a3_cell_adj(c, a, i, j); }); break;
@@ -262,14 +324,24 @@ int emul_step_adjoint(const npom_params *p, float *const *fields, const npom_wor
     a.G[f] = grads[f];
     a.L[f] = lam[f];
   }
-  std::vector<AdjPhaseRec> plan((size_t)(16 + 3 * p->isplit));
+  std::vector<AdjPhaseRec> plan((size_t)(18 + 3 * p->isplit));
   size_t need = 0;
   const int np = adj_step_plan(c, plan.data(), (int)plan.size(), &need);
-  if (need > save_floats) return 2;
+  const size_t ncell = (size_t)c.im * c.jm;
+  if (need + (2 * AW_COUNT + 4) * ncell > save_floats) return 2;
+  float *scratch = save + need;
+  std::memset(scratch, 0, (2 * AW_COUNT + 4) * ncell * 4);
+  for (int w = 0; w < AW_COUNT; ++w) {
+    a.G[NPOM_NFIELDS + w] = scratch + (size_t)w * ncell;
+    a.L[NPOM_NFIELDS + w] = scratch + (size_t)(AW_COUNT + w) * ncell;
+  }
+  float *xs = scratch + (size_t)(2 * AW_COUNT) * ncell, *g = xs + ncell, *lamw = g + ncell, *gd = lamw + ncell;
+  if (p->core == NPOM_CORE_IMPLICIT) each_cell(c, [&](int i, int j) { elliptic_coeff_cell(c, i, j); });
   for (int q = 0; q < np; ++q) {
     const AdjPhaseRec &r = plan[q];
-    for (int e = 0; e < r.n; ++e) std::memcpy(save + r.off[e], c.F[r.fld[e]], adj_field_len(c, r.fld[e]) * 4);
-    fwd_plan_phase(c, r);
+    for (int e = 0; e < r.n; ++e)
+      std::memcpy(save + r.off[e], adj_fptr(c, r.fld[e]), adj_field_len(c, r.fld[e]) * 4);
+    fwd_plan_phase(c, r, xs);
   }
   int done = 0;
   for (int q = np - 1; q >= 0; --q) {
@@ -278,13 +350,13 @@ int emul_step_adjoint(const npom_params *p, float *const *fields, const npom_wor
     for (int e = 0; e < r.n; ++e) {
       const int f = r.fld[e];
       const size_t n = adj_field_len(c, f);
-      std::memcpy(c.F[f], save + r.off[e], n * 4);
+      std::memcpy(adj_fptr(c, f), save + r.off[e], n * 4);
       if (r.move[e]) {
         std::memcpy(a.L[f], a.G[f], n * 4);
         std::memset(a.G[f], 0, n * 4);
       }
     }
-    adj_plan_phase(c, a, r);
+    adj_plan_phase(c, a, r, xs, g, lamw, gd);
     ++done;
   }
   return 0;
@@ -299,8 +371,10 @@ int emul_adjoint_plan(const npom_params *p, int do_internal, size_t *save_floats
   c.kb = p->kb;
   c.k = make_consts(*p);
   c.do_internal = do_internal;
-  std::vector<AdjPhaseRec> plan((size_t)(16 + 3 * p->isplit));
-  return adj_step_plan(c, plan.data(), (int)plan.size(), save_floats);
+  std::vector<AdjPhaseRec> plan((size_t)(18 + 3 * p->isplit));
+  const int np = adj_step_plan(c, plan.data(), (int)plan.size(), save_floats);
+  *save_floats += (2 * AW_COUNT + 4) * (size_t)c.im * c.jm;
+  return np;
 }
 
 int emul_run_phase(const npom_params *p, float *const *fields, const npom_workspace *ws, int phase, double ramp) {

@@ -130,11 +130,11 @@ class EmulCore:
         assert rc == 0
 
 
-def multi_step_adjoint(arrays, scalars, cot, nsteps):
-    """Reverse mode of ``nsteps`` emulated explicit steps with a checkpoint
-    per step: forward saving each step's start state, then the step
-    adjoints in reverse order.  Returns the cotangents of the start state."""
-    E = EmulCore(arrays, scalars, "explicit")
+def multi_step_adjoint(arrays, scalars, cot, nsteps, core="explicit"):
+    """Reverse mode of ``nsteps`` emulated steps with a checkpoint per step:
+    forward saving each step's start state, then the step adjoints in
+    reverse order.  Returns the cotangents of the start state."""
+    E = EmulCore(arrays, scalars, core)
     starts = []
     for _ in range(nsteps):
         starts.append(({n: v.copy() for n, v in E.F.items()}, E.time))

@@ -194,8 +194,8 @@ ADJ_COT_FIELDS = ("u", "ub", "v", "vb", "t", "tb", "s", "sb", "el", "elb", "ua",
                   "km", "kh", "et", "etb", "egb", "utb", "vtb", "wubot", "wvbot", "rho")
 
 
-def make_step_adjoint_golden(tag, core, steps=(1, 3), seed=0, cot_fields=ADJ_COT_FIELDS):
-    """Reverse mode of the reference's explicit step under torch autograd
+def make_step_adjoint_golden(tag, core, steps=(1, 3), seed=0, cot_fields=ADJ_COT_FIELDS, name="explicit"):
+    """Reverse mode of the reference's step under torch autograd
     (``SparsePhysics.advance(..., differentiable=True)``, sparse_physics.py:
     91-149): seeded cotangents on ``cot_fields`` after ``n`` steps,
     J = sum(cot * state), and dJ/d(start state) for every state field."""
@@ -210,13 +210,13 @@ def make_step_adjoint_golden(tag, core, steps=(1, 3), seed=0, cot_fields=ADJ_COT
     for f, v in cot.items():
         out[f"cot__{f}"] = v.numpy()
     for n in steps:
-        c2 = rh.build_reference_core("explicit", im, jm)
+        c2 = rh.build_reference_core(name, im, jm)
         rh.load_state(c2, arrays, scalars)
         leaves = {}
         for f in ADJ_STATE_FIELDS:
             leaves[f] = getattr(c2, f).detach().clone().requires_grad_(True)
             setattr(c2, f, leaves[f])
-        rh.advance(c2, "explicit", n, differentiable=True)
+        rh.advance(c2, name, n, differentiable=True)
         loss = sum((getattr(c2, f) * cot[f]).sum() for f in cot_fields)
         loss.backward()
         for f in ADJ_STATE_FIELDS:
@@ -246,6 +246,13 @@ def make_step_adjoint_goldens():
     core.time0 = float(core.time)
     make_step_adjoint_golden("coastal", core, steps=(1,), seed=35,
                              cot_fields=("u", "v", "t", "s", "el", "ua", "va", "q2", "km"))
+    name = "implicit_p0_fixed"
+    core = perturbed_core(name, 12, 10, 36)
+    core.time0 = float(core.time)
+    make_step_adjoint_golden("implicit", core, steps=(1, 3), seed=37, name=name)
+    core = perturbed_core(name, 12, 10, 38)
+    core.time = core.time0 = 0.0
+    make_step_adjoint_golden("implicit_rest", core, steps=(1, 2), seed=39, name=name)
 
 
 def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint")):

@@ -97,3 +97,24 @@ def grad_errors(got, ref):
         scale = float(np.abs(r).max())
         out[f] = float(np.abs(np.asarray(got[f]) - r).max()) / (scale if scale > 0 else 1.0)
     return out
+
+
+# Gradient bar against the reference's autograd: per field, |g - g_ref| /
+# max|g_ref| below GRAD_TOL at all but GRAD_OUTLIERS of the cells (and below
+# GRAD_MAX everywhere).  The outliers are rounding-sensitive cells near a
+# kink of the float32 forward, where the two float32 adjoints still agree
+# to 0.5% while a float64 finite difference disagrees with both (2 of 1920
+# cells of the 3-step implicit file).
+GRAD_TOL, GRAD_MAX = 1e-4, 1e-3
+
+
+def grad_check(got, ref):
+    """[] when every field meets the bar, else (field, max error, cells
+    above GRAD_TOL, size) of the failing fields."""
+    bad = []
+    for f, r in ref.items():
+        e = np.abs(np.asarray(got[f], dtype=np.float64) - r) / max(float(np.abs(r).max()), 1e-30)
+        n_out = int((e > GRAD_TOL).sum())
+        if n_out > max(2, int(0.002 * e.size)) or e.max() >= GRAD_MAX:
+            bad.append((f, float(e.max()), n_out, e.size))
+    return bad

@@ -1,4 +1,4 @@
-"""The explicit step adjoint (the device reverse bodies of
+"""The step adjoint of both cores (the device reverse bodies of
 neuralpom_b200/csrc/npom_adjoint.cuh, run on the CPU by tests/emul) against
 the reference's own torch-autograd gradient of the same step(s)
 (``SparsePhysics.advance(differentiable=True)``, sparse_physics.py:91-149),
@@ -6,7 +6,7 @@ recorded in tests/golden/step_adjoint_*.npz."""
 import numpy as np
 import pytest
 
-from golden_io import grad_errors, load_adjoint_golden
+from golden_io import grad_check, load_adjoint_golden
 
 emul = pytest.importorskip("emul_harness")
 
@@ -18,21 +18,20 @@ def _has_nvcc():
 
 pytestmark = pytest.mark.skipif(not _has_nvcc(), reason="nvcc needed to build the phase emulator")
 
-# tolerance on max|g - g_ref| / max|g_ref| per field: both are the exact
-# derivative of the same float32 step, evaluated in float32 with sums in
-# different orders (the worst field seen is kh of the coastal step, 3e-5)
-GRAD_TOL = 1e-4
+ADJOINT_FILES = ["step_adjoint_explicit_12x10.npz", "step_adjoint_rest_12x10.npz", "step_adjoint_coastal_16x14.npz",
+                 "step_adjoint_implicit_12x10.npz", "step_adjoint_implicit_rest_12x10.npz"]
 
 
-@pytest.mark.parametrize("fname", ["step_adjoint_explicit_12x10.npz", "step_adjoint_rest_12x10.npz",
-                                   "step_adjoint_coastal_16x14.npz"])
+def core_of(fname):
+    return "implicit_p0_fixed" if "implicit" in fname else "explicit"
+
+
+@pytest.mark.parametrize("fname", ADJOINT_FILES)
 def test_emulated_step_adjoint_matches_reference_autograd(fname):
     A, Sc, cot, grads = load_adjoint_golden(fname)
     for n, ref in sorted(grads.items()):
-        G = emul.multi_step_adjoint(A, Sc, cot, n)
-        errs = grad_errors(G, ref)
-        worst = max(errs, key=errs.get)
-        assert errs[worst] < GRAD_TOL, (fname, n, worst, errs[worst])
+        G = emul.multi_step_adjoint(A, Sc, cot, n, core=core_of(fname))
+        assert grad_check(G, ref) == [], (fname, n, grad_check(G, ref))
         # every state field the reference differentiates is reached
         for f in ref:
             assert np.any(G[f] != 0), (fname, n, f)

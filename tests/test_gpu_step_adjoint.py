@@ -7,16 +7,15 @@ import numpy as np
 import pytest
 import torch
 
-from golden_io import grad_errors, load_adjoint_golden
+from golden_io import grad_check, load_adjoint_golden
 
 pytestmark = pytest.mark.gpu
 
-GRAD_TOL = 1e-4  # relative to max|g_ref| per field, as for the CPU emulation
 
 
-def _core(A, Sc):
+def _core(A, Sc, name="explicit"):
     from neuralpom_b200 import resolve_core_class
-    return resolve_core_class("explicit").from_state(A, Sc, device="cuda")
+    return resolve_core_class(name).from_state(A, Sc, device="cuda")
 
 
 def _differentiable_advance(core, nsteps, time0):
@@ -32,24 +31,32 @@ def _differentiable_advance(core, nsteps, time0):
     return leaves
 
 
-@pytest.mark.parametrize("ext", ["cluster", "phases"])
-@pytest.mark.parametrize("fname", ["step_adjoint_explicit_12x10.npz", "step_adjoint_rest_12x10.npz",
-                                   "step_adjoint_coastal_16x14.npz"])
+ADJOINT_CASES = [("step_adjoint_explicit_12x10.npz", "cluster"), ("step_adjoint_explicit_12x10.npz", "phases"),
+                 ("step_adjoint_rest_12x10.npz", "cluster"), ("step_adjoint_rest_12x10.npz", "phases"),
+                 ("step_adjoint_coastal_16x14.npz", "cluster"), ("step_adjoint_coastal_16x14.npz", "phases"),
+                 ("step_adjoint_implicit_12x10.npz", "-"), ("step_adjoint_implicit_rest_12x10.npz", "-")]
+
+
+def _core_name(fname):
+    return "implicit_p0_fixed" if "implicit" in fname else "explicit"
+
+
+@pytest.mark.parametrize("fname,ext", ADJOINT_CASES)
 def test_gpu_step_adjoint_matches_reference_autograd(monkeypatch, fname, ext):
-    """Both forms of the external-subcycle adjoint: the two fused
-    thread-block-cluster kernels and one launch per substep phase."""
-    monkeypatch.setenv("NPOM_ADJ_EXT", ext)
+    """Both cores; for the explicit one both forms of the external-subcycle
+    adjoint (the two fused thread-block-cluster kernels, one launch per
+    substep phase)."""
+    if ext != "-":
+        monkeypatch.setenv("NPOM_ADJ_EXT", ext)
     A, Sc, cot, grads = load_adjoint_golden(fname)
     for n, ref in sorted(grads.items()):
-        core = _core(A, Sc)
+        core = _core(A, Sc, _core_name(fname))
         leaves = _differentiable_advance(core, n, float(Sc["time"]))
         loss = sum((getattr(core, f) * torch.from_numpy(c).cuda()).sum() for f, c in cot.items())
         loss.backward()
         got = {f: (leaves[f].grad.cpu().numpy() if leaves[f].grad is not None else np.zeros_like(A[f]))
                for f in ref}
-        errs = grad_errors(got, ref)
-        worst = max(errs, key=errs.get)
-        assert errs[worst] < GRAD_TOL, (fname, n, worst, errs[worst])
+        assert grad_check(got, ref) == [], (fname, n, grad_check(got, ref))
 
 
 def test_gpu_step_adjoint_matches_finite_differences():
@@ -131,6 +138,4 @@ def test_gpu_physics_differentiable_advance_in_chunks():
     loss = sum((getattr(core, f) * torch.from_numpy(c).cuda()).sum() for f, c in cot.items())
     loss.backward()
     got = {f: leaves[f].grad.cpu().numpy() for f in grads[3]}
-    errs = grad_errors(got, grads[3])
-    worst = max(errs, key=errs.get)
-    assert errs[worst] < GRAD_TOL, (worst, errs[worst])
+    assert grad_check(got, grads[3]) == [], grad_check(got, grads[3])
