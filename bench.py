@@ -330,6 +330,8 @@ def run_b200(args):
                                    core_name=W["core"])
 
     fa = fam = None
+    if rank == 0 and ws_n == 1 and args.workload == "coastal" and not args.no_fwd_adjoint:
+        fa = coastal_fwd_adjoint(args, dev)
     if rank == 0 and ws_n == 1 and args.workload == "seamount" and not args.no_fwd_adjoint:
         fa, A_dev, t_dev = seamount_fwd_adjoint(core, args, dev)
         case = (A_dev, dict(Sc, time=t_dev, time0=t_dev))
@@ -653,6 +655,35 @@ def seamount_fwd_adjoint(core, args, dev, nsteps=36, reps=3):
                         "checkpoint per internal step, hand-written CUDA step adjoint with the free-surface "
                         "solve's CUDA adjoint",
             "timing": f"median of {reps} samples, CUDA events around forward+backward"}, A, t0
+
+
+def coastal_fwd_adjoint(args, dev, nsteps=360):
+    """BASELINE config 4's differentiation: the explicit core on the
+    354x322x16 coastal basin, ``nsteps`` internal steps (6 h at dtI = 60 s)
+    forward under autograd from the set-up state (tide elevation held at its
+    start value inside the window), MSE(u, v, T, S) against a seeded
+    target, backward to every state field with a checkpoint per internal
+    step.  Reports the peak device memory of the call."""
+    import torch
+    from neuralpom_b200 import _abi, resolve_core_class
+    A, Sc = workload(0, "coastal")
+    core = resolve_core_class("explicit").from_state(A, Sc, device=dev)
+    tgt, _ = _fa_targets(A, 13)
+    tgt = {f: torch.from_numpy(v).to(dev) for f, v in tgt.items()}
+    start = {f: getattr(core, f).detach().clone() for f in _abi.FIELD_NAMES}
+    torch.cuda.synchronize(dev)
+    torch.cuda.reset_peak_memory_stats(dev)
+    base = torch.cuda.memory_allocated(dev)
+    best = fwd_adjoint_timing(core, start, tgt, {}, 1, nsteps, float(Sc["time"]), 1, 1, dev)
+    peak = torch.cuda.max_memory_allocated(dev)
+    days = nsteps * float(core.dti) / 86400.0
+    return {"value": days / (best / 1000.0), "unit": UNIT, "ms_per_sample": best,
+            "peak_hbm_gb": peak / 1e9, "state_and_inputs_gb": base / 1e9,
+            "workload": f"explicit core, 354x322x16 coastal basin (open south boundary, Flather, M2 elevation); "
+                        f"{nsteps} internal steps (6 h) forward under autograd, MSE(u,v,T,S) loss, backward to "
+                        "every state field; checkpoint per internal step (one flat copy of the 58 state fields)",
+            "timing": "one sample after one warm-up, CUDA events around forward+backward; peak_hbm_gb = "
+                      "torch.cuda.max_memory_allocated over the warm-up and the sample"}
 
 
 def fwd_adjoint_sample(args, dev, reps=3):

@@ -287,6 +287,7 @@ NPOM_HD void smag_level_adj(const Ctx &c, const Adj &a, int i, int j, int k, flo
   GA3(v, i - 1, j + 1, k, -lvt);
 }
 
+template <int KM>
 NPOM_HD void baropg_column_adj(const Ctx &c, const Adj &a, int i, int j, const float *lamx, const float *lamy) {
   const int kbm1 = c.kb - 1;
   const float ramp = c.ramp;
@@ -296,7 +297,7 @@ NPOM_HD void baropg_column_adj(const Ctx &c, const Adj &a, int i, int j, const f
     const int bj = comp == 0 ? j : j - 1;
     const float term_dt = F2(dt, i, j) + F2(dt, bi, bj);
     const float dt_diff = F2(dt, i, j) - F2(dt, bi, bj);
-    float r[KMAX], rb[KMAX], V[KMAX], lr[KMAX], lrb[KMAX];
+    float r[KM], rb[KM], V[KM], lr[KM], lrb[KM];
     for (int k = 0; k < kbm1; ++k) {
       r[k] = F3(rho, i, j, k) - F3(rmean, i, j, k);
       rb[k] = F3(rho, bi, bj, k) - F3(rmean, bi, bj, k);
@@ -354,12 +355,13 @@ NPOM_HD void baropg_column_adj(const Ctx &c, const Adj &a, int i, int j, const f
   }
 }
 
+template <int KM>
 NPOM_HD void phase_a2_column_adj(const Ctx &c, const Adj &a, int i, int j) {
   const int kb = c.kb, kbm1 = kb - 1;
   const bool inner = interior(c, i, j);
   const float lsx = LA2(adx2d, i, j), lsy = LA2(ady2d, i, j), lrx = LA2(drx2d, i, j), lry = LA2(dry2d, i, j);
   const float lsa = LA2(aam2d, i, j);
-  float lrhox[KMAX], lrhoy[KMAX], laam[KMAX];
+  float lrhox[KM], lrhoy[KM], laam[KM];
   for (int k = 0; k < kb; ++k) {
     lrhox[k] = LA3(drhox, i, j, k);
     lrhoy[k] = LA3(drhoy, i, j, k);
@@ -376,7 +378,7 @@ NPOM_HD void phase_a2_column_adj(const Ctx &c, const Adj &a, int i, int j) {
   if (inner) {
     for (int k = 0; k < kbm1; ++k) smag_level_adj(c, a, i, j, k, laam[k]);
     GA3(aam, i, j, kbm1, laam[kbm1]);
-    baropg_column_adj(c, a, i, j, lrhox, lrhoy);
+    baropg_column_adj<KM>(c, a, i, j, lrhox, lrhoy);
   } else {
     for (int k = 0; k < kb; ++k) GA3(aam, i, j, k, laam[k]);
   }
@@ -1094,6 +1096,7 @@ NPOM_HD void phase_i5_cell_adj(const Ctx &c, const Adj &a, int i, int j) {
 // ===========================================================================
 // B1: barotropic fix (time_loop.py:440-477)
 // ===========================================================================
+template <int KM>
 NPOM_HD void phase_b1_column_adj(const Ctx &c, const Adj &a, int i, int j) {
   const int kbm1 = c.kb - 1;
   for (int comp = 0; comp < 2; ++comp) {
@@ -1144,12 +1147,13 @@ NPOM_HD void vertvl_yflux_adj(const Ctx &c, const Adj &a, int i, int j, int k, f
   GA2(dt, i, j - 1, t);
 }
 
+template <int KM>
 NPOM_HD void phase_b2a_column_adj(const Ctx &c, const Adj &a, int i, int j) {
   const int kb = c.kb, kbm1 = kb - 1;
   const float fsm = F2(fsm, i, j);
   // bcond 5: explicit masks levels < kb-1, the closed basin every level
   const int kend = is_explicit(c) ? kbm1 : kb;
-  float lw[KMAX];
+  float lw[KM];
   for (int k = 0; k < kb; ++k) lw[k] = LA3(w, i, j, k) * (k < kend ? fsm : 1.0f);
   if (!interior(c, i, j)) {
     for (int k = 0; k < kb; ++k) GA3(w, i, j, k, lw[k]);
@@ -1268,16 +1272,17 @@ NPOM_HD void phase_b2b_point_adj(const Ctx &c, const Adj &a, int i, int j, int k
 // ===========================================================================
 // B3: PROFQ, Mellor-Yamada 2.5 (tracers.py:158-431), explicit forms
 // ===========================================================================
+template <int KM>
 NPOM_HD void phase_b3_column_adj(const Ctx &c, const Adj &a, int i, int j) {
   const int im = c.im, jm = c.jm, kb = c.kb, kbm1 = kb - 1;
   const float dti2 = c.k.dti2, umol2 = c.k.two_umol, grav = c.k.grav, kappa = c.k.kappa, small = c.k.small;
   const float b1 = 16.6f, e1 = 1.8f, e2 = 1.33f;
   const float eps = 1e-20f;
   // ---- forward recomputation (phase_b3_column) ----
-  float A[KMAX], C[KMAX], cc[KMAX], ccs_[KMAX], radv[KMAX], pp[KMAX], boygr[KMAX], lraw[KMAX], l[KMAX];
-  float ghraw[KMAX], gh[KMAX], kn[KMAX], dtef[KMAX], ee1[KMAX], gg1[KMAX], den1[KMAX], ee2[KMAX], gg2[KMAX];
-  float den2[KMAX], wall0[KMAX], wallv[KMAX], uo[KMAX], vo[KMAX];
-  bool clampc[KMAX], clip[KMAX];
+  float A[KM], C[KM], cc[KM], ccs_[KM], radv[KM], pp[KM], boygr[KM], lraw[KM], l[KM];
+  float ghraw[KM], gh[KM], kn[KM], dtef[KM], ee1[KM], gg1[KM], den1[KM], ee2[KM], gg2[KM];
+  float den2[KM], wall0[KM], wallv[KM], uo[KM], vo[KM];
+  bool clampc[KM], clip[KM];
   const float dh = F2(h, i, j) + F2(etf, i, j);
   for (int k = 0; k < kb; ++k) {
     A[k] = 0.0f;
@@ -1386,8 +1391,8 @@ NPOM_HD void phase_b3_column_adj(const Ctx &c, const Adj &a, int i, int j) {
   const float coef1 = (float)(0.74 * (1.0 - 6.0 * 0.92 / 16.6));
   const float coef2 = (float)(3.0 * 0.74 * 10.1 + 18.0 * 0.92 * 0.74);
   const float coef3 = (float)(0.92 * (1.0 - 3.0 * 0.08 - 6.0 * 0.92 / 16.6));
-  float lA[KMAX], lC[KMAX], ldtef[KMAX], lkn[KMAX], lgh[KMAX], ll[KMAX], lcc[KMAX], lboy[KMAX];
-  float luo[KMAX], lvo[KMAX], lee[KMAX], lgg[KMAX];
+  float lA[KM], lC[KM], ldtef[KM], lkn[KM], lgh[KM], ll[KM], lcc[KM], lboy[KM];
+  float luo[KM], lvo[KM], lee[KM], lgg[KM];
   for (int k = 0; k < kb; ++k) {
     lA[k] = lC[k] = ldtef[k] = lkn[k] = lgh[k] = ll[k] = lcc[k] = lboy[k] = 0.0f;
   }
@@ -1785,6 +1790,7 @@ NPOM_HD void phase_b5_point_adj(const Ctx &c, const Adj &a, int i, int j, int k)
 // B6: PROFT of T and S (tracers.py:890-1010, nbc 1 or 3) and explicit
 // bcond 4 on the edge columns (baroclinic.py:666-846)
 // ===========================================================================
+template <int KM>
 NPOM_HD void proft_column_adj(const Ctx &c, const Adj &a, int i, int j, int fld, int nbc, float wfsurf,
                               float fsurf, const float *lout, float &ldh) {
   const int kb = c.kb, kbm1 = kb - 1, kbm2 = kb - 2;
@@ -1794,7 +1800,7 @@ NPOM_HD void proft_column_adj(const Ctx &c, const Adj &a, int i, int j, int fld,
   const float dh = F2(h, i, j) + F2(etf, i, j);
   const float dh2 = dh * dh;
   const float neg_dti2 = -c.k.dti2;
-  float fin[KMAX], av[KMAX], cc[KMAX], ee[KMAX], gg[KMAX], inv[KMAX], outv[KMAX];
+  float fin[KM], av[KM], cc[KM], ee[KM], gg[KM], inv[KM], outv[KM];
   for (int k = 0; k < kb; ++k) {
     fin[k] = ld(fcol + k);
     av[k] = cc[k] = ee[k] = gg[k] = inv[k] = 0.0f;
@@ -1826,7 +1832,7 @@ NPOM_HD void proft_column_adj(const Ctx &c, const Adj &a, int i, int j, int fld,
   outv[kbt] = numT / denT;
   for (int k = kbm1 - 2; k >= 0; --k) outv[k] = ee[k] * outv[k + 1] + gg[k];
   // reverse
-  float lfin[KMAX], la[KMAX], lcc[KMAX], lee[KMAX], lgg[KMAX], lo[KMAX];
+  float lfin[KM], la[KM], lcc[KM], lee[KM], lgg[KM], lo[KM];
   for (int k = 0; k < kb; ++k) {
     lfin[k] = la[k] = lcc[k] = lee[k] = lgg[k] = 0.0f;
     lo[k] = lout[k];
@@ -1960,10 +1966,11 @@ NPOM_HD void bcond4_explicit_level_adj(const Ctx &c, const Adj &a, int i, int j,
   else GA3(v, vi, vj, k, lvel);
 }
 
+template <int KM>
 NPOM_HD void phase_b6_column_adj(const Ctx &c, const Adj &a, int i, int j) {
   const int kb = c.kb, kbm1 = kb - 1;
   float ldh = LA2(tps, i, j);
-  float lu[KMAX], lv[KMAX];
+  float lu[KM], lv[KM];
   for (int k = 0; k < kb; ++k) {
     lu[k] = LA3(uf, i, j, k);
     lv[k] = LA3(vf, i, j, k);
@@ -1975,8 +1982,8 @@ NPOM_HD void phase_b6_column_adj(const Ctx &c, const Adj &a, int i, int j) {
       lv[k] = 0.0f;
     }
   }
-  proft_column_adj(c, a, i, j, NPOM_F_uf, c.k.nbct, F2(wtsurf, i, j), F2(tsurf, i, j), lu, ldh);
-  proft_column_adj(c, a, i, j, NPOM_F_vf, c.k.nbcs, F2(wssurf, i, j), F2(ssurf, i, j), lv, ldh);
+  proft_column_adj<KM>(c, a, i, j, NPOM_F_uf, c.k.nbct, F2(wtsurf, i, j), F2(tsurf, i, j), lu, ldh);
+  proft_column_adj<KM>(c, a, i, j, NPOM_F_vf, c.k.nbcs, F2(wssurf, i, j), F2(ssurf, i, j), lv, ldh);
   GA2(etf, i, j, ldh);
 }
 
@@ -2149,6 +2156,7 @@ NPOM_HD void advv_point_adj(const Ctx &c, const Adj &a, int i, int j, int k, flo
 // PROFU (comp 0) / PROFV (comp 1).  lout: cotangents of the column output
 // (modified); lwbot, ltps: of the stored wubot/wvbot and tps; lfin: out,
 // cotangents of the ADVU/ADVV forecast.
+template <int KM>
 NPOM_HD void profuv_column_adj(const Ctx &c, const Adj &a, int comp, int i, int j, float *lout, float lwbot,
                                float ltps, float *lfin) {
   const int kb = c.kb, kbm1 = kb - 1, kbm2 = kb - 2;
@@ -2162,7 +2170,7 @@ NPOM_HD void profuv_column_adj(const Ctx &c, const Adj &a, int comp, int i, int 
   }
   const int oi = comp == 0 ? i - 1 : i, oj = comp == 0 ? j : j - 1;
   const float dti2 = c.k.dti2, eps = 1e-20f;
-  float fin[KMAX], av[KMAX], cc[KMAX], ee[KMAX], gg[KMAX], inv[KMAX], outv[KMAX];
+  float fin[KM], av[KM], cc[KM], ee[KM], gg[KM], inv[KM], outv[KM];
   for (int k = 0; k < kb; ++k) {
     fin[k] = (k < kb - 1) ? (comp == 0 ? advu_point(c, i, j, k) : advv_point(c, i, j, k)) : 0.0f;
     av[k] = cc[k] = ee[k] = gg[k] = inv[k] = 0.0f;
@@ -2207,7 +2215,7 @@ NPOM_HD void profuv_column_adj(const Ctx &c, const Adj &a, int comp, int i, int 
   outv[kbt] = q * mask;
   for (int k = kbt - 1; k >= 0; --k) outv[k] = (ee[k] * outv[k + 1] + gg[k]) * mask;
   // reverse
-  float la[KMAX], lcc[KMAX], lee[KMAX], lgg[KMAX];
+  float la[KM], lcc[KM], lee[KM], lgg[KM];
   for (int k = 0; k < kb; ++k) la[k] = lcc[k] = lee[k] = lgg[k] = 0.0f;
   lfin[kb - 1] += lout[kb - 1];
   lout[kbt] += -lwbot * tps;
@@ -2319,19 +2327,20 @@ NPOM_HD void bcond3_explicit_edge_adj(const Ctx &c, const Adj &a, int i, int j, 
   }
 }
 
+template <int KM>
 NPOM_HD void phase_b8_column_adj(const Ctx &c, const Adj &a, int i, int j) {
   const int kb = c.kb;
   const bool inner = interior(c, i, j);
-  float luo[KMAX], lvo[KMAX], lfin[KMAX];
+  float luo[KM], lvo[KM], lfin[KM];
   for (int k = 0; k < kb; ++k) {
     luo[k] = LA3(uf, i, j, k);
     lvo[k] = LA3(vf, i, j, k);
   }
   if (is_explicit(c)) bcond3_explicit_edge_adj(c, a, i, j, luo, lvo);
-  profuv_column_adj(c, a, 0, i, j, luo, LA2(wubot, i, j), 0.0f, lfin);
+  profuv_column_adj<KM>(c, a, 0, i, j, luo, LA2(wubot, i, j), 0.0f, lfin);
   if (inner)
     for (int k = 0; k < kb - 1; ++k) advu_point_adj(c, a, i, j, k, lfin[k]);
-  profuv_column_adj(c, a, 1, i, j, lvo, LA2(wvbot, i, j), LA2(tps, i, j), lfin);
+  profuv_column_adj<KM>(c, a, 1, i, j, lvo, LA2(wvbot, i, j), LA2(tps, i, j), lfin);
   if (inner)
     for (int k = 0; k < kb - 1; ++k) advv_point_adj(c, a, i, j, k, lfin[k]);
 }
@@ -2339,6 +2348,7 @@ NPOM_HD void phase_b8_column_adj(const Ctx &c, const Adj &a, int i, int j) {
 // ===========================================================================
 // B9: velocity filter and shift, 2-D shifts (time_loop.py:628-696)
 // ===========================================================================
+template <int KM>
 NPOM_HD void phase_b9_column_adj(const Ctx &c, const Adj &a, int i, int j) {
   const int kb = c.kb, kbm1 = kb - 1;
   if (c.do_internal) {
@@ -2353,7 +2363,7 @@ NPOM_HD void phase_b9_column_adj(const Ctx &c, const Adj &a, int i, int j) {
       const int fb = comp == 0 ? NPOM_F_ub : NPOM_F_vb;
       const int ff = comp == 0 ? NPOM_F_uf : NPOM_F_vf;
       const size_t o = NPOM_I3(c, i, j, 0);
-      float lfnew[KMAX], lterm[KMAX];
+      float lfnew[KM], lterm[KM];
       float ltps = 0.0f;
       for (int k = 0; k < kb; ++k) {
         lfnew[k] = a.L[fa][o + k] + a.L[ff][o + k];

@@ -33,19 +33,33 @@ __global__ void __launch_bounds__(kThreads) k_adj_points(Ctx c, Adj a) {
   else if (PH == AP_B7) phase_b7_point_adj(c, a, i, j, k);
 }
 
-template <int PH>
-__global__ void __launch_bounds__(128) k_adj_cols(Ctx c, Adj a) {
+// column adjoints with their level arrays sized KM (16 for the common
+// kb = 16, so that they stay in registers and L1)
+template <int PH, int KM>
+__device__ __forceinline__ void adj_column(const Ctx &c, const Adj &a, int i, int j) {
+  if (PH == AP_A2) phase_a2_column_adj<KM>(c, a, i, j);
+  else if (PH == AP_B1) phase_b1_column_adj<KM>(c, a, i, j);
+  else if (PH == AP_B2A) phase_b2a_column_adj<KM>(c, a, i, j);
+  else if (PH == AP_B3) phase_b3_column_adj<KM>(c, a, i, j);
+  else if (PH == AP_B6) phase_b6_column_adj<KM>(c, a, i, j);
+  else if (PH == AP_B8) phase_b8_column_adj<KM>(c, a, i, j);
+  else if (PH == AP_B9) phase_b9_column_adj<KM>(c, a, i, j);
+}
+
+template <int PH, int KM>
+__global__ void __launch_bounds__(128) k_adj_cols_t(Ctx c, Adj a) {
   const int n = c.im * c.jm;
   int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= n) return;
   const int j = col % c.jm, i = col / c.jm;
-  if (PH == AP_A2) phase_a2_column_adj(c, a, i, j);
-  else if (PH == AP_B1) phase_b1_column_adj(c, a, i, j);
-  else if (PH == AP_B2A) phase_b2a_column_adj(c, a, i, j);
-  else if (PH == AP_B3) phase_b3_column_adj(c, a, i, j);
-  else if (PH == AP_B6) phase_b6_column_adj(c, a, i, j);
-  else if (PH == AP_B8) phase_b8_column_adj(c, a, i, j);
-  else if (PH == AP_B9) phase_b9_column_adj(c, a, i, j);
+  adj_column<PH, KM>(c, a, i, j);
+}
+
+template <int PH>
+void launch_adj_cols(const Ctx &c, const Adj &a, cudaStream_t s) {
+  const unsigned g = (unsigned)((c.im * c.jm + 127) / 128);
+  if (c.kb == 16) k_adj_cols_t<PH, 16><<<g, 128, 0, s>>>(c, a);
+  else k_adj_cols_t<PH, KMAX><<<g, 128, 0, s>>>(c, a);
 }
 
 __global__ void __launch_bounds__(kThreads) k_adj_cells(Ctx c, Adj a, int phase, int iext, int adv) {
@@ -282,7 +296,6 @@ npom_status launch_adj_phase(const npom_params *p, const npom_workspace *ws, con
   const size_t np = (size_t)c.im * c.jm * c.kb;
   const int ncol = c.im * c.jm;
   const unsigned gp = (unsigned)((np + kThreads - 1) / kThreads), gx = (unsigned)((ncol + kThreads - 1) / kThreads);
-  const unsigned gc = (unsigned)((ncol + 127) / 128);
   switch (r.phase) {
     case AP_EI: {
       // elf/d of the post step -> g = dJ/dx; the solve's adjoint gives
@@ -295,21 +308,21 @@ npom_status launch_adj_phase(const npom_params *p, const npom_workspace *ws, con
     }
     case AP_I5: k_adj_cells<<<gx, kThreads, 0, s>>>(c, a, r.phase, 0, 0); break;
     case AP_A1: k_adj_points<AP_A1><<<gp, kThreads, 0, s>>>(c, a); break;
-    case AP_A2: k_adj_cols<AP_A2><<<gc, 128, 0, s>>>(c, a); break;
+    case AP_A2: launch_adj_cols<AP_A2>(c, a, s); break;
     case AP_A3:
     case AP_E1:
     case AP_E2:
     case AP_E3: k_adj_cells<<<gx, kThreads, 0, s>>>(c, a, r.phase, r.iext, r.adv); break;
-    case AP_B1: k_adj_cols<AP_B1><<<gc, 128, 0, s>>>(c, a); break;
-    case AP_B2A: k_adj_cols<AP_B2A><<<gc, 128, 0, s>>>(c, a); break;
+    case AP_B1: launch_adj_cols<AP_B1>(c, a, s); break;
+    case AP_B2A: launch_adj_cols<AP_B2A>(c, a, s); break;
     case AP_B2B: k_adj_points<AP_B2B><<<gp, kThreads, 0, s>>>(c, a); break;
-    case AP_B3: k_adj_cols<AP_B3><<<gc, 128, 0, s>>>(c, a); break;
+    case AP_B3: launch_adj_cols<AP_B3>(c, a, s); break;
     case AP_B4: k_adj_points<AP_B4><<<gp, kThreads, 0, s>>>(c, a); break;
     case AP_B5: k_adj_points<AP_B5><<<gp, kThreads, 0, s>>>(c, a); break;
-    case AP_B6: k_adj_cols<AP_B6><<<gc, 128, 0, s>>>(c, a); break;
+    case AP_B6: launch_adj_cols<AP_B6>(c, a, s); break;
     case AP_B7: k_adj_points<AP_B7><<<gp, kThreads, 0, s>>>(c, a); break;
-    case AP_B8: k_adj_cols<AP_B8><<<gc, 128, 0, s>>>(c, a); break;
-    case AP_B9: k_adj_cols<AP_B9><<<gc, 128, 0, s>>>(c, a); break;
+    case AP_B8: launch_adj_cols<AP_B8>(c, a, s); break;
+    case AP_B9: launch_adj_cols<AP_B9>(c, a, s); break;
   }
   return NPOM_OK;
 }

@@ -286,21 +286,21 @@ void adj_plan_phase(const Ctx &c, const Adj &a, const AdjPhaseRec &r, const floa
     case AP_EI: imp_reverse(c, a, xs, g, lam, gd); break;
     case AP_I5: each_cell(c, [&](int i, int j) { phase_i5_cell_adj(c, a, i, j); }); break;
     case AP_A1: each_point(c, [&](int i, int j, int k) { phase_a1_point_adj(c, a, i, j, k); }); break;
-    case AP_A2: each_cell(c, [&](int i, int j) { phase_a2_column_adj(c, a, i, j); }); break;
+    case AP_A2: each_cell(c, [&](int i, int j) { phase_a2_column_adj<KMAX>(c, a, i, j); }); break;
     case AP_A3: each_cell(c, [&](int i, int j) { phase_a3_cell_adj(c, a, i, j); }); break;
     case AP_E1: each_cell(c, [&](int i, int j) { ext_phase1_cell_adj(c, a, i, j, r.adv != 0); }); break;
     case AP_E2: each_cell(c, [&](int i, int j) { ext_phase2_cell_adj(c, a, i, j, r.iext); }); break;
     case AP_E3: each_cell(c, [&](int i, int j) { ext_phase3_cell_adj(c, a, i, j, r.iext); }); break;
-    case AP_B1: each_cell(c, [&](int i, int j) { phase_b1_column_adj(c, a, i, j); }); break;
-    case AP_B2A: each_cell(c, [&](int i, int j) { phase_b2a_column_adj(c, a, i, j); }); break;
+    case AP_B1: each_cell(c, [&](int i, int j) { phase_b1_column_adj<KMAX>(c, a, i, j); }); break;
+    case AP_B2A: each_cell(c, [&](int i, int j) { phase_b2a_column_adj<KMAX>(c, a, i, j); }); break;
     case AP_B2B: each_point(c, [&](int i, int j, int k) { phase_b2b_point_adj(c, a, i, j, k); }); break;
-    case AP_B3: each_cell(c, [&](int i, int j) { phase_b3_column_adj(c, a, i, j); }); break;
+    case AP_B3: each_cell(c, [&](int i, int j) { phase_b3_column_adj<KMAX>(c, a, i, j); }); break;
     case AP_B4: each_point(c, [&](int i, int j, int k) { phase_b4_point_adj(c, a, i, j, k); }); break;
     case AP_B5: each_point(c, [&](int i, int j, int k) { phase_b5_point_adj(c, a, i, j, k); }); break;
-    case AP_B6: each_cell(c, [&](int i, int j) { phase_b6_column_adj(c, a, i, j); }); break;
+    case AP_B6: each_cell(c, [&](int i, int j) { phase_b6_column_adj<KMAX>(c, a, i, j); }); break;
     case AP_B7: each_point(c, [&](int i, int j, int k) { phase_b7_point_adj(c, a, i, j, k); }); break;
-    case AP_B8: each_cell(c, [&](int i, int j) { phase_b8_column_adj(c, a, i, j); }); break;
-    case AP_B9: each_cell(c, [&](int i, int j) { phase_b9_column_adj(c, a, i, j); }); break;
+    case AP_B8: each_cell(c, [&](int i, int j) { phase_b8_column_adj<KMAX>(c, a, i, j); }); break;
+    case AP_B9: each_cell(c, [&](int i, int j) { phase_b9_column_adj<KMAX>(c, a, i, j); }); break;
   }
 }
 
