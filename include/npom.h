@@ -278,6 +278,35 @@ npom_status npom_step_implicit_adjoint(const npom_params *p, float *const *field
                                        const npom_clock *clk, float *const *grads,
                                        const npom_adjoint_ws *aws, void *stream);
 
+/* ------------------------------------------------------------------ */
+/* Operators of the corrector coupling (hybrid/sparse_coupling.py:10-82) */
+/* and the cores' dens()/baropg() methods.  fields supplies geometry    */
+/* (h, zz, fsm, dx, dy, dt, dum, dvm) and, for DENS, the ghost level of */
+/* rho; arrays are (im, jm, kb), k fastest.                            */
+/* ------------------------------------------------------------------ */
+
+/* explicit/momentum.py:467-541: rho_out = DENS(t, s) on levels < kb-1,
+ * the ghost level copied from fields[rho]. */
+npom_status npom_dens(const npom_params *p, float *const *fields, const float *t,
+                      const float *s, float *rho_out, void *stream);
+/* Its vector-Jacobian product: grad_t, grad_s (levels < kb-1) and
+ * grad_rho_in (the ghost level) from grad_rho; all outputs written. */
+npom_status npom_dens_adjoint(const npom_params *p, float *const *fields,
+                              const float *t, const float *s, const float *grad_rho,
+                              float *grad_t, float *grad_s, float *grad_rho_in,
+                              void *stream);
+/* explicit/momentum.py:543-700 (the ramp passed in): drhox/drhoy from
+ * rho - rmean; rho_out = (rho - rmean) + rmean, the method's round trip. */
+npom_status npom_baropg(const npom_params *p, float *const *fields, const float *rho,
+                        const float *rmean, double ramp, float *rho_out, float *drhox,
+                        float *drhoy, void *stream);
+/* Its vector-Jacobian product, ACCUMULATED into grad_rho and grad_dt
+ * (d/d rmean = -d/d rho; the round trip has derivative one). */
+npom_status npom_baropg_adjoint(const npom_params *p, float *const *fields,
+                                const float *rho, const float *rmean, double ramp,
+                                const float *grad_drhox, const float *grad_drhoy,
+                                float *grad_rho, float *grad_dt, void *stream);
+
 /* Reads (and with clear != 0 zeroes) the device status word; blocks on
  * the stream. */
 npom_status npom_status_read(const npom_workspace *ws, int clear,

@@ -154,6 +154,14 @@ def load_library():
     lib.npom_proft.restype = i32
     lib.npom_proft.argtypes = [i32, i32, vp, vp, vp, i32, vp, vp, dbl, vp, vp, vp, i32, vp, dbl, vp, vp, vp, vp]
     lib.npom_status_read.restype = i32
+    lib.npom_dens.restype = i32
+    lib.npom_dens.argtypes = [P(NpomParams), P(FieldArray), vp, vp, vp, vp]
+    lib.npom_dens_adjoint.restype = i32
+    lib.npom_dens_adjoint.argtypes = [P(NpomParams), P(FieldArray), vp, vp, vp, vp, vp, vp, vp]
+    lib.npom_baropg.restype = i32
+    lib.npom_baropg.argtypes = [P(NpomParams), P(FieldArray), vp, vp, dbl, vp, vp, vp, vp]
+    lib.npom_baropg_adjoint.restype = i32
+    lib.npom_baropg_adjoint.argtypes = [P(NpomParams), P(FieldArray), vp, vp, dbl, vp, vp, vp, vp, vp]
     lib.npom_adjoint_save_floats.restype = ctypes.c_size_t
     lib.npom_adjoint_save_floats.argtypes = [P(NpomParams)]
     for fn in (lib.npom_step_explicit_adjoint, lib.npom_step_implicit_adjoint):

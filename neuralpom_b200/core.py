@@ -144,6 +144,20 @@ class B200Core:
             ptrs.append(t.data_ptr())
         return _abi.FieldArray(*ptrs)
 
+    def _fields_readonly(self):
+        """Field pointers for operators that only read the state (the
+        coupling's DENS/BAROPG): detached, converted copies where needed;
+        returns (FieldArray, tensors to keep alive)."""
+        keep, ptrs = [], []
+        for n in _abi.FIELD_NAMES:
+            t = getattr(self, n).detach()
+            shp = _abi.field_shape(n, self.im, self.jm, self.kb)
+            if tuple(t.shape) != shp or t.dtype != torch.float32 or t.device != self.device or not t.is_contiguous():
+                t = t.to(device=self.device, dtype=torch.float32).reshape(shp).contiguous()
+            keep.append(t)
+            ptrs.append(t.data_ptr())
+        return _abi.FieldArray(*ptrs), keep
+
     def params(self):
         return state.make_params(self, self.im, self.jm, self.kb, self.core_name,
                                  self.device.index if self.device.index is not None else torch.cuda.current_device())
@@ -210,6 +224,22 @@ class B200Core:
         if self.core_name != "explicit":
             self._eta_solver_iteration_history.extend(its)
         self._raise_for(bits)
+
+    # -- operator methods (override points of the reference cores) ----------
+    def dens(self):
+        """DENS (explicit/momentum.py:467-541): rho on levels < kb-1 from
+        (t, s), returned like the reference as (s, t, rho)."""
+        from .coupling import eos
+        self.rho = eos(self, self.t, self.s)
+        return self.s, self.t, self.rho
+
+    def baropg(self):
+        """BAROPG (explicit/momentum.py:543-700): returns (rho, drhox,
+        drhoy) at the core's ramp; rho goes through the reference's
+        (rho - rmean) + rmean round trip."""
+        from .coupling import _BaropgFunction
+        self.rho, drhox, drhoy = _BaropgFunction.apply(self, self.rho, self.rmean, self.dt)
+        return self.rho, drhox, drhoy
 
     def _differentiable_call(self):
         if not torch.is_grad_enabled():

@@ -409,3 +409,91 @@ npom_status run_step_adjoint(const npom_params *p, float *const *fields, const n
   }
   return cudaGetLastError() == cudaSuccess ? NPOM_OK : NPOM_ERR_CUDA;
 }
+
+// ---------------------------------------------------------------------------
+// Stand-alone DENS and BAROPG with their adjoints (the core's dens() and
+// baropg() operator methods and the corrector coupling: explicit
+// momentum.py:467-700, hybrid/sparse_coupling.py:10-82).
+// ---------------------------------------------------------------------------
+
+// rho_out = DENS(t, s) on levels < kb-1, the ghost level copied from F rho
+__global__ void __launch_bounds__(kThreads) k_dens(Ctx c, const float *t, const float *s, float *rho_out) {
+  const size_t n = (size_t)c.im * c.jm * c.kb;
+  const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int k = (int)(p % c.kb);
+  const size_t col = p / c.kb;
+  const int j = (int)(col % c.jm), i = (int)(col / c.jm);
+  rho_out[p] = k < c.kb - 1 ? dens_point(c, t[p], s[p], i, j, k) : F3(rho, i, j, k);
+}
+
+__global__ void __launch_bounds__(kThreads) k_dens_adj(Ctx c, const float *t, const float *s, const float *g,
+                                                       float *gt, float *gs, float *grho) {
+  const size_t n = (size_t)c.im * c.jm * c.kb;
+  const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int k = (int)(p % c.kb);
+  const size_t col = p / c.kb;
+  const int j = (int)(col % c.jm), i = (int)(col / c.jm);
+  if (k < c.kb - 1) {
+    float dt_, ds_;
+    dens_point_adj(c, t[p], s[p], i, j, k, dt_, ds_);
+    gt[p] = g[p] * dt_;
+    gs[p] = g[p] * ds_;
+    grho[p] = 0.0f;
+  } else {
+    gt[p] = 0.0f;
+    gs[p] = 0.0f;
+    grho[p] = g[p];
+  }
+}
+
+// BAROPG of the column with c.F[rho]/[rmean]/[drhox]/[drhoy] pointing at
+// the caller's arrays; rho_out = (rho - rmean) + rmean, the reference's
+// round trip
+__global__ void __launch_bounds__(128) k_baropg(Ctx c, float *rho_out) {
+  const int n = c.im * c.jm;
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= n) return;
+  const int j = col % c.jm, i = col / c.jm;
+  baropg_column(c, i, j);
+  for (int k = 0; k < c.kb; ++k) {
+    const float rm = F3(rmean, i, j, k);
+    rho_out[NPOM_I3(c, i, j, k)] = (F3(rho, i, j, k) - rm) + rm;
+  }
+}
+
+template <int KM>
+__global__ void __launch_bounds__(128) k_baropg_adj(Ctx c, Adj a, const float *gx, const float *gy) {
+  const int n = c.im * c.jm;
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= n) return;
+  const int j = col % c.jm, i = col / c.jm;
+  if (!interior(c, i, j)) return;
+  float lx[KM], ly[KM];
+  for (int k = 0; k < c.kb; ++k) {
+    lx[k] = gx[NPOM_I3(c, i, j, k)];
+    ly[k] = gy[NPOM_I3(c, i, j, k)];
+  }
+  baropg_column_adj<KM>(c, a, i, j, lx, ly);
+}
+
+bool fields_ok(const npom_params *p, float *const *fields) {
+  if (!p || !fields || p->im < 3 || p->jm < 3 || p->kb < 3 || p->kb > KMAX) return false;
+  for (int f = 0; f < NPOM_NFIELDS; ++f)
+    if (!fields[f]) return false;
+  return cudaSetDevice(p->device) == cudaSuccess;
+}
+
+Ctx fields_ctx(const npom_params *p, float *const *fields) {
+  Ctx c;
+  std::memset(&c, 0, sizeof(c));
+  c.im = p->im;
+  c.jm = p->jm;
+  c.kb = p->kb;
+  for (int f = 0; f < NPOM_NFIELDS; ++f) c.F[f] = fields[f];
+  c.k = make_consts(*p);
+  c.ramp = 1.0f;
+  c.do_internal = 1;
+  return c;
+}

@@ -1167,6 +1167,59 @@ npom_status npom_step_implicit_adjoint(const npom_params *p, float *const *field
   return run_step_adjoint(p, fields, ws, clk, grads, aws, NPOM_CORE_IMPLICIT, (cudaStream_t)stream);
 }
 
+npom_status npom_dens(const npom_params *p, float *const *fields, const float *t, const float *s, float *rho_out,
+                      void *stream) {
+  if (!fields_ok(p, fields) || !t || !s || !rho_out) return NPOM_ERR_ARG;
+  Ctx c = fields_ctx(p, fields);
+  const size_t n = (size_t)c.im * c.jm * c.kb;
+  k_dens<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, (cudaStream_t)stream>>>(c, t, s, rho_out);
+  return cudaGetLastError() == cudaSuccess ? NPOM_OK : NPOM_ERR_CUDA;
+}
+
+npom_status npom_dens_adjoint(const npom_params *p, float *const *fields, const float *t, const float *s,
+                              const float *grad_rho, float *grad_t, float *grad_s, float *grad_rho_in, void *stream) {
+  if (!fields_ok(p, fields) || !t || !s || !grad_rho || !grad_t || !grad_s || !grad_rho_in) return NPOM_ERR_ARG;
+  Ctx c = fields_ctx(p, fields);
+  const size_t n = (size_t)c.im * c.jm * c.kb;
+  k_dens_adj<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, (cudaStream_t)stream>>>(
+      c, t, s, grad_rho, grad_t, grad_s, grad_rho_in);
+  return cudaGetLastError() == cudaSuccess ? NPOM_OK : NPOM_ERR_CUDA;
+}
+
+npom_status npom_baropg(const npom_params *p, float *const *fields, const float *rho, const float *rmean, double ramp,
+                        float *rho_out, float *drhox, float *drhoy, void *stream) {
+  if (!fields_ok(p, fields) || !rho || !rmean || !rho_out || !drhox || !drhoy) return NPOM_ERR_ARG;
+  Ctx c = fields_ctx(p, fields);
+  c.F[NPOM_F_rho] = const_cast<float *>(rho);
+  c.F[NPOM_F_rmean] = const_cast<float *>(rmean);
+  c.F[NPOM_F_drhox] = drhox;
+  c.F[NPOM_F_drhoy] = drhoy;
+  c.ramp = (float)ramp;
+  const int n = c.im * c.jm;
+  k_baropg<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(c, rho_out);
+  return cudaGetLastError() == cudaSuccess ? NPOM_OK : NPOM_ERR_CUDA;
+}
+
+npom_status npom_baropg_adjoint(const npom_params *p, float *const *fields, const float *rho, const float *rmean,
+                                double ramp, const float *grad_drhox, const float *grad_drhoy, float *grad_rho,
+                                float *grad_dt, void *stream) {
+  if (!fields_ok(p, fields) || !rho || !rmean || !grad_drhox || !grad_drhoy || !grad_rho || !grad_dt)
+    return NPOM_ERR_ARG;
+  Ctx c = fields_ctx(p, fields);
+  c.F[NPOM_F_rho] = const_cast<float *>(rho);
+  c.F[NPOM_F_rmean] = const_cast<float *>(rmean);
+  c.ramp = (float)ramp;
+  Adj a;
+  std::memset(&a, 0, sizeof(a));
+  a.G[NPOM_F_rho] = grad_rho;  // accumulated: the caller zeroes or seeds them
+  a.G[NPOM_F_dt] = grad_dt;
+  const int n = c.im * c.jm;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (c.kb == 16) k_baropg_adj<16><<<(n + 127) / 128, 128, 0, s>>>(c, a, grad_drhox, grad_drhoy);
+  else k_baropg_adj<KMAX><<<(n + 127) / 128, 128, 0, s>>>(c, a, grad_drhox, grad_drhoy);
+  return cudaGetLastError() == cudaSuccess ? NPOM_OK : NPOM_ERR_CUDA;
+}
+
 npom_status npom_run_phase(const npom_params *p, float *const *fields, const npom_workspace *ws, int phase,
                            double ramp, void *stream) {
   if (!check_args_dev(p, fields, ws) || phase < 0 || phase >= kNumPhases) return NPOM_ERR_ARG;

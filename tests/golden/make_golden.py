@@ -3,7 +3,7 @@
 Run in a container that holds the reference sources (default
 ``/root/reference/src``, or ``NPOM_REFERENCE_SRC``)::
 
-    python tests/golden/make_golden.py [proft] [steps] [adjoint] [coastal] [step_adjoint]
+    python tests/golden/make_golden.py [proft] [steps] [adjoint] [coastal] [step_adjoint] [coupling]
 
 Writes ``tests/golden/*.npz``.  Every file records the reference's own CPU
 float32 outputs on seeded inputs; nothing here is needed at test time except
@@ -255,7 +255,71 @@ def make_step_adjoint_goldens():
     make_step_adjoint_golden("implicit_rest", core, steps=(1, 2), seed=39, name=name)
 
 
-def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint")):
+COUPLING_LEAVES = ("u", "ub", "v", "vb", "t", "tb", "s", "sb", "rho", "et", "etf", "dt")
+
+
+def make_coupling_golden(im=12, jm=10, seed=41):
+    """The reference's corrector coupling under torch autograd
+    (hybrid/sparse_coupling.py:10-82) on a perturbed explicit core:
+    apply_joint_correction with a seeded raw output large enough to engage
+    the paired limiter, and pressure_velocity_error against a perturbed
+    reference (t, s); seeded cotangents on every output, gradients of the
+    state leaves and of raw."""
+    import torch
+    from neuralpom.hybrid import sparse_coupling as sc
+    core = perturbed_core("explicit", im, jm, seed)
+    arrays, scalars = rh.extract_state(core)
+    out = {f"in__{k}": v for k, v in arrays.items()}
+    for k, v in scalars.items():
+        out[f"scalar__{k}"] = np.asarray(v)
+    g = torch.Generator().manual_seed(seed + 1)
+    raw = (2.0 * torch.randn((sc.OUTPUT_CHANNELS, im, jm), generator=g)).requires_grad_(True)
+    scales = {"u": 0.05, "v": 0.05, "t": 0.2, "s": 0.05}
+    leaves = {}
+    for f in COUPLING_LEAVES:
+        leaves[f] = getattr(core, f).detach().clone().requires_grad_(True)
+        setattr(core, f, leaves[f])
+    info = sc.apply_joint_correction(core, raw, scales)
+    outs = {f: getattr(core, f) for f in ("u", "ub", "v", "vb", "t", "tb", "s", "sb", "rho")}
+    cot = {f: torch.randn(v.shape, generator=g) for f, v in outs.items()}
+    loss = sum((outs[f] * cot[f]).sum() for f in outs) + 3.0 * info["ts_limit_factor"] + 5.0 * info["t_budget"]
+    loss.backward()
+    out["jc__raw"] = raw.detach().numpy()
+    out["jc__scales"] = np.array([scales[f] for f in sc.OUTPUT_FIELDS])
+    for f, v in outs.items():
+        out[f"jc_out__{f}"] = v.detach().numpy()
+        out[f"jc_cot__{f}"] = cot[f].numpy()
+    for k in ("ts_limit_factor", "t_budget", "s_budget"):
+        out[f"jc_info__{k}"] = np.asarray(float(info[k]))
+    out["jc_grad__raw"] = raw.grad.numpy()
+    for f in COUPLING_LEAVES:
+        if leaves[f].grad is not None:
+            out[f"jc_grad__{f}"] = leaves[f].grad.numpy()
+    # pressure_velocity_error on a fresh copy of the start state
+    c2 = rh.build_reference_core("explicit", im, jm)
+    rh.load_state(c2, arrays, scalars)
+    leaves = {}
+    for f in COUPLING_LEAVES:
+        leaves[f] = getattr(c2, f).detach().clone().requires_grad_(True)
+        setattr(c2, f, leaves[f])
+    ref_t = (c2.t.detach() + 0.3 * torch.randn(c2.t.shape, generator=g) * c2.fsm[:, :, None]).requires_grad_(True)
+    ref_s = (c2.s.detach() + 0.05 * torch.randn(c2.s.shape, generator=g) * c2.fsm[:, :, None]).requires_grad_(True)
+    ku, kv = sc.pressure_velocity_error(c2, ref_t, ref_s)
+    cu, cv = torch.randn(ku.shape, generator=g), torch.randn(kv.shape, generator=g)
+    ((ku * cu).sum() + (kv * cv).sum()).backward()
+    out["pv__ref_t"], out["pv__ref_s"] = ref_t.detach().numpy(), ref_s.detach().numpy()
+    out["pv_out__u"], out["pv_out__v"] = ku.detach().numpy(), kv.detach().numpy()
+    out["pv_cot__u"], out["pv_cot__v"] = cu.numpy(), cv.numpy()
+    out["pv_grad__ref_t"], out["pv_grad__ref_s"] = ref_t.grad.numpy(), ref_s.grad.numpy()
+    for f in COUPLING_LEAVES:
+        if leaves[f].grad is not None:
+            out[f"pv_grad__{f}"] = leaves[f].grad.numpy()
+    path = os.path.join(HERE, f"coupling_{im}x{jm}.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "limit factor", float(info["ts_limit_factor"]))
+
+
+def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint", "coupling")):
     src = rh.default_reference_path()
     if src is None:
         raise SystemExit("reference sources not found; set NPOM_REFERENCE_SRC")
@@ -274,7 +338,9 @@ def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint")):
         make_coastal_golden()
     if "step_adjoint" in which:
         make_step_adjoint_goldens()
+    if "coupling" in which:
+        make_coupling_golden()
 
 
 if __name__ == "__main__":
-    main(tuple(sys.argv[1:]) or ("proft", "steps", "adjoint", "coastal", "step_adjoint"))
+    main(tuple(sys.argv[1:]) or ("proft", "steps", "adjoint", "coastal", "step_adjoint", "coupling"))
