@@ -584,11 +584,11 @@ def _fa_targets(A, seed, dev=None):
     return out, incs
 
 
-def fwd_adjoint_timing(core, start, tgt, incs, intervals, steps_per_interval, t0, reps, warm, dev):
+def fwd_adjoint_timing(core, start, tgt, correct, intervals, steps_per_interval, t0, reps, warm, dev):
     """Median CUDA-event time (ms) of forward+backward through the drop-in
     API under torch autograd: every state field a leaf, ``intervals``
     differentiable run_time_loop() calls of ``steps_per_interval`` internal
-    steps with the increments between them, MSE(u, v, T, S) loss,
+    steps with ``correct(core)`` between them, MSE(u, v, T, S) loss,
     backward()."""
     import torch
     from neuralpom_b200 import _abi
@@ -605,9 +605,8 @@ def fwd_adjoint_timing(core, start, tgt, incs, intervals, steps_per_interval, t0
             core.time0 = t0 + k * steps_per_interval * dti / 86400.0
             core.iend = steps_per_interval
             core.run_time_loop()
-            if k < intervals - 1:
-                for f, d in incs.items():
-                    setattr(core, f, getattr(core, f) + d)
+            if k < intervals - 1 and correct is not None:
+                correct(core)
         loss = sum(((getattr(core, f) - tgt[f]) ** 2).mean() for f in tgt)
         loss.backward()
 
@@ -645,7 +644,7 @@ def seamount_fwd_adjoint(core, args, dev, nsteps=36, reps=3):
     tgt, _ = _fa_targets(A, 11)
     tgt = {f: torch.from_numpy(v).to(dev) for f, v in tgt.items()}
     t0 = float(core.time)
-    best = fwd_adjoint_timing(core, start, tgt, {}, 1, nsteps, t0, reps, args.warmup, dev)
+    best = fwd_adjoint_timing(core, start, tgt, None, 1, nsteps, t0, reps, args.warmup, dev)
     days = nsteps * float(core.dti) / 86400.0
     core.time = t0
     return {"value": days / (best / 1000.0), "unit": UNIT, "ms_per_sample": best,
@@ -674,7 +673,7 @@ def coastal_fwd_adjoint(args, dev, nsteps=360):
     torch.cuda.synchronize(dev)
     torch.cuda.reset_peak_memory_stats(dev)
     base = torch.cuda.memory_allocated(dev)
-    best = fwd_adjoint_timing(core, start, tgt, {}, 1, nsteps, float(Sc["time"]), 1, 1, dev)
+    best = fwd_adjoint_timing(core, start, tgt, None, 1, nsteps, float(Sc["time"]), 1, 1, dev)
     peak = torch.cuda.max_memory_allocated(dev)
     days = nsteps * float(core.dti) / 86400.0
     return {"value": days / (best / 1000.0), "unit": UNIT, "ms_per_sample": best,
@@ -693,21 +692,31 @@ def fwd_adjoint_sample(args, dev, reps=3):
     ``fwd_adjoint_timing``)."""
     import torch
     from neuralpom_b200 import _abi, resolve_core_class
+    from neuralpom_b200 import coupling
     A, Sc = midtrain_case(0)
     core = resolve_core_class("explicit").from_state(A, Sc, device=dev)
-    tgt, incs = _fa_targets(A, 7)
+    tgt, _ = _fa_targets(A, 7)
     tgt = {f: torch.from_numpy(v).to(dev) for f, v in tgt.items()}
-    incs = {f: torch.from_numpy(v).to(dev) for f, v in incs.items()}
     start = {f: getattr(core, f).detach().clone() for f in _abi.FIELD_NAMES}
-    best = fwd_adjoint_timing(core, start, tgt, incs, FA_INTERVALS, FA_STEPS_PER_INTERVAL, float(Sc["time"]), reps,
-                              args.warmup, dev)
+    # the network's raw output between intervals (seeded, unit scales),
+    # itself a leaf: gradients reach it as they would reach a U-Net
+    g = torch.Generator(device=dev).manual_seed(17)
+    raw = (1e-3 * torch.randn((coupling.OUTPUT_CHANNELS, core.im, core.jm), generator=g, device=dev)).requires_grad_()
+    scales = {f: 1.0 for f in coupling.OUTPUT_FIELDS}
+
+    def correct(c):
+        coupling.apply_joint_correction(c, raw, scales)
+
+    best = fwd_adjoint_timing(core, start, tgt, correct, FA_INTERVALS, FA_STEPS_PER_INTERVAL, float(Sc["time"]),
+                              reps, args.warmup, dev)
     nint = FA_INTERVALS * FA_STEPS_PER_INTERVAL
     days = nint * float(core.dti) / 86400.0
     return {"value": days / (best / 1000.0), "unit": UNIT, "ms_per_sample": best,
             "workload": f"explicit core, {FA_GRID[0]}x{FA_GRID[1]}x{FA_GRID[2]} noise basin (dtE=6 s, isplit=20, "
                         f"dtI=120 s), T/S/u/v-perturbed member; {FA_INTERVALS} x 1 h intervals ({nint} internal "
-                        "steps) with an additive T/S/u/v increment between them, MSE(u,v,T,S) loss, backward to "
-                        "every state field; checkpoint per internal step, hand-written CUDA step adjoint",
+                        "steps) with apply_joint_correction of a seeded raw (60, im, jm) output (unit scales) between "
+                        "them, MSE(u,v,T,S) loss, backward to every state field and the raw output; checkpoint per "
+                        "internal step, hand-written CUDA step adjoint",
             "timing": f"median of {reps} samples, CUDA events around forward+backward (L2 not flushed: the "
                       "90x82x16 state fits in L2)"}
 
