@@ -95,6 +95,11 @@ def parse():
                     help="ensemble members advanced concurrently on one GPU for the 'ensemble' key (1 = skip)")
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference core on this GPU")
     ap.add_argument("--no-fwd-adjoint", action="store_true", help="skip the forward+adjoint sample")
+    ap.add_argument("--fa-steps", type=int, default=36,
+                    help="internal steps of the headline forward+adjoint sample")
+    ap.add_argument("--fa-reps", type=int, default=3, help="timed forward+adjoint samples (median)")
+    ap.add_argument("--fa-only", action="store_true",
+                    help="headline forward+adjoint sample only (after --warmup forward days); for profiling")
     return ap.parse_args()
 
 
@@ -285,6 +290,15 @@ def run_b200(args):
     bits, _ = core.read_status(nin)
     if bits & (_abi.DEV_TIMEOUT | _abi.DEV_VMAX | _abi.DEV_NONFINITE):
         raise RuntimeError(f"device status 0x{bits:x} during warm-up")
+    if args.fa_only:
+        # profiling mode: the workload's forward+adjoint sample alone
+        if args.workload == "coastal":
+            fa = coastal_fwd_adjoint(args, dev, nsteps=args.fa_steps)
+        else:
+            fa, _, _ = seamount_fwd_adjoint(core, args, dev, nsteps=args.fa_steps, reps=args.fa_reps)
+        if rank == 0:
+            print(json.dumps({"fwd_adjoint": fa}), flush=True)
+        return
 
     launches = 0
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -333,17 +347,17 @@ def run_b200(args):
     if rank == 0 and ws_n == 1 and args.workload == "coastal" and not args.no_fwd_adjoint:
         fa = coastal_fwd_adjoint(args, dev)
     if rank == 0 and ws_n == 1 and args.workload == "seamount" and not args.no_fwd_adjoint:
-        fa, A_dev, t_dev = seamount_fwd_adjoint(core, args, dev)
+        fa, A_dev, t_dev = seamount_fwd_adjoint(core, args, dev, nsteps=args.fa_steps, reps=args.fa_reps)
         case = (A_dev, dict(Sc, time=t_dev, time0=t_dev))
         if not args.no_ref_gpu:
             fa["reference_gpu"] = reference_fwd_adjoint_sample(dev, case=case, core_name=W["core"], seed=11)
         if not args.no_cpu_baseline:
             fa["reference_cpu"] = reference_fwd_adjoint_sample("cpu", internal_steps=3, case=case,
                                                                core_name=W["core"], seed=11)
-        fam = fwd_adjoint_sample(args, dev)
-        if not args.no_ref_gpu:
+        fam = None if args.fa_only else fwd_adjoint_sample(args, dev)
+        if fam is not None and not args.no_ref_gpu:
             fam["reference_gpu"] = reference_fwd_adjoint_sample(dev)
-        if not args.no_cpu_baseline:
+        if fam is not None and not args.no_cpu_baseline:
             fam["reference_cpu"] = reference_fwd_adjoint_sample("cpu", internal_steps=3)
 
     out = {
