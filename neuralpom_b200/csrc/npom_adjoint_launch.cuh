@@ -74,16 +74,25 @@ __global__ void __launch_bounds__(kThreads) k_adj_cells(Ctx c, Adj a, int phase,
   else ext_phase3_cell_adj(c, a, i, j, iext);
 }
 
-// The whole external subcycle of the recomputation on one thread-block
-// cluster (grids of up to kSubClusterCells cells): before each phase every
-// thread saves the values of the fields the phase overwrites at the cells it
-// computes (the same thread-to-cell map, so no barrier is needed between
-// save and compute), then computes the phase; the cluster barrier separates
-// the phases.  Loads go through L2 (Ctx::coh).  save + base is the first
-// external-phase record of the plan; records follow in plan order.
-template <int T>
-__global__ void __launch_bounds__(T, 1) k_adj_ext_forward(Ctx c, float *save) {
-  cgx::cluster_group cl = cgx::this_cluster();
+// The barrier between the phases of the fused external-subcycle adjoint
+// kernels: the hardware cluster barrier (one cluster, up to 16,384 cells)
+// or the counting grid barrier of a cooperative launch (larger grids; its
+// wait is bounded and a timeout sets NPOM_DEV_TIMEOUT).
+template <bool GRID>
+__device__ __forceinline__ bool ext_sync(const Ctx &c) {
+  if (GRID) return grid_barrier(c);
+  cgx::this_cluster().sync();
+  return true;
+}
+
+// The whole external subcycle of the recomputation in one launch: before
+// each phase every thread saves the values of the fields the phase
+// overwrites at the cells it computes (the same thread-to-cell map, so no
+// barrier is needed between save and compute), then computes the phase; a
+// barrier separates the phases.  Loads go through L2 (Ctx::coh).  save is
+// the first external-phase record of the plan; records follow in plan order.
+template <int T, bool GRID>
+__global__ void __launch_bounds__(T, GRID ? 0 : 1) k_adj_ext_forward(Ctx c, float *save) {
   const size_t ncell = (size_t)c.im * c.jm;
   const size_t stride = (size_t)gridDim.x * blockDim.x;
   const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -104,19 +113,18 @@ __global__ void __launch_bounds__(T, 1) k_adj_ext_forward(Ctx c, float *save) {
         else if (ph == 2) (void)ext_phase2_cell(c, i, j, iext);
         else ext_phase3_cell(c, i, j, iext);
       }
-      cl.sync();
+      if (!ext_sync<GRID>(c)) return;
     }
   }
 }
 
-// The reverse sweep of the external subcycle on one cluster: for each
-// phase from the last, restore its inputs and move the cotangents of what it
-// wrote (each thread its own cells), cluster barrier, the phase's adjoint
-// (scatters are atomics in L2; every other read goes through L2 or is of a
-// value the thread itself moved), cluster barrier.
-template <int T>
-__global__ void __launch_bounds__(T, 1) k_adj_ext_reverse(Ctx c, Adj a, const float *save_end) {
-  cgx::cluster_group cl = cgx::this_cluster();
+// The reverse sweep of the external subcycle in one launch: for each phase
+// from the last, restore its inputs and move the cotangents of what it
+// wrote (each thread its own cells), barrier, the phase's adjoint (scatters
+// are atomics in L2; every other read goes through L2 or is of a value the
+// thread itself moved), barrier.
+template <int T, bool GRID>
+__global__ void __launch_bounds__(T, GRID ? 0 : 1) k_adj_ext_reverse(Ctx c, Adj a, const float *save_end) {
   const size_t ncell = (size_t)c.im * c.jm;
   const size_t stride = (size_t)gridDim.x * blockDim.x;
   const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -135,37 +143,51 @@ __global__ void __launch_bounds__(T, 1) k_adj_ext_reverse(Ctx c, Adj a, const fl
           g[q] = 0.0f;
         }
       }
-      cl.sync();
+      if (!ext_sync<GRID>(c)) return;
       for (size_t q = tid; q < ncell; q += stride) {
         const int i = (int)(q / c.jm), j = (int)(q % c.jm);
         if (ph == 3) ext_phase3_cell_adj(c, a, i, j, iext);
         else if (ph == 2) ext_phase2_cell_adj(c, a, i, j, iext);
         else ext_phase1_cell_adj(c, a, i, j, adv);
       }
-      cl.sync();
+      if (!ext_sync<GRID>(c)) return;
     }
   }
 }
 
-const void *const kAdjExtForward[3] = {(const void *)k_adj_ext_forward<256>, (const void *)k_adj_ext_forward<512>,
-                                       (const void *)k_adj_ext_forward<1024>};
-const void *const kAdjExtReverse[3] = {(const void *)k_adj_ext_reverse<256>, (const void *)k_adj_ext_reverse<512>,
-                                       (const void *)k_adj_ext_reverse<1024>};
+const void *const kAdjExtForward[3] = {(const void *)k_adj_ext_forward<256, false>,
+                                       (const void *)k_adj_ext_forward<512, false>,
+                                       (const void *)k_adj_ext_forward<1024, false>};
+const void *const kAdjExtReverse[3] = {(const void *)k_adj_ext_reverse<256, false>,
+                                       (const void *)k_adj_ext_reverse<512, false>,
+                                       (const void *)k_adj_ext_reverse<1024, false>};
+const void *const kAdjExtForwardGrid = (const void *)k_adj_ext_forward<kThreads, true>;
+const void *const kAdjExtReverseGrid = (const void *)k_adj_ext_reverse<kThreads, true>;
 
-// Cluster shape of the fused external-subcycle adjoint kernels (0: use the
-// per-phase launches), decided outside any capture; NPOM_ADJ_EXT=phases
-// forces those.  Both kernels get the shape that fits both.
+// Launch shape of the fused external-subcycle adjoint kernels, decided
+// outside any capture: < 0 a cluster shape (encode_cluster, both kernels
+// get the one that fits both), > 0 cooperative grid blocks (larger grids),
+// 0 one launch per substep phase (NPOM_ADJ_EXT=phases, or no fit).
+// NPOM_ADJ_EXT=grid forces the cooperative form on small grids too.
 int plan_adj_ext(const Ctx &c) {
   const char *env = getenv("NPOM_ADJ_EXT");
   if (env && std::strcmp(env, "phases") == 0) return 0;
+  const bool grid = (env && std::strcmp(env, "grid") == 0);
   const size_t ncell = (size_t)c.im * c.jm;
-  if (ncell > kSubClusterCells) return 0;
-  int f = 0, r = 0;
-  if (plan_cluster(kAdjExtForward, ncell, &f) != cudaSuccess || plan_cluster(kAdjExtReverse, ncell, &r) != cudaSuccess) {
+  if (!grid && ncell <= kSubClusterCells) {
+    int f = 0, r = 0;
+    if (plan_cluster(kAdjExtForward, ncell, &f) == cudaSuccess &&
+        plan_cluster(kAdjExtReverse, ncell, &r) == cudaSuccess)
+      return cluster_ctas(f) <= cluster_ctas(r) ? f : r;
+    cudaGetLastError();
+  }
+  int bf = 0, br = 0;
+  if (coop_blocks(kAdjExtForwardGrid, ncell, &bf) != cudaSuccess ||
+      coop_blocks(kAdjExtReverseGrid, ncell, &br) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
-  return cluster_ctas(f) <= cluster_ctas(r) ? f : r;
+  return std::min(bf, br);
 }
 
 // Implicit free surface, forward: the solution x of the PCG (run without its
@@ -377,6 +399,7 @@ npom_status run_step_adjoint(const npom_params *p, float *const *fields, const n
   const int ext_shape = e0 < e1 ? plan_adj_ext(c) : 0;
   const int ext_threads = ext_shape < 0 ? cluster_threads(ext_shape) : 0;
   const int ext_t = ext_threads == 256 ? 0 : (ext_threads == 512 ? 1 : 2);
+  const bool ext_fused = ext_shape != 0;
   const int ext_ctas = ext_shape < 0 ? cluster_ctas(ext_shape) : 0;
   Ctx cc = c;
   cc.coh = 1;
@@ -385,10 +408,13 @@ npom_status run_step_adjoint(const npom_params *p, float *const *fields, const n
                                        adj_field_len(c, plan[e1 - 1].fld[plan[e1 - 1].n - 1])
                                  : nullptr;
   for (int q = 0; q < np; ++q) {
-    if (ext_ctas > 0 && q >= e0 && q < e1) {
+    if (ext_fused && q >= e0 && q < e1) {
       if (q == e0) {
         void *args[] = {&cc, &ext_save};
-        if (launch_cluster(kAdjExtForward[ext_t], ext_ctas, ext_threads, args, s) != cudaSuccess) return NPOM_ERR_CUDA;
+        const cudaError_t e = ext_shape < 0
+                                  ? launch_cluster(kAdjExtForward[ext_t], ext_ctas, ext_threads, args, s)
+                                  : launch_coop(kAdjExtForwardGrid, ext_shape, args, c.sync, s);
+        if (e != cudaSuccess) return NPOM_ERR_CUDA;
       }
       continue;
     }
@@ -396,10 +422,13 @@ npom_status run_step_adjoint(const npom_params *p, float *const *fields, const n
     launch_fwd_phase(c, plan[q], pplan, is, s);
   }
   for (int q = np - 1; q >= 0; --q) {
-    if (ext_ctas > 0 && q >= e0 && q < e1) {
+    if (ext_fused && q >= e0 && q < e1) {
       if (q == e0) {
         void *args[] = {&cc, &a, &ext_end};
-        if (launch_cluster(kAdjExtReverse[ext_t], ext_ctas, ext_threads, args, s) != cudaSuccess) return NPOM_ERR_CUDA;
+        const cudaError_t e = ext_shape < 0
+                                  ? launch_cluster(kAdjExtReverse[ext_t], ext_ctas, ext_threads, args, s)
+                                  : launch_coop(kAdjExtReverseGrid, ext_shape, args, c.sync, s);
+        if (e != cudaSuccess) return NPOM_ERR_CUDA;
       }
       continue;
     }

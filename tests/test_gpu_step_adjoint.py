@@ -32,8 +32,10 @@ def _differentiable_advance(core, nsteps, time0):
 
 
 ADJOINT_CASES = [("step_adjoint_explicit_12x10.npz", "cluster"), ("step_adjoint_explicit_12x10.npz", "phases"),
+                 ("step_adjoint_explicit_12x10.npz", "grid"),
                  ("step_adjoint_rest_12x10.npz", "cluster"), ("step_adjoint_rest_12x10.npz", "phases"),
                  ("step_adjoint_coastal_16x14.npz", "cluster"), ("step_adjoint_coastal_16x14.npz", "phases"),
+                 ("step_adjoint_coastal_16x14.npz", "grid"),
                  ("step_adjoint_implicit_12x10.npz", "-"), ("step_adjoint_implicit_rest_12x10.npz", "-")]
 
 
@@ -43,9 +45,9 @@ def _core_name(fname):
 
 @pytest.mark.parametrize("fname,ext", ADJOINT_CASES)
 def test_gpu_step_adjoint_matches_reference_autograd(monkeypatch, fname, ext):
-    """Both cores; for the explicit one both forms of the external-subcycle
-    adjoint (the two fused thread-block-cluster kernels, one launch per
-    substep phase)."""
+    """Both cores; for the explicit one every form of the external-subcycle
+    adjoint (the two fused kernels on one thread-block cluster or as
+    cooperative grid launches, one launch per substep phase)."""
     if ext != "-":
         monkeypatch.setenv("NPOM_ADJ_EXT", ext)
     A, Sc, cot, grads = load_adjoint_golden(fname)
@@ -143,8 +145,8 @@ def test_gpu_physics_differentiable_advance_in_chunks():
 
 def test_gpu_coastal_step_adjoint_large_grid_matches_float64_differences():
     """The large-grid forms (flux-once A1/B5 tiles and thread-per-column
-    PROFT in the recomputation, one launch per external-substep phase in the
-    reverse: 150x120 = 18,000 cells) on the coastal basin with its open
+    PROFT in the recomputation, the cooperative grid-barrier kernels of the
+    external subcycle's adjoint: 150x120 = 18,000 cells) on the coastal basin with its open
     boundary: two steps from a developed state, loss = MSE of u, v, T, S
     against a seeded target, the CUDA gradient along 4 random unit
     directions of (T, S, u, v) against central differences (eps = 1e-3) of
