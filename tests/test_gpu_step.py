@@ -223,3 +223,31 @@ def test_gpu_explicit_double_gyre_48_steps_matches_oracle():
         bound = 1e-5 if f in ("t", "s") else max(10.0 * spread, 1e-5)
         err = rel_err(getattr(c, f).cpu().numpy(), S[f])
         assert err <= bound, (f, err, spread)
+
+
+def test_gpu_restart_continues_bitwise(tmp_path):
+    """save_restart after some steps, continue; load_restart, continue the
+    same steps again: bitwise the same state (the reference's bit-exact
+    restart test, tests/test_fixed_core_runtime.py:91-138)."""
+    from neuralpom_b200 import cases, formats, resolve_core_class
+    A, Sc = cases.seamount(24, 20)
+    Sc = dict(Sc)
+    core = resolve_core_class("implicit_p0_fixed").from_state(A, Sc, device="cuda")
+    core.time0 = float(core.time)
+    core.iend = 3
+    core.run_time_loop()
+    formats.save_restart(tmp_path / "restart.pt", core)
+    t_restart = float(core.time)
+
+    def advance():
+        core.time0 = float(core.time)
+        core.iend = 4
+        core.run_time_loop()
+        return {n: getattr(core, n).detach().cpu().clone() for n in ("u", "v", "t", "s", "el", "elb", "q2", "km")}
+
+    first = advance()
+    formats.load_restart(tmp_path / "restart.pt", core)
+    assert float(core.time) == t_restart
+    second = advance()
+    for n in first:
+        assert torch.equal(first[n], second[n]), n
