@@ -91,6 +91,8 @@ typedef struct npom_workspace {
   unsigned int *sync;      /* >= 4 unsigned ints, zero before first use    */
   unsigned int *status;    /* >= 1 unsigned int: OR of NPOM_ERR_* bits     */
   int *cg_iters;           /* >= nsteps ints: PCG iterations of each step  */
+  float *mp3d;             /* nadv 2 only (else may be null): >= 12 *     */
+                           /* im*jm*kb floats of MPDATA scratch            */
 } npom_workspace;
 
 #define NPOM_MAX_COOP_BLOCKS 1024
@@ -115,6 +117,9 @@ typedef struct npom_params {
   double velocity_shapiro, wind_tau0, vmix;
   double period;           /* inertial period in days (ramp = time/period) */
   double inverse_scale;    /* spectral preconditioner: 4 (ni+1)(nj+1)      */
+  double sw;               /* MPDATA antidiffusion weight (nadv 2)         */
+  int32_t nitera;          /* MPDATA iterations (nadv 2)                   */
+  int32_t pad0;
 } npom_params;
 
 enum { NPOM_CORE_EXPLICIT = 0, NPOM_CORE_IMPLICIT = 1 };

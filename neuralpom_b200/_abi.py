@@ -74,12 +74,14 @@ class NpomParams(ctypes.Structure):
             "dti", "dte", "dti2", "dte2", "ispi", "isp2i", "alpha", "smoth", "horcon", "grav", "umol", "tprni",
             "small", "kappa", "rhoref", "tbias", "sbias", "vmaxl", "hmax", "rfe", "rfw", "rfn", "rfs", "aam_min",
             "pi", "eta_tol", "eta_rel_tol", "barotropic_shapiro", "tracer_shapiro", "velocity_shapiro",
-            "wind_tau0", "vmix", "period", "inverse_scale")]
+            "wind_tau0", "vmix", "period", "inverse_scale", "sw")] + [
+        ("nitera", ctypes.c_int32), ("pad0", ctypes.c_int32)]
 
 
 class NpomWorkspace(ctypes.Structure):
     _fields_ = [("buf", ctypes.c_void_p * len(WS_NAMES)), ("partials", ctypes.c_void_p),
-                ("sync", ctypes.c_void_p), ("status", ctypes.c_void_p), ("cg_iters", ctypes.c_void_p)]
+                ("sync", ctypes.c_void_p), ("status", ctypes.c_void_p), ("cg_iters", ctypes.c_void_p),
+                ("mp3d", ctypes.c_void_p)]
 
 
 class NpomClock(ctypes.Structure):

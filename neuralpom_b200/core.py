@@ -116,6 +116,10 @@ class B200Core:
             s.cg_iters = base + 8 * 4
             ws["struct"] = s
             self._ws = ws
+        if int(getattr(self, "nadv", 1)) == 2 and "mp3d" not in self._ws:
+            # MPDATA scratch: mass fluxes and fluxes of T and S
+            self._ws["mp3d"] = torch.zeros(12 * im * jm * self.kb, dtype=torch.float32, device=dev)
+            self._ws["struct"].mp3d = self._ws["mp3d"].data_ptr()
         if self.core_name != "explicit":
             sx, sy, ie = state.spectral_setup(self.dx.detach().cpu().numpy(), self.dy.detach().cpu().numpy(),
                                               self.h.detach().cpu().numpy(), float(self.dti), float(self.grav),

@@ -41,7 +41,8 @@ struct Consts {
   float bshap_q, tshap_q, vshap_q;  // gamma / 4 of the three Shapiro filters
   double bshap, tshap, vshap;
   float implicit_coeff, inverse_scale;
-  int isplit, ispadv, nbct, nbcs, ntp, mode, core, wind_forcing, has_vmix;
+  int isplit, ispadv, nbct, nbcs, ntp, mode, core, wind_forcing, has_vmix, nadv, nitera;
+  float sw;
   int eta_max_iter, eta_precond;
   double eta_tol, eta_rel_tol;
 };
@@ -54,6 +55,7 @@ struct Ctx {
   unsigned int *sync;
   unsigned int *status;
   int *cg_iters;
+  float *mp3d;  // MPDATA scratch (nadv 2)
   Consts k;
   int coh;         // 1: loads bypass L1 (persistent cooperative kernels)
   float ramp;      // per step

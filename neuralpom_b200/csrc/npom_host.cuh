@@ -76,6 +76,9 @@ inline Consts make_consts(const npom_params &p) {
   k.core = p.core;
   k.wind_forcing = p.wind_forcing;
   k.has_vmix = p.has_vmix;
+  k.nadv = p.nadv;
+  k.nitera = p.nitera;
+  k.sw = (float)p.sw;
   k.eta_max_iter = p.eta_max_iter;
   k.eta_precond = p.eta_precond;
   k.eta_tol = p.eta_tol;
@@ -92,6 +95,7 @@ inline bool check_args(const npom_params *p, float *const *fields, const npom_wo
   for (int f = 0; f < NPOM_NFIELDS; ++f)
     if (!fields[f]) return false;
   if (!ws->partials || !ws->sync || !ws->status || !ws->cg_iters) return false;
+  if (p->nadv != 1 && (p->nadv != 2 || p->core != NPOM_CORE_EXPLICIT || !ws->mp3d || p->nitera < 1)) return false;
   for (int w = 0; w < NPOM_NWS; ++w)
     if (!ws->buf[w]) return false;
   return true;
@@ -109,6 +113,7 @@ inline Ctx make_ctx(const npom_params *p, float *const *fields, const npom_works
   c.sync = ws->sync;
   c.status = ws->status;
   c.cg_iters = ws->cg_iters;
+  c.mp3d = ws->mp3d;
   c.k = make_consts(*p);
   c.ramp = 1.0f;
   c.do_internal = 1;

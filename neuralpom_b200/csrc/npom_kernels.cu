@@ -28,6 +28,7 @@
 #include "npom_pcg_cluster.cuh"
 #include "npom_lanes.cuh"
 #include "npom_adjoint.cuh"
+#include "npom_mpdata.cuh"
 
 using namespace npom;
 
@@ -864,7 +865,36 @@ void launch_a1(const Ctx &c, cudaStream_t s) {
 
 // B5 the same way: flux-once tiles from kTileCells cells on (kb == 16, not
 // in mode 4); NPOM_B5=tiles or NPOM_B5=points forces either form.
+__global__ void __launch_bounds__(kThreads) k_mpdata(Ctx c, int pass, int itera) {
+  const size_t n = (size_t)c.im * c.jm * c.kb;
+  const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int k = (int)(p % c.kb);
+  const size_t col = p / c.kb;
+  phase_b5_mpdata_point(c, pass, itera, (int)(col / c.jm), (int)(col % c.jm), k);
+}
+
+// B5 with MPDATA tracer advection (nadv 2): the filter, then ADVT2's passes
+// for T and S together, nitera iterations
+void launch_b5_mpdata(const Ctx &c, cudaStream_t s) {
+  const size_t n = (size_t)c.im * c.jm * c.kb;
+  const unsigned g = (unsigned)((n + kThreads - 1) / kThreads);
+  k_mpdata<<<g, kThreads, 0, s>>>(c, MP_FILTER, 0);
+  k_mpdata<<<g, kThreads, 0, s>>>(c, MP_INIT, 0);
+  for (int it = 1; it <= c.k.nitera; ++it) {
+    k_mpdata<<<g, kThreads, 0, s>>>(c, MP_UPWIND, it);
+    k_mpdata<<<g, kThreads, 0, s>>>(c, MP_FORECAST, it);
+    k_mpdata<<<g, kThreads, 0, s>>>(c, MP_ANTIDIFF, it);
+  }
+  k_mpdata<<<g, kThreads, 0, s>>>(c, MP_DIFFUSION, 0);
+  k_mpdata<<<g, kThreads, 0, s>>>(c, MP_FINISH, 0);
+}
+
 void launch_b5(const Ctx &c, cudaStream_t s) {
+  if (c.k.nadv == 2 && c.k.mode != 4) {
+    launch_b5_mpdata(c, s);
+    return;
+  }
   const size_t ncell = (size_t)c.im * c.jm;
   const char *env = getenv("NPOM_B5");
   bool tiles = c.kb == 16 && c.k.mode != 4 && ncell >= kTileCells;

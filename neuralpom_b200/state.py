@@ -65,8 +65,11 @@ def make_params(s, im, jm, kb, core, device=0):
     p.ispadv = int(get("ispadv", 5))
     p.nbct, p.nbcs, p.ntp = int(get("nbct", 1)), int(get("nbcs", 1)), int(get("ntp", 2))
     p.mode, p.nadv = int(get("mode", 3)), int(get("nadv", 1))
-    if p.nadv != 1:
-        raise ValueError("only the centred tracer advection (nadv=1) is implemented")
+    if p.nadv not in (1, 2) or (p.nadv == 2 and core != "explicit"):
+        raise ValueError("tracer advection: nadv=1 (centred) for both cores, nadv=2 (MPDATA) for the explicit core")
+    p.nitera, p.sw = int(get("nitera", 2)), float(get("sw", 0.5))
+    if p.nitera < 1:
+        raise ValueError("nitera must be positive")
     p.eta_max_iter = int(get("eta_solver_max_iter", 200) or 200)
     pre = str(get("eta_solver_preconditioner", "spectral") or "spectral").strip().lower()
     if implicit and pre not in ("spectral", "jacobi"):

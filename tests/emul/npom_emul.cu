@@ -15,6 +15,7 @@
 
 #include "../../neuralpom_b200/csrc/npom_host.cuh"
 #include "../../neuralpom_b200/csrc/npom_adjoint.cuh"
+#include "../../neuralpom_b200/csrc/npom_mpdata.cuh"
 
 using namespace npom;
 
@@ -193,7 +194,24 @@ void run_phase(const Ctx &c, const npom_params *p, int phase) {
     case 7: each_point(c, [&](int i, int j, int k) { phase_b2b_point(c, i, j, k); }); break;
     case 8: each_cell(c, [&](int i, int j) { phase_b3_column(c, i, j); }); break;
     case 9: each_point(c, [&](int i, int j, int k) { phase_b4_point(c, i, j, k); }); break;
-    case 10: each_point(c, [&](int i, int j, int k) { phase_b5_point(c, i, j, k); }); break;
+    case 10:
+      if (c.k.nadv == 2 && c.k.mode != 4) {
+        auto pass = [&](int ps, int it) {
+          each_point(c, [&](int i, int j, int k) { phase_b5_mpdata_point(c, ps, it, i, j, k); });
+        };
+        pass(MP_FILTER, 0);
+        pass(MP_INIT, 0);
+        for (int it = 1; it <= c.k.nitera; ++it) {
+          pass(MP_UPWIND, it);
+          pass(MP_FORECAST, it);
+          pass(MP_ANTIDIFF, it);
+        }
+        pass(MP_DIFFUSION, 0);
+        pass(MP_FINISH, 0);
+      } else {
+        each_point(c, [&](int i, int j, int k) { phase_b5_point(c, i, j, k); });
+      }
+      break;
     case 11: each_cell(c, [&](int i, int j) { phase_b6_column(c, i, j); }); break;
     case 12: each_point(c, [&](int i, int j, int k) { phase_b7_point(c, i, j, k); }); break;
     case 13: each_cell(c, [&](int i, int j) { phase_b8_column(c, i, j); }); break;

@@ -83,6 +83,7 @@ class EmulCore:
         self.sync = np.zeros(4, np.uint32)
         self.status = np.zeros(1, np.uint32)
         self.cg_iters = np.zeros(4096, np.int32)
+        self.mp3d = np.zeros(12 * im * jm * kb, np.float32)
         self.fa = _abi.FieldArray(*[self.F[n].ctypes.data for n in _abi.FIELD_NAMES])
         self.ws = _abi.NpomWorkspace()
         for i, n in enumerate(_abi.WS_NAMES):
@@ -91,6 +92,7 @@ class EmulCore:
         self.ws.sync = self.sync.ctypes.data
         self.ws.status = self.status.ctypes.data
         self.ws.cg_iters = self.cg_iters.ctypes.data
+        self.ws.mp3d = self.mp3d.ctypes.data
         self.time = float(s.get("time", 0.0))
 
     def steps(self, n):

@@ -3,7 +3,7 @@
 Run in a container that holds the reference sources (default
 ``/root/reference/src``, or ``NPOM_REFERENCE_SRC``)::
 
-    python tests/golden/make_golden.py [proft] [steps] [adjoint] [coastal] [step_adjoint] [coupling]
+    python tests/golden/make_golden.py [proft] [steps] [adjoint] [coastal] [step_adjoint] [coupling] [mpdata]
 
 Writes ``tests/golden/*.npz``.  Every file records the reference's own CPU
 float32 outputs on seeded inputs; nothing here is needed at test time except
@@ -319,7 +319,16 @@ def make_coupling_golden(im=12, jm=10, seed=41):
     print("wrote", path, os.path.getsize(path), "limit factor", float(info["ts_limit_factor"]))
 
 
-def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint", "coupling")):
+def make_mpdata_golden(im=12, jm=10, seed=51):
+    """The explicit core with MPDATA tracer advection (nadv = 2, ADVT2 and
+    SMOL_ADIF, explicit/tracers.py:571-888) on a perturbed production
+    state, 1 and 3 steps."""
+    core = perturbed_core("explicit", im, jm, seed)
+    core.nadv = 2
+    make_step_golden("explicit", im, jm, seed, core=core, tag="mpdata")
+
+
+def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint", "coupling", "mpdata")):
     src = rh.default_reference_path()
     if src is None:
         raise SystemExit("reference sources not found; set NPOM_REFERENCE_SRC")
@@ -340,7 +349,9 @@ def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint", "couplin
         make_step_adjoint_goldens()
     if "coupling" in which:
         make_coupling_golden()
+    if "mpdata" in which:
+        make_mpdata_golden()
 
 
 if __name__ == "__main__":
-    main(tuple(sys.argv[1:]) or ("proft", "steps", "adjoint", "coastal", "step_adjoint", "coupling"))
+    main(tuple(sys.argv[1:]) or ("proft", "steps", "adjoint", "coastal", "step_adjoint", "coupling", "mpdata"))

@@ -10,7 +10,8 @@ from oracle import pom_oracle as O
 pytestmark = pytest.mark.gpu
 
 STEP_FILES = [("step_explicit_12x10.npz", "explicit"), ("step_implicit_12x10.npz", "implicit_p0_fixed"),
-              ("step_implicit_20x18.npz", "implicit_p0_fixed"), ("step_coastal_40x34.npz", "explicit")]
+              ("step_implicit_20x18.npz", "implicit_p0_fixed"), ("step_coastal_40x34.npz", "explicit"),
+              ("step_mpdata_12x10.npz", "explicit")]
 
 
 def _core(arrays, scalars, core):
