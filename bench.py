@@ -45,6 +45,11 @@ WORKLOADS = {
     "gyre": {"grid": (64, 64, 16), "core": "explicit", "internal": 480,
              "desc": "explicit core, 64x64x16 double-gyre basin (dx=20 km, dtE=6 s, isplit=30, seeded "
                      "bathymetry noise), forward; one bench step = one simulated day (480 internal steps)"},
+    "batch": {"grid": None, "core": None, "internal": None,
+              "desc": "64 members on mixed grids in one GPU (24 x 90x82x16, 24 x 128x112x16, 16 x 177x161x16; even "
+                      "members the explicit noise basin at dtI=180 s, odd members the semi-implicit seamount at "
+                      "dtI=300 s, seed = member), one simulated day of every member per bench step; each member "
+                      "its own core and CUDA stream with graph-replayed internal steps"},
     "coastal": {"grid": (354, 322, 16), "core": "explicit", "internal": 60, "horizon": 360,
                 "desc": "explicit core, 354x322x16 coastal basin (dx=500 m, open south boundary with Flather "
                         "condition and M2 elevation 1 m updated every bench step), forward; one bench step = 1 "
@@ -100,6 +105,8 @@ def parse():
     ap.add_argument("--fa-reps", type=int, default=3, help="timed forward+adjoint samples (median)")
     ap.add_argument("--fa-only", action="store_true",
                     help="headline forward+adjoint sample only (after --warmup forward days); for profiling")
+    ap.add_argument("--batch-chunk", type=int, default=24,
+                    help="batch workload: internal steps a member enqueues per round-robin turn")
     return ap.parse_args()
 
 
@@ -218,17 +225,26 @@ def aggregate_days_per_s(n_members, steps, internal_steps, dti, t_max_ms):
 # the B200 arm
 # ---------------------------------------------------------------------------
 
+SUB_CLUSTER_CELLS = 16 * 1024  # largest grid of the one-cluster explicit subcycle
+
+
 def launches_of(core, nsteps, time0):
     """Kernels one npom_step_* call enqueues (see npom_kernels.cu run_steps):
     the operator coefficients once (implicit), then per internal step A1 A2
     A3 + PCG + I5 (implicit) or A1 A2 A3 + subcycle (explicit), the nine
     internal-mode kernels B1-B8 unless the step is the first from rest, and
-    B9."""
+    B9.  With NPOM_SUBCYCLE=phases (or =nocoop on grids above four cells
+    per thread of one cluster) the explicit subcycle is 3 x isplit launches
+    instead of one."""
     implicit = core.core_name != "explicit"
+    sub = 1
+    form = os.environ.get("NPOM_SUBCYCLE")
+    if not implicit and (form == "phases" or (form == "nocoop" and core.im * core.jm > 4 * SUB_CLUSTER_CELLS)):
+        sub = 3 * int(core.params().isplit)
     n = 1 if implicit else 0
     for s in range(nsteps):
         iint = 1 + s
-        n += (5 if implicit else 4) + 1
+        n += (5 if implicit else 3 + sub) + 1
         if (iint != 1 or time0 != 0.0) and core.mode != 2:
             n += 9
     return n
@@ -877,10 +893,168 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# batch workload: 64 members on mixed grids (one GPU)
+# ---------------------------------------------------------------------------
+BATCH_GRIDS = ((90, 82, 24), (128, 112, 24), (177, 161, 16))
+
+
+def batch_member(m, im, jm):
+    """Member m of the batch: even members the explicit noise basin
+    (dtE = 6 s, isplit = 30), odd members the semi-implicit seamount with a
+    seeded 0.2 degC temperature perturbation; clock at 2 days (ramp
+    saturated, so every step replays its graph)."""
+    from neuralpom_b200 import cases
+    if m % 2 == 0:
+        A, Sc = cases.noise_basin(im, jm, kb=16, seed=m)
+        name = "explicit"
+    else:
+        A, Sc = cases.seamount(im, jm, kb=16, dti=DTI)
+        g = np.random.default_rng(100 + m)
+        p = (0.2 * g.standard_normal(A["t"].shape) * A["fsm"][:, :, None]).astype(np.float32)
+        A["t"] = A["t"] + p
+        A["tb"] = A["tb"] + p
+        name = "implicit_p0_fixed"
+    Sc = dict(Sc)
+    Sc.update(time=2.0, time0=2.0)
+    return A, Sc, name
+
+
+def step_algorithmic_bytes(im, jm, kb, core_name):
+    """Algorithmic bytes of one internal step (PHASE_IO, 4 B per element of
+    every distinct array each phase reads or writes)."""
+    n3, n2 = im * jm * kb, im * jm
+    phases = ["A1_forcing_advct", "A2_baropg_smag_means", "A3_advave_predictor"]
+    if core_name == "explicit":
+        phases += ["E_external_explicit"]
+    else:
+        phases += ["E_external", "I5_corrector_filter"]
+    phases += ["B1_barotropic_fix", "B2A_vertvl", "B2B_advq", "B3_profq", "B4_edges_bcond6", "B5_qfilter_advt1",
+               "B6_proft", "B7_tsfilter_dens", "B8_advuv_profuv", "B9_velfilter_shift"]
+    total = 0
+    for ph in phases:
+        r3, r2, w3, w2 = PHASE_IO[ph]
+        total += 4 * ((r3 + w3) * n3 + (r2 + w2) * n2)
+    if core_name != "explicit":
+        ni, nj = im - 2, jm - 2
+        total += 4 * (ni * ni + nj * nj + ni * nj)
+    return total
+
+
+def run_batch(args):
+    # members run concurrently: the explicit subcycle runs on one cluster per
+    # member (up to four cells per thread), never as a cooperative grid, which
+    # needs all of its blocks resident while other streams hold SMs
+    os.environ.setdefault("NPOM_SUBCYCLE", "nocoop")
+    # one hardware queue per stream up to 32 (the default 8 makes streams
+    # that share a queue wait on each other's work); set before the context
+    os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+    import torch
+    from neuralpom_b200 import _abi, build, resolve_core_class
+    ws_n, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    build.build()
+    members = []
+    m = 0
+    for im, jm, count in BATCH_GRIDS:
+        for _ in range(count):
+            A, Sc, name = batch_member(m, im, jm)
+            core = resolve_core_class(name).from_state(A, Sc, device=dev)
+            nday = int(round(86400.0 / float(core.dti)))
+            members.append({"core": core, "stream": torch.cuda.Stream(dev), "nday": nday, "name": name,
+                            "grid": (im, jm), "A": A, "Sc": Sc})
+            m += 1
+    main_stream = torch.cuda.current_stream(dev)
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+
+    def launch_all(steps_of):
+        # members enqueue their steps in turns of --batch-chunk steps, so that
+        # the hardware queues hold every member's work from the start
+        start = torch.cuda.Event()
+        start.record(main_stream)
+        todo = []
+        for mb in members:
+            mb["stream"].wait_event(start)
+            todo.append([mb, steps_of(mb), 0, float(mb["core"].time)])
+        while any(t[2] < t[1] for t in todo):
+            for t in todo:
+                mb, n, done, t0 = t
+                k = min(max(1, args.batch_chunk), n - done)
+                if k > 0:
+                    mb["core"].launch_steps(k, t0, 1 + done, mb["stream"])
+                    t[2] += k
+        for mb, n, _, t0 in todo:
+            mb["core"].time = mb["core"].dti * n / 86400.0 + t0
+            e = torch.cuda.Event()
+            e.record(mb["stream"])
+            main_stream.wait_event(e)
+
+    for _ in range(args.warmup):
+        launch_all(lambda mb: 4)
+    torch.cuda.synchronize(dev)
+    total_ms = 0.0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            l2_flush(flush)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(main_stream)
+            launch_all(lambda mb: mb["nday"])
+            b.record(main_stream)
+            torch.cuda.synchronize(dev)
+            total_ms += a.elapsed_time(b)
+    for mb in members:
+        bits, _ = mb["core"].read_status(0)
+        if bits & (_abi.DEV_TIMEOUT | _abi.DEV_VMAX | _abi.DEV_NONFINITE):
+            raise RuntimeError(f"device status 0x{bits:x} in the batch run")
+    nmem = len(members)
+    value = nmem * args.steps / (total_ms / 1000.0)
+    nbytes = sum(mb["nday"] * step_algorithmic_bytes(*mb["grid"], 16, mb["name"]) for mb in members) * args.steps
+    peak, src = measured_peaks()
+    achieved = nbytes / (total_ms / 1000.0) / 1e9
+    launches = sum(launches_of(mb["core"], mb["nday"], 2.0) for mb in members) * args.steps
+    ref = None
+    if not args.no_ref_gpu:
+        # the reference core looping the members: its time per internal step
+        # on each (grid, core) pair on this GPU, times every member's steps
+        per_step = {}
+        for mb in members:
+            key = (mb["grid"], mb["name"])
+            if key in per_step:
+                continue
+            smp = reference_gpu_sample(mb["A"], mb["Sc"], dev, internal_steps=4, warm=1, reps=1,
+                                       core_name=mb["name"])
+            dti = float(mb["core"].dti)
+            per_step[key] = (4 * dti / 86400.0) / smp["value"] / 4
+        loop_sec = sum(mb["nday"] * per_step[(mb["grid"], mb["name"])] for mb in members)
+        ref = {"value": nmem / loop_sec, "unit": UNIT, "device": str(dev),
+               "sample": "the reference PyTorch core (eager, its default SparsePhysics options) timed over 4 "
+                         "internal steps on each of the 6 (grid, core) pairs on this GPU, looped over every "
+                         "member's day: sum of member steps x time per step",
+               "seconds_per_step": {f"{g[0]}x{g[1]} {n}": v for (g, n), v in per_step.items()}}
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (FP64 PCG dot products)", "data": "synthetic",
+        "config": {"workload": WORKLOADS["batch"]["desc"], "members": nmem,
+                   "explicit_subcycle": os.environ.get("NPOM_SUBCYCLE"), "steps_per_turn": args.batch_chunk,
+                   "hw_queues": os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS"),
+                   "member_days_per_step": nmem, "l2": "flushed (256 MiB write) before every timed step"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": src, "traffic": None, "algorithmic_bytes": nbytes,
+                     "note": "whole batch: algorithmic bytes of every member's steps over the device time"},
+        "reference_gpu_loop": ref, "cpu_baseline": None, "e2e": None, "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch":
+        run_batch(args)
     else:
         run_b200(args)
 

@@ -802,17 +802,44 @@ cudaError_t run_pcg(Ctx c, const PcgPlan &plan, int with_rhs, int with_post, cud
 }
 
 // Launch shape of the explicit subcycle, decided outside any capture:
-// > 0 grid-barrier blocks, < 0 a cluster shape (encode_cluster).
-// NPOM_SUBCYCLE=grid forces the grid-barrier form on small grids too.
+// > 0 grid-barrier blocks, < 0 a cluster shape (encode_cluster), 0 one
+// launch per substep phase.  NPOM_SUBCYCLE=grid forces the grid-barrier
+// form on small grids too; NPOM_SUBCYCLE=phases the per-phase launches,
+// which need no co-residency (for many members advanced concurrently on
+// one GPU, where a cooperative grid may not find all its blocks resident);
+// NPOM_SUBCYCLE=nocoop the cluster form up to kSubClusterCellsShared cells
+// (up to four cells per thread: one 16-SM cluster per member leaves the
+// rest of the GPU to the other members), else the per-phase launches (a
+// cluster is co-scheduled by the hardware, a cooperative grid is not when
+// other streams hold SMs).
+constexpr size_t kSubClusterCellsShared = 4 * kSubClusterCells;
+
 cudaError_t plan_subcycle(const Ctx &c, int *out) {
   const size_t ncell = (size_t)c.im * c.jm;
   const char *env = getenv("NPOM_SUBCYCLE");
+  const bool nocoop = env && std::strcmp(env, "nocoop") == 0;
+  if ((env && std::strcmp(env, "phases") == 0) || (nocoop && ncell > kSubClusterCellsShared)) {
+    *out = 0;
+    return cudaSuccess;
+  }
+  if (nocoop) return plan_cluster(kSubcycleCluster, ncell, out);
   const bool grid = env && std::strcmp(env, "grid") == 0;
   if (!grid && ncell <= kSubClusterCells) return plan_cluster(kSubcycleCluster, ncell, out);
   return coop_blocks((const void *)k_subcycle, ncell, out);
 }
 
+__global__ void __launch_bounds__(kThreads) k_ext_phase(Ctx c, int phase, int iext, int adv);
+
 cudaError_t run_subcycle(Ctx c, int blocks, cudaStream_t s) {
+  if (blocks == 0) {
+    const int n = c.im * c.jm;
+    const unsigned g = (unsigned)((n + kThreads - 1) / kThreads);
+    for (int iext = 1; iext <= c.k.isplit; ++iext) {
+      const int adv = (iext % c.k.ispadv) == 0;
+      for (int ph = 1; ph <= 3; ++ph) k_ext_phase<<<g, kThreads, 0, s>>>(c, ph, iext, adv);
+    }
+    return cudaGetLastError();
+  }
   c.coh = 1;
   void *args[] = {&c};
   if (blocks < 0) {
@@ -821,6 +848,18 @@ cudaError_t run_subcycle(Ctx c, int blocks, cudaStream_t s) {
     return launch_cluster(kSubcycleCluster[t], cluster_ctas(blocks), threads, args, s);
   }
   return launch_coop((const void *)k_subcycle, blocks, args, c.sync, s);
+}
+
+// one phase (1, 2, 3) of one external substep over all cells
+__global__ void __launch_bounds__(kThreads) k_ext_phase(Ctx c, int phase, int iext, int adv) {
+  const int n = c.im * c.jm;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int i = q / c.jm, j = q % c.jm;
+  if (phase == 1) ext_phase1_cell(c, i, j, adv != 0);
+  else if (phase == 2) {
+    if (ext_phase2_cell(c, i, j, iext)) atomicOr(c.status, NPOM_DEV_VMAX);
+  } else ext_phase3_cell(c, i, j, iext);
 }
 
 void launch_b5(const Ctx &c, cudaStream_t s);

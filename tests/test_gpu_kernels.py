@@ -142,8 +142,10 @@ def test_flux_tiles_equal_point_kernel(monkeypatch, case, phase, env, fields):
     from neuralpom_b200 import _abi, cases, resolve_core_class
     if case == "gyre":
         A, Sc = cases.double_gyre(37, 45, "explicit")
-    else:
+    elif case == "coastal":
         A, Sc = cases.coastal_tide(60, 52)
+    else:
+        A, Sc = cases.coastal_tide(180, 160)
     Sc = dict(Sc)
     Sc.update(time=0.25, time0=0.25)
     lib = _lib()
@@ -159,15 +161,18 @@ def test_flux_tiles_equal_point_kernel(monkeypatch, case, phase, env, fields):
                                       ctypes.c_void_p(stream.cuda_stream)), "phase")
         torch.cuda.synchronize()
         outs.append({n: getattr(c, n).cpu().numpy() for n in fields + ("u", "el")})
-    for n in outs[0]:
-        assert np.array_equal(outs[0][n], outs[1][n]), n
+    for other in outs[1:]:
+        for n in outs[0]:
+            assert np.array_equal(outs[0][n], other[n]), n
 
 
-@pytest.mark.parametrize("case", ["gyre", "coastal"])
+@pytest.mark.parametrize("case", ["gyre", "coastal", "coastal_180x160"])
 def test_cluster_subcycle_equals_grid_subcycle(monkeypatch, case):
     """On small grids the explicit external subcycle runs on one thread-block
     cluster with the hardware cluster barrier; it writes bitwise what the
-    grid-barrier form writes, for the phase alone and over whole steps."""
+    grid-barrier form and the one-launch-per-phase form (no barrier at all)
+    write, for the phase alone and over whole steps.  The 180x160 grid runs
+    the cluster form (NPOM_SUBCYCLE=nocoop) with two cells per thread."""
     from neuralpom_b200 import _abi, cases, resolve_core_class
     if case == "gyre":
         A, Sc = cases.double_gyre(37, 45, "explicit")
@@ -179,7 +184,7 @@ def test_cluster_subcycle_equals_grid_subcycle(monkeypatch, case):
     stream = torch.cuda.current_stream()
     names = ("el", "elb", "elf", "ua", "uab", "uaf", "va", "vab", "vaf", "egf", "utf", "vtf", "d", "etf")
     outs = []
-    for form in ("grid", "cluster"):
+    for form in ("grid", "cluster", "phases", "nocoop"):
         monkeypatch.setenv("NPOM_SUBCYCLE", form)
         c = resolve_core_class("explicit").from_state(A, Sc, device="cuda")
         c.launch_steps(2, 0.25, 1, stream)
@@ -191,5 +196,6 @@ def test_cluster_subcycle_equals_grid_subcycle(monkeypatch, case):
         bits, _ = c.read_status(1)
         assert bits == 0
         outs.append({n: getattr(c, n).cpu().numpy() for n in names + ("u", "v", "t")})
-    for n in outs[0]:
-        assert np.array_equal(outs[0][n], outs[1][n]), n
+    for other in outs[1:]:
+        for n in outs[0]:
+            assert np.array_equal(outs[0][n], other[n]), n
