@@ -48,8 +48,9 @@ WORKLOADS = {
     "batch": {"grid": None, "core": None, "internal": None,
               "desc": "64 members on mixed grids in one GPU (24 x 90x82x16, 24 x 128x112x16, 16 x 177x161x16; even "
                       "members the explicit noise basin at dtI=180 s, odd members the semi-implicit seamount at "
-                      "dtI=300 s, seed = member), one simulated day of every member per bench step; each member "
-                      "its own core and CUDA stream with graph-replayed internal steps"},
+                      "dtI=300 s, seed = member), one simulated day of every member per bench step; the members "
+                      "of each core advance as one batch, one launch per phase over all of them, the step "
+                      "replayed as a CUDA graph"},
     "coastal": {"grid": (354, 322, 16), "core": "explicit", "internal": 60, "horizon": 360,
                 "desc": "explicit core, 354x322x16 coastal basin (dx=500 m, open south boundary with Flather "
                         "condition and M2 elevation 1 m updated every bench step), forward; one bench step = 1 "
@@ -106,7 +107,11 @@ def parse():
     ap.add_argument("--fa-only", action="store_true",
                     help="headline forward+adjoint sample only (after --warmup forward days); for profiling")
     ap.add_argument("--batch-chunk", type=int, default=24,
-                    help="batch workload: internal steps a member enqueues per round-robin turn")
+                    help="batch workload: turns per simulated day in which the groups (or members) enqueue "
+                         "their steps")
+    ap.add_argument("--batch-mode", default="launch", choices=("launch", "streams"),
+                    help="batch workload: 'launch' = one launch per phase over all members of a core "
+                         "(npom_step_batch); 'streams' = every member its own core call on its own stream")
     return ap.parse_args()
 
 
@@ -942,15 +947,17 @@ def step_algorithmic_bytes(im, jm, kb, core_name):
 
 
 def run_batch(args):
-    # members run concurrently: the explicit subcycle runs on one cluster per
-    # member (up to four cells per thread), never as a cooperative grid, which
-    # needs all of its blocks resident while other streams hold SMs
-    os.environ.setdefault("NPOM_SUBCYCLE", "nocoop")
-    # one hardware queue per stream up to 32 (the default 8 makes streams
-    # that share a queue wait on each other's work); set before the context
-    os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+    if args.batch_mode == "streams":
+        # members run concurrently: the explicit subcycle runs on one cluster
+        # per member (up to four cells per thread), never as a cooperative
+        # grid, which needs all of its blocks resident while other streams
+        # hold SMs
+        os.environ.setdefault("NPOM_SUBCYCLE", "nocoop")
+        # one hardware queue per stream up to 32 (the default 8 makes streams
+        # that share a queue wait on each other's work); before the context
+        os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     import torch
-    from neuralpom_b200 import _abi, build, resolve_core_class
+    from neuralpom_b200 import _abi, batch, build, resolve_core_class
     ws_n, rank, local = dist_env()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -969,7 +976,7 @@ def run_batch(args):
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=dev)
 
     def launch_all(steps_of):
-        # members enqueue their steps in turns of --batch-chunk steps, so that
+        # members enqueue their steps in --batch-chunk turns a day, so that
         # the hardware queues hold every member's work from the start
         start = torch.cuda.Event()
         start.record(main_stream)
@@ -980,7 +987,7 @@ def run_batch(args):
         while any(t[2] < t[1] for t in todo):
             for t in todo:
                 mb, n, done, t0 = t
-                k = min(max(1, args.batch_chunk), n - done)
+                k = min(max(1, -(-n // max(1, args.batch_chunk))), n - done)
                 if k > 0:
                     mb["core"].launch_steps(k, t0, 1 + done, mb["stream"])
                     t[2] += k
@@ -990,16 +997,47 @@ def run_batch(args):
             e.record(mb["stream"])
             main_stream.wait_event(e)
 
+    groups = {}
+    for mb in members:
+        groups.setdefault(mb["name"], []).append(mb)
+
+    def launch_batched(steps_of):
+        # each core's members advance as one batch (one launch per phase);
+        # the two batches take turns on one stream, --batch-chunk turns a day
+        todo = []
+        for mbs in groups.values():
+            n = steps_of(mbs[0])
+            todo.append([[mb["core"] for mb in mbs], n, 0, float(mbs[0]["core"].time),
+                         max(1, -(-n // max(1, args.batch_chunk)))])
+        launches = 0
+        while any(t[2] < t[1] for t in todo):
+            for t in todo:
+                cores, n, done, t0, per_turn = t
+                k = min(per_turn, n - done)
+                if k > 0:
+                    launches += batch.launch_batch(cores, k, t0, 1 + done, main_stream)
+                    t[2] += k
+        for cores, n, _, t0, _ in todo:
+            for c in cores:
+                c.time = c.dti * n / 86400.0 + t0
+        return launches
+
+    def advance(steps_of):
+        if args.batch_mode == "launch":
+            return launch_batched(steps_of)
+        launch_all(steps_of)
+        return sum(launches_of(mb["core"], steps_of(mb), 2.0) for mb in members)
+
     for _ in range(args.warmup):
-        launch_all(lambda mb: 4)
+        advance(lambda mb: 4)
     torch.cuda.synchronize(dev)
-    total_ms = 0.0
+    total_ms, launches = 0.0, 0
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             l2_flush(flush)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(main_stream)
-            launch_all(lambda mb: mb["nday"])
+            launches += advance(lambda mb: mb["nday"])
             b.record(main_stream)
             torch.cuda.synchronize(dev)
             total_ms += a.elapsed_time(b)
@@ -1012,7 +1050,6 @@ def run_batch(args):
     nbytes = sum(mb["nday"] * step_algorithmic_bytes(*mb["grid"], 16, mb["name"]) for mb in members) * args.steps
     peak, src = measured_peaks()
     achieved = nbytes / (total_ms / 1000.0) / 1e9
-    launches = sum(launches_of(mb["core"], mb["nday"], 2.0) for mb in members) * args.steps
     ref = None
     if not args.no_ref_gpu:
         # the reference core looping the members: its time per internal step
@@ -1036,8 +1073,10 @@ def run_batch(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 (FP64 PCG dot products)", "data": "synthetic",
-        "config": {"workload": WORKLOADS["batch"]["desc"], "members": nmem,
-                   "explicit_subcycle": os.environ.get("NPOM_SUBCYCLE"), "steps_per_turn": args.batch_chunk,
+        "config": {"workload": WORKLOADS["batch"]["desc"], "members": nmem, "mode": args.batch_mode,
+                   "explicit_subcycle": (os.environ.get("NPOM_BATCH_SUBCYCLE", "phases")
+                                         if args.batch_mode == "launch" else os.environ.get("NPOM_SUBCYCLE")),
+                   "turns_per_day": args.batch_chunk,
                    "hw_queues": os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS"),
                    "member_days_per_step": nmem, "l2": "flushed (256 MiB write) before every timed step"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

@@ -96,6 +96,7 @@ typedef struct npom_workspace {
 } npom_workspace;
 
 #define NPOM_MAX_COOP_BLOCKS 1024
+#define NPOM_MAX_BATCH 64  /* members of one npom_step_batch call         */
 
 /* ------------------------------------------------------------------ */
 /* Scalar settings (the Python attributes of the reference BaseCore).  */
@@ -165,6 +166,28 @@ npom_status npom_step_explicit(const npom_params *p, float *const *fields,
 npom_status npom_step_implicit(const npom_params *p, float *const *fields,
                                const npom_workspace *ws, const npom_clock *clk,
                                void *stream);
+
+/* Advance nsteps internal steps of nmembers members of ONE core (each with
+ * its own grid size, state and workspace) over the same clock: every phase
+ * of the step is one launch over all members, and the step is replayed as
+ * one CUDA graph.  Members must share core, kb, isplit, ispadv, mode, nadv,
+ * nitera and device.  Each member computes what npom_step_explicit /
+ * npom_step_implicit computes for it alone (bitwise, except the semi-
+ * implicit members whose PCG runs in the cooperative form, whose FP64 dot
+ * products are summed over a different block count: equal to rounding).
+ * Replaces the reference's per-member loop over run_time_loop
+ * (cores/explicit/time_loop.py:20, cores/implicit_p0_fixed/time_loop.py:38)
+ * for an ensemble; the reference's only batched GPU code is its batched
+ * 5-point elliptic operator (cores/implicit_p0_fixed/triton_kernels.py:104),
+ * one operator, not a step. */
+npom_status npom_step_batch(int32_t nmembers, const npom_params *const *params,
+                            float *const *const *fields,
+                            const npom_workspace *const *ws,
+                            const npom_clock *clk, void *stream);
+
+/* Kernels the last npom_step_batch call of this process launched (graph
+ * replays count their kernel nodes); for launch accounting. */
+long long npom_batch_launches(void);
 
 /* Run one named phase of a step on the current state (operator tests). */
 npom_status npom_run_phase(const npom_params *p, float *const *fields,

@@ -145,6 +145,11 @@ def load_library():
         fn = getattr(lib, name)
         fn.restype = i32
         fn.argtypes = [P(NpomParams), P(FieldArray), P(NpomWorkspace), P(NpomClock), vp]
+    # members as arrays of pointers: params, field-pointer arrays, workspaces
+    lib.npom_step_batch.restype = i32
+    lib.npom_step_batch.argtypes = [i32, vp, vp, vp, P(NpomClock), vp]
+    lib.npom_batch_launches.restype = ctypes.c_longlong
+    lib.npom_batch_launches.argtypes = []
     lib.npom_run_phase.restype = i32
     lib.npom_run_phase.argtypes = [P(NpomParams), P(FieldArray), P(NpomWorkspace), i32, dbl, vp]
     lib.npom_pcg_solve.restype = i32

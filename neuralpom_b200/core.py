@@ -218,6 +218,11 @@ class B200Core:
             with torch.no_grad():
                 self.launch_steps(nsteps, float(self.time0))
             bits, its = self.read_status(nsteps)
+        self._finish_advance(nsteps, bits, its)
+
+    def _finish_advance(self, nsteps, bits, its):
+        """Clock, ramp and PCG history after ``nsteps`` steps from time0;
+        raises for the device status bits."""
         self.iint = nsteps
         self.time = self.dti * nsteps * 1.0 / 86400.0 + self.time0
         if self.lramp:

@@ -58,6 +58,10 @@ struct Ctx {
   float *mp3d;  // MPDATA scratch (nadv 2)
   Consts k;
   int coh;         // 1: loads bypass L1 (persistent cooperative kernels)
+  // the blocks of a cooperative launch that work on this context: blocks
+  // [grid_base, grid_base + grid_blocks) (grid_blocks 0: the whole grid);
+  // several members share one launch, each with its own grid barrier
+  int grid_base, grid_blocks;
   float ramp;      // per step
   int do_internal; // per step: 0 on the first step from time0 == 0
 };

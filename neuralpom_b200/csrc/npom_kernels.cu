@@ -43,10 +43,12 @@ enum PointPhase { PP_A1 = 0, PP_B2B = 1, PP_B4 = 2, PP_B5 = 3, PP_B7 = 4 };
 enum ColPhase { CP_A2 = 0, CP_B1 = 1, CP_B2A = 2, CP_B3 = 3, CP_B6 = 4, CP_B8 = 5, CP_B9 = 6 };
 enum CellPhase { XP_A3 = 0, XP_I5 = 1, XP_COEF = 2 };
 
+// The bodies below map one thread index of a phase onto its grid point,
+// column or cell; the one-member kernels and the batched kernels (many
+// members in one launch) call the same bodies.
 template <int PH>
-__global__ void __launch_bounds__(kThreads) k_points(Ctx c) {
+__device__ __forceinline__ void points_body(const Ctx &c, size_t p) {
   const size_t n = (size_t)c.im * c.jm * c.kb;
-  size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   int k = (int)(p % c.kb);
   size_t col = p / c.kb;
@@ -71,9 +73,13 @@ __global__ void __launch_bounds__(kThreads) k_points(Ctx c) {
 }
 
 template <int PH>
-__global__ void __launch_bounds__(128) k_cols(Ctx c) {
+__global__ void __launch_bounds__(kThreads) k_points(Ctx c) {
+  points_body<PH>(c, (size_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+template <int PH>
+__device__ __forceinline__ void cols_body(const Ctx &c, int col) {
   const int n = c.im * c.jm;
-  int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= n) return;
   int j = col % c.jm, i = col / c.jm;
   if (PH == CP_A2) phase_a2_column(c, i, j);
@@ -85,13 +91,17 @@ __global__ void __launch_bounds__(128) k_cols(Ctx c) {
   else if (PH == CP_B9) phase_b9_column(c, i, j);
 }
 
+template <int PH>
+__global__ void __launch_bounds__(128) k_cols(Ctx c) {
+  cols_body<PH>(c, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 // One 16-lane segment per water column (kb == 16).  Threads past the last
 // column work on a copy of it and store nothing, so that every shuffle sees
 // all 32 lanes of its warp.
 template <int PH>
-__global__ void __launch_bounds__(kThreads) k_lanes(Ctx c) {
+__device__ __forceinline__ void lanes_body(const Ctx &c, int p) {
   const int ncol = c.im * c.jm;
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
   int col = p >> 4;
   const int k = p & (KL - 1);
   const bool st = col < ncol;
@@ -107,9 +117,13 @@ __global__ void __launch_bounds__(kThreads) k_lanes(Ctx c) {
 }
 
 template <int PH>
-__global__ void __launch_bounds__(kThreads) k_cells(Ctx c) {
+__global__ void __launch_bounds__(kThreads) k_lanes(Ctx c) {
+  lanes_body<PH>(c, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+template <int PH>
+__device__ __forceinline__ void cells_body(const Ctx &c, int cell) {
   const int n = c.im * c.jm;
-  int cell = blockIdx.x * blockDim.x + threadIdx.x;
   if (cell >= n) return;
   int j = cell % c.jm, i = cell / c.jm;
   if (PH == XP_A3) {
@@ -119,6 +133,11 @@ __global__ void __launch_bounds__(kThreads) k_cells(Ctx c) {
   } else if (PH == XP_COEF) {
     elliptic_coeff_cell(c, i, j);
   }
+}
+
+template <int PH>
+__global__ void __launch_bounds__(kThreads) k_cells(Ctx c) {
+  cells_body<PH>(c, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // A1 on large grids: every face flux of ADVCT computed once.  A block holds
@@ -254,9 +273,16 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
 
 constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s
 
+// block count and block index within the blocks of this context
+__device__ __forceinline__ unsigned vgrid(const Ctx &c) {
+  return c.grid_blocks ? (unsigned)c.grid_blocks : gridDim.x;
+}
+__device__ __forceinline__ unsigned vblock(const Ctx &c) { return blockIdx.x - (unsigned)c.grid_base; }
+
 // sync[0] counts arrivals and only grows during a launch (the host clears it
 // before every cooperative launch): barrier b of the launch is complete when
-// the count reaches (b + 1) * gridDim.x, so each block waits for the next
+// the count reaches (b + 1) * G (G the blocks of the context), so each
+// block waits for the next
 // multiple of the grid size above its own arrival.  One atomic per block
 // and no reset inside the kernel keep each barrier at two serial L2 round
 // trips.  Returns false after a timeout (or once any block has timed out);
@@ -268,7 +294,8 @@ __device__ bool grid_barrier(const Ctx &c) {
     ok = 1;
     __threadfence();
     const unsigned int arrived = atomicAdd(c.sync, 1u);
-    const unsigned int target = (arrived / gridDim.x + 1u) * gridDim.x;
+    const unsigned int G = vgrid(c);
+    const unsigned int target = (arrived / G + 1u) * G;
     volatile unsigned int *count = c.sync;
     unsigned long long t0 = globaltimer_ns();
     unsigned int spins = 0;
@@ -313,10 +340,10 @@ __device__ void block_sum3(const Ctx &c, double a0, double a1, double a2, int s0
       t1 += red[1][q];
       t2 += red[2][q];
     }
-    const int G = gridDim.x;
-    if (s0 >= 0) c.partials[s0 * G + blockIdx.x] = t0;
-    if (s1 >= 0) c.partials[s1 * G + blockIdx.x] = t1;
-    if (s2 >= 0) c.partials[s2 * G + blockIdx.x] = t2;
+    const int G = vgrid(c), b = vblock(c);
+    if (s0 >= 0) c.partials[s0 * G + b] = t0;
+    if (s1 >= 0) c.partials[s1 * G + b] = t1;
+    if (s2 >= 0) c.partials[s2 * G + b] = t2;
   }
   __syncthreads();
 }
@@ -326,7 +353,7 @@ __device__ double grid_total(const Ctx &c, int slot) {
   __shared__ double tot;
   if (threadIdx.x == 0) {
     double t = 0.0;
-    const int G = gridDim.x;
+    const int G = vgrid(c);
     for (int b = 0; b < G; ++b) t += __ldcg(c.partials + slot * G + b);
     tot = t;
   }
@@ -341,8 +368,8 @@ __device__ double grid_total(const Ctx &c, int slot) {
 __device__ bool precondition(const Ctx &c, double &rz) {
   const int ni = c.im - 2, nj = c.jm - 2;
   const size_t nint = (size_t)ni * nj;
-  const size_t stride = (size_t)gridDim.x * blockDim.x;
-  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t stride = (size_t)vgrid(c) * blockDim.x;
+  const size_t tid = (size_t)vblock(c) * blockDim.x + threadIdx.x;
   float *zv = c.W[NPOM_W_zv];
   const float *r = c.W[NPOM_W_r];
   rz = 0.0;
@@ -387,11 +414,11 @@ __device__ bool precondition(const Ctx &c, double &rz) {
 // the Shapiro filter and closed-basin bcond 1 (core.py:893-916) and
 // d = h + elf.  Iterations -> c.cg_iters[c.sync[2]++] (one slot per solve
 // of the call).
-__global__ void __launch_bounds__(kThreads) k_pcg(Ctx c, int with_rhs, int with_post) {
+__device__ __forceinline__ void pcg_coop_body(const Ctx &c, int with_rhs, int with_post) {
   const int im = c.im, jm = c.jm, ni = im - 2, nj = jm - 2;
   const size_t ncell = (size_t)im * jm, nint = (size_t)ni * nj;
-  const size_t stride = (size_t)gridDim.x * blockDim.x;
-  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t stride = (size_t)vgrid(c) * blockDim.x;
+  const size_t tid = (size_t)vblock(c) * blockDim.x + threadIdx.x;
   float *x = c.W[NPOM_W_x], *r = c.W[NPOM_W_r], *p = c.W[NPOM_W_p], *zv = c.W[NPOM_W_zv];
   float *ap = c.W[NPOM_W_ap], *rhs = c.W[NPOM_W_rhs];
   const float *elf = c.F[NPOM_F_elf];
@@ -511,12 +538,16 @@ __global__ void __launch_bounds__(kThreads) k_pcg(Ctx c, int with_rhs, int with_
   }
 }
 
+__global__ void __launch_bounds__(kThreads) k_pcg(Ctx c, int with_rhs, int with_post) {
+  pcg_coop_body(c, with_rhs, with_post);
+}
+
 // Fused external mode of the explicit core: isplit substeps, three phases
 // each (explicit/time_loop.py:292-431).
-__global__ void __launch_bounds__(kThreads) k_subcycle(Ctx c) {
+__device__ __forceinline__ void subcycle_coop_body(const Ctx &c) {
   const size_t ncell = (size_t)c.im * c.jm;
-  const size_t stride = (size_t)gridDim.x * blockDim.x;
-  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t stride = (size_t)vgrid(c) * blockDim.x;
+  const size_t tid = (size_t)vblock(c) * blockDim.x + threadIdx.x;
   for (int iext = 1; iext <= c.k.isplit; ++iext) {
     bool adv = (iext % c.k.ispadv) == 0;
     for (size_t q = tid; q < ncell; q += stride) ext_phase1_cell(c, (int)(q / c.jm), (int)(q % c.jm), adv);
@@ -529,6 +560,8 @@ __global__ void __launch_bounds__(kThreads) k_subcycle(Ctx c) {
     if (!grid_barrier(c)) return;
   }
 }
+
+__global__ void __launch_bounds__(kThreads) k_subcycle(Ctx c) { subcycle_coop_body(c); }
 
 // The same subcycle for grids of up to kSubClusterCells cells, on one
 // thread-block cluster of at most 16 CTAs of 256, 512 or 1024 threads (the
@@ -828,7 +861,19 @@ cudaError_t plan_subcycle(const Ctx &c, int *out) {
   return coop_blocks((const void *)k_subcycle, ncell, out);
 }
 
-__global__ void __launch_bounds__(kThreads) k_ext_phase(Ctx c, int phase, int iext, int adv);
+// one phase (1, 2, 3) of one external substep at cell q
+__device__ __forceinline__ void ext_phase_body(const Ctx &c, int phase, int iext, int adv, int q) {
+  if (q >= c.im * c.jm) return;
+  const int i = q / c.jm, j = q % c.jm;
+  if (phase == 1) ext_phase1_cell(c, i, j, adv != 0);
+  else if (phase == 2) {
+    if (ext_phase2_cell(c, i, j, iext)) atomicOr(c.status, NPOM_DEV_VMAX);
+  } else ext_phase3_cell(c, i, j, iext);
+}
+
+__global__ void __launch_bounds__(kThreads) k_ext_phase(Ctx c, int phase, int iext, int adv) {
+  ext_phase_body(c, phase, iext, adv, blockIdx.x * blockDim.x + threadIdx.x);
+}
 
 cudaError_t run_subcycle(Ctx c, int blocks, cudaStream_t s) {
   if (blocks == 0) {
@@ -848,18 +893,6 @@ cudaError_t run_subcycle(Ctx c, int blocks, cudaStream_t s) {
     return launch_cluster(kSubcycleCluster[t], cluster_ctas(blocks), threads, args, s);
   }
   return launch_coop((const void *)k_subcycle, blocks, args, c.sync, s);
-}
-
-// one phase (1, 2, 3) of one external substep over all cells
-__global__ void __launch_bounds__(kThreads) k_ext_phase(Ctx c, int phase, int iext, int adv) {
-  const int n = c.im * c.jm;
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= n) return;
-  const int i = q / c.jm, j = q % c.jm;
-  if (phase == 1) ext_phase1_cell(c, i, j, adv != 0);
-  else if (phase == 2) {
-    if (ext_phase2_cell(c, i, j, iext)) atomicOr(c.status, NPOM_DEV_VMAX);
-  } else ext_phase3_cell(c, i, j, iext);
 }
 
 void launch_b5(const Ctx &c, cudaStream_t s);
@@ -904,13 +937,16 @@ void launch_a1(const Ctx &c, cudaStream_t s) {
 
 // B5 the same way: flux-once tiles from kTileCells cells on (kb == 16, not
 // in mode 4); NPOM_B5=tiles or NPOM_B5=points forces either form.
-__global__ void __launch_bounds__(kThreads) k_mpdata(Ctx c, int pass, int itera) {
+__device__ __forceinline__ void mpdata_body(const Ctx &c, int pass, int itera, size_t p) {
   const size_t n = (size_t)c.im * c.jm * c.kb;
-  const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   const int k = (int)(p % c.kb);
   const size_t col = p / c.kb;
   phase_b5_mpdata_point(c, pass, itera, (int)(col / c.jm), (int)(col % c.jm), k);
+}
+
+__global__ void __launch_bounds__(kThreads) k_mpdata(Ctx c, int pass, int itera) {
+  mpdata_body(c, pass, itera, (size_t)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // B5 with MPDATA tracer advection (nadv 2): the filter, then ADVT2's passes
@@ -976,6 +1012,11 @@ cudaError_t enqueue_step(const Ctx &c, int core, const PcgPlan &plan, int sub_bl
 // settings, ramp, do_internal) and device.  Steps with ramp < 1 (the first
 // inertial period from rest) launch directly; every other step replays a
 // cached graph, which removes the host launch cost of the ~15 kernels.
+// The cache holds kGraphCache graphs (every member of a 64-member ensemble
+// on one device keeps its graph, with room for both values of do_internal
+// and both cores); past that the oldest is destroyed.
+constexpr size_t kGraphCache = 256;
+
 struct GraphEntry {
   int device;
   int core;
@@ -1033,7 +1074,7 @@ cudaError_t launch_step_graph(const Ctx &c, int core, const PcgPlan &plan, int s
     g_capture_failed[dev][core] = true;
     return cudaSuccess;
   }
-  if (g_graphs.size() >= 16) {
+  if (g_graphs.size() >= kGraphCache) {
     cudaGraphExecDestroy(g_graphs.front().exec);
     g_graphs.erase(g_graphs.begin());
   }
@@ -1073,6 +1114,8 @@ npom_status run_steps(const npom_params *p, float *const *fields, const npom_wor
   }
   return cudaGetLastError() == cudaSuccess ? NPOM_OK : NPOM_ERR_CUDA;
 }
+
+#include "npom_batch.cuh"
 
 const char *kFieldNames[] = {
 #define NPOM_X_NAME(n) #n,
@@ -1199,6 +1242,16 @@ const char *npom_phase_name(int index) { return (index >= 0 && index < kNumPhase
 npom_status npom_step_explicit(const npom_params *p, float *const *fields, const npom_workspace *ws,
                                const npom_clock *clk, void *stream) {
   return run_steps(p, fields, ws, clk, stream, NPOM_CORE_EXPLICIT);
+}
+
+npom_status npom_step_batch(int32_t nmembers, const npom_params *const *params, float *const *const *fields,
+                            const npom_workspace *const *ws, const npom_clock *clk, void *stream) {
+  return run_batch_steps(nmembers, params, fields, ws, clk, stream);
+}
+
+long long npom_batch_launches(void) {
+  std::lock_guard<std::mutex> lock(g_batch_mutex);
+  return g_batch_launches;
 }
 
 npom_status npom_step_implicit(const npom_params *p, float *const *fields, const npom_workspace *ws,

@@ -337,9 +337,10 @@ __device__ __forceinline__ double cl_precondition(cgx::cluster_group &cl, const 
   return rz;
 }
 
-__global__ void __launch_bounds__(kClusterThreads, 1)
-    k_pcg_cluster(Ctx c, ClusterLayout L, int with_rhs, int with_post) {
-  extern __shared__ __align__(16) float sm[];
+// The solve of one member on the cluster of this block; sm is the dynamic
+// shared memory of the layout L.
+__device__ __forceinline__ void pcg_cluster_body(const Ctx &c, const ClusterLayout &L, float *sm, int with_rhs,
+                                                 int with_post) {
   double *red = reinterpret_cast<double *>(sm + L.floats);
   cgx::cluster_group cl = cgx::this_cluster();
   const int rank = (int)cl.block_rank();
@@ -575,6 +576,12 @@ __global__ void __launch_bounds__(kClusterThreads, 1)
     if (with_post) P2(d, i, j) = F2(h, i, j);
   }
   cl.sync();  // no CTA exits while others may still read its shared memory
+}
+
+__global__ void __launch_bounds__(kClusterThreads, 1)
+    k_pcg_cluster(Ctx c, ClusterLayout L, int with_rhs, int with_post) {
+  extern __shared__ __align__(16) float sm[];
+  pcg_cluster_body(c, L, sm, with_rhs, with_post);
 }
 
 }  // namespace npom
