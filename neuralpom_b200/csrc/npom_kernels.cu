@@ -363,6 +363,57 @@ __device__ double grid_total(const Ctx &c, int slot) {
   return r;
 }
 
+// The DST stages of the spectral preconditioner (dst_stage_i / dst_stage_j:
+// out = Sx src along i, out = src Sy along j) over the ni x nj interior, in
+// tiles of kDstRows x kDstCols outputs per block (one per thread): chunks of
+// kDstChunk terms of both operands are staged in shared memory by coalesced
+// loads, then every thread sums its output's terms in FP64 in index order,
+// the order of dst_stage_i / dst_stage_j (so the values are theirs).  The
+// tiles are dealt to the blocks of the context; epi(a, b, value) stores.
+constexpr int kDstRows = 8, kDstCols = 32, kDstChunk = 64;
+static_assert(kDstRows * kDstCols == kThreads, "one output per thread");
+
+template <bool ALONG_I, class Epi>
+__device__ __forceinline__ void dst_tiles(const Ctx &c, const float *src, bool src_is_grid, Epi &&epi) {
+  __shared__ float lt[kDstRows][kDstChunk + 1];
+  __shared__ float rt[kDstChunk][kDstCols + 1];
+  const int ni = c.im - 2, nj = c.jm - 2;
+  const int K = ALONG_I ? ni : nj;
+  const float *sx = c.W[NPOM_W_sx], *sy = c.W[NPOM_W_sy];
+  const int tiles_b = (nj + kDstCols - 1) / kDstCols;
+  const int tiles = ((ni + kDstRows - 1) / kDstRows) * tiles_b;
+  const int tr = threadIdx.x / kDstCols, tc = threadIdx.x % kDstCols;
+  for (int tile = (int)vblock(c); tile < tiles; tile += (int)vgrid(c)) {
+    const int a0 = (tile / tiles_b) * kDstRows, b0 = (tile % tiles_b) * kDstCols;
+    double acc = 0.0;
+    for (int m0 = 0; m0 < K; m0 += kDstChunk) {
+      const int mc = min(kDstChunk, K - m0);
+      __syncthreads();  // the previous chunk is consumed
+      for (int e = threadIdx.x; e < kDstRows * kDstChunk; e += blockDim.x) {
+        const int r = e / kDstChunk, k = e % kDstChunk;
+        float v = 0.0f;
+        if (a0 + r < ni && k < mc)
+          v = ALONG_I ? __ldcg(sx + (size_t)(a0 + r) * ni + m0 + k) : __ldcg(src + (size_t)(a0 + r) * nj + m0 + k);
+        lt[r][k] = v;
+      }
+      for (int e = threadIdx.x; e < kDstChunk * kDstCols; e += blockDim.x) {
+        const int k = e / kDstCols, col = e % kDstCols;
+        float v = 0.0f;
+        if (k < mc && b0 + col < nj) {
+          if (!ALONG_I) v = __ldcg(sy + (size_t)(m0 + k) * nj + b0 + col);
+          else if (src_is_grid) v = __ldcg(src + NPOM_I2(c, m0 + k + 1, b0 + col + 1));
+          else v = __ldcg(src + (size_t)(m0 + k) * nj + b0 + col);
+        }
+        rt[k][col] = v;
+      }
+      __syncthreads();
+      for (int k = 0; k < mc; ++k) acc += (double)lt[tr][k] * (double)rt[k][tc];
+    }
+    const int a = a0 + tr, b = b0 + tc;
+    if (a < ni && b < nj) epi(a, b, (float)acc);
+  }
+}
+
 // z = M^-1 r over the interior; returns after its own trailing barrier.
 // Accumulates r.z into *rz of this thread.
 __device__ bool precondition(const Ctx &c, double &rz) {
@@ -375,28 +426,23 @@ __device__ bool precondition(const Ctx &c, double &rz) {
   rz = 0.0;
   if (c.k.eta_precond == NPOM_PRECOND_SPECTRAL) {
     float *t1 = c.W[NPOM_W_t1], *t2 = c.W[NPOM_W_t2];
-    for (size_t q = tid; q < nint; q += stride) {
-      int a = (int)(q / nj), b = (int)(q % nj);
-      t1[q] = dst_stage_i(c, r, true, a, b);
-    }
+    const float *ie = c.W[NPOM_W_inv_eigs];
+    dst_tiles<true>(c, r, true, [&](int a, int b, float v) { t1[(size_t)a * nj + b] = v; });
     if (!grid_barrier(c)) return false;
-    for (size_t q = tid; q < nint; q += stride) {
-      int a = (int)(q / nj), b = (int)(q % nj);
-      t2[q] = dst_stage_j(c, t1, a, b) * __ldcg(c.W[NPOM_W_inv_eigs] + q);
-    }
+    dst_tiles<false>(c, t1, false, [&](int a, int b, float v) {
+      const size_t q = (size_t)a * nj + b;
+      t2[q] = v * __ldcg(ie + q);
+    });
     if (!grid_barrier(c)) return false;
-    for (size_t q = tid; q < nint; q += stride) {
-      int a = (int)(q / nj), b = (int)(q % nj);
-      t1[q] = dst_stage_i(c, t2, false, a, b);
-    }
+    dst_tiles<true>(c, t2, false, [&](int a, int b, float v) { t1[(size_t)a * nj + b] = v; });
     if (!grid_barrier(c)) return false;
-    for (size_t q = tid; q < nint; q += stride) {
-      int a = (int)(q / nj), b = (int)(q % nj);
-      float zval = dst_stage_j(c, t1, a, b) / c.k.inverse_scale;
-      size_t o = NPOM_I2(c, a + 1, b + 1);
+    const float inv_scale = c.k.inverse_scale;
+    dst_tiles<false>(c, t1, false, [&](int a, int b, float v) {
+      const float zval = v / inv_scale;
+      const size_t o = NPOM_I2(c, a + 1, b + 1);
       zv[o] = zval;
       rz += (double)__ldcg(r + o) * (double)zval;
-    }
+    });
   } else {
     for (size_t q = tid; q < nint; q += stride) {
       int a = (int)(q / nj), b = (int)(q % nj);

@@ -96,7 +96,11 @@ def test_gpu_core_dens_baropg_methods_match_the_step():
     S = {k: v.copy() for k, v in A.items()}
     im, jm, kb = A["u"].shape
     P = oracle_params(dict(Sc, im=im, jm=jm, kb=kb), A, "explicit")
-    S["rho"] = O.dens(S, P)
-    assert _rel(rho.cpu().numpy(), S["rho"]) < 1e-6
+    assert _rel(rho.cpu().numpy(), O.dens(S, P)) < 1e-6
+    # BAROPG differences nearly equal densities, which magnifies the ulp
+    # differences of the two EOS evaluations (the oracle's float32 power and
+    # square root come from numpy's host-CPU-dependent SIMD paths): it is
+    # checked on the same rho
+    S["rho"] = rho.cpu().numpy()
     _, ox, oy = O.baropg(S, P)
     assert _rel(px.cpu().numpy(), ox) < 1e-6 and _rel(py.cpu().numpy(), oy) < 1e-6
