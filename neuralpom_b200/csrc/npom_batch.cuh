@@ -23,14 +23,18 @@
 //     cooperative form are summed per block, so a member that gets fewer
 //     blocks than it gets alone sums them in another order (results agree
 //     to rounding, not bitwise);
+//   A1 and B5 (kb == 16): the flux-once tiles of every member in one
+//     launch (bitwise the point kernels' values), with one rows-per-tile
+//     value for the whole batch;
 //   the step is captured once as a CUDA graph per value of do_internal and
 //   replayed (steps whose ramp is 1 for every member).
 #pragma once
 
 constexpr int kMaxBatch = NPOM_MAX_BATCH;
 
-enum BatchShape { BS_POINTS = 0, BS_LANES, BS_COLS, BS_CELLS, BS_SUB, BS_PCG, BS_NSHAPES };
-constexpr int kBatchThreads[BS_NSHAPES] = {kThreads, kThreads, 128, kThreads, kThreads, kThreads};
+enum BatchShape { BS_POINTS = 0, BS_LANES, BS_COLS, BS_CELLS, BS_A1T, BS_B5T, BS_SUB, BS_PCG, BS_NSHAPES };
+constexpr int kBatchThreads[BS_NSHAPES] = {kThreads, kThreads, 128, kThreads, kA1Threads, kB5Threads,
+                                           kThreads, kThreads};
 
 struct BatchTable {
   int count[BS_NSHAPES];                 // members (slots) of each shape
@@ -38,6 +42,8 @@ struct BatchTable {
   int start[BS_NSHAPES][kMaxBatch + 1];  // slot -> first block; start[count] = blocks of the launch
   int clu_count[2], clu_nc[2];           // cluster PCG: members and CTAs per cluster (8, 16)
   int clu_member[2][kMaxBatch];
+  int tile_strips[2][kMaxBatch];         // flux-once A1 / B5 tiles: column strips of each member
+  int tile_ichunk[2];                    // rows per tile (one value for all members)
   int nm;
   ClusterLayout L[kMaxBatch];
   Ctx ctx[kMaxBatch];
@@ -59,7 +65,7 @@ __device__ __forceinline__ void batch_copy_ctx(const Ctx *src, Ctx &dst) {
 // step's values; for the cooperative shapes L2 loads and the member's block
 // range as its grid).  Returns the block index within the member.
 template <int S>
-__device__ __forceinline__ int batch_enter(const BatchTable *t, const BatchStep &v, Ctx &sc) {
+__device__ __forceinline__ int batch_enter(const BatchTable *t, const BatchStep &v, Ctx &sc, int *member = nullptr) {
   __shared__ int s_slot;
   if (threadIdx.x == 0) {
     const int *st = t->start[S];
@@ -74,6 +80,7 @@ __device__ __forceinline__ int batch_enter(const BatchTable *t, const BatchStep 
   __syncthreads();
   const int slot = s_slot;
   const int m = t->member[S][slot];
+  if (member) *member = m;
   batch_copy_ctx(&t->ctx[m], sc);
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -115,6 +122,24 @@ __global__ void __launch_bounds__(kThreads) kb_cells(const BatchTable *t, BatchS
   __shared__ Ctx sc;
   const int lb = batch_enter<BS_CELLS>(t, v, sc);
   cells_body<PH>(sc, lb * blockDim.x + threadIdx.x);
+}
+
+// the flux-once A1 / B5 tiles of every member: block lb of a member is
+// strip lb % strips, row chunk lb / strips
+__global__ void __launch_bounds__(kA1Threads) kb_a1_tiles(const BatchTable *t, BatchStep v) {
+  __shared__ Ctx sc;
+  int m = 0;
+  const int lb = batch_enter<BS_A1T>(t, v, sc, &m);
+  const int st = t->tile_strips[0][m];
+  a1_tiles_body(sc, t->tile_ichunk[0], lb % st, lb / st);
+}
+
+__global__ void __launch_bounds__(kB5Threads) kb_b5_tiles(const BatchTable *t, BatchStep v) {
+  __shared__ Ctx sc;
+  int m = 0;
+  const int lb = batch_enter<BS_B5T>(t, v, sc, &m);
+  const int st = t->tile_strips[1][m];
+  b5_tiles_body(sc, t->tile_ichunk[1], lb % st, lb / st);
 }
 
 __global__ void __launch_bounds__(kThreads) kb_ext(const BatchTable *t, BatchStep v, int phase, int iext, int adv) {
@@ -182,6 +207,7 @@ struct BatchPlan {
   int clu_count[2] = {}, clu_nc[2] = {};
   size_t clu_smem[2] = {};
   bool lanes = false, b6_cols = false;
+  bool a1_tiles = false, b5_tiles = false;
   bool sub_req = false;   // NPOM_BATCH_SUBCYCLE=coop when the plan was made
   bool sub_coop = false;  // the cooperative subcycle is in use
   int nadv = 1, nitera = 0, mode = 3, isplit = 0, ispadv = 1;
@@ -259,6 +285,35 @@ cudaError_t make_batch_plan(const std::vector<Ctx> &ctx, int core, BatchPlan *P)
     columns += (size_t)ctx[m].im * ctx[m].jm;
   }
   P->b6_cols = !P->lanes || columns >= kProftThreadColumns;
+  // flux-once tiles for A1 and B5 (kb == 16; B5 not in mode 4 nor with
+  // MPDATA); NPOM_A1=points / NPOM_B5=points keep the point kernels.  Rows
+  // per tile: about 16 tiles per SM over the whole batch
+  {
+    const char *ea = getenv("NPOM_A1"), *eb = getenv("NPOM_B5");
+    P->a1_tiles = c0.kb == 16 && !(ea && std::strcmp(ea, "points") == 0);
+    P->b5_tiles = c0.kb == 16 && c0.k.mode != 4 && c0.k.nadv != 2 && !(eb && std::strcmp(eb, "points") == 0);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    for (int g = 0; g < 2; ++g) {
+      const int cols = g == 0 ? kA1Cols : kB5Cols;
+      size_t rows = 0;
+      for (int m = 0; m < nm; ++m) rows += (size_t)ctx[m].im * ((ctx[m].jm + cols - 1) / cols);
+      const int ichunk = std::max(2, (int)((rows + 16 * (size_t)sms - 1) / (16 * (size_t)sms)));
+      T->tile_ichunk[g] = ichunk;
+      const int S = g == 0 ? BS_A1T : BS_B5T;
+      int at = 0;
+      T->count[S] = nm;
+      for (int m = 0; m < nm; ++m) {
+        const int strips = (ctx[m].jm + cols - 1) / cols;
+        T->tile_strips[g][m] = strips;
+        T->member[S][m] = m;
+        T->start[S][m] = at;
+        at += strips * ((ctx[m].im + ichunk - 1) / ichunk);
+      }
+      T->start[S][nm] = at;
+      P->blocks[S] = at;
+    }
+  }
   // the plain shapes: every member, blocks to cover its work
   for (int S = BS_POINTS; S <= BS_CELLS; ++S) {
     int at = 0;
@@ -416,7 +471,8 @@ cudaError_t batch_pcg(const BatchPlan &P, const BatchStep &v, cudaStream_t s) {
 
 // one internal step of every member (the order of enqueue_step)
 cudaError_t enqueue_batch_step(const BatchPlan &P, const BatchStep &v, cudaStream_t s) {
-  batch_points<PP_A1>(P, v, s);
+  if (P.a1_tiles) kb_a1_tiles<<<P.blocks[BS_A1T], kA1Threads, 0, s>>>(P.d_table, v);
+  else batch_points<PP_A1>(P, v, s);
   batch_cols<CP_A2>(P, v, s);
   batch_cells<XP_A3>(P, v, s);
   cudaError_t e;
@@ -446,6 +502,8 @@ cudaError_t enqueue_batch_step(const BatchPlan &P, const BatchStep &v, cudaStrea
       }
       kb_mpdata<<<g, kThreads, 0, s>>>(t, v, MP_DIFFUSION, 0);
       kb_mpdata<<<g, kThreads, 0, s>>>(t, v, MP_FINISH, 0);
+    } else if (P.b5_tiles) {
+      kb_b5_tiles<<<P.blocks[BS_B5T], kB5Threads, 0, s>>>(P.d_table, v);
     } else {
       batch_points<PP_B5>(P, v, s);
     }

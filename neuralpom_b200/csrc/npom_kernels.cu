@@ -150,12 +150,13 @@ __global__ void __launch_bounds__(kThreads) k_cells(Ctx c) {
 constexpr int kA1Cols = 16;
 constexpr int kA1Threads = 16 * (kA1Cols + 2);
 
-__global__ void __launch_bounds__(kA1Threads) k_a1_tiles(Ctx c, int ichunk) {
+// strip bx of kA1Cols columns, rows [by * ichunk, (by + 1) * ichunk)
+__device__ __forceinline__ void a1_tiles_body(const Ctx &c, int ichunk, int bx, int by) {
   __shared__ float s_yu[kA1Cols + 2][16], s_yv[kA1Cols + 2][16], s_cv[kA1Cols + 2][16];
   const int k = threadIdx.x & 15;
   const int r = threadIdx.x >> 4;  // row r holds column j0 - 1 + r
-  const int j = blockIdx.x * kA1Cols - 1 + r;
-  const int i0 = blockIdx.y * ichunk, i1 = min(c.im, i0 + ichunk);
+  const int j = bx * kA1Cols - 1 + r;
+  const int i0 = by * ichunk, i1 = min(c.im, i0 + ichunk);
   const bool jin = j >= 0 && j < c.jm;
   const bool out_row = jin && r >= 1 && r <= kA1Cols;
   const bool lev = k < c.kb - 1;
@@ -206,6 +207,10 @@ __global__ void __launch_bounds__(kA1Threads) k_a1_tiles(Ctx c, int ichunk) {
   }
 }
 
+__global__ void __launch_bounds__(kA1Threads) k_a1_tiles(Ctx c, int ichunk) {
+  a1_tiles_body(c, ichunk, blockIdx.x, blockIdx.y);
+}
+
 // B5 on large grids: the ADVT1 face fluxes of T and S computed once per
 // face.  A block holds kB5Cols output columns (plus the column above) x 16
 // levels and marches along i; the x-face fluxes stay in registers, the
@@ -214,12 +219,13 @@ __global__ void __launch_bounds__(kA1Threads) k_a1_tiles(Ctx c, int ichunk) {
 constexpr int kB5Cols = 16;
 constexpr int kB5Threads = 16 * (kB5Cols + 1);
 
-__global__ void __launch_bounds__(kB5Threads) k_b5_tiles(Ctx c, int ichunk) {
+// strip bx of kB5Cols columns, rows [by * ichunk, (by + 1) * ichunk)
+__device__ __forceinline__ void b5_tiles_body(const Ctx &c, int ichunk, int bx, int by) {
   __shared__ float s_yt[kB5Cols + 1][16], s_ys[kB5Cols + 1][16];
   const int k = threadIdx.x & 15;
   const int r = threadIdx.x >> 4;  // row r holds column j0 + r
-  const int j = blockIdx.x * kB5Cols + r;
-  const int i0 = blockIdx.y * ichunk, i1 = min(c.im, i0 + ichunk);
+  const int j = bx * kB5Cols + r;
+  const int i0 = by * ichunk, i1 = min(c.im, i0 + ichunk);
   const bool jin = j < c.jm;
   const bool out_row = jin && r < kB5Cols;
   const bool lev = k < c.kb - 1;
@@ -260,6 +266,10 @@ __global__ void __launch_bounds__(kB5Threads) k_b5_tiles(Ctx c, int ichunk) {
     xt = xt_n;
     xs = xs_n;
   }
+}
+
+__global__ void __launch_bounds__(kB5Threads) k_b5_tiles(Ctx c, int ichunk) {
+  b5_tiles_body(c, ichunk, blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------
