@@ -387,6 +387,17 @@ cudaError_t make_batch_plan(const std::vector<Ctx> &ctx, int core, BatchPlan *P)
         e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         if (e != cudaSuccess) return e;
       }
+      // a cluster shape that cannot be resident sends its members to the
+      // cooperative form
+      for (int g = 0; g < 2; ++g) {
+        if (P->clu_count[g] == 0 || cluster_launchable(fn, P->clu_nc[g], (size_t)smem)) continue;
+        for (int q = 0; q < T->clu_count[g]; ++q) {
+          const int m = T->clu_member[g][q];
+          coop.push_back(m);
+          work.push_back((size_t)(ctx[m].im - 2) * (ctx[m].jm - 2));
+        }
+        T->clu_count[g] = P->clu_count[g] = 0;
+      }
     }
     int total = 0;
     if (!batch_coop_shares((const void *)kb_pcg, coop, work, T->start[BS_PCG], &total)) return cudaErrorInvalidValue;

@@ -359,13 +359,16 @@ __device__ void block_sum3(const Ctx &c, double a0, double a1, double a2, int s0
 }
 
 // sum of one partial slot over blocks, identical in every block
+// (warp 0: lane l sums the partials l, l + 32, ... in order, then a fixed
+// shuffle tree; the loads of the lanes are in flight together)
 __device__ double grid_total(const Ctx &c, int slot) {
   __shared__ double tot;
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < 32) {
     double t = 0.0;
     const int G = vgrid(c);
-    for (int b = 0; b < G; ++b) t += __ldcg(c.partials + slot * G + b);
-    tot = t;
+    for (int b = threadIdx.x; b < G; b += 32) t += __ldcg(c.partials + slot * G + b);
+    for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
+    if (threadIdx.x == 0) tot = t;
   }
   __syncthreads();
   double r = tot;
@@ -814,8 +817,10 @@ void launch_cells(const Ctx &c, cudaStream_t s) {
 }
 
 // Cluster PCG when the interior fits in one cluster's shared memory (8 CTAs,
-// or 16 with the non-portable cluster size); NPOM_PCG=coop forces the
-// grid-barrier kernel, NPOM_PCG_CTAS=16 prefers the 16-CTA cluster.
+// or 16 with the non-portable cluster size), first with the Sy fragment
+// table in shared memory, then with Sy read from global memory (128x112
+// interiors); NPOM_PCG=coop forces the grid-barrier kernel,
+// NPOM_PCG_CTAS=16 prefers the 16-CTA cluster.
 bool pcg_cluster_layout(const Ctx &c, ClusterLayout *out) {
   const char *env = getenv("NPOM_PCG");
   if (env && std::strcmp(env, "coop") == 0) return false;
@@ -824,11 +829,13 @@ bool pcg_cluster_layout(const Ctx &c, ClusterLayout *out) {
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return false;
   const char *ctas = getenv("NPOM_PCG_CTAS");
   const bool prefer16 = ctas && std::strcmp(ctas, "16") == 0;
-  for (int nc : {prefer16 ? 16 : 8, prefer16 ? 8 : 16}) {
-    ClusterLayout L = cluster_layout(c.im, c.jm, nc);
-    if (L.fits && L.bytes() <= (size_t)optin) {
-      *out = L;
-      return true;
+  for (bool sy_global : {false, true}) {
+    for (int nc : {prefer16 ? 16 : 8, prefer16 ? 8 : 16}) {
+      ClusterLayout L = cluster_layout(c.im, c.jm, nc, sy_global);
+      if (L.fits && L.bytes() <= (size_t)optin) {
+        *out = L;
+        return true;
+      }
     }
   }
   return false;
@@ -876,8 +883,31 @@ struct PcgPlan {
   int coop_blocks;
 };
 
+// true when at least one cluster of nc CTAs of kClusterThreads with smem
+// bytes of dynamic shared memory can be resident (attributes already set)
+bool cluster_launchable(const void *fn, int nc, size_t smem) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nc);
+  cfg.blockDim = dim3(kClusterThreads);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = nc;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, fn, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return n > 0;
+}
+
 cudaError_t plan_pcg(const Ctx &c, PcgPlan *plan) {
-  plan->cluster = pcg_cluster_layout(c, &plan->L) && ensure_cluster_attrs(plan->L);
+  plan->cluster = pcg_cluster_layout(c, &plan->L) && ensure_cluster_attrs(plan->L) &&
+                  cluster_launchable((const void *)k_pcg_cluster, plan->L.nc, plan->L.bytes());
   plan->coop_blocks = 0;
   if (plan->cluster) return cudaSuccess;
   return coop_blocks((const void *)k_pcg, (size_t)(c.im - 2) * (c.jm - 2), &plan->coop_blocks);

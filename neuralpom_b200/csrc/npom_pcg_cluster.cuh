@@ -61,13 +61,15 @@ struct ClusterLayout {
   // float offsets in dynamic shared memory
   int x, r, z, ap, rhs, p, zh, h4, c4, iart, ie, gr, gc, sxf, syf, t1f;
   int floats;
-  bool fits;  // rows <= 16 and one column tile per warp
+  bool fits;       // rows <= 16 and one column tile per warp
+  bool sy_global;  // Sy read from global memory in the j-stages (no room for its fragments)
   size_t red_doubles() const { return (size_t)kRedSlots * nc * kClusterWarps; }
   size_t bytes() const { return (size_t)floats * sizeof(float) + red_doubles() * sizeof(double); }
 };
 
-inline ClusterLayout cluster_layout(int im, int jm, int nc) {
+inline ClusterLayout cluster_layout(int im, int jm, int nc, bool sy_global = false) {
   ClusterLayout L;
+  L.sy_global = sy_global;
   L.ni = im - 2;
   L.nj = jm - 2;
   L.nc = nc;
@@ -98,7 +100,8 @@ inline ClusterLayout cluster_layout(int im, int jm, int nc) {
   L.gr = take(8 * L.kti * L.gp);           // full residual, zero-padded rows/columns
   L.gc = take(8 * L.kti * L.gp);           // full half-transformed field
   L.sxf = take(L.kti * 32 * 8);            // Sx slab as A fragments: per k-tile 32 lanes x hi4, then 32 x lo4
-  L.syf = take(L.nt * L.nt * 32 * 4);      // Sy as B fragments: (hi x2, lo x2) per lane, k-tile, column tile
+  // Sy as B fragments: (hi x2, lo x2) per lane, k-tile, column tile
+  L.syf = sy_global ? -1 : take(L.nt * L.nt * 32 * 4);
   L.t1f = take(L.nt * 32 * 4);             // i-stage result as A fragments of the j-stage
   L.floats = o;
   return L;
@@ -264,28 +267,58 @@ __device__ __forceinline__ void cl_dst_i(const ClusterLayout &L, float *sm, cons
 }
 
 // j-stage: C[r][l] = sum_b T[r][b] Sy[b][l] for the column tile of this
-// warp; epi(row, col, value) for the rows < nr and columns < nj
+// warp; epi(row, col, value) for the rows < nr and columns < nj.  With
+// L.sy_global the B operand comes from Sy in global memory (syg): the lane's
+// values of every k-tile of the warp's column tile are loaded up front and
+// split as the fragment table splits them, so the products are the same.
 template <class Epi>
-__device__ __forceinline__ void cl_dst_j(const ClusterLayout &L, float *sm, int nr, Epi &&epi) {
+__device__ __forceinline__ void cl_dst_j(const ClusterLayout &L, float *sm, int nr, const float *syg, Epi &&epi) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (w >= L.nt) return;
   const int g = lane >> 2, t = lane & 3;
   const float4 *af = reinterpret_cast<const float4 *>(sm + L.t1f);
-  const float4 *bf = reinterpret_cast<const float4 *>(sm + L.syf);
   float hh[4] = {0.f, 0.f, 0.f, 0.f}, hl[4] = {0.f, 0.f, 0.f, 0.f}, lh[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll 2
-  for (int kt = 0; kt < L.nt; ++kt) {
-    const float4 av = af[kt * 32 + lane];
-    const float4 b = bf[(kt * L.nt + w) * 32 + lane];
-    unsigned ah0, al0, ah1, al1, ah2, al2, ah3, al3;
-    tf32_split(av.x, ah0, al0);
-    tf32_split(av.y, ah1, al1);
-    tf32_split(av.z, ah2, al2);
-    tf32_split(av.w, ah3, al3);
-    const unsigned bh0 = __float_as_uint(b.x), bh1 = __float_as_uint(b.y);
-    mma_tf32(hh, ah0, ah1, ah2, ah3, bh0, bh1);
-    mma_tf32(hl, ah0, ah1, ah2, ah3, __float_as_uint(b.z), __float_as_uint(b.w));
-    mma_tf32(lh, al0, al1, al2, al3, bh0, bh1);
+  if (L.sy_global) {
+    const int col = 8 * w + g, nj = L.nj;
+    float v0[kClusterWarps], v1[kClusterWarps];
+#pragma unroll
+    for (int kt = 0; kt < kClusterWarps; ++kt) {
+      const int b0 = 8 * kt + t, b1 = b0 + 4;
+      v0[kt] = (kt < L.nt && b0 < nj && col < nj) ? __ldg(syg + (size_t)b0 * nj + col) : 0.0f;
+      v1[kt] = (kt < L.nt && b1 < nj && col < nj) ? __ldg(syg + (size_t)b1 * nj + col) : 0.0f;
+    }
+#pragma unroll
+    for (int kt = 0; kt < kClusterWarps; ++kt) {
+      if (kt < L.nt) {
+        const float4 av = af[kt * 32 + lane];
+        unsigned ah0, al0, ah1, al1, ah2, al2, ah3, al3, bh0, bl0, bh1, bl1;
+        tf32_split(av.x, ah0, al0);
+        tf32_split(av.y, ah1, al1);
+        tf32_split(av.z, ah2, al2);
+        tf32_split(av.w, ah3, al3);
+        tf32_split(v0[kt], bh0, bl0);
+        tf32_split(v1[kt], bh1, bl1);
+        mma_tf32(hh, ah0, ah1, ah2, ah3, bh0, bh1);
+        mma_tf32(hl, ah0, ah1, ah2, ah3, bl0, bl1);
+        mma_tf32(lh, al0, al1, al2, al3, bh0, bh1);
+      }
+    }
+  } else {
+    const float4 *bf = reinterpret_cast<const float4 *>(sm + L.syf);
+  #pragma unroll 2
+    for (int kt = 0; kt < L.nt; ++kt) {
+      const float4 av = af[kt * 32 + lane];
+      const float4 b = bf[(kt * L.nt + w) * 32 + lane];
+      unsigned ah0, al0, ah1, al1, ah2, al2, ah3, al3;
+      tf32_split(av.x, ah0, al0);
+      tf32_split(av.y, ah1, al1);
+      tf32_split(av.z, ah2, al2);
+      tf32_split(av.w, ah3, al3);
+      const unsigned bh0 = __float_as_uint(b.x), bh1 = __float_as_uint(b.y);
+      mma_tf32(hh, ah0, ah1, ah2, ah3, bh0, bh1);
+      mma_tf32(hl, ah0, ah1, ah2, ah3, __float_as_uint(b.z), __float_as_uint(b.w));
+      mma_tf32(lh, al0, al1, al2, al3, bh0, bh1);
+    }
   }
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
@@ -299,7 +332,8 @@ __device__ __forceinline__ void cl_dst_j(const ClusterLayout &L, float *sm, int 
 // field into gc (one cluster barrier inside), writes z, pushes the z rows
 // that neighbours keep as halo and returns this thread's share of r.z.
 __device__ __forceinline__ double cl_precondition(cgx::cluster_group &cl, const ClusterLayout &L, float *sm, int nr,
-                                                  int rank, int a0, float inverse_scale, bool spectral) {
+                                                  int rank, int a0, float inverse_scale, bool spectral,
+                                                  const float *syg) {
   const int nj = L.nj;
   float *z = sm + L.z;
   const float *r = sm + L.r;
@@ -326,14 +360,14 @@ __device__ __forceinline__ double cl_precondition(cgx::cluster_group &cl, const 
   // DST along j times the inverse eigenvalues, pushed into every CTA's gc
   // (staged in the ap slab, free until the next operator apply)
   float *stage = sm + L.ap;
-  cl_dst_j(L, sm, nr, [&](int ra, int l, float acc) { stage[ra * nj + l] = acc * ie[ra * nj + l]; });
+  cl_dst_j(L, sm, nr, syg, [&](int ra, int l, float acc) { stage[ra * nj + l] = acc * ie[ra * nj + l]; });
   __syncthreads();
   cl_push_slab(cl, L, sm, L.ap, L.gc, a0, nr);
   cl.sync();  // gc complete in every CTA
   cl_dst_i(L, sm, sm + L.gc);
   __syncthreads();
   // DST along j divided by the scale: z
-  cl_dst_j(L, sm, nr, [&](int ra, int l, float acc) { finish(ra, l, acc / inverse_scale); });
+  cl_dst_j(L, sm, nr, syg, [&](int ra, int l, float acc) { finish(ra, l, acc / inverse_scale); });
   return rz;
 }
 
@@ -411,8 +445,8 @@ __device__ __forceinline__ void pcg_cluster_body(const Ctx &c, const ClusterLayo
       dst[0] = make_float4(__uint_as_float(hi[0]), __uint_as_float(hi[1]), __uint_as_float(hi[2]), __uint_as_float(hi[3]));
       dst[32] = make_float4(__uint_as_float(lo[0]), __uint_as_float(lo[1]), __uint_as_float(lo[2]), __uint_as_float(lo[3]));
     }
-    // Sy as split B fragments
-    for (int f = threadIdx.x; f < L.nt * L.nt * 32; f += blockDim.x) {
+    // Sy as split B fragments (kept in global memory with sy_global)
+    for (int f = threadIdx.x; !L.sy_global && f < L.nt * L.nt * 32; f += blockDim.x) {
       const int lane = f & 31, tile = f >> 5, kt = tile / L.nt, ct = tile - kt * L.nt, g = lane >> 2, t = lane & 3;
       const int col = 8 * ct + g, b0 = 8 * kt + t, b1 = b0 + 4;
       const float v0 = (b0 < nj && col < nj) ? sy[(size_t)b0 * nj + col] : 0.0f;
@@ -449,7 +483,7 @@ __device__ __forceinline__ void pcg_cluster_body(const Ctx &c, const ClusterLayo
   cl_push_partial(cl, rr, red, 3, nc, rank);
   cl.sync();  // r pushed everywhere; neighbours' x halo reads done
   const double rs0 = cl_partial_total(red, 3, nc);
-  double rz = cl_precondition(cl, L, sm, nr, rank, a0, c.k.inverse_scale, spectral);
+  double rz = cl_precondition(cl, L, sm, nr, rank, a0, c.k.inverse_scale, spectral, c.W[NPOM_W_sy]);
   cl_push_partial(cl, rz, red, 2, nc, rank);
   cl.sync();  // z halo rows and r.z partials in place
   double rho_old = cl_partial_total(red, 2, nc);
@@ -517,7 +551,7 @@ __device__ __forceinline__ void pcg_cluster_body(const Ctx &c, const ClusterLayo
       converged = true;
       break;
     }
-    rz = cl_precondition(cl, L, sm, nr, rank, a0, c.k.inverse_scale, spectral);
+    rz = cl_precondition(cl, L, sm, nr, rank, a0, c.k.inverse_scale, spectral, c.W[NPOM_W_sy]);
     cl_push_partial(cl, rz, red, 2, nc, rank);
     cl.sync();
     const double rho_new = cl_partial_total(red, 2, nc);
