@@ -1028,6 +1028,11 @@ def run_batch(args):
         launch_all(steps_of)
         return sum(launches_of(mb["core"], steps_of(mb), 2.0) for mb in members)
 
+    # a bench step is one simulated day of every member; --internal-steps
+    # replaces the day by that many internal steps of every member (profiling)
+    def steps_of(mb):
+        return args.internal_steps or mb["nday"]
+
     for _ in range(args.warmup):
         advance(lambda mb: 4)
     torch.cuda.synchronize(dev)
@@ -1037,7 +1042,7 @@ def run_batch(args):
             l2_flush(flush)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(main_stream)
-            launches += advance(lambda mb: mb["nday"])
+            launches += advance(steps_of)
             b.record(main_stream)
             torch.cuda.synchronize(dev)
             total_ms += a.elapsed_time(b)
@@ -1046,8 +1051,9 @@ def run_batch(args):
         if bits & (_abi.DEV_TIMEOUT | _abi.DEV_VMAX | _abi.DEV_NONFINITE):
             raise RuntimeError(f"device status 0x{bits:x} in the batch run")
     nmem = len(members)
-    value = nmem * args.steps / (total_ms / 1000.0)
-    nbytes = sum(mb["nday"] * step_algorithmic_bytes(*mb["grid"], 16, mb["name"]) for mb in members) * args.steps
+    member_days = sum(steps_of(mb) * float(mb["core"].dti) / 86400.0 for mb in members) * args.steps
+    value = member_days / (total_ms / 1000.0)
+    nbytes = sum(steps_of(mb) * step_algorithmic_bytes(*mb["grid"], 16, mb["name"]) for mb in members) * args.steps
     peak, src = measured_peaks()
     achieved = nbytes / (total_ms / 1000.0) / 1e9
     ref = None
@@ -1078,7 +1084,8 @@ def run_batch(args):
                                          if args.batch_mode == "launch" else os.environ.get("NPOM_SUBCYCLE")),
                    "turns_per_day": args.batch_chunk,
                    "hw_queues": os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS"),
-                   "member_days_per_step": nmem, "l2": "flushed (256 MiB write) before every timed step"},
+                   "member_days_per_step": member_days / args.steps, "internal_steps": args.internal_steps,
+                   "l2": "flushed (256 MiB write) before every timed step"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": src, "traffic": None, "algorithmic_bytes": nbytes,
                      "note": "whole batch: algorithmic bytes of every member's steps over the device time"},

@@ -15,7 +15,8 @@
 //     all members (NPOM_BATCH_SUBCYCLE=phases, the default), or one
 //     cooperative launch for the whole subcycle in which each member's
 //     blocks meet at their own grid barrier (=coop);
-//   PCG (semi-implicit core): one cluster launch per cluster size, one
+//   PCG (semi-implicit core): one cluster launch per cluster shape (CTAs,
+//     Sy in shared or global memory), one
 //     cluster per member whose interior fits the cluster layout (the
 //     member's own shared-memory layout, as when it runs alone); one
 //     cooperative launch for the other members, each on its own share of
@@ -40,8 +41,9 @@ struct BatchTable {
   int count[BS_NSHAPES];                 // members (slots) of each shape
   int member[BS_NSHAPES][kMaxBatch];     // slot -> member
   int start[BS_NSHAPES][kMaxBatch + 1];  // slot -> first block; start[count] = blocks of the launch
-  int clu_count[2], clu_nc[2];           // cluster PCG: members and CTAs per cluster (8, 16)
-  int clu_member[2][kMaxBatch];
+  // cluster PCG groups g = (nc > 8) + 2 * sy_global: members, CTAs per cluster
+  int clu_count[4], clu_nc[4];
+  int clu_member[4][kMaxBatch];
   int tile_strips[2][kMaxBatch];         // flux-once A1 / B5 tiles: column strips of each member
   int tile_ichunk[2];                    // rows per tile (one value for all members)
   int nm;
@@ -167,7 +169,8 @@ __global__ void __launch_bounds__(kThreads) kb_pcg(const BatchTable *t, BatchSte
 }
 
 // cluster group g of the table: consecutive clusters of clu_nc[g] CTAs,
-// one member each
+// one member each (SYG: the group's layouts read Sy from global memory)
+template <bool SYG>
 __global__ void __launch_bounds__(kClusterThreads, 1)
     kb_pcg_cluster(const BatchTable *t, BatchStep v, int g, int with_rhs, int with_post) {
   extern __shared__ __align__(16) float sm[];
@@ -182,7 +185,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1)
     sc.do_internal = v.do_internal;
   }
   __syncthreads();
-  pcg_cluster_body(sc, sL, sm, with_rhs, with_post);
+  pcg_cluster_body<SYG>(sc, sL, sm, with_rhs, with_post);
 }
 
 // clears words [0, words) of the control block of every member (the
@@ -204,8 +207,8 @@ struct BatchPlan {
   std::vector<Ctx> key;
   BatchTable *d_table = nullptr;
   int blocks[BS_NSHAPES] = {};
-  int clu_count[2] = {}, clu_nc[2] = {};
-  size_t clu_smem[2] = {};
+  int clu_count[4] = {}, clu_nc[4] = {};
+  size_t clu_smem[4] = {};
   bool lanes = false, b6_cols = false;
   bool a1_tiles = false, b5_tiles = false;
   bool sub_req = false;   // NPOM_BATCH_SUBCYCLE=coop when the plan was made
@@ -258,6 +261,10 @@ bool batch_coop_shares(const void *fn, const std::vector<int> &members, const st
   start[n] = at;
   *total = at;
   return at <= cap;
+}
+
+const void *batch_cluster_fn(int g) {
+  return g >= 2 ? (const void *)kb_pcg_cluster<true> : (const void *)kb_pcg_cluster<false>;
 }
 
 cudaError_t make_batch_plan(const std::vector<Ctx> &ctx, int core, BatchPlan *P) {
@@ -359,7 +366,7 @@ cudaError_t make_batch_plan(const std::vector<Ctx> &ctx, int core, BatchPlan *P)
       ClusterLayout L{};
       const bool fits = pcg_cluster_layout(ctx[m], &L) && L.bytes() + kBatchStaticSmem <= (size_t)optin;
       if (fits) {
-        const int g = L.nc > 8 ? 1 : 0;
+        const int g = (L.nc > 8 ? 1 : 0) + (L.sy_global ? 2 : 0);
         T->L[m] = L;
         T->clu_member[g][T->clu_count[g]++] = m;
         T->clu_nc[g] = L.nc;
@@ -369,35 +376,33 @@ cudaError_t make_batch_plan(const std::vector<Ctx> &ctx, int core, BatchPlan *P)
         work.push_back((size_t)(ctx[m].im - 2) * (ctx[m].jm - 2));
       }
     }
-    for (int g = 0; g < 2; ++g) {
+    for (int g = 0; g < 4; ++g) {
       P->clu_count[g] = T->clu_count[g];
       P->clu_nc[g] = T->clu_nc[g];
-    }
-    if (P->clu_count[0] + P->clu_count[1] > 0) {
-      // the attribute only grows (plans made earlier keep their launches valid)
-      static int smem_set[64] = {0};
-      const void *fn = (const void *)kb_pcg_cluster;
-      const int smem = (int)std::max(P->clu_smem[0], P->clu_smem[1]);
-      if (smem > smem_set[dev]) {
+      if (P->clu_count[g] == 0) continue;
+      // the attribute only grows (plans made earlier keep their launches
+      // valid); a cluster shape that cannot be resident sends its members
+      // to the cooperative form
+      static int smem_set[64][2] = {};
+      const int v = g >> 1;
+      const void *fn = batch_cluster_fn(g);
+      const int smem = (int)P->clu_smem[g];
+      if (smem > smem_set[dev][v]) {
         e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
-        smem_set[dev] = smem;
+        smem_set[dev][v] = smem;
       }
-      if (P->clu_count[1] > 0) {
+      if (P->clu_nc[g] > 8) {
         e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         if (e != cudaSuccess) return e;
       }
-      // a cluster shape that cannot be resident sends its members to the
-      // cooperative form
-      for (int g = 0; g < 2; ++g) {
-        if (P->clu_count[g] == 0 || cluster_launchable(fn, P->clu_nc[g], (size_t)smem)) continue;
-        for (int q = 0; q < T->clu_count[g]; ++q) {
-          const int m = T->clu_member[g][q];
-          coop.push_back(m);
-          work.push_back((size_t)(ctx[m].im - 2) * (ctx[m].jm - 2));
-        }
-        T->clu_count[g] = P->clu_count[g] = 0;
+      if (cluster_launchable(fn, P->clu_nc[g], (size_t)smem)) continue;
+      for (int q = 0; q < T->clu_count[g]; ++q) {
+        const int m = T->clu_member[g][q];
+        coop.push_back(m);
+        work.push_back((size_t)(ctx[m].im - 2) * (ctx[m].jm - 2));
       }
+      T->clu_count[g] = P->clu_count[g] = 0;
     }
     int total = 0;
     if (!batch_coop_shares((const void *)kb_pcg, coop, work, T->start[BS_PCG], &total)) return cudaErrorInvalidValue;
@@ -456,12 +461,12 @@ cudaError_t batch_pcg(const BatchPlan &P, const BatchStep &v, cudaStream_t s) {
   const BatchTable *t = P.d_table;
   BatchStep vv = v;
   int with_rhs = 1, with_post = 1;
-  for (int g = 0; g < 2; ++g) {
+  for (int g = 0; g < 4; ++g) {
     if (P.clu_count[g] == 0) continue;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(P.clu_count[g] * P.clu_nc[g]);
     cfg.blockDim = dim3(kClusterThreads);
-    cfg.dynamicSmemBytes = std::max(P.clu_smem[0], P.clu_smem[1]);
+    cfg.dynamicSmemBytes = P.clu_smem[g];
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -470,7 +475,8 @@ cudaError_t batch_pcg(const BatchPlan &P, const BatchStep &v, cudaStream_t s) {
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cudaError_t e = cudaLaunchKernelEx(&cfg, kb_pcg_cluster, t, vv, g, with_rhs, with_post);
+    cudaError_t e = g >= 2 ? cudaLaunchKernelEx(&cfg, kb_pcg_cluster<true>, t, vv, g, with_rhs, with_post)
+                           : cudaLaunchKernelEx(&cfg, kb_pcg_cluster<false>, t, vv, g, with_rhs, with_post);
     if (e != cudaSuccess) return e;
   }
   if (P.blocks[BS_PCG] > 0) {
@@ -530,7 +536,8 @@ cudaError_t enqueue_batch_step(const BatchPlan &P, const BatchStep &v, cudaStrea
 int batch_step_launches(const BatchPlan &P, int do_internal) {
   int n = 3 + 1;  // A1 A2 A3, B9
   if (P.core == NPOM_CORE_IMPLICIT) {
-    n += (P.clu_count[0] > 0) + (P.clu_count[1] > 0) + (P.blocks[BS_PCG] > 0 ? 2 : 0) + 1;
+    for (int g = 0; g < 4; ++g) n += P.clu_count[g] > 0;
+    n += (P.blocks[BS_PCG] > 0 ? 2 : 0) + 1;
   } else {
     n += P.sub_coop ? 2 : 3 * P.isplit;
   }

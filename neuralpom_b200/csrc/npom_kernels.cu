@@ -842,20 +842,26 @@ bool pcg_cluster_layout(const Ctx &c, ClusterLayout *out) {
 }
 
 // Kernel attributes are set once per device (not inside graph captures).
+// The cluster PCG kernel instance of a layout.
+const void *pcg_cluster_fn(const ClusterLayout &L) {
+  return L.sy_global ? (const void *)k_pcg_cluster<true> : (const void *)k_pcg_cluster<false>;
+}
+
 bool ensure_cluster_attrs(const ClusterLayout &L) {
-  static int smem_set[64] = {0};
-  static bool nonportable[64] = {false};
+  static int smem_set[64][2] = {};
+  static bool nonportable[64][2] = {};
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
-  const void *fn = (const void *)k_pcg_cluster;
-  if ((int)L.bytes() > smem_set[dev]) {
+  const void *fn = pcg_cluster_fn(L);
+  const int v = L.sy_global ? 1 : 0;
+  if ((int)L.bytes() > smem_set[dev][v]) {
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.bytes()) != cudaSuccess)
       return false;
-    smem_set[dev] = (int)L.bytes();
+    smem_set[dev][v] = (int)L.bytes();
   }
-  if (L.nc > 8 && !nonportable[dev]) {
+  if (L.nc > 8 && !nonportable[dev][v]) {
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) return false;
-    nonportable[dev] = true;
+    nonportable[dev][v] = true;
   }
   return true;
 }
@@ -873,7 +879,8 @@ cudaError_t run_pcg_cluster(const Ctx &c, const ClusterLayout &L, int with_rhs, 
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_pcg_cluster, c, L, with_rhs, with_post);
+  if (L.sy_global) return cudaLaunchKernelEx(&cfg, k_pcg_cluster<true>, c, L, with_rhs, with_post);
+  return cudaLaunchKernelEx(&cfg, k_pcg_cluster<false>, c, L, with_rhs, with_post);
 }
 
 // Launch shape of the PCG for this grid, decided outside any capture.
@@ -907,7 +914,7 @@ bool cluster_launchable(const void *fn, int nc, size_t smem) {
 
 cudaError_t plan_pcg(const Ctx &c, PcgPlan *plan) {
   plan->cluster = pcg_cluster_layout(c, &plan->L) && ensure_cluster_attrs(plan->L) &&
-                  cluster_launchable((const void *)k_pcg_cluster, plan->L.nc, plan->L.bytes());
+                  cluster_launchable(pcg_cluster_fn(plan->L), plan->L.nc, plan->L.bytes());
   plan->coop_blocks = 0;
   if (plan->cluster) return cudaSuccess;
   return coop_blocks((const void *)k_pcg, (size_t)(c.im - 2) * (c.jm - 2), &plan->coop_blocks);

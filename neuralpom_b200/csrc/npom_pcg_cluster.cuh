@@ -268,17 +268,18 @@ __device__ __forceinline__ void cl_dst_i(const ClusterLayout &L, float *sm, cons
 
 // j-stage: C[r][l] = sum_b T[r][b] Sy[b][l] for the column tile of this
 // warp; epi(row, col, value) for the rows < nr and columns < nj.  With
-// L.sy_global the B operand comes from Sy in global memory (syg): the lane's
+// SYG (layouts with sy_global) the B operand comes from Sy in global memory
+// (syg): the lane's
 // values of every k-tile of the warp's column tile are loaded up front and
 // split as the fragment table splits them, so the products are the same.
-template <class Epi>
+template <bool SYG, class Epi>
 __device__ __forceinline__ void cl_dst_j(const ClusterLayout &L, float *sm, int nr, const float *syg, Epi &&epi) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (w >= L.nt) return;
   const int g = lane >> 2, t = lane & 3;
   const float4 *af = reinterpret_cast<const float4 *>(sm + L.t1f);
   float hh[4] = {0.f, 0.f, 0.f, 0.f}, hl[4] = {0.f, 0.f, 0.f, 0.f}, lh[4] = {0.f, 0.f, 0.f, 0.f};
-  if (L.sy_global) {
+  if (SYG) {
     const int col = 8 * w + g, nj = L.nj;
     float v0[kClusterWarps], v1[kClusterWarps];
 #pragma unroll
@@ -331,6 +332,7 @@ __device__ __forceinline__ void cl_dst_j(const ClusterLayout &L, float *sm, int 
 // the cluster barrier after the push passed).  Pushes the half-transformed
 // field into gc (one cluster barrier inside), writes z, pushes the z rows
 // that neighbours keep as halo and returns this thread's share of r.z.
+template <bool SYG>
 __device__ __forceinline__ double cl_precondition(cgx::cluster_group &cl, const ClusterLayout &L, float *sm, int nr,
                                                   int rank, int a0, float inverse_scale, bool spectral,
                                                   const float *syg) {
@@ -360,19 +362,20 @@ __device__ __forceinline__ double cl_precondition(cgx::cluster_group &cl, const 
   // DST along j times the inverse eigenvalues, pushed into every CTA's gc
   // (staged in the ap slab, free until the next operator apply)
   float *stage = sm + L.ap;
-  cl_dst_j(L, sm, nr, syg, [&](int ra, int l, float acc) { stage[ra * nj + l] = acc * ie[ra * nj + l]; });
+  cl_dst_j<SYG>(L, sm, nr, syg, [&](int ra, int l, float acc) { stage[ra * nj + l] = acc * ie[ra * nj + l]; });
   __syncthreads();
   cl_push_slab(cl, L, sm, L.ap, L.gc, a0, nr);
   cl.sync();  // gc complete in every CTA
   cl_dst_i(L, sm, sm + L.gc);
   __syncthreads();
   // DST along j divided by the scale: z
-  cl_dst_j(L, sm, nr, syg, [&](int ra, int l, float acc) { finish(ra, l, acc / inverse_scale); });
+  cl_dst_j<SYG>(L, sm, nr, syg, [&](int ra, int l, float acc) { finish(ra, l, acc / inverse_scale); });
   return rz;
 }
 
 // The solve of one member on the cluster of this block; sm is the dynamic
 // shared memory of the layout L.
+template <bool SYG>
 __device__ __forceinline__ void pcg_cluster_body(const Ctx &c, const ClusterLayout &L, float *sm, int with_rhs,
                                                  int with_post) {
   double *red = reinterpret_cast<double *>(sm + L.floats);
@@ -446,7 +449,7 @@ __device__ __forceinline__ void pcg_cluster_body(const Ctx &c, const ClusterLayo
       dst[32] = make_float4(__uint_as_float(lo[0]), __uint_as_float(lo[1]), __uint_as_float(lo[2]), __uint_as_float(lo[3]));
     }
     // Sy as split B fragments (kept in global memory with sy_global)
-    for (int f = threadIdx.x; !L.sy_global && f < L.nt * L.nt * 32; f += blockDim.x) {
+    for (int f = threadIdx.x; !SYG && f < L.nt * L.nt * 32; f += blockDim.x) {
       const int lane = f & 31, tile = f >> 5, kt = tile / L.nt, ct = tile - kt * L.nt, g = lane >> 2, t = lane & 3;
       const int col = 8 * ct + g, b0 = 8 * kt + t, b1 = b0 + 4;
       const float v0 = (b0 < nj && col < nj) ? sy[(size_t)b0 * nj + col] : 0.0f;
@@ -483,7 +486,7 @@ __device__ __forceinline__ void pcg_cluster_body(const Ctx &c, const ClusterLayo
   cl_push_partial(cl, rr, red, 3, nc, rank);
   cl.sync();  // r pushed everywhere; neighbours' x halo reads done
   const double rs0 = cl_partial_total(red, 3, nc);
-  double rz = cl_precondition(cl, L, sm, nr, rank, a0, c.k.inverse_scale, spectral, c.W[NPOM_W_sy]);
+  double rz = cl_precondition<SYG>(cl, L, sm, nr, rank, a0, c.k.inverse_scale, spectral, c.W[NPOM_W_sy]);
   cl_push_partial(cl, rz, red, 2, nc, rank);
   cl.sync();  // z halo rows and r.z partials in place
   double rho_old = cl_partial_total(red, 2, nc);
@@ -551,7 +554,7 @@ __device__ __forceinline__ void pcg_cluster_body(const Ctx &c, const ClusterLayo
       converged = true;
       break;
     }
-    rz = cl_precondition(cl, L, sm, nr, rank, a0, c.k.inverse_scale, spectral, c.W[NPOM_W_sy]);
+    rz = cl_precondition<SYG>(cl, L, sm, nr, rank, a0, c.k.inverse_scale, spectral, c.W[NPOM_W_sy]);
     cl_push_partial(cl, rz, red, 2, nc, rank);
     cl.sync();
     const double rho_new = cl_partial_total(red, 2, nc);
@@ -612,10 +615,12 @@ __device__ __forceinline__ void pcg_cluster_body(const Ctx &c, const ClusterLayo
   cl.sync();  // no CTA exits while others may still read its shared memory
 }
 
+// SYG: the layout reads Sy from global memory (L.sy_global)
+template <bool SYG>
 __global__ void __launch_bounds__(kClusterThreads, 1)
     k_pcg_cluster(Ctx c, ClusterLayout L, int with_rhs, int with_post) {
   extern __shared__ __align__(16) float sm[];
-  pcg_cluster_body(c, L, sm, with_rhs, with_post);
+  pcg_cluster_body<SYG>(c, L, sm, with_rhs, with_post);
 }
 
 }  // namespace npom
