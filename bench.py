@@ -109,6 +109,8 @@ def parse():
     ap.add_argument("--batch-chunk", type=int, default=24,
                     help="batch workload: turns per simulated day in which the groups (or members) enqueue "
                          "their steps")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the 64-member batch ('batch' key of the default workload)")
     ap.add_argument("--batch-mode", default="launch", choices=("launch", "streams"),
                     help="batch workload: 'launch' = one launch per phase over all members of a core "
                          "(npom_step_batch); 'streams' = every member its own core call on its own stream")
@@ -381,6 +383,10 @@ def run_b200(args):
         if fam is not None and not args.no_cpu_baseline:
             fam["reference_cpu"] = reference_fwd_adjoint_sample("cpu", internal_steps=3)
 
+    bat = None
+    if rank == 0 and ws_n == 1 and args.workload == "seamount" and not args.no_batch and not args.fa_only:
+        bat = batch_summary(args)
+
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws_n, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -391,7 +397,8 @@ def run_b200(args):
                    "pcg_iterations_last_step": (its[-1] if its else None) if W["core"] != "explicit" else None,
                    "members": ws_n, "parallelism": f"ensemble x{ws_n}" if ws_n > 1 else "single member",
                    "l2": "flushed (256 MiB write) before every timed step"},
-        "roofline": roofline, "cpu_baseline": cpu, "reference_gpu": ref_gpu, "ensemble": ens, "fwd_adjoint": fa, "fwd_adjoint_midtrain": fam, "e2e": e2e,
+        "roofline": roofline, "cpu_baseline": cpu, "reference_gpu": ref_gpu, "ensemble": ens, "fwd_adjoint": fa,
+        "fwd_adjoint_midtrain": fam, "batch": bat, "e2e": e2e,
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
@@ -947,6 +954,26 @@ def step_algorithmic_bytes(im, jm, kb, core_name):
 
 
 def run_batch(args):
+    print(json.dumps(batch_measure(args)), flush=True)
+
+
+def batch_summary(args):
+    """The 64-member batch (one timed simulated day of every member) as a
+    key of the default bench line."""
+    import copy
+    import torch
+    a = copy.copy(args)
+    a.steps, a.warmup, a.internal_steps, a.batch_mode = 1, 1, None, "launch"
+    out = batch_measure(a)
+    torch.cuda.empty_cache()
+    ref = out["reference_gpu_loop"]
+    return {"value": out["value"], "unit": out["unit"], "ms_per_step": out["ms_per_step"], "steps": 1,
+            "warmup": 1, "workload": out["config"]["workload"], "gpu_launches": out["gpu_launches"],
+            "hbm_frac": out["roofline"]["frac"], "reference_gpu_loop": ref["value"] if ref else None,
+            "clocks": out["clocks"]}
+
+
+def batch_measure(args):
     if args.batch_mode == "streams":
         # members run concurrently: the explicit subcycle runs on one cluster
         # per member (up to four cells per thread), never as a cooperative
@@ -1092,7 +1119,9 @@ def run_batch(args):
         "reference_gpu_loop": ref, "cpu_baseline": None, "e2e": None, "gpu_launches": launches,
         "clocks": clk.summary(),
     }
-    print(json.dumps(out), flush=True)
+    for mb in members:
+        mb["core"] = None
+    return out
 
 
 def main():
