@@ -366,7 +366,7 @@ def run_b200(args):
         cpu = reference_cpu_sample(A, Sc, internal_steps=args.ref_internal_steps, warm=1, reps=2,
                                    core_name=W["core"])
 
-    fa = fam = None
+    fa = fam = famb = None
     if rank == 0 and ws_n == 1 and args.workload == "coastal" and not args.no_fwd_adjoint:
         fa = coastal_fwd_adjoint(args, dev)
     if rank == 0 and ws_n == 1 and args.workload == "seamount" and not args.no_fwd_adjoint:
@@ -378,6 +378,7 @@ def run_b200(args):
             fa["reference_cpu"] = reference_fwd_adjoint_sample("cpu", internal_steps=3, case=case,
                                                                core_name=W["core"], seed=11)
         fam = None if args.fa_only else fwd_adjoint_sample(args, dev)
+        famb = None if args.fa_only else fwd_adjoint_midtrain_batch(args, dev)
         if fam is not None and not args.no_ref_gpu:
             fam["reference_gpu"] = reference_fwd_adjoint_sample(dev)
         if fam is not None and not args.no_cpu_baseline:
@@ -398,7 +399,7 @@ def run_b200(args):
                    "members": ws_n, "parallelism": f"ensemble x{ws_n}" if ws_n > 1 else "single member",
                    "l2": "flushed (256 MiB write) before every timed step"},
         "roofline": roofline, "cpu_baseline": cpu, "reference_gpu": ref_gpu, "ensemble": ens, "fwd_adjoint": fa,
-        "fwd_adjoint_midtrain": fam, "batch": bat, "e2e": e2e,
+        "fwd_adjoint_midtrain": fam, "fwd_adjoint_midtrain_batch": famb, "batch": bat, "e2e": e2e,
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
@@ -761,6 +762,91 @@ def fwd_adjoint_sample(args, dev, reps=3):
                         "internal step, hand-written CUDA step adjoint",
             "timing": f"median of {reps} samples, CUDA events around forward+backward (L2 not flushed: the "
                       "90x82x16 state fits in L2)"}
+
+
+def fwd_adjoint_midtrain_batch(args, dev, members=8, reps=3):
+    """BASELINE config 2 as stated: the Midtrain-shaped forward+adjoint for
+    a batch of ``members`` seeded members (``midtrain_case(m)``), each with
+    its own core, raw correction output and CUDA stream.  Every member's
+    three differentiable intervals are enqueued on its stream through
+    run_time_loop with ``status_deferred`` (no host synchronisation between
+    intervals); the loss is the sum of the members' MSE(u, v, T, S) and one
+    backward() reaches every member's state leaves and raw output.  Timed
+    with CUDA events on the launching stream around forward+backward; the
+    device status of every member is checked after each sample."""
+    import torch
+    from neuralpom_b200 import _abi, coupling, resolve_core_class
+    main = torch.cuda.current_stream(dev)
+    mem = []
+    for m in range(members):
+        A, Sc = midtrain_case(m)
+        core = resolve_core_class("explicit").from_state(A, Sc, device=dev)
+        core.status_deferred = True
+        tgt, _ = _fa_targets(A, 7 + m)
+        g = torch.Generator(device=dev).manual_seed(17 + m)
+        mem.append({"core": core, "t0": float(Sc["time"]), "stream": torch.cuda.Stream(dev),
+                    "tgt": {f: torch.from_numpy(v).to(dev) for f, v in tgt.items()},
+                    "start": {f: getattr(core, f).detach().clone() for f in _abi.FIELD_NAMES},
+                    "raw0": 1e-3 * torch.randn((coupling.OUTPUT_CHANNELS, core.im, core.jm), generator=g,
+                                               device=dev)})
+    scales = {f: 1.0 for f in coupling.OUTPUT_FIELDS}
+
+    def prepare():
+        for mb in mem:
+            c = mb["core"]
+            for f in _abi.FIELD_NAMES:
+                setattr(c, f, mb["start"][f].clone())
+            mb["leaves"] = [getattr(c, f).requires_grad_(True) for f in _abi.ADJ_STATE_FIELDS]
+            mb["raw"] = mb["raw0"].clone().requires_grad_()
+
+    def fwd_bwd():
+        go = torch.cuda.Event()
+        go.record(main)
+        losses = []
+        for mb in mem:
+            c, st = mb["core"], mb["stream"]
+            st.wait_event(go)
+            with torch.cuda.stream(st):
+                dti = float(c.dti)
+                for k in range(FA_INTERVALS):
+                    c.time0 = mb["t0"] + k * FA_STEPS_PER_INTERVAL * dti / 86400.0
+                    c.iend = FA_STEPS_PER_INTERVAL
+                    c.run_time_loop()
+                    if k < FA_INTERVALS - 1:
+                        coupling.apply_joint_correction(c, mb["raw"], scales)
+                losses.append(sum(((getattr(c, f) - mb["tgt"][f]) ** 2).mean() for f in mb["tgt"]))
+        for mb in mem:
+            main.wait_stream(mb["stream"])
+        for loss in losses:
+            loss.record_stream(main)
+        torch.stack(losses).sum().backward()
+
+    for _ in range(max(args.warmup, 1)):
+        prepare()
+        fwd_bwd()
+    torch.cuda.synchronize(dev)
+    ms = []
+    for _ in range(reps):
+        prepare()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(main)
+        fwd_bwd()
+        e1.record(main)
+        torch.cuda.synchronize(dev)
+        ms.append(e0.elapsed_time(e1))
+        for mb in mem:
+            mb["core"].check_deferred_status()
+            assert mb["raw"].grad is not None and all(t.grad is not None for t in mb["leaves"][:12])
+    best = statistics.median(ms)
+    nint = FA_INTERVALS * FA_STEPS_PER_INTERVAL
+    days = members * nint * float(mem[0]["core"].dti) / 86400.0
+    return {"value": days / (best / 1000.0), "unit": UNIT, "ms_per_sample": best, "members": members,
+            "workload": f"{members} seeded members of the Midtrain-shaped case (explicit core, "
+                        f"{FA_GRID[0]}x{FA_GRID[1]}x{FA_GRID[2]}, {FA_INTERVALS} x 1 h with apply_joint_correction "
+                        "between intervals), each on its own core and CUDA stream; sum of the members' "
+                        "MSE(u,v,T,S), one backward to every member's state and raw output",
+            "timing": f"median of {reps} samples, CUDA events around forward+backward of all members"}
 
 
 def reference_fwd_adjoint_sample(device, internal_steps=6, case=None, core_name="explicit", seed=7):

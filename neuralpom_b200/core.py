@@ -204,21 +204,35 @@ class B200Core:
         When grad mode is on and a state tensor requires grad, the advance
         is one differentiable node whose backward is the hand-written step
         adjoint; the state attributes are rebound to its outputs, as the
-        reference's autograd path rebinds them."""
+        reference's autograd path rebinds them.
+
+        With ``status_deferred`` set the call only enqueues: the device
+        status is not read back (no host synchronisation, so the members of
+        an ensemble on their own streams overlap) and accumulates until
+        ``check_deferred_status()``; no PCG iteration history is recorded."""
         nsteps = int(self.iend)
         if nsteps < 0:
             raise ValueError("iend must be non-negative")
+        deferred = getattr(self, "status_deferred", False)
         if self._differentiable_call():
             outs = _StepsFunction.apply(self, nsteps, float(self.time0),
                                         *[getattr(self, f) for f in _abi.ADJ_STATE_FIELDS])
             for f, o in zip(_abi.ADJ_STATE_FIELDS, outs):
                 setattr(self, f, o)
-            bits, its = self.read_status(nsteps)
         else:
             with torch.no_grad():
                 self.launch_steps(nsteps, float(self.time0))
-            bits, its = self.read_status(nsteps)
+        bits, its = (0, []) if deferred else self.read_status(nsteps)
         self._finish_advance(nsteps, bits, its)
+
+    def check_deferred_status(self):
+        """Reads and clears the status accumulated by the advances made with
+        ``status_deferred`` set (after the work of every stream on the
+        device); raises for it like ``run_time_loop``."""
+        if self.device.type == "cuda":
+            torch.cuda.synchronize(self.device)
+        bits, _ = self.read_status(0)
+        self._raise_for(bits)
 
     def _finish_advance(self, nsteps, bits, its):
         """Clock, ramp and PCG history after ``nsteps`` steps from time0;
@@ -226,7 +240,7 @@ class B200Core:
         self.iint = nsteps
         self.time = self.dti * nsteps * 1.0 / 86400.0 + self.time0
         if self.lramp:
-            r = float(np.float32(self.time) / np.float32(float(self.period)))
+            r = float(np.float32(self.time) / np.float32(state.host_scalar(self.period)))
             self.ramp = 1.0 if r > 1.0 else r
         else:
             self.ramp = 1.0
@@ -303,9 +317,16 @@ class _StepsFunction(torch.autograd.Function):
             dyn.views[n].copy_(t.detach().reshape(dyn.views[n].shape))
             setattr(core, n, dyn.views[n])
         ckpt = torch.empty((max(nsteps, 1), dyn.flat.numel()), dtype=torch.float32, device=dev)
+        # the call's structs once: the fields live in dyn for the whole call
+        lib = _abi.load_library()
+        p, fa, ws = core.params(), core._fields(), core._workspace()
+        fn = lib.npom_step_explicit if core.core_name == "explicit" else lib.npom_step_implicit
+        st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
         for n in range(nsteps):
             ckpt[n].copy_(dyn.flat)
-            core.launch_steps(1, time0, first_iint=n + 1)
+            clk = _abi.NpomClock(float(time0), n + 1, 1)
+            _abi.check(fn(ctypes.byref(p), ctypes.byref(fa), ctypes.byref(ws["struct"]), ctypes.byref(clk), st),
+                       "npom step")
         ctx.core, ctx.nsteps, ctx.time0 = core, nsteps, time0
         ctx.save_for_backward(ckpt)
         outs = tuple(dyn.views[n].clone() for n in _abi.ADJ_STATE_FIELDS)

@@ -349,6 +349,13 @@ npom_status launch_adj_phase(const npom_params *p, const npom_workspace *ws, con
   return NPOM_OK;
 }
 
+npom_status enqueue_step_adjoint(const npom_params *p, const npom_workspace *ws, const Ctx &c, const Adj &a,
+                                 const AdjPhaseRec *plan, int np, const ImpScratch &is, float *scratch,
+                                 float *save, int core, cudaStream_t s);
+npom_status step_adjoint_graph(const npom_params *p, const npom_workspace *ws, const Ctx &c, const Adj &a,
+                               const AdjPhaseRec *plan, int np, const ImpScratch &is, float *scratch, float *save,
+                               cudaStream_t s, bool *launched);
+
 npom_status run_step_adjoint(const npom_params *p, float *const *fields, const npom_workspace *ws,
                              const npom_clock *clk, float *const *grads, const npom_adjoint_ws *aws, int core,
                              cudaStream_t s) {
@@ -382,6 +389,20 @@ npom_status run_step_adjoint(const npom_params *p, float *const *fields, const n
   is.g = is.xs + ncell;
   is.lam = is.g + ncell;
   is.gd = is.lam + ncell;
+  if (core == NPOM_CORE_EXPLICIT && graphs_enabled()) {
+    bool done = false;
+    const npom_status st = step_adjoint_graph(p, ws, c, a, plan.data(), np, is, scratch, aws->save, s, &done);
+    if (st != NPOM_OK || done) return st;
+  }
+  return enqueue_step_adjoint(p, ws, c, a, plan.data(), np, is, scratch, aws->save, core, s);
+}
+
+// The launches of one step adjoint (recompute with saves, then the reverse
+// walk) on s.
+npom_status enqueue_step_adjoint(const npom_params *p, const npom_workspace *ws, const Ctx &c, const Adj &a,
+                                 const AdjPhaseRec *plan, int np, const ImpScratch &is, float *scratch,
+                                 float *save, int core, cudaStream_t s) {
+  const size_t ncell = (size_t)c.im * c.jm;
   // workspace cotangents live inside one step
   if (cudaMemsetAsync(scratch, 0, (size_t)AW_COUNT * ncell * sizeof(float), s) != cudaSuccess) return NPOM_ERR_CUDA;
   PcgPlan pplan{};
@@ -403,8 +424,9 @@ npom_status run_step_adjoint(const npom_params *p, float *const *fields, const n
   const int ext_ctas = ext_shape < 0 ? cluster_ctas(ext_shape) : 0;
   Ctx cc = c;
   cc.coh = 1;
-  float *ext_save = e0 < e1 ? aws->save + plan[e0].off[0] : nullptr;
-  const float *ext_end = e0 < e1 ? aws->save + plan[e1 - 1].off[plan[e1 - 1].n - 1] +
+  Adj aa = a;
+  float *ext_save = e0 < e1 ? save + plan[e0].off[0] : nullptr;
+  const float *ext_end = e0 < e1 ? save + plan[e1 - 1].off[plan[e1 - 1].n - 1] +
                                        adj_field_len(c, plan[e1 - 1].fld[plan[e1 - 1].n - 1])
                                  : nullptr;
   for (int q = 0; q < np; ++q) {
@@ -418,13 +440,13 @@ npom_status run_step_adjoint(const npom_params *p, float *const *fields, const n
       }
       continue;
     }
-    k_save_fields<<<field_list_grid(c, plan[q]), kThreads, 0, s>>>(c, plan[q], aws->save);
+    k_save_fields<<<field_list_grid(c, plan[q]), kThreads, 0, s>>>(c, plan[q], save);
     launch_fwd_phase(c, plan[q], pplan, is, s);
   }
   for (int q = np - 1; q >= 0; --q) {
     if (ext_fused && q >= e0 && q < e1) {
       if (q == e0) {
-        void *args[] = {&cc, &a, &ext_end};
+        void *args[] = {&cc, &aa, &ext_end};
         const cudaError_t e = ext_shape < 0
                                   ? launch_cluster(kAdjExtReverse[ext_t], ext_ctas, ext_threads, args, s)
                                   : launch_coop(kAdjExtReverseGrid, ext_shape, args, c.sync, s);
@@ -432,11 +454,83 @@ npom_status run_step_adjoint(const npom_params *p, float *const *fields, const n
       }
       continue;
     }
-    k_restore_move<<<field_list_grid(c, plan[q]), kThreads, 0, s>>>(c, a, plan[q], aws->save);
+    k_restore_move<<<field_list_grid(c, plan[q]), kThreads, 0, s>>>(c, a, plan[q], save);
     const npom_status st = launch_adj_phase(p, ws, c, a, plan[q], is, s);
     if (st != NPOM_OK) return st;
   }
   return cudaGetLastError() == cudaSuccess ? NPOM_OK : NPOM_ERR_CUDA;
+}
+
+// CUDA graphs of the explicit step adjoint: the launch sequence is fixed
+// by the context (pointers, constants, ramp, do_internal), the cotangent
+// and lambda pointers and the save buffer, so the steps of a backward pass
+// (and, as the allocator hands back the same buffers, the next passes)
+// replay one graph instead of enqueueing several hundred kernels from the
+// host.  The semi-implicit adjoint is not captured: its free-surface solve
+// reads a scale back to the host in the middle of the step.
+struct AdjGraphKey {
+  Ctx c;
+  Adj a;
+  float *save;
+};
+
+struct AdjGraphEntry {
+  int device;
+  AdjGraphKey key;
+  cudaGraphExec_t exec;
+};
+
+std::mutex g_adj_graph_mutex;
+std::vector<AdjGraphEntry> g_adj_graphs;
+bool g_adj_capture_failed[64] = {};
+constexpr size_t kAdjGraphCache = 64;
+
+npom_status step_adjoint_graph(const npom_params *p, const npom_workspace *ws, const Ctx &c, const Adj &a,
+                               const AdjPhaseRec *plan, int np, const ImpScratch &is, float *scratch, float *save,
+                               cudaStream_t s, bool *launched) {
+  *launched = false;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return NPOM_OK;
+  AdjGraphKey key;
+  std::memset(&key, 0, sizeof(key));
+  key.c = c;
+  key.a = a;
+  key.save = save;
+  std::lock_guard<std::mutex> lock(g_adj_graph_mutex);
+  for (auto &g : g_adj_graphs) {
+    if (g.device == dev && std::memcmp(&g.key, &key, sizeof(key)) == 0) {
+      if (cudaGraphLaunch(g.exec, s) != cudaSuccess) return NPOM_ERR_CUDA;
+      *launched = true;
+      return NPOM_OK;
+    }
+  }
+  if (g_adj_capture_failed[dev]) return NPOM_OK;
+  std::lock_guard<std::mutex> glock(g_graph_mutex);  // the capture stream is shared
+  if (!g_capture_stream[dev] && cudaStreamCreateWithFlags(&g_capture_stream[dev], cudaStreamNonBlocking) != cudaSuccess)
+    return NPOM_ERR_CUDA;
+  cudaStream_t cs = g_capture_stream[dev];
+  if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return NPOM_ERR_CUDA;
+  const npom_status le = enqueue_step_adjoint(p, ws, c, a, plan, np, is, scratch, save, NPOM_CORE_EXPLICIT, cs);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(cs, &graph);
+  cudaGraphExec_t exec = nullptr;
+  if (le != NPOM_OK || e != cudaSuccess || !graph || cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    g_adj_capture_failed[dev] = true;
+    return NPOM_OK;  // not captured: the caller launches directly
+  }
+  cudaGraphDestroy(graph);
+  if (g_adj_graphs.size() >= kAdjGraphCache) {
+    // a replaced graph may still be in flight on some stream
+    if (cudaDeviceSynchronize() != cudaSuccess) return NPOM_ERR_CUDA;
+    cudaGraphExecDestroy(g_adj_graphs.front().exec);
+    g_adj_graphs.erase(g_adj_graphs.begin());
+  }
+  g_adj_graphs.push_back(AdjGraphEntry{dev, key, exec});
+  if (cudaGraphLaunch(exec, s) != cudaSuccess) return NPOM_ERR_CUDA;
+  *launched = true;
+  return NPOM_OK;
 }
 
 // ---------------------------------------------------------------------------

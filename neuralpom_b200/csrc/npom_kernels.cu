@@ -1099,7 +1099,6 @@ cudaError_t enqueue_step(const Ctx &c, int core, const PcgPlan &plan, int sub_bl
   return cudaGetLastError();
 }
 
-#include "npom_adjoint_launch.cuh"
 
 // CUDA graphs of one internal step, keyed by the launch context (pointers,
 // settings, ramp, do_internal) and device.  Steps with ramp < 1 (the first
@@ -1208,6 +1207,7 @@ npom_status run_steps(const npom_params *p, float *const *fields, const npom_wor
   return cudaGetLastError() == cudaSuccess ? NPOM_OK : NPOM_ERR_CUDA;
 }
 
+#include "npom_adjoint_launch.cuh"
 #include "npom_batch.cuh"
 
 const char *kFieldNames[] = {

@@ -53,6 +53,25 @@ def default_scalars(core):
     return derived_time(s)
 
 
+def host_scalar(v):
+    """float of a Python number or a one-element tensor.  A device tensor
+    (the reference keeps ``period`` as one) is read back once and the value
+    kept on the tensor with its version counter, so later reads (the step's
+    host bookkeeping) do not wait for the work queued on the device; an
+    in-place write to the tensor bumps the version and forces a new read."""
+    if not hasattr(v, "detach"):
+        return float(np.asarray(v, dtype=np.float64).reshape(-1)[0])
+    hit = getattr(v, "_npom_host_value", None)
+    if hit is not None and hit[0] == v._version:
+        return hit[1]
+    val = float(v.detach().reshape(-1)[0].cpu().item())
+    try:
+        v._npom_host_value = (v._version, val)
+    except (AttributeError, RuntimeError):
+        pass
+    return val
+
+
 def make_params(s, im, jm, kb, core, device=0):
     """npom_params from a mapping (or object) of the reference scalars."""
     get = (lambda k, d=None: s.get(k, d)) if isinstance(s, dict) else (lambda k, d=None: getattr(s, k, d))
@@ -93,10 +112,7 @@ def make_params(s, im, jm, kb, core, device=0):
         raise ValueError("a non-zero internal-velocity Shapiro filter is not implemented (production uses 0)")
     tau0 = get("double_gyre_wind_stress_pa", None)
     p.wind_tau0 = 0.1 if tau0 is None else float(tau0)
-    period = get("period", 1.0)
-    if hasattr(period, "detach"):
-        period = period.detach().reshape(-1)[0].cpu().item()
-    p.period = float(np.asarray(period, dtype=np.float64).reshape(-1)[0])
+    p.period = host_scalar(get("period", 1.0))
     p.inverse_scale = 4.0 * (im - 1) * (jm - 1)
     return p
 

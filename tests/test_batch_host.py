@@ -28,3 +28,16 @@ def test_run_batch_requires_one_clock():
     b = types.SimpleNamespace(iend=4, time0=0.0)
     with pytest.raises(ValueError, match="one clock"):
         batch.run_batch([a, b])
+
+
+def test_host_scalar_reads_a_tensor_once_per_version():
+    """The ramp period is a tensor in the reference's state; its host value
+    is read once and re-read after an in-place write."""
+    import torch
+    from neuralpom_b200 import state
+    t = torch.full((), 3.0)
+    assert state.host_scalar(t) == 3.0
+    assert state.host_scalar(t) == 3.0
+    t.fill_(5.0)
+    assert state.host_scalar(t) == 5.0
+    assert state.host_scalar(2.5) == 2.5

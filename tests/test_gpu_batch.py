@@ -111,3 +111,52 @@ def test_batch_ensemble_of_equal_grids_is_bitwise():
         assert sb[0] == 0
         for n in a:
             assert np.array_equal(a[n], b[n], equal_nan=True), (m, n)
+
+
+def test_deferred_status_members_on_streams_match_sequential():
+    """Differentiable advances of two members with ``status_deferred``, each
+    on its own CUDA stream with no host synchronisation between intervals,
+    give bitwise the outputs of the same members advanced one after the
+    other with the status read after every call, and their gradients to
+    1e-5 (the step adjoint scatters with atomic adds, whose order, and so
+    the last bits, vary from run to run)."""
+    from neuralpom_b200 import _abi, cases, resolve_core_class
+    members = [cases.noise_basin(37, 45, seed=s) for s in (3, 4)]
+
+    def run(deferred):
+        main = torch.cuda.current_stream()
+        streams = [torch.cuda.Stream() for _ in members]
+        cores, leaves, losses = [], [], []
+        for (A, Sc), st in zip(members, streams):
+            c = resolve_core_class("explicit").from_state(A, dict(Sc, time=0.25, time0=0.25), device="cuda")
+            c.status_deferred = deferred
+            lv = [getattr(c, f).requires_grad_(True) for f in ("t", "u", "el")]
+            go = torch.cuda.Event()
+            go.record(main)
+            st.wait_event(go)
+            with torch.cuda.stream(st if deferred else main):
+                for k in range(2):
+                    c.time0, c.iend = 0.25 + k * 3 * float(c.dti) / 86400.0, 3
+                    c.run_time_loop()
+                loss = (c.t ** 2).mean() + (c.u ** 2).mean()
+            main.wait_stream(st)
+            loss.record_stream(main)
+            cores.append(c)
+            leaves.append(lv)
+            losses.append(loss)
+        torch.stack(losses).sum().backward()
+        torch.cuda.synchronize()
+        for c in cores:
+            if deferred:
+                c.check_deferred_status()
+        return ([{f: getattr(c, f).detach().cpu().numpy() for f in ("t", "u", "el", "q2")} for c in cores],
+                [[t.grad.cpu().numpy() for t in lv] for lv in leaves])
+
+    outs0, grads0 = run(False)
+    outs1, grads1 = run(True)
+    for a, b in zip(outs0, outs1):
+        for f in a:
+            assert np.array_equal(a[f], b[f]), f
+    for ga, gb in zip(grads0, grads1):
+        for x, y in zip(ga, gb):
+            assert np.abs(x).max() > 0 and rel_err(y, x) <= 1e-5, rel_err(y, x)
