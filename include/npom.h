@@ -220,8 +220,9 @@ npom_status npom_pcg_solve(const npom_params *p, float *const *fields,
  *              zero guess (ws->cg_iters[0] receives the iterations);
  *   grad_d   = dJ/dd, the transposed depth stencil of the operator at the
  *              forward solution x.
- * d2d is the depth the forward solve used.  The scale is read back to the
- * host once (one stream synchronisation), so the call is not capturable.
+ * d2d is the depth the forward solve used.  The rhs scale stays on the
+ * device; the call synchronises its stream once, to check the cotangent
+ * before the solve, so it is not capturable.
  * Replaces cores/implicit_p0_fixed/core.py:24 _ImplicitEtaSolveFunction
  * (backward :46-59, _solve_implicit_eta_adjoint :231-252,
  * _apply_elliptic_operator_depth_adjoint :645-675).  A non-finite
@@ -299,8 +300,10 @@ npom_status npom_step_explicit_adjoint(const npom_params *p, float *const *field
  * 38-688 under torch autograd; the free-surface solve differentiates as
  * _ImplicitEtaSolveFunction, core.py:24-59).  Supported settings: mode 3,
  * nadv 1, nbct/nbcs 1 or 3, zero barotropic and tracer Shapiro filters.
- * Returns NPOM_ERR_DEVICE when the solve's cotangent is not finite; one
- * host synchronisation per call (the adjoint solve's scale). */
+ * No host synchronisation: the solve's rhs scale stays on the device, and
+ * a non-finite cotangent propagates into the gradients as it does under
+ * the reference's autograd.  Both step adjoints are replayed from a cached
+ * CUDA graph per (pointers, constants, ramp) after their first call. */
 npom_status npom_step_implicit_adjoint(const npom_params *p, float *const *fields,
                                        const npom_workspace *ws,
                                        const npom_clock *clk, float *const *grads,

@@ -322,9 +322,12 @@ npom_status launch_adj_phase(const npom_params *p, const npom_workspace *ws, con
     case AP_EI: {
       // elf/d of the post step -> g = dJ/dx; the solve's adjoint gives
       // lambda = A^-T g and dJ/dd; then the rhs and the transports
+      // (no host read-back: a non-finite cotangent propagates into the
+      // gradients, as under the reference's autograd)
       k_imp_post_grad<<<gx, kThreads, 0, s>>>(c, a, is.g);
-      const npom_status st = npom_pcg_adjoint(p, c.F, ws, is.g, is.xs, c.F[NPOM_F_d], is.lam, is.gd, (void *)s);
-      if (st != NPOM_OK) return st;
+      if (enqueue_adj_prep(c, ws, is.g, 0, s) != cudaSuccess ||
+          enqueue_adj_solve(c, ws, is.xs, is.lam, is.gd, s) != cudaSuccess)
+        return NPOM_ERR_CUDA;
       k_imp_rhs_adj<<<gx, kThreads, 0, s>>>(c, a, is.lam, is.gd);
       break;
     }
@@ -389,7 +392,7 @@ npom_status run_step_adjoint(const npom_params *p, float *const *fields, const n
   is.g = is.xs + ncell;
   is.lam = is.g + ncell;
   is.gd = is.lam + ncell;
-  if (core == NPOM_CORE_EXPLICIT && graphs_enabled()) {
+  if (graphs_enabled()) {
     bool done = false;
     const npom_status st = step_adjoint_graph(p, ws, c, a, plan.data(), np, is, scratch, aws->save, s, &done);
     if (st != NPOM_OK || done) return st;
@@ -466,8 +469,8 @@ npom_status enqueue_step_adjoint(const npom_params *p, const npom_workspace *ws,
 // and lambda pointers and the save buffer, so the steps of a backward pass
 // (and, as the allocator hands back the same buffers, the next passes)
 // replay one graph instead of enqueueing several hundred kernels from the
-// host.  The semi-implicit adjoint is not captured: its free-surface solve
-// reads a scale back to the host in the middle of the step.
+// host.  Both cores: the adjoint of the free-surface solve keeps its rhs
+// scale on the device.
 struct AdjGraphKey {
   Ctx c;
   Adj a;
@@ -510,7 +513,7 @@ npom_status step_adjoint_graph(const npom_params *p, const npom_workspace *ws, c
     return NPOM_ERR_CUDA;
   cudaStream_t cs = g_capture_stream[dev];
   if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return NPOM_ERR_CUDA;
-  const npom_status le = enqueue_step_adjoint(p, ws, c, a, plan, np, is, scratch, save, NPOM_CORE_EXPLICIT, cs);
+  const npom_status le = enqueue_step_adjoint(p, ws, c, a, plan, np, is, scratch, save, p->core, cs);
   cudaGraph_t graph = nullptr;
   const cudaError_t e = cudaStreamEndCapture(cs, &graph);
   cudaGraphExec_t exec = nullptr;

@@ -62,6 +62,10 @@ struct Ctx {
   // [grid_base, grid_base + grid_blocks) (grid_blocks 0: the whole grid);
   // several members share one launch, each with its own grid barrier
   int grid_base, grid_blocks;
+  // when set: the PCG's absolute tolerance is eta_tol / max(f, 1) with f
+  // the float whose bits are stored here (the adjoint solve's rhs scale,
+  // kept on the device)
+  const unsigned int *tol_scale_bits;
   float ramp;      // per step
   int do_internal; // per step: 0 on the first step from time0 == 0
 };

@@ -524,7 +524,7 @@ __device__ __forceinline__ void pcg_coop_body(const Ctx &c, int with_rhs, int wi
     size_t o = NPOM_I2(c, (int)(q / nj) + 1, (int)(q % nj) + 1);
     p[o] = __ldcg(zv + o);
   }
-  const double tol_sq = c.k.eta_tol * c.k.eta_tol;
+  const double tol = pcg_abs_tol(c), tol_sq = tol * tol;
   const double rel_sq = c.k.eta_rel_tol * c.k.eta_rel_tol * (rs0 > 1e-30 ? rs0 : 1e-30);
   int its = 0;
   bool converged = false;
@@ -1207,6 +1207,10 @@ npom_status run_steps(const npom_params *p, float *const *fields, const npom_wor
   return cudaGetLastError() == cudaSuccess ? NPOM_OK : NPOM_ERR_CUDA;
 }
 
+cudaError_t enqueue_adj_prep(const Ctx &c, const npom_workspace *ws, const float *grad_x, int flag, cudaStream_t s);
+cudaError_t enqueue_adj_solve(const Ctx &c, const npom_workspace *ws, const float *x, float *grad_rhs, float *grad_d,
+                              cudaStream_t s);
+
 #include "npom_adjoint_launch.cuh"
 #include "npom_batch.cuh"
 
@@ -1233,7 +1237,8 @@ constexpr int kNumPhases = (int)(sizeof(kPhaseNames) / sizeof(kPhaseNames[0]));
 
 // rhs = g / area into the rhs workspace; max |rhs| as float bits (a
 // non-negative float orders like its bit pattern, NaN above infinity)
-__global__ void k_adj_prep(Ctx c, const float *g, unsigned int *maxbits) {
+// (flag: non-finite values set NPOM_DEV_NONFINITE in the status word)
+__global__ void k_adj_prep(Ctx c, const float *g, unsigned int *maxbits, int flag) {
   const size_t n = (size_t)c.im * c.jm;
   unsigned int m = 0u;
   for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
@@ -1241,16 +1246,18 @@ __global__ void k_adj_prep(Ctx c, const float *g, unsigned int *maxbits) {
     const float v = g[o] / adj_area(c, i, j);
     c.W[NPOM_W_rhs][o] = v;
     const float a = fabsf(v);
-    if (!(a <= 3.4028235e38f)) atomicOr(c.status, NPOM_DEV_NONFINITE);
+    if (flag && !(a <= 3.4028235e38f)) atomicOr(c.status, NPOM_DEV_NONFINITE);
     m = max(m, __float_as_uint(a));
   }
   m = __reduce_max_sync(0xffffffffu, m);
   if ((threadIdx.x & 31) == 0) atomicMax(maxbits, m);
 }
 
-// normalised rhs (rhs / scale) and a zero initial guess
-__global__ void k_adj_scale(Ctx c, float scale, float *x) {
+// normalised rhs (rhs / scale) and a zero initial guess; the scale from
+// the bits k_adj_prep stored
+__global__ void k_adj_scale(Ctx c, const unsigned int *scale_bits, float *x) {
   const size_t n = (size_t)c.im * c.jm;
+  const float scale = adj_scale_of(scale_bits);
   for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
     c.W[NPOM_W_rhs][o] = c.W[NPOM_W_rhs][o] / scale;
     x[o] = 0.0f;
@@ -1259,8 +1266,10 @@ __global__ void k_adj_scale(Ctx c, float scale, float *x) {
 
 // grad_d = -(depth adjoint), gathered per cell in the reference's order
 // (adj_grad_d_cell)
-__global__ void k_adj_grad_d(Ctx c, const float *x, const float *sol, float scale, float *grad_d) {
+__global__ void k_adj_grad_d(Ctx c, const float *x, const float *sol, const unsigned int *scale_bits,
+                             float *grad_d) {
   const size_t n = (size_t)c.im * c.jm;
+  const float scale = adj_scale_of(scale_bits);
   for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
     const int i = (int)(o / c.jm), j = (int)(o - (size_t)i * c.jm);
     grad_d[o] = adj_grad_d_cell(c, x, sol, scale, i, j);
@@ -1268,12 +1277,47 @@ __global__ void k_adj_grad_d(Ctx c, const float *x, const float *sol, float scal
 }
 
 // lambda = solution * area * scale, in place
-__global__ void k_adj_lambda(Ctx c, float scale, float *sol) {
+__global__ void k_adj_lambda(Ctx c, const unsigned int *scale_bits, float *sol) {
   const size_t n = (size_t)c.im * c.jm;
+  const float scale = adj_scale_of(scale_bits);
   for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
     const int i = (int)(o / c.jm), j = (int)(o - (size_t)i * c.jm);
     sol[o] = (sol[o] * adj_area(c, i, j)) * scale;
   }
+}
+
+// The adjoint solve on s: rhs = g / area and its scale (prep), then
+// rhs / scale, the coefficients, the PCG from a zero guess with the
+// scaled absolute tolerance, grad_d and lambda.  The scale stays on the
+// device (ws->sync[3]: the float bits of max |g / area|), so nothing is
+// read back to the host.
+cudaError_t enqueue_adj_prep(const Ctx &c, const npom_workspace *ws, const float *grad_x, int flag, cudaStream_t s) {
+  const size_t n = (size_t)c.im * c.jm;
+  const int blocks = std::max(1, std::min(blocks_for(n, kThreads), 1024));
+  cudaError_t e = cudaMemsetAsync(ws->sync, 0, 4 * sizeof(unsigned int), s);
+  if (e != cudaSuccess) return e;
+  k_adj_prep<<<blocks, kThreads, 0, s>>>(c, grad_x, ws->sync + 3, flag);
+  return cudaGetLastError();
+}
+
+cudaError_t enqueue_adj_solve(const Ctx &c, const npom_workspace *ws, const float *x, float *grad_rhs, float *grad_d,
+                              cudaStream_t s) {
+  const size_t n = (size_t)c.im * c.jm;
+  const int blocks = std::max(1, std::min(blocks_for(n, kThreads), 1024));
+  const unsigned int *bits = ws->sync + 3;
+  k_adj_scale<<<blocks, kThreads, 0, s>>>(c, bits, grad_rhs);
+  launch_cells<XP_COEF>(c, s);
+  Ctx ca = c;
+  ca.F[NPOM_F_elf] = grad_rhs;  // zero guess in, A^-1 (g/area/scale) out
+  ca.tol_scale_bits = bits;     // the forward's stopping test on the scaled system
+  PcgPlan plan{};
+  cudaError_t e = plan_pcg(ca, &plan);
+  if (e != cudaSuccess) return e;
+  e = run_pcg(ca, plan, 0, 0, s);
+  if (e != cudaSuccess) return e;
+  k_adj_grad_d<<<blocks, kThreads, 0, s>>>(c, x, grad_rhs, bits, grad_d);
+  k_adj_lambda<<<blocks, kThreads, 0, s>>>(c, bits, grad_rhs);
+  return cudaGetLastError();
 }
 
 }  // namespace
@@ -1514,30 +1558,15 @@ npom_status npom_pcg_adjoint(const npom_params *p, float *const *fields, const n
   cudaStream_t s = (cudaStream_t)stream;
   Ctx c = make_ctx(p, fields, ws);
   c.F[NPOM_F_d] = const_cast<float *>(d2d);
-  const size_t n = (size_t)c.im * c.jm;
-  const int blocks = std::max(1, std::min(blocks_for(n, kThreads), 1024));
-  if (cudaMemsetAsync(ws->sync, 0, 4 * sizeof(unsigned int), s) != cudaSuccess) return NPOM_ERR_CUDA;
-  k_adj_prep<<<blocks, kThreads, 0, s>>>(c, grad_x, ws->sync + 3);
-  unsigned int bits = 0u, status = 0u;
-  if (cudaMemcpyAsync(&bits, ws->sync + 3, sizeof(bits), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-      cudaMemcpyAsync(&status, ws->status, sizeof(status), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+  if (enqueue_adj_prep(c, ws, grad_x, 1, s) != cudaSuccess) return NPOM_ERR_CUDA;
+  // a non-finite cotangent is reported before any solve (one host sync)
+  unsigned int status = 0u;
+  if (cudaMemcpyAsync(&status, ws->status, sizeof(status), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess)
     return NPOM_ERR_CUDA;
   if (status & NPOM_DEV_NONFINITE) return NPOM_ERR_DEVICE;
-  float amax = 0.0f;
-  std::memcpy(&amax, &bits, sizeof(amax));
-  const float scale = amax > 1.0f ? amax : 1.0f;  // clamp_min(1)
-  k_adj_scale<<<blocks, kThreads, 0, s>>>(c, scale, grad_rhs);
-  launch_cells<XP_COEF>(c, s);
-  Ctx ca = c;
-  ca.F[NPOM_F_elf] = grad_rhs;               // zero guess in, A^-1 (g/area/scale) out
-  ca.k.eta_tol = p->eta_tol / (double)scale;  // same stopping test as the forward
-  PcgPlan plan{};
-  if (plan_pcg(ca, &plan) != cudaSuccess) return NPOM_ERR_CUDA;
-  if (run_pcg(ca, plan, 0, 0, s) != cudaSuccess) return NPOM_ERR_CUDA;
-  k_adj_grad_d<<<blocks, kThreads, 0, s>>>(c, x, grad_rhs, scale, grad_d);
-  k_adj_lambda<<<blocks, kThreads, 0, s>>>(c, scale, grad_rhs);
-  return cudaGetLastError() == cudaSuccess ? NPOM_OK : NPOM_ERR_CUDA;
+  if (enqueue_adj_solve(c, ws, x, grad_rhs, grad_d, s) != cudaSuccess) return NPOM_ERR_CUDA;
+  return NPOM_OK;
 }
 
 npom_status npom_pcg_solve_static(const npom_params *p, float *const *fields, const float *rhs, const float *sx,

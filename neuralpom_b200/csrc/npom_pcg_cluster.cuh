@@ -373,6 +373,16 @@ __device__ __forceinline__ double cl_precondition(cgx::cluster_group &cl, const 
   return rz;
 }
 
+// The rhs scale of the adjoint solve from its float bits (clamp_min(1); a
+// NaN gives 1, as on the host), and the PCG's absolute tolerance.
+__device__ __forceinline__ float adj_scale_of(const unsigned int *bits) {
+  const float a = __uint_as_float(*bits);
+  return a > 1.0f ? a : 1.0f;
+}
+__device__ __forceinline__ double pcg_abs_tol(const Ctx &c) {
+  return c.tol_scale_bits ? c.k.eta_tol / (double)adj_scale_of(c.tol_scale_bits) : c.k.eta_tol;
+}
+
 // The solve of one member on the cluster of this block; sm is the dynamic
 // shared memory of the layout L.
 template <bool SYG>
@@ -496,7 +506,7 @@ __device__ __forceinline__ void pcg_cluster_body(const Ctx &c, const ClusterLayo
     p[b] = has_up ? sm[L.zh + b] : 0.0f;
     p[(nr + 1) * nj + b] = has_down ? sm[L.zh + nj + b] : 0.0f;
   }
-  const double tol_sq = c.k.eta_tol * c.k.eta_tol;
+  const double tol = pcg_abs_tol(c), tol_sq = tol * tol;
   const double rel_sq = c.k.eta_rel_tol * c.k.eta_rel_tol * (rs0 > 1e-30 ? rs0 : 1e-30);
   int its = 0;
   bool converged = false;
