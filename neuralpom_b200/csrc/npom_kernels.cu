@@ -297,19 +297,34 @@ __device__ __forceinline__ unsigned vblock(const Ctx &c) { return blockIdx.x - (
 // and no reset inside the kernel keep each barrier at two serial L2 round
 // trips.  Returns false after a timeout (or once any block has timed out);
 // the caller then returns.
+//
+// Ordering: the block barrier orders every thread's writes before thread
+// 0's arrival, a release at GPU scope; thread 0 polls with acquire loads,
+// and the closing block barrier orders the acquire before every thread's
+// later reads (which in the cooperative kernels go through L2).  The
+// release/acquire pair replaces two full fences.
+__device__ __forceinline__ unsigned int atom_add_release_gpu(unsigned int *p, unsigned int v) {
+  unsigned int old;
+  asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int *p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
 __device__ bool grid_barrier(const Ctx &c) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     ok = 1;
-    __threadfence();
-    const unsigned int arrived = atomicAdd(c.sync, 1u);
+    const unsigned int arrived = atom_add_release_gpu(c.sync, 1u);
     const unsigned int G = vgrid(c);
     const unsigned int target = (arrived / G + 1u) * G;
-    volatile unsigned int *count = c.sync;
     unsigned long long t0 = globaltimer_ns();
     unsigned int spins = 0;
-    while ((int)(*count - target) < 0) {
+    while ((int)(ld_acquire_gpu(c.sync) - target) < 0) {
       if ((++spins & 63u) == 0) {
         if (*(volatile unsigned int *)c.status & NPOM_DEV_TIMEOUT) {
           ok = 0;
@@ -322,7 +337,6 @@ __device__ bool grid_barrier(const Ctx &c) {
         }
       }
     }
-    __threadfence();
   }
   __syncthreads();
   return ok != 0;
