@@ -276,6 +276,12 @@ typedef struct npom_adjoint_ws {
   float *lam[NPOM_NFIELDS];  /* one array per field, sized like it      */
   float *save;               /* >= npom_adjoint_save_floats(p) floats   */
   size_t save_floats;        /* capacity of save                        */
+  const float *pcg_x;        /* semi-implicit core, may be NULL: the raw */
+                             /* solution of this step's free-surface    */
+                             /* solve (the workspace plane "x" after     */
+                             /* the forward npom_step_implicit call of   */
+                             /* the step), so the recomputation replays  */
+                             /* it instead of solving again             */
 } npom_adjoint_ws;
 
 /* Size of the per-step save area (floats) for these settings. */

@@ -93,7 +93,7 @@ FieldArray = ctypes.c_void_p * len(FIELD_NAMES)
 
 class NpomAdjointWs(ctypes.Structure):
     _fields_ = [("lam", ctypes.c_void_p * len(FIELD_NAMES)), ("save", ctypes.c_void_p),
-                ("save_floats", ctypes.c_size_t)]
+                ("save_floats", ctypes.c_size_t), ("pcg_x", ctypes.c_void_p)]
 
 
 # State fields of the explicit core that carry a cotangent through a step:

@@ -320,15 +320,21 @@ class _StepsFunction(torch.autograd.Function):
         # the call's structs once: the fields live in dyn for the whole call
         lib = _abi.load_library()
         p, fa, ws = core.params(), core._fields(), core._workspace()
-        fn = lib.npom_step_explicit if core.core_name == "explicit" else lib.npom_step_implicit
+        implicit = core.core_name != "explicit"
+        fn = lib.npom_step_implicit if implicit else lib.npom_step_explicit
         st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+        # semi-implicit core: the raw solution of every step's free-surface
+        # solve (workspace plane x), so the step adjoint replays the solve
+        xck = torch.empty((max(nsteps, 1), im * jm) if implicit else (1, 1), dtype=torch.float32, device=dev)
         for n in range(nsteps):
             ckpt[n].copy_(dyn.flat)
             clk = _abi.NpomClock(float(time0), n + 1, 1)
             _abi.check(fn(ctypes.byref(p), ctypes.byref(fa), ctypes.byref(ws["struct"]), ctypes.byref(clk), st),
                        "npom step")
+            if implicit:
+                xck[n].copy_(ws["bufs"]["x"].reshape(-1))
         ctx.core, ctx.nsteps, ctx.time0 = core, nsteps, time0
-        ctx.save_for_backward(ckpt)
+        ctx.save_for_backward(ckpt, xck)
         outs = tuple(dyn.views[n].clone() for n in _abi.ADJ_STATE_FIELDS)
         for n, o in zip(_abi.ADJ_STATE_FIELDS, outs):
             setattr(core, n, o)
@@ -336,7 +342,7 @@ class _StepsFunction(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, *grads):
-        (ckpt,) = ctx.saved_tensors
+        ckpt, xck = ctx.saved_tensors
         core = ctx.core
         lib = _abi.load_library()
         dev = core.device
@@ -363,6 +369,9 @@ class _StepsFunction(torch.autograd.Function):
             aws.lam[i] = Lm.views[n].data_ptr()
         aws.save = save.data_ptr()
         aws.save_floats = save.numel()
+        implicit = core.core_name != "explicit"
+        xfix = torch.empty(im * jm if implicit else 1, dtype=torch.float32, device=dev)
+        aws.pcg_x = xfix.data_ptr() if implicit else None
         fa = _abi.FieldArray(*[work.views[n].data_ptr() for n in names])
         ga = _abi.FieldArray(*[G.views[n].data_ptr() for n in names])
         ws = core._workspace()
@@ -370,6 +379,8 @@ class _StepsFunction(torch.autograd.Function):
         fn = lib.npom_step_explicit_adjoint if core.core_name == "explicit" else lib.npom_step_implicit_adjoint
         for n in reversed(range(ctx.nsteps)):
             work.flat[:ndyn].copy_(ckpt[n])
+            if implicit:
+                xfix.copy_(xck[n])
             clk = _abi.NpomClock(float(ctx.time0), int(n + 1), 1)
             status = fn(ctypes.byref(p), ctypes.byref(fa), ctypes.byref(ws["struct"]), ctypes.byref(clk),
                         ctypes.byref(ga), ctypes.byref(aws), ctypes.c_void_p(st.cuda_stream))

@@ -194,6 +194,20 @@ int plan_adj_ext(const Ctx &c) {
 // post step) is kept in xs; then the Shapiro filter (gamma 0) and masks of
 // the post step, d = h + elf, ring values -- the same arithmetic as
 // k_pcg_cluster's post step.
+// The forward solve (with its rhs set-up, no post step) without solving:
+// the stored transports of the set-up, and elf = the raw solution the
+// forward pass kept (ring 0).  The solve is deterministic, so this writes
+// what run_pcg(with_rhs, no post) writes to the fields the step reads.
+__global__ void __launch_bounds__(kThreads) k_imp_replay(Ctx c, const float *x) {
+  const int n = c.im * c.jm;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int i = q / c.jm, j = q % c.jm;
+  P2(fluxua, i, j) = rhs_fluxua(c, i, j);
+  P2(fluxva, i, j) = rhs_fluxva(c, i, j);
+  P2(elf, i, j) = interior(c, i, j) ? x[q] : 0.0f;
+}
+
 __global__ void __launch_bounds__(kThreads) k_imp_post(Ctx c, const float *xs) {
   const int n = c.im * c.jm;
   int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -275,6 +289,7 @@ dim3 field_list_grid(const Ctx &c, const AdjPhaseRec &r) {
 constexpr int kAdjScratchPlanes = 2 * AW_COUNT + 4;
 
 struct ImpScratch {
+  const float *xsaved;  // the forward solve's raw solution, or null (solve again)
   float *xs, *g, *lam, *gd;
 };
 
@@ -284,8 +299,12 @@ void launch_fwd_phase(const Ctx &c, const AdjPhaseRec &r, const PcgPlan &pplan, 
   const unsigned gx = (unsigned)((ncell + kThreads - 1) / kThreads);
   switch (r.phase) {
     case AP_EI:
-      cudaMemsetAsync(c.sync, 0, 4 * sizeof(unsigned int), s);
-      run_pcg(c, pplan, 1, 0, s);
+      if (is.xsaved) {
+        k_imp_replay<<<gx, kThreads, 0, s>>>(c, is.xsaved);
+      } else {
+        cudaMemsetAsync(c.sync, 0, 4 * sizeof(unsigned int), s);
+        run_pcg(c, pplan, 1, 0, s);
+      }
       cudaMemcpyAsync(is.xs, c.F[NPOM_F_elf], (size_t)ncell * sizeof(float), cudaMemcpyDeviceToDevice, s);
       k_imp_post<<<gx, kThreads, 0, s>>>(c, is.xs);
       break;
@@ -388,6 +407,7 @@ npom_status run_step_adjoint(const npom_params *p, float *const *fields, const n
     a.L[NPOM_NFIELDS + w] = scratch + (size_t)(AW_COUNT + w) * ncell;
   }
   ImpScratch is;
+  is.xsaved = core == NPOM_CORE_IMPLICIT ? aws->pcg_x : nullptr;
   is.xs = scratch + (size_t)(2 * AW_COUNT) * ncell;
   is.g = is.xs + ncell;
   is.lam = is.g + ncell;
@@ -475,6 +495,7 @@ struct AdjGraphKey {
   Ctx c;
   Adj a;
   float *save;
+  const float *xsaved;
 };
 
 struct AdjGraphEntry {
@@ -499,6 +520,7 @@ npom_status step_adjoint_graph(const npom_params *p, const npom_workspace *ws, c
   key.c = c;
   key.a = a;
   key.save = save;
+  key.xsaved = is.xsaved;
   std::lock_guard<std::mutex> lock(g_adj_graph_mutex);
   for (auto &g : g_adj_graphs) {
     if (g.device == dev && std::memcmp(&g.key, &key, sizeof(key)) == 0) {

@@ -611,6 +611,7 @@ __device__ __forceinline__ void pcg_cluster_body(const Ctx &c, const ClusterLayo
       ev = x0;
     }
     P2(elf, i, j) = ev;
+    c.W[NPOM_W_x][NPOM_I2(c, i, j)] = x0;  // the raw solution, as the grid-barrier form leaves it
   }
   // ring cells
   for (int q = gt; q < 2 * (im + jm); q += gs) {
@@ -620,6 +621,7 @@ __device__ __forceinline__ void pcg_cluster_body(const Ctx &c, const ClusterLayo
     else if (q < 2 * im + jm) { i = 0; j = q - 2 * im; }
     else { i = im - 1; j = q - 2 * im - jm; }
     P2(elf, i, j) = 0.0f;
+    c.W[NPOM_W_x][NPOM_I2(c, i, j)] = 0.0f;
     if (with_post) P2(d, i, j) = F2(h, i, j);
   }
   cl.sync();  // no CTA exits while others may still read its shared memory
