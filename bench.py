@@ -522,8 +522,14 @@ def dominant_kernel_roofline(core, stream, dev, reps=20):
     traffic = NCU_DRAM_BYTES.get(name) if (im, jm, kb) == GRID else None
     step_bytes = sum(phase_bytes(ph) for ph in times)
     step_ms = sum(times.values())
+    notes = {
+        "E_external": "the PCG / external subcycle is bound by synchronisation latency (cluster or grid "
+                      "barriers per iteration or substep), not by HBM: its arrays stay on chip or in L2; "
+                      "profiles/ has its ncu capture",
+    }
     return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": src, "traffic": traffic, "algorithmic_bytes": nbytes,
+            "note": notes.get(name),
             "launch_ms": times[name], "phase_ms": {k: round(v, 5) for k, v in times.items()},
             "phase_frac": {k: round(phase_bytes(k) / (v / 1000.0) / 1e9 / peak, 4) for k, v in times.items()},
             "step": {"algorithmic_bytes": step_bytes, "ms": step_ms,
