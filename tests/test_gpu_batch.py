@@ -176,3 +176,16 @@ def test_mpdata_batch_is_bitwise_members_alone():
         assert sa[0] == 0 and sb[0] == 0, (m, sa, sb)
         for n in a:
             assert np.array_equal(a[n], b[n], equal_nan=True), (m, n, rel_err(b[n], a[n]))
+
+
+@pytest.mark.parametrize("core", ["explicit", "implicit_p0_fixed"])
+def test_batch_with_twelve_levels_is_bitwise_members_alone(core):
+    """kb = 12: the batch runs every column phase one thread per column and
+    A1/B5 as point kernels (the 16-lane and tile forms need kb = 16); each
+    member bitwise what it computes alone."""
+    from neuralpom_b200 import cases
+    members = [cases.double_gyre(22, 20, core, kb=12), cases.double_gyre(30, 26, core, kb=12)]
+    for m, (a, b, sa, sb) in enumerate(_run_both(members, core, 0.25, 3)):
+        assert sa[0] == 0 and sb[0] == 0, (m, sa, sb)
+        for n in a:
+            assert np.array_equal(a[n], b[n], equal_nan=True), (m, n, rel_err(b[n], a[n]))
