@@ -189,3 +189,18 @@ def test_batch_with_twelve_levels_is_bitwise_members_alone(core):
         assert sa[0] == 0 and sb[0] == 0, (m, sa, sb)
         for n in a:
             assert np.array_equal(a[n], b[n], equal_nan=True), (m, n, rel_err(b[n], a[n]))
+
+
+def test_batch_inside_the_ramp_period_is_bitwise_members_alone():
+    """Members whose forcing ramp has not saturated (lramp with periods of
+    0.5 and 2 days, from time 0.1): every step launches directly with each
+    member's own ramp value; each member bitwise what it computes alone."""
+    from neuralpom_b200 import cases
+    members = []
+    for (im, jm, seed), period in (((37, 45, 7), 0.5), ((48, 40, 8), 2.0)):
+        A, Sc = cases.noise_basin(im, jm, seed=seed)
+        members.append((A, dict(Sc, lramp=True, period=period)))
+    for m, (a, b, sa, sb) in enumerate(_run_both(members, "explicit", 0.1, 3)):
+        assert sa[0] == 0 and sb[0] == 0, (m, sa, sb)
+        for n in a:
+            assert np.array_equal(a[n], b[n], equal_nan=True), (m, n, rel_err(b[n], a[n]))
