@@ -198,3 +198,26 @@ def test_gpu_coastal_step_adjoint_large_grid_matches_float64_differences():
         ads.append(sum(float((grads[f] * dirs[f]).sum()) for f in target))
     fds, ads = np.array(fds), np.array(ads)
     assert np.abs(fds - ads).max() / np.sqrt((ads ** 2).mean()) < 2e-3, (fds, ads)
+
+
+def test_gpu_implicit_adjoint_on_the_global_sy_cluster_layout(monkeypatch):
+    """128x112 interiors solve on the 16-CTA cluster layout that reads Sy
+    from global memory, in the forward and in the adjoint solve; the
+    gradients of two differentiable steps agree with those of the
+    grid-barrier PCG (a different rounding of the same solver) to 1e-3."""
+    from neuralpom_b200 import cases, resolve_core_class
+    A, Sc = cases.seamount(128, 112)
+    Sc = dict(Sc, time=1.0, time0=1.0)
+    grads = []
+    for form in ("coop", "cluster"):
+        monkeypatch.setenv("NPOM_PCG", form)
+        c = resolve_core_class("implicit_p0_fixed").from_state(A, Sc, device="cuda")
+        leaves = [getattr(c, f).requires_grad_(True) for f in ("t", "u", "el")]
+        c.time0, c.iend = 1.0, 2
+        c.run_time_loop()
+        loss = (c.u ** 2).mean() + (c.v ** 2).mean() + 1e-2 * (c.t ** 2).mean()
+        loss.backward()
+        grads.append([t.grad.detach().cpu().numpy() for t in leaves])
+    for x, y in zip(*grads):
+        scale = float(np.abs(x).max())
+        assert scale > 0 and float(np.abs(y - x).max()) <= 1e-3 * scale
