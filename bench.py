@@ -109,6 +109,9 @@ def parse():
     ap.add_argument("--batch-chunk", type=int, default=24,
                     help="batch workload: turns per simulated day in which the groups (or members) enqueue "
                          "their steps")
+    ap.add_argument("--batch-streams", type=int, default=2, choices=(1, 2),
+                    help="batch workload: the explicit and semi-implicit batches on one stream in turns (1) or "
+                         "each on its own stream (2, the default)")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the 64-member batch ('batch' key of the default workload)")
     ap.add_argument("--batch-mode", default="launch", choices=("launch", "streams"),
@@ -1066,6 +1069,15 @@ def batch_summary(args):
 
 
 def batch_measure(args):
+    if args.batch_mode == "launch" and args.batch_streams == 2:
+        if os.environ.get("NPOM_BATCH_SUBCYCLE") == "coop":
+            # two batches that both launch cooperative grids share one stream
+            args.batch_streams = 1
+        else:
+            # only the semi-implicit batch launches a cooperative grid (the
+            # PCG of its largest members); capping its blocks per member
+            # leaves SMs to the explicit batch on the other stream
+            os.environ.setdefault("NPOM_BATCH_PCG_BLOCKS", "64")
     if args.batch_mode == "streams":
         # members run concurrently: the explicit subcycle runs on one cluster
         # per member (up to four cells per thread), never as a cooperative
@@ -1120,25 +1132,36 @@ def batch_measure(args):
     for mb in members:
         groups.setdefault(mb["name"], []).append(mb)
 
+    group_streams = [torch.cuda.Stream(dev) for _ in groups] if args.batch_streams == 2 else None
+
     def launch_batched(steps_of):
         # each core's members advance as one batch (one launch per phase);
-        # the two batches take turns on one stream, --batch-chunk turns a day
+        # the two batches take turns on one stream (or run each on its own
+        # stream), --batch-chunk turns a day
         todo = []
-        for mbs in groups.values():
+        if group_streams:
+            go = torch.cuda.Event()
+            go.record(main_stream)
+        for g, mbs in enumerate(groups.values()):
             n = steps_of(mbs[0])
+            st = group_streams[g] if group_streams else main_stream
+            if group_streams:
+                st.wait_event(go)
             todo.append([[mb["core"] for mb in mbs], n, 0, float(mbs[0]["core"].time),
-                         max(1, -(-n // max(1, args.batch_chunk)))])
+                         max(1, -(-n // max(1, args.batch_chunk))), st])
         launches = 0
         while any(t[2] < t[1] for t in todo):
             for t in todo:
-                cores, n, done, t0, per_turn = t
+                cores, n, done, t0, per_turn, st = t
                 k = min(per_turn, n - done)
                 if k > 0:
-                    launches += batch.launch_batch(cores, k, t0, 1 + done, main_stream)
+                    launches += batch.launch_batch(cores, k, t0, 1 + done, st)
                     t[2] += k
-        for cores, n, _, t0, _ in todo:
+        for cores, n, _, t0, _, st in todo:
             for c in cores:
                 c.time = c.dti * n / 86400.0 + t0
+            if group_streams:
+                main_stream.wait_stream(st)
         return launches
 
     def advance(steps_of):
@@ -1201,7 +1224,8 @@ def batch_measure(args):
         "config": {"workload": WORKLOADS["batch"]["desc"], "members": nmem, "mode": args.batch_mode,
                    "explicit_subcycle": (os.environ.get("NPOM_BATCH_SUBCYCLE", "phases")
                                          if args.batch_mode == "launch" else os.environ.get("NPOM_SUBCYCLE")),
-                   "turns_per_day": args.batch_chunk,
+                   "turns_per_day": args.batch_chunk, "streams": args.batch_streams,
+                   "pcg_blocks_per_member": os.environ.get("NPOM_BATCH_PCG_BLOCKS"),
                    "hw_queues": os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS"),
                    "member_days_per_step": member_days / args.steps, "internal_steps": args.internal_steps,
                    "l2": "flushed (256 MiB write) before every timed step"},

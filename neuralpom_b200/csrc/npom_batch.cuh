@@ -234,7 +234,7 @@ bool batch_subcycle_coop() {
 // their work (at least one each, at most what covers the work); false when
 // the members outnumber the co-resident blocks
 bool batch_coop_shares(const void *fn, const std::vector<int> &members, const std::vector<size_t> &work,
-                       int start[], int *total) {
+                       int start[], int *total, int max_per_member = NPOM_MAX_COOP_BLOCKS) {
   int dev = 0, sms = 0, per_sm = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return false;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return false;
@@ -255,7 +255,7 @@ bool batch_coop_shares(const void *fn, const std::vector<int> &members, const st
     const double share = (double)(cap - n) * (double)work[s] / (double)(sum ? sum : 1);
     int b = 1 + (int)share;
     b = std::min(b, std::max(1, blocks_for(work[s], kThreads)));
-    b = std::min(b, NPOM_MAX_COOP_BLOCKS);
+    b = std::min(b, std::min(max_per_member, NPOM_MAX_COOP_BLOCKS));
     at += b;
   }
   start[n] = at;
@@ -405,7 +405,12 @@ cudaError_t make_batch_plan(const std::vector<Ctx> &ctx, int core, BatchPlan *P)
       T->clu_count[g] = P->clu_count[g] = 0;
     }
     int total = 0;
-    if (!batch_coop_shares((const void *)kb_pcg, coop, work, T->start[BS_PCG], &total)) return cudaErrorInvalidValue;
+    // NPOM_BATCH_PCG_BLOCKS caps the blocks of each member's cooperative
+    // solve (its barrier waits hold their SMs)
+    const char *cap_env = getenv("NPOM_BATCH_PCG_BLOCKS");
+    const int per_member = cap_env ? std::max(1, atoi(cap_env)) : NPOM_MAX_COOP_BLOCKS;
+    if (!batch_coop_shares((const void *)kb_pcg, coop, work, T->start[BS_PCG], &total, per_member))
+      return cudaErrorInvalidValue;
     T->count[BS_PCG] = (int)coop.size();
     for (size_t s = 0; s < coop.size(); ++s) T->member[BS_PCG][s] = coop[s];
     P->blocks[BS_PCG] = total;
