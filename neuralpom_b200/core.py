@@ -310,6 +310,8 @@ class _StepsFunction(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, core, nsteps, time0, *state):
+        # outputs without a cotangent reach backward as None (no zero fills)
+        ctx.set_materialize_grads(False)
         dev = core.device
         im, jm, kb = core.im, core.jm, core.kb
         dyn = _StateBuffer(_abi.ADJ_STATE_FIELDS, im, jm, kb, dev)
