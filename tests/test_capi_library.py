@@ -47,6 +47,10 @@ def test_argument_errors_need_no_gpu(lib):
                           None, None) == 0
     assert lib.npom_step_implicit(None, None, None, None, None) == 1
     assert lib.npom_pcg_adjoint(None, None, None, None, None, None, None, None, None) == 1
+    # the ensemble call: no members, too many members, null arrays
+    assert lib.npom_step_batch(0, None, None, None, None, None) == 1
+    assert lib.npom_step_batch(65, None, None, None, None, None) == 1
+    assert lib.npom_step_batch(2, None, None, None, None, None) == 1
 
 
 def test_library_is_sm100a(lib):
