@@ -495,6 +495,12 @@ __device__ __forceinline__ void pcg_coop_body(const Ctx &c, int with_rhs, int wi
   float *x = c.W[NPOM_W_x], *r = c.W[NPOM_W_r], *p = c.W[NPOM_W_p], *zv = c.W[NPOM_W_zv];
   float *ap = c.W[NPOM_W_ap], *rhs = c.W[NPOM_W_rhs];
   const float *elf = c.F[NPOM_F_elf];
+  // With the spectral preconditioner the Jacobi-diagonal plane is free and
+  // holds the next search direction: the update p' = p * beta + z is then
+  // computed inside the next operator apply (from the unchanged p and z)
+  // instead of being stored first, which saves one grid barrier per
+  // iteration with the same values.
+  float *pnext = c.k.eta_precond == NPOM_PRECOND_SPECTRAL ? c.W[NPOM_W_diag] : nullptr;
   // setup: rhs (+ stored transports), initial guess with zero ring, zeroed
   // ring of every work vector
   for (size_t q = tid; q < ncell; q += stride) {
@@ -513,6 +519,7 @@ __device__ __forceinline__ void pcg_coop_body(const Ctx &c, int with_rhs, int wi
       p[q] = 0.0f;
       zv[q] = 0.0f;
       ap[q] = 0.0f;
+      if (pnext) pnext[q] = 0.0f;
     }
   }
   if (!grid_barrier(c)) return;
@@ -543,14 +550,29 @@ __device__ __forceinline__ void pcg_coop_body(const Ctx &c, int with_rhs, int wi
   int its = 0;
   bool converged = false;
   if (!grid_barrier(c)) return;
+  bool pending = false;  // p' = p * beta_p + z not stored yet
+  float beta_p = 0.0f;
   for (int it = 1; it <= c.k.eta_max_iter; ++it) {
     double pap = 0.0;
     for (size_t q = tid; q < nint; q += stride) {
       int i = (int)(q / nj) + 1, j = (int)(q % nj) + 1;
       size_t o = NPOM_I2(c, i, j);
-      float a = elliptic_apply_cell(c, p, i, j);
+      float a, pv;
+      if (pending) {
+        a = elliptic_apply_cell_pz(c, p, zv, beta_p, i, j, &pv);
+        pnext[o] = pv;  // read back by this thread only until the next barrier
+      } else {
+        a = elliptic_apply_cell(c, p, i, j);
+        pv = __ldcg(p + o);
+      }
       ap[o] = a;
-      pap += (double)__ldcg(p + o) * (double)a;
+      pap += (double)pv * (double)a;
+    }
+    if (pending) {
+      float *t = p;
+      p = pnext;
+      pnext = t;
+      pending = false;
     }
     block_sum3(c, pap, 0.0, 0.0, 0, -1, -1);
     if (!grid_barrier(c)) return;
@@ -577,11 +599,16 @@ __device__ __forceinline__ void pcg_coop_body(const Ctx &c, int with_rhs, int wi
     if (!grid_barrier(c)) return;
     double rho_new = grid_total(c, 2);
     float beta = (float)(rho_new / (rho_old + 1e-30));
+    rho_old = rho_new;
+    if (pnext) {
+      pending = true;
+      beta_p = beta;
+      continue;
+    }
     for (size_t q = tid; q < nint; q += stride) {
       size_t o = NPOM_I2(c, (int)(q / nj) + 1, (int)(q % nj) + 1);
       p[o] = __ldcg(p + o) * beta + __ldcg(zv + o);
     }
-    rho_old = rho_new;
     if (!grid_barrier(c)) return;
   }
   if (tid == 0) {

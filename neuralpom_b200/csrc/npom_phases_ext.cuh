@@ -150,6 +150,36 @@ NPOM_HD float elliptic_apply_cell(const Ctx &c, const float *eta, int i, int j) 
   return e - c.k.implicit_coeff * div;
 }
 
+// The same operator applied to p' = p * beta + z (p on the ring cells),
+// from the unchanged p and z: every value p' takes is computed with the
+// expression the PCG's direction update stores, so the result is the
+// operator applied to the stored p'.  *centre receives p' at (i, j).
+NPOM_HD float elliptic_apply_cell_pz(const Ctx &c, const float *p, const float *z, float beta, int i, int j,
+                                     float *centre) {
+  const int jm = c.jm;
+  auto pv = [&](int ii, int jj) {
+    const size_t q = NPOM_I2(c, ii, jj);
+    const float v = ldc(c, p + q);
+    return interior(c, ii, jj) ? v * beta + ldc(c, z + q) : v;
+  };
+  const size_t o = NPOM_I2(c, i, j);
+  float e = pv(i, j);
+  *centre = e;
+  if (!interior(c, i, j)) return e;
+  const float *dd = c.F[NPOM_F_d];
+  float d0 = ldc(c, dd + o);
+  float he = 0.5f * (ldc(c, dd + o + jm) + d0);
+  float hw = 0.5f * (d0 + ldc(c, dd + o - jm));
+  float hn = 0.5f * (ldc(c, dd + o + 1) + d0);
+  float hs = 0.5f * (d0 + ldc(c, dd + o - 1));
+  float fe = he * (pv(i + 1, j) - e) * W2(ce, i, j) * F2(dum, i + 1, j);
+  float fw = hw * (e - pv(i - 1, j)) * W2(cw, i, j) * F2(dum, i, j);
+  float fn = hn * (pv(i, j + 1) - e) * W2(cn, i, j) * F2(dvm, i, j + 1);
+  float fs = hs * (e - pv(i, j - 1)) * W2(cs, i, j) * F2(dvm, i, j);
+  float div = (fe - fw + fn - fs) * W2(inv_art, i, j);
+  return e - c.k.implicit_coeff * div;
+}
+
 // Jacobi diagonal (core.py:677-700)
 NPOM_HD float jacobi_diag_cell(const Ctx &c, int i, int j) {
   if (!interior(c, i, j)) return 1.0f;
