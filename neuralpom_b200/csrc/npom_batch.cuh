@@ -373,7 +373,7 @@ cudaError_t make_batch_plan(const std::vector<Ctx> &ctx, int core, BatchPlan *P)
         P->clu_smem[g] = std::max(P->clu_smem[g], L.bytes());
       } else {
         coop.push_back(m);
-        work.push_back((size_t)(ctx[m].im - 2) * (ctx[m].jm - 2));
+        work.push_back(pcg_coop_work(ctx[m]));
       }
     }
     for (int g = 0; g < 4; ++g) {
@@ -400,7 +400,7 @@ cudaError_t make_batch_plan(const std::vector<Ctx> &ctx, int core, BatchPlan *P)
       for (int q = 0; q < T->clu_count[g]; ++q) {
         const int m = T->clu_member[g][q];
         coop.push_back(m);
-        work.push_back((size_t)(ctx[m].im - 2) * (ctx[m].jm - 2));
+        work.push_back(pcg_coop_work(ctx[m]));
       }
       T->clu_count[g] = P->clu_count[g] = 0;
     }

@@ -953,12 +953,25 @@ bool cluster_launchable(const void *fn, int nc, size_t smem) {
   return n > 0;
 }
 
+// Work of the grid-barrier PCG in threads: one per interior cell, and at
+// least one block per DST tile (a block holding two tiles would double
+// every DST stage).
+size_t pcg_coop_work(const Ctx &c) {
+  const size_t ni = (size_t)(c.im - 2), nj = (size_t)(c.jm - 2);
+  size_t work = ni * nj;
+  if (c.k.eta_precond == NPOM_PRECOND_SPECTRAL) {
+    const size_t tiles = ((ni + kDstRows - 1) / kDstRows) * ((nj + kDstCols - 1) / kDstCols);
+    work = std::max(work, tiles * (size_t)kThreads);
+  }
+  return work;
+}
+
 cudaError_t plan_pcg(const Ctx &c, PcgPlan *plan) {
   plan->cluster = pcg_cluster_layout(c, &plan->L) && ensure_cluster_attrs(plan->L) &&
                   cluster_launchable(pcg_cluster_fn(plan->L), plan->L.nc, plan->L.bytes());
   plan->coop_blocks = 0;
   if (plan->cluster) return cudaSuccess;
-  return coop_blocks((const void *)k_pcg, (size_t)(c.im - 2) * (c.jm - 2), &plan->coop_blocks);
+  return coop_blocks((const void *)k_pcg, pcg_coop_work(c), &plan->coop_blocks);
 }
 
 cudaError_t run_pcg(Ctx c, const PcgPlan &plan, int with_rhs, int with_post, cudaStream_t s) {
