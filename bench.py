@@ -1076,8 +1076,10 @@ def batch_measure(args):
         else:
             # only the semi-implicit batch launches a cooperative grid (the
             # PCG of its largest members); capping its blocks per member
-            # leaves SMs to the explicit batch on the other stream
-            os.environ.setdefault("NPOM_BATCH_PCG_BLOCKS", "64")
+            # leaves SMs to the explicit batch on the other stream.  56 is
+            # two DST-tile rounds for the 177x161 members (110 tiles):
+            # measured best of 40 / 56 / 64 / 112 for this mix of grids
+            os.environ.setdefault("NPOM_BATCH_PCG_BLOCKS", "56")
     if args.batch_mode == "streams":
         # members run concurrently: the explicit subcycle runs on one cluster
         # per member (up to four cells per thread), never as a cooperative
