@@ -15,15 +15,15 @@
 //     all members (NPOM_BATCH_SUBCYCLE=phases, the default), or one
 //     cooperative launch for the whole subcycle in which each member's
 //     blocks meet at their own grid barrier (=coop);
-//   PCG (semi-implicit core): one cluster launch per cluster shape (CTAs,
-//     Sy in shared or global memory), one
-//     cluster per member whose interior fits the cluster layout (the
-//     member's own shared-memory layout, as when it runs alone); one
-//     cooperative launch for the other members, each on its own share of
-//     the blocks with its own grid barrier.  The FP64 dot products of the
-//     cooperative form are summed per block, so a member that gets fewer
-//     blocks than it gets alone sums them in another order (results agree
-//     to rounding, not bitwise);
+//   PCG (semi-implicit core): one cluster launch per cluster shape (8 or
+//     16 CTAs, Sy in shared or global memory), one cluster per member
+//     whose interior fits a cluster layout (the member's own layout, as
+//     when it runs alone); one cooperative launch for the other members,
+//     each on its own share of the co-resident blocks (at most
+//     NPOM_BATCH_PCG_BLOCKS each when set) with its own grid barrier.  The
+//     FP64 dot products of the cooperative form are summed per block, so a
+//     member that gets fewer blocks than it gets alone sums them in another
+//     order (results agree to rounding, not bitwise);
 //   A1 and B5 (kb == 16): the flux-once tiles of every member in one
 //     launch (bitwise the point kernels' values), with one rows-per-tile
 //     value for the whole batch;
