@@ -58,9 +58,10 @@ WORKLOADS = {
 }
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the
-# phase's kernel at 90x82x16, from the ncu capture summarised in
-# profiles/k_pcg_cluster_seamount_90x82x16.md
-NCU_DRAM_BYTES = {"E_external": 561152}
+# phase's kernel at 90x82x16, read from one ncu capture of that kernel (not
+# measured by this script); reported with the capture it comes from.
+NCU_DRAM_BYTES = {"E_external": (561152, "ncu --set full capture of one k_pcg_cluster launch "
+                                         "(90x82x16 seamount, in-step input)")}
 
 # Distinct arrays each phase reads / writes (3-D count, 2-D count): the
 # algorithmic-byte rule bytes = 4 * (sum of read numel + sum of written numel).
@@ -522,16 +523,18 @@ def dominant_kernel_roofline(core, stream, dev, reps=20):
     sec = times[name] / 1000.0
     achieved = nbytes / sec / 1e9
     peak, src = measured_peaks()
-    traffic = NCU_DRAM_BYTES.get(name) if (im, jm, kb) == GRID else None
+    traffic, traffic_src = NCU_DRAM_BYTES.get(name, (None, None)) if (im, jm, kb) == GRID else (None, None)
     step_bytes = sum(phase_bytes(ph) for ph in times)
     step_ms = sum(times.values())
     notes = {
         "E_external": "the PCG / external subcycle is bound by synchronisation latency (cluster or grid "
                       "barriers per iteration or substep), not by HBM: its arrays stay on chip or in L2; "
-                      "profiles/ has its ncu capture",
+                      "frac is reported against HBM for the record only",
     }
-    return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_source": src, "traffic": traffic, "algorithmic_bytes": nbytes,
+    bound = "sync-latency" if name == "E_external" else "hbm"
+    return {"kernel": name, "bound": bound, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": src, "traffic": traffic, "traffic_source": traffic_src,
+            "algorithmic_bytes": nbytes,
             "note": notes.get(name),
             "launch_ms": times[name], "phase_ms": {k: round(v, 5) for k, v in times.items()},
             "phase_frac": {k: round(phase_bytes(k) / (v / 1000.0) / 1e9 / peak, 4) for k, v in times.items()},

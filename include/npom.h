@@ -254,7 +254,10 @@ npom_status npom_pcg_adjoint(const npom_params *p, float *const *fields,
  *     before reading it.
  *   - First call per device: looks up the scratch address with
  *     cudaGetSymbolAddress (device p->device current); make it before any
- *     stream capture.
+ *     stream capture.  The address is kept per device together with the
+ *     calling thread's current context, and looked up again when a call
+ *     comes from another context of that device (after cudaDeviceReset,
+ *     or under a context the caller made current).
  *   - Concurrency: calls on one device share the scratch; overlapping
  *     calls (other streams, other threads) race.  Serialise them.
  *   - Outputs: iters_out and status_out (device int / unsigned int, may be

@@ -54,6 +54,7 @@ class B200Core:
         self._refresh_derived()
         self._ws = None
         self._ws_key = None
+        self._ws_geo = None
         self._eta_solver_iteration_history = []
         self._eta_adjoint_iteration_history = []
 
@@ -95,7 +96,13 @@ class B200Core:
 
     # -- workspace ---------------------------------------------------------
     def _workspace(self):
-        geo = tuple((n, getattr(self, n).data_ptr(), getattr(self, n)._version) for n in ("dx", "dy", "h"))
+        # the spectral operator depends on dx, dy and h: a tensor replaced by
+        # another one (a new object, even at a recycled address with a fresh
+        # version counter) or modified in place (a new version) rebuilds it.
+        # The key holds the objects' ids and _ws_geo keeps the objects alive,
+        # so an id in the key cannot be recycled by a new tensor.
+        geo = tuple((n, id(getattr(self, n)), getattr(self, n).data_ptr(), getattr(self, n)._version)
+                    for n in ("dx", "dy", "h"))
         key = (self.im, self.jm, self.kb, self.device, geo, float(self.dti), float(self.alpha))
         if self._ws is not None and self._ws_key == key:
             return self._ws
@@ -129,6 +136,7 @@ class B200Core:
             b["sy"].copy_(torch.from_numpy(sy))
             b["inv_eigs"].copy_(torch.from_numpy(ie))
         self._ws_key = key
+        self._ws_geo = tuple(getattr(self, n) for n in ("dx", "dy", "h"))
         return self._ws
 
     def _fields(self):

@@ -889,8 +889,10 @@ const void *pcg_cluster_fn(const ClusterLayout &L) {
 }
 
 bool ensure_cluster_attrs(const ClusterLayout &L) {
+  static std::mutex mu;
   static int smem_set[64][2] = {};
   static bool nonportable[64][2] = {};
+  std::lock_guard<std::mutex> lock(mu);
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
   const void *fn = pcg_cluster_fn(L);
@@ -1385,8 +1387,10 @@ cudaError_t enqueue_adj_solve(const Ctx &c, const npom_workspace *ws, const floa
 // model that owns only its state arrays and has no device allocator of its
 // own (a Fortran or C POM driver linked against this library), or a
 // real-time loop that forbids allocation once it has started.  The
-// address is looked up once per device; calls on one device share the
-// scratch and must not overlap.
+// address is looked up on the first call per device (and again when the
+// calling context of that device changes), so that first call should come
+// before any stream capture; calls on one device share the scratch and must
+// not overlap.
 // ---------------------------------------------------------------------------
 constexpr size_t kStaticCells = NPOM_STATIC_MAX_CELLS;
 constexpr int kStaticPlanes = 15;  // rhs x r p zv ap ce cw cn cs inv_art diag t1 t2 + one never touched
@@ -1400,17 +1404,43 @@ static __device__ __align__(256) unsigned char g_pcg_scratch[kStaticBytes];
 namespace {
 
 std::mutex g_static_mutex;
+// One entry per device: the context the address was looked up in (the
+// calling thread's current context) and the address.  A call from another
+// context of the device (after cudaDeviceReset, or a non-primary context
+// made current by the caller) looks the symbol up again.
+void *g_static_ctx[64] = {};
 unsigned char *g_static_addr[64] = {};
+
+// The calling thread's current driver context, through the runtime's driver
+// entry point (no link against libcuda); null if it cannot be resolved.
+void *current_context() {
+  typedef int (*get_current_fn)(void **);
+  static get_current_fn fn = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<get_current_fn>(f);
+    looked_up = true;
+  }
+  void *ctx = nullptr;
+  if (!fn || fn(&ctx) != 0) return nullptr;
+  return ctx;
+}
 
 // Device address of g_pcg_scratch on `dev`, which must be current.
 cudaError_t static_scratch(int dev, unsigned char **out) {
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lock(g_static_mutex);
-  if (!g_static_addr[dev]) {
+  void *ctx = current_context();
+  if (!g_static_addr[dev] || !ctx || ctx != g_static_ctx[dev]) {
     unsigned char *ptr = nullptr;
     cudaError_t e = cudaGetSymbolAddress((void **)&ptr, g_pcg_scratch);
     if (e != cudaSuccess) return e;
     g_static_addr[dev] = ptr;
+    g_static_ctx[dev] = ctx;
   }
   *out = g_static_addr[dev];
   return cudaSuccess;
@@ -1638,7 +1668,7 @@ npom_status npom_pcg_solve_static(const npom_params *p, float *const *fields, co
   float *planes = reinterpret_cast<float *>(base);
   int next = 0;
   auto plane = [&]() { return planes + (size_t)(next++) * kStaticCells; };
-  npom_workspace ws;
+  npom_workspace ws{};
   for (int w : {NPOM_W_rhs, NPOM_W_x, NPOM_W_r, NPOM_W_p, NPOM_W_zv, NPOM_W_ap, NPOM_W_ce, NPOM_W_cw, NPOM_W_cn,
                 NPOM_W_cs, NPOM_W_inv_art, NPOM_W_diag, NPOM_W_t1, NPOM_W_t2})
     ws.buf[w] = plane();

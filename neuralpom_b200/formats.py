@@ -28,7 +28,7 @@ import torch
 from .core import NUMERICS_VERSION
 
 # Attributes rebuilt on restore instead of saved.
-SCRATCH = frozenset({"device", "_ws", "_ws_key", "_eta_solver_iteration_history",
+SCRATCH = frozenset({"device", "_ws", "_ws_key", "_ws_geo", "_eta_solver_iteration_history",
                      "_eta_adjoint_iteration_history"})
 
 
@@ -70,6 +70,7 @@ def restore(core, state):
     core.device = device
     core._ws = None
     core._ws_key = None
+    core._ws_geo = None
     core._eta_solver_iteration_history = []
     core._eta_adjoint_iteration_history = []
 

@@ -31,8 +31,11 @@ def import_reference(path):
 
 
 def default_reference_path():
+    """The reference package location: ``NPOM_REFERENCE_SRC`` (a ``src``
+    directory of the reference sources) if set, else the ``pip install
+    --target baseline/_ref`` copy next to this repository; None if neither
+    holds the ``neuralpom`` package."""
     for cand in (os.environ.get("NPOM_REFERENCE_SRC", ""),
-                 "/root/reference/src",
                  os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "baseline", "_ref")):
         if cand and os.path.isdir(os.path.join(cand, "neuralpom")):
             return cand

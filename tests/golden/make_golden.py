@@ -1,7 +1,8 @@
 """Generate the golden vectors that pin the oracle to the reference core.
 
-Run in a container that holds the reference sources (default
-``/root/reference/src``, or ``NPOM_REFERENCE_SRC``)::
+Run where the reference package is importable: ``NPOM_REFERENCE_SRC`` names
+the ``src`` directory of its sources (or the ``baseline/_ref`` install is
+used)::
 
     python tests/golden/make_golden.py [proft] [steps] [adjoint] [coastal] [step_adjoint] [coupling] [mpdata]
 

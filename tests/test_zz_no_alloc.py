@@ -29,9 +29,10 @@ def test_static_solve_rejects_grids_above_the_scratch_limit():
     assert _abi.STATUS_NAMES[rc] == "NPOM_ERR_TOO_LARGE"
 
 
-def _case(im, jm):
+def _case(im, jm, precond="spectral"):
     from neuralpom_b200 import cases, resolve_core_class
     A, Sc = cases.seamount(im, jm)
+    Sc = dict(Sc, eta_solver_preconditioner=precond)
     core = resolve_core_class("implicit_p0_fixed").from_state(A, Sc, device="cuda")
     g = torch.Generator(device="cpu").manual_seed(1000 * im + jm)
     fsm = core.fsm
@@ -61,25 +62,31 @@ def _solve_allocating(_abi, lib, core, rhs, x0):
 def _solve_static(_abi, lib, core, rhs, x0):
     p, ws = core.params(), core._workspace()     # ws only supplies the spectral operator inputs
     b = ws["bufs"]
+    # the Jacobi preconditioner needs no spectral inputs: pass null for them
+    spectral = p.eta_precond == _abi.PRECOND_SPECTRAL
+    sx, sy, ie = ((b["sx"].data_ptr(), b["sy"].data_ptr(), b["inv_eigs"].data_ptr()) if spectral
+                  else (None, None, None))
     x = x0.clone()
     fields = _fields_with_elf(_abi, core, x)
     out = torch.full((2,), -1, dtype=torch.int32, device="cuda")
     st = torch.cuda.current_stream()
     rc = lib.npom_pcg_solve_static(ctypes.byref(p), ctypes.byref(fields), ctypes.c_void_p(rhs.data_ptr()),
-                                   ctypes.c_void_p(b["sx"].data_ptr()), ctypes.c_void_p(b["sy"].data_ptr()),
-                                   ctypes.c_void_p(b["inv_eigs"].data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                   ctypes.c_void_p(sx), ctypes.c_void_p(sy), ctypes.c_void_p(ie),
+                                   ctypes.c_void_p(out.data_ptr()),
                                    ctypes.c_void_p(out.data_ptr() + 4), ctypes.c_void_p(st.cuda_stream))
     _abi.check(rc, "npom_pcg_solve_static")
     torch.cuda.synchronize()
     return x, int(out[0].item()), int(out[1].item())
 
 
-# 90x82: the cluster PCG; 150x150 (148 interior rows): the grid-barrier PCG
+# 90x82: the cluster PCG; 150x150 (148 interior rows): the grid-barrier PCG;
+# each with the spectral preconditioner and with Jacobi (null spectral inputs)
 @pytest.mark.gpu
+@pytest.mark.parametrize("precond", ["spectral", "jacobi"])
 @pytest.mark.parametrize("im,jm", [(90, 82), (150, 150)])
-def test_static_solve_equals_allocating_solve_on_two_consecutive_calls(im, jm):
+def test_static_solve_equals_allocating_solve_on_two_consecutive_calls(im, jm, precond):
     _abi, lib = _lib()
-    core, rhs, x0 = _case(im, jm)
+    core, rhs, x0 = _case(im, jm, precond)
     rhs_before = rhs.clone()
     xa, ia = _solve_allocating(_abi, lib, core, rhs, x0)
     assert ia > 0
