@@ -48,7 +48,7 @@ def compare_day(case, im, jm, core, steps):
     """GPU run against the three oracle runs; returns the per-field table
     and the PCG iteration lists (GPU, float32 oracle)."""
     results = oracle_runs([(case, im, jm, core, steps, v) for v in ("fp32", "fp32_ulp", "fp64")])
-    (o32, it32, b32), (oulp, _, bulp), (o64, it64, b64) = results
+    (o32, it32, b32), (oulp, itulp, bulp), (o64, it64, b64) = results
     g, itg = _gpu_run(case, im, jm, core, steps)
     rows = {}
     for f in FIELDS:
@@ -61,9 +61,13 @@ def compare_day(case, im, jm, core, steps):
                        for n, name in enumerate(("volume", "layer_t", "layer_s"))}
     if itg or it32:
         d = np.array(itg) - np.array(it32)
+        du = np.array(itulp) - np.array(it32)
         rows["pcg_iterations"] = {"gpu_total": int(sum(itg)), "oracle32_total": int(sum(it32)),
                                   "fp64_total": int(sum(it64)), "max_abs_step_diff": int(np.abs(d).max()),
                                   "steps_differing": int(np.count_nonzero(d)),
+                                  "first_differing_step": int(np.argmax(d != 0)) + 1 if d.any() else None,
+                                  "ulp_max_abs_step_diff": int(np.abs(du).max()),
+                                  "ulp_steps_differing": int(np.count_nonzero(du)),
                                   "gpu_min": int(min(itg)), "gpu_max": int(max(itg)),
                                   "first_steps_gpu": itg[:12], "first_steps_oracle32": it32[:12]}
     _report(f"{case}_{im}x{jm}_{core}_{steps}", rows)
@@ -90,9 +94,12 @@ def test_gpu_seamount_full_day_matches_oracle_and_fp64():
     assert len(itg) == 288
     _check(rows)
     p = rows["pcg_iterations"]
-    # the same stopping rule on the same system: per-step counts agree, up
-    # to one iteration where the state has moved by its float32 sensitivity
-    assert p["max_abs_step_diff"] <= 1, p
+    # the same stopping rule on the same system: identical counts over the
+    # first simulated hour; later, as the flow amplifies rounding (the 1-ulp
+    # oracle run's own counts drift by as much), per-step counts within the
+    # 1-ulp run's deviation plus one, and the day's total within 1 %
+    assert itg[:12] == it32[:12], p
+    assert p["max_abs_step_diff"] <= p["ulp_max_abs_step_diff"] + 1, p
     assert abs(p["gpu_total"] - p["oracle32_total"]) <= max(3, p["oracle32_total"] // 100), p
 
 
