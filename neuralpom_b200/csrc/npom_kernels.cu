@@ -870,12 +870,20 @@ bool pcg_cluster_layout(const Ctx &c, ClusterLayout *out) {
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return false;
   const char *ctas = getenv("NPOM_PCG_CTAS");
   const bool prefer16 = ctas && std::strcmp(ctas, "16") == 0;
+  // the replicated-residual form (three cluster barriers per iteration)
+  // where its extra full-grid copy fits; NPOM_PCG=pushed keeps the
+  // pushed-residual form (four barriers) for comparisons
+  const bool spectral = c.k.eta_precond == NPOM_PRECOND_SPECTRAL;
+  const bool allow_rep = spectral && !(env && std::strcmp(env, "pushed") == 0);
   for (bool sy_global : {false, true}) {
     for (int nc : {prefer16 ? 16 : 8, prefer16 ? 8 : 16}) {
-      ClusterLayout L = cluster_layout(c.im, c.jm, nc, sy_global);
-      if (L.fits && L.bytes() <= (size_t)optin) {
-        *out = L;
-        return true;
+      for (bool rep : {true, false}) {
+        if (rep && !allow_rep) continue;
+        ClusterLayout L = cluster_layout(c.im, c.jm, nc, sy_global, rep);
+        if (L.fits && L.bytes() <= (size_t)optin) {
+          *out = L;
+          return true;
+        }
       }
     }
   }

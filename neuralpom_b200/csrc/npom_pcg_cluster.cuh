@@ -21,7 +21,19 @@
 //     partials in a fixed order with a butterfly, so every warp of every CTA
 //     holds bitwise the same total and takes the same convergence decision.
 // The cluster barrier (release/acquire) that follows each producer phase is
-// what makes the pushed data visible; four per iteration.
+// what makes the pushed data visible.
+//
+// Two loop forms, with the same vectors bit for bit:
+//   * replicated residual (layouts with room for a third full-grid copy, gap:
+//     90x82 on 8 CTAs): the operator product Ap is pushed into every CTA's
+//     gap together with the p.Ap partials, and every CTA then advances the
+//     WHOLE residual copy gr itself, r = r - alpha*Ap with the owner's own
+//     expression on the same bits.  The residual never travels and its norm
+//     is summed by every CTA over the whole grid in one fixed order (the same
+//     bits everywhere, so every CTA stops at the same iteration).  Three
+//     cluster barriers per iteration: p.Ap, the DST transpose, r.z;
+//   * pushed residual (larger interiors): the new r rows are pushed into gr
+//     and the r.r partials reduced; four cluster barriers per iteration.
 //
 // Arithmetic follows implicit_p0_fixed/core.py:460-589 (eager PCG) and
 // :591-639 (operator), :762-773 (spectral preconditioner, the DSTs as dense
@@ -52,7 +64,7 @@ namespace cgx = cooperative_groups;
 
 constexpr int kClusterThreads = 512;
 constexpr int kClusterWarps = kClusterThreads / 32;
-constexpr int kRedSlots = 4;  // pap, r.r, r.z, r0.r0
+constexpr int kRedSlots = 5;  // pap, r.r, r.z, r0.r0, and one CTA-local slot for block totals
 
 struct ClusterLayout {
   int ni, nj, nc, rows;  // interior size, CTAs, rows per CTA (<= 16: one MMA row tile)
@@ -60,6 +72,7 @@ struct ClusterLayout {
   int gp;                // row pitch of gr/gc: >= 8*nt and 8 or 24 (mod 32), conflict-free B-fragment loads
   // float offsets in dynamic shared memory
   int x, r, z, ap, rhs, p, zh, h4, c4, iart, ie, gr, gc, sxf, syf, t1f;
+  int gap;         // full-grid copy of Ap (replicated-residual form), -1 when absent
   int floats;
   bool fits;       // rows <= 16 and one column tile per warp
   bool sy_global;  // Sy read from global memory in the j-stages (no room for its fragments)
@@ -67,7 +80,7 @@ struct ClusterLayout {
   size_t bytes() const { return (size_t)floats * sizeof(float) + red_doubles() * sizeof(double); }
 };
 
-inline ClusterLayout cluster_layout(int im, int jm, int nc, bool sy_global = false) {
+inline ClusterLayout cluster_layout(int im, int jm, int nc, bool sy_global = false, bool replicated = false) {
   ClusterLayout L;
   L.sy_global = sy_global;
   L.ni = im - 2;
@@ -103,6 +116,7 @@ inline ClusterLayout cluster_layout(int im, int jm, int nc, bool sy_global = fal
   // Sy as B fragments: (hi x2, lo x2) per lane, k-tile, column tile
   L.syf = sy_global ? -1 : take(L.nt * L.nt * 32 * 4);
   L.t1f = take(L.nt * 32 * 4);             // i-stage result as A fragments of the j-stage
+  L.gap = replicated ? take(8 * L.kti * L.gp) : -1;  // full Ap, zero-padded like gr
   L.floats = o;
   return L;
 }
@@ -125,6 +139,19 @@ __device__ __forceinline__ double cl_partial_total(const double *red, int slot, 
   double t = 0.0;
   if (lane < kClusterWarps)
     for (int q = 0; q < nc; ++q) t += red[(slot * nc + q) * kClusterWarps + lane];
+  for (int off = 16; off > 0; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
+  return t;
+}
+
+// CTA total of every thread's v, the same bits in every warp (a fixed
+// butterfly in each warp, then the warp totals in a fixed butterfly); slot
+// holds kClusterWarps doubles of this CTA.  Contains a __syncthreads.
+__device__ __forceinline__ double cl_block_total(double v, double *slot) {
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) slot[w] = v;
+  __syncthreads();
+  double t = lane < kClusterWarps ? slot[lane] : 0.0;
   for (int off = 16; off > 0; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
   return t;
 }
@@ -443,6 +470,7 @@ __device__ __forceinline__ void pcg_cluster_body(const Ctx &c, const ClusterLayo
     for (int e = threadIdx.x; e < 8 * L.kti * L.gp; e += blockDim.x) {
       sm[L.gr + e] = 0.0f;
       sm[L.gc + e] = 0.0f;
+      if (L.gap >= 0) sm[L.gap + e] = 0.0f;
     }
     // Sx rows of the slab as split A fragments (zero outside the slab)
     for (int f = threadIdx.x; f < L.kti * 32; f += blockDim.x) {
@@ -511,7 +539,62 @@ __device__ __forceinline__ void pcg_cluster_body(const Ctx &c, const ClusterLayo
   int its = 0;
   bool converged = false;
   __syncthreads();  // p and its halo rows complete in this CTA
-  for (int it = 1; it <= c.k.eta_max_iter; ++it) {
+  const bool replicated = spectral && L.gap >= 0;
+  for (int it = 1; replicated && it <= c.k.eta_max_iter; ++it) {
+    // ---- replicated-residual form: three cluster barriers per iteration
+    double pap = cl_spmv(L, sm, coeff, nr, sm + L.ap, true);
+    __syncthreads();  // the Ap slab complete before it is pushed
+    cl_push_slab(cl, L, sm, L.ap, L.gap, a0, nr);
+    cl_push_partial(cl, pap, red, 0, nc, rank);
+    cl.sync();  // Ap rows and p.Ap partials in every CTA
+    const double denom = cl_partial_total(red, 0, nc);
+    const float alpha = (float)(rho_old / (denom + 1e-30));
+    for (int e = threadIdx.x; e < n; e += blockDim.x) sm[L.x + e] = sm[L.x + e] + alpha * p[nj + e];
+    // the whole residual, in every CTA, with the owner's expression
+    float4 *gr4 = reinterpret_cast<float4 *>(sm + L.gr);
+    const float4 *ga4 = reinterpret_cast<const float4 *>(sm + L.gap);
+    double rs = 0.0;
+    for (int e4 = threadIdx.x; e4 < 2 * L.kti * L.gp; e4 += blockDim.x) {
+      float4 rv = gr4[e4];
+      const float4 av = ga4[e4];
+      rv.x = rv.x - alpha * av.x;
+      rv.y = rv.y - alpha * av.y;
+      rv.z = rv.z - alpha * av.z;
+      rv.w = rv.w - alpha * av.w;
+      gr4[e4] = rv;
+      rs += (double)rv.x * (double)rv.x;
+      rs += (double)rv.y * (double)rv.y;
+      rs += (double)rv.z * (double)rv.z;
+      rs += (double)rv.w * (double)rv.w;
+    }
+    const double rsn = cl_block_total(rs, red + (size_t)4 * nc * kClusterWarps);  // gr complete after this
+    its = it;
+    if (rsn <= tol_sq || rsn <= rel_sq || rsn <= 1e-30) {
+      converged = true;
+      break;
+    }
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+      const int ra = e / nj;
+      sm[L.r + e] = sm[L.gr + (a0 + ra) * L.gp + (e - ra * nj)];
+    }
+    rz = cl_precondition<SYG>(cl, L, sm, nr, rank, a0, c.k.inverse_scale, spectral, c.W[NPOM_W_sy]);
+    cl_push_partial(cl, rz, red, 2, nc, rank);
+    cl.sync();  // z halo rows and r.z partials in place
+    const double rho_new = cl_partial_total(red, 2, nc);
+    const float beta = (float)(rho_new / (rho_old + 1e-30));
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+      float *pp = p + nj + e;
+      *pp = *pp * beta + sm[L.z + e];
+    }
+    for (int b = threadIdx.x; b < nj; b += blockDim.x) {
+      if (has_up) p[b] = p[b] * beta + sm[L.zh + b];
+      if (has_down) p[(nr + 1) * nj + b] = p[(nr + 1) * nj + b] * beta + sm[L.zh + nj + b];
+    }
+    rho_old = rho_new;
+    __syncthreads();
+  }
+  for (int it = 1; !replicated && it <= c.k.eta_max_iter; ++it) {
+    // ---- pushed-residual form: four cluster barriers per iteration
     double pap = cl_spmv(L, sm, coeff, nr, sm + L.ap, true);
     cl_push_partial(cl, pap, red, 0, nc, rank);
     cl.sync();

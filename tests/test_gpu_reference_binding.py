@@ -28,6 +28,11 @@ CASES = [("step_implicit_12x10.npz", "implicit_p0_fixed"), ("step_explicit_12x10
 COMPARED = ("u", "v", "t", "s", "el", "elf", "ua", "va", "q2", "q2l", "km", "kh", "w", "rho", "aam", "uaf")
 
 
+@pytest.fixture(autouse=True)
+def _reference_importable():
+    rh.import_reference(REF)
+
+
 def _physics_kw(core_name):
     return dict(core_name="explicit", compiled_kernels=()) if core_name == "explicit" else {}
 
