@@ -97,6 +97,7 @@ def parse():
     ap.add_argument("--ref-internal-steps", type=int, default=6, help="reference arm: internal steps per sample")
     ap.add_argument("--ref-device", default="cpu")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the per-field error against a float64 reference day")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--members", type=int, default=8,
                     help="ensemble members advanced concurrently on one GPU for the 'ensemble' key (1 = skip)")
@@ -363,7 +364,12 @@ def run_b200(args):
 
     ref_gpu = None
     if rank == 0 and ws_n == 1 and not args.no_ref_gpu:
-        ref_gpu = reference_gpu_sample(A, Sc, dev, core_name=W["core"])
+        ref_gpu = reference_modes(reference_gpu_sample, W["core"], dev, A=A, Sc=Sc, device=dev,
+                                  core_name=W["core"])
+
+    fp64 = None
+    if rank == 0 and ws_n == 1 and not args.no_fp64 and args.workload in ("seamount", "gyre"):
+        fp64 = fp64_day_error(A, Sc, nin, dev, W["core"])
 
     cpu = None
     if rank == 0 and ws_n == 1 and not args.no_cpu_baseline:
@@ -377,7 +383,8 @@ def run_b200(args):
         fa, A_dev, t_dev = seamount_fwd_adjoint(core, args, dev, nsteps=args.fa_steps, reps=args.fa_reps)
         case = (A_dev, dict(Sc, time=t_dev, time0=t_dev))
         if not args.no_ref_gpu:
-            fa["reference_gpu"] = reference_fwd_adjoint_sample(dev, case=case, core_name=W["core"], seed=11)
+            fa["reference_gpu"] = reference_modes(reference_fwd_adjoint_sample, W["core"], dev, device=dev,
+                                                  case=case, core_name=W["core"], seed=11)
         if not args.no_cpu_baseline:
             fa["reference_cpu"] = reference_fwd_adjoint_sample("cpu", internal_steps=3, case=case,
                                                                core_name=W["core"], seed=11)
@@ -402,6 +409,10 @@ def run_b200(args):
                    "pcg_iterations_last_step": (its[-1] if its else None) if W["core"] != "explicit" else None,
                    "members": ws_n, "parallelism": f"ensemble x{ws_n}" if ws_n > 1 else "single member",
                    "l2": "flushed (256 MiB write) before every timed step"},
+        "pcg_iterations_timed": ({"per_step_min": int(min(its)), "per_step_max": int(max(its)),
+                                  "per_step_mean": float(np.mean(its)), "steps": len(its)}
+                                 if (its and W["core"] != "explicit") else None),
+        "fp64_error": fp64,
         "roofline": roofline, "cpu_baseline": cpu, "reference_gpu": ref_gpu, "ensemble": ens, "fwd_adjoint": fa,
         "fwd_adjoint_midtrain": fam, "fwd_adjoint_midtrain_batch": famb, "batch": bat, "e2e": e2e,
         "gpu_launches": launches,
@@ -740,6 +751,28 @@ def coastal_fwd_adjoint(args, dev, nsteps=360):
                       "torch.cuda.max_memory_allocated over the warm-up and the sample"}
 
 
+def reference_coupling():
+    """The reference's own corrector coupling module
+    (hybrid/sparse_coupling.py), which runs unchanged on a B200 core: its
+    EOS and pressure-gradient calls go to the core's dens()/baropg(), the
+    CUDA operators with hand-written adjoints."""
+    import importlib
+    import types
+    for path in (os.environ.get("NPOM_REFERENCE_SRC", ""), os.path.join(ROOT, "baseline", "_ref")):
+        if path and os.path.isdir(os.path.join(path, "neuralpom")):
+            break
+    else:
+        raise RuntimeError("the reference package (baseline/_ref) is needed for the corrector coupling")
+    if "netCDF4" not in sys.modules:
+        try:
+            importlib.import_module("netCDF4")
+        except ModuleNotFoundError:  # imported by the reference's cores, never used
+            sys.modules["netCDF4"] = types.ModuleType("netCDF4")
+    if path not in sys.path:
+        sys.path.insert(0, path)
+    return importlib.import_module("neuralpom.hybrid.sparse_coupling")
+
+
 def fwd_adjoint_sample(args, dev, reps=3):
     """The Midtrain-shaped forward+adjoint: the explicit-core member of
     ``midtrain_case``, three differentiable 1 h intervals with the
@@ -747,7 +780,7 @@ def fwd_adjoint_sample(args, dev, reps=3):
     ``fwd_adjoint_timing``)."""
     import torch
     from neuralpom_b200 import _abi, resolve_core_class
-    from neuralpom_b200 import coupling
+    coupling = reference_coupling()
     A, Sc = midtrain_case(0)
     core = resolve_core_class("explicit").from_state(A, Sc, device=dev)
     tgt, _ = _fa_targets(A, 7)
@@ -787,7 +820,8 @@ def fwd_adjoint_midtrain_batch(args, dev, members=8, reps=3):
     with CUDA events on the launching stream around forward+backward; the
     device status of every member is checked after each sample."""
     import torch
-    from neuralpom_b200 import _abi, coupling, resolve_core_class
+    from neuralpom_b200 import _abi, resolve_core_class
+    coupling = reference_coupling()
     main = torch.cuda.current_stream(dev)
     mem = []
     for m in range(members):
@@ -861,7 +895,37 @@ def fwd_adjoint_midtrain_batch(args, dev, members=8, reps=3):
             "timing": f"median of {reps} samples, CUDA events around forward+backward of all members"}
 
 
-def reference_fwd_adjoint_sample(device, internal_steps=6, case=None, core_name="explicit", seed=7):
+# The reference's registered GPU training setup for the implicit core
+# (configs/examples/implicit_1h.json:7-12): compiled strict vertical kernels
+# and the Triton CG operator (hybrid/sparse_physics.py:19-28).
+REF_FAST_MODE = {"acceleration": "strict_vertical_compiled", "cg_backend": "triton", "compiled_kernels": ("proft",)}
+
+
+def reference_modes(fn, core_name, device, **kw):
+    """``fn`` timed under the reference's default options (eager, torch CG)
+    and, for the implicit core on a GPU, under its compiled training setup;
+    the line reports the faster (the reference's best on this GPU) and
+    every mode's figure."""
+    modes = {"eager": {}}
+    if core_name != "explicit" and str(device) != "cpu":
+        modes["strict_vertical_compiled+triton_cg"] = REF_FAST_MODE
+    out = {}
+    for name, opts in modes.items():
+        try:
+            out[name] = fn(physics_kw=opts, **kw)
+        except Exception as exc:  # a mode the reference cannot run here is reported, not fatal
+            out[name] = {"error": f"{type(exc).__name__}: {exc}"[:300]}
+    ok = {k: v for k, v in out.items() if "value" in v}
+    if not ok:
+        return {"error": "no reference mode ran", "modes": out}
+    best = max(ok, key=lambda k: ok[k]["value"])
+    res = dict(ok[best])
+    res["mode"] = best
+    res["modes"] = {k: (v.get("value") if "value" in v else v) for k, v in out.items()}
+    return res
+
+
+def reference_fwd_adjoint_sample(device, internal_steps=6, case=None, core_name="explicit", seed=7, physics_kw=None):
     """The reference core under torch autograd
     (SparsePhysics.advance(differentiable=True) + backward) on the same
     state: ``internal_steps`` steps, wall clock."""
@@ -878,7 +942,7 @@ def reference_fwd_adjoint_sample(device, internal_steps=6, case=None, core_name=
             t = getattr(core, k).detach().clone().requires_grad_(True)
             setattr(core, k, t)
             leaves.append(t)
-        rh.advance(core, core_name, n, differentiable=True, device=device)
+        rh.advance(core, core_name, n, differentiable=True, device=device, **(physics_kw or {}))
         loss = sum(((getattr(core, f) - torch.from_numpy(v).to(device)) ** 2).mean() for f, v in tgt.items())
         loss.backward()
         for k, v in list(vars(core).items()):
@@ -896,8 +960,8 @@ def reference_fwd_adjoint_sample(device, internal_steps=6, case=None, core_name=
     return {"value": days / sec, "unit": UNIT, "device": str(device),
             "threads": (os.cpu_count() or 1) if device == "cpu" else None,
             "sample": f"{internal_steps} internal steps forward+backward of the {_basin_name(A)} (reference "
-                      f"{core_name} core, torch autograd through SparsePhysics.advance(differentiable=True), after a "
-                      "1-step warm-up; wall clock)"}
+                      f"{core_name} core, torch autograd through SparsePhysics.advance(differentiable=True"
+                      f"{', ' + str(physics_kw) if physics_kw else ''}), after a 1-step warm-up; wall clock)"}
 
 
 def reference_core(A, Sc, device="cpu", core_name="implicit_p0_fixed"):
@@ -927,6 +991,91 @@ def reference_core(A, Sc, device="cpu", core_name="implicit_p0_fixed"):
     return core, rh
 
 
+class ReferenceFloat64:
+    """Context in which the reference core computes in float64: the
+    default dtype is float64 and the float32 scratch its step allocates
+    explicitly (explicit/momentum.py:25-28,144-147,555-556 and the tracer
+    routines) is allocated as float64 instead.  The core's own tensors are
+    promoted by ``promote``."""
+
+    NAMES = ("zeros", "ones", "empty", "full", "tensor", "arange", "linspace", "zeros_like", "ones_like",
+             "empty_like", "full_like", "as_tensor")
+
+    def __enter__(self):
+        import torch
+        self.torch = torch
+        self.saved = {n: getattr(torch, n) for n in self.NAMES}
+
+        def wrap(fn):
+            def alloc(*a, **k):
+                if k.get("dtype") is torch.float32:
+                    k["dtype"] = torch.float64
+                return fn(*a, **k)
+            return alloc
+        self.prev = torch.get_default_dtype()
+        for n in self.NAMES:
+            setattr(torch, n, wrap(self.saved[n]))
+        torch.set_default_dtype(torch.float64)
+        return self
+
+    def __exit__(self, *exc):
+        for n, fn in self.saved.items():
+            setattr(self.torch, n, fn)
+        self.torch.set_default_dtype(self.prev)
+
+    @staticmethod
+    def promote(core):
+        import torch
+        for k, v in list(vars(core).items()):
+            if torch.is_tensor(v) and v.dtype == torch.float32:
+                setattr(core, k, v.to(torch.float64))
+        # solver caches are rebuilt from the promoted geometry
+        core._accel_cache_ready = False
+        core._spectral_eta_preconditioner_cache = None
+        core._cg_work = {}
+
+
+FP64_FIELDS = ("u", "v", "t", "s", "el", "ua", "va", "q2", "q2l", "km", "kh", "w", "rho")
+
+
+def fp64_day_error(A, Sc, nin, dev, core_name):
+    """Error of every field of the B200 step after ``nin`` internal steps
+    from the workload's initial state, against the reference core's own run
+    of the same steps in float64 on the same device (outside the timed
+    region), and the PCG iteration counts of both runs."""
+    import torch
+    from neuralpom_b200 import resolve_core_class
+    b = resolve_core_class(core_name).from_state(A, Sc, device=dev)
+    b.time0, b.iend = float(b.time), nin
+    b.run_time_loop()
+    got = {f: getattr(b, f).detach().cpu().numpy().astype(np.float64) for f in FP64_FIELDS}
+    its_b = list(b._eta_solver_iteration_history)
+    core, rh = reference_core(A, Sc, dev, core_name)
+    ReferenceFloat64.promote(core)
+    if hasattr(core, "_eta_solver_iteration_history"):
+        core._eta_solver_iteration_history = []
+    t0 = time.perf_counter()
+    with ReferenceFloat64():
+        if hasattr(core, "_build_acceleration_cache"):
+            core._build_acceleration_cache()
+        rh.advance(core, core_name, nin, device=dev)
+    torch.cuda.synchronize(dev)
+    sec = time.perf_counter() - t0
+    ref = {f: getattr(core, f).detach().cpu().numpy() for f in FP64_FIELDS}
+    assert all(v.dtype == np.float64 for v in ref.values())
+    err = {f: float(np.abs(got[f] - ref[f]).max() / max(float(np.abs(ref[f]).max()), 1e-30)) for f in FP64_FIELDS}
+    out = {"fields": err, "metric": "max|b200 - ref64| / max|ref64| per field",
+           "run": f"{nin} internal steps from the workload's initial state; the reference core in float64 "
+                  f"(float32 scratch promoted) on {dev}, {sec:.1f} s, outside the timed region"}
+    its_r = list(getattr(core, "_eta_solver_iteration_history", []))
+    if its_b:
+        out["pcg_iterations"] = {"b200_total": int(sum(its_b)), "b200_min": int(min(its_b)),
+                                 "b200_max": int(max(its_b)), "b200_mean": float(np.mean(its_b)),
+                                 "ref64_total": int(sum(its_r)) if its_r else None,
+                                 "first_12_b200": its_b[:12], "first_12_ref64": its_r[:12]}
+    return out
+
+
 def _basin_name(A):
     im, jm, kb = A["u"].shape
     return f"{im}x{jm}x{kb} basin"
@@ -950,23 +1099,26 @@ def reference_cpu_sample(A, Sc, internal_steps=6, warm=1, reps=2, device="cpu", 
                       f"(reference PyTorch core {core_name}, {device}, after {warm} warm-up step)"}
 
 
-def reference_gpu_sample(A, Sc, device, internal_steps=12, warm=2, reps=2, core_name="implicit_p0_fixed"):
-    """The reference PyTorch core (eager mode, torch CG: the reference's
-    default SparsePhysics options) on this GPU, on the same basin: the
-    comparison the B200 core is built to beat on the same hardware."""
+def reference_gpu_sample(A, Sc, device, internal_steps=12, warm=2, reps=2, core_name="implicit_p0_fixed",
+                         physics_kw=None):
+    """The reference PyTorch core on this GPU, on the same basin, under the
+    SparsePhysics options ``physics_kw`` (default: eager mode, torch CG):
+    the comparison the B200 core is built to beat on the same hardware."""
     import torch
     core, rh = reference_core(A, Sc, device, core_name)
-    rh.advance(core, core_name, warm, device=device)
+    kw = physics_kw or {}
+    rh.advance(core, core_name, warm, device=device, **kw)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(reps):
-        rh.advance(core, core_name, internal_steps, device=device)
+        rh.advance(core, core_name, internal_steps, device=device, **kw)
     torch.cuda.synchronize()
     sec = time.perf_counter() - t0
     days = reps * internal_steps * float(core.dti) / 86400.0
     return {"value": days / sec, "unit": UNIT, "device": str(device),
             "sample": f"{reps} x {internal_steps} internal steps of the {_basin_name(A)} (reference PyTorch core "
-                      f"{core_name}, eager, after {warm} warm-up steps; wall clock around synchronised calls)"}
+                      f"{core_name}, {kw or 'eager, torch CG'}, after {warm} warm-up steps; wall clock around "
+                      "synchronised calls)"}
 
 
 def run_reference(args):

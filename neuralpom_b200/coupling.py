@@ -1,15 +1,15 @@
-"""Corrector coupling around the B200 step: the endpoint correction a
-neural model applies between physics intervals, with the reference's API
-(``src/neuralpom/hybrid/sparse_coupling.py:10-82``).
+"""The two physics operators of the corrector coupling on the B200 library:
+the equation of state and the baroclinic pressure gradient, as CUDA kernels
+with hand-written adjoints (``npom_dens``/``npom_dens_adjoint``,
+``npom_baropg``/``npom_baropg_adjoint``) behind ``torch.autograd.Function``.
 
-The state updates, budget projections and limits are a few reductions once
-per interval and stay in PyTorch (differentiable by autograd).  The two
-physics operators inside -- the equation of state and the baroclinic
-pressure gradient -- run as CUDA kernels with hand-written adjoints
-(``npom_dens``/``npom_dens_adjoint``, ``npom_baropg``/
-``npom_baropg_adjoint``).  The cores' ``dens()`` and ``baropg()`` methods
-use the same kernels, so the reference's own coupling functions also accept
-a B200 core.
+The cores' operator methods ``dens()`` and ``baropg()`` use them, which is
+all the reference's own coupling module needs: its ``eos``,
+``apply_joint_correction`` and ``pressure_velocity_error``
+(``src/neuralpom/hybrid/sparse_coupling.py:10-82``) run unchanged on a B200
+core and differentiate through these operators.  The rest of that module
+(increment scaling, budget projections, limits) is a few reductions per
+physics interval and stays the reference's PyTorch code.
 """
 from __future__ import annotations
 
@@ -18,11 +18,6 @@ import ctypes
 import torch
 
 from . import _abi
-
-OUTPUT_FIELDS = ("u", "v", "t", "s")
-LEVELS = 15
-OUTPUT_CHANNELS = 4 * LEVELS
-
 
 def _call(core):
     lib = _abi.load_library()
@@ -120,72 +115,3 @@ def eos(core, t, s):
     (sparse_coupling.py:10-15): DENS on levels < kb-1, the ghost level of
     the core's rho."""
     return _DensFunction.apply(core, t, s, core.rho)
-
-
-def volume_weights(core, field="t"):
-    """Cell volumes of the corrected levels (sparse_coupling.py:18-20)."""
-    mask = core.dum if field in ("u", "ub") else (core.dvm if field in ("v", "vb") else core.fsm)
-    return (core.art * mask * (core.h + core.et))[:, :, None] * core.dz[:LEVELS][None, None, :]
-
-
-def weighted_mse(x, y, w):
-    return ((x - y).square() * w).sum() / w.expand_as(x).sum().clamp_min(1e-20)
-
-
-def budget_project(increment, weights):
-    """Remove the volume-weighted mean of each level on the wet cells, so
-    the increment moves tracer within a layer and the physics keeps the
-    vertical budget (sparse_coupling.py:27-32)."""
-    level_mean = (increment * weights).sum((0, 1), keepdim=True) / weights.sum((0, 1), keepdim=True).clamp_min(1e-20)
-    return (increment - level_mean) * (weights > 0)
-
-
-def paired_limit(increments, scales, cap):
-    """One common factor for a pair of increments so that neither exceeds
-    cap scale units (sparse_coupling.py:35-39); returns the scaled pair and
-    the factor."""
-    peak = torch.stack([(x / sc).abs().amax() for x, sc in zip(increments, scales)]).amax()
-    factor = (cap / peak.clamp_min(cap)).clamp(max=1.0)
-    return [factor * x for x in increments], factor
-
-
-def apply_joint_correction(core, raw, scales, cap=5.0):
-    """Add a network's raw (60, im, jm) output to u, v, T, S and their
-    previous time levels (sparse_coupling.py:42-67): per-field scales,
-    depth-mean-free velocity increments, layer-budget-free tracer
-    increments, paired limits, then the EOS refresh.  Differentiable in
-    raw and in the state."""
-    if core.kbm1 != LEVELS or tuple(raw.shape) != (OUTPUT_CHANNELS, core.im, core.jm):
-        raise ValueError(f"Unexpected grid/output contract: {core.kbm1}, {tuple(raw.shape)}")
-    inc = {f: raw[n * LEVELS:(n + 1) * LEVELS].permute(1, 2, 0) * scales[f] for n, f in enumerate(OUTPUT_FIELDS)}
-    dz = core.dz[:LEVELS].view(1, 1, -1)
-    for f, mask in (("u", core.dum), ("v", core.dvm)):
-        inc[f] = (inc[f] - (inc[f] * dz).sum(2, keepdim=True) / dz.sum()) * mask[:, :, None]
-    w = volume_weights(core)
-    for f in ("t", "s"):
-        inc[f] = budget_project(inc[f], w)
-    (inc["t"], inc["s"]), factor = paired_limit([inc["t"], inc["s"]], [scales["t"], scales["s"]], cap)
-    (inc["u"], inc["v"]), _ = paired_limit([inc["u"], inc["v"]], [scales["u"], scales["v"]], cap)
-    for f, prev in (("u", "ub"), ("v", "vb"), ("t", "tb"), ("s", "sb")):
-        for name in (f, prev):
-            x = getattr(core, name)
-            # the ghost level keeps the core's value
-            setattr(core, name, torch.cat((x[:, :, :LEVELS] + inc[f], x[:, :, LEVELS:]), dim=2))
-    core.rho = eos(core, core.t, core.s)
-    return {"ts_limit_factor": factor, "t_budget": (w * inc["t"]).sum() / w.sum(),
-            "s_budget": (w * inc["s"]).sum() / w.sum()}
-
-
-def pressure_velocity_error(core, reference_t, reference_s):
-    """Velocity kick of the baroclinic pressure-gradient difference between
-    the core's (t, s) and a reference (t, s) on the core's geometry
-    (sparse_coupling.py:70-82): BAROPG is linear in rho at fixed geometry,
-    so it is evaluated once on the density difference with rmean = 0."""
-    drho = eos(core, core.t, core.s) - eos(core, reference_t, reference_s)
-    _, px, py = _BaropgFunction.apply(core, drho, torch.zeros_like(core.rmean), core.dt)
-    depth = core.h + core.etf
-    du = (depth + torch.roll(depth, 1, 0)) * core.aru
-    dv = (depth + torch.roll(depth, 1, 1)) * core.arv
-    kick_u = -2.0 * core.dti2 * px[:, :, :LEVELS] / du[:, :, None].clamp_min(1e-20)
-    kick_v = -2.0 * core.dti2 * py[:, :, :LEVELS] / dv[:, :, None].clamp_min(1e-20)
-    return kick_u * core.dum[:, :, None], kick_v * core.dvm[:, :, None]

@@ -1,15 +1,27 @@
-"""Corrector coupling on the B200 core (neuralpom_b200.coupling; the CUDA
-DENS/BAROPG operators with hand-written adjoints) against the reference's
-hybrid/sparse_coupling.py:10-82 under torch autograd (golden vectors):
-apply_joint_correction with the paired limiter engaged, and
-pressure_velocity_error."""
+"""Corrector coupling on the B200 core against the reference's autograd
+(golden vectors of hybrid/sparse_coupling.py:10-82): the reference's own
+coupling functions, run on a B200 core, whose dens()/baropg() methods are the
+CUDA DENS/BAROPG operators with hand-written adjoints
+(neuralpom_b200.coupling): apply_joint_correction with the paired limiter
+engaged, and pressure_velocity_error."""
 import numpy as np
 import pytest
 import torch
 
 from golden_io import golden_path
+from oracle import ref_harness as rh
 
+REF = rh.default_reference_path()
 pytestmark = pytest.mark.gpu
+
+
+def _sparse_coupling():
+    if REF is None:
+        pytest.skip("reference package not importable")
+    rh.import_reference(REF)
+    from neuralpom.hybrid import sparse_coupling
+    return sparse_coupling
+
 
 LEAVES = ("u", "ub", "v", "vb", "t", "tb", "s", "sb", "rho", "et", "etf", "dt")
 
@@ -36,7 +48,7 @@ def _rel(a, b):
 
 
 def test_gpu_apply_joint_correction_matches_reference():
-    from neuralpom_b200 import coupling
+    coupling = _sparse_coupling()
     z, A, Sc = _load()
     core, leaves = _core(A, Sc)
     raw = torch.tensor(z["jc__raw"], device="cuda", requires_grad=True)
@@ -63,7 +75,7 @@ def test_gpu_apply_joint_correction_matches_reference():
 
 
 def test_gpu_pressure_velocity_error_matches_reference():
-    from neuralpom_b200 import coupling
+    coupling = _sparse_coupling()
     z, A, Sc = _load()
     core, leaves = _core(A, Sc)
     ref_t = torch.tensor(z["pv__ref_t"], device="cuda", requires_grad=True)
