@@ -901,13 +901,14 @@ def fwd_adjoint_midtrain_batch(args, dev, members=8, reps=3):
 REF_FAST_MODE = {"acceleration": "strict_vertical_compiled", "cg_backend": "triton", "compiled_kernels": ("proft",)}
 
 
-def reference_modes(fn, core_name, where, **kw):
+def reference_modes(fn, kind, where, **kw):
     """``fn`` timed under the reference's default options (eager, torch CG)
-    and, for the implicit core on a GPU, under its compiled training setup;
+    and, for the implicit core (``kind``) on a GPU (``where``), under its
+    compiled training setup;
     the line reports the faster (the reference's best on this GPU) and
     every mode's figure."""
     modes = {"eager": {}}
-    if core_name != "explicit" and str(where) != "cpu":
+    if kind != "explicit" and str(where) != "cpu":
         modes["strict_vertical_compiled+triton_cg"] = REF_FAST_MODE
     out = {}
     for name, opts in modes.items():
