@@ -870,16 +870,20 @@ bool pcg_cluster_layout(const Ctx &c, ClusterLayout *out) {
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return false;
   const char *ctas = getenv("NPOM_PCG_CTAS");
   const bool prefer16 = ctas && std::strcmp(ctas, "16") == 0;
-  // the replicated-residual form (three cluster barriers per iteration)
-  // where its extra full-grid copy fits; NPOM_PCG=pushed keeps the
-  // pushed-residual form (four barriers) for comparisons
+  // the replicated-residual form where its extra full-grid copy fits, with
+  // its exchanges by bulk copies and mbarriers where the rows allow them;
+  // NPOM_PCG=sync keeps the replicated form with cluster barriers,
+  // NPOM_PCG=pushed the pushed-residual form (four barriers), for comparisons
   const bool spectral = c.k.eta_precond == NPOM_PRECOND_SPECTRAL;
   const bool allow_rep = spectral && !(env && std::strcmp(env, "pushed") == 0);
+  const bool allow_bulk = allow_rep && !(env && std::strcmp(env, "sync") == 0);
+  const bool forms[3][2] = {{true, true}, {true, false}, {false, false}};  // (replicated, bulk)
   for (bool sy_global : {false, true}) {
     for (int nc : {prefer16 ? 16 : 8, prefer16 ? 8 : 16}) {
-      for (bool rep : {true, false}) {
-        if (rep && !allow_rep) continue;
-        ClusterLayout L = cluster_layout(c.im, c.jm, nc, sy_global, rep);
+      for (const auto &f : forms) {
+        if ((f[0] && !allow_rep) || (f[1] && !allow_bulk)) continue;
+        ClusterLayout L = cluster_layout(c.im, c.jm, nc, sy_global, f[0], f[1]);
+        if (f[1] && !L.bulk) continue;
         if (L.fits && L.bytes() <= (size_t)optin) {
           *out = L;
           return true;

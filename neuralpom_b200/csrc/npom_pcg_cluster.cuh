@@ -73,16 +73,26 @@ struct ClusterLayout {
   // float offsets in dynamic shared memory
   int x, r, z, ap, rhs, p, zh, h4, c4, iart, ie, gr, gc, sxf, syf, t1f;
   int gap;         // full-grid copy of Ap (replicated-residual form), -1 when absent
+  int st1, st2;    // bulk form: the slab rows of Ap and of the half-transformed field at pitch gp
   int floats;
   bool fits;       // rows <= 16 and one column tile per warp
   bool sy_global;  // Sy read from global memory in the j-stages (no room for its fragments)
-  size_t red_doubles() const { return (size_t)kRedSlots * nc * kClusterWarps; }
-  size_t bytes() const { return (size_t)floats * sizeof(float) + red_doubles() * sizeof(double); }
+  bool bulk;       // exchanges by bulk copies and mbarriers (replicated form, nj % 4 == 0)
+  __host__ __device__ size_t red_doubles() const { return (size_t)kRedSlots * nc * kClusterWarps; }
+  // three mbarriers (one per exchange) after the reduction slots in the bulk form
+  size_t bytes() const {
+    return (size_t)floats * sizeof(float) + red_doubles() * sizeof(double) + (bulk ? 4 * sizeof(uint64_t) : 0);
+  }
 };
 
-inline ClusterLayout cluster_layout(int im, int jm, int nc, bool sy_global = false, bool replicated = false) {
+inline ClusterLayout cluster_layout(int im, int jm, int nc, bool sy_global = false, bool replicated = false,
+                                    bool bulk = false) {
   ClusterLayout L;
   L.sy_global = sy_global;
+  // the replicated and bulk forms keep Sy in shared memory (their loops are
+  // compiled for that placement only)
+  if (sy_global) replicated = bulk = false;
+  L.bulk = bulk && replicated && ((jm - 2) % 4 == 0);
   L.ni = im - 2;
   L.nj = jm - 2;
   L.nc = nc;
@@ -117,6 +127,8 @@ inline ClusterLayout cluster_layout(int im, int jm, int nc, bool sy_global = fal
   L.syf = sy_global ? -1 : take(L.nt * L.nt * 32 * 4);
   L.t1f = take(L.nt * 32 * 4);             // i-stage result as A fragments of the j-stage
   L.gap = replicated ? take(8 * L.kti * L.gp) : -1;  // full Ap, zero-padded like gr
+  L.st1 = L.bulk ? take(L.rows * L.gp) : -1;
+  L.st2 = L.bulk ? take(L.rows * L.gp) : -1;
   L.floats = o;
   return L;
 }
@@ -156,6 +168,124 @@ __device__ __forceinline__ double cl_block_total(double v, double *slot) {
   return t;
 }
 
+// ---- exchanges by bulk copies and mbarriers (the bulk form) ----------------
+// A producer hands data to every consumer with cp.async.bulk (shared::cta
+// -> shared::cluster) or st.async, both completing on the CONSUMER's
+// mbarrier with the number of bytes delivered; a consumer waits only for the
+// bytes it expects (mbarrier.try_wait with acquire at cluster scope).  No
+// thread issues the per-element remote stores, and no cluster barrier (with
+// its release fence over every outstanding remote store) is needed.  Every
+// wait is bounded: after kExchangeTimeoutNs the CTA records NPOM_DEV_TIMEOUT
+// and leaves the PCG loop.
+constexpr unsigned long long kExchangeTimeoutNs = 500000000ull;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// the shared::cluster address of the same offset in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t cluster_addr(uint32_t local, int rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local), "r"(rank));
+  return r;
+}
+
+__device__ __forceinline__ void mb_init(uint64_t *mb, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mb)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mb_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// this CTA's own arrival on its mbarrier for the current phase, with the
+// bytes that the phase's producers will deliver
+__device__ __forceinline__ void mb_expect(uint64_t *mb, uint32_t bytes) {
+  uint64_t state;
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
+               : "=l"(state)
+               : "r"(smem_u32(mb)), "r"(bytes)
+               : "memory");
+  (void)state;
+}
+
+__device__ __forceinline__ bool mb_try_wait(uint64_t *mb, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(mb)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// generic-proxy writes of this thread to shared memory, ordered before the
+// bulk copies (async proxy) issued after the next barrier
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void bulk_s2s(uint32_t dst_cluster, uint32_t src_cta, uint32_t bytes,
+                                         uint32_t mbar_cluster) {
+  asm volatile("cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(dst_cluster), "r"(src_cta), "r"(bytes), "r"(mbar_cluster)
+               : "memory");
+}
+
+__device__ __forceinline__ void st_async_f64(uint32_t dst_cluster, double v, uint32_t mbar_cluster) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b64 [%0], %1, [%2];"
+               ::"r"(dst_cluster), "l"((unsigned long long)__double_as_longlong(v)), "r"(mbar_cluster)
+               : "memory");
+}
+
+// Every thread waits for the phase of parity `parity` (bounded); the
+// outcome is made uniform over the CTA, so all its threads take the same
+// branch afterwards.  Returns false (and records NPOM_DEV_TIMEOUT) if a
+// thread of the CTA gave up.
+__device__ __forceinline__ bool xb_wait(uint64_t *mb, uint32_t parity, unsigned int *status) {
+  bool ok = mb_try_wait(mb, parity);
+  if (!ok) {
+    const unsigned long long t0 = global_ns();
+    for (unsigned n = 0;; ++n) {
+      if (mb_try_wait(mb, parity)) {
+        ok = true;
+        break;
+      }
+      if ((n & 63u) == 63u && global_ns() - t0 > kExchangeTimeoutNs) {
+        atomicOr(status, NPOM_DEV_TIMEOUT);
+        break;
+      }
+    }
+  }
+  return __syncthreads_or(ok ? 0 : 1) == 0;
+}
+
+// Warp partial of a dot product (the same butterfly as cl_push_partial),
+// stored by st.async into slot `slot` of every CTA, counted on that CTA's
+// mbarrier mb.
+__device__ __forceinline__ void xb_push_partial(double v, double *red, int slot, int nc, int rank, uint64_t *mb) {
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane < nc)
+    st_async_f64(cluster_addr(smem_u32(red + (slot * nc + rank) * kClusterWarps + w), lane), v,
+                 cluster_addr(smem_u32(mb), lane));
+}
+
+// The slab rows at src (pitch gp, nr rows) into rows a0.. of the full-grid
+// copy at dst in every CTA (one bulk copy per CTA, issued by one thread),
+// counted on the mbarrier mb of each.  The caller made src visible to the
+// async proxy and synchronised the CTA.
+__device__ __forceinline__ void xb_send_slab(const ClusterLayout &L, float *sm, int src, int dst, int a0, int nr,
+                                             uint64_t *mb) {
+  if (threadIdx.x != 0 || nr <= 0) return;
+  const uint32_t s = smem_u32(sm + src), d = smem_u32(sm + dst + a0 * L.gp), b = smem_u32(mb);
+  const uint32_t bytes = (uint32_t)(nr * L.gp * (int)sizeof(float));
+  for (int q = 0; q < L.nc; ++q) bulk_s2s(cluster_addr(d, q), s, bytes, cluster_addr(b, q));
+}
+
 // fetch halo rows of p from the neighbouring CTAs (zero outside the domain);
 // used for the initial residual and the final filter only
 __device__ __forceinline__ void cl_halo(cgx::cluster_group &cl, const ClusterLayout &L, float *sm, int rank, int nr) {
@@ -184,7 +314,8 @@ __device__ __forceinline__ void cl_halo(cgx::cluster_group &cl, const ClusterLay
 // ap = A p on the slab (p has its halo rows in place); returns this thread's
 // share of p.Ap when asked
 __device__ __forceinline__ double cl_spmv(const ClusterLayout &L, float *sm, float coeff, int nr, float *out,
-                                          bool dot_with_p) {
+                                          bool dot_with_p, int opitch = -1) {
+  const int op = opitch < 0 ? L.nj : opitch;
   const float *p = sm + L.p;
   const float4 *h4 = reinterpret_cast<const float4 *>(sm + L.h4);
   const float4 *c4 = reinterpret_cast<const float4 *>(sm + L.c4);
@@ -205,7 +336,7 @@ __device__ __forceinline__ double cl_spmv(const ClusterLayout &L, float *sm, flo
     float fs = h.w * (ev - e_s) * cc.w;
     float div = (fe - fw + fn - fs) * sm[L.iart + e];
     float a = ev - coeff * div;
-    out[e] = a;
+    out[ra * op + b] = a;
     if (dot_with_p) acc += (double)ev * (double)a;
   }
   return acc;
@@ -400,6 +531,67 @@ __device__ __forceinline__ double cl_precondition(cgx::cluster_group &cl, const 
   return rz;
 }
 
+// Bulk form of cl_precondition (spectral only): the half-transformed slab
+// goes to every CTA's gc by bulk copies counted on mbarrier mb[1]; r is read
+// from the whole-residual copy gr.  Writes z (no halo push: the caller's
+// r.z exchange carries the halo rows) and returns this thread's share of
+// r.z.  `failed` is set (uniformly over the CTA) if the wait gave up.
+template <bool SYG>
+__device__ __forceinline__ double cl_precondition_bulk(const ClusterLayout &L, float *sm, int nr, int a0,
+                                                       float inverse_scale, const float *syg, uint64_t *mb,
+                                                       unsigned &ph1, unsigned int *status, bool &failed) {
+  const int nj = L.nj, gp = L.gp;
+  float *z = sm + L.z;
+  const float *gr = sm + L.gr;
+  const float *ie = sm + L.ie;
+  float *stage = sm + L.st2;
+  double rz = 0.0;
+  cl_dst_i(L, sm, sm + L.gr);
+  __syncthreads();
+  cl_dst_j<SYG>(L, sm, nr, syg, [&](int ra, int l, float acc) { stage[ra * gp + l] = acc * ie[ra * nj + l]; });
+  fence_proxy_async_smem();
+  __syncthreads();
+  if (threadIdx.x == 0) mb_expect(mb + 1, (uint32_t)(L.ni * gp * (int)sizeof(float)));
+  xb_send_slab(L, sm, L.st2, L.gc, a0, nr, mb + 1);
+  if (!xb_wait(mb + 1, ph1, status)) failed = true;
+  ph1 ^= 1u;
+  if (failed) return 0.0;
+  cl_dst_i(L, sm, sm + L.gc);
+  __syncthreads();
+  cl_dst_j<SYG>(L, sm, nr, syg, [&](int ra, int l, float acc) {
+    const float zv = acc / inverse_scale;
+    z[ra * nj + l] = zv;
+    rz += (double)gr[(a0 + ra) * gp + l] * (double)zv;
+  });
+  return rz;
+}
+
+// Bulk form of the r.z exchange: the z rows that the neighbours keep as
+// halo (first row up, last row down) and every warp's r.z partial, counted
+// on mbarrier mb[2]; the caller wrote z in every thread.
+__device__ __forceinline__ void xb_exchange_rz(const ClusterLayout &L, float *sm, double rz, double *red, int nr,
+                                               int rank, bool has_up, bool has_down, uint64_t *mb, unsigned &ph2,
+                                               unsigned int *status, bool &failed) {
+  const int nj = L.nj, nc = L.nc;
+  fence_proxy_async_smem();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const uint32_t row = (uint32_t)(nj * (int)sizeof(float));
+    mb_expect(mb + 2, (uint32_t)(nc * kClusterWarps * (int)sizeof(double)) + (has_up ? row : 0u) +
+                          (has_down ? row : 0u));
+    const uint32_t bar = smem_u32(mb + 2);
+    if (has_up)  // first own row -> the lower halo of the CTA above
+      bulk_s2s(cluster_addr(smem_u32(sm + L.zh + nj), rank - 1), smem_u32(sm + L.z), row,
+               cluster_addr(bar, rank - 1));
+    if (has_down)  // last own row -> the upper halo of the CTA below
+      bulk_s2s(cluster_addr(smem_u32(sm + L.zh), rank + 1), smem_u32(sm + L.z + (nr - 1) * nj), row,
+               cluster_addr(bar, rank + 1));
+  }
+  xb_push_partial(rz, red, 2, nc, rank, mb + 2);
+  if (!xb_wait(mb + 2, ph2, status)) failed = true;
+  ph2 ^= 1u;
+}
+
 // The rhs scale of the adjoint solve from its float bits (clamp_min(1); a
 // NaN gives 1, as on the host), and the PCG's absolute tolerance.
 __device__ __forceinline__ float adj_scale_of(const unsigned int *bits) {
@@ -416,6 +608,13 @@ template <bool SYG>
 __device__ __forceinline__ void pcg_cluster_body(const Ctx &c, const ClusterLayout &L, float *sm, int with_rhs,
                                                  int with_post) {
   double *red = reinterpret_cast<double *>(sm + L.floats);
+  uint64_t *mb = reinterpret_cast<uint64_t *>(red + L.red_doubles());  // bulk form: three mbarriers
+  unsigned ph0 = 0u, ph1 = 0u, ph2 = 0u;
+  bool failed = false;
+  if (L.bulk && threadIdx.x == 0) {
+    for (int k = 0; k < 3; ++k) mb_init(mb + k, 1u);
+    mb_init_fence();  // visible cluster-wide before the set-up's first cluster barrier
+  }
   cgx::cluster_group cl = cgx::this_cluster();
   const int rank = (int)cl.block_rank();
   const int im = c.im, jm = c.jm, nj = L.nj, nc = L.nc;
@@ -463,6 +662,7 @@ __device__ __forceinline__ void pcg_cluster_body(const Ctx &c, const ClusterLayo
     if (spectral) sm[L.ie + e] = c.W[NPOM_W_inv_eigs][(size_t)(a0 + ra) * nj + b];
   }
   for (int b = threadIdx.x; b < 2 * nj; b += blockDim.x) sm[L.zh + b] = 0.0f;
+  if (L.bulk) fence_proxy_async_smem();
   if (spectral) {
     const float *sx = c.W[NPOM_W_sx], *sy = c.W[NPOM_W_sy];
     const int ni = L.ni;
@@ -471,6 +671,15 @@ __device__ __forceinline__ void pcg_cluster_body(const Ctx &c, const ClusterLayo
       sm[L.gr + e] = 0.0f;
       sm[L.gc + e] = 0.0f;
       if (L.gap >= 0) sm[L.gap + e] = 0.0f;
+    }
+    if (L.bulk) {
+      // staging rows at pitch gp: the padding columns stay zero (they are
+      // copied into the zero-padded full-grid copies)
+      for (int e = threadIdx.x; e < L.rows * L.gp; e += blockDim.x) {
+        sm[L.st1 + e] = 0.0f;
+        sm[L.st2 + e] = 0.0f;
+      }
+      fence_proxy_async_smem();  // these buffers are written by bulk copies from here on
     }
     // Sx rows of the slab as split A fragments (zero outside the slab)
     for (int f = threadIdx.x; f < L.kti * 32; f += blockDim.x) {
@@ -524,9 +733,18 @@ __device__ __forceinline__ void pcg_cluster_body(const Ctx &c, const ClusterLayo
   cl_push_partial(cl, rr, red, 3, nc, rank);
   cl.sync();  // r pushed everywhere; neighbours' x halo reads done
   const double rs0 = cl_partial_total(red, 3, nc);
-  double rz = cl_precondition<SYG>(cl, L, sm, nr, rank, a0, c.k.inverse_scale, spectral, c.W[NPOM_W_sy]);
-  cl_push_partial(cl, rz, red, 2, nc, rank);
-  cl.sync();  // z halo rows and r.z partials in place
+  double rz = 0.0;
+  if constexpr (!SYG) {
+    if (L.bulk) {
+      rz = cl_precondition_bulk<SYG>(L, sm, nr, a0, c.k.inverse_scale, c.W[NPOM_W_sy], mb, ph1, c.status, failed);
+      if (!failed) xb_exchange_rz(L, sm, rz, red, nr, rank, has_up, has_down, mb, ph2, c.status, failed);
+    }
+  }
+  if (!L.bulk) {
+    rz = cl_precondition<SYG>(cl, L, sm, nr, rank, a0, c.k.inverse_scale, spectral, c.W[NPOM_W_sy]);
+    cl_push_partial(cl, rz, red, 2, nc, rank);
+    cl.sync();  // z halo rows and r.z partials in place
+  }
   double rho_old = cl_partial_total(red, 2, nc);
   float *p = sm + L.p;
   for (int e = threadIdx.x; e < n; e += blockDim.x) p[nj + e] = sm[L.z + e];
@@ -539,7 +757,63 @@ __device__ __forceinline__ void pcg_cluster_body(const Ctx &c, const ClusterLayo
   int its = 0;
   bool converged = false;
   __syncthreads();  // p and its halo rows complete in this CTA
-  const bool replicated = spectral && L.gap >= 0;
+  const bool replicated = spectral && L.gap >= 0 && !L.bulk;
+  if constexpr (!SYG) {
+  for (int it = 1; L.bulk && !failed && it <= c.k.eta_max_iter; ++it) {
+    // ---- bulk form: the replicated-residual iteration, exchanges by bulk
+    // copies counted on mbarriers (no cluster barrier in the loop)
+    double pap = cl_spmv(L, sm, coeff, nr, sm + L.st1, true, L.gp);
+    fence_proxy_async_smem();
+    __syncthreads();  // the Ap slab complete (and visible to the async proxy) before it is sent
+    if (threadIdx.x == 0)
+      mb_expect(mb, (uint32_t)(L.ni * L.gp * (int)sizeof(float) + nc * kClusterWarps * (int)sizeof(double)));
+    xb_send_slab(L, sm, L.st1, L.gap, a0, nr, mb);
+    xb_push_partial(pap, red, 0, nc, rank, mb);
+    if (!xb_wait(mb, ph0, c.status)) failed = true;
+    ph0 ^= 1u;
+    if (failed) break;
+    const double denom = cl_partial_total(red, 0, nc);
+    const float alpha = (float)(rho_old / (denom + 1e-30));
+    for (int e = threadIdx.x; e < n; e += blockDim.x) sm[L.x + e] = sm[L.x + e] + alpha * p[nj + e];
+    float4 *gr4 = reinterpret_cast<float4 *>(sm + L.gr);
+    const float4 *ga4 = reinterpret_cast<const float4 *>(sm + L.gap);
+    double rs = 0.0;
+    for (int e4 = threadIdx.x; e4 < 2 * L.kti * L.gp; e4 += blockDim.x) {
+      float4 rv = gr4[e4];
+      const float4 av = ga4[e4];
+      rv.x = rv.x - alpha * av.x;
+      rv.y = rv.y - alpha * av.y;
+      rv.z = rv.z - alpha * av.z;
+      rv.w = rv.w - alpha * av.w;
+      gr4[e4] = rv;
+      rs += (double)rv.x * (double)rv.x;
+      rs += (double)rv.y * (double)rv.y;
+      rs += (double)rv.z * (double)rv.z;
+      rs += (double)rv.w * (double)rv.w;
+    }
+    const double rsn = cl_block_total(rs, red + (size_t)4 * nc * kClusterWarps);  // gr complete after this
+    its = it;
+    if (rsn <= tol_sq || rsn <= rel_sq || rsn <= 1e-30) {
+      converged = true;
+      break;
+    }
+    rz = cl_precondition_bulk<SYG>(L, sm, nr, a0, c.k.inverse_scale, c.W[NPOM_W_sy], mb, ph1, c.status, failed);
+    if (failed) break;
+    xb_exchange_rz(L, sm, rz, red, nr, rank, has_up, has_down, mb, ph2, c.status, failed);
+    if (failed) break;
+    const double rho_new = cl_partial_total(red, 2, nc);
+    const float beta = (float)(rho_new / (rho_old + 1e-30));
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+      float *pp = p + nj + e;
+      *pp = *pp * beta + sm[L.z + e];
+    }
+    for (int b = threadIdx.x; b < nj; b += blockDim.x) {
+      if (has_up) p[b] = p[b] * beta + sm[L.zh + b];
+      if (has_down) p[(nr + 1) * nj + b] = p[(nr + 1) * nj + b] * beta + sm[L.zh + nj + b];
+    }
+    rho_old = rho_new;
+    __syncthreads();
+  }
   for (int it = 1; replicated && it <= c.k.eta_max_iter; ++it) {
     // ---- replicated-residual form: three cluster barriers per iteration
     double pap = cl_spmv(L, sm, coeff, nr, sm + L.ap, true);
@@ -593,7 +867,8 @@ __device__ __forceinline__ void pcg_cluster_body(const Ctx &c, const ClusterLayo
     rho_old = rho_new;
     __syncthreads();
   }
-  for (int it = 1; !replicated && it <= c.k.eta_max_iter; ++it) {
+  }  // !SYG: bulk and replicated forms
+  for (int it = 1; !replicated && !L.bulk && it <= c.k.eta_max_iter; ++it) {
     // ---- pushed-residual form: four cluster barriers per iteration
     double pap = cl_spmv(L, sm, coeff, nr, sm + L.ap, true);
     cl_push_partial(cl, pap, red, 0, nc, rank);
