@@ -109,10 +109,13 @@ inline ClusterLayout cluster_layout(int im, int jm, int nc, bool sy_global = fal
     o += (n + 3) & ~3;
     return at;
   };
+  // bulk form: r and ap are the staging rows of its exchanges after the
+  // set-up (pitch gp), so they hold rows*gp floats
+  const int rstage = L.bulk ? L.rows * L.gp : rn;
   L.x = take(rn);
-  L.r = take(rn);
+  L.r = take(rstage);
   L.z = take(rn);
-  L.ap = take(rn);
+  L.ap = take(rstage);
   L.rhs = take(rn);
   L.p = take((L.rows + 2) * L.nj);
   L.zh = take(2 * L.nj);
@@ -127,8 +130,8 @@ inline ClusterLayout cluster_layout(int im, int jm, int nc, bool sy_global = fal
   L.syf = sy_global ? -1 : take(L.nt * L.nt * 32 * 4);
   L.t1f = take(L.nt * 32 * 4);             // i-stage result as A fragments of the j-stage
   L.gap = replicated ? take(8 * L.kti * L.gp) : -1;  // full Ap, zero-padded like gr
-  L.st1 = L.bulk ? take(L.rows * L.gp) : -1;
-  L.st2 = L.bulk ? take(L.rows * L.gp) : -1;
+  L.st1 = L.bulk ? L.ap : -1;  // Ap rows sent to every CTA's gap
+  L.st2 = L.bulk ? L.r : -1;   // half-transformed rows sent to every CTA's gc
   L.floats = o;
   return L;
 }
@@ -672,15 +675,7 @@ __device__ __forceinline__ void pcg_cluster_body(const Ctx &c, const ClusterLayo
       sm[L.gc + e] = 0.0f;
       if (L.gap >= 0) sm[L.gap + e] = 0.0f;
     }
-    if (L.bulk) {
-      // staging rows at pitch gp: the padding columns stay zero (they are
-      // copied into the zero-padded full-grid copies)
-      for (int e = threadIdx.x; e < L.rows * L.gp; e += blockDim.x) {
-        sm[L.st1 + e] = 0.0f;
-        sm[L.st2 + e] = 0.0f;
-      }
-      fence_proxy_async_smem();  // these buffers are written by bulk copies from here on
-    }
+    if (L.bulk) fence_proxy_async_smem();  // gc and gap are written by bulk copies from here on
     // Sx rows of the slab as split A fragments (zero outside the slab)
     for (int f = threadIdx.x; f < L.kti * 32; f += blockDim.x) {
       const int kt = f >> 5, lane = f & 31, g = lane >> 2, t = lane & 3;
@@ -736,6 +731,15 @@ __device__ __forceinline__ void pcg_cluster_body(const Ctx &c, const ClusterLayo
   double rz = 0.0;
   if constexpr (!SYG) {
     if (L.bulk) {
+      // the set-up is done with the r and ap slabs: from here on they are the
+      // staging rows (pitch gp) of the exchanges, whose padding columns must
+      // stay zero (they land in the zero-padded full-grid copies)
+      for (int e = threadIdx.x; e < L.rows * L.gp; e += blockDim.x) {
+        sm[L.st1 + e] = 0.0f;
+        sm[L.st2 + e] = 0.0f;
+      }
+      fence_proxy_async_smem();
+      __syncthreads();
       rz = cl_precondition_bulk<SYG>(L, sm, nr, a0, c.k.inverse_scale, c.W[NPOM_W_sy], mb, ph1, c.status, failed);
       if (!failed) xb_exchange_rz(L, sm, rz, red, nr, rank, has_up, has_down, mb, ph2, c.status, failed);
     }
