@@ -98,6 +98,7 @@ def parse():
     ap.add_argument("--ref-device", default="cpu")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the per-field error against a float64 reference day")
+    ap.add_argument("--no-batch-tune", action="store_true", help="batch workload: the library's launch rules only")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--members", type=int, default=8,
                     help="ensemble members advanced concurrently on one GPU for the 'ensemble' key (1 = skip)")
@@ -1221,7 +1222,7 @@ def batch_summary(args):
     return {"value": out["value"], "unit": out["unit"], "ms_per_step": out["ms_per_step"], "steps": 1,
             "warmup": 1, "workload": out["config"]["workload"], "gpu_launches": out["gpu_launches"],
             "hbm_frac": out["roofline"]["frac"], "reference_gpu_loop": ref["value"] if ref else None,
-            "clocks": out["clocks"]}
+            "clocks": out["clocks"], "autotune": out["autotune"]}
 
 
 def batch_measure(args):
@@ -1229,13 +1230,10 @@ def batch_measure(args):
         if os.environ.get("NPOM_BATCH_SUBCYCLE") == "coop":
             # two batches that both launch cooperative grids share one stream
             args.batch_streams = 1
-        else:
-            # only the semi-implicit batch launches a cooperative grid (the
-            # PCG of its largest members); capping its blocks per member
-            # leaves SMs to the explicit batch on the other stream.  56 is
-            # two DST-tile rounds for the 177x161 members (110 tiles):
-            # measured best of 40 / 56 / 64 / 112 for this mix of grids
-            os.environ.setdefault("NPOM_BATCH_PCG_BLOCKS", "56")
+        # otherwise only the semi-implicit batch launches a cooperative grid
+        # (the PCG of its largest members); the autotuner picks the cap on
+        # its blocks per member, which leaves SMs to the explicit batch on
+        # the other stream (npom_tuning.batch_pcg_blocks)
     if args.batch_mode == "streams":
         # members run concurrently: the explicit subcycle runs on one cluster
         # per member (up to four cells per thread), never as a cooperative
@@ -1336,16 +1334,75 @@ def batch_measure(args):
     for _ in range(args.warmup):
         advance(lambda mb: 4)
     torch.cuda.synchronize(dev)
-    total_ms, launches = 0.0, 0
-    with ClockSampler(local) as clk:
+
+    def set_tuning(tuning):
+        # tuning: {(core name, knob): value}; members of one core share it
+        for name, mbs in groups.items():
+            t = {k: v for (g, k), v in tuning.items() if g == name and v}
+            for mb in mbs:
+                mb["core"].tuning = t or None
+
+    def timed_day():
+        total, n = 0.0, 0
         for _ in range(args.steps):
             l2_flush(flush)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(main_stream)
-            launches += advance(steps_of)
+            n += advance(steps_of)
             b.record(main_stream)
             torch.cuda.synchronize(dev)
-            total_ms += a.elapsed_time(b)
+            total += a.elapsed_time(b)
+        return total, n
+
+    tune_info = None
+    if args.batch_mode == "launch" and not args.no_batch_tune:
+        # the autotuner over both batches together (they share the GPU):
+        # one simulated hour of every member per candidate, median of 2
+        from neuralpom_b200 import autotune
+        space = {}
+        for name, mbs in groups.items():
+            for k, vals in autotune.space_for(mbs[0]["core"], batch=True).items():
+                if k in ("pcg_form",) or (k == "subcycle_form" and args.batch_streams == 2):
+                    continue  # cooperative grids stay with the rules on shared SMs
+                space[(name, k)] = vals
+
+        def measure(tuning):
+            set_tuning(tuning)
+            try:
+                advance(lambda mb: max(1, mb["nday"] // 24))
+                ts = []
+                for _ in range(2):
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record(main_stream)
+                    advance(lambda mb: max(1, mb["nday"] // 24))
+                    b.record(main_stream)
+                    torch.cuda.synchronize(dev)
+                    ts.append(a.elapsed_time(b))
+            except Exception:
+                return float("inf")
+            bad = 0
+            for mb in members:
+                bits, _ = mb["core"].read_status(0)
+                bad |= bits & (_abi.DEV_TIMEOUT | _abi.DEV_VMAX | _abi.DEV_NONFINITE)
+            return float("inf") if bad else statistics.median(ts)
+
+        log = []
+        t0 = time.perf_counter()
+        best, t_best, t_rule = autotune.search(measure, space, log=log)
+        set_tuning({})
+        rule_ms, _ = timed_day()
+        set_tuning(best)
+        tune_info = {"tuning": {f"{g}.{k}": v for (g, k), v in best.items()},
+                     "rule_value": sum(steps_of(mb) * float(mb["core"].dti) / 86400.0 for mb in members) * args.steps
+                     / (rule_ms / 1000.0),
+                     "hour_ms_rule": t_rule, "hour_ms_tuned": t_best, "candidates": len(log),
+                     "search_s": time.perf_counter() - t0,
+                     "note": "coordinate descent over npom_tuning (A1/B5 forms and tile rows, column form, PCG "
+                             "CTA count and cooperative block cap, per core batch); rule_value: the library's "
+                             "rules, no cap"}
+    total_ms, launches = 0.0, 0
+    with ClockSampler(local) as clk:
+        total_ms, launches = timed_day()
     for mb in members:
         bits, _ = mb["core"].read_status(0)
         if bits & (_abi.DEV_TIMEOUT | _abi.DEV_VMAX | _abi.DEV_NONFINITE):
@@ -1391,7 +1448,7 @@ def batch_measure(args):
                      "peak_source": src, "traffic": None, "algorithmic_bytes": nbytes,
                      "note": "whole batch: algorithmic bytes of every member's steps over the device time"},
         "reference_gpu_loop": ref, "cpu_baseline": None, "e2e": None, "gpu_launches": launches,
-        "clocks": clk.summary(),
+        "clocks": clk.summary(), "autotune": tune_info,
     }
     for mb in members:
         mb["core"] = None

@@ -101,6 +101,28 @@ typedef struct npom_workspace {
 /* ------------------------------------------------------------------ */
 /* Scalar settings (the Python attributes of the reference BaseCore).  */
 /* ------------------------------------------------------------------ */
+/* Launch shapes of the step (the autotuner's search space).  Every form
+ * computes the same values: bit for bit, except the cooperative-grid PCG,
+ * whose FP64 dot products are summed over its blocks (equal to rounding).
+ * 0 in every field keeps the library's rules; the NPOM_* environment
+ * switches (comparisons) take precedence over these fields.  No
+ * counterpart in the reference, whose PyTorch step has no launch shapes. */
+typedef struct npom_tuning {
+  int32_t a1_form;             /* A1 (advct): 0 rule (tiles from 16384 cells), 1 points, 2 flux-once tiles */
+  int32_t b5_form;             /* B5 (advt1): the same choices                                           */
+  int32_t tile_blocks_per_sm;  /* A1/B5 tiles: rows per tile for about this many blocks per SM (0: 16) */
+  int32_t column_form;         /* kb = 16 column phases: 0 rule (lanes; PROFT one thread per column
+                                  from 16384 columns), 1 lanes everywhere, 2 one thread per column     */
+  int32_t subcycle_form;       /* explicit subcycle: 0 rule, 1 one cluster (up to 16384 cells),
+                                  2 grid barrier, 3 one launch per substep phase                        */
+  int32_t pcg_form;            /* 0 rule (cluster: bulk, replicated, pushed; else cooperative grid),
+                                  1 pushed-residual cluster, 2 replicated cluster with cluster
+                                  barriers, 3 cooperative grid                                          */
+  int32_t pcg_ctas;            /* cluster PCG: 0 rule (8 CTAs first), 16 (16 CTAs first)               */
+  int32_t batch_pcg_blocks;    /* npom_step_batch: cap on each member's cooperative-PCG blocks (0 none) */
+  int32_t reserved[2];
+} npom_tuning;
+
 typedef struct npom_params {
   int32_t device;          /* CUDA device ordinal the pointers live on     */
   int32_t im, jm, kb;
@@ -121,6 +143,7 @@ typedef struct npom_params {
   double sw;               /* MPDATA antidiffusion weight (nadv 2)         */
   int32_t nitera;          /* MPDATA iterations (nadv 2)                   */
   int32_t pad0;
+  npom_tuning tuning;      /* launch shapes (all zero: the library's rules) */
 } npom_params;
 
 enum { NPOM_CORE_EXPLICIT = 0, NPOM_CORE_IMPLICIT = 1 };

@@ -66,6 +66,16 @@ def ws_shape(name, im, jm):
     return (im, jm)
 
 
+TUNING_FIELDS = ("a1_form", "b5_form", "tile_blocks_per_sm", "column_form", "subcycle_form", "pcg_form", "pcg_ctas",
+                 "batch_pcg_blocks")
+
+
+class NpomTuning(ctypes.Structure):
+    """Launch shapes of the step (``npom_tuning``): all zero keeps the
+    library's rules."""
+    _fields_ = [(n, ctypes.c_int32) for n in TUNING_FIELDS] + [("reserved", ctypes.c_int32 * 2)]
+
+
 class NpomParams(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int32) for n in (
         "device", "im", "jm", "kb", "core", "isplit", "ispadv", "nbct", "nbcs", "ntp", "mode", "nadv",
@@ -75,7 +85,7 @@ class NpomParams(ctypes.Structure):
             "small", "kappa", "rhoref", "tbias", "sbias", "vmaxl", "hmax", "rfe", "rfw", "rfn", "rfs", "aam_min",
             "pi", "eta_tol", "eta_rel_tol", "barotropic_shapiro", "tracer_shapiro", "velocity_shapiro",
             "wind_tau0", "vmix", "period", "inverse_scale", "sw")] + [
-        ("nitera", ctypes.c_int32), ("pad0", ctypes.c_int32)]
+        ("nitera", ctypes.c_int32), ("pad0", ctypes.c_int32), ("tuning", NpomTuning)]
 
 
 class NpomWorkspace(ctypes.Structure):

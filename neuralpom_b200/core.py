@@ -55,6 +55,9 @@ class B200Core:
         self._ws = None
         self._ws_key = None
         self._ws_geo = None
+        # launch shapes of the step (npom_tuning fields; None: the library's
+        # rules), e.g. from neuralpom_b200.autotune
+        self.tuning = None
         self._eta_solver_iteration_history = []
         self._eta_adjoint_iteration_history = []
 

@@ -225,9 +225,12 @@ constexpr size_t kBatchPlanCache = 16;
 // kernels launched by the last npom_step_batch call of this process
 long long g_batch_launches = 0;
 
-bool batch_subcycle_coop() {
+// the batched explicit subcycle as one cooperative launch: NPOM_BATCH_SUBCYCLE
+// =coop, or the grid-barrier subcycle form in the first member's tuning
+bool batch_subcycle_coop(const Ctx &c0) {
   const char *env = getenv("NPOM_BATCH_SUBCYCLE");
-  return env && std::strcmp(env, "coop") == 0;
+  if (env) return std::strcmp(env, "coop") == 0;
+  return c0.tune.subcycle_form == 2;
 }
 
 // blocks of a cooperative launch of fn dealt to the members in proportion to
@@ -297,15 +300,18 @@ cudaError_t make_batch_plan(const std::vector<Ctx> &ctx, int core, BatchPlan *P)
   // per tile: about 16 tiles per SM over the whole batch
   {
     const char *ea = getenv("NPOM_A1"), *eb = getenv("NPOM_B5");
-    P->a1_tiles = c0.kb == 16 && !(ea && std::strcmp(ea, "points") == 0);
-    P->b5_tiles = c0.kb == 16 && c0.k.mode != 4 && c0.k.nadv != 2 && !(eb && std::strcmp(eb, "points") == 0);
+    const bool a1_points = ea ? std::strcmp(ea, "points") == 0 : c0.tune.a1_form == 1;
+    const bool b5_points = eb ? std::strcmp(eb, "points") == 0 : c0.tune.b5_form == 1;
+    P->a1_tiles = c0.kb == 16 && !a1_points;
+    P->b5_tiles = c0.kb == 16 && c0.k.mode != 4 && c0.k.nadv != 2 && !b5_points;
+    const int per_sm = c0.tune.tile_blocks_per_sm > 0 ? c0.tune.tile_blocks_per_sm : 16;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     for (int g = 0; g < 2; ++g) {
       const int cols = g == 0 ? kA1Cols : kB5Cols;
       size_t rows = 0;
       for (int m = 0; m < nm; ++m) rows += (size_t)ctx[m].im * ((ctx[m].jm + cols - 1) / cols);
-      const int ichunk = std::max(2, (int)((rows + 16 * (size_t)sms - 1) / (16 * (size_t)sms)));
+      const int ichunk = std::max(2, (int)((rows + per_sm * (size_t)sms - 1) / (per_sm * (size_t)sms)));
       T->tile_ichunk[g] = ichunk;
       const int S = g == 0 ? BS_A1T : BS_B5T;
       int at = 0;
@@ -335,7 +341,7 @@ cudaError_t make_batch_plan(const std::vector<Ctx> &ctx, int core, BatchPlan *P)
     T->start[S][nm] = at;
     P->blocks[S] = at;
   }
-  P->sub_req = batch_subcycle_coop();
+  P->sub_req = batch_subcycle_coop(c0);
   if (core == NPOM_CORE_EXPLICIT) {
     P->sub_coop = P->sub_req;
     if (P->sub_coop) {
@@ -408,7 +414,8 @@ cudaError_t make_batch_plan(const std::vector<Ctx> &ctx, int core, BatchPlan *P)
     // NPOM_BATCH_PCG_BLOCKS caps the blocks of each member's cooperative
     // solve (its barrier waits hold their SMs)
     const char *cap_env = getenv("NPOM_BATCH_PCG_BLOCKS");
-    const int per_member = cap_env ? std::max(1, atoi(cap_env)) : NPOM_MAX_COOP_BLOCKS;
+    const int cap = cap_env ? std::max(1, atoi(cap_env)) : c0.tune.batch_pcg_blocks;
+    const int per_member = cap > 0 ? std::min(cap, NPOM_MAX_COOP_BLOCKS) : NPOM_MAX_COOP_BLOCKS;
     if (!batch_coop_shares((const void *)kb_pcg, coop, work, T->start[BS_PCG], &total, per_member))
       return cudaErrorInvalidValue;
     T->count[BS_PCG] = (int)coop.size();
@@ -613,7 +620,7 @@ npom_status run_batch_steps(int nm, const npom_params *const *p, float *const *c
   cudaStream_t s = (cudaStream_t)stream;
   std::vector<Ctx> ctx(nm);
   for (int m = 0; m < nm; ++m) ctx[m] = make_ctx(p[m], fields[m], ws[m]);
-  const bool sub_req = batch_subcycle_coop();
+  const bool sub_req = batch_subcycle_coop(ctx[0]);
   std::lock_guard<std::mutex> lock(g_batch_mutex);
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return NPOM_ERR_CUDA;

@@ -68,6 +68,7 @@ struct Ctx {
   const unsigned int *tol_scale_bits;
   float ramp;      // per step
   int do_internal; // per step: 0 on the first step from time0 == 0
+  npom_tuning tune;  // launch shapes (host-side decisions only)
 };
 
 NPOM_HD float ldc(const Ctx &c, const float *p) {

@@ -117,6 +117,7 @@ inline Ctx make_ctx(const npom_params *p, float *const *fields, const npom_works
   c.k = make_consts(*p);
   c.ramp = 1.0f;
   c.do_internal = 1;
+  c.tune = p->tuning;
   return c;
 }
 

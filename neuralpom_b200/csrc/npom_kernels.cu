@@ -833,7 +833,8 @@ void launch_points(const Ctx &c, cudaStream_t s) {
 bool lanes_enabled(const Ctx &c) {
   if (c.kb != KL) return false;
   const char *env = getenv("NPOM_LANES");
-  return !(env && std::strcmp(env, "0") == 0);
+  if (env) return std::strcmp(env, "0") != 0;
+  return c.tune.column_form != 2;
 }
 
 // Columns from which PROFT runs one thread per column: its lane form issues
@@ -845,7 +846,8 @@ constexpr size_t kProftThreadColumns = 16384;
 template <int PH>
 void launch_cols(const Ctx &c, cudaStream_t s) {
   size_t n = (size_t)c.im * c.jm;
-  if (lanes_enabled(c) && !(PH == CP_B6 && n >= kProftThreadColumns)) {
+  const bool proft_threads = PH == CP_B6 && n >= kProftThreadColumns && c.tune.column_form != 1;
+  if (lanes_enabled(c) && !proft_threads) {
     k_lanes<PH><<<blocks_for(n * KL, kThreads), kThreads, 0, s>>>(c);
   } else {
     k_cols<PH><<<blocks_for(n, 128), 128, 0, s>>>(c);
@@ -865,18 +867,21 @@ void launch_cells(const Ctx &c, cudaStream_t s) {
 bool pcg_cluster_layout(const Ctx &c, ClusterLayout *out) {
   const char *env = getenv("NPOM_PCG");
   if (env && std::strcmp(env, "coop") == 0) return false;
+  if (!env && c.tune.pcg_form == 3) return false;
   int dev = 0, optin = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return false;
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return false;
   const char *ctas = getenv("NPOM_PCG_CTAS");
-  const bool prefer16 = ctas && std::strcmp(ctas, "16") == 0;
+  const bool prefer16 = ctas ? std::strcmp(ctas, "16") == 0 : c.tune.pcg_ctas == 16;
   // the replicated-residual form where its extra full-grid copy fits, with
   // its exchanges by bulk copies and mbarriers where the rows allow them;
   // NPOM_PCG=sync keeps the replicated form with cluster barriers,
   // NPOM_PCG=pushed the pushed-residual form (four barriers), for comparisons
   const bool spectral = c.k.eta_precond == NPOM_PRECOND_SPECTRAL;
-  const bool allow_rep = spectral && !(env && std::strcmp(env, "pushed") == 0);
-  const bool allow_bulk = allow_rep && !(env && std::strcmp(env, "sync") == 0);
+  const bool pushed = env ? std::strcmp(env, "pushed") == 0 : c.tune.pcg_form == 1;
+  const bool sync = env ? std::strcmp(env, "sync") == 0 : c.tune.pcg_form == 2;
+  const bool allow_rep = spectral && !pushed;
+  const bool allow_bulk = allow_rep && !sync;
   const bool forms[3][2] = {{true, true}, {true, false}, {false, false}};  // (replicated, bulk)
   for (bool sy_global : {false, true}) {
     for (int nc : {prefer16 ? 16 : 8, prefer16 ? 8 : 16}) {
@@ -1011,13 +1016,15 @@ constexpr size_t kSubClusterCellsShared = 4 * kSubClusterCells;
 cudaError_t plan_subcycle(const Ctx &c, int *out) {
   const size_t ncell = (size_t)c.im * c.jm;
   const char *env = getenv("NPOM_SUBCYCLE");
+  const int form = c.tune.subcycle_form;
   const bool nocoop = env && std::strcmp(env, "nocoop") == 0;
-  if ((env && std::strcmp(env, "phases") == 0) || (nocoop && ncell > kSubClusterCellsShared)) {
+  const bool phases = env ? std::strcmp(env, "phases") == 0 : form == 3;
+  if (phases || (nocoop && ncell > kSubClusterCellsShared)) {
     *out = 0;
     return cudaSuccess;
   }
   if (nocoop) return plan_cluster(kSubcycleCluster, ncell, out);
-  const bool grid = env && std::strcmp(env, "grid") == 0;
+  const bool grid = env ? std::strcmp(env, "grid") == 0 : form == 2;
   if (!grid && ncell <= kSubClusterCells) return plan_cluster(kSubcycleCluster, ncell, out);
   return coop_blocks((const void *)k_subcycle, ncell, out);
 }
@@ -1080,6 +1087,7 @@ void launch_a1(const Ctx &c, cudaStream_t s) {
   const size_t ncell = (size_t)c.im * c.jm;
   const char *env = getenv("NPOM_A1");
   bool tiles = c.kb == 16 && ncell >= kTileCells;
+  if (!env && c.tune.a1_form) tiles = c.kb == 16 && c.tune.a1_form == 2;
   if (env && c.kb == 16 && std::strcmp(env, "tiles") == 0) tiles = true;
   if (env && std::strcmp(env, "points") == 0) tiles = false;
   if (!tiles) {
@@ -1090,7 +1098,8 @@ void launch_a1(const Ctx &c, cudaStream_t s) {
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int strips = (c.jm + kA1Cols - 1) / kA1Cols;
   // short marches, many blocks: ~16 blocks per SM (measured best at 354x322)
-  const int want = std::max(1, (16 * sms + strips - 1) / strips);
+  const int per_sm = c.tune.tile_blocks_per_sm > 0 ? c.tune.tile_blocks_per_sm : 16;
+  const int want = std::max(1, (per_sm * sms + strips - 1) / strips);
   const int ichunk = std::max(2, (c.im + want - 1) / want);
   const int chunks = (c.im + ichunk - 1) / ichunk;
   k_a1_tiles<<<dim3(strips, chunks), kA1Threads, 0, s>>>(c, ichunk);
@@ -1134,6 +1143,7 @@ void launch_b5(const Ctx &c, cudaStream_t s) {
   const size_t ncell = (size_t)c.im * c.jm;
   const char *env = getenv("NPOM_B5");
   bool tiles = c.kb == 16 && c.k.mode != 4 && ncell >= kTileCells;
+  if (!env && c.tune.b5_form) tiles = c.kb == 16 && c.k.mode != 4 && c.tune.b5_form == 2;
   if (env && c.kb == 16 && c.k.mode != 4 && std::strcmp(env, "tiles") == 0) tiles = true;
   if (env && std::strcmp(env, "points") == 0) tiles = false;
   if (!tiles) {
@@ -1143,7 +1153,8 @@ void launch_b5(const Ctx &c, cudaStream_t s) {
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int strips = (c.jm + kB5Cols - 1) / kB5Cols;
-  const int want = std::max(1, (16 * sms + strips - 1) / strips);
+  const int per_sm = c.tune.tile_blocks_per_sm > 0 ? c.tune.tile_blocks_per_sm : 16;
+  const int want = std::max(1, (per_sm * sms + strips - 1) / strips);
   const int ichunk = std::max(2, (c.im + want - 1) / want);
   const int chunks = (c.im + ichunk - 1) / ichunk;
   k_b5_tiles<<<dim3(strips, chunks), kB5Threads, 0, s>>>(c, ichunk);

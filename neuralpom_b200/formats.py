@@ -28,7 +28,7 @@ import torch
 from .core import NUMERICS_VERSION
 
 # Attributes rebuilt on restore instead of saved.
-SCRATCH = frozenset({"device", "_ws", "_ws_key", "_ws_geo", "_eta_solver_iteration_history",
+SCRATCH = frozenset({"device", "_ws", "_ws_key", "_ws_geo", "tuning", "_eta_solver_iteration_history",
                      "_eta_adjoint_iteration_history"})
 
 

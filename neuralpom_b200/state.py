@@ -114,6 +114,11 @@ def make_params(s, im, jm, kb, core, device=0):
     p.wind_tau0 = 0.1 if tau0 is None else float(tau0)
     p.period = host_scalar(get("period", 1.0))
     p.inverse_scale = 4.0 * (im - 1) * (jm - 1)
+    tuning = get("tuning", None) or {}
+    for k, v in dict(tuning).items():
+        if k not in _abi.TUNING_FIELDS:
+            raise ValueError(f"unknown tuning field {k!r}")
+        setattr(p.tuning, k, int(v))
     return p
 
 
