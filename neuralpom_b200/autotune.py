@@ -16,8 +16,8 @@ and keeps the fastest.
 * ``tune(core)`` -- times ``steps`` internal steps of the core from its
   current state for every candidate (CUDA events, the median of ``reps``),
   restores the state after each, then checks the winner against the rules:
-  the fields after the same steps must be equal bit for bit (to 1e-5 where
-  the cooperative-grid PCG sums its dot products in another order).
+  the fields after the same steps must be equal bit for bit (every form in
+  the search space computes the same values).
 * The winners are cached in a JSON file keyed on device, core, grid and the
   settings that change the step's kernels (``NPOM_TUNING_CACHE``, default
   ``~/.cache/neuralpom_b200/tuning.json``); ``apply(core)`` gives a core its
@@ -42,7 +42,10 @@ SPACE = {
     "tile_blocks_per_sm": (0, 8, 32),
     "column_form": (0, 1, 2),
     "subcycle_form": (0, 2, 3),
-    "pcg_form": (0, 1, 2, 3),
+    # the cooperative-grid PCG (3) is left to the rules, which pick it where
+    # no cluster layout fits: it sums its FP64 dot products over its blocks,
+    # so it agrees with the cluster forms only to rounding
+    "pcg_form": (0, 1, 2),
     "pcg_ctas": (0, 16),
 }
 BATCH_SPACE = dict(SPACE, batch_pcg_blocks=(0, 32, 40, 56, 64, 112))
@@ -175,8 +178,7 @@ def tune(core, steps=4, reps=3, min_gain=0.02, check=True):
                                   min_gain=min_gain, log=log)
     checked = True
     if check and best:
-        tol = 1e-5 if best.get("pcg_form") == 3 else None
-        checked = same_result(core, best, steps, rel_tol=tol)
+        checked = same_result(core, best, steps)
         if not checked:
             best, t_best = {}, t_base
     return best, {"rule_ms_per_step": t_base, "tuned_ms_per_step": t_best, "candidates": len(log),
