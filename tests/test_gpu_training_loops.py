@@ -121,6 +121,7 @@ def _golden_path():
     here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
     if here not in sys.path:
         sys.path.insert(0, here)
+    rh.import_reference(REF)
 
 
 @pytest.mark.parametrize("core_name,im,jm", [("implicit_p0_fixed", 20, 18), ("explicit", 12, 10)])
