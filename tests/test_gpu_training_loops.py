@@ -13,7 +13,6 @@ the same core class bound to the B200 library
 (``neuralpom_b200.reference_binding``) -- and the losses and the gradients
 reaching the model's parameters are compared.
 """
-import copy
 
 import numpy as np
 import pytest
