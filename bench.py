@@ -99,6 +99,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the per-field error against a float64 reference day")
     ap.add_argument("--no-batch-tune", action="store_true", help="batch workload: the library's launch rules only")
+    ap.add_argument("--no-coastal", action="store_true", help="skip the 354x322x16 coastal forward+adjoint sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--members", type=int, default=8,
                     help="ensemble members advanced concurrently on one GPU for the 'ensemble' key (1 = skip)")
@@ -400,6 +401,14 @@ def run_b200(args):
     if rank == 0 and ws_n == 1 and args.workload == "seamount" and not args.no_batch and not args.fa_only:
         bat = batch_summary(args)
 
+    # the coastal configuration's differentiation at its own size (354x322x16,
+    # 6 h, checkpoint per internal step): days/s and peak device memory
+    coastal = None
+    if rank == 0 and ws_n == 1 and args.workload == "seamount" and not args.no_fwd_adjoint and not args.no_coastal:
+        torch.cuda.empty_cache()
+        coastal = coastal_fwd_adjoint(args, dev)
+        torch.cuda.empty_cache()
+
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws_n, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -415,7 +424,8 @@ def run_b200(args):
                                  if (its and W["core"] != "explicit") else None),
         "fp64_error": fp64,
         "roofline": roofline, "cpu_baseline": cpu, "reference_gpu": ref_gpu, "ensemble": ens, "fwd_adjoint": fa,
-        "fwd_adjoint_midtrain": fam, "fwd_adjoint_midtrain_batch": famb, "batch": bat, "e2e": e2e,
+        "fwd_adjoint_midtrain": fam, "fwd_adjoint_midtrain_batch": famb, "fwd_adjoint_coastal": coastal,
+        "batch": bat, "e2e": e2e,
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }

@@ -68,3 +68,32 @@ def oracle_runs(jobs):
     ctx = mp.get_context("spawn")
     with ctx.Pool(processes=len(jobs)) as pool:
         return pool.starmap(oracle_run, jobs)
+
+
+def fd_loss(path, scalars, core, steps, index, sign, eps):
+    """Float64 oracle loss after ``steps`` steps from the start state stored
+    in the ``.npz`` at ``path`` (``start__*`` arrays, ``target__*`` and
+    ``scale__*`` of the loss fields, ``dir{index}__*`` directions), with the
+    start moved by ``sign * eps`` along direction ``index``: sum over the
+    loss fields of mean((S - target)^2) / scale^2."""
+    from golden_io import oracle_params
+    from oracle import pom_oracle as O
+    z = np.load(path)
+    start = {k[7:]: z[k] for k in z.files if k.startswith("start__")}
+    S = {n: v.astype(np.float64) for n, v in start.items()}
+    fields = [k[8:] for k in z.files if k.startswith("target__")]
+    for f in fields:
+        S[f] = S[f] + sign * eps * z[f"dir{index}__{f}"]
+    P = oracle_params(dict(scalars), start, core)
+    O.run(S, P, steps, core)
+    return sum(float(((S[f] - z[f"target__{f}"]) ** 2).mean()) / float(z[f"scale__{f}"]) ** 2 for f in fields)
+
+
+def fd_losses(path, scalars, core, steps, ndirs, eps, workers=8):
+    """(plus, minus) float64 losses of ``fd_loss`` for every direction, in
+    parallel spawned workers."""
+    jobs = [(path, scalars, core, steps, i, s, eps) for i in range(ndirs) for s in (1.0, -1.0)]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(processes=min(workers, len(jobs))) as pool:
+        out = pool.starmap(fd_loss, jobs)
+    return [(out[2 * i], out[2 * i + 1]) for i in range(ndirs)]
