@@ -55,38 +55,11 @@ __global__ void __launch_bounds__(128) k_adj_cols_t(Ctx c, Adj a) {
   adj_column<PH, KM>(c, a, i, j);
 }
 
-// Threads per block of the column adjoints: one thread per column keeps its
-// column's intermediates in per-thread local arrays (up to ~2.3 KB for
-// PROFQ), which stay in L1 only if the columns are spread over every SM.
-// So the blocks are as large as possible (up to 128) while there are at
-// least as many blocks as SMs; NPOM_ADJ_COLS_BLOCK fixes the size (32, 64
-// or 128) for comparisons.  Every thread computes the same values either
-// way.
-int adj_cols_block(int ncols) {
-  static int sms = 0;
-  if (sms == 0) {
-    int dev = 0, v = 148;
-    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
-    sms = v > 0 ? v : 148;
-  }
-  const char *env = getenv("NPOM_ADJ_COLS_BLOCK");
-  if (env) {
-    const int b = atoi(env);
-    if (b == 32 || b == 64 || b == 128) return b;
-  }
-  for (int b : {128, 64}) {
-    if ((ncols + b - 1) / b >= sms) return b;
-  }
-  return 32;
-}
-
 template <int PH>
 void launch_adj_cols(const Ctx &c, const Adj &a, cudaStream_t s) {
-  const int n = c.im * c.jm;
-  const int b = adj_cols_block(n);
-  const unsigned g = (unsigned)((n + b - 1) / b);
-  if (c.kb == 16) k_adj_cols_t<PH, 16><<<g, b, 0, s>>>(c, a);
-  else k_adj_cols_t<PH, KMAX><<<g, b, 0, s>>>(c, a);
+  const unsigned g = (unsigned)((c.im * c.jm + 127) / 128);
+  if (c.kb == 16) k_adj_cols_t<PH, 16><<<g, 128, 0, s>>>(c, a);
+  else k_adj_cols_t<PH, KMAX><<<g, 128, 0, s>>>(c, a);
 }
 
 __global__ void __launch_bounds__(kThreads) k_adj_cells(Ctx c, Adj a, int phase, int iext, int adv) {
