@@ -142,9 +142,17 @@ typedef struct npom_params {
   double inverse_scale;    /* spectral preconditioner: 4 (ni+1)(nj+1)      */
   double sw;               /* MPDATA antidiffusion weight (nadv 2)         */
   int32_t nitera;          /* MPDATA iterations (nadv 2)                   */
-  int32_t pad0;
+  int32_t profq_form;      /* NPOM_PROFQ_PRODUCTION or NPOM_PROFQ_POM08    */
   npom_tuning tuning;      /* launch shapes (all zero: the library's rules) */
+  double zsh;              /* POM08-WAD profq: roughness added to the mixing length (m) */
 } npom_params;
+
+/* PROFQ forms.  PRODUCTION: the cores' own operator (explicit/tracers.py:158,
+ * implicit_p0_fixed/tracers.py:156).  POM08: the POM08-WAD closure of the
+ * reference's case policies (cores/case_adapters/fortran_compat.py:26-147,
+ * installed by dg_policy.py, coastal_compat.py, jzb_compat.py): forward
+ * only, as in the reference, which validates it for forward comparisons. */
+enum { NPOM_PROFQ_PRODUCTION = 0, NPOM_PROFQ_POM08 = 1 };
 
 enum { NPOM_CORE_EXPLICIT = 0, NPOM_CORE_IMPLICIT = 1 };
 enum { NPOM_PRECOND_JACOBI = 0, NPOM_PRECOND_SPECTRAL = 1 };

@@ -2559,7 +2559,10 @@ inline int adj_step_plan(const Ctx &c, AdjPhaseRec *out, int cap, size_t *save_f
 // surface flux (nbc 1) or value (nbc 3) conditions; for the implicit core
 // the production Shapiro filters (gamma 0).
 inline bool adj_supported(const npom_params *p) {
-  const bool base = p->mode == 3 && p->nadv == 1 && (p->nbct == 1 || p->nbct == 3) && (p->nbcs == 1 || p->nbcs == 3);
+  // the POM08-WAD PROFQ is forward only, as in the reference's case
+  // policies (which refuse advancement with gradients)
+  const bool base = p->mode == 3 && p->nadv == 1 && (p->nbct == 1 || p->nbct == 3) &&
+                    (p->nbcs == 1 || p->nbcs == 3) && p->profq_form == NPOM_PROFQ_PRODUCTION;
   if (p->core == NPOM_CORE_EXPLICIT) return base;
   return base && p->core == NPOM_CORE_IMPLICIT && p->barotropic_shapiro == 0.0 && p->tracer_shapiro == 0.0;
 }

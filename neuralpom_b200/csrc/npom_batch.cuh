@@ -605,6 +605,9 @@ bool batch_uniform(const npom_params *const *p, int nm) {
         b->mode != a->mode || b->nadv != a->nadv || b->nitera != a->nitera || b->device != a->device)
       return false;
   }
+  // the POM08-WAD PROFQ has no lane body, which the batched column phases use
+  for (int m = 0; m < nm; ++m)
+    if (p[m]->profq_form != NPOM_PROFQ_PRODUCTION) return false;
   return true;
 }
 

@@ -45,6 +45,8 @@ struct Consts {
   float sw;
   int eta_max_iter, eta_precond;
   double eta_tol, eta_rel_tol;
+  int profq_pom08;     // PROFQ in the POM08-WAD form
+  float kappa_zsh;     // POM08-WAD: kappa * zsh (folded in double)
 };
 
 struct Ctx {

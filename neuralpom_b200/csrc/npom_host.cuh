@@ -50,6 +50,8 @@ inline Consts make_consts(const npom_params &p) {
   k.prof_const1 = (float)std::pow(16.6, 2.0 / 3.0);
   k.prof_gg0 = (float)std::pow(15.8 * 100.0, 2.0 / 3.0);
   k.surfl = 2.0e5f;
+  k.profq_pom08 = p.profq_form == NPOM_PROFQ_POM08 ? 1 : 0;
+  k.kappa_zsh = (float)(p.kappa * p.zsh);
   k.wind_kf = (float)(-(p.wind_tau0 / p.rhoref));
   k.two_pi = (float)(2.0 * p.pi);
   k.hmax = (float)p.hmax;

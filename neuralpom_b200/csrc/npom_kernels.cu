@@ -847,7 +847,9 @@ template <int PH>
 void launch_cols(const Ctx &c, cudaStream_t s) {
   size_t n = (size_t)c.im * c.jm;
   const bool proft_threads = PH == CP_B6 && n >= kProftThreadColumns && c.tune.column_form != 1;
-  if (lanes_enabled(c) && !proft_threads) {
+  // the POM08-WAD PROFQ has only the thread-per-column body
+  const bool pom08 = PH == CP_B3 && c.k.profq_pom08;
+  if (lanes_enabled(c) && !proft_threads && !pom08) {
     k_lanes<PH><<<blocks_for(n * KL, kThreads), kThreads, 0, s>>>(c);
   } else {
     k_cols<PH><<<blocks_for(n, 128), 128, 0, s>>>(c);

@@ -116,7 +116,13 @@ NPOM_HD void phase_b2b_point(const Ctx &c, int i, int j, int k) {
 // implicit_p0_fixed/tracers.py:156-430).  Writes l, kq and the raw km/kh
 // (edge copies follow in B4), and the q2/q2l forecasts into uf/vf.
 // ---------------------------------------------------------------------------
+NPOM_HD void phase_b3_pom08_column(const Ctx &c, int i, int j);
+
 NPOM_HD void phase_b3_column(const Ctx &c, int i, int j) {
+  if (c.k.profq_pom08) {
+    phase_b3_pom08_column(c, i, j);
+    return;
+  }
   const int im = c.im, jm = c.jm, kb = c.kb, kbm1 = kb - 1;
   const float dti2 = c.k.dti2, umol2 = c.k.two_umol, grav = c.k.grav, kappa = c.k.kappa;
   const float small = c.k.small;
@@ -259,6 +265,153 @@ NPOM_HD void phase_b3_column(const Ctx &c, int i, int j) {
 }
 
 // ---------------------------------------------------------------------------
+// B3 in the POM08-WAD form of the reference's case policies
+// (cores/case_adapters/fortran_compat.py:26-147, after pom08.f with nwad=0):
+// sound speed from the fixed reference pressure of (-zz * max(h, 0)),
+// buoyancy over h + et, exact stress norms and square roots (no epsilon),
+// |q2b| and |q2lb| on the interior levels (written back: the time loop keeps
+// them as q2b/q2lb), the q2 sweep with reciprocal pivots, the q2l sweep with
+// Dirichlet values on the second and the penultimate level, |q2| and |q2l|
+// forecasts instead of clipping, kn = (kappa zsh + l) sqrt|q2| and
+// kq = (0.20 kn + kq) / 2.  km/kh edges follow in B4 (north/south first).
+// ---------------------------------------------------------------------------
+NPOM_HD void phase_b3_pom08_column(const Ctx &c, int i, int j) {
+  const int im = c.im, jm = c.jm, kb = c.kb, kbm1 = kb - 1;
+  const float dti2 = c.k.dti2, umol2 = c.k.two_umol, grav = c.k.grav, kappa = c.k.kappa;
+  const float small = c.k.small;
+  float A[KMAX], C[KMAX], diss[KMAX], prod[KMAX], gh[KMAX], l[KMAX], snd[KMAX], boy[KMAX];
+  float qb[KMAX], ee[KMAX], gg[KMAX], usol[KMAX], vsol[KMAX];
+  const float dh = F2(h, i, j) + F2(etf, i, j);
+  for (int k = 0; k < kb; ++k) {
+    A[k] = 0.0f;
+    C[k] = 0.0f;
+  }
+  for (int k = 1; k < kbm1; ++k) {
+    float den_a = F1(dzz, k - 1) * F1(dz, k) * dh * dh;
+    float den_c = F1(dzz, k - 1) * F1(dz, k - 1) * dh * dh;
+    A[k] = c.k.neg_dti2 * (F3(kq, i, j, k + 1) + F3(kq, i, j, k) + umol2) * 0.5f / den_a;
+    C[k] = c.k.neg_dti2 * (F3(kq, i, j, k - 1) + F3(kq, i, j, k) + umol2) * 0.5f / den_c;
+  }
+  // stresses on [0, im-1) x [0, jm-1) (fortran_compat.py:42-53)
+  const bool sb = (i < im - 1) && (j < jm - 1);
+  float l0 = 0.0f, surface_q = 0.0f, bottom = F3(uf, i, j, kb - 1);
+  if (sb) {
+    float us_ = 0.5f * (F2(wusurf, i, j) + F2(wusurf, i + 1, j));
+    float vs_ = 0.5f * (F2(wvsurf, i, j) + F2(wvsurf, i, j + 1));
+    float ub_ = 0.5f * (F2(wubot, i, j) + F2(wubot, i + 1, j));
+    float vb_ = 0.5f * (F2(wvbot, i, j) + F2(wvbot, i, j + 1));
+    float utau2 = sqrtf(us_ * us_ + vs_ * vs_);
+    float btau2 = sqrtf(ub_ * ub_ + vb_ * vb_);
+    l0 = c.k.surfl * utau2 / grav;
+    surface_q = c.k.prof_gg0 * utau2;
+    bottom = btau2 * c.k.prof_const1;
+  }
+  // sound speed from the fixed reference pressure (:56-60)
+  const float hpos = fmaxf_t(F2(h, i, j), 0.0f);
+  for (int k = 0; k < kbm1; ++k) {
+    float pd = c.k.g_rhoref * (-F1(zz, k) * hpos);
+    pd = pd * 1.0e-5f;
+    float p = pd * 10.0f;
+    float tp = F3(t, i, j, k) + c.k.tbias;
+    float sp = F3(s, i, j, k) + c.k.sbias;
+    float snd0 = 1449.1f + 0.00821f * p + 4.55f * tp - 0.045f * (tp * tp) + 1.34f * (sp - 35.0f);
+    snd[k] = snd0 / sqrtf((1.0f - 0.01642f * p / snd0) * (1.0f - 0.40f * p / (snd0 * snd0)));
+  }
+  for (int k = 0; k < kb; ++k) {
+    float q = F3(q2b, i, j, k), ql = F3(q2lb, i, j, k);
+    if (k >= 1 && k < kbm1) {
+      q = fabsf(q);
+      ql = fabsf(ql);
+      P3(q2b, i, j, k) = q;
+      P3(q2lb, i, j, k) = ql;
+    }
+    qb[k] = q;
+    if (k >= 1 && k < kbm1) l[k] = fabsf(ql / q);
+  }
+  // buoyancy, length scale, stability (:68-84)
+  const float ddep = F2(h, i, j) + F2(et, i, j);
+  const float kl0 = kappa * l0;
+  for (int k = 0; k < kb; ++k) {
+    boy[k] = 0.0f;
+    gh[k] = 0.0f;
+  }
+  l[0] = kl0;
+  l[kb - 1] = 0.0f;
+  for (int k = 1; k < kbm1; ++k) {
+    float b = grav * (F3(rho, i, j, k - 1) - F3(rho, i, j, k)) / (F1(dzz, k - 1) * ddep);
+    b = b + c.k.g2x2 / (snd[k - 1] * snd[k - 1] + snd[k] * snd[k]);
+    float ll = l[k];
+    if (F1(z, k) > -0.5f) ll = fmaxf_t(ll, kl0);
+    boy[k] = b;
+    l[k] = ll;
+    gh[k] = fminf_t((ll * ll) * b / qb[k], 0.028f);
+  }
+  // production on the interior (:86-94)
+  for (int k = 0; k < kb; ++k) prod[k] = 0.0f;
+  if (interior(c, i, j)) {
+    for (int k = 1; k < kbm1; ++k) {
+      float du = F3(u, i, j, k) - F3(u, i, j, k - 1) + F3(u, i + 1, j, k) - F3(u, i + 1, j, k - 1);
+      float dv = F3(v, i, j, k) - F3(v, i, j, k - 1) + F3(v, i, j + 1, k) - F3(v, i, j + 1, k - 1);
+      float den = F1(dzz, k - 1) * dh;
+      den = den * den;
+      float pr = F3(km, i, j, k) * 0.25f * (du * du + dv * dv) / den;
+      prod[k] = pr + F3(kh, i, j, k) * boy[k];
+    }
+  }
+  for (int k = 0; k < kb; ++k) diss[k] = sqrtf(fabsf(qb[k])) / (16.6f * l[k] + small);
+  // q2: the sweep with reciprocal pivots (:97-105)
+  ee[0] = 0.0f;
+  gg[0] = surface_q;
+  for (int k = 1; k < kbm1; ++k) {
+    float inv = 1.0f / (A[k] + C[k] * (1.0f - ee[k - 1]) - (c.k.two_dti2 * diss[k] + 1.0f));
+    ee[k] = A[k] * inv;
+    gg[k] = (c.k.neg_two_dti2 * prod[k] + C[k] * gg[k - 1] - F3(uf, i, j, k)) * inv;
+  }
+  usol[kb - 1] = bottom;
+  for (int k = kbm1 - 1; k >= 0; --k) usol[k] = ee[k] * usol[k + 1] + gg[k];
+  // q2l: Dirichlet values on the second and the penultimate level (:107-130)
+  const float z0 = F1(z, 0), zb = F1(z, kb - 1);
+  const float q21 = F3(q2, i, j, 1), q2p = F3(q2, i, j, kbm1 - 1);
+  ee[0] = 0.0f;
+  gg[0] = 0.0f;
+  ee[1] = 0.0f;
+  gg[1] = ((-kappa) * F1(z, 1)) * dh * q21;
+  for (int k = 2; k < kbm1; ++k) {
+    float zk = F1(z, k);
+    float wall = (1.0f / fabsf(zk - z0) + 1.0f / fabsf(zk - zb)) * l[k] / (dh * kappa);
+    float ds = diss[k] * (1.0f + 1.33f * (wall * wall));
+    float inv = 1.0f / (A[k] + C[k] * (1.0f - ee[k - 1]) - (dti2 * ds + 1.0f));
+    ee[k] = A[k] * inv;
+    float rhs = (k == kbm1 - 1) ? (kappa * (1.0f + F1(z, kbm1 - 1))) * dh * q2p : F3(vf, i, j, k);
+    gg[k] = (dti2 * (-prod[k] * l[k] * 1.8f) + C[k] * gg[k - 1] - rhs) * inv;
+  }
+  vsol[0] = 0.0f;
+  vsol[kb - 1] = 0.0f;
+  for (int k = kbm1 - 1; k >= 1; --k) vsol[k] = ee[k] * vsol[k + 1] + gg[k];
+  for (int k = 1; k < kbm1; ++k) {
+    usol[k] = fabsf(usol[k]);
+    vsol[k] = fabsf(vsol[k]);
+  }
+  // stability functions and mixing (:134-144); km/kh edges in B4
+  const float coef4 = (float)(18.0 * 0.92 * 0.92 + 9.0 * 0.92 * 0.74);
+  const float coef5 = (float)(9.0 * 0.92 * 0.74);
+  const float coef1 = (float)(0.74 * (1.0 - 6.0 * 0.92 / 16.6));
+  const float coef2 = (float)(3.0 * 0.74 * 10.1 + 18.0 * 0.92 * 0.74);
+  const float coef3 = (float)(0.92 * (1.0 - 3.0 * 0.08 - 6.0 * 0.92 / 16.6));
+  for (int k = 0; k < kb; ++k) {
+    float sh = coef1 / (1.0f - coef2 * gh[k]);
+    float sm = (coef3 + sh * coef4 * gh[k]) / (1.0f - coef5 * gh[k]);
+    float kn = (c.k.kappa_zsh + l[k]) * sqrtf(fabsf(F3(q2, i, j, k)));
+    P3(l, i, j, k) = l[k];
+    P3(kq, i, j, k) = (kn * 0.20f + F3(kq, i, j, k)) * 0.5f;
+    P3(km, i, j, k) = (kn * sm + F3(km, i, j, k)) * 0.5f;
+    P3(kh, i, j, k) = (kn * sh + F3(kh, i, j, k)) * 0.5f;
+    P3(uf, i, j, k) = usol[k];
+    P3(vf, i, j, k) = vsol[k];
+  }
+}
+
+// ---------------------------------------------------------------------------
 // B4 (edge point): km/kh edge copies of PROFQ (tracers.py:425-429) and, for
 // the explicit core, bcond 6 upstream values of the q2/q2l forecasts
 // (baroclinic.py:856-919).  Runs over every (i, j, k); non-edge points exit.
@@ -274,9 +427,13 @@ NPOM_HD void phase_b4_point(const Ctx &c, int i, int j, int k) {
     if (j == 0 || j == jm - 1) {
       int sj = (j == 0) ? 1 : jm - 2;
       // column pass copies from the row-pass result at (i, sj)
+      // corners: the production operator copies along i first (the source
+      // row's own mask, fsm(i, sj)); the POM08-WAD form copies along j first
+      // (fortran_compat.py:19-24: the source's mask at the corner row, fsm(si, j))
       float src;
-      if (i == 0) src = ld(arr + NPOM_I3(c, 1, sj, k)) * F2(fsm, 0, sj);
-      else if (i == im - 1) src = ld(arr + NPOM_I3(c, im - 2, sj, k)) * F2(fsm, im - 1, sj);
+      const bool jfirst = c.k.profq_pom08 != 0;
+      if (i == 0) src = ld(arr + NPOM_I3(c, 1, sj, k)) * (jfirst ? F2(fsm, 1, j) : F2(fsm, 0, sj));
+      else if (i == im - 1) src = ld(arr + NPOM_I3(c, im - 2, sj, k)) * (jfirst ? F2(fsm, im - 2, j) : F2(fsm, im - 1, sj));
       else src = ld(arr + NPOM_I3(c, i, sj, k));
       val = src * F2(fsm, i, j);
     } else {

@@ -114,6 +114,11 @@ def make_params(s, im, jm, kb, core, device=0):
     p.wind_tau0 = 0.1 if tau0 is None else float(tau0)
     p.period = host_scalar(get("period", 1.0))
     p.inverse_scale = 4.0 * (im - 1) * (jm - 1)
+    form = str(get("profq_form", "production") or "production").strip().lower()
+    if form not in ("production", "pom08"):
+        raise ValueError(f"unknown profq form {form!r} (production or pom08)")
+    p.profq_form = _abi.PROFQ_POM08 if form == "pom08" else _abi.PROFQ_PRODUCTION
+    p.zsh = float(get("zsh", 0.01))
     tuning = get("tuning", None) or {}
     for k, v in dict(tuning).items():
         if k not in _abi.TUNING_FIELDS:

@@ -808,6 +808,124 @@ def profq(S, P, uf, vf, implicit_variant):
                 a=A, c=C)
 
 
+def profq_pom08(S, P, uf, vf):
+    """The POM08-WAD closure of the reference's case policies.
+
+    Restates ``cores/case_adapters/fortran_compat.py:26-147`` (``profq``
+    bound by ``install``, ``:147-161``, with the default reference pressure
+    and ``zsh``): sound speed from the fixed pressure of -zz*max(h, 0),
+    buoyancy over h + et, exact stress norms, |q2b| / |q2lb| on the interior
+    levels (returned as the new q2b / q2lb, which the time loop keeps),
+    reciprocal pivots, Dirichlet q2l values on the second and penultimate
+    levels, |q2| / |q2l| forecasts, kn = (kappa*zsh + l)*sqrt|q2|,
+    kq = (0.20*kn + kq)*0.5, and km/kh edges with the north/south copies
+    first.  Returns the dict of ``profq`` plus q2b and q2lb."""
+    t, s, rho, u, v = S["t"], S["s"], S["rho"], S["u"], S["v"]
+    q2, q2b, q2lb = S["q2"], S["q2b"], S["q2lb"]
+    km_in, kh_in, kq_in = S["km"], S["kh"], S["kq"]
+    h, etf, et, fsm = S["h"], S["etf"], S["et"], S["fsm"]
+    dz, dzz, zz, z = S["dz"], S["dzz"], S["zz"], S["z"]
+    im, jm, kb = q2.shape
+    kbm1 = kb - 1
+    dti2, umol, grav, kappa, small = P.dti2, P.umol, P.grav, P.kappa, P.small
+    zsh = float(getattr(P, "zsh", 0.01))
+    zero = np.zeros_like(h)
+    dh = h + etf
+    aa = np.zeros_like(q2)
+    ca = np.zeros_like(q2)
+    for k in range(1, kbm1):
+        aa[:, :, k] = -dti2 * (kq_in[:, :, k + 1] + kq_in[:, :, k] + 2 * umol) * .5 / (dzz[k - 1] * dz[k] * dh * dh)
+        ca[:, :, k] = -dti2 * (kq_in[:, :, k - 1] + kq_in[:, :, k] + 2 * umol) * .5 / (dzz[k - 1] * dz[k - 1] * dh * dh)
+    us = .5 * (S["wusurf"][:-1, :-1] + S["wusurf"][1:, :-1])
+    vs = .5 * (S["wvsurf"][:-1, :-1] + S["wvsurf"][:-1, 1:])
+    ub = .5 * (S["wubot"][:-1, :-1] + S["wubot"][1:, :-1])
+    vb = .5 * (S["wvbot"][:-1, :-1] + S["wvbot"][:-1, 1:])
+    utau2 = np.sqrt(us * us + vs * vs)
+    btau2 = np.sqrt(ub * ub + vb * vb)
+    l0 = zero.copy()
+    l0[:-1, :-1] = 2.e5 * utau2 / grav
+    surface_q = zero.copy()
+    surface_q[:-1, :-1] = (15.8 * 100.) ** (2. / 3.) * utau2
+    bottom = uf[:, :, -1].copy()
+    bottom[:-1, :-1] = btau2 * (16.6 ** (2. / 3.))
+    pdens = grav * P.rhoref * (-zz[None, None, :] * np.maximum(h[:, :, None], 0.)) * 1.e-5
+    pdens = pdens.astype(q2.dtype)
+    p = pdens[:, :, :kbm1] * 10.
+    tp = t[:, :, :kbm1] + P.tbias
+    sp = s[:, :, :kbm1] + P.sbias
+    sound = 1449.1 + .00821 * p + 4.55 * tp - .045 * (tp * tp) + 1.34 * (sp - 35.)
+    sound = sound / np.sqrt((1. - .01642 * p / sound) * (1. - .40 * p / (sound * sound)))
+    qb = q2b.copy()
+    qlb = q2lb.copy()
+    qb[:, :, 1:kbm1] = np.abs(q2b[:, :, 1:kbm1])
+    qlb[:, :, 1:kbm1] = np.abs(q2lb[:, :, 1:kbm1])
+    boygr = np.zeros_like(q2)
+    l_out = np.zeros_like(q2)
+    gh = np.zeros_like(q2)
+    l_out[:, :, 0] = kappa * l0
+    depth = h + et
+    for k in range(1, kbm1):
+        b = grav * (rho[:, :, k - 1] - rho[:, :, k]) / (dzz[k - 1] * depth)
+        b = b + grav ** 2 * 2. / (sound[:, :, k - 1] * sound[:, :, k - 1] + sound[:, :, k] * sound[:, :, k])
+        ll = np.abs(qlb[:, :, k] / qb[:, :, k])
+        if z[k] > -.5:
+            ll = np.maximum(ll, kappa * l0)
+        boygr[:, :, k] = b
+        l_out[:, :, k] = ll
+        gh[:, :, k] = np.minimum((ll * ll) * b / qb[:, :, k], .028)
+    prod = np.zeros_like(q2)
+    for k in range(1, kbm1):
+        du = u[1:-1, 1:-1, k] - u[1:-1, 1:-1, k - 1] + u[2:, 1:-1, k] - u[2:, 1:-1, k - 1]
+        dv = v[1:-1, 1:-1, k] - v[1:-1, 1:-1, k - 1] + v[1:-1, 2:, k] - v[1:-1, 2:, k - 1]
+        den = dzz[k - 1] * dh[1:-1, 1:-1]
+        pr = km_in[1:-1, 1:-1, k] * .25 * (du * du + dv * dv) / (den * den)
+        prod[1:-1, 1:-1, k] = pr + kh_in[1:-1, 1:-1, k] * boygr[1:-1, 1:-1, k]
+    diss = np.sqrt(np.abs(qb)) / (16.6 * l_out + small)
+    e = [zero]
+    g = [surface_q]
+    for k in range(1, kbm1):
+        inv = 1. / (aa[:, :, k] + ca[:, :, k] * (1. - e[k - 1]) - (2. * dti2 * diss[:, :, k] + 1.))
+        e.append(aa[:, :, k] * inv)
+        g.append((-2. * dti2 * prod[:, :, k] + ca[:, :, k] * g[k - 1] - uf[:, :, k]) * inv)
+    usol = np.zeros_like(q2)
+    usol[:, :, kb - 1] = bottom
+    for k in range(kbm1 - 1, -1, -1):
+        usol[:, :, k] = e[k] * usol[:, :, k + 1] + g[k]
+    e2 = [zero, zero]
+    g2 = [zero, (-kappa * z[1]) * dh * q2[:, :, 1]]
+    for k in range(2, kbm1):
+        wall = (1. / np.abs(z[k] - z[0]) + 1. / np.abs(z[k] - z[-1])) * l_out[:, :, k] / (dh * kappa)
+        ds = diss[:, :, k] * (1. + 1.33 * (wall * wall))
+        inv = 1. / (aa[:, :, k] + ca[:, :, k] * (1. - e2[k - 1]) - (dti2 * ds + 1.))
+        e2.append(aa[:, :, k] * inv)
+        rhs = (kappa * (1. + z[kbm1 - 1])) * dh * q2[:, :, kbm1 - 1] if k == kbm1 - 1 else vf[:, :, k]
+        g2.append((dti2 * (-prod[:, :, k] * l_out[:, :, k] * 1.8) + ca[:, :, k] * g2[k - 1] - rhs) * inv)
+    vsol = np.zeros_like(q2)
+    for k in range(kbm1 - 1, 0, -1):
+        vsol[:, :, k] = e2[k] * vsol[:, :, k + 1] + g2[k]
+    usol[:, :, 1:kbm1] = np.abs(usol[:, :, 1:kbm1])
+    vsol[:, :, 1:kbm1] = np.abs(vsol[:, :, 1:kbm1])
+    coef1 = .74 * (1. - 6. * .92 / 16.6)
+    coef2 = 3. * .74 * 10.1 + 18. * .92 * .74
+    coef3 = .92 * (1. - 3. * .08 - 6. * .92 / 16.6)
+    coef4 = 18. * .92 * .92 + 9. * .92 * .74
+    coef5 = 9. * .92 * .74
+    sh = coef1 / (1. - coef2 * gh)
+    sm = (coef3 + sh * coef4 * gh) / (1. - coef5 * gh)
+    kn = (kappa * zsh + l_out) * np.sqrt(np.abs(q2))
+    kq_out = (kn * .20 + kq_in) * .5
+    km_out = (kn * sm + km_in) * .5
+    kh_out = (kn * sh + kh_in) * .5
+    for arr in (km_out, kh_out):
+        # north/south first, then east/west (fortran_compat.py:19-24)
+        arr[:, 0] = arr[:, 1] * fsm[:, 0][:, None]
+        arr[:, jm - 1] = arr[:, jm - 2] * fsm[:, jm - 1][:, None]
+        arr[0] = arr[1] * fsm[0][:, None]
+        arr[im - 1] = arr[im - 2] * fsm[im - 1][:, None]
+    return dict(l=l_out, kq=kq_out, km=km_out, kh=kh_out, uf=usol, vf=vsol, cc=sound, a=aa, c=ca,
+                q2b=qb, q2lb=qlb)
+
+
 # ---------------------------------------------------------------------------
 # tracer advection (ADVT1) and vertical diffusion (PROFT)
 # ---------------------------------------------------------------------------
@@ -1555,7 +1673,11 @@ def step_explicit(S, P):
         uf = advq(S, P, S["q2b"], S["q2"], uf)
         vf = advq(S, P, S["q2lb"], S["q2l"], vf)
         S["uf"], S["vf"] = uf, vf
-        R = profq(S, P, uf, vf, implicit_variant=False)
+        if getattr(P, "profq_form", "production") == "pom08":
+            R = profq_pom08(S, P, uf, vf)
+            S["q2b"], S["q2lb"] = R["q2b"], R["q2lb"]
+        else:
+            R = profq(S, P, uf, vf, implicit_variant=False)
         S["l"], S["kq"], S["km"], S["kh"] = R["l"], R["kq"], R["km"], R["kh"]
         S["dtef"] = R["cc"]
         F = {"uf": R["uf"], "vf": R["vf"]}
@@ -1703,7 +1825,11 @@ def step_implicit(S, P, C=None, SC=None, dot_dtype=np.float64):
         uf = advq(S, P, S["q2b"], S["q2"], np.zeros_like(S["u"]))
         vf = advq(S, P, S["q2lb"], S["q2l"], np.zeros_like(S["u"]))
         S["uf"], S["vf"] = uf, vf
-        R = profq(S, P, uf, vf, implicit_variant=True)
+        if getattr(P, "profq_form", "production") == "pom08":
+            R = profq_pom08(S, P, uf, vf)
+            S["q2b"], S["q2lb"] = R["q2b"], R["q2lb"]
+        else:
+            R = profq(S, P, uf, vf, implicit_variant=True)
         S["l"], S["kq"], S["km"], S["kh"] = R["l"], R["kq"], R["km"], R["kh"]
         S["dtef"] = R["cc"]
         F = {"uf": R["uf"], "vf": R["vf"]}

@@ -72,7 +72,8 @@ def extract_state(core):
         if torch.is_tensor(v) and v.is_floating_point() and not k.startswith("_"):
             arrays[k] = v.detach().cpu().numpy().copy()
     scalars = {}
-    for k in SCALAR_NAMES + IMPLICIT_SCALARS:
+    # case-policy settings a harness puts on a core (the POM08-WAD closure)
+    for k in SCALAR_NAMES + IMPLICIT_SCALARS + ("profq_form", "zsh"):
         if hasattr(core, k):
             val = getattr(core, k)
             if isinstance(val, (bool, int, float, str)):

@@ -329,7 +329,23 @@ def make_mpdata_golden(im=12, jm=10, seed=51):
     make_step_golden("explicit", im, jm, seed, core=core, tag="mpdata")
 
 
-def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint", "coupling", "mpdata")):
+def make_pom08_goldens():
+    """Both cores with the POM08-WAD closure of the reference's case
+    policies bound by the reference's own installer
+    (cores/case_adapters/fortran_compat.py:147-161, default reference
+    pressure, zsh = 0.01 m) on perturbed production states: 1 and 3 steps of
+    the explicit 12x10 core, 1 and 2 of the implicit 20x18 core."""
+    from neuralpom.cores.case_adapters import fortran_compat
+    for name, im, jm, seed, steps in (("explicit", 12, 10, 61, (1, 3)), ("implicit_p0_fixed", 20, 18, 62, (1, 2))):
+        core = perturbed_core(name, im, jm, seed)
+        fortran_compat.install(core, zsh=0.01)
+        core.profq_form = "pom08"
+        core.zsh = 0.01
+        tag = "pom08_explicit" if name == "explicit" else "pom08_implicit"
+        make_step_golden(name, im, jm, seed, steps=steps, core=core, tag=tag)
+
+
+def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint", "coupling", "mpdata", "pom08")):
     src = rh.default_reference_path()
     if src is None:
         raise SystemExit("reference sources not found; set NPOM_REFERENCE_SRC")
@@ -352,7 +368,10 @@ def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint", "couplin
         make_coupling_golden()
     if "mpdata" in which:
         make_mpdata_golden()
+    if "pom08" in which:
+        make_pom08_goldens()
 
 
 if __name__ == "__main__":
-    main(tuple(sys.argv[1:]) or ("proft", "steps", "adjoint", "coastal", "step_adjoint", "coupling", "mpdata"))
+    main(tuple(sys.argv[1:]) or ("proft", "steps", "adjoint", "coastal", "step_adjoint", "coupling", "mpdata",
+                                 "pom08"))

@@ -60,3 +60,13 @@ def test_tuning_reaches_npom_params():
     assert p.tuning.a1_form == 1 and p.tuning.batch_pcg_blocks == 56 and p.tuning.pcg_form == 0
     with pytest.raises(ValueError):
         state.make_params(dict(s, tuning={"warp_size": 16}), 64, 64, 16, "explicit")
+
+
+def test_profq_form_reaches_npom_params():
+    s = dict(state.default_scalars("explicit"), profq_form="pom08", zsh=0.02)
+    p = state.make_params(s, 12, 10, 16, "explicit")
+    assert p.profq_form == _abi.PROFQ_POM08 and abs(p.zsh - 0.02) < 1e-15
+    p = state.make_params(dict(state.default_scalars("explicit")), 12, 10, 16, "explicit")
+    assert p.profq_form == _abi.PROFQ_PRODUCTION and abs(p.zsh - 0.01) < 1e-15
+    with pytest.raises(ValueError):
+        state.make_params(dict(s, profq_form="pom2k"), 12, 10, 16, "explicit")
