@@ -1003,50 +1003,6 @@ def reference_core(A, Sc, device="cpu", core_name="implicit_p0_fixed"):
     return core, rh
 
 
-class ReferenceFloat64:
-    """Context in which the reference core computes in float64: the
-    default dtype is float64 and the float32 scratch its step allocates
-    explicitly (explicit/momentum.py:25-28,144-147,555-556 and the tracer
-    routines) is allocated as float64 instead.  The core's own tensors are
-    promoted by ``promote``."""
-
-    NAMES = ("zeros", "ones", "empty", "full", "tensor", "arange", "linspace", "zeros_like", "ones_like",
-             "empty_like", "full_like", "as_tensor")
-
-    def __enter__(self):
-        import torch
-        self.torch = torch
-        self.saved = {n: getattr(torch, n) for n in self.NAMES}
-
-        def wrap(fn):
-            def alloc(*a, **k):
-                if k.get("dtype") is torch.float32:
-                    k["dtype"] = torch.float64
-                return fn(*a, **k)
-            return alloc
-        self.prev = torch.get_default_dtype()
-        for n in self.NAMES:
-            setattr(torch, n, wrap(self.saved[n]))
-        torch.set_default_dtype(torch.float64)
-        return self
-
-    def __exit__(self, *exc):
-        for n, fn in self.saved.items():
-            setattr(self.torch, n, fn)
-        self.torch.set_default_dtype(self.prev)
-
-    @staticmethod
-    def promote(core):
-        import torch
-        for k, v in list(vars(core).items()):
-            if torch.is_tensor(v) and v.dtype == torch.float32:
-                setattr(core, k, v.to(torch.float64))
-        # solver caches are rebuilt from the promoted geometry
-        core._accel_cache_ready = False
-        core._spectral_eta_preconditioner_cache = None
-        core._cg_work = {}
-
-
 FP64_FIELDS = ("u", "v", "t", "s", "el", "ua", "va", "q2", "q2l", "km", "kh", "w", "rho")
 
 
@@ -1063,11 +1019,11 @@ def fp64_day_error(A, Sc, nin, dev, core_name):
     got = {f: getattr(b, f).detach().cpu().numpy().astype(np.float64) for f in FP64_FIELDS}
     its_b = list(b._eta_solver_iteration_history)
     core, rh = reference_core(A, Sc, dev, core_name)
-    ReferenceFloat64.promote(core)
+    rh.ReferenceFloat64.promote(core)
     if hasattr(core, "_eta_solver_iteration_history"):
         core._eta_solver_iteration_history = []
     t0 = time.perf_counter()
-    with ReferenceFloat64():
+    with rh.ReferenceFloat64():
         if hasattr(core, "_build_acceleration_cache"):
             core._build_acceleration_cache()
         rh.advance(core, core_name, nin, device=dev)

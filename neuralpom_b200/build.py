@@ -21,6 +21,7 @@ LIBNAME = "libnpom_b200.so"
 SOURCES = ["npom_kernels.cu"]
 HEADERS = ["npom_ctx.cuh", "npom_phases_a.cuh", "npom_phases_ext.cuh", "npom_phases_int.cuh", "npom_host.cuh",
            "npom_pcg_cluster.cuh", "npom_lanes.cuh", "npom_adjoint.cuh", "npom_adjoint_launch.cuh", "npom_mpdata.cuh",
+           "npom_mpdata_adjoint.cuh",
            "npom_batch.cuh"]
 
 NVCC_FLAGS = [

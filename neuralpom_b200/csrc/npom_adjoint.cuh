@@ -28,7 +28,11 @@ namespace npom {
 // by the predictor, read by the free-surface solve and the corrector): their
 // slots follow the fields in Adj.
 enum AdjWs { AW_us = 0, AW_vs, AW_den_u, AW_den_v, AW_d_baro, AW_COUNT };
-constexpr int kAdjSlots = NPOM_NFIELDS + AW_COUNT;
+// The MPDATA scratch (nadv 2: per tracer xm ym zw xf yf zf, 3-D) carries a
+// cotangent between the passes of B5: its slots follow the workspace's.
+constexpr int kAdjMpSlots = 12;
+constexpr int kAdjSlots = NPOM_NFIELDS + AW_COUNT + kAdjMpSlots;
+NPOM_HD int mp_slot(int tracer, int arr) { return NPOM_NFIELDS + AW_COUNT + tracer * 6 + arr; }
 
 NPOM_HD int aw_ws(int k) {
   return k == AW_us ? NPOM_W_us
@@ -40,8 +44,12 @@ struct Adj {
   float *L[kAdjSlots];
 };
 
-// state array of a slot: a field or a workspace array
-NPOM_HD float *adj_fptr(const Ctx &c, int id) { return id < NPOM_NFIELDS ? c.F[id] : c.W[aw_ws(id - NPOM_NFIELDS)]; }
+// state array of a slot: a field, a workspace array or an MPDATA scratch array
+NPOM_HD float *adj_fptr(const Ctx &c, int id) {
+  if (id < NPOM_NFIELDS) return c.F[id];
+  if (id < NPOM_NFIELDS + AW_COUNT) return c.W[aw_ws(id - NPOM_NFIELDS)];
+  return c.mp3d + (size_t)(id - NPOM_NFIELDS - AW_COUNT) * ((size_t)c.im * c.jm * c.kb);
+}
 
 NPOM_HD void aadd(float *p, float v) {
 #if defined(__CUDA_ARCH__)
@@ -2414,8 +2422,14 @@ namespace npom {
 
 enum AdjPhase {
   AP_A1 = 0, AP_A2, AP_A3, AP_E1, AP_E2, AP_E3, AP_B1, AP_B2A, AP_B2B, AP_B3, AP_B4, AP_B5, AP_B6, AP_B7, AP_B8, AP_B9,
-  AP_EI, AP_I5
+  AP_EI, AP_I5,
+  // B5 with MPDATA (nadv 2), pass by pass: the q2/q2l filter, mass fluxes,
+  // per iteration (iext = the iteration) upstream fluxes, forecast and
+  // antidiffusive fluxes, then the diffusive fluxes and the final update
+  AP_MQ, AP_MINIT, AP_MUP, AP_MFC, AP_MAD, AP_MDIF, AP_MFIN
 };
+// phases of one step's plan at most (isplit substeps of three phases)
+NPOM_HD int adj_plan_capacity(int isplit, int nitera) { return 24 + 3 * isplit + 3 * nitera; }
 constexpr int kAdjMaxFields = 16;
 
 struct AdjPhaseRec {
@@ -2426,7 +2440,8 @@ struct AdjPhaseRec {
 };
 
 NPOM_HD size_t adj_field_len(const Ctx &c, int f) {
-  return (f >= NPOM_F_u && f <= NPOM_F_curv) ? (size_t)c.im * c.jm * c.kb : (size_t)c.im * c.jm;
+  const bool three_d = (f >= NPOM_F_u && f <= NPOM_F_curv) || f >= NPOM_NFIELDS + AW_COUNT;
+  return three_d ? (size_t)c.im * c.jm * c.kb : (size_t)c.im * c.jm;
 }
 
 // The 2-D fields external-substep phase ph (1, 2, 3) of substep iext
@@ -2534,12 +2549,39 @@ inline int adj_step_plan(const Ctx &c, AdjPhaseRec *out, int cap, size_t *save_f
       add(r, NPOM_F_uf, 1);
       add(r, NPOM_F_vf, 1);
     }
-    r = begin(AP_B5, 0, 0);
-    for (int f : {NPOM_F_q2b, NPOM_F_q2, NPOM_F_q2lb, NPOM_F_q2l, NPOM_F_uf, NPOM_F_vf, NPOM_F_t, NPOM_F_tb,
-                  NPOM_F_s, NPOM_F_sb})
-      add(r, f, 1);
-    if (imp && c.k.has_vmix)
-      for (int f : {NPOM_F_kh, NPOM_F_km, NPOM_F_kq}) add(r, f, 1);
+    if (c.k.nadv == 2 && c.k.mode != 4) {
+      r = begin(AP_MQ, 0, 0);
+      for (int f : {NPOM_F_q2b, NPOM_F_q2, NPOM_F_q2lb, NPOM_F_q2l}) add(r, f, 1);
+      r = begin(AP_MINIT, 0, 0);
+      for (int tr = 0; tr < 2; ++tr)
+        for (int m = 0; m < 3; ++m) add(r, mp_slot(tr, m), 1);
+      add(r, NPOM_F_tb, 1);
+      add(r, NPOM_F_sb, 1);
+      for (int it = 1; it <= c.k.nitera; ++it) {
+        r = begin(AP_MUP, it, 0);
+        for (int tr = 0; tr < 2; ++tr)
+          for (int m = 3; m < 6; ++m) add(r, mp_slot(tr, m), 1);
+        r = begin(AP_MFC, it, 0);
+        add(r, NPOM_F_uf, 1);
+        add(r, NPOM_F_vf, 1);
+        r = begin(AP_MAD, it, 0);
+        for (int tr = 0; tr < 2; ++tr)
+          for (int m = 0; m < 3; ++m) add(r, mp_slot(tr, m), 1);
+      }
+      r = begin(AP_MDIF, 0, 0);
+      for (int tr = 0; tr < 2; ++tr)
+        for (int m = 3; m < 5; ++m) add(r, mp_slot(tr, m), 1);
+      r = begin(AP_MFIN, 0, 0);
+      add(r, NPOM_F_uf, 1);
+      add(r, NPOM_F_vf, 1);
+    } else {
+      r = begin(AP_B5, 0, 0);
+      for (int f : {NPOM_F_q2b, NPOM_F_q2, NPOM_F_q2lb, NPOM_F_q2l, NPOM_F_uf, NPOM_F_vf, NPOM_F_t, NPOM_F_tb,
+                    NPOM_F_s, NPOM_F_sb})
+        add(r, f, 1);
+      if (imp && c.k.has_vmix)
+        for (int f : {NPOM_F_kh, NPOM_F_km, NPOM_F_kq}) add(r, f, 1);
+    }
     r = begin(AP_B6, 0, 0);
     for (int f : {NPOM_F_uf, NPOM_F_vf, NPOM_F_tps}) add(r, f, 1);
     r = begin(AP_B7, 0, 0);
@@ -2561,10 +2603,41 @@ inline int adj_step_plan(const Ctx &c, AdjPhaseRec *out, int cap, size_t *save_f
 inline bool adj_supported(const npom_params *p) {
   // the POM08-WAD PROFQ is forward only, as in the reference's case
   // policies (which refuse advancement with gradients)
-  const bool base = p->mode == 3 && p->nadv == 1 && (p->nbct == 1 || p->nbct == 3) &&
-                    (p->nbcs == 1 || p->nbcs == 3) && p->profq_form == NPOM_PROFQ_PRODUCTION;
-  if (p->core == NPOM_CORE_EXPLICIT) return base;
-  return base && p->core == NPOM_CORE_IMPLICIT && p->barotropic_shapiro == 0.0 && p->tracer_shapiro == 0.0;
+  const bool base = p->mode == 3 && (p->nbct == 1 || p->nbct == 3) && (p->nbcs == 1 || p->nbcs == 3) &&
+                    p->profq_form == NPOM_PROFQ_PRODUCTION;
+  // MPDATA (nadv 2) is an explicit-core setting
+  if (p->core == NPOM_CORE_EXPLICIT) return base && (p->nadv == 1 || p->nadv == 2);
+  return base && p->nadv == 1 && p->core == NPOM_CORE_IMPLICIT && p->barotropic_shapiro == 0.0 &&
+         p->tracer_shapiro == 0.0;
+}
+
+// The scratch of one step adjoint, after the plan's saves: G and L of the
+// workspace slots, the PCG solution, g, lambda and grad d (2-D planes),
+// then with MPDATA G and L of its slots (3-D arrays).
+constexpr int kAdjScratchPlanes = 2 * AW_COUNT + 4;
+NPOM_HD bool adj_has_mp(const Ctx &c) { return c.k.nadv == 2 && c.k.mode != 4; }
+inline size_t adj_scratch_floats(const Ctx &c) {
+  const size_t ncell = (size_t)c.im * c.jm;
+  return (size_t)kAdjScratchPlanes * ncell + (adj_has_mp(c) ? (size_t)2 * kAdjMpSlots * ncell * c.kb : 0);
+}
+// the floats of the scratch that start each step at zero: G of the
+// workspace slots, then (a separate range) G of the MPDATA slots
+inline size_t adj_mp_offset(const Ctx &c) { return (size_t)kAdjScratchPlanes * c.im * c.jm; }
+inline size_t adj_mp_zero_floats(const Ctx &c) {
+  return adj_has_mp(c) ? (size_t)kAdjMpSlots * c.im * c.jm * c.kb : 0;
+}
+// points the workspace and MPDATA slots of a into scratch
+inline void adj_bind_scratch(const Ctx &c, Adj &a, float *scratch) {
+  const size_t ncell = (size_t)c.im * c.jm, n3 = ncell * c.kb;
+  for (int w = 0; w < AW_COUNT; ++w) {
+    a.G[NPOM_NFIELDS + w] = scratch + (size_t)w * ncell;
+    a.L[NPOM_NFIELDS + w] = scratch + (size_t)(AW_COUNT + w) * ncell;
+  }
+  float *mp = scratch + adj_mp_offset(c);
+  for (int q = 0; q < kAdjMpSlots; ++q) {
+    a.G[NPOM_NFIELDS + AW_COUNT + q] = adj_has_mp(c) ? mp + (size_t)q * n3 : nullptr;
+    a.L[NPOM_NFIELDS + AW_COUNT + q] = adj_has_mp(c) ? mp + (size_t)(kAdjMpSlots + q) * n3 : nullptr;
+  }
 }
 
 }  // namespace npom

@@ -18,6 +18,16 @@ __global__ void __launch_bounds__(kThreads) k_ext_fwd(Ctx c, int phase, int iext
   else ext_phase3_cell(c, i, j, iext);
 }
 
+// the reverse of one MPDATA pass of B5 (plan phase ph, iteration it)
+__global__ void __launch_bounds__(kThreads) k_adj_mpdata(Ctx c, Adj a, int ph, int it) {
+  const size_t n = (size_t)c.im * c.jm * c.kb;
+  size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int k = (int)(p % c.kb);
+  const size_t col = p / c.kb;
+  mp_phase_adj(c, a, ph, it, (int)(col / c.jm), (int)(col % c.jm), k);
+}
+
 template <int PH>
 __global__ void __launch_bounds__(kThreads) k_adj_points(Ctx c, Adj a) {
   const size_t n = (size_t)c.im * c.jm * c.kb;
@@ -284,10 +294,6 @@ dim3 field_list_grid(const Ctx &c, const AdjPhaseRec &r) {
   return dim3((unsigned)std::max<size_t>(blocks, 1), (unsigned)std::max(r.n, 1));
 }
 
-// scratch planes of one step adjoint, after the plan's save records:
-// G and L of the workspace slots, the PCG solution, g, lambda, grad d
-constexpr int kAdjScratchPlanes = 2 * AW_COUNT + 4;
-
 struct ImpScratch {
   const float *xsaved;  // the forward solve's raw solution, or null (solve again)
   float *xs, *g, *lam, *gd;
@@ -329,6 +335,17 @@ void launch_fwd_phase(const Ctx &c, const AdjPhaseRec &r, const PcgPlan &pplan, 
     case AP_B7: launch_points<PP_B7>(c, s); break;
     case AP_B8: launch_cols<CP_B8>(c, s); break;
     case AP_B9: launch_cols<CP_B9>(c, s); break;
+    case AP_MQ:
+    case AP_MINIT:
+    case AP_MUP:
+    case AP_MFC:
+    case AP_MAD:
+    case AP_MDIF:
+    case AP_MFIN: {
+      const size_t n = (size_t)c.im * c.jm * c.kb;
+      k_mpdata<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, s>>>(c, mp_pass_of(r.phase), r.iext);
+      break;
+    }
   }
 }
 
@@ -367,6 +384,13 @@ npom_status launch_adj_phase(const npom_params *p, const npom_workspace *ws, con
     case AP_B7: k_adj_points<AP_B7><<<gp, kThreads, 0, s>>>(c, a); break;
     case AP_B8: launch_adj_cols<AP_B8>(c, a, s); break;
     case AP_B9: launch_adj_cols<AP_B9>(c, a, s); break;
+    case AP_MQ:
+    case AP_MINIT:
+    case AP_MUP:
+    case AP_MFC:
+    case AP_MAD:
+    case AP_MDIF:
+    case AP_MFIN: k_adj_mpdata<<<gp, kThreads, 0, s>>>(c, a, r.phase, r.iext); break;
   }
   return NPOM_OK;
 }
@@ -396,16 +420,13 @@ npom_status run_step_adjoint(const npom_params *p, float *const *fields, const n
     a.G[f] = grads[f];
     a.L[f] = aws->lam[f];
   }
-  std::vector<AdjPhaseRec> plan((size_t)(18 + 3 * p->isplit));
+  std::vector<AdjPhaseRec> plan((size_t)adj_plan_capacity(p->isplit, p->nitera));
   size_t need = 0;
   const int np = adj_step_plan(c, plan.data(), (int)plan.size(), &need);
   const size_t ncell = (size_t)c.im * c.jm;
-  if (need + kAdjScratchPlanes * ncell > aws->save_floats) return NPOM_ERR_ARG;
+  if (need + adj_scratch_floats(c) > aws->save_floats) return NPOM_ERR_ARG;
   float *scratch = aws->save + need;
-  for (int w = 0; w < AW_COUNT; ++w) {
-    a.G[NPOM_NFIELDS + w] = scratch + (size_t)w * ncell;
-    a.L[NPOM_NFIELDS + w] = scratch + (size_t)(AW_COUNT + w) * ncell;
-  }
+  adj_bind_scratch(c, a, scratch);
   ImpScratch is;
   is.xsaved = core == NPOM_CORE_IMPLICIT ? aws->pcg_x : nullptr;
   is.xs = scratch + (size_t)(2 * AW_COUNT) * ncell;
@@ -426,8 +447,11 @@ npom_status enqueue_step_adjoint(const npom_params *p, const npom_workspace *ws,
                                  const AdjPhaseRec *plan, int np, const ImpScratch &is, float *scratch,
                                  float *save, int core, cudaStream_t s) {
   const size_t ncell = (size_t)c.im * c.jm;
-  // workspace cotangents live inside one step
+  // workspace and MPDATA cotangents live inside one step
   if (cudaMemsetAsync(scratch, 0, (size_t)AW_COUNT * ncell * sizeof(float), s) != cudaSuccess) return NPOM_ERR_CUDA;
+  if (adj_mp_zero_floats(c) &&
+      cudaMemsetAsync(scratch + adj_mp_offset(c), 0, adj_mp_zero_floats(c) * sizeof(float), s) != cudaSuccess)
+    return NPOM_ERR_CUDA;
   PcgPlan pplan{};
   if (core == NPOM_CORE_IMPLICIT) {
     if (plan_pcg(c, &pplan) != cudaSuccess) return NPOM_ERR_CUDA;

@@ -29,6 +29,7 @@
 #include "npom_lanes.cuh"
 #include "npom_adjoint.cuh"
 #include "npom_mpdata.cuh"
+#include "npom_mpdata_adjoint.cuh"
 
 using namespace npom;
 
@@ -1512,15 +1513,12 @@ size_t npom_adjoint_save_floats(const npom_params *p) {
   c.im = p->im;
   c.jm = p->jm;
   c.kb = p->kb;
-  c.k.isplit = p->isplit;
-  c.k.ispadv = p->ispadv;
-  c.k.core = p->core;
-  c.k.has_vmix = p->has_vmix;
+  c.k = make_consts(*p);
   c.do_internal = 1;
-  std::vector<AdjPhaseRec> plan((size_t)(18 + 3 * p->isplit));
+  std::vector<AdjPhaseRec> plan((size_t)adj_plan_capacity(p->isplit, p->nitera));
   size_t need = 0;
   adj_step_plan(c, plan.data(), (int)plan.size(), &need);
-  return need + (size_t)kAdjScratchPlanes * (size_t)p->im * p->jm;
+  return need + adj_scratch_floats(c);
 }
 
 npom_status npom_step_explicit_adjoint(const npom_params *p, float *const *fields, const npom_workspace *ws,

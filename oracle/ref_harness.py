@@ -105,3 +105,47 @@ def advance(core, name, steps, differentiable=False, device="cpu", **physics_kw)
     kw = dict(core_name="explicit", compiled_kernels=()) if name == "explicit" else {}
     kw.update(physics_kw)
     SparsePhysics(device, **kw).advance(core, steps=steps, differentiable=differentiable)
+
+
+class ReferenceFloat64:
+    """Context in which the reference core computes in float64: the
+    default dtype is float64 and the float32 scratch its step allocates
+    explicitly (explicit/momentum.py:25-28,144-147,555-556 and the tracer
+    routines) is allocated as float64 instead.  The core's own tensors are
+    promoted by ``promote``."""
+
+    NAMES = ("zeros", "ones", "empty", "full", "tensor", "arange", "linspace", "zeros_like", "ones_like",
+             "empty_like", "full_like", "as_tensor")
+
+    def __enter__(self):
+        import torch
+        self.torch = torch
+        self.saved = {n: getattr(torch, n) for n in self.NAMES}
+
+        def wrap(fn):
+            def alloc(*a, **k):
+                if k.get("dtype") is torch.float32:
+                    k["dtype"] = torch.float64
+                return fn(*a, **k)
+            return alloc
+        self.prev = torch.get_default_dtype()
+        for n in self.NAMES:
+            setattr(torch, n, wrap(self.saved[n]))
+        torch.set_default_dtype(torch.float64)
+        return self
+
+    def __exit__(self, *exc):
+        for n, fn in self.saved.items():
+            setattr(self.torch, n, fn)
+        self.torch.set_default_dtype(self.prev)
+
+    @staticmethod
+    def promote(core):
+        import torch
+        for k, v in list(vars(core).items()):
+            if torch.is_tensor(v) and v.dtype == torch.float32:
+                setattr(core, k, v.to(torch.float64))
+        # solver caches are rebuilt from the promoted geometry
+        core._accel_cache_ready = False
+        core._spectral_eta_preconditioner_cache = None
+        core._cg_work = {}

@@ -16,6 +16,7 @@
 #include "../../neuralpom_b200/csrc/npom_host.cuh"
 #include "../../neuralpom_b200/csrc/npom_adjoint.cuh"
 #include "../../neuralpom_b200/csrc/npom_mpdata.cuh"
+#include "../../neuralpom_b200/csrc/npom_mpdata_adjoint.cuh"
 
 using namespace npom;
 
@@ -295,6 +296,15 @@ void fwd_plan_phase(const Ctx &c, const AdjPhaseRec &r, float *xs) {
     case AP_B7: each_point(c, [&](int i, int j, int k) { phase_b7_point(c, i, j, k); }); break;
     case AP_B8: each_cell(c, [&](int i, int j) { phase_b8_column(c, i, j); }); break;
     case AP_B9: each_cell(c, [&](int i, int j) { phase_b9_column(c, i, j); }); break;
+    case AP_MQ:
+    case AP_MINIT:
+    case AP_MUP:
+    case AP_MFC:
+    case AP_MAD:
+    case AP_MDIF:
+    case AP_MFIN:
+      each_point(c, [&](int i, int j, int k) { phase_b5_mpdata_point(c, mp_pass_of(r.phase), r.iext, i, j, k); });
+      break;
   }
 }
 
@@ -319,6 +329,15 @@ void adj_plan_phase(const Ctx &c, const Adj &a, const AdjPhaseRec &r, const floa
     case AP_B7: each_point(c, [&](int i, int j, int k) { phase_b7_point_adj(c, a, i, j, k); }); break;
     case AP_B8: each_cell(c, [&](int i, int j) { phase_b8_column_adj<KMAX>(c, a, i, j); }); break;
     case AP_B9: each_cell(c, [&](int i, int j) { phase_b9_column_adj<KMAX>(c, a, i, j); }); break;
+    case AP_MQ:
+    case AP_MINIT:
+    case AP_MUP:
+    case AP_MFC:
+    case AP_MAD:
+    case AP_MDIF:
+    case AP_MFIN:
+      each_point(c, [&](int i, int j, int k) { mp_phase_adj(c, a, r.phase, r.iext, i, j, k); });
+      break;
   }
 }
 
@@ -342,17 +361,14 @@ int emul_step_adjoint(const npom_params *p, float *const *fields, const npom_wor
     a.G[f] = grads[f];
     a.L[f] = lam[f];
   }
-  std::vector<AdjPhaseRec> plan((size_t)(18 + 3 * p->isplit));
+  std::vector<AdjPhaseRec> plan((size_t)adj_plan_capacity(p->isplit, p->nitera));
   size_t need = 0;
   const int np = adj_step_plan(c, plan.data(), (int)plan.size(), &need);
   const size_t ncell = (size_t)c.im * c.jm;
-  if (need + (2 * AW_COUNT + 4) * ncell > save_floats) return 2;
+  if (need + adj_scratch_floats(c) > save_floats) return 2;
   float *scratch = save + need;
-  std::memset(scratch, 0, (2 * AW_COUNT + 4) * ncell * 4);
-  for (int w = 0; w < AW_COUNT; ++w) {
-    a.G[NPOM_NFIELDS + w] = scratch + (size_t)w * ncell;
-    a.L[NPOM_NFIELDS + w] = scratch + (size_t)(AW_COUNT + w) * ncell;
-  }
+  std::memset(scratch, 0, adj_scratch_floats(c) * 4);
+  adj_bind_scratch(c, a, scratch);
   float *xs = scratch + (size_t)(2 * AW_COUNT) * ncell, *g = xs + ncell, *lamw = g + ncell, *gd = lamw + ncell;
   if (p->core == NPOM_CORE_IMPLICIT) each_cell(c, [&](int i, int j) { elliptic_coeff_cell(c, i, j); });
   for (int q = 0; q < np; ++q) {
@@ -389,9 +405,9 @@ int emul_adjoint_plan(const npom_params *p, int do_internal, size_t *save_floats
   c.kb = p->kb;
   c.k = make_consts(*p);
   c.do_internal = do_internal;
-  std::vector<AdjPhaseRec> plan((size_t)(18 + 3 * p->isplit));
+  std::vector<AdjPhaseRec> plan((size_t)adj_plan_capacity(p->isplit, p->nitera));
   const int np = adj_step_plan(c, plan.data(), (int)plan.size(), save_floats);
-  *save_floats += (2 * AW_COUNT + 4) * (size_t)c.im * c.jm;
+  *save_floats += adj_scratch_floats(c);
   return np;
 }
 

@@ -17,7 +17,7 @@ SRC = os.path.join(ROOT, "tests", "emul", "npom_emul.cu")
 OUT = os.path.join(ROOT, "tests", "emul", "_build", "libnpom_emul.so")
 DEPS = [SRC] + [os.path.join(ROOT, "neuralpom_b200", "csrc", f) for f in
                 ("npom_ctx.cuh", "npom_phases_a.cuh", "npom_phases_ext.cuh", "npom_phases_int.cuh", "npom_host.cuh",
-                 "npom_adjoint.cuh")]
+                 "npom_adjoint.cuh", "npom_mpdata.cuh", "npom_mpdata_adjoint.cuh")]
 
 _LIB = None
 

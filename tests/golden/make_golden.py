@@ -329,6 +329,59 @@ def make_mpdata_golden(im=12, jm=10, seed=51):
     make_step_golden("explicit", im, jm, seed, core=core, tag="mpdata")
 
 
+def make_mpdata_adjoint_golden(im=12, jm=10, seed=52, steps=(1, 3), ndirs=2, eps=1e-6):
+    """Reverse mode of the explicit step with MPDATA tracer advection
+    (nadv = 2) on a perturbed production state, 1 and 3 steps.
+
+    The reference's autograd of ADVT2 is not the derivative of its forward:
+    SMOL_ADIF reassigns slices of the mass fluxes in place after abs() and
+    the square have saved them (explicit/tracers.py:607-633,648-667,
+    685-706).  Without the step checkpoint torch refuses that backward;
+    under SparsePhysics' non-reentrant checkpoint (sparse_physics.py:140)
+    the recomputation hands the backward the overwritten tensors,
+    so the u, v, etb, ... gradients it returns differ from the forward's
+    derivative by a few per cent.  This file therefore also records
+    directional derivatives of the reference's own forward in float64:
+    for every field autograd differentiates, ``ndirs`` seeded relative
+    directions d = r |x| (r standard normal: no value crosses zero, so the
+    clamps of the small turbulence fields keep their branch;
+    ``dir{n}__{f}__{q}``) and the central difference
+    (J(x + eps d) - J(x - eps d)) / (2 eps) of J = sum(cot * state after n
+    steps) (``fd{n}__{f}__{q}``)."""
+    import torch
+    core = perturbed_core("explicit", im, jm, seed)
+    core.nadv = 2
+    core.time0 = float(core.time)
+    make_step_adjoint_golden("mpdata", core, steps=steps, seed=seed + 1)
+    path = os.path.join(HERE, f"step_adjoint_mpdata_{im}x{jm}.npz")
+    z = dict(np.load(path))
+    A = {k[4:]: v for k, v in z.items() if k.startswith("in__")}
+    Sc = {k[8:]: v.item() for k, v in z.items() if k.startswith("scalar__")}
+    cot = {k[5:]: v for k, v in z.items() if k.startswith("cot__")}
+    g = np.random.default_rng(seed + 2)
+
+    def loss(n, f, d):
+        c2 = rh.build_reference_core("explicit", im, jm)
+        rh.load_state(c2, A, Sc)
+        rh.ReferenceFloat64.promote(c2)
+        with rh.ReferenceFloat64():
+            setattr(c2, f, getattr(c2, f) + torch.from_numpy(d))
+            rh.advance(c2, "explicit", n)
+        return sum(float((getattr(c2, h).detach().double() * torch.from_numpy(cot[h]).double()).sum())
+                   for h in cot)
+
+    for n in steps:
+        fields = [k.split("__")[1] for k in z if k.startswith(f"grad{n}__")]
+        for f in fields:
+            for q in range(ndirs):
+                d = g.standard_normal(A[f].shape) * np.abs(A[f].astype(np.float64))
+                z[f"dir{n}__{f}__{q}"] = d.astype(np.float32)
+                d = z[f"dir{n}__{f}__{q}"].astype(np.float64)
+                z[f"fd{n}__{f}__{q}"] = np.asarray((loss(n, f, eps * d) - loss(n, f, -eps * d)) / (2 * eps))
+    np.savez_compressed(path, **z)
+    print("wrote", path, os.path.getsize(path))
+
+
 def make_pom08_goldens():
     """Both cores with the POM08-WAD closure of the reference's case
     policies bound by the reference's own installer
@@ -368,6 +421,7 @@ def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint", "couplin
         make_coupling_golden()
     if "mpdata" in which:
         make_mpdata_golden()
+        make_mpdata_adjoint_golden()
     if "pom08" in which:
         make_pom08_goldens()
 

@@ -90,6 +90,34 @@ def load_adjoint_golden(name):
     return A, Sc, cot, grads
 
 
+def load_directional_golden(name):
+    """{nsteps: {field: [(direction, float64 central difference), ...]}}
+    of a step_adjoint_*.npz file that records directional derivatives of
+    the reference's forward (``dir{n}__{f}__{q}`` / ``fd{n}__{f}__{q}``)."""
+    z = np.load(golden_path(name))
+    out = {}
+    for k in z.files:
+        if k.startswith("dir"):
+            n, f, q = k[3:].split("__")
+            out.setdefault(int(n), {}).setdefault(f, []).append((z[k].astype(np.float64),
+                                                                 float(z[f"fd{n}__{f}__{q}"])))
+    return out
+
+
+def directional_check(got, dirs, tol):
+    """[] when every directional derivative ad = <got_f, d> meets
+    |ad - fd| <= tol * sum|got_f * d| (the size of the derivative before
+    its terms cancel), else (field, ad, fd) of the failing ones."""
+    bad = []
+    for f, pairs in dirs.items():
+        g = np.asarray(got[f], dtype=np.float64)
+        for d, fd in pairs:
+            ad = float((g * d).sum())
+            if abs(ad - fd) > tol * max(float(np.abs(g * d).sum()), 1e-30):
+                bad.append((f, ad, fd))
+    return bad
+
+
 def grad_errors(got, ref):
     """max|g - g_ref| / max|g_ref| per field of ``ref``."""
     out = {}
