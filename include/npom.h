@@ -328,7 +328,8 @@ size_t npom_adjoint_save_floats(const npom_params *p);
  * the cotangent of field f after the step, on exit the cotangent of f
  * before it (vector-Jacobian product, accumulated in place).  Geometry,
  * forcing and open-boundary arrays are constants.  Supported settings:
- * explicit core, mode 3, nadv 1, nbct/nbcs 1 or 3; else NPOM_ERR_ARG.
+ * explicit core, mode 3, nadv 1 or 2 (MPDATA), nbct/nbcs 1 or 3, the
+ * production PROFQ; else NPOM_ERR_ARG.
  * The caller's save area also holds the step's scratch:
  * npom_adjoint_save_floats includes it. */
 npom_status npom_step_explicit_adjoint(const npom_params *p, float *const *fields,
