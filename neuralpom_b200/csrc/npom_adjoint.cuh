@@ -2552,6 +2552,8 @@ inline int adj_step_plan(const Ctx &c, AdjPhaseRec *out, int cap, size_t *save_f
     if (c.k.nadv == 2 && c.k.mode != 4) {
       r = begin(AP_MQ, 0, 0);
       for (int f : {NPOM_F_q2b, NPOM_F_q2, NPOM_F_q2lb, NPOM_F_q2l}) add(r, f, 1);
+      if (imp && c.k.has_vmix)
+        for (int f : {NPOM_F_kh, NPOM_F_km, NPOM_F_kq}) add(r, f, 1);
       r = begin(AP_MINIT, 0, 0);
       for (int tr = 0; tr < 2; ++tr)
         for (int m = 0; m < 3; ++m) add(r, mp_slot(tr, m), 1);
@@ -2605,9 +2607,8 @@ inline bool adj_supported(const npom_params *p) {
   // policies (which refuse advancement with gradients)
   const bool base = p->mode == 3 && (p->nbct == 1 || p->nbct == 3) && (p->nbcs == 1 || p->nbcs == 3) &&
                     p->profq_form == NPOM_PROFQ_PRODUCTION;
-  // MPDATA (nadv 2) is an explicit-core setting
   if (p->core == NPOM_CORE_EXPLICIT) return base && (p->nadv == 1 || p->nadv == 2);
-  return base && p->nadv == 1 && p->core == NPOM_CORE_IMPLICIT && p->barotropic_shapiro == 0.0 &&
+  return base && (p->nadv == 1 || p->nadv == 2) && p->core == NPOM_CORE_IMPLICIT && p->barotropic_shapiro == 0.0 &&
          p->tracer_shapiro == 0.0;
 }
 

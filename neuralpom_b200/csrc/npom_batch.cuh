@@ -619,7 +619,6 @@ npom_status run_batch_steps(int nm, const npom_params *const *p, float *const *c
   if (!batch_uniform(p, nm)) return NPOM_ERR_ARG;
   const int core = p[0]->core;
   if (core != NPOM_CORE_EXPLICIT && core != NPOM_CORE_IMPLICIT) return NPOM_ERR_ARG;
-  if (p[0]->nadv == 2 && core != NPOM_CORE_EXPLICIT) return NPOM_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   std::vector<Ctx> ctx(nm);
   for (int m = 0; m < nm; ++m) ctx[m] = make_ctx(p[m], fields[m], ws[m]);

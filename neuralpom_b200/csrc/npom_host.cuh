@@ -97,7 +97,7 @@ inline bool check_args(const npom_params *p, float *const *fields, const npom_wo
   for (int f = 0; f < NPOM_NFIELDS; ++f)
     if (!fields[f]) return false;
   if (!ws->partials || !ws->sync || !ws->status || !ws->cg_iters) return false;
-  if (p->nadv != 1 && (p->nadv != 2 || p->core != NPOM_CORE_EXPLICIT || !ws->mp3d || p->nitera < 1)) return false;
+  if (p->nadv != 1 && (p->nadv != 2 || !ws->mp3d || p->nitera < 1)) return false;
   for (int w = 0; w < NPOM_NWS; ++w)
     if (!ws->buf[w]) return false;
   return true;

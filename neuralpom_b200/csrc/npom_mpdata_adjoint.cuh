@@ -39,8 +39,17 @@ NPOM_HD void mp_up_adj(const Adj &a, int tr, int arr, size_t o, float F, float i
   aadd(&a.G[fbm][oo], lam * 0.5f * (F - af));
 }
 
-// the q2/q2l filter (phase_b5_filter) of B5
+// the q2/q2l filter (phase_b5_filter) of B5, and on the semi-implicit core
+// the clamp of kh, km, kq to [0, vmix]: the gradient passes where
+// 0 <= x <= vmix
 NPOM_HD void mp_filter_adj(const Ctx &c, const Adj &a, int i, int j, int k) {
+  if (!is_explicit(c) && c.k.has_vmix) {
+    const float vm = c.k.vmix;
+    const float kh = F3(kh, i, j, k), km = F3(km, i, j, k), kq = F3(kq, i, j, k);
+    GA3(kh, i, j, k, (kh >= 0.0f && kh <= vm) ? LA3(kh, i, j, k) : 0.0f);
+    GA3(km, i, j, k, (km >= 0.0f && km <= vm) ? LA3(km, i, j, k) : 0.0f);
+    GA3(kq, i, j, k, (kq >= 0.0f && kq <= vm) ? LA3(kq, i, j, k) : 0.0f);
+  }
   const float fsm = F2(fsm, i, j), hs = c.k.half_smoth, ohs = 1.0f - 2.0f * hs;
   const float lq2b = LA3(q2b, i, j, k), lq2lb = LA3(q2lb, i, j, k);
   GA3(q2, i, j, k, lq2b * ohs);

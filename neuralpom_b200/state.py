@@ -84,8 +84,8 @@ def make_params(s, im, jm, kb, core, device=0):
     p.ispadv = int(get("ispadv", 5))
     p.nbct, p.nbcs, p.ntp = int(get("nbct", 1)), int(get("nbcs", 1)), int(get("ntp", 2))
     p.mode, p.nadv = int(get("mode", 3)), int(get("nadv", 1))
-    if p.nadv not in (1, 2) or (p.nadv == 2 and core != "explicit"):
-        raise ValueError("tracer advection: nadv=1 (centred) for both cores, nadv=2 (MPDATA) for the explicit core")
+    if p.nadv not in (1, 2):
+        raise ValueError("tracer advection: nadv=1 (centred) or nadv=2 (MPDATA)")
     p.nitera, p.sw = int(get("nitera", 2)), float(get("sw", 0.5))
     if p.nitera < 1:
         raise ValueError("nitera must be positive")

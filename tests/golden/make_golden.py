@@ -321,15 +321,21 @@ def make_coupling_golden(im=12, jm=10, seed=41):
 
 
 def make_mpdata_golden(im=12, jm=10, seed=51):
-    """The explicit core with MPDATA tracer advection (nadv = 2, ADVT2 and
-    SMOL_ADIF, explicit/tracers.py:571-888) on a perturbed production
-    state, 1 and 3 steps."""
+    """Both cores with MPDATA tracer advection (nadv = 2, ADVT2 and
+    SMOL_ADIF, explicit/tracers.py:571-888; the semi-implicit core reaches
+    its copy through its numerics policy, implicit_p0_fixed/numerics/
+    double_gyre.py:60-74) on perturbed production states, 1 and 3 steps."""
     core = perturbed_core("explicit", im, jm, seed)
     core.nadv = 2
     make_step_golden("explicit", im, jm, seed, core=core, tag="mpdata")
+    name = "implicit_p0_fixed"
+    core = perturbed_core(name, im, jm, seed + 5)
+    core.nadv = 2
+    make_step_golden(name, im, jm, seed + 5, core=core, tag="mpdata_implicit")
 
 
-def make_mpdata_adjoint_golden(im=12, jm=10, seed=52, steps=(1, 3), ndirs=2, eps=1e-6):
+def make_mpdata_adjoint_golden(im=12, jm=10, seed=52, steps=(1, 3), ndirs=2, eps=1e-6, name="explicit",
+                               tag="mpdata"):
     """Reverse mode of the explicit step with MPDATA tracer advection
     (nadv = 2) on a perturbed production state, 1 and 3 steps.
 
@@ -349,11 +355,11 @@ def make_mpdata_adjoint_golden(im=12, jm=10, seed=52, steps=(1, 3), ndirs=2, eps
     (J(x + eps d) - J(x - eps d)) / (2 eps) of J = sum(cot * state after n
     steps) (``fd{n}__{f}__{q}``)."""
     import torch
-    core = perturbed_core("explicit", im, jm, seed)
+    core = perturbed_core(name, im, jm, seed)
     core.nadv = 2
     core.time0 = float(core.time)
-    make_step_adjoint_golden("mpdata", core, steps=steps, seed=seed + 1)
-    path = os.path.join(HERE, f"step_adjoint_mpdata_{im}x{jm}.npz")
+    make_step_adjoint_golden(tag, core, steps=steps, seed=seed + 1, name=name)
+    path = os.path.join(HERE, f"step_adjoint_{tag}_{im}x{jm}.npz")
     z = dict(np.load(path))
     A = {k[4:]: v for k, v in z.items() if k.startswith("in__")}
     Sc = {k[8:]: v.item() for k, v in z.items() if k.startswith("scalar__")}
@@ -361,12 +367,14 @@ def make_mpdata_adjoint_golden(im=12, jm=10, seed=52, steps=(1, 3), ndirs=2, eps
     g = np.random.default_rng(seed + 2)
 
     def loss(n, f, d):
-        c2 = rh.build_reference_core("explicit", im, jm)
+        c2 = rh.build_reference_core(name, im, jm)
         rh.load_state(c2, A, Sc)
         rh.ReferenceFloat64.promote(c2)
         with rh.ReferenceFloat64():
+            if hasattr(c2, "_build_acceleration_cache"):
+                c2._build_acceleration_cache()
             setattr(c2, f, getattr(c2, f) + torch.from_numpy(d))
-            rh.advance(c2, "explicit", n)
+            rh.advance(c2, name, n)
         return sum(float((getattr(c2, h).detach().double() * torch.from_numpy(cot[h]).double()).sum())
                    for h in cot)
 
@@ -422,6 +430,7 @@ def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint", "couplin
     if "mpdata" in which:
         make_mpdata_golden()
         make_mpdata_adjoint_golden()
+        make_mpdata_adjoint_golden(seed=54, steps=(1, 2), name="implicit_p0_fixed", tag="mpdata_implicit")
     if "pom08" in which:
         make_pom08_goldens()
 

@@ -37,22 +37,28 @@ def test_emulated_step_adjoint_matches_reference_autograd(fname):
             assert np.any(G[f] != 0), (fname, n, f)
 
 
-def test_emulated_mpdata_adjoint_matches_reference_float64_differences():
-    """MPDATA tracer advection (nadv = 2): the emulated adjoint of 1 and 3
-    steps along two seeded directions per differentiated field against
+MPDATA_ADJOINT = [("step_adjoint_mpdata_12x10.npz", "explicit"),
+                  ("step_adjoint_mpdata_implicit_12x10.npz", "implicit_p0_fixed")]
+
+
+@pytest.mark.parametrize("fname,core", MPDATA_ADJOINT)
+def test_emulated_mpdata_adjoint_matches_reference_float64_differences(fname, core):
+    """MPDATA tracer advection (nadv = 2), both cores: the emulated adjoint
+    of 1 and 3 steps (explicit; 1 and 2 semi-implicit) along two seeded
+    directions per differentiated field against
     central differences of the reference's own forward in float64 (the
     reference's autograd of this path reads tensors its forward overwrote
     in place, so its gradient is recorded but not the bar: its utb
     derivative, for one, is 5.6e-3 off after one step).  Tolerance, of
-    sum |g * d|: 2e-3 after one step, 2e-2 after three (the float32
+    sum |g * d|: 2e-3 after one step, 2e-2 after more (the float32
     trajectory's own Jacobian; the reference's autograd sits as far from
     the float64 differences on the fields it gets right); and every field
     the reference differentiates is reached."""
-    A, Sc, cot, grads = load_adjoint_golden("step_adjoint_mpdata_12x10.npz")
-    dirs = load_directional_golden("step_adjoint_mpdata_12x10.npz")
-    assert int(Sc["nadv"]) == 2 and sorted(dirs) == [1, 3]
+    A, Sc, cot, grads = load_adjoint_golden(fname)
+    dirs = load_directional_golden(fname)
+    assert int(Sc["nadv"]) == 2 and len(dirs) == 2
     for n, per_field in sorted(dirs.items()):
-        G = emul.multi_step_adjoint(A, Sc, cot, n, core="explicit")
+        G = emul.multi_step_adjoint(A, Sc, cot, n, core=core)
         tol = 2e-3 if n == 1 else 2e-2
         assert directional_check(G, per_field, tol) == [], (n, directional_check(G, per_field, tol))
         for f in grads[n]:

@@ -63,13 +63,16 @@ def test_emulated_step_matches_oracle_on_cases(name):
         assert rel_err(E.F[f], S[f]) < 2e-4, (name, f, rel_err(E.F[f], S[f]))
 
 
-def test_emulated_mpdata_step_matches_reference():
+@pytest.mark.parametrize("fname,core", [("step_mpdata_12x10.npz", "explicit"),
+                                        ("step_mpdata_implicit_12x10.npz", "implicit_p0_fixed")])
+def test_emulated_mpdata_step_matches_reference(fname, core):
     """MPDATA tracer advection (nadv = 2: ADVT2 + SMOL_ADIF,
-    explicit/tracers.py:571-888), the device bodies run on the CPU, against
-    the reference's own steps (1e-5 after one step, 1e-4 after three)."""
-    A, Sc, OUT = load_step_golden("step_mpdata_12x10.npz")
+    explicit/tracers.py:571-888, on the semi-implicit core through its
+    numerics policy), the device bodies run on the CPU, against the
+    reference's own steps (1e-5 after one step, 1e-4 after three)."""
+    A, Sc, OUT = load_step_golden(fname)
     assert int(Sc["nadv"]) == 2
-    E = emul.EmulCore(A, Sc, "explicit")
+    E = emul.EmulCore(A, Sc, core)
     done = 0
     for n in sorted(OUT):
         E.steps(n - done)
@@ -80,6 +83,6 @@ def test_emulated_mpdata_step_matches_reference():
                 continue
             assert rel_err(E.F[f], ref) < tol, (n, f, rel_err(E.F[f], ref))
     # and the centred scheme on the same inputs is far from it
-    E1 = emul.EmulCore(A, dict(Sc, nadv=1), "explicit")
+    E1 = emul.EmulCore(A, dict(Sc, nadv=1), core)
     E1.steps(1)
     assert rel_err(E1.F["t"], OUT[1]["t"]) > 3e-5      # 7e-5: one step of different advection

@@ -11,7 +11,7 @@ pytestmark = pytest.mark.gpu
 
 STEP_FILES = [("step_explicit_12x10.npz", "explicit"), ("step_implicit_12x10.npz", "implicit_p0_fixed"),
               ("step_implicit_20x18.npz", "implicit_p0_fixed"), ("step_coastal_40x34.npz", "explicit"),
-              ("step_mpdata_12x10.npz", "explicit"),
+              ("step_mpdata_12x10.npz", "explicit"), ("step_mpdata_implicit_12x10.npz", "implicit_p0_fixed"),
               # the POM08-WAD closure of the reference's case policies
               ("step_pom08_explicit_12x10.npz", "explicit"), ("step_pom08_implicit_20x18.npz", "implicit_p0_fixed")]
 

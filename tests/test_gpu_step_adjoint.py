@@ -61,16 +61,18 @@ def test_gpu_step_adjoint_matches_reference_autograd(monkeypatch, fname, ext):
         assert grad_check(got, ref) == [], (fname, n, grad_check(got, ref))
 
 
-def test_gpu_mpdata_step_adjoint_matches_reference_float64_differences():
-    """MPDATA tracer advection (nadv = 2): the CUDA step adjoint of 1 and 3
-    steps along the golden's seeded directions against central differences
-    of the reference's forward in float64, the bar of the emulated adjoint
-    (of sum |g * d|: 2e-3 after one step, 2e-2 after three)."""
-    A, Sc, cot, grads = load_adjoint_golden("step_adjoint_mpdata_12x10.npz")
-    dirs = load_directional_golden("step_adjoint_mpdata_12x10.npz")
+@pytest.mark.parametrize("fname", ["step_adjoint_mpdata_12x10.npz", "step_adjoint_mpdata_implicit_12x10.npz"])
+def test_gpu_mpdata_step_adjoint_matches_reference_float64_differences(fname):
+    """MPDATA tracer advection (nadv = 2), both cores: the CUDA step adjoint
+    of 1 and 3 steps (1 and 2 semi-implicit) along the golden's seeded
+    directions against central differences of the reference's forward in
+    float64, the bar of the emulated adjoint (of sum |g * d|: 2e-3 after
+    one step, 2e-2 after more)."""
+    A, Sc, cot, grads = load_adjoint_golden(fname)
+    dirs = load_directional_golden(fname)
     assert int(Sc["nadv"]) == 2
     for n, per_field in sorted(dirs.items()):
-        core = _core(A, Sc)
+        core = _core(A, Sc, _core_name(fname))
         leaves = _differentiable_advance(core, n, float(Sc["time"]))
         loss = sum((getattr(core, f) * torch.from_numpy(c).cuda()).sum() for f, c in cot.items())
         loss.backward()
