@@ -384,6 +384,17 @@ npom_status npom_baropg_adjoint(const npom_params *p, float *const *fields,
 npom_status npom_status_read(const npom_workspace *ws, int clear,
                              unsigned int *out_bits, void *stream);
 
+/* Failure-path diagnostic (no reference counterpart): runs one of the
+ * library's bounded waits on a condition that nothing satisfies, so that
+ * it runs out the way a lost block or a lost peer CTA would make it:
+ *   which = 0  the grid barrier of the cooperative kernels (one block of a
+ *              two-block grid; gives up after 2 s),
+ *   which = 1  the mbarrier wait of the cluster PCG's bulk exchanges (its
+ *              own arrival, with bytes that never come; 0.5 s).
+ * The wait records NPOM_DEV_TIMEOUT in ws's status word and the kernel
+ * returns; the context stays usable.  Clears ws's barrier words first. */
+npom_status npom_wait_selftest(int which, const npom_workspace *ws, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -187,6 +187,8 @@ def load_library():
         fn.argtypes = [P(NpomParams), P(FieldArray), P(NpomWorkspace), P(NpomClock), P(FieldArray),
                        P(NpomAdjointWs), vp]
     lib.npom_status_read.argtypes = [P(NpomWorkspace), i32, P(ctypes.c_uint), vp]
+    lib.npom_wait_selftest.restype = i32
+    lib.npom_wait_selftest.argtypes = [i32, P(NpomWorkspace), vp]
     check_layout(lib)
     _LIB = lib
     return lib

@@ -1294,6 +1294,30 @@ cudaError_t enqueue_adj_solve(const Ctx &c, const npom_workspace *ws, const floa
                               cudaStream_t s);
 
 #include "npom_adjoint_launch.cuh"
+
+// The bounded waits, run out on purpose (npom_wait_selftest): one block of
+// a virtual two-block grid at the grid barrier -- the second block never
+// arrives -- and one CTA at an exchange mbarrier whose bytes never come.
+__global__ void __launch_bounds__(kThreads) k_selftest_grid_wait(unsigned int *sync, unsigned int *status) {
+  Ctx c;
+  memset(&c, 0, sizeof(c));
+  c.sync = sync;
+  c.status = status;
+  c.grid_blocks = 2;
+  c.grid_base = 0;
+  (void)grid_barrier(c);
+}
+
+__global__ void __launch_bounds__(kClusterThreads) k_selftest_exchange_wait(unsigned int *status) {
+  __shared__ uint64_t mb;
+  if (threadIdx.x == 0) {
+    mb_init(&mb, 1);
+    mb_init_fence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) mb_expect(&mb, 16);
+  (void)xb_wait(&mb, 0, status);
+}
 #include "npom_batch.cuh"
 
 const char *kFieldNames[] = {
@@ -1723,6 +1747,15 @@ npom_status npom_pcg_solve_static(const npom_params *p, float *const *fields, co
   if (status_out &&
       cudaMemcpyAsync(status_out, ws.status, sizeof(unsigned int), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
     return NPOM_ERR_CUDA;
+  return cudaGetLastError() == cudaSuccess ? NPOM_OK : NPOM_ERR_CUDA;
+}
+
+npom_status npom_wait_selftest(int which, const npom_workspace *ws, void *stream) {
+  if (!ws || !ws->sync || !ws->status || (which != 0 && which != 1)) return NPOM_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (cudaMemsetAsync(ws->sync, 0, 4 * sizeof(unsigned int), s) != cudaSuccess) return NPOM_ERR_CUDA;
+  if (which == 0) k_selftest_grid_wait<<<1, kThreads, 0, s>>>(ws->sync, ws->status);
+  else k_selftest_exchange_wait<<<1, kClusterThreads, 0, s>>>(ws->status);
   return cudaGetLastError() == cudaSuccess ? NPOM_OK : NPOM_ERR_CUDA;
 }
 
