@@ -1,16 +1,21 @@
 """The Midtrain-shaped configuration (explicit core, 90x82x16 noise basin,
 dtE = 6 s, isplit = 20, dtI = 120 s, T/S/u/v-perturbed member) at its own
-size: the hand-written step adjoint of its 3 h window against central
-differences of the float64 oracle.
+size: the hand-written step adjoint against central differences of the
+float64 oracle.
 
-90 differentiable internal steps (the configuration's three 1 h intervals
-of physics) through the drop-in API, loss = MSE of u, v, T, S against a
-seeded target, the gradient along 16 random unit directions of (T, S, u, v)
-against central differences (eps = 1e-3) of the oracle in float64 (run in
-parallel worker processes), within 2e-3 of the rms directional derivative,
-the bar of the smaller checks.  The corrector increments between the
-intervals are left out: the oracle restates the physics only (the coupling
-is checked against the reference's own autograd in test_gpu_coupling).
+The window's loss is smooth only over a short horizon.  Measured on the
+float64 oracle along one unit direction of (T, S, u, v): over 10 steps the
+central difference is the same to 1e-7 for eps = 1e-7 and 1e-8; over 30
+steps it still moves by 1e-3 between eps = 1e-6 and 1e-8, and by 40%
+between eps = 1e-3 and 1e-5; over the full 90 steps eps = 1e-3 and 1e-5
+give opposite signs.  The noise member drives the turbulence closure's
+clamps and |.| terms and the limiters across their kinks at every
+perturbation size, so a finite difference over the whole 3 h window does
+not measure a derivative.  The check therefore runs the first 10 steps
+(20 min, every phase of the step 10 times, 200 external substeps) at the
+configuration's full size: 16 random unit directions, eps = 1e-7, within
+2e-3 of the rms directional derivative (the float32 and float64 Jacobians
+differ at that level), the bar of the smaller checks.
 """
 import os
 import tempfile
@@ -24,13 +29,13 @@ from oracle_days import fd_losses
 pytestmark = pytest.mark.gpu
 
 
-def test_gpu_midtrain_90x82_window_adjoint_matches_float64_differences():
+def test_gpu_midtrain_90x82_adjoint_matches_float64_differences():
     import bench
     from neuralpom_b200 import _abi, resolve_core_class
     A, Sc = bench.midtrain_case(0)
     im, jm, kb = A["u"].shape
     t0 = float(Sc["time"])
-    steps = bench.FA_INTERVALS * bench.FA_STEPS_PER_INTERVAL
+    steps = 10
     core = resolve_core_class("explicit").from_state(A, Sc, device="cuda")
     start = {f: getattr(core, f).detach().cpu().numpy().copy() for f in A}
     rng = np.random.default_rng(23)
@@ -64,8 +69,8 @@ def test_gpu_midtrain_90x82_window_adjoint_matches_float64_differences():
             arrays.update({f"dir{i}__{f}": v for f, v in d.items()})
         np.savez(path, **arrays)
         scal = dict(Sc, im=im, jm=jm, kb=kb, time=t0, time0=t0)
-        pairs = fd_losses(path, scal, "explicit", steps, len(dirs), 1e-3, workers=min(16, os.cpu_count() or 1))
-    fds = np.array([(p - m) / 2e-3 for p, m in pairs])
+        pairs = fd_losses(path, scal, "explicit", steps, len(dirs), 1e-7, workers=min(16, os.cpu_count() or 1))
+    fds = np.array([(p - m) / 2e-7 for p, m in pairs])
     rms = float(np.sqrt((ads ** 2).mean()))
     err = np.abs(fds - ads) / rms
     print("midtrain 90x82 FD", fds, "adjoint", ads, "max err / rms", err.max(), "median", np.median(err))
