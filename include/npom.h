@@ -143,6 +143,7 @@ typedef struct npom_params {
   double sw;               /* MPDATA antidiffusion weight (nadv 2)         */
   int32_t nitera;          /* MPDATA iterations (nadv 2)                   */
   int32_t profq_form;      /* NPOM_PROFQ_PRODUCTION or NPOM_PROFQ_POM08    */
+  int32_t obc_form;        /* NPOM_OBC_NATIVE or NPOM_OBC_SEAMOUNT          */
   npom_tuning tuning;      /* launch shapes (all zero: the library's rules) */
   double zsh;              /* POM08-WAD profq: roughness added to the mixing length (m) */
 } npom_params;
@@ -153,6 +154,16 @@ typedef struct npom_params {
  * installed by dg_policy.py, coastal_compat.py, jzb_compat.py): forward
  * only, as in the reference, which validates it for forward comparisons. */
 enum { NPOM_PROFQ_PRODUCTION = 0, NPOM_PROFQ_POM08 = 1 };
+
+/* Boundary policy (obc_form).  NATIVE: the core's own bcond (closed walls,
+ * or the explicit core's Flather/upstream open boundary).  SEAMOUNT: the
+ * explicit core with the seamount case policy's boundary
+ * (cores/case_adapters/seamount_boundary.py:9-47): η ghost copies and
+ * characteristic radiation on the east and west edges, Orlanski radiation
+ * of u and of T/S (with the exterior profile on inflow), 1e-10 turbulence
+ * edges; the north and south edges are walls.  Forward only (the reference
+ * refuses gradients through its case policies). */
+enum { NPOM_OBC_NATIVE = 0, NPOM_OBC_SEAMOUNT = 1 };
 
 enum { NPOM_CORE_EXPLICIT = 0, NPOM_CORE_IMPLICIT = 1 };
 enum { NPOM_PRECOND_JACOBI = 0, NPOM_PRECOND_SPECTRAL = 1 };

@@ -36,6 +36,7 @@ FIELDS_3D = tuple("u ub uf v vb vf w t tb s sb rho rmean tclim sclim q2 q2b q2l 
 CORE_EXPLICIT, CORE_IMPLICIT = 0, 1
 PRECOND_JACOBI, PRECOND_SPECTRAL = 0, 1
 PROFQ_PRODUCTION, PROFQ_POM08 = 0, 1
+OBC_NATIVE, OBC_SEAMOUNT = 0, 1
 DEV_VMAX, DEV_TIMEOUT, DEV_PCG_MAXIT, DEV_NONFINITE = 0x1, 0x2, 0x4, 0x8
 MAX_COOP_BLOCKS = 1024
 
@@ -86,7 +87,8 @@ class NpomParams(ctypes.Structure):
             "small", "kappa", "rhoref", "tbias", "sbias", "vmaxl", "hmax", "rfe", "rfw", "rfn", "rfs", "aam_min",
             "pi", "eta_tol", "eta_rel_tol", "barotropic_shapiro", "tracer_shapiro", "velocity_shapiro",
             "wind_tau0", "vmix", "period", "inverse_scale", "sw")] + [
-        ("nitera", ctypes.c_int32), ("profq_form", ctypes.c_int32), ("tuning", NpomTuning), ("zsh", ctypes.c_double)]
+        ("nitera", ctypes.c_int32), ("profq_form", ctypes.c_int32),
+        ("obc_form", ctypes.c_int32), ("tuning", NpomTuning), ("zsh", ctypes.c_double)]
 
 
 class NpomWorkspace(ctypes.Structure):

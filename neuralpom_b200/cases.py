@@ -320,3 +320,55 @@ def coastal_tide(im=354, jm=322, kb=16, dte=2.0, isplit=30, dx=500.0, seed=4, la
     A["tbs"] = A["tb"][:, 0, :].copy()
     A["sbs"] = A["sb"][:, 0, :].copy()
     return finish_initialization(A, s, core)
+
+
+def seamount_policy(A, s):
+    """The seamount case policy's set-up on a state (cores/case_adapters/
+    seamount_runtime.py:7-25): the exterior elevations, transports and T/S
+    profiles taken from the current state's edge rows and columns, rf = 1,
+    alpha and smoth of the explicit core, the POM08-WAD closure (zsh =
+    0.01 m) and the seamount boundary (``obc_form``)."""
+    A = dict(A)
+    A["uabe"], A["uabw"] = A["uab"][-2, :].copy(), A["uab"][1, :].copy()
+    A["vabn"], A["vabs"] = A["va"][:, -2].copy(), A["va"][:, 1].copy()
+    A["ele"], A["elw"] = A["el"][-1, :].copy(), A["el"][0, :].copy()
+    A["eln"], A["els"] = A["el"][:, -1].copy(), A["el"][:, 0].copy()
+    for key, name, axis, index in (("tbe", "t", 0, -1), ("tbw", "t", 0, 0), ("sbe", "s", 0, -1), ("sbw", "s", 0, 0),
+                                   ("tbn", "t", 1, -1), ("tbs", "t", 1, 0), ("sbn", "s", 1, -1), ("sbs", "s", 1, 0)):
+        A[key] = np.ascontiguousarray(A[name][index, :, :] if axis == 0 else A[name][:, index, :]).copy()
+    s = dict(s, rfe=1.0, rfw=1.0, rfn=1.0, rfs=1.0, alpha=0.225, smoth=0.1, profq_form="pom08", zsh=0.01,
+             obc_form="seamount")
+    return A, s
+
+
+def open_seamount(im=65, jm=49, kb=16, dte=5.0, isplit=30, dx=5.0e3, u0=0.1, lat=40.0):
+    """Explicit seamount with open east and west edges, the geometry the
+    seamount case policy serves (registered at 65x49x16 with dtE/dtI = 5/150
+    s): flat 4500 m with a Gaussian seamount (height 4000 m, e-folding 25
+    km) at the centre, dx = dy, walls on the north and south edges, water
+    on the east and west edges, T = 10 + 10 exp(z/1000 m), S = 35, uniform
+    inflow u0, f-plane at ``lat``, no wind; with ``seamount_policy``
+    applied."""
+    core = "explicit"
+    s = state.default_scalars(core)
+    s.update(dte=dte, isplit=isplit, hmax=4500.0)
+    state.derived_time(s)
+    A = _zeros(im, jm, kb)
+    A["dx"][:] = dx
+    A["dy"][:] = dx
+    A["north_e"][:] = lat
+    A["cor"][:] = F32(2.0 * 7.2921e-5 * math.sin(math.radians(lat)))
+    x = (np.arange(im, dtype=np.float64) - (im - 1) / 2.0) * dx
+    y = (np.arange(jm, dtype=np.float64) - (jm - 1) / 2.0) * dx
+    r2 = x[:, None] ** 2 + y[None, :] ** 2
+    h = (4500.0 - 4000.0 * np.exp(-r2 / (25.0e3 ** 2))).astype(F32)
+    h[:, 0] = 1.0
+    h[:, -1] = 1.0
+    A["h"] = h
+    A["z"], A["zz"], A["dz"], A["dzz"] = sigma_levels(kb)
+    areas_masks(A)
+    _with_profile(A, s, lambda z: 10.0 + 10.0 * np.exp(z / 1000.0), 35.0)
+    A["ub"][:, :, : kb - 1] = F32(u0) * A["dum"][:, :, None]
+    A["uab"][:] = F32(u0) * A["dum"]
+    A, s = finish_initialization(A, s, core)
+    return seamount_policy(A, s)

@@ -605,9 +605,10 @@ bool batch_uniform(const npom_params *const *p, int nm) {
         b->mode != a->mode || b->nadv != a->nadv || b->nitera != a->nitera || b->device != a->device)
       return false;
   }
-  // the POM08-WAD PROFQ has no lane body, which the batched column phases use
+  // the POM08-WAD PROFQ has no lane body, which the batched column phases
+  // use, and the seamount boundary's Orlanski passes are not batched
   for (int m = 0; m < nm; ++m)
-    if (p[m]->profq_form != NPOM_PROFQ_PRODUCTION) return false;
+    if (p[m]->profq_form != NPOM_PROFQ_PRODUCTION || p[m]->obc_form != NPOM_OBC_NATIVE) return false;
   return true;
 }
 

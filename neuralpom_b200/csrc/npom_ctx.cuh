@@ -47,6 +47,7 @@ struct Consts {
   double eta_tol, eta_rel_tol;
   int profq_pom08;     // PROFQ in the POM08-WAD form
   float kappa_zsh;     // POM08-WAD: kappa * zsh (folded in double)
+  int obc_seamount;    // the seamount case policy's boundary (explicit core)
 };
 
 struct Ctx {

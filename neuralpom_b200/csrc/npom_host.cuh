@@ -52,6 +52,7 @@ inline Consts make_consts(const npom_params &p) {
   k.surfl = 2.0e5f;
   k.profq_pom08 = p.profq_form == NPOM_PROFQ_POM08 ? 1 : 0;
   k.kappa_zsh = (float)(p.kappa * p.zsh);
+  k.obc_seamount = p.obc_form == NPOM_OBC_SEAMOUNT ? 1 : 0;
   k.wind_kf = (float)(-(p.wind_tau0 / p.rhoref));
   k.two_pi = (float)(2.0 * p.pi);
   k.hmax = (float)p.hmax;
@@ -98,6 +99,9 @@ inline bool check_args(const npom_params *p, float *const *fields, const npom_wo
     if (!fields[f]) return false;
   if (!ws->partials || !ws->sync || !ws->status || !ws->cg_iters) return false;
   if (p->nadv != 1 && (p->nadv != 2 || !ws->mp3d || p->nitera < 1)) return false;
+  if (p->obc_form != NPOM_OBC_NATIVE &&
+      (p->obc_form != NPOM_OBC_SEAMOUNT || p->core != NPOM_CORE_EXPLICIT || p->im < 6))
+    return false;
   for (int w = 0; w < NPOM_NWS; ++w)
     if (!ws->buf[w]) return false;
   return true;

@@ -1068,6 +1068,22 @@ cudaError_t run_subcycle(Ctx c, int blocks, cudaStream_t s) {
 
 void launch_b5(const Ctx &c, cudaStream_t s);
 
+// The seamount policy's Orlanski edges, one thread per (j, k): which 0 the
+// u edges (bcond 3, after B8), 1 the T/S edges (bcond 4, after B6).
+__global__ void __launch_bounds__(kThreads) k_obc_seamount(Ctx c, int which) {
+  const int n = c.jm * c.kb;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  if (which == 0) obc_seamount_u_point(c, q / c.kb, q % c.kb);
+  else obc_seamount_ts_point(c, q / c.kb, q % c.kb);
+}
+
+void launch_obc_seamount(const Ctx &c, int which, cudaStream_t s) {
+  if (!c.k.obc_seamount) return;
+  const int n = c.jm * c.kb;
+  k_obc_seamount<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(c, which);
+}
+
 void internal_mode(const Ctx &c, cudaStream_t s) {
   launch_cols<CP_B1>(c, s);
   launch_cols<CP_B2A>(c, s);
@@ -1076,8 +1092,10 @@ void internal_mode(const Ctx &c, cudaStream_t s) {
   launch_points<PP_B4>(c, s);
   launch_b5(c, s);
   launch_cols<CP_B6>(c, s);
+  launch_obc_seamount(c, 1, s);
   launch_points<PP_B7>(c, s);
   launch_cols<CP_B8>(c, s);
+  launch_obc_seamount(c, 0, s);
 }
 
 // Enqueue one internal step (all its kernels) on s.
@@ -1644,9 +1662,15 @@ npom_status npom_run_phase(const npom_params *p, float *const *fields, const npo
     case 8: launch_cols<CP_B3>(c, s); break;
     case 9: launch_points<PP_B4>(c, s); break;
     case 10: launch_b5(c, s); break;
-    case 11: launch_cols<CP_B6>(c, s); break;
+    case 11:
+      launch_cols<CP_B6>(c, s);
+      launch_obc_seamount(c, 1, s);
+      break;
     case 12: launch_points<PP_B7>(c, s); break;
-    case 13: launch_cols<CP_B8>(c, s); break;
+    case 13:
+      launch_cols<CP_B8>(c, s);
+      launch_obc_seamount(c, 0, s);
+      break;
     case 14: launch_cols<CP_B9>(c, s); break;
   }
   if (e != cudaSuccess) return NPOM_ERR_CUDA;

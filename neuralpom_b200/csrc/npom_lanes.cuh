@@ -363,7 +363,7 @@ __device__ __forceinline__ void lane_b6(const Ctx &c, int i, int j, int k, bool 
   float sf = lane_proft(c, k, F3(vf, i, j, k), khk, kh_next, F2(wssurf, i, j), F2(ssurf, i, j), c.k.nbcs, dh, swrad);
   // explicit bcond 4 (upstream T/S at the edges) replaces levels
   // 0..kbm1-1 of an edge column; each lane evaluates its own level
-  if (is_explicit(c) && k < KL - 1 && (i == 0 || i == c.im - 1 || j == 0 || j == c.jm - 1)) {
+  if (is_explicit(c) && !c.k.obc_seamount && k < KL - 1 && (i == 0 || i == c.im - 1 || j == 0 || j == c.jm - 1)) {
     float ub, vb;
     if (bcond4_explicit_level(c, i, j, k, ub, vb)) {
       tf = ub;
@@ -501,7 +501,7 @@ __device__ __forceinline__ void lane_b8(const Ctx &c, int i, int j, int k, bool 
   float uo, vo, wub, wvb, tpsu, tpsv;
   lane_profuv(c, 0, i, j, k, fu, uo, wub, tpsu);
   lane_profuv(c, 1, i, j, k, fv, vo, wvb, tpsv);
-  if (is_explicit(c)) lane_bcond3_explicit(c, i, j, k, uo, vo);
+  if (is_explicit(c) && !c.k.obc_seamount) lane_bcond3_explicit(c, i, j, k, uo, vo);
   if (!st) return;
   P3(uf, i, j, k) = uo;
   P3(vf, i, j, k) = vo;

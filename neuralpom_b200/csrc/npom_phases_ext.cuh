@@ -293,13 +293,31 @@ NPOM_HD float ext_elf_interior(const Ctx &c, int i, int j) {
 // elf after the explicit bcond 1 (baroclinic.py:510-524): edges copy the
 // adjacent cell (rows first, then columns, so corners take the diagonal
 // interior value), then the whole field is masked by fsm.
+NPOM_HD float ext_elf_cell_seamount(const Ctx &c, int i, int j);
+
 NPOM_HD float ext_elf_cell(const Ctx &c, int i, int j) {
+  if (c.k.obc_seamount) return ext_elf_cell_seamount(c, i, j);
   int si = i, sj = j;
   if (si == 0) si = 1;
   if (si == c.im - 1) si = c.im - 2;
   if (sj == 0) sj = 1;
   if (sj == c.jm - 1) sj = c.jm - 2;
   return ext_elf_interior(c, si, sj) * F2(fsm, i, j);
+}
+
+// elf after the seamount policy's bcond 1 (seamount_boundary.py:9-11,15):
+// only the east and west edges copy the adjacent column, then the mask.
+// The north and south rows keep the value they hold (the interior update
+// does not reach them).  A corner reads that value of its neighbour in the
+// row, which the neighbour's own thread rewrites as value * fsm in this
+// phase; the two agree wherever they matter: a corner outside the sea is 0
+// without the read, and a sea corner's neighbour is sea as well.
+NPOM_HD float ext_elf_cell_seamount(const Ctx &c, int i, int j) {
+  const float fsm = F2(fsm, i, j);
+  const int si = i == 0 ? 1 : (i == c.im - 1 ? c.im - 2 : i);
+  if (si != i && (j == 0 || j == c.jm - 1) && fsm == 0.0f) return 0.0f;
+  const float raw = interior(c, si, j) ? ext_elf_interior(c, si, j) : F2(elf, si, j);
+  return raw * fsm;
 }
 
 // Phase 1 of a substep: elf with bcond 1, and the stored fluxua/fluxva:
@@ -362,7 +380,19 @@ NPOM_HD bool ext_phase2_cell(const Ctx &c, int i, int j, int iext) {
   // normal/tangential components on the ring, then masks.
   const float ramp = c.ramp, g = c.k.grav;
   auto rad = [&](float hh) { return sqrtf(fmaxf_t(g / fmaxf_t(hh, 1e-8f), 1e-8f)); };
-  if (j >= 1 && j <= jm - 2) {
+  if (c.k.obc_seamount) {
+    // the seamount policy (seamount_boundary.py:12-16): characteristic
+    // radiation about the exterior elevation on the west and east edges
+    // only, the west ghost column a copy, no normal flow through them
+    if (j >= 1 && j <= jm - 2) {
+      if (i == 1 || i == 0) uaf = ramp * F1(uabw, j) - sqrtf(g / F2(h, 1, j)) * (F2(el, 1, j) - F1(elw, j));
+      if (i == 0) vaf = 0.0f;
+      if (i == im - 1) {
+        uaf = ramp * F1(uabe, j) + sqrtf(g / F2(h, im - 2, j)) * (F2(el, im - 2, j) - F1(ele, j));
+        vaf = 0.0f;
+      }
+    }
+  } else if (j >= 1 && j <= jm - 2) {
     if (i == im - 1) {
       float te = c.k.rfe * rad(F2(h, im - 2, j)) * (F2(el, im - 2, j) - F1(ele, j));
       uaf = (F1(uabe, j) + te) * ramp;
@@ -374,7 +404,7 @@ NPOM_HD bool ext_phase2_cell(const Ctx &c, int i, int j, int iext) {
     }
     if (i == 0) vaf = 0.0f;
   }
-  if (i >= 1 && i <= im - 2) {
+  if (!c.k.obc_seamount && i >= 1 && i <= im - 2) {
     if (j == jm - 1) {
       float tn = c.k.rfn * rad(F2(h, i, jm - 2)) * (F2(el, i, jm - 2) - F1(eln, i));
       vaf = (F1(vabn, i) + tn) * ramp;

@@ -446,6 +446,15 @@ NPOM_HD void phase_b4_point(const Ctx &c, int i, int j, int k) {
     arr[NPOM_I3(c, i, j, k)] = val;
   }
   if (!is_explicit(c)) return;
+  if (c.k.obc_seamount) {
+    // the seamount policy's bcond 6 (seamount_boundary.py:45-47): 1e-10 on
+    // the east and west edges (B5 then applies uf * fsm + 1e-10)
+    if (i == 0 || i == im - 1) {
+      P3(uf, i, j, k) = 1e-10f;
+      P3(vf, i, j, k) = 1e-10f;
+    }
+    return;
+  }
   // explicit bcond 6 on the edges (east, west, north, south order)
   const float dti = c.k.dti, small = c.k.small;
   float ufv = F3(uf, i, j, k), vfv = F3(vf, i, j, k);
@@ -715,7 +724,8 @@ NPOM_HD void phase_b6_column(const Ctx &c, int i, int j) {
   q.fsurf = F2(ssurf, i, j);
   float dh = proft_column(q);
   P2(tps, i, j) = dh;
-  if (is_explicit(c) && (i == 0 || i == c.im - 1 || j == 0 || j == c.jm - 1)) bcond4_explicit_edge(c, i, j, ufc, vfc);
+  if (is_explicit(c) && !c.k.obc_seamount && (i == 0 || i == c.im - 1 || j == 0 || j == c.jm - 1))
+    bcond4_explicit_edge(c, i, j, ufc, vfc);
 }
 
 // Explicit bcond 4 at level k (< kbm1) of an edge column: upstream T/S on
@@ -1045,7 +1055,7 @@ NPOM_HD void phase_b8_column(const Ctx &c, int i, int j) {
   profuv_column(c, 0, i, j, fin, uo, wub, tpsu);
   for (int k = 0; k < kb; ++k) fin[k] = (inner && k < kb - 1) ? advv_point(c, i, j, k) : 0.0f;
   profuv_column(c, 1, i, j, fin, vo, wvb, tpsv);
-  if (is_explicit(c)) bcond3_explicit_edge(c, i, j, uo, vo);
+  if (is_explicit(c) && !c.k.obc_seamount) bcond3_explicit_edge(c, i, j, uo, vo);
   for (int k = 0; k < kb; ++k) {
     P3(uf, i, j, k) = uo[k];
     P3(vf, i, j, k) = vo[k];
@@ -1100,6 +1110,60 @@ NPOM_HD void phase_b9_column(const Ctx &c, int i, int j) {
   P2(utb, i, j) = F2(utf, i, j);
   P2(vtb, i, j) = F2(vtf, i, j);
   P2(vfluxb, i, j) = F2(vfluxf, i, j);
+}
+
+// ---------------------------------------------------------------------------
+// The seamount case policy's Orlanski edges (seamount_boundary.py:17-37), one
+// thread per (j, k): after B8 for u (bcond 3), after B6 for T and S (bcond
+// 4).  They read the new values of the columns next to the edges, which
+// other threads of those phases compute, so they run as a pass of their
+// own; the masks follow in B9 and B7, after the edges, as in the reference.
+// A zero denominator becomes 0.01, the Orlanski ratio is clamped to [0, 1].
+// ---------------------------------------------------------------------------
+NPOM_HD float orlanski_ratio(float past_near, float out_near, float cur_next) {
+  float den = out_near + past_near - 2.0f * cur_next;
+  if (den == 0.0f) den = 0.01f;
+  return fminf_t(fmaxf_t((past_near - out_near) / den, 0.0f), 1.0f);
+}
+
+// bcond 3: u on the west (column 1, from 2 and 3) and east (im-1, from
+// im-2 and im-3) edges, no v through them, the west ghost column a copy
+NPOM_HD void obc_seamount_u_point(const Ctx &c, int j, int k) {
+  const int im = c.im;
+  if (j < 1 || j > c.jm - 2 || k >= c.kb - 1) return;
+  float *uf = c.F[NPOM_F_uf], *vf = c.F[NPOM_F_vf];
+  for (int side = 0; side < 2; ++side) {
+    const int edge = side == 0 ? 1 : im - 1, near = side == 0 ? 2 : im - 2, nexti = side == 0 ? 3 : im - 3;
+    const float cl = orlanski_ratio(F3(ub, near, j, k), uf[NPOM_I3(c, near, j, k)], F3(u, nexti, j, k));
+    uf[NPOM_I3(c, edge, j, k)] = (F3(ub, edge, j, k) * (1.0f - cl) + 2.0f * cl * F3(u, near, j, k)) / (1.0f + cl);
+    vf[NPOM_I3(c, side == 0 ? 0 : im - 1, j, k)] = 0.0f;
+  }
+  uf[NPOM_I3(c, 0, j, k)] = uf[NPOM_I3(c, 1, j, k)];
+}
+
+// bcond 4: T (uf) and S (vf) on the west (column 0) and east (im-1) edges;
+// where the ratio is 0 and the flow at the edge enters, the exterior
+// profile (tbw/sbw, tbe/sbe) instead
+NPOM_HD void obc_seamount_ts_point(const Ctx &c, int j, int k) {
+  const int im = c.im;
+  if (k >= c.kb - 1) return;
+  const size_t eo = (size_t)j * c.kb + k;
+  for (int side = 0; side < 2; ++side) {
+    const int edge = side == 0 ? 0 : im - 1, near = side == 0 ? 1 : im - 2, nexti = side == 0 ? 2 : im - 3;
+    const float vel = F3(ub, side == 0 ? 1 : im - 1, j, k);
+    const float sign = side == 0 ? 1.0f : -1.0f;
+    for (int tr = 0; tr < 2; ++tr) {
+      float *out = c.F[tr == 0 ? NPOM_F_uf : NPOM_F_vf];
+      const float *past = c.F[tr == 0 ? NPOM_F_tb : NPOM_F_sb];
+      const float *cur = c.F[tr == 0 ? NPOM_F_t : NPOM_F_s];
+      const float *ext = c.F[side == 0 ? (tr == 0 ? NPOM_F_tbw : NPOM_F_sbw) : (tr == 0 ? NPOM_F_tbe : NPOM_F_sbe)];
+      const float cl =
+          orlanski_ratio(ld(past + NPOM_I3(c, near, j, k)), out[NPOM_I3(c, near, j, k)], ld(cur + NPOM_I3(c, nexti, j, k)));
+      const float value =
+          (ld(past + NPOM_I3(c, edge, j, k)) * (1.0f - cl) + 2.0f * cl * ld(cur + NPOM_I3(c, near, j, k))) / (1.0f + cl);
+      out[NPOM_I3(c, edge, j, k)] = (cl == 0.0f && sign * vel >= 0.0f) ? ld(ext + eo) : value;
+    }
+  }
 }
 
 }  // namespace npom

@@ -119,6 +119,12 @@ def make_params(s, im, jm, kb, core, device=0):
         raise ValueError(f"unknown profq form {form!r} (production or pom08)")
     p.profq_form = _abi.PROFQ_POM08 if form == "pom08" else _abi.PROFQ_PRODUCTION
     p.zsh = float(get("zsh", 0.01))
+    obc = str(get("obc_form", "native") or "native").strip().lower()
+    if obc not in ("native", "seamount"):
+        raise ValueError(f"unknown boundary policy {obc!r} (native or seamount)")
+    if obc == "seamount" and implicit:
+        raise ValueError("the seamount boundary policy is built for the explicit core")
+    p.obc_form = _abi.OBC_SEAMOUNT if obc == "seamount" else _abi.OBC_NATIVE
     tuning = get("tuning", None) or {}
     for k, v in dict(tuning).items():
         if k not in _abi.TUNING_FIELDS:

@@ -73,7 +73,7 @@ def extract_state(core):
             arrays[k] = v.detach().cpu().numpy().copy()
     scalars = {}
     # case-policy settings a harness puts on a core (the POM08-WAD closure)
-    for k in SCALAR_NAMES + IMPLICIT_SCALARS + ("profq_form", "zsh"):
+    for k in SCALAR_NAMES + IMPLICIT_SCALARS + ("profq_form", "zsh", "obc_form"):
         if hasattr(core, k):
             val = getattr(core, k)
             if isinstance(val, (bool, int, float, str)):

@@ -213,9 +213,19 @@ void run_phase(const Ctx &c, const npom_params *p, int phase) {
         each_point(c, [&](int i, int j, int k) { phase_b5_point(c, i, j, k); });
       }
       break;
-    case 11: each_cell(c, [&](int i, int j) { phase_b6_column(c, i, j); }); break;
+    case 11:
+      each_cell(c, [&](int i, int j) { phase_b6_column(c, i, j); });
+      if (c.k.obc_seamount)
+        for (int j = 0; j < c.jm; ++j)
+          for (int k = 0; k < c.kb; ++k) obc_seamount_ts_point(c, j, k);
+      break;
     case 12: each_point(c, [&](int i, int j, int k) { phase_b7_point(c, i, j, k); }); break;
-    case 13: each_cell(c, [&](int i, int j) { phase_b8_column(c, i, j); }); break;
+    case 13:
+      each_cell(c, [&](int i, int j) { phase_b8_column(c, i, j); });
+      if (c.k.obc_seamount)
+        for (int j = 0; j < c.jm; ++j)
+          for (int k = 0; k < c.kb; ++k) obc_seamount_u_point(c, j, k);
+      break;
     case 14: each_cell(c, [&](int i, int j) { phase_b9_column(c, i, j); }); break;
   }
 }

@@ -5,6 +5,7 @@ the ``src`` directory of its sources (or the ``baseline/_ref`` install is
 used)::
 
     python tests/golden/make_golden.py [proft] [steps] [adjoint] [coastal] [step_adjoint] [coupling] [mpdata]
+        [pom08] [seamount]
 
 Writes ``tests/golden/*.npz``.  Every file records the reference's own CPU
 float32 outputs on seeded inputs; nothing here is needed at test time except
@@ -390,6 +391,35 @@ def make_mpdata_adjoint_golden(im=12, jm=10, seed=52, steps=(1, 3), ndirs=2, eps
     print("wrote", path, os.path.getsize(path))
 
 
+def make_seamount_golden(im=24, jm=18, seed=71, steps=(1, 3)):
+    """The explicit core under the reference's seamount case policy
+    (cores/case_adapters/seamount_runtime.py:7-25: the seamount boundary of
+    seamount_boundary.py and the POM08-WAD closure), installed by the
+    reference's own installer on an open-east/west seamount
+    (``cases.open_seamount``) with seeded T and u perturbations, clock at
+    0.25 day; 1 and 3 steps."""
+    import torch
+    sys.path.insert(0, ROOT)
+    from neuralpom_b200 import cases
+    from neuralpom.cores.case_adapters import seamount_runtime
+    A, Sc = cases.open_seamount(im, jm)
+    g = np.random.default_rng(seed)
+    fsm3, dum3 = A["fsm"][:, :, None], A["dum"][:, :, None]
+    for f, sd, m in (("t", 0.2, fsm3), ("u", 0.02, dum3), ("v", 0.02, A["dvm"][:, :, None])):
+        p = (sd * g.standard_normal(A[f].shape) * m).astype(np.float32)
+        p[:, :, -1] = 0.0
+        A[f] = A[f] + p
+        A[f[0] + "b"] = A[f[0] + "b"] + p
+    A, Sc = cases.seamount_policy(A, Sc)
+    Sc = dict(Sc, time=0.25, time0=0.25)
+    core = rh.build_reference_core("explicit", im, jm)
+    rh.load_state(core, {k: v for k, v in A.items() if hasattr(core, k)}, Sc)
+    seamount_runtime.install(core, "explicit")
+    torch.set_default_dtype(torch.float32)
+    core.profq_form, core.zsh, core.obc_form = "pom08", 0.01, "seamount"
+    make_step_golden("explicit", im, jm, seed, steps=steps, core=core, tag="seamount_explicit")
+
+
 def make_pom08_goldens():
     """Both cores with the POM08-WAD closure of the reference's case
     policies bound by the reference's own installer
@@ -406,7 +436,7 @@ def make_pom08_goldens():
         make_step_golden(name, im, jm, seed, steps=steps, core=core, tag=tag)
 
 
-def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint", "coupling", "mpdata", "pom08")):
+def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint", "coupling", "mpdata", "pom08", "seamount")):
     src = rh.default_reference_path()
     if src is None:
         raise SystemExit("reference sources not found; set NPOM_REFERENCE_SRC")
@@ -433,8 +463,10 @@ def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint", "couplin
         make_mpdata_adjoint_golden(seed=54, steps=(1, 2), name="implicit_p0_fixed", tag="mpdata_implicit")
     if "pom08" in which:
         make_pom08_goldens()
+    if "seamount" in which:
+        make_seamount_golden()
 
 
 if __name__ == "__main__":
     main(tuple(sys.argv[1:]) or ("proft", "steps", "adjoint", "coastal", "step_adjoint", "coupling", "mpdata",
-                                 "pom08"))
+                                 "pom08", "seamount"))

@@ -70,3 +70,16 @@ def test_profq_form_reaches_npom_params():
     assert p.profq_form == _abi.PROFQ_PRODUCTION and abs(p.zsh - 0.01) < 1e-15
     with pytest.raises(ValueError):
         state.make_params(dict(s, profq_form="pom2k"), 12, 10, 16, "explicit")
+
+
+def test_boundary_policy_reaches_npom_params():
+    """obc_form: native by default, seamount for the explicit core only."""
+    s = dict(state.default_scalars("explicit"), obc_form="seamount")
+    assert state.make_params(s, 24, 18, 16, "explicit").obc_form == _abi.OBC_SEAMOUNT
+    assert state.make_params(dict(state.default_scalars("explicit")), 24, 18, 16, "explicit").obc_form == \
+        _abi.OBC_NATIVE
+    with pytest.raises(ValueError):
+        state.make_params(dict(s, obc_form="orlanski"), 24, 18, 16, "explicit")
+    with pytest.raises(ValueError):
+        state.make_params(dict(state.default_scalars("implicit_p0_fixed"), obc_form="seamount"), 24, 18, 16,
+                          "implicit_p0_fixed")

@@ -17,7 +17,9 @@ def _has_nvcc():
 pytestmark = pytest.mark.skipif(not _has_nvcc(), reason="nvcc needed to build the phase emulator")
 
 STEP_FILES = [("step_explicit_12x10.npz", "explicit"), ("step_implicit_12x10.npz", "implicit_p0_fixed"),
-              ("step_implicit_20x18.npz", "implicit_p0_fixed")]
+              ("step_implicit_20x18.npz", "implicit_p0_fixed"),
+              # the reference's seamount case policy (boundary and POM08-WAD closure)
+              ("step_seamount_explicit_24x18.npz", "explicit")]
 
 
 @pytest.mark.parametrize("fname,core", STEP_FILES)
