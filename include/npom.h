@@ -93,6 +93,9 @@ typedef struct npom_workspace {
   int *cg_iters;           /* >= nsteps ints: PCG iterations of each step  */
   float *mp3d;             /* nadv 2 only (else may be null): >= 12 *     */
                            /* im*jm*kb floats of MPDATA scratch            */
+  float *tide;             /* NPOM_OBC_COASTAL only (else may be null):    */
+                           /* 3 planes of im*jm: 1 at tide cells, their   */
+                           /* amplitude (m) and phase (degrees)           */
 } npom_workspace;
 
 #define NPOM_MAX_COOP_BLOCKS 1024
@@ -143,7 +146,7 @@ typedef struct npom_params {
   double sw;               /* MPDATA antidiffusion weight (nadv 2)         */
   int32_t nitera;          /* MPDATA iterations (nadv 2)                   */
   int32_t profq_form;      /* NPOM_PROFQ_PRODUCTION or NPOM_PROFQ_POM08    */
-  int32_t obc_form;        /* NPOM_OBC_NATIVE or NPOM_OBC_SEAMOUNT          */
+  int32_t obc_form;        /* NPOM_OBC_NATIVE, _SEAMOUNT or _COASTAL       */
   npom_tuning tuning;      /* launch shapes (all zero: the library's rules) */
   double zsh;              /* POM08-WAD profq: roughness added to the mixing length (m) */
 } npom_params;
@@ -163,7 +166,16 @@ enum { NPOM_PROFQ_PRODUCTION = 0, NPOM_PROFQ_POM08 = 1 };
  * of u and of T/S (with the exterior profile on inflow), 1e-10 turbulence
  * edges; the north and south edges are walls.  Forward only (the reference
  * refuses gradients through its case policies). */
-enum { NPOM_OBC_NATIVE = 0, NPOM_OBC_SEAMOUNT = 1 };
+enum { NPOM_OBC_NATIVE = 0, NPOM_OBC_SEAMOUNT = 1, NPOM_OBC_COASTAL = 2 };
+/* COASTAL: the explicit core with the coastal tide policy
+ * (cores/case_adapters/coastal_boundary.py:8-31, coastal_compat.py and the
+ * policy's step copies): the tidal elevation
+ * amp cos(w t - phase) imposed at the cells the workspace's tide planes
+ * flag, at every external substep; characteristic radiation on all four
+ * edges with the total depth d; the bcond 3 blend weight from d; no 1e-8
+ * in the bottom-drag speed; cbc from the new depth after the external
+ * substeps (zsh 0.01 m, z0b 0.005 m, clipped to [0.0025, 1]).  Forward
+ * only. */
 
 enum { NPOM_CORE_EXPLICIT = 0, NPOM_CORE_IMPLICIT = 1 };
 enum { NPOM_PRECOND_JACOBI = 0, NPOM_PRECOND_SPECTRAL = 1 };

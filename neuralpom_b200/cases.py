@@ -372,3 +372,58 @@ def open_seamount(im=65, jm=49, kb=16, dte=5.0, isplit=30, dx=5.0e3, u0=0.1, lat
     A["uab"][:] = F32(u0) * A["dum"]
     A, s = finish_initialization(A, s, core)
     return seamount_policy(A, s)
+
+
+def coastal_policy(A, s, tide_i, tide_j, tide_amp, tide_phase):
+    """The coastal tide policy's set-up on a state (cores/case_adapters/
+    coastal_boundary.py:33-40 and coastal_compat.py:13-23): the tide table
+    (0-based cells, amplitude in m, phase in degrees), rf = 1, alpha and
+    smoth of the explicit core, the POM08-WAD closure (zsh = 0.01 m) and
+    the coastal boundary (``obc_form``)."""
+    A = dict(A)
+    A["tide_i"] = np.asarray(tide_i, F32)
+    A["tide_j"] = np.asarray(tide_j, F32)
+    A["tide_amp"] = np.asarray(tide_amp, F32)
+    A["tide_phase"] = np.asarray(tide_phase, F32)
+    s = dict(s, rfe=1.0, rfw=1.0, rfn=1.0, rfs=1.0, alpha=0.225, smoth=0.1, profq_form="pom08", zsh=0.01,
+             obc_form="coastal")
+    return A, s
+
+
+def tidal_inlet(im=40, jm=30, kb=5, dte=1.0, isplit=10, dx=500.0, lat=30.0, amplitude=1.0):
+    """The geometry the coastal tide policy serves (registered at 161x101x5,
+    dtE/dtI = 1/10 s, from data that is not in the repository): a shelf
+    closed on the west, north and south, depth 2 m at the west wall growing
+    to 60 m at the open east edge, T = 15 degC, S = 31 psu + 1 psu per 10 m,
+    f-plane at ``lat``, no wind; with ``coastal_policy`` applied and the
+    tide table of the registered case's layout: every interior cell of the
+    column next to the east edge, here with amplitude ``amplitude`` scaled
+    by 0.8-1.0 along the column and a phase of 2 degrees per row."""
+    core = "explicit"
+    s = state.default_scalars(core)
+    s.update(dte=dte, isplit=isplit, hmax=60.0)
+    state.derived_time(s)
+    A = _zeros(im, jm, kb)
+    A["dx"][:] = dx
+    A["dy"][:] = dx
+    A["north_e"][:] = lat
+    A["cor"][:] = F32(2.0 * 7.2921e-5 * math.sin(math.radians(lat)))
+    x = np.arange(im, dtype=np.float64) / (im - 1)
+    h = np.broadcast_to((2.0 + 58.0 * x)[:, None], (im, jm)).astype(F32).copy()
+    h[0, :] = 1.0
+    h[:, 0] = 1.0
+    h[:, -1] = 1.0
+    A["h"] = h
+    A["z"], A["zz"], A["dz"], A["dzz"] = sigma_levels(kb)
+    areas_masks(A)
+    depths = (A["z"][None, None, :] * A["h"][:, :, None]).astype(F32)
+    A["tb"][:] = F32(15.0)
+    A["sb"] = (F32(31.0) - F32(0.1) * depths).astype(F32)
+    A["tclim"] = A["tb"].copy()
+    A["sclim"] = A["sb"].copy()
+    A["rho"] = dens_np(A["tb"], A["sb"], A["h"], A["zz"], A["fsm"], s)
+    A["rmean"] = A["rho"].copy()
+    A, s = finish_initialization(A, s, core)
+    rows = np.arange(1, jm - 1)
+    amp = amplitude * (0.8 + 0.2 * rows / max(jm - 2, 1))
+    return coastal_policy(A, s, np.full(rows.shape, im - 2), rows, amp, 2.0 * rows)

@@ -126,6 +126,12 @@ class B200Core:
             s.cg_iters = base + 8 * 4
             ws["struct"] = s
             self._ws = ws
+        if str(getattr(self, "obc_form", "native")).lower() == "coastal" and "tide" not in self._ws:
+            # the coastal tide policy's table as three planes (flag, amplitude, phase)
+            planes = state.tide_planes(im, jm, *(state.host_array(getattr(self, n))
+                                                 for n in ("tide_i", "tide_j", "tide_amp", "tide_phase")))
+            self._ws["tide"] = torch.from_numpy(planes).to(dev).contiguous()
+            self._ws["struct"].tide = self._ws["tide"].data_ptr()
         if int(getattr(self, "nadv", 1)) == 2 and "mp3d" not in self._ws:
             # MPDATA scratch: mass fluxes and fluxes of T and S
             self._ws["mp3d"] = torch.zeros(12 * im * jm * self.kb, dtype=torch.float32, device=dev)

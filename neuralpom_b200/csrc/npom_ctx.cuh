@@ -48,6 +48,10 @@ struct Consts {
   int profq_pom08;     // PROFQ in the POM08-WAD form
   float kappa_zsh;     // POM08-WAD: kappa * zsh (folded in double)
   int obc_seamount;    // the seamount case policy's boundary (explicit core)
+  int obc_coastal;     // the coastal tide policy (explicit core)
+  double tide_w;       // tide angular speed, rad/h, as the policy writes it
+  double dte_d;        // dte in double (tide time of a substep)
+  float zsh_cbc, z0b_cbc, cbcmin, cbcmax;  // coastal policy's drag coefficient
 };
 
 struct Ctx {
@@ -59,6 +63,8 @@ struct Ctx {
   unsigned int *status;
   int *cg_iters;
   float *mp3d;  // MPDATA scratch (nadv 2)
+  const float *tide;  // coastal policy: tide flag, amplitude, phase planes
+  double tide_t0;     // coastal policy: seconds at the start of the step
   Consts k;
   int coh;         // 1: loads bypass L1 (persistent cooperative kernels)
   // the blocks of a cooperative launch that work on this context: blocks

@@ -53,6 +53,15 @@ inline Consts make_consts(const npom_params &p) {
   k.profq_pom08 = p.profq_form == NPOM_PROFQ_POM08 ? 1 : 0;
   k.kappa_zsh = (float)(p.kappa * p.zsh);
   k.obc_seamount = p.obc_form == NPOM_OBC_SEAMOUNT ? 1 : 0;
+  k.obc_coastal = p.obc_form == NPOM_OBC_COASTAL ? 1 : 0;
+  // coastal_boundary.py:8-9: (29.03225806451612*3.1416/180) in double
+  k.tide_w = 29.03225806451612 * 3.1416 / 180.0;
+  k.dte_d = p.dte;
+  // coastal_compat.py:6-16
+  k.zsh_cbc = 0.01f;
+  k.z0b_cbc = 0.005f;
+  k.cbcmin = 0.0025f;
+  k.cbcmax = 1.0f;
   k.wind_kf = (float)(-(p.wind_tau0 / p.rhoref));
   k.two_pi = (float)(2.0 * p.pi);
   k.hmax = (float)p.hmax;
@@ -100,7 +109,8 @@ inline bool check_args(const npom_params *p, float *const *fields, const npom_wo
   if (!ws->partials || !ws->sync || !ws->status || !ws->cg_iters) return false;
   if (p->nadv != 1 && (p->nadv != 2 || !ws->mp3d || p->nitera < 1)) return false;
   if (p->obc_form != NPOM_OBC_NATIVE &&
-      (p->obc_form != NPOM_OBC_SEAMOUNT || p->core != NPOM_CORE_EXPLICIT || p->im < 6))
+      ((p->obc_form != NPOM_OBC_SEAMOUNT && p->obc_form != NPOM_OBC_COASTAL) || p->core != NPOM_CORE_EXPLICIT ||
+       p->im < 6 || p->jm < 6 || (p->obc_form == NPOM_OBC_COASTAL && !ws->tide)))
     return false;
   for (int w = 0; w < NPOM_NWS; ++w)
     if (!ws->buf[w]) return false;
@@ -120,6 +130,7 @@ inline Ctx make_ctx(const npom_params *p, float *const *fields, const npom_works
   c.status = ws->status;
   c.cg_iters = ws->cg_iters;
   c.mp3d = ws->mp3d;
+  c.tide = ws->tide;
   c.k = make_consts(*p);
   c.ramp = 1.0f;
   c.do_internal = 1;

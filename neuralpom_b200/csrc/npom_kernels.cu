@@ -651,7 +651,7 @@ __device__ __forceinline__ void subcycle_coop_body(const Ctx &c) {
   const size_t tid = (size_t)vblock(c) * blockDim.x + threadIdx.x;
   for (int iext = 1; iext <= c.k.isplit; ++iext) {
     bool adv = (iext % c.k.ispadv) == 0;
-    for (size_t q = tid; q < ncell; q += stride) ext_phase1_cell(c, (int)(q / c.jm), (int)(q % c.jm), adv);
+    for (size_t q = tid; q < ncell; q += stride) ext_phase1_cell(c, (int)(q / c.jm), (int)(q % c.jm), adv, iext);
     if (!grid_barrier(c)) return;
     bool exceed = false;
     for (size_t q = tid; q < ncell; q += stride) exceed |= ext_phase2_cell(c, (int)(q / c.jm), (int)(q % c.jm), iext);
@@ -682,7 +682,7 @@ __global__ void __launch_bounds__(T, 1) k_subcycle_cluster(Ctx c) {
   const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   for (int iext = 1; iext <= c.k.isplit; ++iext) {
     bool adv = (iext % c.k.ispadv) == 0;
-    for (size_t q = tid; q < ncell; q += stride) ext_phase1_cell(c, (int)(q / c.jm), (int)(q % c.jm), adv);
+    for (size_t q = tid; q < ncell; q += stride) ext_phase1_cell(c, (int)(q / c.jm), (int)(q % c.jm), adv, iext);
     cl.sync();
     bool exceed = false;
     for (size_t q = tid; q < ncell; q += stride) exceed |= ext_phase2_cell(c, (int)(q / c.jm), (int)(q % c.jm), iext);
@@ -1036,7 +1036,7 @@ cudaError_t plan_subcycle(const Ctx &c, int *out) {
 __device__ __forceinline__ void ext_phase_body(const Ctx &c, int phase, int iext, int adv, int q) {
   if (q >= c.im * c.jm) return;
   const int i = q / c.jm, j = q % c.jm;
-  if (phase == 1) ext_phase1_cell(c, i, j, adv != 0);
+  if (phase == 1) ext_phase1_cell(c, i, j, adv != 0, iext);
   else if (phase == 2) {
     if (ext_phase2_cell(c, i, j, iext)) atomicOr(c.status, NPOM_DEV_VMAX);
   } else ext_phase3_cell(c, i, j, iext);
@@ -1181,6 +1181,11 @@ void launch_b5(const Ctx &c, cudaStream_t s) {
   k_b5_tiles<<<dim3(strips, chunks), kB5Threads, 0, s>>>(c, ichunk);
 }
 
+__global__ void __launch_bounds__(kThreads) k_cbc_coastal(Ctx c) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < c.im * c.jm) cbc_coastal_cell(c, q / c.jm, q % c.jm);
+}
+
 cudaError_t enqueue_step(const Ctx &c, int core, const PcgPlan &plan, int sub_blocks, cudaStream_t s) {
   launch_a1(c, s);
   launch_cols<CP_A2>(c, s);
@@ -1193,6 +1198,10 @@ cudaError_t enqueue_step(const Ctx &c, int core, const PcgPlan &plan, int sub_bl
   } else {
     e = run_subcycle(c, sub_blocks, s);
     if (e != cudaSuccess) return e;
+    if (c.k.obc_coastal) {
+      const int n = c.im * c.jm;
+      k_cbc_coastal<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(c);
+    }
   }
   if (c.do_internal) internal_mode(c, s);
   launch_cols<CP_B9>(c, s);
@@ -1298,8 +1307,11 @@ npom_status run_steps(const npom_params *p, float *const *fields, const npom_wor
     double time = p->dti * iint * 1.0 / 86400.0 + clk->time0;
     c.ramp = ramp_of(p, time);
     c.do_internal = ((iint != 1 || clk->time0 != 0.0) && p->mode != 2) ? 1 : 0;
+    // the coastal policy's tide time of the step's first substep (its
+    // launches change every step: no graph replay)
+    c.tide_t0 = time * 86400.0 - p->dti;
     bool done = false;
-    if (graphs && c.ramp == 1.0f) {
+    if (graphs && c.ramp == 1.0f && !c.k.obc_coastal) {
       if (launch_step_graph(c, core, plan, sub_blocks, s, &done) != cudaSuccess) return NPOM_ERR_CUDA;
     }
     if (!done && enqueue_step(c, core, plan, sub_blocks, s) != cudaSuccess) return NPOM_ERR_CUDA;

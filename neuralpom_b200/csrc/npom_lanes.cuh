@@ -420,20 +420,23 @@ __device__ __forceinline__ void lane_profuv(const Ctx &c, int comp, int i, int j
   if (!interior(c, i, j)) return;
   const int kbt = kbm1 - 1;
   float cbc_avg, mag;
+  // the coastal tide policy's step copy drops the 1e-8 of the bottom speed
+  // (coastal_explicit_momentum.py:327,435)
+  const float eps8 = c.k.obc_coastal ? 0.0f : 1e-8f;
   if (comp == 0) {
     cbc_avg = 0.5f * (F2(cbc, i, j) + F2(cbc, i - 1, j));
     float usq = F3(ub, i, j, kbt);
     usq = usq * usq;
     float vsum = F3(vb, i, j, kbt) + F3(vb, i, j + 1, kbt) + F3(vb, i - 1, j, kbt) + F3(vb, i - 1, j + 1, kbt);
     float va = 0.25f * vsum;
-    mag = sqrtf(usq + va * va + 1e-8f);
+    mag = sqrtf(usq + va * va + eps8);
   } else {
     cbc_avg = 0.5f * (F2(cbc, i, j) + F2(cbc, i, j - 1));
     float vsq = F3(vb, i, j, kbt);
     vsq = vsq * vsq;
     float usum = F3(ub, i, j, kbt) + F3(ub, i + 1, j, kbt) + F3(ub, i, j - 1, kbt) + F3(ub, i + 1, j - 1, kbt);
     float ua = 0.25f * usum;
-    mag = sqrtf(ua * ua + vsq + 1e-8f);
+    mag = sqrtf(ua * ua + vsq + eps8);
   }
   tps = cbc_avg * mag;
   const float mask = comp == 0 ? F2(dum, i, j) : F2(dvm, i, j);
@@ -460,16 +463,17 @@ __device__ __forceinline__ void lane_bcond3_explicit(const Ctx &c, int i, int j,
   if (k >= kbm1) return;
   const float hmax = c.k.hmax;
   auto ga_of = [&](float hh) { return sqrtf(fmaxf_t(hh / hmax, 1e-8f)); };
+  const int gf = c.k.obc_coastal ? NPOM_F_d : NPOM_F_h;  // coastal policy: total depth
   if (j >= 1 && j <= jm - 2) {
     if (i == im - 1) {
-      float ga = ga_of(F2(h, im - 1, j));
+      float ga = ga_of(ld(c.F[gf] + NPOM_I2(c, im - 1, j)));
       float ui = 0.25f * F3(u, im - 2, j - 1, k) + 0.50f * F3(u, im - 2, j, k) + 0.25f * F3(u, im - 2, j + 1, k);
       float uo2 = 0.25f * F3(u, im - 1, j - 1, k) + 0.50f * F3(u, im - 1, j, k) + 0.25f * F3(u, im - 1, j + 1, k);
       uo = ga * ui + (1.0f - ga) * uo2;
       vo = 0.0f;
     }
     if (i == 1 || i == 0) {
-      float ga = ga_of(F2(h, 0, j));
+      float ga = ga_of(ld(c.F[gf] + NPOM_I2(c, 0, j)));
       float ui = 0.25f * F3(u, 2, j - 1, k) + 0.50f * F3(u, 2, j, k) + 0.25f * F3(u, 2, j + 1, k);
       float uo2 = 0.25f * F3(u, 1, j - 1, k) + 0.50f * F3(u, 1, j, k) + 0.25f * F3(u, 1, j + 1, k);
       uo = ga * ui + (1.0f - ga) * uo2;
@@ -478,14 +482,14 @@ __device__ __forceinline__ void lane_bcond3_explicit(const Ctx &c, int i, int j,
   }
   if (i >= 1 && i <= im - 2) {
     if (j == jm - 1) {
-      float ga = ga_of(F2(h, i, jm - 1));
+      float ga = ga_of(ld(c.F[gf] + NPOM_I2(c, i, jm - 1)));
       float vi = 0.25f * F3(v, i - 1, jm - 2, k) + 0.50f * F3(v, i, jm - 2, k) + 0.25f * F3(v, i + 1, jm - 2, k);
       float vo2 = 0.25f * F3(v, i - 1, jm - 1, k) + 0.50f * F3(v, i, jm - 1, k) + 0.25f * F3(v, i + 1, jm - 1, k);
       vo = ga * vi + (1.0f - ga) * vo2;
       uo = 0.0f;
     }
     if (j == 1 || j == 0) {
-      float ga = ga_of(F2(h, i, 0));
+      float ga = ga_of(ld(c.F[gf] + NPOM_I2(c, i, 0)));
       float vi = 0.25f * F3(v, i - 1, 2, k) + 0.50f * F3(v, i, 2, k) + 0.25f * F3(v, i + 1, 2, k);
       float vo2 = 0.25f * F3(v, i - 1, 1, k) + 0.50f * F3(v, i, 1, k) + 0.25f * F3(v, i + 1, 1, k);
       vo = ga * vi + (1.0f - ga) * vo2;

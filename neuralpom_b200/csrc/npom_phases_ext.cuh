@@ -294,9 +294,11 @@ NPOM_HD float ext_elf_interior(const Ctx &c, int i, int j) {
 // adjacent cell (rows first, then columns, so corners take the diagonal
 // interior value), then the whole field is masked by fsm.
 NPOM_HD float ext_elf_cell_seamount(const Ctx &c, int i, int j);
+NPOM_HD float ext_elf_cell_coastal(const Ctx &c, int i, int j, int iext);
 
-NPOM_HD float ext_elf_cell(const Ctx &c, int i, int j) {
+NPOM_HD float ext_elf_cell(const Ctx &c, int i, int j, int iext) {
   if (c.k.obc_seamount) return ext_elf_cell_seamount(c, i, j);
+  if (c.k.obc_coastal) return ext_elf_cell_coastal(c, i, j, iext);
   int si = i, sj = j;
   if (si == 0) si = 1;
   if (si == c.im - 1) si = c.im - 2;
@@ -320,13 +322,31 @@ NPOM_HD float ext_elf_cell_seamount(const Ctx &c, int i, int j) {
   return raw * fsm;
 }
 
+// elf after the coastal tide policy's bcond 1 (coastal_boundary.py:8-21):
+// at the flagged cells the tide amp cos(w t - phase) at the substep's time
+// t = (time * 86400 - dti) + dte * (iext - 1) s, the argument w t / 3600
+// formed in double and rounded once, as the policy's Python floats are; no
+// edge copies; then the mask.
+NPOM_HD float ext_elf_cell_coastal(const Ctx &c, int i, int j, int iext) {
+  const size_t o = NPOM_I2(c, i, j), n2 = (size_t)c.im * c.jm;
+  float raw;
+  if (c.tide[o] != 0.0f) {
+    const double sec = c.tide_t0 + c.k.dte_d * (double)(iext - 1);
+    const float arg = (float)(c.k.tide_w * sec / 3600.0);
+    raw = c.tide[n2 + o] * cosf(arg - c.tide[2 * n2 + o] * 3.1416f / 180.0f);
+  } else {
+    raw = interior(c, i, j) ? ext_elf_interior(c, i, j) : F2(elf, i, j);
+  }
+  return raw * F2(fsm, i, j);
+}
+
 // Phase 1 of a substep: elf with bcond 1, and the stored fluxua/fluxva:
 // the transports (time_loop.py:299-305), or on ADVAVE substeps
 // (iext % ispadv == 0) the ADVAVE outputs that overwrite them.  ADVAVE reads
 // fluxua/fluxva only on row 0 / column 0, which no phase writes, so both
 // fit in one phase.
-NPOM_HD void ext_phase1_cell(const Ctx &c, int i, int j, bool do_advave) {
-  P2(elf, i, j) = ext_elf_cell(c, i, j);
+NPOM_HD void ext_phase1_cell(const Ctx &c, int i, int j, bool do_advave, int iext = 1) {
+  P2(elf, i, j) = ext_elf_cell(c, i, j, iext);
   if (do_advave) {
     AdvaveOut o = advave_cell(c, i, j);
     P2(advua, i, j) = o.advua;
@@ -342,11 +362,11 @@ NPOM_HD void ext_phase1_cell(const Ctx &c, int i, int j, bool do_advave) {
   }
 }
 
-// Phase 2: uaf/vaf with bcond 2 and the etf time filter
-// (time_loop.py:326-391).  Returns |vaf| > vmaxl.
-NPOM_HD bool ext_phase2_cell(const Ctx &c, int i, int j, int iext) {
-  const int im = c.im, jm = c.jm;
-  float uaf = F2(uaf, i, j), vaf = F2(vaf, i, j);
+// uaf/vaf of phase 2 before bcond 2 (time_loop.py:326-383): the momentum
+// update on the interior, the values the fields hold elsewhere
+NPOM_HD void ext_uvaf_raw(const Ctx &c, int i, int j, float &uaf, float &vaf) {
+  uaf = F2(uaf, i, j);
+  vaf = F2(vaf, i, j);
   if (interior(c, i, j)) {
     const float g4 = c.k.quarter_g, al = c.k.alpha, a12 = c.k.one_m_2alpha;
     float d0 = F2(d, i, j);
@@ -376,11 +396,59 @@ NPOM_HD bool ext_phase2_cell(const Ctx &c, int i, int j, int iext) {
                  c.k.four_dte * vp;
     vaf = numv / (denv + 1e-20f);
   }
+}
+
+// The coastal tide policy's bcond 2 (coastal_boundary.py:22-28):
+// characteristic radiation with the total depth d on the east, west, north
+// and south edges in that order, the west and south ghosts copies.  A value
+// that reads a neighbour's new uaf/vaf recomputes that neighbour's interior
+// update (the same expression on the same inputs, so the same bits).
+NPOM_HD void bcond2_coastal(const Ctx &c, int i, int j, float &uaf, float &vaf) {
+  const int im = c.im, jm = c.jm;
+  const float g = c.k.grav;
+  auto rad = [&](int ii, int jj) { return sqrtf(g / F2(d, ii, jj)); };
+  float un, vn;
+  if (j >= 1 && j <= jm - 2) {
+    if (i == im - 1) {
+      ext_uvaf_raw(c, im - 2, j, un, vn);
+      uaf = un + c.k.rfe * rad(im - 2, j) * (F2(el, im - 2, j) - F2(el, im - 1, j));
+      vaf = 0.0f;
+    }
+    if (i == 1 || i == 0) {
+      if (i == 0) ext_uvaf_raw(c, 1, j, un, vn);
+      else un = uaf;
+      uaf = un - c.k.rfw * rad(1, j) * (F2(el, 1, j) - F2(el, 0, j));
+      if (i == 0) vaf = 0.0f;
+    }
+  }
+  if (i >= 1 && i <= im - 2) {
+    if (j == jm - 1) {
+      ext_uvaf_raw(c, i, jm - 2, un, vn);
+      vaf = vn + c.k.rfn * rad(i, jm - 2) * (F2(el, i, jm - 2) - F2(el, i, jm - 1));
+      uaf = 0.0f;
+    }
+    if (j == 1 || j == 0) {
+      if (j == 0) ext_uvaf_raw(c, i, 1, un, vn);
+      else vn = vaf;
+      vaf = vn - c.k.rfs * rad(i, 1) * (F2(el, i, 1) - F2(el, i, 0));
+      if (j == 0) uaf = 0.0f;
+    }
+  }
+}
+
+// Phase 2: uaf/vaf with bcond 2 and the etf time filter
+// (time_loop.py:326-391).  Returns |vaf| > vmaxl.
+NPOM_HD bool ext_phase2_cell(const Ctx &c, int i, int j, int iext) {
+  const int im = c.im, jm = c.jm;
+  float uaf, vaf;
+  ext_uvaf_raw(c, i, j, uaf, vaf);
   // bcond 2 (baroclinic.py:529-571): open-boundary (Flather) values, zero
   // normal/tangential components on the ring, then masks.
   const float ramp = c.ramp, g = c.k.grav;
   auto rad = [&](float hh) { return sqrtf(fmaxf_t(g / fmaxf_t(hh, 1e-8f), 1e-8f)); };
-  if (c.k.obc_seamount) {
+  if (c.k.obc_coastal) {
+    bcond2_coastal(c, i, j, uaf, vaf);
+  } else if (c.k.obc_seamount) {
     // the seamount policy (seamount_boundary.py:12-16): characteristic
     // radiation about the exterior elevation on the west and east edges
     // only, the west ghost column a copy, no normal flow through them
@@ -404,7 +472,7 @@ NPOM_HD bool ext_phase2_cell(const Ctx &c, int i, int j, int iext) {
     }
     if (i == 0) vaf = 0.0f;
   }
-  if (!c.k.obc_seamount && i >= 1 && i <= im - 2) {
+  if (!c.k.obc_seamount && !c.k.obc_coastal && i >= 1 && i <= im - 2) {
     if (j == jm - 1) {
       float tn = c.k.rfn * rad(F2(h, i, jm - 2)) * (F2(el, i, jm - 2) - F1(eln, i));
       vaf = (F1(vabn, i) + tn) * ramp;
@@ -462,6 +530,18 @@ NPOM_HD void ext_phase3_cell(const Ctx &c, int i, int j, int iext) {
       P2(vtf, i, j) = F2(vtf, i, j) + vaf * ds * c.k.isp2i;
     }
   }
+}
+
+// The coastal tide policy's drag coefficient (coastal_compat.py:5-11):
+// (kappa / log((zsh + (1 + zz[kbm1-1]) d) / z0b))^2 on sea cells, cbcmin on
+// land, clipped to [cbcmin, cbcmax].  The policy updates it after every
+// external substep from the new depth; only the last update reaches a
+// reader (the bottom stress of B8), so it runs once after the subcycle.
+NPOM_HD void cbc_coastal_cell(const Ctx &c, int i, int j) {
+  const float ratio = (c.k.zsh_cbc + (1.0f + F1(zz, c.kb - 2)) * F2(d, i, j)) / c.k.z0b_cbc;
+  const float q = c.k.kappa / logf(ratio);
+  const float v = F2(fsm, i, j) > 0.0f ? q * q : c.k.cbcmin;
+  P2(cbc, i, j) = fminf_t(fmaxf_t(v, c.k.cbcmin), c.k.cbcmax);
 }
 
 }  // namespace npom

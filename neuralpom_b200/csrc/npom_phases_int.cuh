@@ -970,20 +970,23 @@ NPOM_HD void profuv_column(const Ctx &c, int comp, int i, int j, const float *fi
   if (!interior(c, i, j)) return;
   const int kbt = kbm1 - 1;
   float cbc_avg, mag;
+  // the coastal tide policy's step copy drops the 1e-8 of the bottom speed
+  // (coastal_explicit_momentum.py:327,435)
+  const float eps8 = c.k.obc_coastal ? 0.0f : 1e-8f;
   if (comp == 0) {
     cbc_avg = 0.5f * (F2(cbc, i, j) + F2(cbc, i - 1, j));
     float usq = F3(ub, i, j, kbt);
     usq = usq * usq;
     float vsum = F3(vb, i, j, kbt) + F3(vb, i, j + 1, kbt) + F3(vb, i - 1, j, kbt) + F3(vb, i - 1, j + 1, kbt);
     float va = 0.25f * vsum;
-    mag = sqrtf(usq + va * va + 1e-8f);
+    mag = sqrtf(usq + va * va + eps8);
   } else {
     cbc_avg = 0.5f * (F2(cbc, i, j) + F2(cbc, i, j - 1));
     float vsq = F3(vb, i, j, kbt);
     vsq = vsq * vsq;
     float usum = F3(ub, i, j, kbt) + F3(ub, i + 1, j, kbt) + F3(ub, i, j - 1, kbt) + F3(ub, i + 1, j - 1, kbt);
     float ua = 0.25f * usum;
-    mag = sqrtf(ua * ua + vsq + 1e-8f);
+    mag = sqrtf(ua * ua + vsq + eps8);
   }
   tps = cbc_avg * mag;
   float fric = tps * dti2 / (-F1(dz, kbt) * dhf);
@@ -1003,9 +1006,12 @@ NPOM_HD void bcond3_explicit_edge(const Ctx &c, int i, int j, float *ufo, float 
   const int im = c.im, jm = c.jm, kbm1 = c.kb - 1;
   const float hmax = c.k.hmax;
   auto ga_of = [&](float hh) { return sqrtf(fmaxf_t(hh / hmax, 1e-8f)); };
+  // the coastal tide policy weighs by the total depth d (its step copy,
+  // coastal_explicit_baroclinic.py:586-641), the native bcond by h
+  const int gf = c.k.obc_coastal ? NPOM_F_d : NPOM_F_h;
   if (j >= 1 && j <= jm - 2) {
     if (i == im - 1) {
-      float ga = ga_of(F2(h, im - 1, j));
+      float ga = ga_of(ld(c.F[gf] + NPOM_I2(c, im - 1, j)));
       for (int k = 0; k < kbm1; ++k) {
         float ui = 0.25f * F3(u, im - 2, j - 1, k) + 0.50f * F3(u, im - 2, j, k) + 0.25f * F3(u, im - 2, j + 1, k);
         float uo = 0.25f * F3(u, im - 1, j - 1, k) + 0.50f * F3(u, im - 1, j, k) + 0.25f * F3(u, im - 1, j + 1, k);
@@ -1014,7 +1020,7 @@ NPOM_HD void bcond3_explicit_edge(const Ctx &c, int i, int j, float *ufo, float 
       }
     }
     if (i == 1 || i == 0) {
-      float ga = ga_of(F2(h, 0, j));
+      float ga = ga_of(ld(c.F[gf] + NPOM_I2(c, 0, j)));
       for (int k = 0; k < kbm1; ++k) {
         float ui = 0.25f * F3(u, 2, j - 1, k) + 0.50f * F3(u, 2, j, k) + 0.25f * F3(u, 2, j + 1, k);
         float uo = 0.25f * F3(u, 1, j - 1, k) + 0.50f * F3(u, 1, j, k) + 0.25f * F3(u, 1, j + 1, k);
@@ -1025,7 +1031,7 @@ NPOM_HD void bcond3_explicit_edge(const Ctx &c, int i, int j, float *ufo, float 
   }
   if (i >= 1 && i <= im - 2) {
     if (j == jm - 1) {
-      float ga = ga_of(F2(h, i, jm - 1));
+      float ga = ga_of(ld(c.F[gf] + NPOM_I2(c, i, jm - 1)));
       for (int k = 0; k < kbm1; ++k) {
         float vi = 0.25f * F3(v, i - 1, jm - 2, k) + 0.50f * F3(v, i, jm - 2, k) + 0.25f * F3(v, i + 1, jm - 2, k);
         float vo = 0.25f * F3(v, i - 1, jm - 1, k) + 0.50f * F3(v, i, jm - 1, k) + 0.25f * F3(v, i + 1, jm - 1, k);
@@ -1034,7 +1040,7 @@ NPOM_HD void bcond3_explicit_edge(const Ctx &c, int i, int j, float *ufo, float 
       }
     }
     if (j == 1 || j == 0) {
-      float ga = ga_of(F2(h, i, 0));
+      float ga = ga_of(ld(c.F[gf] + NPOM_I2(c, i, 0)));
       for (int k = 0; k < kbm1; ++k) {
         float vi = 0.25f * F3(v, i - 1, 2, k) + 0.50f * F3(v, i, 2, k) + 0.25f * F3(v, i + 1, 2, k);
         float vo = 0.25f * F3(v, i - 1, 1, k) + 0.50f * F3(v, i, 1, k) + 0.25f * F3(v, i + 1, 1, k);

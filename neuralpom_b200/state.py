@@ -53,6 +53,13 @@ def default_scalars(core):
     return derived_time(s)
 
 
+def host_array(v):
+    """numpy copy of an array or a tensor (on any device)."""
+    if hasattr(v, "detach"):
+        return v.detach().cpu().numpy()
+    return np.asarray(v)
+
+
 def host_scalar(v):
     """float of a Python number or a one-element tensor.  A device tensor
     (the reference keeps ``period`` as one) is read back once and the value
@@ -120,11 +127,11 @@ def make_params(s, im, jm, kb, core, device=0):
     p.profq_form = _abi.PROFQ_POM08 if form == "pom08" else _abi.PROFQ_PRODUCTION
     p.zsh = float(get("zsh", 0.01))
     obc = str(get("obc_form", "native") or "native").strip().lower()
-    if obc not in ("native", "seamount"):
-        raise ValueError(f"unknown boundary policy {obc!r} (native or seamount)")
-    if obc == "seamount" and implicit:
-        raise ValueError("the seamount boundary policy is built for the explicit core")
-    p.obc_form = _abi.OBC_SEAMOUNT if obc == "seamount" else _abi.OBC_NATIVE
+    if obc not in ("native", "seamount", "coastal"):
+        raise ValueError(f"unknown boundary policy {obc!r} (native, seamount or coastal)")
+    if obc != "native" and implicit:
+        raise ValueError(f"the {obc} boundary policy is built for the explicit core")
+    p.obc_form = {"native": _abi.OBC_NATIVE, "seamount": _abi.OBC_SEAMOUNT, "coastal": _abi.OBC_COASTAL}[obc]
     tuning = get("tuning", None) or {}
     for k, v in dict(tuning).items():
         if k not in _abi.TUNING_FIELDS:
@@ -157,3 +164,18 @@ def spectral_setup(dx, dy, h, dti, grav, alpha, dtype=np.float32):
         return (2.0 * np.sin(np.pi * np.outer(k, k) / (n + 1))).astype(dtype)
 
     return sine(ni), sine(nj), np.ascontiguousarray(inv_eigs)
+
+
+def tide_planes(im, jm, tide_i, tide_j, amp, phase):
+    """The coastal tide policy's table (0-based cell indices, amplitudes in
+    m, phases in degrees; coastal_boundary.py:33-40 reads them 1-based from
+    its data file) as the three im x jm planes of ``npom_workspace.tide``:
+    1 at the tide cells, their amplitude, their phase.  A repeated cell
+    keeps its last entry, as the policy's indexed assignment does."""
+    out = np.zeros((3, im, jm), np.float32)
+    for i, j, a, p in zip(np.asarray(tide_i).astype(np.int64).ravel(), np.asarray(tide_j).astype(np.int64).ravel(),
+                          np.asarray(amp, np.float32).ravel(), np.asarray(phase, np.float32).ravel()):
+        out[0, i, j] = 1.0
+        out[1, i, j] = a
+        out[2, i, j] = p
+    return out

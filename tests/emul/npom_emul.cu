@@ -164,7 +164,7 @@ void pcg(const Ctx &c, int step, int with_rhs, int with_post) {
 void subcycle(const Ctx &c) {
   for (int iext = 1; iext <= c.k.isplit; ++iext) {
     bool adv = (iext % c.k.ispadv) == 0;
-    each_cell(c, [&](int i, int j) { ext_phase1_cell(c, i, j, adv); });
+    each_cell(c, [&](int i, int j) { ext_phase1_cell(c, i, j, adv, iext); });
     each_cell(c, [&](int i, int j) {
       if (ext_phase2_cell(c, i, j, iext)) *c.status |= NPOM_DEV_VMAX;
     });
@@ -439,6 +439,7 @@ int emul_steps(const npom_params *p, float *const *fields, const npom_workspace 
     double time = p->dti * iint * 1.0 / 86400.0 + clk->time0;
     c.ramp = ramp_of(p, time);
     c.do_internal = ((iint != 1 || clk->time0 != 0.0) && p->mode != 2) ? 1 : 0;
+    c.tide_t0 = time * 86400.0 - p->dti;
     run_phase(c, p, 0);
     run_phase(c, p, 1);
     run_phase(c, p, 2);
@@ -447,6 +448,7 @@ int emul_steps(const npom_params *p, float *const *fields, const npom_workspace 
       run_phase(c, p, 4);
     } else {
       subcycle(c);
+      if (c.k.obc_coastal) each_cell(c, [&](int i, int j) { cbc_coastal_cell(c, i, j); });
     }
     if (c.do_internal)
       for (int ph = 5; ph <= 13; ++ph) run_phase(c, p, ph);

@@ -420,6 +420,56 @@ def make_seamount_golden(im=24, jm=18, seed=71, steps=(1, 3)):
     make_step_golden("explicit", im, jm, seed, steps=steps, core=core, tag="seamount_explicit")
 
 
+def make_coastal_policy_golden(im=24, jm=18, steps=(1, 3)):
+    """The explicit core under the reference's coastal tide policy, set up
+    the way its registry does (cores/case_adapters/registry.py:146-156: the
+    policy's step copies bound as methods, coastal_boundary.install with a
+    tide table file, coastal_compat.install with the POM08-WAD closure) on
+    ``cases.tidal_inlet`` (kb = 16), clock at 0.25 day; one internal step
+    per call with the tide substep counter reset, as the registry's
+    advancement does (registry.py:44-63); 1 and 3 steps."""
+    import tempfile
+    import torch
+    from importlib import import_module
+    sys.path.insert(0, ROOT)
+    from neuralpom_b200 import cases
+    from neuralpom.cores.case_adapters import coastal_boundary, coastal_compat, registry
+    A, Sc = cases.tidal_inlet(im, jm, kb=16)
+    Sc = dict(Sc, time=0.25, time0=0.25)
+    core = rh.build_reference_core("explicit", im, jm)
+    rh.load_state(core, {k: v for k, v in A.items() if hasattr(core, k)}, Sc)
+    core.alpha, core.smoth = 0.225, 0.1
+    for module, cls in (("momentum", "MomentumMixin"), ("tracers", "TracersMixin"), ("time_loop", "TimeLoopMixin")):
+        registry._bind_mixin(core, getattr(import_module(f"neuralpom.cores.case_adapters.kernels.coastal_explicit_{module}"),
+                                           cls))
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "tide.dat")
+        np.savetxt(path, np.c_[A["tide_i"] + 1, A["tide_j"] + 1, A["tide_amp"], A["tide_phase"]])
+        coastal_boundary.install(core, "explicit", path)
+    coastal_compat.install(core)
+    torch.set_default_dtype(torch.float32)
+    core.profq_form, core.zsh, core.obc_form = "pom08", 0.01, "coastal"
+
+    arrays, scalars = rh.extract_state(core)
+    out = {f"in__{k}": v for k, v in arrays.items()}
+    for k, v in scalars.items():
+        out[f"scalar__{k}"] = np.asarray(v)
+    done = 0
+    for n in steps:
+        while done < n:
+            core._tide_substep = 0
+            rh.advance(core, "explicit", 1)
+            done += 1
+        a, _ = rh.extract_state(core)
+        for f in OUTPUT_FIELDS:
+            out[f"out{n}__{f}"] = a[f]
+        out[f"out{n}__cbc"] = a["cbc"]
+        out[f"out{n}__scalar_time"] = np.asarray(float(core.time))
+    path = os.path.join(HERE, f"step_coastal_policy_{im}x{jm}.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path))
+
+
 def make_pom08_goldens():
     """Both cores with the POM08-WAD closure of the reference's case
     policies bound by the reference's own installer
@@ -465,6 +515,7 @@ def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint", "couplin
         make_pom08_goldens()
     if "seamount" in which:
         make_seamount_golden()
+        make_coastal_policy_golden()
 
 
 if __name__ == "__main__":

@@ -15,7 +15,9 @@ STEP_FILES = [("step_explicit_12x10.npz", "explicit"), ("step_implicit_12x10.npz
               # the POM08-WAD closure of the reference's case policies
               ("step_pom08_explicit_12x10.npz", "explicit"), ("step_pom08_implicit_20x18.npz", "implicit_p0_fixed"),
               # the seamount case policy (its boundary with the POM08-WAD closure)
-              ("step_seamount_explicit_24x18.npz", "explicit")]
+              ("step_seamount_explicit_24x18.npz", "explicit"),
+              # the coastal tide policy (tide cells, four-edge radiation, step copies, closure)
+              ("step_coastal_policy_24x18.npz", "explicit")]
 
 
 def _core(arrays, scalars, core):
