@@ -161,14 +161,14 @@ enum { NPOM_PROFQ_PRODUCTION = 0, NPOM_PROFQ_POM08 = 1 };
 /* Boundary policy (obc_form).  NATIVE: the core's own bcond (closed walls,
  * or the explicit core's Flather/upstream open boundary).  SEAMOUNT: the
  * explicit core with the seamount case policy's boundary
- * (cores/case_adapters/seamount_boundary.py:9-47): η ghost copies and
+ * (cores/case_adapters/seamount_boundary.py:9-43): η ghost copies and
  * characteristic radiation on the east and west edges, Orlanski radiation
  * of u and of T/S (with the exterior profile on inflow), 1e-10 turbulence
  * edges; the north and south edges are walls.  Forward only (the reference
  * refuses gradients through its case policies). */
 enum { NPOM_OBC_NATIVE = 0, NPOM_OBC_SEAMOUNT = 1, NPOM_OBC_COASTAL = 2 };
 /* COASTAL: the explicit core with the coastal tide policy
- * (cores/case_adapters/coastal_boundary.py:8-31, coastal_compat.py and the
+ * (cores/case_adapters/coastal_boundary.py:9-30, coastal_compat.py and the
  * policy's step copies): the tidal elevation
  * amp cos(w t - phase) imposed at the cells the workspace's tide planes
  * flag, at every external substep; characteristic radiation on all four

@@ -324,7 +324,7 @@ def coastal_tide(im=354, jm=322, kb=16, dte=2.0, isplit=30, dx=500.0, seed=4, la
 
 def seamount_policy(A, s):
     """The seamount case policy's set-up on a state (cores/case_adapters/
-    seamount_runtime.py:7-25): the exterior elevations, transports and T/S
+    seamount_runtime.py:6-25): the exterior elevations, transports and T/S
     profiles taken from the current state's edge rows and columns, rf = 1,
     alpha and smoth of the explicit core, the POM08-WAD closure (zsh =
     0.01 m) and the seamount boundary (``obc_form``)."""
@@ -376,7 +376,7 @@ def open_seamount(im=65, jm=49, kb=16, dte=5.0, isplit=30, dx=5.0e3, u0=0.1, lat
 
 def coastal_policy(A, s, tide_i, tide_j, tide_amp, tide_phase):
     """The coastal tide policy's set-up on a state (cores/case_adapters/
-    coastal_boundary.py:33-40 and coastal_compat.py:13-23): the tide table
+    coastal_boundary.py:55-65 and coastal_compat.py:12-23): the tide table
     (0-based cells, amplitude in m, phase in degrees), rf = 1, alpha and
     smoth of the explicit core, the POM08-WAD closure (zsh = 0.01 m) and
     the coastal boundary (``obc_form``)."""

@@ -54,10 +54,10 @@ inline Consts make_consts(const npom_params &p) {
   k.kappa_zsh = (float)(p.kappa * p.zsh);
   k.obc_seamount = p.obc_form == NPOM_OBC_SEAMOUNT ? 1 : 0;
   k.obc_coastal = p.obc_form == NPOM_OBC_COASTAL ? 1 : 0;
-  // coastal_boundary.py:8-9: (29.03225806451612*3.1416/180) in double
+  // coastal_boundary.py:9-10: (29.03225806451612*3.1416/180) in double
   k.tide_w = 29.03225806451612 * 3.1416 / 180.0;
   k.dte_d = p.dte;
-  // coastal_compat.py:6-16
+  // coastal_compat.py:4-16
   k.zsh_cbc = 0.01f;
   k.z0b_cbc = 0.005f;
   k.cbcmin = 0.0025f;

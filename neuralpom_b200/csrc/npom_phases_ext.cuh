@@ -307,7 +307,7 @@ NPOM_HD float ext_elf_cell(const Ctx &c, int i, int j, int iext) {
   return ext_elf_interior(c, si, sj) * F2(fsm, i, j);
 }
 
-// elf after the seamount policy's bcond 1 (seamount_boundary.py:9-11,15):
+// elf after the seamount policy's bcond 1 (seamount_boundary.py:9-12,15):
 // only the east and west edges copy the adjacent column, then the mask.
 // The north and south rows keep the value they hold (the interior update
 // does not reach them).  A corner reads that value of its neighbour in the
@@ -322,7 +322,7 @@ NPOM_HD float ext_elf_cell_seamount(const Ctx &c, int i, int j) {
   return raw * fsm;
 }
 
-// elf after the coastal tide policy's bcond 1 (coastal_boundary.py:8-21):
+// elf after the coastal tide policy's bcond 1 (coastal_boundary.py:9-22):
 // at the flagged cells the tide amp cos(w t - phase) at the substep's time
 // t = (time * 86400 - dti) + dte * (iext - 1) s, the argument w t / 3600
 // formed in double and rounded once, as the policy's Python floats are; no
@@ -398,7 +398,7 @@ NPOM_HD void ext_uvaf_raw(const Ctx &c, int i, int j, float &uaf, float &vaf) {
   }
 }
 
-// The coastal tide policy's bcond 2 (coastal_boundary.py:22-28):
+// The coastal tide policy's bcond 2 (coastal_boundary.py:23-29):
 // characteristic radiation with the total depth d on the east, west, north
 // and south edges in that order, the west and south ghosts copies.  A value
 // that reads a neighbour's new uaf/vaf recomputes that neighbour's interior
@@ -449,7 +449,7 @@ NPOM_HD bool ext_phase2_cell(const Ctx &c, int i, int j, int iext) {
   if (c.k.obc_coastal) {
     bcond2_coastal(c, i, j, uaf, vaf);
   } else if (c.k.obc_seamount) {
-    // the seamount policy (seamount_boundary.py:12-16): characteristic
+    // the seamount policy (seamount_boundary.py:16-19): characteristic
     // radiation about the exterior elevation on the west and east edges
     // only, the west ghost column a copy, no normal flow through them
     if (j >= 1 && j <= jm - 2) {
@@ -532,7 +532,7 @@ NPOM_HD void ext_phase3_cell(const Ctx &c, int i, int j, int iext) {
   }
 }
 
-// The coastal tide policy's drag coefficient (coastal_compat.py:5-11):
+// The coastal tide policy's drag coefficient (coastal_compat.py:4-11):
 // (kappa / log((zsh + (1 + zz[kbm1-1]) d) / z0b))^2 on sea cells, cbcmin on
 // land, clipped to [cbcmin, cbcmax].  The policy updates it after every
 // external substep from the new depth; only the last update reaches a

@@ -447,7 +447,7 @@ NPOM_HD void phase_b4_point(const Ctx &c, int i, int j, int k) {
   }
   if (!is_explicit(c)) return;
   if (c.k.obc_seamount) {
-    // the seamount policy's bcond 6 (seamount_boundary.py:45-47): 1e-10 on
+    // the seamount policy's bcond 6 (seamount_boundary.py:40-42): 1e-10 on
     // the east and west edges (B5 then applies uf * fsm + 1e-10)
     if (i == 0 || i == im - 1) {
       P3(uf, i, j, k) = 1e-10f;
@@ -1119,7 +1119,7 @@ NPOM_HD void phase_b9_column(const Ctx &c, int i, int j) {
 }
 
 // ---------------------------------------------------------------------------
-// The seamount case policy's Orlanski edges (seamount_boundary.py:17-37), one
+// The seamount case policy's Orlanski edges (seamount_boundary.py:20-38), one
 // thread per (j, k): after B8 for u (bcond 3), after B6 for T and S (bcond
 // 4).  They read the new values of the columns next to the edges, which
 // other threads of those phases compute, so they run as a pass of their

@@ -168,7 +168,7 @@ def spectral_setup(dx, dy, h, dti, grav, alpha, dtype=np.float32):
 
 def tide_planes(im, jm, tide_i, tide_j, amp, phase):
     """The coastal tide policy's table (0-based cell indices, amplitudes in
-    m, phases in degrees; coastal_boundary.py:33-40 reads them 1-based from
+    m, phases in degrees; coastal_boundary.py:55-65 reads them 1-based from
     its data file) as the three im x jm planes of ``npom_workspace.tide``:
     1 at the tide cells, their amplitude, their phase.  A repeated cell
     keeps its last entry, as the policy's indexed assignment does."""

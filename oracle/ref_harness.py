@@ -71,7 +71,7 @@ def extract_state(core):
     for k, v in vars(core).items():
         if torch.is_tensor(v) and v.is_floating_point() and not k.startswith("_"):
             arrays[k] = v.detach().cpu().numpy().copy()
-    # the coastal tide policy's table (coastal_boundary.py:33-40), 0-based
+    # the coastal tide policy's table (coastal_boundary.py:55-65), 0-based
     for k in ("_tide_i", "_tide_j", "_tide_amp", "_tide_phase"):
         if torch.is_tensor(getattr(core, k, None)):
             arrays[k[1:]] = getattr(core, k).detach().cpu().numpy().astype(np.float32)

@@ -393,7 +393,7 @@ def make_mpdata_adjoint_golden(im=12, jm=10, seed=52, steps=(1, 3), ndirs=2, eps
 
 def make_seamount_golden(im=24, jm=18, seed=71, steps=(1, 3)):
     """The explicit core under the reference's seamount case policy
-    (cores/case_adapters/seamount_runtime.py:7-25: the seamount boundary of
+    (cores/case_adapters/seamount_runtime.py:6-25: the seamount boundary of
     seamount_boundary.py and the POM08-WAD closure), installed by the
     reference's own installer on an open-east/west seamount
     (``cases.open_seamount``) with seeded T and u perturbations, clock at
@@ -422,12 +422,12 @@ def make_seamount_golden(im=24, jm=18, seed=71, steps=(1, 3)):
 
 def make_coastal_policy_golden(im=24, jm=18, steps=(1, 3)):
     """The explicit core under the reference's coastal tide policy, set up
-    the way its registry does (cores/case_adapters/registry.py:146-156: the
+    the way its registry does (cores/case_adapters/registry.py:136-146: the
     policy's step copies bound as methods, coastal_boundary.install with a
     tide table file, coastal_compat.install with the POM08-WAD closure) on
     ``cases.tidal_inlet`` (kb = 16), clock at 0.25 day; one internal step
     per call with the tide substep counter reset, as the registry's
-    advancement does (registry.py:44-63); 1 and 3 steps."""
+    advancement does (registry.py:38-63); 1 and 3 steps."""
     import tempfile
     import torch
     from importlib import import_module
