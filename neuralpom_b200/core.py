@@ -232,6 +232,13 @@ class B200Core:
             raise ValueError("iend must be non-negative")
         deferred = getattr(self, "status_deferred", False)
         if self._differentiable_call():
+            policy = (str(getattr(self, "profq_form", "production")).lower() != "production" or
+                      str(getattr(self, "obc_form", "native")).lower() != "native")
+            if policy:
+                # as the reference's case-policy registry does
+                # (cores/case_adapters/registry.py:38-41)
+                raise RuntimeError("Registered case policies require advancement inside torch.no_grad(); "
+                                   "their training adjoints are unvalidated.")
             outs = _StepsFunction.apply(self, nsteps, float(self.time0),
                                         *[getattr(self, f) for f in _abi.ADJ_STATE_FIELDS])
             for f, o in zip(_abi.ADJ_STATE_FIELDS, outs):

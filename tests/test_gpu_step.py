@@ -263,3 +263,16 @@ def test_gpu_restart_continues_bitwise(tmp_path):
     second = advance()
     for n in first:
         assert torch.equal(first[n], second[n]), n
+
+
+@pytest.mark.parametrize("fname", ["step_pom08_explicit_12x10.npz", "step_seamount_explicit_24x18.npz",
+                                   "step_coastal_policy_24x18.npz"])
+def test_gpu_case_policies_refuse_gradients(fname):
+    """The case policies advance forward only, as the reference's registry
+    requires (cores/case_adapters/registry.py:38-41)."""
+    A, Sc, OUT = load_step_golden(fname)
+    c = _core(A, Sc, "explicit")
+    c.t = c.t.detach().clone().requires_grad_(True)
+    c.time0, c.iend = float(Sc["time"]), 1
+    with pytest.raises(RuntimeError, match="no_grad"):
+        c.run_time_loop()
