@@ -2291,7 +2291,10 @@ NPOM_HD void profuv_column_adj(const Ctx &c, const Adj &a, int comp, int i, int 
 
 // explicit bcond 3: levels overwritten by the edge formulas take their
 // cotangent out of luo/lvo
-NPOM_HD void bcond3_explicit_edge_adj(const Ctx &c, const Adj &a, int i, int j, float *luo, float *lvo) {
+// comps: 1 the u edges, 2 the v edges, 3 both (their cotangents and
+// scatters are independent)
+NPOM_HD void bcond3_explicit_edge_adj(const Ctx &c, const Adj &a, int i, int j, float *luo, float *lvo,
+                                      int comps = 3) {
   const int im = c.im, jm = c.jm, kbm1 = c.kb - 1;
   enum { KEEP = 0, EAST, WEST, NORTH, SOUTH, ZERO };
   int su = KEEP, sv = KEEP;
@@ -2303,11 +2306,13 @@ NPOM_HD void bcond3_explicit_edge_adj(const Ctx &c, const Adj &a, int i, int j, 
     if (j == jm - 1) { sv = NORTH; su = ZERO; }
     if (j == 1 || j == 0) { sv = SOUTH; if (j == 0) su = ZERO; }
   }
+  if (!(comps & 1)) su = KEEP;
+  if (!(comps & 2)) sv = KEEP;
   if (su == KEEP && sv == KEEP) return;
   const float hmax = c.k.hmax;
   auto ga_of = [&](float hh) { return sqrtf(fmaxf_t(hh / hmax, 1e-8f)); };
   for (int k = 0; k < kbm1; ++k) {
-    const float lu = luo[k], lv = lvo[k];
+    const float lu = (comps & 1) ? luo[k] : 0.0f, lv = (comps & 2) ? lvo[k] : 0.0f;
     if (su == EAST || su == WEST) {
       const float ga = su == EAST ? ga_of(F2(h, im - 1, j)) : ga_of(F2(h, 0, j));
       const int ii = su == EAST ? im - 2 : 2, io = su == EAST ? im - 1 : 1;
@@ -2335,22 +2340,31 @@ NPOM_HD void bcond3_explicit_edge_adj(const Ctx &c, const Adj &a, int i, int j, 
   }
 }
 
+// one component of B8 (comp 0: ADVU, PROFU and the u edges of bcond 3;
+// 1: the v side, which also carries the cotangent of tps): the two share
+// no intermediate, so the device runs them on two threads
 template <int KM>
-NPOM_HD void phase_b8_column_adj(const Ctx &c, const Adj &a, int i, int j) {
+NPOM_HD void phase_b8_comp_adj(const Ctx &c, const Adj &a, int comp, int i, int j) {
   const int kb = c.kb;
   const bool inner = interior(c, i, j);
-  float luo[KM], lvo[KM], lfin[KM];
-  for (int k = 0; k < kb; ++k) {
-    luo[k] = LA3(uf, i, j, k);
-    lvo[k] = LA3(vf, i, j, k);
+  float lo[KM], lfin[KM];
+  for (int k = 0; k < kb; ++k) lo[k] = comp == 0 ? LA3(uf, i, j, k) : LA3(vf, i, j, k);
+  if (is_explicit(c)) bcond3_explicit_edge_adj(c, a, i, j, lo, lo, comp == 0 ? 1 : 2);
+  if (comp == 0) {
+    profuv_column_adj<KM>(c, a, 0, i, j, lo, LA2(wubot, i, j), 0.0f, lfin);
+    if (inner)
+      for (int k = 0; k < kb - 1; ++k) advu_point_adj(c, a, i, j, k, lfin[k]);
+  } else {
+    profuv_column_adj<KM>(c, a, 1, i, j, lo, LA2(wvbot, i, j), LA2(tps, i, j), lfin);
+    if (inner)
+      for (int k = 0; k < kb - 1; ++k) advv_point_adj(c, a, i, j, k, lfin[k]);
   }
-  if (is_explicit(c)) bcond3_explicit_edge_adj(c, a, i, j, luo, lvo);
-  profuv_column_adj<KM>(c, a, 0, i, j, luo, LA2(wubot, i, j), 0.0f, lfin);
-  if (inner)
-    for (int k = 0; k < kb - 1; ++k) advu_point_adj(c, a, i, j, k, lfin[k]);
-  profuv_column_adj<KM>(c, a, 1, i, j, lvo, LA2(wvbot, i, j), LA2(tps, i, j), lfin);
-  if (inner)
-    for (int k = 0; k < kb - 1; ++k) advv_point_adj(c, a, i, j, k, lfin[k]);
+}
+
+template <int KM>
+NPOM_HD void phase_b8_column_adj(const Ctx &c, const Adj &a, int i, int j) {
+  phase_b8_comp_adj<KM>(c, a, 0, i, j);
+  phase_b8_comp_adj<KM>(c, a, 1, i, j);
 }
 
 // ===========================================================================

@@ -65,6 +65,16 @@ __global__ void __launch_bounds__(128) k_adj_cols_t(Ctx c, Adj a) {
   adj_column<PH, KM>(c, a, i, j);
 }
 
+// B8's adjoint on two threads per column, u and v (adjacent lanes)
+template <int KM>
+__global__ void __launch_bounds__(128) k_adj_b8_split(Ctx c, Adj a) {
+  const int n = 2 * c.im * c.jm;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int col = q >> 1;
+  phase_b8_comp_adj<KM>(c, a, q & 1, col / c.jm, col % c.jm);
+}
+
 template <int PH>
 void launch_adj_cols(const Ctx &c, const Adj &a, cudaStream_t s) {
   const unsigned g = (unsigned)((c.im * c.jm + 127) / 128);
@@ -382,7 +392,12 @@ npom_status launch_adj_phase(const npom_params *p, const npom_workspace *ws, con
     case AP_B5: k_adj_points<AP_B5><<<gp, kThreads, 0, s>>>(c, a); break;
     case AP_B6: launch_adj_cols<AP_B6>(c, a, s); break;
     case AP_B7: k_adj_points<AP_B7><<<gp, kThreads, 0, s>>>(c, a); break;
-    case AP_B8: launch_adj_cols<AP_B8>(c, a, s); break;
+    case AP_B8: {
+      const unsigned g = (unsigned)((2 * c.im * c.jm + 127) / 128);
+      if (c.kb == 16) k_adj_b8_split<16><<<g, 128, 0, s>>>(c, a);
+      else k_adj_b8_split<KMAX><<<g, 128, 0, s>>>(c, a);
+      break;
+    }
     case AP_B9: launch_adj_cols<AP_B9>(c, a, s); break;
     case AP_MQ:
     case AP_MINIT:
