@@ -5,7 +5,7 @@ the ``src`` directory of its sources (or the ``baseline/_ref`` install is
 used)::
 
     python tests/golden/make_golden.py [proft] [steps] [adjoint] [coastal] [step_adjoint] [coupling] [mpdata]
-        [pom08] [seamount]
+        [pom08] [seamount] [shapiro]
 
 Writes ``tests/golden/*.npz``.  Every file records the reference's own CPU
 float32 outputs on seeded inputs; nothing here is needed at test time except
@@ -470,6 +470,18 @@ def make_coastal_policy_golden(im=24, jm=18, steps=(1, 3)):
     print("wrote", path, os.path.getsize(path))
 
 
+def make_shapiro_golden(im=20, jm=18, seed=81, gamma=0.05):
+    """The semi-implicit core with its spatial Shapiro filters on (barotropic
+    elevation after the solve, core.py:893-916, and tracers,
+    numerics/double_gyre.py:78-131; production runs them at gamma 0) on a
+    perturbed production state, 1 and 3 steps."""
+    name = "implicit_p0_fixed"
+    core = perturbed_core(name, im, jm, seed)
+    core.barotropic_shapiro = gamma
+    core.tracer_shapiro = gamma
+    make_step_golden(name, im, jm, seed, core=core, tag="implicit_shapiro")
+
+
 def make_pom08_goldens():
     """Both cores with the POM08-WAD closure of the reference's case
     policies bound by the reference's own installer
@@ -486,7 +498,8 @@ def make_pom08_goldens():
         make_step_golden(name, im, jm, seed, steps=steps, core=core, tag=tag)
 
 
-def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint", "coupling", "mpdata", "pom08", "seamount")):
+def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint", "coupling", "mpdata", "pom08", "seamount",
+                "shapiro")):
     src = rh.default_reference_path()
     if src is None:
         raise SystemExit("reference sources not found; set NPOM_REFERENCE_SRC")
@@ -516,8 +529,10 @@ def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint", "couplin
     if "seamount" in which:
         make_seamount_golden()
         make_coastal_policy_golden()
+    if "shapiro" in which:
+        make_shapiro_golden()
 
 
 if __name__ == "__main__":
     main(tuple(sys.argv[1:]) or ("proft", "steps", "adjoint", "coastal", "step_adjoint", "coupling", "mpdata",
-                                 "pom08", "seamount"))
+                                 "pom08", "seamount", "shapiro"))

@@ -17,7 +17,9 @@ STEP_FILES = [("step_explicit_12x10.npz", "explicit"), ("step_implicit_12x10.npz
               # the seamount case policy (its boundary with the POM08-WAD closure)
               ("step_seamount_explicit_24x18.npz", "explicit"),
               # the coastal tide policy (tide cells, four-edge radiation, step copies, closure)
-              ("step_coastal_policy_24x18.npz", "explicit")]
+              ("step_coastal_policy_24x18.npz", "explicit"),
+              # the semi-implicit core with its spatial Shapiro filters on (gamma 0.05)
+              ("step_implicit_shapiro_20x18.npz", "implicit_p0_fixed")]
 
 
 def _core(arrays, scalars, core):

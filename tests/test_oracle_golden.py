@@ -9,7 +9,9 @@ from oracle import pom_oracle as O
 STEP_FILES = [("step_explicit_12x10.npz", "explicit"), ("step_implicit_12x10.npz", "implicit_p0_fixed"),
               ("step_implicit_20x18.npz", "implicit_p0_fixed"), ("step_coastal_40x34.npz", "explicit"),
               # the POM08-WAD closure of the reference's case policies
-              ("step_pom08_explicit_12x10.npz", "explicit"), ("step_pom08_implicit_20x18.npz", "implicit_p0_fixed")]
+              ("step_pom08_explicit_12x10.npz", "explicit"), ("step_pom08_implicit_20x18.npz", "implicit_p0_fixed"),
+              # the semi-implicit core with its spatial Shapiro filters on
+              ("step_implicit_shapiro_20x18.npz", "implicit_p0_fixed")]
 PROGNOSTIC = ("u", "v", "t", "s", "el", "q2", "q2l", "km", "kh", "w", "rho", "ua", "va", "elf", "etf")
 
 
