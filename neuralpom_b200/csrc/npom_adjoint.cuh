@@ -297,7 +297,7 @@ NPOM_HD void smag_level_adj(const Ctx &c, const Adj &a, int i, int j, int k, flo
 
 template <int KM>
 NPOM_HD void baropg_column_adj(const Ctx &c, const Adj &a, int i, int j, const float *lamx, const float *lamy) {
-  const int kbm1 = c.kb - 1;
+  const int kbm1 = (KM == 16 ? 16 : c.kb) - 1;
   const float ramp = c.ramp;
   for (int comp = 0; comp < 2; ++comp) {
     const float *lam = comp == 0 ? lamx : lamy;
@@ -365,7 +365,7 @@ NPOM_HD void baropg_column_adj(const Ctx &c, const Adj &a, int i, int j, const f
 
 template <int KM>
 NPOM_HD void phase_a2_column_adj(const Ctx &c, const Adj &a, int i, int j) {
-  const int kb = c.kb, kbm1 = kb - 1;
+  const int kb = KM == 16 ? 16 : c.kb, kbm1 = kb - 1;
   const bool inner = interior(c, i, j);
   const float lsx = LA2(adx2d, i, j), lsy = LA2(ady2d, i, j), lrx = LA2(drx2d, i, j), lry = LA2(dry2d, i, j);
   const float lsa = LA2(aam2d, i, j);
@@ -1106,7 +1106,7 @@ NPOM_HD void phase_i5_cell_adj(const Ctx &c, const Adj &a, int i, int j) {
 // ===========================================================================
 template <int KM>
 NPOM_HD void phase_b1_column_adj(const Ctx &c, const Adj &a, int i, int j) {
-  const int kbm1 = c.kb - 1;
+  const int kbm1 = (KM == 16 ? 16 : c.kb) - 1;
   for (int comp = 0; comp < 2; ++comp) {
     const int fld = comp == 0 ? NPOM_F_u : NPOM_F_v;
     const size_t o = NPOM_I3(c, i, j, 0);
@@ -1157,7 +1157,7 @@ NPOM_HD void vertvl_yflux_adj(const Ctx &c, const Adj &a, int i, int j, int k, f
 
 template <int KM>
 NPOM_HD void phase_b2a_column_adj(const Ctx &c, const Adj &a, int i, int j) {
-  const int kb = c.kb, kbm1 = kb - 1;
+  const int kb = KM == 16 ? 16 : c.kb, kbm1 = kb - 1;
   const float fsm = F2(fsm, i, j);
   // bcond 5: explicit masks levels < kb-1, the closed basin every level
   const int kend = is_explicit(c) ? kbm1 : kb;
@@ -1282,7 +1282,9 @@ NPOM_HD void phase_b2b_point_adj(const Ctx &c, const Adj &a, int i, int j, int k
 // ===========================================================================
 template <int KM>
 NPOM_HD void phase_b3_column_adj(const Ctx &c, const Adj &a, int i, int j) {
-  const int im = c.im, jm = c.jm, kb = c.kb, kbm1 = kb - 1;
+  // KM == 16 is instantiated for kb == 16 only: a compile-time level count
+  // lets the compiler unroll the level loops and keep the column in registers
+  const int im = c.im, jm = c.jm, kb = KM == 16 ? 16 : c.kb, kbm1 = kb - 1;
   const float dti2 = c.k.dti2, umol2 = c.k.two_umol, grav = c.k.grav, kappa = c.k.kappa, small = c.k.small;
   const float b1 = 16.6f, e1 = 1.8f, e2 = 1.33f;
   const float eps = 1e-20f;
@@ -1801,7 +1803,7 @@ NPOM_HD void phase_b5_point_adj(const Ctx &c, const Adj &a, int i, int j, int k)
 template <int KM>
 NPOM_HD void proft_column_adj(const Ctx &c, const Adj &a, int i, int j, int fld, int nbc, float wfsurf,
                               float fsurf, const float *lout, float &ldh) {
-  const int kb = c.kb, kbm1 = kb - 1, kbm2 = kb - 2;
+  const int kb = KM == 16 ? 16 : c.kb, kbm1 = kb - 1, kbm2 = kb - 2;
   const size_t o = NPOM_I3(c, i, j, 0);
   const float *fcol = c.F[fld] + o;
   const float *khc = c.F[NPOM_F_kh] + o;
@@ -2167,7 +2169,7 @@ NPOM_HD void advv_point_adj(const Ctx &c, const Adj &a, int i, int j, int k, flo
 template <int KM>
 NPOM_HD void profuv_column_adj(const Ctx &c, const Adj &a, int comp, int i, int j, float *lout, float lwbot,
                                float ltps, float *lfin) {
-  const int kb = c.kb, kbm1 = kb - 1, kbm2 = kb - 2;
+  const int kb = KM == 16 ? 16 : c.kb, kbm1 = kb - 1, kbm2 = kb - 2;
   for (int k = 0; k < kb; ++k) lfin[k] = 0.0f;
   if (i < 1 || j < 1 || !interior(c, i, j)) {
     // out = fin, wbot keeps its value
@@ -2372,7 +2374,7 @@ NPOM_HD void phase_b8_column_adj(const Ctx &c, const Adj &a, int i, int j) {
 // ===========================================================================
 template <int KM>
 NPOM_HD void phase_b9_column_adj(const Ctx &c, const Adj &a, int i, int j) {
-  const int kb = c.kb, kbm1 = kb - 1;
+  const int kb = KM == 16 ? 16 : c.kb, kbm1 = kb - 1;
   if (c.do_internal) {
     const float hs = c.k.half_smoth;
     const bool ring = (i == 0 || i == c.im - 1 || j == 0 || j == c.jm - 1);

@@ -1308,8 +1308,9 @@ npom_status run_steps(const npom_params *p, float *const *fields, const npom_wor
     c.ramp = ramp_of(p, time);
     c.do_internal = ((iint != 1 || clk->time0 != 0.0) && p->mode != 2) ? 1 : 0;
     // the coastal policy's tide time of the step's first substep (its
-    // launches change every step: no graph replay)
-    c.tide_t0 = time * 86400.0 - p->dti;
+    // launches change every step: no graph replay).  Other steps keep 0:
+    // the context is the key of the step graphs
+    c.tide_t0 = c.k.obc_coastal ? time * 86400.0 - p->dti : 0.0;
     bool done = false;
     if (graphs && c.ramp == 1.0f && !c.k.obc_coastal) {
       if (launch_step_graph(c, core, plan, sub_blocks, s, &done) != cudaSuccess) return NPOM_ERR_CUDA;
