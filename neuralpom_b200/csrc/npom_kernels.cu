@@ -97,6 +97,13 @@ __global__ void __launch_bounds__(128) k_cols(Ctx c) {
   cols_body<PH>(c, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
+// PROFT one thread per column at kb == 16: the level loops unroll and the
+// column stays in registers
+__global__ void __launch_bounds__(128) k_cols_b6_kb16(Ctx c) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col < c.im * c.jm) phase_b6_column<16>(c, col / c.jm, col % c.jm);
+}
+
 // One 16-lane segment per water column (kb == 16).  Threads past the last
 // column work on a copy of it and store nothing, so that every shuffle sees
 // all 32 lanes of its warp.
@@ -852,6 +859,8 @@ void launch_cols(const Ctx &c, cudaStream_t s) {
   const bool pom08 = PH == CP_B3 && c.k.profq_pom08;
   if (lanes_enabled(c) && !proft_threads && !pom08) {
     k_lanes<PH><<<blocks_for(n * KL, kThreads), kThreads, 0, s>>>(c);
+  } else if (PH == CP_B6 && c.kb == 16) {
+    k_cols_b6_kb16<<<blocks_for(n, 128), 128, 0, s>>>(c);
   } else {
     k_cols<PH><<<blocks_for(n, 128), 128, 0, s>>>(c);
   }

@@ -621,9 +621,12 @@ struct ProftCol {
   float dti2, umol;
 };
 
+// KM: the level arrays; KM == 16 is used for kb == 16 only, whose
+// compile-time level count lets the loops unroll into registers
+template <int KM = KMAX>
 NPOM_HD float proft_column(const ProftCol &q) {
-  const int kb = q.kb, kbm1 = kb - 1, kbm2 = kb - 2;
-  float a[KMAX], cc[KMAX], ee[KMAX], gg[KMAX], rad[KMAX], fin[KMAX];
+  const int kb = KM == 16 ? 16 : q.kb, kbm1 = kb - 1, kbm2 = kb - 2;
+  float a[KM], cc[KM], ee[KM], gg[KM], rad[KM], fin[KM];
   for (int k = 0; k < kb; ++k) {
     a[k] = 0.0f;
     cc[k] = 0.0f;
@@ -677,7 +680,7 @@ NPOM_HD float proft_column(const ProftCol &q) {
   float num = cc[kbt] * gg[kbt - 1] - fin[kbt] + rt;
   float den = cc[kbt] * (1.0f - ee[kbt - 1]) - 1.0f;
   float nxt = num / (den + 1e-20f);
-  float outv[KMAX];
+  float outv[KM];
   for (int k = 0; k < kb; ++k) outv[k] = fin[k];
   outv[kbt] = nxt;
   for (int k = kbm1 - 2; k >= 0; --k) {
@@ -695,6 +698,7 @@ NPOM_HD float proft_column(const ProftCol &q) {
 NPOM_HD void bcond4_explicit_edge(const Ctx &c, int i, int j, float *ufc, float *vfc);
 NPOM_HD bool bcond4_explicit_level(const Ctx &c, int i, int j, int k, float &uo, float &vo);
 
+template <int KM = KMAX>
 NPOM_HD void phase_b6_column(const Ctx &c, int i, int j) {
   const int kb = c.kb;
   ProftCol q;
@@ -716,13 +720,13 @@ NPOM_HD void phase_b6_column(const Ctx &c, int i, int j) {
   q.nbc = c.k.nbct;
   q.wfsurf = F2(wtsurf, i, j);
   q.fsurf = F2(tsurf, i, j);
-  proft_column(q);
+  proft_column<KM>(q);
   q.f = vfc;
   q.out = vfc;
   q.nbc = c.k.nbcs;
   q.wfsurf = F2(wssurf, i, j);
   q.fsurf = F2(ssurf, i, j);
-  float dh = proft_column(q);
+  float dh = proft_column<KM>(q);
   P2(tps, i, j) = dh;
   if (is_explicit(c) && !c.k.obc_seamount && (i == 0 || i == c.im - 1 || j == 0 || j == c.jm - 1))
     bcond4_explicit_edge(c, i, j, ufc, vfc);
