@@ -119,6 +119,14 @@ __global__ void __launch_bounds__(128) kb_cols(const BatchTable *t, BatchStep v)
   cols_body<PH>(sc, lb * blockDim.x + threadIdx.x);
 }
 
+// thread-per-column PROFT with 16 levels at compile time (k_cols_b6_kb16)
+__global__ void __launch_bounds__(128) kb_cols_b6_kb16(const BatchTable *t, BatchStep v) {
+  __shared__ Ctx sc;
+  const int lb = batch_enter<BS_COLS>(t, v, sc);
+  const int col = lb * blockDim.x + threadIdx.x;
+  if (col < sc.im * sc.jm) phase_b6_column<16>(sc, col / sc.jm, col % sc.jm);
+}
+
 template <int PH>
 __global__ void __launch_bounds__(kThreads) kb_cells(const BatchTable *t, BatchStep v) {
   __shared__ Ctx sc;
@@ -210,6 +218,7 @@ struct BatchPlan {
   int clu_count[4] = {}, clu_nc[4] = {};
   size_t clu_smem[4] = {};
   bool lanes = false, b6_cols = false;
+  bool kb16 = false;      // every member has 16 levels (batch_uniform: one kb)
   bool a1_tiles = false, b5_tiles = false;
   bool sub_req = false;   // NPOM_BATCH_SUBCYCLE=coop when the plan was made
   bool sub_coop = false;  // the cooperative subcycle is in use
@@ -281,6 +290,7 @@ cudaError_t make_batch_plan(const std::vector<Ctx> &ctx, int core, BatchPlan *P)
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
   const Ctx &c0 = ctx[0];
   P->lanes = c0.kb == KL && lanes_enabled(c0);
+  P->kb16 = c0.kb == 16;
   P->nadv = c0.k.nadv;
   P->nitera = c0.k.nitera;
   P->mode = c0.k.mode;
@@ -442,6 +452,7 @@ cudaError_t batch_launch_coop(const void *fn, int blocks, void **args, const Bat
 template <int PH>
 void batch_cols(const BatchPlan &P, const BatchStep &v, cudaStream_t s) {
   if (P.lanes && !(PH == CP_B6 && P.b6_cols)) kb_lanes<PH><<<P.blocks[BS_LANES], kThreads, 0, s>>>(P.d_table, v);
+  else if (PH == CP_B6 && P.kb16) kb_cols_b6_kb16<<<P.blocks[BS_COLS], 128, 0, s>>>(P.d_table, v);
   else kb_cols<PH><<<P.blocks[BS_COLS], 128, 0, s>>>(P.d_table, v);
 }
 
