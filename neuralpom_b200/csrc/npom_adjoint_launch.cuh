@@ -142,7 +142,10 @@ __global__ void __launch_bounds__(T, GRID ? 0 : 1) k_adj_ext_forward(Ctx c, floa
 // from the last, restore its inputs and move the cotangents of what it
 // wrote (each thread its own cells), barrier, the phase's adjoint (scatters
 // are atomics in L2; every other read goes through L2 or is of a value the
-// thread itself moved), barrier.
+// thread itself moved), barrier.  The barrier after phase 3's adjoint is
+// left out: phase 2's restore and move (uaf, vaf, etf) at a cell touch
+// only values that phase 3's adjoint reads or scatters at that same cell,
+// and the same thread handles the cell in both loops.
 template <int T, bool GRID>
 __global__ void __launch_bounds__(T, GRID ? 0 : 1) k_adj_ext_reverse(Ctx c, Adj a, const float *save_end) {
   const size_t ncell = (size_t)c.im * c.jm;
@@ -170,7 +173,7 @@ __global__ void __launch_bounds__(T, GRID ? 0 : 1) k_adj_ext_reverse(Ctx c, Adj 
         else if (ph == 2) ext_phase2_cell_adj(c, a, i, j, iext);
         else ext_phase1_cell_adj(c, a, i, j, adv);
       }
-      if (!ext_sync<GRID>(c)) return;
+      if (ph != 3 && !ext_sync<GRID>(c)) return;
     }
   }
 }
