@@ -142,10 +142,14 @@ __global__ void __launch_bounds__(T, GRID ? 0 : 1) k_adj_ext_forward(Ctx c, floa
 // from the last, restore its inputs and move the cotangents of what it
 // wrote (each thread its own cells), barrier, the phase's adjoint (scatters
 // are atomics in L2; every other read goes through L2 or is of a value the
-// thread itself moved), barrier.  The barrier after phase 3's adjoint is
-// left out: phase 2's restore and move (uaf, vaf, etf) at a cell touch
-// only values that phase 3's adjoint reads or scatters at that same cell,
-// and the same thread handles the cell in both loops.
+// thread itself moved), barrier.  Phase 3's adjoint needs neither: at a
+// cell it reads and scatters the fields that phase 3 wrote (and that its
+// restore and move touch) only at that cell, and elf of its west and south
+// neighbours, which phase 3 does not write; phase 2's restore and move
+// (uaf, vaf, etf) likewise touch only values that phase 3's adjoint reads
+// or scatters at the same cell.  The same thread handles a cell in all
+// these loops, so restore 3, adjoint 3 and restore 2 run without a
+// barrier between them.
 template <int T, bool GRID>
 __global__ void __launch_bounds__(T, GRID ? 0 : 1) k_adj_ext_reverse(Ctx c, Adj a, const float *save_end) {
   const size_t ncell = (size_t)c.im * c.jm;
@@ -166,7 +170,7 @@ __global__ void __launch_bounds__(T, GRID ? 0 : 1) k_adj_ext_reverse(Ctx c, Adj 
           g[q] = 0.0f;
         }
       }
-      if (!ext_sync<GRID>(c)) return;
+      if (ph != 3 && !ext_sync<GRID>(c)) return;
       for (size_t q = tid; q < ncell; q += stride) {
         const int i = (int)(q / c.jm), j = (int)(q % c.jm);
         if (ph == 3) ext_phase3_cell_adj(c, a, i, j, iext);
