@@ -51,6 +51,10 @@ WORKLOADS = {
                       "dtI=300 s, seed = member), one simulated day of every member per bench step; the members "
                       "of each core advance as one batch, one launch per phase over all of them, the step "
                       "replayed as a CUDA graph"},
+    "channel": {"grid": GRID, "core": "implicit_p0_fixed", "internal": 288,
+                "desc": "semi-implicit core, 90x82x16 seamount channel periodic in x (two halo columns on each "
+                        "side, unique columns 2..87, walls in y; PCG preconditioned by Hartley along x times "
+                        "DST-I along y, cooperative-grid form), forward"},
     "coastal": {"grid": (354, 322, 16), "core": "explicit", "internal": 60, "horizon": 360,
                 "desc": "explicit core, 354x322x16 coastal basin (dx=500 m, open south boundary with Flather "
                         "condition and M2 elevation 1 m updated every bench step), forward; one bench step = 1 "
@@ -100,6 +104,7 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true", help="skip the per-field error against a float64 reference day")
     ap.add_argument("--no-batch-tune", action="store_true", help="batch workload: the library's launch rules only")
     ap.add_argument("--no-coastal", action="store_true", help="skip the 354x322x16 coastal forward+adjoint sample")
+    ap.add_argument("--no-periodic", action="store_true", help="skip the periodic-x channel sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--members", type=int, default=8,
                     help="ensemble members advanced concurrently on one GPU for the 'ensemble' key (1 = skip)")
@@ -146,6 +151,9 @@ def workload(member=0, name="seamount"):
         Sc = dict(Sc)
         Sc.update(time=0.25, time0=0.25)   # internal mode from the first step
         return A, Sc
+    if name == "channel":
+        A, Sc = cases.seamount_channel(*GRID[:2], kb=GRID[2], dti=DTI)
+        return A, dict(Sc)
     A, Sc = cases.seamount(*GRID[:2], kb=GRID[2], dti=DTI)
     if member:
         # ensemble members: seeded temperature perturbation (0.2 degC)
@@ -370,7 +378,7 @@ def run_b200(args):
                                   core_name=W["core"])
 
     fp64 = None
-    if rank == 0 and ws_n == 1 and not args.no_fp64 and args.workload in ("seamount", "gyre"):
+    if rank == 0 and ws_n == 1 and not args.no_fp64 and args.workload in ("seamount", "gyre", "channel"):
         fp64 = fp64_day_error(A, Sc, nin, dev, W["core"])
 
     cpu = None
@@ -396,6 +404,10 @@ def run_b200(args):
             fam["reference_gpu"] = reference_fwd_adjoint_sample(dev)
         if fam is not None and not args.no_cpu_baseline:
             fam["reference_cpu"] = reference_fwd_adjoint_sample("cpu", internal_steps=3)
+
+    per = None
+    if rank == 0 and ws_n == 1 and args.workload == "seamount" and not args.no_periodic:
+        per = periodic_sample(args, dev, flush)
 
     bat = None
     if rank == 0 and ws_n == 1 and args.workload == "seamount" and not args.no_batch and not args.fa_only:
@@ -425,7 +437,7 @@ def run_b200(args):
         "fp64_error": fp64,
         "roofline": roofline, "cpu_baseline": cpu, "reference_gpu": ref_gpu, "ensemble": ens, "fwd_adjoint": fa,
         "fwd_adjoint_midtrain": fam, "fwd_adjoint_midtrain_batch": famb, "fwd_adjoint_coastal": coastal,
-        "batch": bat, "e2e": e2e,
+        "batch": bat, "periodic_x": per, "e2e": e2e,
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
@@ -434,6 +446,46 @@ def run_b200(args):
     if pg:
         pg.barrier()
         pg.destroy_process_group()
+
+
+def periodic_sample(args, dev, flush, days=2):
+    """The headline basin as a channel periodic in x (the configuration's
+    boundary; the reference has none, so the headline runs closed walls):
+    one day of warm-up, then ``days`` simulated days timed with CUDA events
+    on the launching stream, L2 flushed before each."""
+    import torch
+    from neuralpom_b200 import _abi, resolve_core_class
+    W = WORKLOADS["channel"]
+    A, Sc = workload(name="channel")
+    core = resolve_core_class(W["core"]).from_state(A, Sc, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    nin = W["internal"]
+
+    def day():
+        t0 = float(core.time)
+        core.launch_steps(nin, t0, 1, stream)
+        core.time = core.dti * nin / 86400.0 + t0
+
+    day()
+    bits, _ = core.read_status(nin)
+    if bits & (_abi.DEV_TIMEOUT | _abi.DEV_VMAX | _abi.DEV_NONFINITE | _abi.DEV_PCG_MAXIT):
+        raise RuntimeError(f"periodic channel: device status 0x{bits:x} during warm-up")
+    ms = []
+    for _ in range(days):
+        l2_flush(flush)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        day()
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        ms.append(a.elapsed_time(b))
+    bits, its = core.read_status(nin)
+    if bits & (_abi.DEV_TIMEOUT | _abi.DEV_VMAX | _abi.DEV_NONFINITE | _abi.DEV_PCG_MAXIT):
+        raise RuntimeError(f"periodic channel: device status 0x{bits:x}")
+    per_day = statistics.median(ms)
+    return {"workload": W["desc"], "days_per_s": 1000.0 / per_day, "ms_per_day": per_day, "days_timed": days,
+            "pcg_iterations_last_call": {"mean": float(np.mean(its)), "min": int(min(its)), "max": int(max(its))}
+            if its else None}
 
 
 def ensemble_sample(args, W, nin, dev, flush):
@@ -545,7 +597,9 @@ def dominant_kernel_roofline(core, stream, dev, reps=20):
     sec = times[name] / 1000.0
     achieved = nbytes / sec / 1e9
     peak, src = measured_peaks()
-    traffic, traffic_src = NCU_DRAM_BYTES.get(name, (None, None)) if (im, jm, kb) == GRID else (None, None)
+    # the capture is of the closed basin's cluster solve
+    closed = (im, jm, kb) == GRID and not bool(getattr(core, "periodic_x", False))
+    traffic, traffic_src = NCU_DRAM_BYTES.get(name, (None, None)) if closed else (None, None)
     step_bytes = sum(phase_bytes(ph) for ph in times)
     step_ms = sum(times.values())
     notes = {

@@ -149,6 +149,7 @@ typedef struct npom_params {
   int32_t obc_form;        /* NPOM_OBC_NATIVE, _SEAMOUNT or _COASTAL       */
   npom_tuning tuning;      /* launch shapes (all zero: the library's rules) */
   double zsh;              /* POM08-WAD profq: roughness added to the mixing length (m) */
+  int32_t periodic_x;      /* 1: periodic in x (implicit core; see below)  */
 } npom_params;
 
 /* PROFQ forms.  PRODUCTION: the cores' own operator (explicit/tracers.py:158,
@@ -176,6 +177,20 @@ enum { NPOM_OBC_NATIVE = 0, NPOM_OBC_SEAMOUNT = 1, NPOM_OBC_COASTAL = 2 };
  * in the bottom-drag speed; cbc from the new depth after the external
  * substeps (zsh 0.01 m, z0b 0.005 m, clipped to [0.0025, 1]).  Forward
  * only. */
+
+/* Periodic x (periodic_x = 1).  No counterpart in the reference, whose
+ * only lateral boundaries are walls and open edges (its cores zero or
+ * radiate the ring).  The semi-implicit core only, with native boundaries,
+ * nadv 1 and the Jacobi preconditioner (the DST-I assumes walls in x).
+ * Columns 0, 1 and im-2, im-1 are halo copies of im-4, im-3 and 2, 3:
+ * the unique columns are 2..im-3 (period im-4), walls stay on the j
+ * edges.  After every phase of the step each plane of the state gets the
+ * halo copy, and the free-surface solve's unknowns are the unique columns
+ * with the operator's x neighbours wrapped.  Two halo columns because the
+ * reference's operators compute some intermediates only from column 1 or
+ * 2 on; with them every unique column is computed exactly as an interior
+ * column of a wider basin (the step is translation-equivariant in x).
+ * Forward only: the step adjoints and npom_step_batch refuse it. */
 
 enum { NPOM_CORE_EXPLICIT = 0, NPOM_CORE_IMPLICIT = 1 };
 enum { NPOM_PRECOND_JACOBI = 0, NPOM_PRECOND_SPECTRAL = 1 };

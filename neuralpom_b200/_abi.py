@@ -88,7 +88,8 @@ class NpomParams(ctypes.Structure):
             "pi", "eta_tol", "eta_rel_tol", "barotropic_shapiro", "tracer_shapiro", "velocity_shapiro",
             "wind_tau0", "vmix", "period", "inverse_scale", "sw")] + [
         ("nitera", ctypes.c_int32), ("profq_form", ctypes.c_int32),
-        ("obc_form", ctypes.c_int32), ("tuning", NpomTuning), ("zsh", ctypes.c_double)]
+        ("obc_form", ctypes.c_int32), ("tuning", NpomTuning), ("zsh", ctypes.c_double),
+        ("periodic_x", ctypes.c_int32)]
 
 
 class NpomWorkspace(ctypes.Structure):

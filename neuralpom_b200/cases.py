@@ -208,11 +208,18 @@ def _with_profile(A, s, t_of_z, salinity):
     A["rmean"] = A["rho"].copy()
 
 
-def seamount(im=90, jm=82, kb=16, dti=300.0, isplit=30, dx=5.0e3, u0=0.1, eta_tol=1e-10):
+def seamount(im=90, jm=82, kb=16, dti=300.0, isplit=30, dx=5.0e3, u0=0.1, eta_tol=1e-10, periodic_x=False):
     """Semi-implicit benchmark basin: flat 4500 m bottom with a Gaussian
     seamount (height 4000 m, e-folding 25 km) at the centre, dx = dy = 5 km,
     closed walls (the reference's ClosedBasinBoundary), f-plane at 40N,
-    T = 10 + 10 exp(z/1000 m), S = 35, uniform initial inflow u0, no wind."""
+    T = 10 + 10 exp(z/1000 m), S = 35, uniform initial inflow u0, no wind.
+
+    periodic_x: a channel periodic in x with walls in y instead (the
+    reference has no periodic boundary).  The unique columns are 2..im-3
+    (period (im-4) dx); columns 0, 1 and im-2, im-1 are halo copies
+    (``wrap_x``); the seamount sits at the centre of the unique columns
+    with its distance measured to the nearest periodic image; the η-solve's
+    spectral preconditioner is Hartley along x times DST-I along y."""
     core = "implicit_p0_fixed"
     s = state.default_scalars(core)
     s.update(dte=dti / isplit, isplit=isplit)
@@ -223,21 +230,56 @@ def seamount(im=90, jm=82, kb=16, dti=300.0, isplit=30, dx=5.0e3, u0=0.1, eta_to
     A["dy"][:] = dx
     A["north_e"][:] = 40.0
     A["cor"][:] = F32(2.0 * 7.2921e-5 * math.sin(math.radians(40.0)))
-    x = (np.arange(im, dtype=np.float64) - (im - 1) / 2.0) * dx
     y = (np.arange(jm, dtype=np.float64) - (jm - 1) / 2.0) * dx
+    if periodic_x:
+        period = (im - 4) * dx
+        x = (np.arange(im, dtype=np.float64) - 2.0 - (im - 5) / 2.0) * dx
+        x = x - period * np.round(x / period)
+    else:
+        x = (np.arange(im, dtype=np.float64) - (im - 1) / 2.0) * dx
     r2 = x[:, None] ** 2 + y[None, :] ** 2
     h = (4500.0 - 4000.0 * np.exp(-r2 / (25.0e3 ** 2))).astype(F32)
-    h[0, :] = 1.0
-    h[-1, :] = 1.0
+    if not periodic_x:
+        h[0, :] = 1.0
+        h[-1, :] = 1.0
     h[:, 0] = 1.0
     h[:, -1] = 1.0
     A["h"] = h
     A["z"], A["zz"], A["dz"], A["dzz"] = sigma_levels(kb)
+    if periodic_x:
+        wrap_x(A["h"])
     areas_masks(A)
+    if periodic_x:
+        for n in ("aru", "arv", "fsm", "dum", "dvm"):
+            wrap_x(A[n])
+        s["periodic_x"] = True
     _with_profile(A, s, lambda z: 10.0 + 10.0 * np.exp(z / 1000.0), 35.0)
     A["ub"][:, :, : kb - 1] = F32(u0) * A["dum"][:, :, None]
     A["uab"][:] = F32(u0) * A["dum"]
-    return finish_initialization(A, s, core)
+    A, s = finish_initialization(A, s, core)
+    if periodic_x:
+        for n, a in A.items():
+            if np.ndim(a) >= 2 and a.shape[:2] == (im, jm):
+                wrap_x(a)
+    return A, s
+
+
+def seamount_channel(im=90, jm=82, kb=16, **kw):
+    """The benchmark seamount as a channel periodic in x (walls in y):
+    ``seamount(periodic_x=True)``; at 90x82 the unique columns are 2..87."""
+    return seamount(im, jm, kb, periodic_x=True, **kw)
+
+
+def wrap_x(a):
+    """Halo columns of a periodic-x plane (i first), two on each side:
+    columns 0, 1 take im-4, im-3 and columns im-2, im-1 take 2, 3.  A
+    u-point column i is the west face of cell i, so the copy serves every
+    staggering."""
+    n = a.shape[0]
+    a[0] = a[n - 4]
+    a[1] = a[n - 3]
+    a[n - 2] = a[2]
+    a[n - 1] = a[3]
 
 
 def noise_basin(im=64, jm=64, kb=16, dte=6.0, isplit=30, dx=20.0e3, seed=0, core="explicit"):

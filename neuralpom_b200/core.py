@@ -106,7 +106,8 @@ class B200Core:
         # so an id in the key cannot be recycled by a new tensor.
         geo = tuple((n, id(getattr(self, n)), getattr(self, n).data_ptr(), getattr(self, n)._version)
                     for n in ("dx", "dy", "h"))
-        key = (self.im, self.jm, self.kb, self.device, geo, float(self.dti), float(self.alpha))
+        key = (self.im, self.jm, self.kb, self.device, geo, float(self.dti), float(self.alpha),
+               bool(getattr(self, "periodic_x", False)))
         if self._ws is not None and self._ws_key == key:
             return self._ws
         im, jm, dev = self.im, self.jm, self.device
@@ -139,11 +140,10 @@ class B200Core:
         if self.core_name != "explicit":
             sx, sy, ie = state.spectral_setup(self.dx.detach().cpu().numpy(), self.dy.detach().cpu().numpy(),
                                               self.h.detach().cpu().numpy(), float(self.dti), float(self.grav),
-                                              float(self.alpha))
+                                              float(self.alpha), periodic_x=bool(getattr(self, "periodic_x", False)))
             b = self._ws["bufs"]
-            b["sx"].copy_(torch.from_numpy(sx))
-            b["sy"].copy_(torch.from_numpy(sy))
-            b["inv_eigs"].copy_(torch.from_numpy(ie))
+            for n, a in (("sx", sx), ("sy", sy), ("inv_eigs", ie)):
+                state.fill_flat(b[n], a)
         self._ws_key = key
         self._ws_geo = tuple(getattr(self, n) for n in ("dx", "dy", "h"))
         return self._ws
@@ -239,6 +239,8 @@ class B200Core:
                 # (cores/case_adapters/registry.py:38-41)
                 raise RuntimeError("Registered case policies require advancement inside torch.no_grad(); "
                                    "their training adjoints are unvalidated.")
+            if bool(getattr(self, "periodic_x", False)):
+                raise RuntimeError("periodic x is forward only: advance inside torch.no_grad()")
             outs = _StepsFunction.apply(self, nsteps, float(self.time0),
                                         *[getattr(self, f) for f in _abi.ADJ_STATE_FIELDS])
             for f, o in zip(_abi.ADJ_STATE_FIELDS, outs):

@@ -2621,8 +2621,9 @@ inline int adj_step_plan(const Ctx &c, AdjPhaseRec *out, int cap, size_t *save_f
 inline bool adj_supported(const npom_params *p) {
   // the POM08-WAD PROFQ is forward only, as in the reference's case
   // policies (which refuse advancement with gradients)
+  // (periodic x is forward only too: its halo copies have no reverse here)
   const bool base = p->mode == 3 && (p->nbct == 1 || p->nbct == 3) && (p->nbcs == 1 || p->nbcs == 3) &&
-                    p->profq_form == NPOM_PROFQ_PRODUCTION && p->obc_form == NPOM_OBC_NATIVE;
+                    p->profq_form == NPOM_PROFQ_PRODUCTION && p->obc_form == NPOM_OBC_NATIVE && !p->periodic_x;
   if (p->core == NPOM_CORE_EXPLICIT) return base && (p->nadv == 1 || p->nadv == 2);
   return base && (p->nadv == 1 || p->nadv == 2) && p->core == NPOM_CORE_IMPLICIT && p->barotropic_shapiro == 0.0 &&
          p->tracer_shapiro == 0.0;

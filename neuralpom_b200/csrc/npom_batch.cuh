@@ -617,9 +617,11 @@ bool batch_uniform(const npom_params *const *p, int nm) {
       return false;
   }
   // the POM08-WAD PROFQ has no lane body, which the batched column phases
-  // use, and the seamount boundary's Orlanski passes are not batched
+  // use, and the seamount boundary's Orlanski passes and the periodic-x
+  // halo copies are not batched
   for (int m = 0; m < nm; ++m)
-    if (p[m]->profq_form != NPOM_PROFQ_PRODUCTION || p[m]->obc_form != NPOM_OBC_NATIVE) return false;
+    if (p[m]->profq_form != NPOM_PROFQ_PRODUCTION || p[m]->obc_form != NPOM_OBC_NATIVE || p[m]->periodic_x)
+      return false;
   return true;
 }
 

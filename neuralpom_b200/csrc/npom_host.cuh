@@ -54,6 +54,7 @@ inline Consts make_consts(const npom_params &p) {
   k.kappa_zsh = (float)(p.kappa * p.zsh);
   k.obc_seamount = p.obc_form == NPOM_OBC_SEAMOUNT ? 1 : 0;
   k.obc_coastal = p.obc_form == NPOM_OBC_COASTAL ? 1 : 0;
+  k.periodic_x = p.periodic_x ? 1 : 0;
   // coastal_boundary.py:9-10: (29.03225806451612*3.1416/180) in double
   k.tide_w = 29.03225806451612 * 3.1416 / 180.0;
   k.dte_d = p.dte;
@@ -111,6 +112,10 @@ inline bool check_args(const npom_params *p, float *const *fields, const npom_wo
   if (p->obc_form != NPOM_OBC_NATIVE &&
       ((p->obc_form != NPOM_OBC_SEAMOUNT && p->obc_form != NPOM_OBC_COASTAL) || p->core != NPOM_CORE_EXPLICIT ||
        p->im < 6 || p->jm < 6 || (p->obc_form == NPOM_OBC_COASTAL && !ws->tide)))
+    return false;
+  if (p->periodic_x &&
+      (p->periodic_x != 1 || p->core != NPOM_CORE_IMPLICIT || p->obc_form != NPOM_OBC_NATIVE || p->nadv != 1 ||
+       p->im < 8))
     return false;
   for (int w = 0; w < NPOM_NWS; ++w)
     if (!ws->buf[w]) return false;

@@ -412,7 +412,9 @@ template <bool ALONG_I, class Epi>
 __device__ __forceinline__ void dst_tiles(const Ctx &c, const float *src, bool src_is_grid, Epi &&epi) {
   __shared__ float lt[kDstRows][kDstChunk + 1];
   __shared__ float rt[kDstChunk][kDstCols + 1];
-  const int ni = c.im - 2, nj = c.jm - 2;
+  // rows: the solve's unknowns (with periodic x the unique columns, Sx the
+  // Hartley matrix of the period)
+  const int i0 = pcg_i0(c), ni = c.im - 2 * i0, nj = c.jm - 2;
   const int K = ALONG_I ? ni : nj;
   const float *sx = c.W[NPOM_W_sx], *sy = c.W[NPOM_W_sy];
   const int tiles_b = (nj + kDstCols - 1) / kDstCols;
@@ -436,7 +438,7 @@ __device__ __forceinline__ void dst_tiles(const Ctx &c, const float *src, bool s
         float v = 0.0f;
         if (k < mc && b0 + col < nj) {
           if (!ALONG_I) v = __ldcg(sy + (size_t)(m0 + k) * nj + b0 + col);
-          else if (src_is_grid) v = __ldcg(src + NPOM_I2(c, m0 + k + 1, b0 + col + 1));
+          else if (src_is_grid) v = __ldcg(src + NPOM_I2(c, m0 + k + i0, b0 + col + 1));
           else v = __ldcg(src + (size_t)(m0 + k) * nj + b0 + col);
         }
         rt[k][col] = v;
@@ -452,8 +454,8 @@ __device__ __forceinline__ void dst_tiles(const Ctx &c, const float *src, bool s
 // z = M^-1 r over the interior; returns after its own trailing barrier.
 // Accumulates r.z into *rz of this thread.
 __device__ bool precondition(const Ctx &c, double &rz) {
-  const int ni = c.im - 2, nj = c.jm - 2;
-  const size_t nint = (size_t)ni * nj;
+  const int nj = c.jm - 2, i0 = pcg_i0(c);
+  const size_t nint = (size_t)(c.im - 2 * i0) * nj;
   const size_t stride = (size_t)vgrid(c) * blockDim.x;
   const size_t tid = (size_t)vblock(c) * blockDim.x + threadIdx.x;
   float *zv = c.W[NPOM_W_zv];
@@ -474,14 +476,14 @@ __device__ bool precondition(const Ctx &c, double &rz) {
     const float inv_scale = c.k.inverse_scale;
     dst_tiles<false>(c, t1, false, [&](int a, int b, float v) {
       const float zval = v / inv_scale;
-      const size_t o = NPOM_I2(c, a + 1, b + 1);
+      const size_t o = NPOM_I2(c, a + i0, b + 1);
       zv[o] = zval;
       rz += (double)__ldcg(r + o) * (double)zval;
     });
   } else {
     for (size_t q = tid; q < nint; q += stride) {
       int a = (int)(q / nj), b = (int)(q % nj);
-      size_t o = NPOM_I2(c, a + 1, b + 1);
+      size_t o = NPOM_I2(c, a + i0, b + 1);
       float rv = __ldcg(r + o);
       float zval = rv / (__ldcg(c.W[NPOM_W_diag] + o) + 1e-30f);
       zv[o] = zval;
@@ -496,8 +498,10 @@ __device__ bool precondition(const Ctx &c, double &rz) {
 // d = h + elf.  Iterations -> c.cg_iters[c.sync[2]++] (one slot per solve
 // of the call).
 __device__ __forceinline__ void pcg_coop_body(const Ctx &c, int with_rhs, int with_post) {
-  const int im = c.im, jm = c.jm, ni = im - 2, nj = jm - 2;
-  const size_t ncell = (size_t)im * jm, nint = (size_t)ni * nj;
+  // unknowns: rows i0 .. im-1-i0 (the interior, or the unique columns of a
+  // periodic-x basin)
+  const int im = c.im, jm = c.jm, i0 = pcg_i0(c), nj = jm - 2;
+  const size_t ncell = (size_t)im * jm, nint = (size_t)(im - 2 * i0) * nj;
   const size_t stride = (size_t)vgrid(c) * blockDim.x;
   const size_t tid = (size_t)vblock(c) * blockDim.x + threadIdx.x;
   float *x = c.W[NPOM_W_x], *r = c.W[NPOM_W_r], *p = c.W[NPOM_W_p], *zv = c.W[NPOM_W_zv];
@@ -533,7 +537,7 @@ __device__ __forceinline__ void pcg_coop_body(const Ctx &c, int with_rhs, int wi
   if (!grid_barrier(c)) return;
   double rr = 0.0;
   for (size_t q = tid; q < nint; q += stride) {
-    int i = (int)(q / nj) + 1, j = (int)(q % nj) + 1;
+    int i = (int)(q / nj) + i0, j = (int)(q % nj) + 1;
     size_t o = NPOM_I2(c, i, j);
     float a = elliptic_apply_cell(c, x, i, j);
     float rv = __ldcg(rhs + o) - a;
@@ -550,7 +554,7 @@ __device__ __forceinline__ void pcg_coop_body(const Ctx &c, int with_rhs, int wi
   double rs0 = grid_total(c, 1);
   double rho_old = grid_total(c, 2);
   for (size_t q = tid; q < nint; q += stride) {
-    size_t o = NPOM_I2(c, (int)(q / nj) + 1, (int)(q % nj) + 1);
+    size_t o = NPOM_I2(c, (int)(q / nj) + i0, (int)(q % nj) + 1);
     p[o] = __ldcg(zv + o);
   }
   const double tol = pcg_abs_tol(c), tol_sq = tol * tol;
@@ -563,7 +567,7 @@ __device__ __forceinline__ void pcg_coop_body(const Ctx &c, int with_rhs, int wi
   for (int it = 1; it <= c.k.eta_max_iter; ++it) {
     double pap = 0.0;
     for (size_t q = tid; q < nint; q += stride) {
-      int i = (int)(q / nj) + 1, j = (int)(q % nj) + 1;
+      int i = (int)(q / nj) + i0, j = (int)(q % nj) + 1;
       size_t o = NPOM_I2(c, i, j);
       float a, pv;
       if (pending) {
@@ -588,7 +592,7 @@ __device__ __forceinline__ void pcg_coop_body(const Ctx &c, int with_rhs, int wi
     float alpha = (float)(rho_old / (denom + 1e-30));
     double rs = 0.0;
     for (size_t q = tid; q < nint; q += stride) {
-      size_t o = NPOM_I2(c, (int)(q / nj) + 1, (int)(q % nj) + 1);
+      size_t o = NPOM_I2(c, (int)(q / nj) + i0, (int)(q % nj) + 1);
       x[o] = __ldcg(x + o) + alpha * __ldcg(p + o);
       float rv = __ldcg(r + o) - alpha * __ldcg(ap + o);
       r[o] = rv;
@@ -614,7 +618,7 @@ __device__ __forceinline__ void pcg_coop_body(const Ctx &c, int with_rhs, int wi
       continue;
     }
     for (size_t q = tid; q < nint; q += stride) {
-      size_t o = NPOM_I2(c, (int)(q / nj) + 1, (int)(q % nj) + 1);
+      size_t o = NPOM_I2(c, (int)(q / nj) + i0, (int)(q % nj) + 1);
       p[o] = __ldcg(p + o) * beta + __ldcg(zv + o);
     }
     if (!grid_barrier(c)) return;
@@ -627,8 +631,17 @@ __device__ __forceinline__ void pcg_coop_body(const Ctx &c, int with_rhs, int wi
   }
   if (!grid_barrier(c)) return;
   if (!with_post) {
-    // raw solution into elf (the ring of x is zero)
-    for (size_t q = tid; q < ncell; q += stride) c.F[NPOM_F_elf][q] = __ldcg(x + q);
+    // raw solution into elf (the ring of x is zero; with periodic x the
+    // halo columns are the copies of their unique columns)
+    for (size_t q = tid; q < ncell; q += stride) {
+      size_t src = q;
+      if (c.k.periodic_x) {
+        const int i = (int)(q / jm), j = (int)(q % jm);
+        const int iw = i < 2 ? i + im - 4 : (i > im - 3 ? i - (im - 4) : i);
+        src = NPOM_I2(c, iw, j);
+      }
+      c.F[NPOM_F_elf][q] = __ldcg(x + src);
+    }
     return;
   }
   for (size_t q = tid; q < ncell; q += stride) {
@@ -636,7 +649,8 @@ __device__ __forceinline__ void pcg_coop_body(const Ctx &c, int with_rhs, int wi
     float e = 0.0f;
     if (interior(c, i, j)) {
       float x0 = __ldcg(x + q);
-      float sm = x0 + c.k.bshap_q * (__ldcg(x + q + jm) + __ldcg(x + q - jm) + __ldcg(x + q + 1) + __ldcg(x + q - 1) - 4.0f * x0);
+      const size_t qe = NPOM_I2(c, pcg_east(c, i), j), qw = NPOM_I2(c, pcg_west(c, i), j);
+      float sm = x0 + c.k.bshap_q * (__ldcg(x + qe) + __ldcg(x + qw) + __ldcg(x + q + 1) + __ldcg(x + q - 1) - 4.0f * x0);
       float fsm = F2(fsm, i, j);
       e = (sm * fsm) * fsm;
       if (!(fabsf(e) <= 3.0e38f)) atomicOr(c.status, NPOM_DEV_NONFINITE);
@@ -877,6 +891,9 @@ void launch_cells(const Ctx &c, cudaStream_t s) {
 // interiors); NPOM_PCG=coop forces the grid-barrier kernel,
 // NPOM_PCG_CTAS=16 prefers the 16-CTA cluster.
 bool pcg_cluster_layout(const Ctx &c, ClusterLayout *out) {
+  // periodic x: the cooperative grid form, whose operator wraps its x
+  // neighbours (the cluster forms' slabs assume the Dirichlet ring)
+  if (c.k.periodic_x) return false;
   const char *env = getenv("NPOM_PCG");
   if (env && std::strcmp(env, "coop") == 0) return false;
   if (!env && c.tune.pcg_form == 3) return false;
@@ -1093,17 +1110,74 @@ void launch_obc_seamount(const Ctx &c, int which, cudaStream_t s) {
   k_obc_seamount<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(c, which);
 }
 
+// The periodic-x halo copy after a phase: in every plane of the state (the
+// 2-D geometry and state, the 3-D state) and the workspace planes that
+// carry values from one phase to the next, columns 0, 1 take im-4, im-3
+// and columns im-2, im-1 take 2, 3.  Sources are unique columns and
+// destinations halo columns (im >= 8), so the copies are independent.
+// Planes are (i, j[, k]) with i slowest: a column is jm*depth contiguous
+// floats.  blockIdx.y is the plane.
+constexpr int kWrapGeom = NPOM_F_north_e - NPOM_F_h + 1;
+constexpr int kWrap3d = NPOM_F_curv - NPOM_F_u + 1;
+constexpr int kWrap2d = NPOM_F_ssurf - NPOM_F_el + 1;
+constexpr int kWrapPlanes = kWrapGeom + kWrap3d + kWrap2d + 5;
+
+// the workspace planes read by a later phase: us, vs, den_u, den_v, d_baro
+__device__ __forceinline__ int wrap_ws(int w) {
+  return w == 0 ? NPOM_W_us : w == 1 ? NPOM_W_vs : w == 2 ? NPOM_W_den_u : w == 3 ? NPOM_W_den_v : NPOM_W_d_baro;
+}
+
+__global__ void __launch_bounds__(kThreads) k_wrap_x(Ctx c) {
+  const int slot = blockIdx.y;
+  float *a;
+  int depth = 1;
+  if (slot < kWrapGeom) {
+    a = c.F[NPOM_F_h + slot];
+  } else if (slot < kWrapGeom + kWrap3d) {
+    a = c.F[NPOM_F_u + slot - kWrapGeom];
+    depth = c.kb;
+  } else if (slot < kWrapGeom + kWrap3d + kWrap2d) {
+    a = c.F[NPOM_F_el + slot - kWrapGeom - kWrap3d];
+  } else {
+    a = c.W[wrap_ws(slot - kWrapGeom - kWrap3d - kWrap2d)];
+  }
+  const size_t col = (size_t)c.jm * depth;
+  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 4 * col) return;
+  const int which = (int)(e / col);
+  const size_t off = e - (size_t)which * col;
+  const int im = c.im;
+  const int dst = which == 0 ? 0 : which == 1 ? 1 : which == 2 ? im - 2 : im - 1;
+  const int src = which == 0 ? im - 4 : which == 1 ? im - 3 : which == 2 ? 2 : 3;
+  a[(size_t)dst * col + off] = a[(size_t)src * col + off];
+}
+
+void launch_wrap_x(const Ctx &c, cudaStream_t s) {
+  if (!c.k.periodic_x) return;
+  const size_t n = 4 * (size_t)c.jm * c.kb;
+  k_wrap_x<<<dim3((unsigned)((n + kThreads - 1) / kThreads), kWrapPlanes), kThreads, 0, s>>>(c);
+}
+
 void internal_mode(const Ctx &c, cudaStream_t s) {
   launch_cols<CP_B1>(c, s);
+  launch_wrap_x(c, s);
   launch_cols<CP_B2A>(c, s);
+  launch_wrap_x(c, s);
   launch_points<PP_B2B>(c, s);
+  launch_wrap_x(c, s);
   launch_cols<CP_B3>(c, s);
+  launch_wrap_x(c, s);
   launch_points<PP_B4>(c, s);
+  launch_wrap_x(c, s);
   launch_b5(c, s);
+  launch_wrap_x(c, s);
   launch_cols<CP_B6>(c, s);
+  launch_wrap_x(c, s);
   launch_obc_seamount(c, 1, s);
   launch_points<PP_B7>(c, s);
+  launch_wrap_x(c, s);
   launch_cols<CP_B8>(c, s);
+  launch_wrap_x(c, s);
   launch_obc_seamount(c, 0, s);
 }
 
@@ -1197,13 +1271,18 @@ __global__ void __launch_bounds__(kThreads) k_cbc_coastal(Ctx c) {
 
 cudaError_t enqueue_step(const Ctx &c, int core, const PcgPlan &plan, int sub_blocks, cudaStream_t s) {
   launch_a1(c, s);
+  launch_wrap_x(c, s);
   launch_cols<CP_A2>(c, s);
+  launch_wrap_x(c, s);
   launch_cells<XP_A3>(c, s);
+  launch_wrap_x(c, s);
   cudaError_t e;
   if (core == NPOM_CORE_IMPLICIT) {
     e = run_pcg(c, plan, 1, 1, s);
     if (e != cudaSuccess) return e;
+    launch_wrap_x(c, s);
     launch_cells<XP_I5>(c, s);
+    launch_wrap_x(c, s);
   } else {
     e = run_subcycle(c, sub_blocks, s);
     if (e != cudaSuccess) return e;
@@ -1214,6 +1293,7 @@ cudaError_t enqueue_step(const Ctx &c, int core, const PcgPlan &plan, int sub_bl
   }
   if (c.do_internal) internal_mode(c, s);
   launch_cols<CP_B9>(c, s);
+  launch_wrap_x(c, s);
   return cudaGetLastError();
 }
 
@@ -1696,6 +1776,7 @@ npom_status npom_run_phase(const npom_params *p, float *const *fields, const npo
     case 14: launch_cols<CP_B9>(c, s); break;
   }
   if (e != cudaSuccess) return NPOM_ERR_CUDA;
+  launch_wrap_x(c, s);  // the phase's periodic-x halo copy, as in the step
   return cudaGetLastError() == cudaSuccess ? NPOM_OK : NPOM_ERR_CUDA;
 }
 

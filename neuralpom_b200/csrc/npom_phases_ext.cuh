@@ -129,8 +129,21 @@ NPOM_HD void elliptic_coeff_cell(const Ctx &c, int i, int j) {
   PW2(inv_art, i, j) = 1.0f / (F2(art, i, j) + 1e-20f);
 }
 
+// The unknowns of the free-surface solve: rows pcg_i0 .. im-1-pcg_i0 of
+// the interior columns 1..jm-2 -- the interior (Dirichlet ring), or with
+// periodic x the unique columns 2..im-3 (the halo columns 1 and im-2 are
+// copies, not unknowns).
+NPOM_HD int pcg_i0(const Ctx &c) { return c.k.periodic_x ? 2 : 1; }
+
+// Row of the x neighbour of unknown row i seen by the solve's vectors (the
+// geometry's halo columns are copies already): i -/+ 1, wrapped across
+// the period with periodic x.
+NPOM_HD int pcg_west(const Ctx &c, int i) { return (c.k.periodic_x && i == 2) ? c.im - 3 : i - 1; }
+NPOM_HD int pcg_east(const Ctx &c, int i) { return (c.k.periodic_x && i == c.im - 3) ? 2 : i + 1; }
+
 // out = eta - coeff * div(D grad eta) / art on the interior (core.py:591-639);
-// eta is a workspace or field vector with a zero Dirichlet ring.
+// eta is a workspace or field vector with a zero Dirichlet ring (with
+// periodic x its x neighbours are read across the period).
 NPOM_HD float elliptic_apply_cell(const Ctx &c, const float *eta, int i, int j) {
   const size_t o = NPOM_I2(c, i, j);
   float e = ldc(c, eta + o);
@@ -142,8 +155,10 @@ NPOM_HD float elliptic_apply_cell(const Ctx &c, const float *eta, int i, int j) 
   float hw = 0.5f * (d0 + ldc(c, dd + o - jm));
   float hn = 0.5f * (ldc(c, dd + o + 1) + d0);
   float hs = 0.5f * (d0 + ldc(c, dd + o - 1));
-  float fe = he * (ldc(c, eta + o + jm) - e) * W2(ce, i, j) * F2(dum, i + 1, j);
-  float fw = hw * (e - ldc(c, eta + o - jm)) * W2(cw, i, j) * F2(dum, i, j);
+  const float ee = ldc(c, eta + NPOM_I2(c, pcg_east(c, i), j));
+  const float ew = ldc(c, eta + NPOM_I2(c, pcg_west(c, i), j));
+  float fe = he * (ee - e) * W2(ce, i, j) * F2(dum, i + 1, j);
+  float fw = hw * (e - ew) * W2(cw, i, j) * F2(dum, i, j);
   float fn = hn * (ldc(c, eta + o + 1) - e) * W2(cn, i, j) * F2(dvm, i, j + 1);
   float fs = hs * (e - ldc(c, eta + o - 1)) * W2(cs, i, j) * F2(dvm, i, j);
   float div = (fe - fw + fn - fs) * W2(inv_art, i, j);
@@ -172,8 +187,8 @@ NPOM_HD float elliptic_apply_cell_pz(const Ctx &c, const float *p, const float *
   float hw = 0.5f * (d0 + ldc(c, dd + o - jm));
   float hn = 0.5f * (ldc(c, dd + o + 1) + d0);
   float hs = 0.5f * (d0 + ldc(c, dd + o - 1));
-  float fe = he * (pv(i + 1, j) - e) * W2(ce, i, j) * F2(dum, i + 1, j);
-  float fw = hw * (e - pv(i - 1, j)) * W2(cw, i, j) * F2(dum, i, j);
+  float fe = he * (pv(pcg_east(c, i), j) - e) * W2(ce, i, j) * F2(dum, i + 1, j);
+  float fw = hw * (e - pv(pcg_west(c, i), j)) * W2(cw, i, j) * F2(dum, i, j);
   float fn = hn * (pv(i, j + 1) - e) * W2(cn, i, j) * F2(dvm, i, j + 1);
   float fs = hs * (e - pv(i, j - 1)) * W2(cs, i, j) * F2(dvm, i, j);
   float div = (fe - fw + fn - fs) * W2(inv_art, i, j);
@@ -196,12 +211,14 @@ NPOM_HD float jacobi_diag_cell(const Ctx &c, int i, int j) {
 // Spectral preconditioner stages (core.py:762-773): DST-I along i, along j,
 // scale by the inverse eigenvalues, DST-I along i, along j, / inverse_scale.
 // Index (a, b) runs over the ni x nj interior.
+// With periodic x the rows are the unique columns (ni = im-4, grid row
+// a + 2) and Sx is the Hartley matrix of the period (see spectral_setup).
 NPOM_HD float dst_stage_i(const Ctx &c, const float *src, bool src_is_grid, int a, int b) {
-  const int ni = c.im - 2, nj = c.jm - 2;
+  const int i0 = pcg_i0(c), ni = c.im - 2 * i0, nj = c.jm - 2;
   const float *sx = c.W[NPOM_W_sx];
   double acc = 0.0;
   for (int m = 0; m < ni; ++m) {
-    float v = src_is_grid ? ldc(c, src + NPOM_I2(c, m + 1, b + 1)) : ldc(c, src + (size_t)m * nj + b);
+    float v = src_is_grid ? ldc(c, src + NPOM_I2(c, m + i0, b + 1)) : ldc(c, src + (size_t)m * nj + b);
     acc += (double)ldc(c, sx + (size_t)a * ni + m) * (double)v;
   }
   return (float)acc;

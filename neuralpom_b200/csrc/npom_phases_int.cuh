@@ -936,7 +936,7 @@ NPOM_HD float advv_point(const Ctx &c, int i, int j, int k) {
 // forecast fin[] of that column.  Returns wbot; writes out[] and tps.
 NPOM_HD void profuv_column(const Ctx &c, int comp, int i, int j, const float *fin, float *out, float &wbot,
                            float &tps) {
-  const int kb = c.kb, kbm1 = kb - 1, kbm2 = kb - 2, im = c.im, jm = c.jm;
+  const int kb = c.kb, kbm1 = kb - 1, kbm2 = kb - 2;
   for (int k = 0; k < kb; ++k) out[k] = fin[k];
   wbot = comp == 0 ? F2(wubot, i, j) : F2(wvbot, i, j);
   tps = 0.0f;

@@ -132,6 +132,18 @@ def make_params(s, im, jm, kb, core, device=0):
     if obc != "native" and implicit:
         raise ValueError(f"the {obc} boundary policy is built for the explicit core")
     p.obc_form = {"native": _abi.OBC_NATIVE, "seamount": _abi.OBC_SEAMOUNT, "coastal": _abi.OBC_COASTAL}[obc]
+    # periodic x: two halo columns on each side, unique columns 2..im-3
+    # (no counterpart in the reference, whose lateral boundaries are walls
+    # and open edges)
+    periodic = bool(get("periodic_x", False))
+    if periodic:
+        if not implicit:
+            raise ValueError("periodic x is built for the semi-implicit core")
+        if obc != "native" or int(p.nadv) != 1 or im < 8:
+            raise ValueError("periodic x needs native boundaries, nadv 1 and im >= 8")
+        # Hartley along the period (im-4 unique columns) times DST-I in y
+        p.inverse_scale = 2.0 * (im - 4) * (jm - 1)
+    p.periodic_x = 1 if periodic else 0
     tuning = get("tuning", None) or {}
     for k, v in dict(tuning).items():
         if k not in _abi.TUNING_FIELDS:
@@ -140,22 +152,35 @@ def make_params(s, im, jm, kb, core, device=0):
     return p
 
 
-def spectral_setup(dx, dy, h, dti, grav, alpha, dtype=np.float32):
+def spectral_setup(dx, dy, h, dti, grav, alpha, dtype=np.float32, periodic_x=False):
     """DST-I matrices and inverse eigenvalues of the spectral preconditioner
     (``implicit_p0_fixed/core.py:730-760``; torch.median picks the lower
-    middle value)."""
+    middle value).
+
+    periodic_x (no counterpart in the reference): the rows are the n = im-4
+    unique columns and Sx is the Hartley matrix cas(2 pi k m / n) =
+    cos + sin, which is symmetric with Sx Sx = n I and diagonalises the
+    periodic second difference with the eigenvalues 4 sin^2(pi k / n) --
+    so z = Sx ((Sx r Sy) * inv_eigs) Sy / (2 n (nj + 1)) is the same
+    symmetric two-sided product as the DST-I form.  The medians are taken
+    over the unique columns."""
     im, jm = dx.shape
-    ni, nj = im - 2, jm - 2
+    rows = slice(2, im - 2) if periodic_x else slice(1, im - 1)
+    ni, nj = (im - 4 if periodic_x else im - 2), jm - 2
 
     def tmedian(a):
         flat = np.sort(np.asarray(a, dtype=dtype).reshape(-1))
         return flat[(flat.size - 1) // 2]
 
-    dx0, dy0, h0 = tmedian(dx[1:-1, 1:-1]), tmedian(dy[1:-1, 1:-1]), tmedian(h[1:-1, 1:-1])
+    dx0, dy0, h0 = tmedian(dx[rows, 1:-1]), tmedian(dy[rows, 1:-1]), tmedian(h[rows, 1:-1])
     coeff = 4.0 * (dti ** 2) * grav * alpha
-    kx = np.arange(1, ni + 1, dtype=dtype).reshape(-1, 1)
     ky = np.arange(1, nj + 1, dtype=dtype).reshape(1, -1)
-    lam_x = 4.0 * np.square(np.sin(np.pi * kx / (2.0 * (ni + 1)))) / (dx0 * dx0 + 1e-30)
+    if periodic_x:
+        kx = np.arange(0, ni, dtype=dtype).reshape(-1, 1)
+        lam_x = 4.0 * np.square(np.sin(np.pi * kx / ni)) / (dx0 * dx0 + 1e-30)
+    else:
+        kx = np.arange(1, ni + 1, dtype=dtype).reshape(-1, 1)
+        lam_x = 4.0 * np.square(np.sin(np.pi * kx / (2.0 * (ni + 1)))) / (dx0 * dx0 + 1e-30)
     lam_y = 4.0 * np.square(np.sin(np.pi * ky / (2.0 * (nj + 1)))) / (dy0 * dy0 + 1e-30)
     inv_eigs = (1.0 / (1.0 + coeff * h0 * (lam_x + lam_y))).astype(dtype)
 
@@ -163,7 +188,28 @@ def spectral_setup(dx, dy, h, dti, grav, alpha, dtype=np.float32):
         k = np.arange(1, n + 1, dtype=np.float64)
         return (2.0 * np.sin(np.pi * np.outer(k, k) / (n + 1))).astype(dtype)
 
-    return sine(ni), sine(nj), np.ascontiguousarray(inv_eigs)
+    sx = hartley(ni, dtype) if periodic_x else sine(ni)
+    return sx, sine(nj), np.ascontiguousarray(inv_eigs)
+
+
+def hartley(n, dtype=np.float32):
+    """The n x n Hartley matrix cas(2 pi k m / n) = cos + sin (symmetric,
+    its square is n I)."""
+    k = np.arange(n, dtype=np.float64)
+    t = 2.0 * np.pi * np.outer(k, k) / n
+    return (np.cos(t) + np.sin(t)).astype(dtype)
+
+
+def fill_flat(buf, arr):
+    """Write arr row-major into the first arr.size elements of the flat
+    buffer buf (numpy array or torch tensor): the periodic-x preconditioner
+    arrays are smaller than the workspace planes sized for the interior."""
+    n = int(np.asarray(arr).size)
+    if hasattr(buf, "view") and not isinstance(buf, np.ndarray):
+        import torch
+        buf.view(-1)[:n].copy_(torch.from_numpy(np.ascontiguousarray(arr).reshape(-1)))
+    else:
+        buf.reshape(-1)[:n] = np.asarray(arr).reshape(-1)
 
 
 def tide_planes(im, jm, tide_i, tide_j, amp, phase):

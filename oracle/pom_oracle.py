@@ -541,6 +541,59 @@ def _zero_ring(a):
     a[:, -1] = 0.0
 
 
+# ---------------------------------------------------------------------------
+# periodic-x halo (no counterpart in the reference, whose only lateral
+# boundaries are walls and open edges)
+# ---------------------------------------------------------------------------
+
+# per-edge open-boundary arrays and the 1-D vertical grid: not planes of the grid
+_NOT_PLANES = frozenset(("z", "zz", "dz", "dzz", "ele", "elw", "eln", "els", "uabe", "uabw", "vabn", "vabs",
+                         "tbe", "sbe", "tbw", "sbw", "tbn", "sbn", "tbs", "sbs"))
+
+
+def wrap_x(a):
+    """Halo columns of a periodic-x plane (2-D or 3-D, i first), two on
+    each side: columns 0, 1 are copies of im-4, im-3 and columns im-2,
+    im-1 of 2, 3, so the unique columns are 2..im-3 (period im-4).  Two
+    columns because the reference's operators compute some intermediates
+    (advct's x-fluxes, the curvature term of advx) only from column 1 or
+    2 on: with two halo columns every unique column is computed exactly as
+    an interior column of a wider basin.  A u-point column i is the west
+    face of cell i, so the same copy serves every staggering."""
+    im = a.shape[0]
+    a[0] = a[im - 4]
+    a[1] = a[im - 3]
+    a[im - 2] = a[2]
+    a[im - 1] = a[3]
+
+
+def periodic_fill(S, P, *extra):
+    """The periodic-x halo fill after a phase of the step: every plane of
+    the state (and the phase's extra planes) gets wrap_x.  Nothing when
+    the core is not periodic in x."""
+    if not getattr(P, "periodic_x", False):
+        return
+    im, jm = P.im, P.jm
+    for name, a in S.items():
+        if name in _NOT_PLANES or not isinstance(a, np.ndarray) or a.ndim not in (2, 3):
+            continue
+        if a.shape[:2] == (im, jm):
+            wrap_x(a)
+    for a in extra:
+        wrap_x(a)
+
+
+def _pcg_ring(a, periodic):
+    """The ring of a PCG vector: zero (the Dirichlet ring), or with
+    periodic x zero on the j walls and the halo columns wrapped."""
+    if not periodic:
+        _zero_ring(a)
+        return
+    a[:, 0] = 0.0
+    a[:, -1] = 0.0
+    wrap_x(a)
+
+
 def bcond_implicit(S, P, idx, F):
     """Closed-basin boundary policy of the implicit core.
 
@@ -1265,14 +1318,27 @@ def dst1_matrix(n, dtype=np.float64):
     return (2.0 * np.sin(np.pi * np.outer(k, k) / (n + 1))).astype(dtype)
 
 
+def hartley_matrix(n):
+    """H[k, m] = cas(2 pi k m / n) = cos + sin: symmetric, H H = n I, and
+    H C H = n diag(lambda) for a symmetric circulant C (the periodic second
+    difference: lambda_k = 4 sin^2(pi k / n)).  No counterpart in the
+    reference, which has no periodic boundary."""
+    k = np.arange(n, dtype=np.float64)
+    t = 2.0 * np.pi * np.outer(k, k) / n
+    return np.cos(t) + np.sin(t)
+
+
 def spectral_cache(S, P, C):
     """Restates ``implicit_p0_fixed/core.py:730-760`` (median spacings and
     depth of the interior, eigenvalues of the constant-coefficient
-    operator)."""
+    operator).  With ``P.periodic_x`` the rows are the unique columns
+    2..im-3 and the x transform is the Hartley matrix of the period (its
+    eigenvalues 4 sin^2(pi k / n) / dx^2, scale n * 2(nj+1))."""
     dx, dy, h = S["dx"], S["dy"], S["h"]
     im, jm = dx.shape
-    i, j = slice(1, im - 1), slice(1, jm - 1)
-    ni, nj = im - 2, jm - 2
+    periodic = bool(getattr(P, "periodic_x", False))
+    i, j = (slice(2, im - 2) if periodic else slice(1, im - 1)), slice(1, jm - 1)
+    ni, nj = (im - 4 if periodic else im - 2), jm - 2
     dt_ = dx.dtype
 
     def tmedian(a):
@@ -1281,20 +1347,26 @@ def spectral_cache(S, P, C):
         return flat[(flat.size - 1) // 2]
 
     dx0, dy0, h0 = tmedian(dx[i, j]), tmedian(dy[i, j]), tmedian(h[i, j])
-    kx = np.arange(1, ni + 1, dtype=dt_).reshape(-1, 1)
     ky = np.arange(1, nj + 1, dtype=dt_).reshape(1, -1)
-    lam_x = 4.0 * np.square(np.sin(np.pi * kx / (2.0 * (ni + 1)))) / (dx0 * dx0 + 1e-30)
+    if periodic:
+        kx = np.arange(0, ni, dtype=dt_).reshape(-1, 1)
+        lam_x = 4.0 * np.square(np.sin(np.pi * kx / ni)) / (dx0 * dx0 + 1e-30)
+    else:
+        kx = np.arange(1, ni + 1, dtype=dt_).reshape(-1, 1)
+        lam_x = 4.0 * np.square(np.sin(np.pi * kx / (2.0 * (ni + 1)))) / (dx0 * dx0 + 1e-30)
     lam_y = 4.0 * np.square(np.sin(np.pi * ky / (2.0 * (nj + 1)))) / (dy0 * dy0 + 1e-30)
     inv_eigs = 1.0 / (1.0 + C["coeff"] * h0 * (lam_x + lam_y))
-    return dict(inv_eigs=inv_eigs.astype(dt_), inverse_scale=4.0 * (ni + 1) * (nj + 1),
-                sx=dst1_matrix(ni), sy=dst1_matrix(nj))
+    sx = hartley_matrix(ni) if periodic else dst1_matrix(ni)
+    scale = 2.0 * ni * (nj + 1) if periodic else 4.0 * (ni + 1) * (nj + 1)
+    return dict(inv_eigs=inv_eigs.astype(dt_), inverse_scale=scale, sx=sx, sy=dst1_matrix(nj), rows=i)
 
 
 def spectral_apply(r, SC):
-    """z = DST(DST(r_int) * inv_eigs) / (4(ni+1)(nj+1)) on the interior.
+    """z = DST(DST(r_int) * inv_eigs) / (4(ni+1)(nj+1)) on the interior
+    (the rows of ``SC['rows']``; Hartley along a periodic x).
     Restates ``implicit_p0_fixed/core.py:762-773``."""
     im, jm = r.shape
-    i, j = slice(1, im - 1), slice(1, jm - 1)
+    i, j = SC.get("rows", slice(1, im - 1)), slice(1, jm - 1)
     dt_ = r.dtype
     x = r[i, j].astype(np.float64)
     coef = (SC["sx"] @ x @ SC["sy"]).astype(dt_)
@@ -1305,22 +1377,28 @@ def spectral_apply(r, SC):
     return z
 
 
-def pcg_solve(rhs, d, x0, S, P, C, SC, max_iter, tol, rel_tol, precond, dot_dtype=np.float64):
+def pcg_solve(rhs, d, x0, S, P, C, SC, max_iter, tol, rel_tol, precond, dot_dtype=np.float64, periodic=False):
     """Preconditioned CG for the implicit free surface (Dirichlet ring).
 
     Restates ``implicit_p0_fixed/core.py:460-589`` (non-graph branch): stop
     when rs <= tol^2, rs <= rel_tol^2*max(rs0, 1e-30) or rs <= 1e-30.  Dot
     products are accumulated in ``dot_dtype`` (float64 here; the reference's
-    are float32).  Returns (x, iterations).
+    are float32).  With ``periodic`` (periodic x) the ring of the iterated
+    vectors is wrapped in i instead of zeroed (``_pcg_ring``), which makes
+    the operator periodic; the unknowns are then the unique columns
+    2..im-3 (the dot products run over them only).  Returns (x,
+    iterations).
     """
     im, jm = rhs.shape
     I, J = slice(1, im - 1), slice(1, jm - 1)
+    # the unknowns: the interior, or the unique columns 2..im-3 when periodic
+    IU = slice(2, im - 2) if periodic else I
 
     def dot(a, b):
-        return float(np.sum(a[I, J].astype(dot_dtype) * b[I, J].astype(dot_dtype)))
+        return float(np.sum(a[IU, J].astype(dot_dtype) * b[IU, J].astype(dot_dtype)))
 
     x = x0.copy()
-    _zero_ring(x)
+    _pcg_ring(x, periodic)
     rw = rhs.copy()
     _zero_ring(rw)
     ap = elliptic_apply(x, d, C)
@@ -1339,12 +1417,12 @@ def pcg_solve(rhs, d, x0, S, P, C, SC, max_iter, tol, rel_tol, precond, dot_dtyp
     its = 0
     dt_ = rhs.dtype
     for it in range(1, max_iter + 1):
-        _zero_ring(p)
+        _pcg_ring(p, periodic)
         ap = elliptic_apply(p, d, C)
         denom = dot(p, ap)
         alpha = rho_old / (denom + 1e-30)
         x = x + np.asarray(alpha, dtype=dt_) * p
-        _zero_ring(x)
+        _pcg_ring(x, periodic)
         r = r - np.asarray(alpha, dtype=dt_) * ap
         rs = dot(r, r)
         its = it
@@ -1358,9 +1436,9 @@ def pcg_solve(rhs, d, x0, S, P, C, SC, max_iter, tol, rel_tol, precond, dot_dtyp
         rho_new = dot(r, z)
         beta = rho_new / (rho_old + 1e-30)
         p = p * np.asarray(beta, dtype=dt_) + z
-        _zero_ring(p)
+        _pcg_ring(p, periodic)
         rho_old = rho_new
-    _zero_ring(x)
+    _pcg_ring(x, periodic)
     return x, its
 
 
@@ -1734,6 +1812,12 @@ def step_implicit(S, P, C=None, SC=None, dot_dtype=np.float64):
     (``boundary/closed_basin.py``, ``forcing/surface.py``,
     ``numerics/double_gyre.py``).  ``S['_eta_prev']`` (optional) plays the
     role of ``_eta_prev_solution``.  Returns the PCG iteration count.
+
+    With ``P.periodic_x`` the x edges are periodic instead of walls (the
+    reference has no periodic boundary): after each phase of the CUDA step
+    (A1, A2, A3, the η-solve, I5, B1-B9; the comments below name them)
+    every plane gets the halo fill ``periodic_fill``, and the η-solve's
+    operator wraps in x (``pcg_solve(periodic=True)``).
     """
     im, jm, kb = P.im, P.jm, P.kb
     kbm1 = kb - 1
@@ -1754,9 +1838,11 @@ def step_implicit(S, P, C=None, SC=None, dot_dtype=np.float64):
     surface_fluxes(S, P)
     curv, advx, advy = advct(S, P)
     S["curv"], S["advx"], S["advy"] = curv, advx, advy
+    periodic_fill(S, P)  # A1
     S["rho"], S["drhox"], S["drhoy"] = baropg(S, P)
     S["aam"] = smagorinsky_implicit(S, P)
     S["adx2d"], S["ady2d"], S["drx2d"], S["dry2d"], S["aam2d"] = vertical_means(S, P)
+    periodic_fill(S, P)  # A2
     fluxua, fluxva, tps = S["fluxua"].copy(), S["fluxva"].copy(), S["tps"].copy()
     S["advua"], S["advva"] = advave(S, P, fluxua, fluxva, tps)
     S["fluxua"], S["fluxva"], S["tps"] = fluxua, fluxva, tps
@@ -1776,16 +1862,19 @@ def step_implicit(S, P, C=None, SC=None, dot_dtype=np.float64):
     F = {"uaf": us, "vaf": vs}
     bcond_implicit(S, P, 2, F)
     us, vs = F["uaf"], F["vaf"]
+    periodic_fill(S, P, us, vs)  # A3 (den_u, den_v: interior arrays, pointwise)
     S["fluxua"], S["fluxva"], rhs = barotropic_rhs(S, P, us, vs)
     prev = S.get("_eta_prev")
     x0 = 2.0 * S["elf"] - prev if prev is not None else S["elf"]
     elf, its = pcg_solve(rhs, S["d"], x0, S, P, C, SC, int(P.eta_solver_max_iter), float(P.eta_solver_tol),
-                         float(P.eta_solver_rel_tol), P.eta_solver_preconditioner, dot_dtype=dot_dtype)
+                         float(P.eta_solver_rel_tol), P.eta_solver_preconditioner, dot_dtype=dot_dtype,
+                         periodic=bool(getattr(P, "periodic_x", False)))
     elf = barotropic_shapiro(elf, S, float(P.barotropic_shapiro))
     F = {"elf": elf}
     bcond_implicit(S, P, 1, F)
     S["elf"] = F["elf"]
     S["d"] = S["h"] + S["elf"]
+    periodic_fill(S, P)  # the η-solve
     ui, vi = barotropic_corrector(S, P, us, vs, den_u, den_v)
     uaf, vaf = S["uaf"].copy(), S["vaf"].copy()
     uaf[1:im - 1, 1:jm - 1] = ui
@@ -1815,16 +1904,20 @@ def step_implicit(S, P, C=None, SC=None, dot_dtype=np.float64):
         utf[1:im, :] = c * (S["uab"][1:im, :] * (d_baro[1:im, :] + d_baro[0:im - 1, :]) + S["ua"][1:im, :] * (d[1:im, :] + d[0:im - 1, :]))
         vtf[:, 1:jm] = c * (S["vab"][:, 1:jm] * (d_baro[:, 1:jm] + d_baro[:, 0:jm - 1]) + S["va"][:, 1:jm] * (d[:, 1:jm] + d[:, 0:jm - 1]))
         S["utf"], S["vtf"] = utf, vtf
+    periodic_fill(S, P)  # I5
 
     if ok and (iint != 1 or P.time0 != 0.0) and P.mode != 2:
         _barotropic_fix(S, P)
+        periodic_fill(S, P)  # B1
         S["w"] = vertvl(S, P)
         F = {"w": S["w"]}
         bcond_implicit(S, P, 5, F)
         S["w"] = F["w"]
+        periodic_fill(S, P)  # B2A
         uf = advq(S, P, S["q2b"], S["q2"], np.zeros_like(S["u"]))
         vf = advq(S, P, S["q2lb"], S["q2l"], np.zeros_like(S["u"]))
         S["uf"], S["vf"] = uf, vf
+        periodic_fill(S, P)  # B2B
         if getattr(P, "profq_form", "production") == "pom08":
             R = profq_pom08(S, P, uf, vf)
             S["q2b"], S["q2lb"] = R["q2b"], R["q2lb"]
@@ -1832,9 +1925,12 @@ def step_implicit(S, P, C=None, SC=None, dot_dtype=np.float64):
             R = profq(S, P, uf, vf, implicit_variant=True)
         S["l"], S["kq"], S["km"], S["kh"] = R["l"], R["kq"], R["km"], R["kh"]
         S["dtef"] = R["cc"]
-        F = {"uf": R["uf"], "vf": R["vf"]}
+        S["uf"], S["vf"] = R["uf"], R["vf"]
+        periodic_fill(S, P)  # B3
+        F = {"uf": S["uf"], "vf": S["vf"]}
         bcond_implicit(S, P, 6, F)
         S["uf"], S["vf"] = F["uf"], F["vf"]
+        periodic_fill(S, P)  # B4
         q2 = S["q2"] + 0.5 * P.smoth * (S["uf"] + S["q2b"] - 2.0 * S["q2"])
         q2l = S["q2l"] + 0.5 * P.smoth * (S["vf"] + S["q2lb"] - 2.0 * S["q2l"])
         S["q2b"], S["q2"], S["q2lb"], S["q2l"] = q2, S["uf"].copy(), q2l, S["vf"].copy()
@@ -1845,11 +1941,13 @@ def step_implicit(S, P, C=None, SC=None, dot_dtype=np.float64):
         if P.mode != 4:
             S["tb"], S["t"], uf = advt1(S, P, S["tb"], S["t"], S["tclim"])
             S["sb"], S["s"], vf = advt1(S, P, S["sb"], S["s"], S["sclim"])
+            periodic_fill(S, P, uf, vf)  # B5
             uf, _ = proft(uf, S["wtsurf"], S["tsurf"], P.nbct, S["h"], S["etf"], P.dti2, S["dz"], S["dzz"],
                           S["swrad"], P.ntp, S["kh"], P.umol, S["z"])
             vf, dh = proft(vf, S["wssurf"], S["ssurf"], P.nbcs, S["h"], S["etf"], P.dti2, S["dz"], S["dzz"],
                            S["swrad"], P.ntp, S["kh"], P.umol, S["z"])
             S["tps"] = dh
+            periodic_fill(S, P, uf, vf)  # B6
             F = {"uf": uf, "vf": vf}
             bcond_implicit(S, P, 4, F)
             uf, vf = F["uf"], F["vf"]
@@ -1865,6 +1963,7 @@ def step_implicit(S, P, C=None, SC=None, dot_dtype=np.float64):
             S["uf"], S["vf"] = uf, vf
             S["tb"], S["t"], S["sb"], S["s"] = t, uf.copy(), s, vf.copy()
             S["rho"] = dens(S, P)
+            periodic_fill(S, P)  # B7
         S["uf"] = advu(S, P)
         S["vf"] = advv(S, P)
         S["uf"], S["wubot"], _ = profuv(S, P, "u")
@@ -1872,6 +1971,7 @@ def step_implicit(S, P, C=None, SC=None, dot_dtype=np.float64):
         F = {"uf": S["uf"], "vf": S["vf"]}
         bcond_implicit(S, P, 3, F)
         S["uf"], S["vf"] = F["uf"], F["vf"]
+        periodic_fill(S, P)  # B8
         _internal_velocity_filter(S, P, shapiro=float(P.velocity_shapiro))
 
     S["egb"] = S["egf"].copy()
@@ -1881,6 +1981,7 @@ def step_implicit(S, P, C=None, SC=None, dot_dtype=np.float64):
     S["utb"] = S["utf"].copy()
     S["vtb"] = S["vtf"].copy()
     S["vfluxb"] = S["vfluxf"].copy()
+    periodic_fill(S, P)  # B9
     if vamax > P.vmaxl:
         raise VmaxExceeded(f"Barotropic velocity {vamax} exceeds limit {P.vmaxl} at time {P.time}")
     return its

@@ -45,9 +45,25 @@ void a1(const Ctx &c) {
   });
 }
 
+// the periodic-x halo copy after a phase (k_wrap_x): every plane of the
+// state and the workspace planes a later phase reads
+void wrap_x(const Ctx &c) {
+  if (!c.k.periodic_x) return;
+  auto copy = [&](float *a, int depth) {
+    const size_t col = (size_t)c.jm * depth;
+    const int dst[4] = {0, 1, c.im - 2, c.im - 1}, src[4] = {c.im - 4, c.im - 3, 2, 3};
+    for (int w = 0; w < 4; ++w) std::memcpy(a + dst[w] * col, a + src[w] * col, col * sizeof(float));
+  };
+  for (int f = NPOM_F_h; f <= NPOM_F_north_e; ++f) copy(c.F[f], 1);
+  for (int f = NPOM_F_u; f <= NPOM_F_curv; ++f) copy(c.F[f], c.kb);
+  for (int f = NPOM_F_el; f <= NPOM_F_ssurf; ++f) copy(c.F[f], 1);
+  for (int w : {NPOM_W_us, NPOM_W_vs, NPOM_W_den_u, NPOM_W_den_v, NPOM_W_d_baro}) copy(c.W[w], 1);
+}
+
+// dot product over the unknowns of the free-surface solve
 double dot_int(const Ctx &c, const float *a, const float *b) {
   double s = 0.0;
-  for (int i = 1; i < c.im - 1; ++i)
+  for (int i = pcg_i0(c); i < c.im - pcg_i0(c); ++i)
     for (int j = 1; j < c.jm - 1; ++j) {
       size_t o = NPOM_I2(c, i, j);
       s += (double)a[o] * (double)b[o];
@@ -56,11 +72,14 @@ double dot_int(const Ctx &c, const float *a, const float *b) {
 }
 
 void precondition(const Ctx &c) {
-  const int ni = c.im - 2, nj = c.jm - 2;
+  int ni = c.im - 2;
+  const int nj = c.jm - 2;
   float *zv = c.W[NPOM_W_zv];
   const float *r = c.W[NPOM_W_r];
   if (c.k.eta_precond == NPOM_PRECOND_SPECTRAL) {
     float *t1 = c.W[NPOM_W_t1], *t2 = c.W[NPOM_W_t2];
+    const int i0 = pcg_i0(c);
+    ni = c.im - 2 * i0;
     for (int a = 0; a < ni; ++a)
       for (int b = 0; b < nj; ++b) t1[(size_t)a * nj + b] = dst_stage_i(c, r, true, a, b);
     for (int a = 0; a < ni; ++a)
@@ -69,9 +88,9 @@ void precondition(const Ctx &c) {
     for (int a = 0; a < ni; ++a)
       for (int b = 0; b < nj; ++b) t1[(size_t)a * nj + b] = dst_stage_i(c, t2, false, a, b);
     for (int a = 0; a < ni; ++a)
-      for (int b = 0; b < nj; ++b) zv[NPOM_I2(c, a + 1, b + 1)] = dst_stage_j(c, t1, a, b) / c.k.inverse_scale;
+      for (int b = 0; b < nj; ++b) zv[NPOM_I2(c, a + i0, b + 1)] = dst_stage_j(c, t1, a, b) / c.k.inverse_scale;
   } else {
-    for (int i = 1; i < c.im - 1; ++i)
+    for (int i = pcg_i0(c); i < c.im - pcg_i0(c); ++i)
       for (int j = 1; j < c.jm - 1; ++j) {
         size_t o = NPOM_I2(c, i, j);
         zv[o] = r[o] / (c.W[NPOM_W_diag][o] + 1e-30f);
@@ -80,7 +99,7 @@ void precondition(const Ctx &c) {
 }
 
 void pcg(const Ctx &c, int step, int with_rhs, int with_post) {
-  const int im = c.im, jm = c.jm;
+  const int im = c.im, jm = c.jm, i0 = pcg_i0(c);
   float *x = c.W[NPOM_W_x], *r = c.W[NPOM_W_r], *p = c.W[NPOM_W_p], *zv = c.W[NPOM_W_zv];
   float *ap = c.W[NPOM_W_ap], *rhs = c.W[NPOM_W_rhs];
   each_cell(c, [&](int i, int j) {
@@ -99,7 +118,7 @@ void pcg(const Ctx &c, int step, int with_rhs, int with_post) {
     x[q] = in ? c.F[NPOM_F_elf][q] : 0.0f;
     if (!in) r[q] = p[q] = zv[q] = ap[q] = 0.0f;
   });
-  for (int i = 1; i < im - 1; ++i)
+  for (int i = i0; i < im - i0; ++i)
     for (int j = 1; j < jm - 1; ++j) {
       size_t o = NPOM_I2(c, i, j);
       r[o] = rhs[o] - elliptic_apply_cell(c, x, i, j);
@@ -108,18 +127,18 @@ void pcg(const Ctx &c, int step, int with_rhs, int with_post) {
   double rs0 = dot_int(c, r, r);
   precondition(c);
   double rho_old = dot_int(c, r, zv);
-  for (int i = 1; i < im - 1; ++i)
+  for (int i = i0; i < im - i0; ++i)
     for (int j = 1; j < jm - 1; ++j) p[NPOM_I2(c, i, j)] = zv[NPOM_I2(c, i, j)];
   const double tol_sq = c.k.eta_tol * c.k.eta_tol;
   const double rel_sq = c.k.eta_rel_tol * c.k.eta_rel_tol * (rs0 > 1e-30 ? rs0 : 1e-30);
   int its = 0;
   bool conv = false;
   for (int it = 1; it <= c.k.eta_max_iter; ++it) {
-    for (int i = 1; i < im - 1; ++i)
+    for (int i = i0; i < im - i0; ++i)
       for (int j = 1; j < jm - 1; ++j) ap[NPOM_I2(c, i, j)] = elliptic_apply_cell(c, p, i, j);
     double denom = dot_int(c, p, ap);
     float alpha = (float)(rho_old / (denom + 1e-30));
-    for (int i = 1; i < im - 1; ++i)
+    for (int i = i0; i < im - i0; ++i)
       for (int j = 1; j < jm - 1; ++j) {
         size_t o = NPOM_I2(c, i, j);
         x[o] = x[o] + alpha * p[o];
@@ -134,7 +153,7 @@ void pcg(const Ctx &c, int step, int with_rhs, int with_post) {
     precondition(c);
     double rho_new = dot_int(c, r, zv);
     float beta = (float)(rho_new / (rho_old + 1e-30));
-    for (int i = 1; i < im - 1; ++i)
+    for (int i = i0; i < im - i0; ++i)
       for (int j = 1; j < jm - 1; ++j) {
         size_t o = NPOM_I2(c, i, j);
         p[o] = p[o] * beta + zv[o];
@@ -144,7 +163,10 @@ void pcg(const Ctx &c, int step, int with_rhs, int with_post) {
   c.cg_iters[step] = its;
   if (!conv) *c.status |= NPOM_DEV_PCG_MAXIT;
   if (!with_post) {
-    each_cell(c, [&](int i, int j) { P2(elf, i, j) = x[NPOM_I2(c, i, j)]; });
+    each_cell(c, [&](int i, int j) {
+      const int iw = !c.k.periodic_x ? i : i < 2 ? i + im - 4 : (i > im - 3 ? i - (im - 4) : i);
+      P2(elf, i, j) = x[NPOM_I2(c, iw, j)];
+    });
     return;
   }
   each_cell(c, [&](int i, int j) {
@@ -152,7 +174,8 @@ void pcg(const Ctx &c, int step, int with_rhs, int with_post) {
     float e = 0.0f;
     if (interior(c, i, j)) {
       float x0 = x[q];
-      float sm = x0 + c.k.bshap_q * (x[q + jm] + x[q - jm] + x[q + 1] + x[q - 1] - 4.0f * x0);
+      const size_t qe = NPOM_I2(c, pcg_east(c, i), j), qw = NPOM_I2(c, pcg_west(c, i), j);
+      float sm = x0 + c.k.bshap_q * (x[qe] + x[qw] + x[q + 1] + x[q - 1] - 4.0f * x0);
       float fsm = F2(fsm, i, j);
       e = (sm * fsm) * fsm;
     }
@@ -228,6 +251,7 @@ void run_phase(const Ctx &c, const npom_params *p, int phase) {
       break;
     case 14: each_cell(c, [&](int i, int j) { phase_b9_column(c, i, j); }); break;
   }
+  wrap_x(c);
 }
 
 // the implicit free-surface phase of the recomputation: PCG without its post
@@ -445,6 +469,7 @@ int emul_steps(const npom_params *p, float *const *fields, const npom_workspace 
     run_phase(c, p, 2);
     if (p->core == NPOM_CORE_IMPLICIT) {
       pcg(c, n, 1, 1);
+      wrap_x(c);
       run_phase(c, p, 4);
     } else {
       subcycle(c);

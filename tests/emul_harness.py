@@ -75,10 +75,9 @@ class EmulCore:
         self.params = state.make_params(s, im, jm, kb, core)
         if core != "explicit":
             sx, sy, ie = state.spectral_setup(self.F["dx"], self.F["dy"], self.F["h"], s["dti"], s["grav"],
-                                              s["alpha"])
-            self.W["sx"][...] = sx
-            self.W["sy"][...] = sy
-            self.W["inv_eigs"][...] = ie
+                                              s["alpha"], periodic_x=bool(s.get("periodic_x", False)))
+            for n, a in (("sx", sx), ("sy", sy), ("inv_eigs", ie)):
+                state.fill_flat(self.W[n], a)
         self.partials = np.zeros(4 * _abi.MAX_COOP_BLOCKS, np.float64)
         self.sync = np.zeros(4, np.uint32)
         self.status = np.zeros(1, np.uint32)
