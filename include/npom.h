@@ -167,7 +167,15 @@ enum { NPOM_PROFQ_PRODUCTION = 0, NPOM_PROFQ_POM08 = 1 };
  * of u and of T/S (with the exterior profile on inflow), 1e-10 turbulence
  * edges; the north and south edges are walls.  Forward only (the reference
  * refuses gradients through its case policies). */
-enum { NPOM_OBC_NATIVE = 0, NPOM_OBC_SEAMOUNT = 1, NPOM_OBC_COASTAL = 2 };
+enum { NPOM_OBC_NATIVE = 0, NPOM_OBC_SEAMOUNT = 1, NPOM_OBC_COASTAL = 2, NPOM_OBC_JZB = 3 };
+/* JZB: the explicit core with the Jiaozhou Bay tide policy
+ * (cores/case_adapters/jzb_boundary.py, jzb_compat.py and the coastal
+ * policy's step copies): the coastal policy's machinery (tide planes, no
+ * 1e-8 in the bottom-drag speed, cbc after the substeps) with the bay's
+ * M2 speed, the tide times fsm at its cells and the edges copying the
+ * adjacent cell (bcond 1); Sommerfeld radiation of the transports on all
+ * four edges (bcond 2) and of the internal velocities (bcond 3), both
+ * ramped; cbc from depths >= 0.05 m with z0b 0.01 m.  Forward only. */
 /* COASTAL: the explicit core with the coastal tide policy
  * (cores/case_adapters/coastal_boundary.py:9-30, coastal_compat.py and the
  * policy's step copies): the tidal elevation

@@ -36,7 +36,7 @@ FIELDS_3D = tuple("u ub uf v vb vf w t tb s sb rho rmean tclim sclim q2 q2b q2l 
 CORE_EXPLICIT, CORE_IMPLICIT = 0, 1
 PRECOND_JACOBI, PRECOND_SPECTRAL = 0, 1
 PROFQ_PRODUCTION, PROFQ_POM08 = 0, 1
-OBC_NATIVE, OBC_SEAMOUNT, OBC_COASTAL = 0, 1, 2
+OBC_NATIVE, OBC_SEAMOUNT, OBC_COASTAL, OBC_JZB = 0, 1, 2, 3
 DEV_VMAX, DEV_TIMEOUT, DEV_PCG_MAXIT, DEV_NONFINITE = 0x1, 0x2, 0x4, 0x8
 MAX_COOP_BLOCKS = 1024
 

@@ -469,3 +469,61 @@ def tidal_inlet(im=40, jm=30, kb=5, dte=1.0, isplit=10, dx=500.0, lat=30.0, ampl
     rows = np.arange(1, jm - 1)
     amp = amplitude * (0.8 + 0.2 * rows / max(jm - 2, 1))
     return coastal_policy(A, s, np.full(rows.shape, im - 2), rows, amp, 2.0 * rows)
+
+
+def jzb_policy(A, s, tide_i, tide_j, tide_amp, tide_phase):
+    """The Jiaozhou Bay tide policy's set-up on a state
+    (cores/case_adapters/jzb_boundary.py:200-215 and jzb_compat.py:30-70):
+    the tide table (0-based cells, amplitude in m, phase in degrees), rf = 1,
+    alpha and smoth of the explicit core, the bay's settings (mode 4, a
+    3-day ramp, horcon 0.1, hmax 60 m, tprni 0.2, umol 2e-5), the POM08-WAD
+    closure (zsh = 0.01 m) and the bay's boundary (``obc_form``)."""
+    A = dict(A)
+    A["tide_i"] = np.asarray(tide_i, F32)
+    A["tide_j"] = np.asarray(tide_j, F32)
+    A["tide_amp"] = np.asarray(tide_amp, F32)
+    A["tide_phase"] = np.asarray(tide_phase, F32)
+    A["period"] = np.asarray(F32(3.0))
+    s = dict(s, rfe=1.0, rfw=1.0, rfn=1.0, rfs=1.0, alpha=0.225, smoth=0.1, profq_form="pom08", zsh=0.01,
+             obc_form="jzb", mode=4, lramp=True, period=3.0, horcon=0.1, hmax=60.0, tprni=0.2, umol=2.0e-5)
+    return A, s
+
+
+def bay(im=40, jm=30, kb=16, dte=1.0, isplit=10, dx=500.0, lat=36.0, amplitude=1.0):
+    """The geometry the Jiaozhou Bay policy serves (registered at 312x213x17,
+    dtE/dtI = 1/10 s, from data that is not in the repository): a bay closed
+    on the west, east and north, open to the sea on the south edge, depth 2 m
+    at the head growing to 40 m at the mouth, T = 15 degC, S = 31 psu + 1 psu
+    per 10 m, f-plane at ``lat``, no wind, horizontal viscosity 50 m^2/s at
+    rest; with ``jzb_policy`` applied and a tide table of the registered
+    layout: every interior cell of the row next to the open edge, with
+    amplitude ``amplitude`` scaled by 0.8-1.0 along the row and a phase of
+    1.5 degrees per column."""
+    core = "explicit"
+    s = state.default_scalars(core)
+    s.update(dte=dte, isplit=isplit, hmax=60.0, aam_init=50.0)
+    state.derived_time(s)
+    A = _zeros(im, jm, kb)
+    A["dx"][:] = dx
+    A["dy"][:] = dx
+    A["north_e"][:] = lat
+    A["cor"][:] = F32(2.0 * 7.2921e-5 * math.sin(math.radians(lat)))
+    y = np.arange(jm, dtype=np.float64) / (jm - 1)
+    h = np.broadcast_to((40.0 - 38.0 * y)[None, :], (im, jm)).astype(F32).copy()
+    h[0, :] = 1.0
+    h[-1, :] = 1.0
+    h[:, -1] = 1.0
+    A["h"] = h
+    A["z"], A["zz"], A["dz"], A["dzz"] = sigma_levels(kb)
+    areas_masks(A)
+    depths = (A["z"][None, None, :] * A["h"][:, :, None]).astype(F32)
+    A["tb"][:] = F32(15.0)
+    A["sb"] = (F32(31.0) - F32(0.1) * depths).astype(F32)
+    A["tclim"] = A["tb"].copy()
+    A["sclim"] = A["sb"].copy()
+    A["rho"] = dens_np(A["tb"], A["sb"], A["h"], A["zz"], A["fsm"], s)
+    A["rmean"] = A["rho"].copy()
+    A, s = finish_initialization(A, s, core)
+    cols = np.arange(1, im - 1)
+    amp = amplitude * (0.8 + 0.2 * cols / max(im - 2, 1))
+    return jzb_policy(A, s, cols, np.full(cols.shape, 1), amp, 1.5 * cols)

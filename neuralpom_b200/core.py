@@ -127,7 +127,7 @@ class B200Core:
             s.cg_iters = base + 8 * 4
             ws["struct"] = s
             self._ws = ws
-        if str(getattr(self, "obc_form", "native")).lower() == "coastal" and "tide" not in self._ws:
+        if str(getattr(self, "obc_form", "native")).lower() in ("coastal", "jzb") and "tide" not in self._ws:
             # the coastal tide policy's table as three planes (flag, amplitude, phase)
             planes = state.tide_planes(im, jm, *(state.host_array(getattr(self, n))
                                                  for n in ("tide_i", "tide_j", "tide_amp", "tide_phase")))

@@ -48,11 +48,13 @@ struct Consts {
   int profq_pom08;     // PROFQ in the POM08-WAD form
   float kappa_zsh;     // POM08-WAD: kappa * zsh (folded in double)
   int obc_seamount;    // the seamount case policy's boundary (explicit core)
-  int obc_coastal;     // the coastal tide policy (explicit core)
+  int obc_coastal;     // the coastal tide policy's machinery (explicit core; also set for JZB)
+  int obc_jzb;         // the Jiaozhou Bay tide policy (explicit core)
   int periodic_x;      // periodic x: two halo columns each side, unique columns 2..im-3
   double tide_w;       // tide angular speed, rad/h, as the policy writes it
   double dte_d;        // dte in double (tide time of a substep)
   float zsh_cbc, z0b_cbc, cbcmin, cbcmax;  // coastal policy's drag coefficient
+  float hc_cbc;                           // JZB: the drag law from this depth on
 };
 
 struct Ctx {

@@ -53,14 +53,17 @@ inline Consts make_consts(const npom_params &p) {
   k.profq_pom08 = p.profq_form == NPOM_PROFQ_POM08 ? 1 : 0;
   k.kappa_zsh = (float)(p.kappa * p.zsh);
   k.obc_seamount = p.obc_form == NPOM_OBC_SEAMOUNT ? 1 : 0;
-  k.obc_coastal = p.obc_form == NPOM_OBC_COASTAL ? 1 : 0;
+  k.obc_coastal = (p.obc_form == NPOM_OBC_COASTAL || p.obc_form == NPOM_OBC_JZB) ? 1 : 0;
+  k.obc_jzb = p.obc_form == NPOM_OBC_JZB ? 1 : 0;
   k.periodic_x = p.periodic_x ? 1 : 0;
   // coastal_boundary.py:9-10: (29.03225806451612*3.1416/180) in double
-  k.tide_w = 29.03225806451612 * 3.1416 / 180.0;
+  // the policies' M2 angular speeds (rad/h) as they write them
+  k.tide_w = k.obc_jzb ? 28.98410424 * 3.1416 / 180.0 : 29.03225806451612 * 3.1416 / 180.0;
   k.dte_d = p.dte;
   // coastal_compat.py:4-16
   k.zsh_cbc = 0.01f;
-  k.z0b_cbc = 0.005f;
+  k.z0b_cbc = k.obc_jzb ? 0.01f : 0.005f;
+  k.hc_cbc = 0.05f;
   k.cbcmin = 0.0025f;
   k.cbcmax = 1.0f;
   k.wind_kf = (float)(-(p.wind_tau0 / p.rhoref));
@@ -110,8 +113,9 @@ inline bool check_args(const npom_params *p, float *const *fields, const npom_wo
   if (!ws->partials || !ws->sync || !ws->status || !ws->cg_iters) return false;
   if (p->nadv != 1 && (p->nadv != 2 || !ws->mp3d || p->nitera < 1)) return false;
   if (p->obc_form != NPOM_OBC_NATIVE &&
-      ((p->obc_form != NPOM_OBC_SEAMOUNT && p->obc_form != NPOM_OBC_COASTAL) || p->core != NPOM_CORE_EXPLICIT ||
-       p->im < 6 || p->jm < 6 || (p->obc_form == NPOM_OBC_COASTAL && !ws->tide)))
+      ((p->obc_form != NPOM_OBC_SEAMOUNT && p->obc_form != NPOM_OBC_COASTAL && p->obc_form != NPOM_OBC_JZB) ||
+       p->core != NPOM_CORE_EXPLICIT || p->im < 6 || p->jm < 6 ||
+       ((p->obc_form == NPOM_OBC_COASTAL || p->obc_form == NPOM_OBC_JZB) && !ws->tide)))
     return false;
   if (p->periodic_x &&
       (p->periodic_x != 1 || p->core != NPOM_CORE_IMPLICIT || p->obc_form != NPOM_OBC_NATIVE || p->nadv != 1 ||

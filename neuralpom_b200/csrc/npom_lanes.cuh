@@ -505,7 +505,8 @@ __device__ __forceinline__ void lane_b8(const Ctx &c, int i, int j, int k, bool 
   float uo, vo, wub, wvb, tpsu, tpsv;
   lane_profuv(c, 0, i, j, k, fu, uo, wub, tpsu);
   lane_profuv(c, 1, i, j, k, fv, vo, wvb, tpsv);
-  if (is_explicit(c) && !c.k.obc_seamount) lane_bcond3_explicit(c, i, j, k, uo, vo);
+  if (c.k.obc_jzb) jzb_bcond3_level(c, i, j, k, uo, vo);
+  else if (is_explicit(c) && !c.k.obc_seamount) lane_bcond3_explicit(c, i, j, k, uo, vo);
   if (!st) return;
   P3(uf, i, j, k) = uo;
   P3(vf, i, j, k) = vo;

@@ -312,9 +312,11 @@ NPOM_HD float ext_elf_interior(const Ctx &c, int i, int j) {
 // interior value), then the whole field is masked by fsm.
 NPOM_HD float ext_elf_cell_seamount(const Ctx &c, int i, int j);
 NPOM_HD float ext_elf_cell_coastal(const Ctx &c, int i, int j, int iext);
+NPOM_HD float ext_elf_cell_jzb(const Ctx &c, int i, int j, int iext);
 
 NPOM_HD float ext_elf_cell(const Ctx &c, int i, int j, int iext) {
   if (c.k.obc_seamount) return ext_elf_cell_seamount(c, i, j);
+  if (c.k.obc_jzb) return ext_elf_cell_jzb(c, i, j, iext);
   if (c.k.obc_coastal) return ext_elf_cell_coastal(c, i, j, iext);
   int si = i, sj = j;
   if (si == 0) si = 1;
@@ -353,6 +355,28 @@ NPOM_HD float ext_elf_cell_coastal(const Ctx &c, int i, int j, int iext) {
     raw = c.tide[n2 + o] * cosf(arg - c.tide[2 * n2 + o] * 3.1416f / 180.0f);
   } else {
     raw = interior(c, i, j) ? ext_elf_interior(c, i, j) : F2(elf, i, j);
+  }
+  return raw * F2(fsm, i, j);
+}
+
+// elf after the Jiaozhou Bay policy's bcond 1 (jzb_boundary.py:17-49): at
+// the flagged cells the tide amp cos(w (t / 3600) - phase) times fsm there
+// (t as in the coastal policy, the argument's product formed in double from
+// t / 3600); then the edges copy the adjacent cell (west and east, then
+// south and north, so a corner takes the diagonal interior value) and the
+// whole field is masked.  A tide cell on the ring is overwritten by the
+// copy, so every value comes from the interior cell (si, sj).
+NPOM_HD float ext_elf_cell_jzb(const Ctx &c, int i, int j, int iext) {
+  const int si = i == 0 ? 1 : (i == c.im - 1 ? c.im - 2 : i);
+  const int sj = j == 0 ? 1 : (j == c.jm - 1 ? c.jm - 2 : j);
+  const size_t o = NPOM_I2(c, si, sj), n2 = (size_t)c.im * c.jm;
+  float raw;
+  if (c.tide[o] != 0.0f) {
+    const double sec = c.tide_t0 + c.k.dte_d * (double)(iext - 1);
+    const float arg = (float)(c.k.tide_w * (sec / 3600.0));
+    raw = c.tide[n2 + o] * cosf(arg - c.tide[2 * n2 + o] * 3.1416f / 180.0f) * F2(fsm, si, sj);
+  } else {
+    raw = ext_elf_interior(c, si, sj);
   }
   return raw * F2(fsm, i, j);
 }
@@ -453,6 +477,44 @@ NPOM_HD void bcond2_coastal(const Ctx &c, int i, int j, float &uaf, float &vaf) 
   }
 }
 
+// The Jiaozhou Bay policy's bcond 2 (jzb_boundary.py:51-86): Sommerfeld
+// radiation of the transports, uaf on the east edge (from ua at im-2) and at
+// column 1 (from ua at 2), vaf on the north edge (from va at jm-2) and at
+// row 1 (from va at 2), with the weight dte sqrt(max(g d, 0)) / dx (dy)
+// at the depth cell the policy names, times ramp, wherever that d > 0;
+// there the tangential component on the outer ring is zero.  Reads only
+// ua, va and d, none of which the phase writes; the edge sets do not
+// overlap, so their order does not matter.
+NPOM_HD void bcond2_jzb(const Ctx &c, int i, int j, float &uaf, float &vaf) {
+  const int im = c.im, jm = c.jm;
+  const float g = c.k.grav, dte = (float)c.k.dte_d, ramp = c.ramp;
+  auto gae = [&](int ii, int jj, float len) { return dte * sqrtf(fmaxf_t(g * F2(d, ii, jj), 0.0f)) / len; };
+  if (j >= 1 && j <= jm - 2) {
+    if (i == im - 1 && F2(d, im - 1, j) > 0.0f) {
+      const float w = gae(im - 1, j, F2(dx, im - 1, j));
+      uaf = (w * F2(ua, im - 2, j) + (1.0f - w) * F2(ua, im - 1, j)) * ramp;
+      vaf = 0.0f;
+    }
+    if ((i == 1 || i == 0) && F2(d, 1, j) > 0.0f) {
+      const float w = gae(1, j, F2(dx, 1, j));
+      if (i == 1) uaf = ramp * (w * F2(ua, 2, j) + (1.0f - w) * F2(ua, 1, j));
+      else vaf = 0.0f;
+    }
+  }
+  if (i >= 1 && i <= im - 2) {
+    if (j == jm - 1 && F2(d, i, jm - 1) > 0.0f) {
+      const float w = gae(i, jm - 1, F2(dy, i, jm - 1));
+      vaf = (w * F2(va, i, jm - 2) + (1.0f - w) * F2(va, i, jm - 1)) * ramp;
+      uaf = 0.0f;
+    }
+    if ((j == 1 || j == 0) && F2(d, i, 1) > 0.0f) {
+      const float w = gae(i, 1, F2(dy, i, 1));
+      if (j == 1) vaf = (w * F2(va, i, 2) + (1.0f - w) * F2(va, i, 1)) * ramp;
+      else uaf = 0.0f;
+    }
+  }
+}
+
 // Phase 2: uaf/vaf with bcond 2 and the etf time filter
 // (time_loop.py:326-391).  Returns |vaf| > vmaxl.
 NPOM_HD bool ext_phase2_cell(const Ctx &c, int i, int j, int iext) {
@@ -463,7 +525,9 @@ NPOM_HD bool ext_phase2_cell(const Ctx &c, int i, int j, int iext) {
   // normal/tangential components on the ring, then masks.
   const float ramp = c.ramp, g = c.k.grav;
   auto rad = [&](float hh) { return sqrtf(fmaxf_t(g / fmaxf_t(hh, 1e-8f), 1e-8f)); };
-  if (c.k.obc_coastal) {
+  if (c.k.obc_jzb) {
+    bcond2_jzb(c, i, j, uaf, vaf);
+  } else if (c.k.obc_coastal) {
     bcond2_coastal(c, i, j, uaf, vaf);
   } else if (c.k.obc_seamount) {
     // the seamount policy (seamount_boundary.py:16-19): characteristic
@@ -554,10 +618,14 @@ NPOM_HD void ext_phase3_cell(const Ctx &c, int i, int j, int iext) {
 // land, clipped to [cbcmin, cbcmax].  The policy updates it after every
 // external substep from the new depth; only the last update reaches a
 // reader (the bottom stress of B8), so it runs once after the subcycle.
+// The Jiaozhou Bay policy's law (jzb_compat.py:8-27) also needs d >= 0.05 m
+// and takes z0b = 0.01 m.
 NPOM_HD void cbc_coastal_cell(const Ctx &c, int i, int j) {
-  const float ratio = (c.k.zsh_cbc + (1.0f + F1(zz, c.kb - 2)) * F2(d, i, j)) / c.k.z0b_cbc;
+  const float dd = F2(d, i, j);
+  const bool valid = F2(fsm, i, j) > 0.0f && (!c.k.obc_jzb || dd >= c.k.hc_cbc);
+  const float ratio = (c.k.zsh_cbc + (1.0f + F1(zz, c.kb - 2)) * (valid ? dd : 1.0f)) / c.k.z0b_cbc;
   const float q = c.k.kappa / logf(ratio);
-  const float v = F2(fsm, i, j) > 0.0f ? q * q : c.k.cbcmin;
+  const float v = valid ? q * q : c.k.cbcmin;
   P2(cbc, i, j) = fminf_t(fmaxf_t(v, c.k.cbcmin), c.k.cbcmax);
 }
 

@@ -1055,6 +1055,53 @@ NPOM_HD void bcond3_explicit_edge(const Ctx &c, int i, int j, float *ufo, float 
   }
 }
 
+// The Jiaozhou Bay policy's bcond 3 (jzb_boundary.py:88-140) at one level
+// k < kbm1: u on the east edge and at column 1 (its ghost column 0 a copy),
+// v on the north edge and at row 1 (its ghost row 0 a copy), each the blend
+// ga * (1-2-1 average across the edge one cell inside) + (1 - ga) * (the
+// same at the edge) with ga = sqrt(max(d / hmax, 0)) at the depth cell the
+// policy names (east and north edges, column 0, row 1), times ramp except
+// on the north edge, wherever that d > 0; there the tangential component
+// on the outer ring is zero.  Reads u, v and d only; the edge sets touch
+// different values, so their order does not matter.  The masks follow in
+// B9.
+NPOM_HD void jzb_bcond3_level(const Ctx &c, int i, int j, int k, float &uo, float &vo) {
+  const int im = c.im, jm = c.jm;
+  if (k >= c.kb - 1) return;
+  const float hmax = c.k.hmax, ramp = c.ramp;
+  auto ga_of = [&](int ii, int jj) { return sqrtf(fmaxf_t(F2(d, ii, jj) / hmax, 0.0f)); };
+  auto avg_u = [&](int ii) {
+    return 0.25f * F3(u, ii, j - 1, k) + 0.50f * F3(u, ii, j, k) + 0.25f * F3(u, ii, j + 1, k);
+  };
+  auto avg_v = [&](int jj) {
+    return 0.25f * F3(v, i - 1, jj, k) + 0.50f * F3(v, i, jj, k) + 0.25f * F3(v, i + 1, jj, k);
+  };
+  if (j >= 1 && j <= jm - 2) {
+    if (i == im - 1 && F2(d, im - 1, j) > 0.0f) {
+      const float ga = ga_of(im - 1, j);
+      uo = (ga * avg_u(im - 2) + (1.0f - ga) * avg_u(im - 1)) * ramp;
+      vo = 0.0f;
+    }
+    if ((i == 1 || i == 0) && F2(d, 0, j) > 0.0f) {
+      const float ga = ga_of(0, j);
+      uo = (ga * avg_u(2) + (1.0f - ga) * avg_u(1)) * ramp;
+      if (i == 0) vo = 0.0f;
+    }
+  }
+  if (i >= 1 && i <= im - 2) {
+    if (j == jm - 1 && F2(d, i, jm - 1) > 0.0f) {
+      const float ga = ga_of(i, jm - 1);
+      vo = ga * avg_v(jm - 2) + (1.0f - ga) * avg_v(jm - 1);
+      uo = 0.0f;
+    }
+    if ((j == 1 || j == 0) && F2(d, i, 1) > 0.0f) {
+      const float ga = ga_of(i, 1);
+      vo = (ga * avg_v(2) + (1.0f - ga) * avg_v(1)) * ramp;
+      if (j == 0) uo = 0.0f;
+    }
+  }
+}
+
 NPOM_HD void phase_b8_column(const Ctx &c, int i, int j) {
   const int kb = c.kb;
   float fin[KMAX], uo[KMAX], vo[KMAX];
@@ -1065,7 +1112,11 @@ NPOM_HD void phase_b8_column(const Ctx &c, int i, int j) {
   profuv_column(c, 0, i, j, fin, uo, wub, tpsu);
   for (int k = 0; k < kb; ++k) fin[k] = (inner && k < kb - 1) ? advv_point(c, i, j, k) : 0.0f;
   profuv_column(c, 1, i, j, fin, vo, wvb, tpsv);
-  if (is_explicit(c) && !c.k.obc_seamount) bcond3_explicit_edge(c, i, j, uo, vo);
+  if (c.k.obc_jzb) {
+    for (int k = 0; k < kb; ++k) jzb_bcond3_level(c, i, j, k, uo[k], vo[k]);
+  } else if (is_explicit(c) && !c.k.obc_seamount) {
+    bcond3_explicit_edge(c, i, j, uo, vo);
+  }
   for (int k = 0; k < kb; ++k) {
     P3(uf, i, j, k) = uo[k];
     P3(vf, i, j, k) = vo[k];

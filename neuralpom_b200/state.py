@@ -127,11 +127,12 @@ def make_params(s, im, jm, kb, core, device=0):
     p.profq_form = _abi.PROFQ_POM08 if form == "pom08" else _abi.PROFQ_PRODUCTION
     p.zsh = float(get("zsh", 0.01))
     obc = str(get("obc_form", "native") or "native").strip().lower()
-    if obc not in ("native", "seamount", "coastal"):
-        raise ValueError(f"unknown boundary policy {obc!r} (native, seamount or coastal)")
+    if obc not in ("native", "seamount", "coastal", "jzb"):
+        raise ValueError(f"unknown boundary policy {obc!r} (native, seamount, coastal or jzb)")
     if obc != "native" and implicit:
         raise ValueError(f"the {obc} boundary policy is built for the explicit core")
-    p.obc_form = {"native": _abi.OBC_NATIVE, "seamount": _abi.OBC_SEAMOUNT, "coastal": _abi.OBC_COASTAL}[obc]
+    p.obc_form = {"native": _abi.OBC_NATIVE, "seamount": _abi.OBC_SEAMOUNT, "coastal": _abi.OBC_COASTAL,
+                  "jzb": _abi.OBC_JZB}[obc]
     # periodic x: two halo columns on each side, unique columns 2..im-3
     # (no counterpart in the reference, whose lateral boundaries are walls
     # and open edges)

@@ -91,7 +91,7 @@ class EmulCore:
         self.ws.sync = self.sync.ctypes.data
         self.ws.status = self.status.ctypes.data
         self.ws.cg_iters = self.cg_iters.ctypes.data
-        if str(s.get("obc_form", "native")).lower() == "coastal":
+        if str(s.get("obc_form", "native")).lower() in ("coastal", "jzb"):
             self.tide = state.tide_planes(im, jm, arrays["tide_i"], arrays["tide_j"], arrays["tide_amp"],
                                           arrays["tide_phase"])
             self.ws.tide = self.tide.ctypes.data

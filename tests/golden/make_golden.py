@@ -470,6 +470,57 @@ def make_coastal_policy_golden(im=24, jm=18, steps=(1, 3)):
     print("wrote", path, os.path.getsize(path))
 
 
+def make_jzb_policy_golden(im=24, jm=18, steps=(1, 3)):
+    """The explicit core under the reference's Jiaozhou Bay tide policy, set
+    up the way its registry does (cores/case_adapters/registry.py:147-156:
+    the coastal step copies bound as methods, jzb_boundary.install with a
+    tide table file, jzb_compat.install with the POM08-WAD closure) on
+    ``cases.bay`` (kb = 16), clock at 0.25 day (ramp 0.083 of the bay's
+    3-day ramp); one internal step per call with the tide substep counter
+    reset, as the registry's advancement does (registry.py:38-63); 1 and 3
+    steps."""
+    import tempfile
+    import torch
+    from importlib import import_module
+    sys.path.insert(0, ROOT)
+    from neuralpom_b200 import cases
+    from neuralpom.cores.case_adapters import jzb_boundary, jzb_compat, registry
+    A, Sc = cases.bay(im, jm, kb=16)
+    Sc = dict(Sc, time=0.25, time0=0.25)
+    core = rh.build_reference_core("explicit", im, jm)
+    rh.load_state(core, {k: v for k, v in A.items() if hasattr(core, k) and k != "period"}, Sc)
+    core.alpha, core.smoth = 0.225, 0.1
+    for module, cls in (("momentum", "MomentumMixin"), ("tracers", "TracersMixin"), ("time_loop", "TimeLoopMixin")):
+        registry._bind_mixin(core, getattr(import_module(f"neuralpom.cores.case_adapters.kernels.coastal_explicit_{module}"),
+                                           cls))
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "tide.dat")
+        np.savetxt(path, np.c_[A["tide_i"] + 1, A["tide_j"] + 1, A["tide_amp"], A["tide_phase"]])
+        jzb_boundary.install(core, "explicit", path)
+    jzb_compat.install(core)
+    torch.set_default_dtype(torch.float32)
+    core.profq_form, core.zsh, core.obc_form = "pom08", 0.01, "jzb"
+
+    arrays, scalars = rh.extract_state(core)
+    out = {f"in__{k}": v for k, v in arrays.items()}
+    for k, v in scalars.items():
+        out[f"scalar__{k}"] = np.asarray(v)
+    done = 0
+    for n in steps:
+        while done < n:
+            core._tide_substep = 0
+            rh.advance(core, "explicit", 1)
+            done += 1
+        a, _ = rh.extract_state(core)
+        for f in OUTPUT_FIELDS:
+            out[f"out{n}__{f}"] = a[f]
+        out[f"out{n}__cbc"] = a["cbc"]
+        out[f"out{n}__scalar_time"] = np.asarray(float(core.time))
+    path = os.path.join(HERE, f"step_jzb_policy_{im}x{jm}.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path))
+
+
 def make_shapiro_golden(im=20, jm=18, seed=81, gamma=0.05):
     """The semi-implicit core with its spatial Shapiro filters on (barotropic
     elevation after the solve, core.py:893-916, and tracers,
@@ -499,7 +550,7 @@ def make_pom08_goldens():
 
 
 def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint", "coupling", "mpdata", "pom08", "seamount",
-                "shapiro")):
+                "shapiro", "jzb")):
     src = rh.default_reference_path()
     if src is None:
         raise SystemExit("reference sources not found; set NPOM_REFERENCE_SRC")
@@ -531,8 +582,10 @@ def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint", "couplin
         make_coastal_policy_golden()
     if "shapiro" in which:
         make_shapiro_golden()
+    if "jzb" in which:
+        make_jzb_policy_golden()
 
 
 if __name__ == "__main__":
     main(tuple(sys.argv[1:]) or ("proft", "steps", "adjoint", "coastal", "step_adjoint", "coupling", "mpdata",
-                                 "pom08", "seamount", "shapiro"))
+                                 "pom08", "seamount", "shapiro", "jzb"))

@@ -22,6 +22,8 @@ STEP_FILES = [("step_explicit_12x10.npz", "explicit"), ("step_implicit_12x10.npz
               ("step_seamount_explicit_24x18.npz", "explicit"),
               # the reference's coastal tide policy (its boundary, step copies and closure)
               ("step_coastal_policy_24x18.npz", "explicit"),
+              # the reference's Jiaozhou Bay tide policy (its boundary, the coastal step copies, closure)
+              ("step_jzb_policy_24x18.npz", "explicit"),
               ("step_implicit_shapiro_20x18.npz", "implicit_p0_fixed")]
 
 
