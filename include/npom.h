@@ -168,6 +168,13 @@ enum { NPOM_PROFQ_PRODUCTION = 0, NPOM_PROFQ_POM08 = 1 };
  * edges; the north and south edges are walls.  Forward only (the reference
  * refuses gradients through its case policies). */
 enum { NPOM_OBC_NATIVE = 0, NPOM_OBC_SEAMOUNT = 1, NPOM_OBC_COASTAL = 2, NPOM_OBC_JZB = 3 };
+/* COASTAL and JZB on the semi-implicit core (barotropic_shapiro 0): the
+ * policy's step copy (the old depth in the corrector's pressure-gradient
+ * transport, cbc after the filter), its bcond 2 on u* and on the corrected
+ * transports, its own free-surface solve -- CG on the interior sea cells
+ * that are not tide cells, weighted by the cell areas, for the part beyond
+ * the tidal lift (coastal_boundary.py:31-54, jzb_boundary.py:150-197) --
+ * and the explicit step copy's bcond 3-6. */
 /* JZB: the explicit core with the Jiaozhou Bay tide policy
  * (cores/case_adapters/jzb_boundary.py, jzb_compat.py and the coastal
  * policy's step copies): the coastal policy's machinery (tide planes, no

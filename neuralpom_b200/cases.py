@@ -416,23 +416,25 @@ def open_seamount(im=65, jm=49, kb=16, dte=5.0, isplit=30, dx=5.0e3, u0=0.1, lat
     return seamount_policy(A, s)
 
 
-def coastal_policy(A, s, tide_i, tide_j, tide_amp, tide_phase):
+def coastal_policy(A, s, tide_i, tide_j, tide_amp, tide_phase, core="explicit"):
     """The coastal tide policy's set-up on a state (cores/case_adapters/
-    coastal_boundary.py:55-65 and coastal_compat.py:12-23): the tide table
-    (0-based cells, amplitude in m, phase in degrees), rf = 1, alpha and
-    smoth of the explicit core, the POM08-WAD closure (zsh = 0.01 m) and
+    coastal_boundary.py:55-65 and coastal_compat.py:12-23, registry.py:
+    137-138): the tide table (0-based cells, amplitude in m, phase in
+    degrees), rf = 1, alpha and smoth of the core (0.225 / 0.1 explicit,
+    0.333 / 0.15 semi-implicit), the POM08-WAD closure (zsh = 0.01 m) and
     the coastal boundary (``obc_form``)."""
     A = dict(A)
     A["tide_i"] = np.asarray(tide_i, F32)
     A["tide_j"] = np.asarray(tide_j, F32)
     A["tide_amp"] = np.asarray(tide_amp, F32)
     A["tide_phase"] = np.asarray(tide_phase, F32)
-    s = dict(s, rfe=1.0, rfw=1.0, rfn=1.0, rfs=1.0, alpha=0.225, smoth=0.1, profq_form="pom08", zsh=0.01,
+    alpha, smoth = (0.225, 0.1) if core == "explicit" else (0.333, 0.15)
+    s = dict(s, rfe=1.0, rfw=1.0, rfn=1.0, rfs=1.0, alpha=alpha, smoth=smoth, profq_form="pom08", zsh=0.01,
              obc_form="coastal")
     return A, s
 
 
-def tidal_inlet(im=40, jm=30, kb=5, dte=1.0, isplit=10, dx=500.0, lat=30.0, amplitude=1.0):
+def tidal_inlet(im=40, jm=30, kb=5, dte=1.0, isplit=10, dx=500.0, lat=30.0, amplitude=1.0, core="explicit"):
     """The geometry the coastal tide policy serves (registered at 161x101x5,
     dtE/dtI = 1/10 s, from data that is not in the repository): a shelf
     closed on the west, north and south, depth 2 m at the west wall growing
@@ -440,8 +442,9 @@ def tidal_inlet(im=40, jm=30, kb=5, dte=1.0, isplit=10, dx=500.0, lat=30.0, ampl
     f-plane at ``lat``, no wind; with ``coastal_policy`` applied and the
     tide table of the registered case's layout: every interior cell of the
     column next to the east edge, here with amplitude ``amplitude`` scaled
-    by 0.8-1.0 along the column and a phase of 2 degrees per row."""
-    core = "explicit"
+    by 0.8-1.0 along the column and a phase of 2 degrees per row.  ``core``
+    "implicit_p0_fixed" gives the semi-implicit core's scalars (its
+    dti = dte * isplit, the policy's own spatial filters off)."""
     s = state.default_scalars(core)
     s.update(dte=dte, isplit=isplit, hmax=60.0)
     state.derived_time(s)
@@ -468,10 +471,10 @@ def tidal_inlet(im=40, jm=30, kb=5, dte=1.0, isplit=10, dx=500.0, lat=30.0, ampl
     A, s = finish_initialization(A, s, core)
     rows = np.arange(1, jm - 1)
     amp = amplitude * (0.8 + 0.2 * rows / max(jm - 2, 1))
-    return coastal_policy(A, s, np.full(rows.shape, im - 2), rows, amp, 2.0 * rows)
+    return coastal_policy(A, s, np.full(rows.shape, im - 2), rows, amp, 2.0 * rows, core=core)
 
 
-def jzb_policy(A, s, tide_i, tide_j, tide_amp, tide_phase):
+def jzb_policy(A, s, tide_i, tide_j, tide_amp, tide_phase, core="explicit"):
     """The Jiaozhou Bay tide policy's set-up on a state
     (cores/case_adapters/jzb_boundary.py:200-215 and jzb_compat.py:30-70):
     the tide table (0-based cells, amplitude in m, phase in degrees), rf = 1,
@@ -484,12 +487,13 @@ def jzb_policy(A, s, tide_i, tide_j, tide_amp, tide_phase):
     A["tide_amp"] = np.asarray(tide_amp, F32)
     A["tide_phase"] = np.asarray(tide_phase, F32)
     A["period"] = np.asarray(F32(3.0))
-    s = dict(s, rfe=1.0, rfw=1.0, rfn=1.0, rfs=1.0, alpha=0.225, smoth=0.1, profq_form="pom08", zsh=0.01,
+    alpha, smoth = (0.225, 0.1) if core == "explicit" else (0.333, 0.15)
+    s = dict(s, rfe=1.0, rfw=1.0, rfn=1.0, rfs=1.0, alpha=alpha, smoth=smoth, profq_form="pom08", zsh=0.01,
              obc_form="jzb", mode=4, lramp=True, period=3.0, horcon=0.1, hmax=60.0, tprni=0.2, umol=2.0e-5)
     return A, s
 
 
-def bay(im=40, jm=30, kb=16, dte=1.0, isplit=10, dx=500.0, lat=36.0, amplitude=1.0):
+def bay(im=40, jm=30, kb=16, dte=1.0, isplit=10, dx=500.0, lat=36.0, amplitude=1.0, core="explicit"):
     """The geometry the Jiaozhou Bay policy serves (registered at 312x213x17,
     dtE/dtI = 1/10 s, from data that is not in the repository): a bay closed
     on the west, east and north, open to the sea on the south edge, depth 2 m
@@ -498,8 +502,8 @@ def bay(im=40, jm=30, kb=16, dte=1.0, isplit=10, dx=500.0, lat=36.0, amplitude=1
     rest; with ``jzb_policy`` applied and a tide table of the registered
     layout: every interior cell of the row next to the open edge, with
     amplitude ``amplitude`` scaled by 0.8-1.0 along the row and a phase of
-    1.5 degrees per column."""
-    core = "explicit"
+    1.5 degrees per column.  ``core`` "implicit_p0_fixed" gives the
+    semi-implicit core's scalars."""
     s = state.default_scalars(core)
     s.update(dte=dte, isplit=isplit, hmax=60.0, aam_init=50.0)
     state.derived_time(s)
@@ -526,4 +530,4 @@ def bay(im=40, jm=30, kb=16, dte=1.0, isplit=10, dx=500.0, lat=36.0, amplitude=1
     A, s = finish_initialization(A, s, core)
     cols = np.arange(1, im - 1)
     amp = amplitude * (0.8 + 0.2 * cols / max(im - 2, 1))
-    return jzb_policy(A, s, cols, np.full(cols.shape, 1), amp, 1.5 * cols)
+    return jzb_policy(A, s, cols, np.full(cols.shape, 1), amp, 1.5 * cols, core=core)

@@ -112,10 +112,15 @@ inline bool check_args(const npom_params *p, float *const *fields, const npom_wo
     if (!fields[f]) return false;
   if (!ws->partials || !ws->sync || !ws->status || !ws->cg_iters) return false;
   if (p->nadv != 1 && (p->nadv != 2 || !ws->mp3d || p->nitera < 1)) return false;
+  // the seamount policy on the explicit core; the tide policies on either
+  // core (the semi-implicit one with its Shapiro filter at 0, as their
+  // installers set it)
+  const bool tide_policy = p->obc_form == NPOM_OBC_COASTAL || p->obc_form == NPOM_OBC_JZB;
   if (p->obc_form != NPOM_OBC_NATIVE &&
-      ((p->obc_form != NPOM_OBC_SEAMOUNT && p->obc_form != NPOM_OBC_COASTAL && p->obc_form != NPOM_OBC_JZB) ||
-       p->core != NPOM_CORE_EXPLICIT || p->im < 6 || p->jm < 6 ||
-       ((p->obc_form == NPOM_OBC_COASTAL || p->obc_form == NPOM_OBC_JZB) && !ws->tide)))
+      ((p->obc_form != NPOM_OBC_SEAMOUNT && !tide_policy) ||
+       (p->obc_form == NPOM_OBC_SEAMOUNT && p->core != NPOM_CORE_EXPLICIT) || p->im < 6 || p->jm < 6 ||
+       (tide_policy && !ws->tide) ||
+       (tide_policy && p->core == NPOM_CORE_IMPLICIT && p->barotropic_shapiro != 0.0)))
     return false;
   if (p->periodic_x &&
       (p->periodic_x != 1 || p->core != NPOM_CORE_IMPLICIT || p->obc_form != NPOM_OBC_NATIVE || p->nadv != 1 ||

@@ -42,7 +42,7 @@ constexpr int kThreads = 256;
 // ---------------------------------------------------------------------------
 enum PointPhase { PP_A1 = 0, PP_B2B = 1, PP_B4 = 2, PP_B5 = 3, PP_B7 = 4 };
 enum ColPhase { CP_A2 = 0, CP_B1 = 1, CP_B2A = 2, CP_B3 = 3, CP_B6 = 4, CP_B8 = 5, CP_B9 = 6 };
-enum CellPhase { XP_A3 = 0, XP_I5 = 1, XP_COEF = 2 };
+enum CellPhase { XP_A3 = 0, XP_I5 = 1, XP_COEF = 2, XP_I5A = 3 };
 
 // The bodies below map one thread index of a phase onto its grid point,
 // column or cell; the one-member kernels and the batched kernels (many
@@ -140,6 +140,8 @@ __device__ __forceinline__ void cells_body(const Ctx &c, int cell) {
     if (phase_i5_cell(c, i, j)) atomicOr(c.status, NPOM_DEV_VMAX);
   } else if (PH == XP_COEF) {
     elliptic_coeff_cell(c, i, j);
+  } else if (PH == XP_I5A) {
+    phase_i5a_cell(c, i, j);
   }
 }
 
@@ -664,6 +666,111 @@ __global__ void __launch_bounds__(kThreads) k_pcg(Ctx c, int with_rhs, int with_
   pcg_coop_body(c, with_rhs, with_post);
 }
 
+// The tide policies' free-surface solve on the semi-implicit core
+// (coastal_boundary.py:31-54, jzb_boundary.py:150-197), one cooperative
+// launch: the RHS and stored transports as the production solve sets them
+// up, then CG without preconditioner on the free nodes (the interior sea
+// cells that are not tide cells) for the homogeneous problem A x = b,
+// b = rhs - A(lift) (the tidal lift), with the cell areas as dot-product
+// weights (FP64 sums), x0 = 0, at most min(max_iter, 500) iterations,
+// stopping at the top of an iteration once rr <= max(1e-30, 1e-24 rr0);
+// the count it + 1 goes to the iteration history; then elf = x + lift
+// with the step's bcond 1 (policy_elf).  The depth is not updated (the
+// step copy keeps the old d for the corrector).  Three grid barriers per
+// iteration.
+__device__ __forceinline__ void cg_policy_body(const Ctx &c) {
+  const int im = c.im, jm = c.jm;
+  const size_t ncell = (size_t)im * jm;
+  const size_t stride = (size_t)vgrid(c) * blockDim.x;
+  const size_t tid = (size_t)vblock(c) * blockDim.x + threadIdx.x;
+  float *x = c.W[NPOM_W_x], *r = c.W[NPOM_W_r], *p = c.W[NPOM_W_p], *ap = c.W[NPOM_W_ap];
+  float *rhs = c.W[NPOM_W_rhs], *lift = c.W[NPOM_W_zv];
+  for (size_t q = tid; q < ncell; q += stride) {
+    const int i = (int)(q / jm), j = (int)(q % jm);
+    rhs[q] = rhs_cell(c, i, j);
+    P2(fluxua, i, j) = rhs_fluxua(c, i, j);
+    P2(fluxva, i, j) = rhs_fluxva(c, i, j);
+    lift[q] = policy_lift(c, i, j);
+  }
+  if (!grid_barrier(c)) return;
+  double rr = 0.0;
+  for (size_t q = tid; q < ncell; q += stride) {
+    const int i = (int)(q / jm), j = (int)(q % jm);
+    const bool fixed = policy_fixed(c, i, j);
+    const float b = fixed ? 0.0f : __ldcg(rhs + q) - elliptic_apply_cell(c, lift, i, j);
+    x[q] = 0.0f;
+    r[q] = b;
+    p[q] = b;
+    const float w = fixed ? 0.0f : F2(art, i, j);
+    rr += (double)(w * b) * (double)b;
+  }
+  block_sum3(c, rr, 0.0, 0.0, 1, -1, -1);
+  if (!grid_barrier(c)) return;
+  rr = grid_total(c, 1);
+  const double thr = fmax(1e-30, rr * 1e-24);
+  const int nmax = c.k.eta_max_iter < 500 ? c.k.eta_max_iter : 500;
+  int its = nmax;
+  for (int it = 0; it < nmax; ++it) {
+    if (rr <= thr) {
+      its = it + 1;
+      break;
+    }
+    double den = 0.0;
+    for (size_t q = tid; q < ncell; q += stride) {
+      const int i = (int)(q / jm), j = (int)(q % jm);
+      const bool fixed = policy_fixed(c, i, j);
+      const float a = fixed ? 0.0f : elliptic_apply_cell(c, p, i, j);
+      ap[q] = a;
+      const float w = fixed ? 0.0f : F2(art, i, j);
+      den += (double)(w * __ldcg(p + q)) * (double)a;
+    }
+    block_sum3(c, den, 0.0, 0.0, 0, -1, -1);
+    if (!grid_barrier(c)) return;
+    const float alpha = (float)(rr / (grid_total(c, 0) + 1e-40));
+    double nw = 0.0;
+    for (size_t q = tid; q < ncell; q += stride) {
+      const int i = (int)(q / jm), j = (int)(q % jm);
+      x[q] = __ldcg(x + q) + alpha * __ldcg(p + q);
+      const float rv = __ldcg(r + q) - alpha * __ldcg(ap + q);
+      r[q] = rv;
+      const float w = policy_fixed(c, i, j) ? 0.0f : F2(art, i, j);
+      nw += (double)(w * rv) * (double)rv;
+    }
+    block_sum3(c, nw, 0.0, 0.0, 1, -1, -1);
+    if (!grid_barrier(c)) return;
+    nw = grid_total(c, 1);
+    const float beta = (float)(nw / (rr + 1e-40));
+    for (size_t q = tid; q < ncell; q += stride) p[q] = __ldcg(r + q) + beta * __ldcg(p + q);
+    rr = nw;
+    if (!grid_barrier(c)) return;
+  }
+  if (tid == 0) {
+    unsigned int slot = c.sync[2];
+    c.cg_iters[slot] = its;
+    c.sync[2] = slot + 1;
+  }
+  for (size_t q = tid; q < ncell; q += stride) {
+    const int i = (int)(q / jm), j = (int)(q % jm);
+    const float e = policy_elf(c, x, i, j);
+    if (!(fabsf(e) <= 3.0e38f)) atomicOr(c.status, NPOM_DEV_NONFINITE);
+    P2(elf, i, j) = e;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_cg_policy(Ctx c) { cg_policy_body(c); }
+
+// The coastal policy's bcond 2 lines (policy_bc2_line): jm + im lines
+__global__ void __launch_bounds__(kThreads) k_policy_bc2(Ctx c, int which) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < c.jm + c.im) policy_bc2_line(c, t, which);
+}
+
+void launch_policy_bc2(const Ctx &c, int which, cudaStream_t s) {
+  if (!c.k.obc_coastal || c.k.obc_jzb) return;
+  const int n = c.jm + c.im;
+  k_policy_bc2<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(c, which);
+}
+
 // Fused external mode of the explicit core: isplit substeps, three phases
 // each (explicit/time_loop.py:292-431).
 __device__ __forceinline__ void subcycle_coop_body(const Ctx &c) {
@@ -1015,14 +1122,25 @@ size_t pcg_coop_work(const Ctx &c) {
 }
 
 cudaError_t plan_pcg(const Ctx &c, PcgPlan *plan) {
+  plan->coop_blocks = 0;
+  if (c.k.obc_coastal) {
+    // the tide policies' own solve (k_cg_policy)
+    plan->cluster = false;
+    return coop_blocks((const void *)k_cg_policy, (size_t)c.im * c.jm, &plan->coop_blocks);
+  }
   plan->cluster = pcg_cluster_layout(c, &plan->L) && ensure_cluster_attrs(plan->L) &&
                   cluster_launchable(pcg_cluster_fn(plan->L), plan->L.nc, plan->L.bytes());
-  plan->coop_blocks = 0;
   if (plan->cluster) return cudaSuccess;
   return coop_blocks((const void *)k_pcg, pcg_coop_work(c), &plan->coop_blocks);
 }
 
 cudaError_t run_pcg(Ctx c, const PcgPlan &plan, int with_rhs, int with_post, cudaStream_t s) {
+  if (c.k.obc_coastal) {
+    // the policy solve always sets up its RHS and applies its bcond 1
+    c.coh = 1;
+    void *args[] = {&c};
+    return launch_coop((const void *)k_cg_policy, plan.coop_blocks, args, c.sync, s);
+  }
   if (plan.cluster) return run_pcg_cluster(c, plan.L, with_rhs, with_post, s);
   c.coh = 1;
   void *args[] = {&c, &with_rhs, &with_post};
@@ -1278,11 +1396,23 @@ cudaError_t enqueue_step(const Ctx &c, int core, const PcgPlan &plan, int sub_bl
   launch_wrap_x(c, s);
   cudaError_t e;
   if (core == NPOM_CORE_IMPLICIT) {
+    launch_policy_bc2(c, 0, s);
     e = run_pcg(c, plan, 1, 1, s);
     if (e != cudaSuccess) return e;
     launch_wrap_x(c, s);
+    if (c.k.obc_coastal) {
+      // the tide policies: corrector with bcond 2 first, then the filter
+      // and shifts, then cbc from the new depth (coastal_implicit_time_loop
+      // .py:351-352)
+      launch_cells<XP_I5A>(c, s);
+      launch_policy_bc2(c, 1, s);
+    }
     launch_cells<XP_I5>(c, s);
     launch_wrap_x(c, s);
+    if (c.k.obc_coastal) {
+      const int n = c.im * c.jm;
+      k_cbc_coastal<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(c);
+    }
   } else {
     e = run_subcycle(c, sub_blocks, s);
     if (e != cudaSuccess) return e;
@@ -1399,7 +1529,8 @@ npom_status run_steps(const npom_params *p, float *const *fields, const npom_wor
     // the coastal policy's tide time of the step's first substep (its
     // launches change every step: no graph replay).  Other steps keep 0:
     // the context is the key of the step graphs
-    c.tide_t0 = c.k.obc_coastal ? time * 86400.0 - p->dti : 0.0;
+    // (the semi-implicit core's solve time: time * 86400 - dte)
+    c.tide_t0 = !c.k.obc_coastal ? 0.0 : time * 86400.0 - (core == NPOM_CORE_IMPLICIT ? p->dte : p->dti);
     bool done = false;
     if (graphs && c.ramp == 1.0f && !c.k.obc_coastal) {
       if (launch_step_graph(c, core, plan, sub_blocks, s, &done) != cudaSuccess) return NPOM_ERR_CUDA;
@@ -1741,7 +1872,10 @@ npom_status npom_run_phase(const npom_params *p, float *const *fields, const npo
   switch (phase) {
     case 0: launch_a1(c, s); break;
     case 1: launch_cols<CP_A2>(c, s); break;
-    case 2: launch_cells<XP_A3>(c, s); break;
+    case 2:
+      launch_cells<XP_A3>(c, s);
+      if (p->core == NPOM_CORE_IMPLICIT) launch_policy_bc2(c, 0, s);
+      break;
     case 3:
       if (cudaMemsetAsync(ws->sync, 0, 4 * sizeof(unsigned int), s) != cudaSuccess) return NPOM_ERR_CUDA;
       if (p->core == NPOM_CORE_IMPLICIT) {
@@ -1757,7 +1891,17 @@ npom_status npom_run_phase(const npom_params *p, float *const *fields, const npo
         if (e == cudaSuccess) e = run_subcycle(c, blocks, s);
       }
       break;
-    case 4: launch_cells<XP_I5>(c, s); break;
+    case 4:
+      if (c.k.obc_coastal && p->core == NPOM_CORE_IMPLICIT) {
+        launch_cells<XP_I5A>(c, s);
+        launch_policy_bc2(c, 1, s);
+      }
+      launch_cells<XP_I5>(c, s);
+      if (c.k.obc_coastal && p->core == NPOM_CORE_IMPLICIT) {
+        const int n = c.im * c.jm;
+        k_cbc_coastal<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(c);
+      }
+      break;
     case 5: launch_cols<CP_B1>(c, s); break;
     case 6: launch_cols<CP_B2A>(c, s); break;
     case 7: launch_points<PP_B2B>(c, s); break;

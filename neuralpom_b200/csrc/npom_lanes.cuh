@@ -363,7 +363,7 @@ __device__ __forceinline__ void lane_b6(const Ctx &c, int i, int j, int k, bool 
   float sf = lane_proft(c, k, F3(vf, i, j, k), khk, kh_next, F2(wssurf, i, j), F2(ssurf, i, j), c.k.nbcs, dh, swrad);
   // explicit bcond 4 (upstream T/S at the edges) replaces levels
   // 0..kbm1-1 of an edge column; each lane evaluates its own level
-  if (is_explicit(c) && !c.k.obc_seamount && k < KL - 1 && (i == 0 || i == c.im - 1 || j == 0 || j == c.jm - 1)) {
+  if (explicit_bc(c) && !c.k.obc_seamount && k < KL - 1 && (i == 0 || i == c.im - 1 || j == 0 || j == c.jm - 1)) {
     float ub, vb;
     if (bcond4_explicit_level(c, i, j, k, ub, vb)) {
       tf = ub;
@@ -506,7 +506,7 @@ __device__ __forceinline__ void lane_b8(const Ctx &c, int i, int j, int k, bool 
   lane_profuv(c, 0, i, j, k, fu, uo, wub, tpsu);
   lane_profuv(c, 1, i, j, k, fv, vo, wvb, tpsv);
   if (c.k.obc_jzb) jzb_bcond3_level(c, i, j, k, uo, vo);
-  else if (is_explicit(c) && !c.k.obc_seamount) lane_bcond3_explicit(c, i, j, k, uo, vo);
+  else if (explicit_bc(c) && !c.k.obc_seamount) lane_bcond3_explicit(c, i, j, k, uo, vo);
   if (!st) return;
   P3(uf, i, j, k) = uo;
   P3(vf, i, j, k) = vo;
@@ -534,7 +534,7 @@ __device__ __forceinline__ void lane_b9(const Ctx &c, int i, int j, int k, bool 
       float *ff = comp == 0 ? c.F[NPOM_F_uf] : c.F[NPOM_F_vf];
       const size_t o = NPOM_I3(c, i, j, k);
       float x = ff[o] * mask;
-      if (!is_explicit(c) && ring) x = 0.0f;
+      if (!explicit_bc(c) && ring) x = 0.0f;
       const float cur = fa[o];
       const float term = x + fb[o] - 2.0f * cur;
       const float tps = seg_sum(term * dzk, kbm1);

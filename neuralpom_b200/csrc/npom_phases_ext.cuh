@@ -17,6 +17,8 @@ namespace npom {
 // adx2d/ady2d -= advua/advva, egf and provisional utf/vtf; implicit core
 // also stores d_baro and the predictor (u*, v*) with bcond 2.
 // ---------------------------------------------------------------------------
+NPOM_HD void bcond2_jzb(const Ctx &c, int i, int j, float &uaf, float &vaf);
+
 NPOM_HD void phase_a3_cell(const Ctx &c, int i, int j) {
   const int im = c.im, jm = c.jm;
   // rho = (rho - rmean) + rmean (momentum.py:554,698)
@@ -70,7 +72,21 @@ NPOM_HD void phase_a3_cell(const Ctx &c, int i, int j) {
     us = us * F2(dum, i, j);
     vs = vs * F2(dvm, i, j);
   }
-  if (i == 0 || i == im - 1 || j == 0 || j == jm - 1) {
+  const bool ring = i == 0 || i == im - 1 || j == 0 || j == jm - 1;
+  if (c.k.obc_coastal) {
+    // the tide policies' bcond 2 on u*, v* (coastal_boundary.py:23-29,
+    // jzb_boundary.py:51-86): the ring keeps the predictor's raw values (ua,
+    // va); the bay's Sommerfeld edges read only ua, va and d; the coastal
+    // radiation reads the neighbours' new u*, v* (policy_bc2_line, next
+    // launch); then the masks
+    if (ring) {
+      us = F2(ua, i, j);
+      vs = F2(va, i, j);
+    }
+    if (c.k.obc_jzb) bcond2_jzb(c, i, j, us, vs);
+    us = us * F2(dum, i, j);
+    vs = vs * F2(dvm, i, j);
+  } else if (ring) {
     us = 0.0f;
     vs = 0.0f;
   }
@@ -234,16 +250,26 @@ NPOM_HD float dst_stage_j(const Ctx &c, const float *src, int a, int b) {
 // Corrector, closed-basin bcond 2, etf, Robert-Asselin filter, state shifts,
 // egf and endpoint transports (core.py:918-943, time_loop.py:309-387).
 // Returns true when |vaf| exceeds vmaxl at this cell.
-NPOM_HD bool phase_i5_cell(const Ctx &c, int i, int j) {
+// The corrector and its bcond 2 (core.py:918-943).  The tide policies'
+// step copy leaves d at its old value for the pressure-gradient transport
+// (coastal_implicit_time_loop.py:301-303), keeps the raw ring (the old uaf)
+// and applies the policy's bcond 2, like the predictor's.
+NPOM_HD void i5_uvaf(const Ctx &c, int i, int j, float &uaf, float &vaf) {
   const int im = c.im, jm = c.jm;
   const float elf0 = F2(elf, i, j);
-  float uaf = F2(uaf, i, j), vaf = F2(vaf, i, j);
+  uaf = F2(uaf, i, j);
+  vaf = F2(vaf, i, j);
   if (interior(c, i, j)) {
     const float g4 = c.k.quarter_g, al = c.k.alpha;
     float h0 = F2(h, i, j);
     float dnew = h0 + elf0;
     float dnew_w = F2(h, i - 1, j) + F2(elf, i - 1, j);
     float dnew_s = F2(h, i, j - 1) + F2(elf, i, j - 1);
+    if (c.k.obc_coastal) {
+      dnew = F2(d, i, j);
+      dnew_w = F2(d, i - 1, j);
+      dnew_s = F2(d, i, j - 1);
+    }
     float gu = g4 * (F2(dy, i, j) + F2(dy, i - 1, j)) * (dnew + dnew_w) * al * (elf0 - F2(elf, i - 1, j));
     float gv = g4 * (F2(dx, i, j) + F2(dx, i, j - 1)) * (dnew + dnew_s) * al * (elf0 - F2(elf, i, j - 1));
     float dfu = (h0 + elf0 + F2(h, i - 1, j) + F2(elf, i - 1, j)) * F2(aru, i, j);
@@ -251,11 +277,34 @@ NPOM_HD bool phase_i5_cell(const Ctx &c, int i, int j) {
     uaf = (W2(us, i, j) * W2(den_u, i, j) - c.k.four_dti * gu) / (dfu + 1e-20f) * F2(dum, i, j);
     vaf = (W2(vs, i, j) * W2(den_v, i, j) - c.k.four_dti * gv) / (dfv + 1e-20f) * F2(dvm, i, j);
   }
+  if (c.k.obc_coastal && c.k.obc_jzb) bcond2_jzb(c, i, j, uaf, vaf);
   uaf = uaf * F2(dum, i, j);
   vaf = vaf * F2(dvm, i, j);
-  if (i == 0 || i == im - 1 || j == 0 || j == jm - 1) {
+  if (!c.k.obc_coastal && (i == 0 || i == im - 1 || j == 0 || j == jm - 1)) {
     uaf = 0.0f;
     vaf = 0.0f;
+  }
+}
+
+// Phase I5a of the tide policies: the corrector with bcond 2 into uaf/vaf
+// (the coastal radiation's edges follow in policy_bc2_line); I5 then reads
+// them.  Reads ua, va, d and uaf, none of which it writes elsewhere.
+NPOM_HD void phase_i5a_cell(const Ctx &c, int i, int j) {
+  float uaf, vaf;
+  i5_uvaf(c, i, j, uaf, vaf);
+  P2(uaf, i, j) = uaf;
+  P2(vaf, i, j) = vaf;
+}
+
+NPOM_HD bool phase_i5_cell(const Ctx &c, int i, int j) {
+  const int im = c.im, jm = c.jm;
+  const float elf0 = F2(elf, i, j);
+  float uaf, vaf;
+  if (c.k.obc_coastal) {
+    uaf = F2(uaf, i, j);
+    vaf = F2(vaf, i, j);
+  } else {
+    i5_uvaf(c, i, j, uaf, vaf);
   }
   P2(uaf, i, j) = uaf;
   P2(vaf, i, j) = vaf;
@@ -611,6 +660,101 @@ NPOM_HD void ext_phase3_cell(const Ctx &c, int i, int j, int iext) {
       P2(vtf, i, j) = F2(vtf, i, j) + vaf * ds * c.k.isp2i;
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// The semi-implicit core under the coastal or Jiaozhou Bay tide policy.
+// ---------------------------------------------------------------------------
+
+// The coastal policy's bcond 2 on the semi-implicit core's u*, v* (after
+// A3, which = 0, on the us/vs planes) or uaf, vaf (after I5a, which = 1):
+// line t < jm handles row j = t (east edge, then column 1 and its ghost
+// column 0), line jm + i column i (north edge, then row 1 and its ghost row
+// 0), in coastal_boundary.py:23-29's formulas with el and the depth d the
+// step holds (the old depth: the step copy updates d after the corrector).
+// Each line writes values no other line reads or writes; the masks apply.
+NPOM_HD void policy_bc2_line(const Ctx &c, int t, int which) {
+  const int im = c.im, jm = c.jm;
+  float *ua = which == 0 ? c.W[NPOM_W_us] : c.F[NPOM_F_uaf];
+  float *va = which == 0 ? c.W[NPOM_W_vs] : c.F[NPOM_F_vaf];
+  const float g = c.k.grav;
+  auto rad = [&](int ii, int jj) { return sqrtf(g / F2(d, ii, jj)); };
+  if (t < jm) {
+    const int j = t;
+    if (j < 1 || j > jm - 2) return;
+    const float ue = ld(ua + NPOM_I2(c, im - 2, j)) + c.k.rfe * rad(im - 2, j) * (F2(el, im - 2, j) - F2(el, im - 1, j));
+    ua[NPOM_I2(c, im - 1, j)] = ue * F2(dum, im - 1, j);
+    va[NPOM_I2(c, im - 1, j)] = 0.0f * F2(dvm, im - 1, j);
+    const float uw = ld(ua + NPOM_I2(c, 1, j)) - c.k.rfw * rad(1, j) * (F2(el, 1, j) - F2(el, 0, j));
+    ua[NPOM_I2(c, 1, j)] = uw * F2(dum, 1, j);
+    ua[NPOM_I2(c, 0, j)] = uw * F2(dum, 0, j);
+    va[NPOM_I2(c, 0, j)] = 0.0f * F2(dvm, 0, j);
+  } else if (t < jm + im) {
+    const int i = t - jm;
+    if (i < 1 || i > im - 2) return;
+    const float vn = ld(va + NPOM_I2(c, i, jm - 2)) + c.k.rfn * rad(i, jm - 2) * (F2(el, i, jm - 2) - F2(el, i, jm - 1));
+    va[NPOM_I2(c, i, jm - 1)] = vn * F2(dvm, i, jm - 1);
+    ua[NPOM_I2(c, i, jm - 1)] = 0.0f * F2(dum, i, jm - 1);
+    const float vs = ld(va + NPOM_I2(c, i, 1)) - c.k.rfs * rad(i, 1) * (F2(el, i, 1) - F2(el, i, 0));
+    va[NPOM_I2(c, i, 1)] = vs * F2(dvm, i, 1);
+    va[NPOM_I2(c, i, 0)] = vs * F2(dvm, i, 0);
+    ua[NPOM_I2(c, i, 0)] = 0.0f * F2(dum, i, 0);
+  }
+}
+
+// The tide policies' elevation at a tide-table cell at the step's solve
+// time t = time * 86400 - dte (c.tide_t0): the coastal policy's
+// amp cos(w t / 3600 - phase), the bay's amp cos(w (t / 3600) - phase)
+// (coastal_boundary.py:9-10, jzb_boundary.py:17-21); the caller applies the
+// bay's fsm.
+NPOM_HD float policy_tide(const Ctx &c, size_t o) {
+  const size_t n2 = (size_t)c.im * c.jm;
+  const double sec = c.tide_t0;
+  const float arg = c.k.obc_jzb ? (float)(c.k.tide_w * (sec / 3600.0)) : (float)(c.k.tide_w * sec / 3600.0);
+  return c.tide[n2 + o] * cosf(arg - c.tide[2 * n2 + o] * 3.1416f / 180.0f);
+}
+
+// The policy solve's fixed nodes (not unknowns): the ring, land and the
+// tide cells (coastal_boundary.py:62-64, jzb_boundary.py:208-211).
+NPOM_HD bool policy_fixed(const Ctx &c, int i, int j) {
+  return !interior(c, i, j) || F2(fsm, i, j) == 0.0f || c.tide[NPOM_I2(c, i, j)] != 0.0f;
+}
+
+// The solve's lift: the tide at the tide cells, zero elsewhere; the bay's
+// times fsm there, then its edges copying the adjacent cell and the mask
+// (jzb_boundary.py:152-157).
+NPOM_HD float policy_lift(const Ctx &c, int i, int j) {
+  if (c.k.obc_jzb) {
+    const int si = i == 0 ? 1 : (i == c.im - 1 ? c.im - 2 : i);
+    const int sj = j == 0 ? 1 : (j == c.jm - 1 ? c.jm - 2 : j);
+    const size_t o = NPOM_I2(c, si, sj);
+    const float v = c.tide[o] != 0.0f ? policy_tide(c, o) * F2(fsm, si, sj) : 0.0f;
+    return v * F2(fsm, i, j);
+  }
+  const size_t o = NPOM_I2(c, i, j);
+  return c.tide[o] != 0.0f ? policy_tide(c, o) : 0.0f;
+}
+
+// elf after the policy solve and the step's bcond 1 (core.py:913-916 with
+// the Shapiro filter at gamma 0): from x + lift (x holds the solution, zero
+// on the fixed nodes), the interior masked, the tide cells set to the tide
+// and the mask; the bay's edges copy the adjacent cell first (the solve's
+// own copy, then bcond 1's, both of the same interior cell).
+NPOM_HD float policy_elf(const Ctx &c, const float *x, int i, int j) {
+  auto inner = [&](int ii, int jj) {
+    const size_t o = NPOM_I2(c, ii, jj);
+    const float fsm = F2(fsm, ii, jj);
+    if (c.tide[o] != 0.0f) return c.k.obc_jzb ? policy_tide(c, o) * fsm : policy_tide(c, o);
+    float v = ld(x + o) + policy_lift(c, ii, jj);
+    if (c.k.obc_jzb) v = v * fsm;
+    return interior(c, ii, jj) ? v * fsm : v;
+  };
+  if (c.k.obc_jzb) {
+    const int si = i == 0 ? 1 : (i == c.im - 1 ? c.im - 2 : i);
+    const int sj = j == 0 ? 1 : (j == c.jm - 1 ? c.jm - 2 : j);
+    return inner(si, sj) * F2(fsm, i, j);
+  }
+  return inner(i, j) * F2(fsm, i, j);
 }
 
 // The coastal tide policy's drag coefficient (coastal_compat.py:4-11):

@@ -13,6 +13,12 @@ constexpr int KMAX = 64;  // largest kb the column bodies accept
 
 NPOM_HD bool is_explicit(const Ctx &c) { return c.k.core == NPOM_CORE_EXPLICIT; }
 
+// bcond 3-6 in the explicit core's form: the explicit core, and the
+// semi-implicit core under the coastal or Jiaozhou Bay tide policy, whose
+// boundary hands indices 3-6 to the explicit step copy's bcond
+// (case_adapters/coastal_boundary.py:29, jzb_boundary.py:142)
+NPOM_HD bool explicit_bc(const Ctx &c) { return is_explicit(c) || c.k.obc_coastal; }
+
 // ---------------------------------------------------------------------------
 // B1 (column): u/v barotropic fix (explicit time_loop.py:440-477).
 // ---------------------------------------------------------------------------
@@ -445,7 +451,7 @@ NPOM_HD void phase_b4_point(const Ctx &c, int i, int j, int k) {
     // /columns, and the corner sources are edge-free by construction).
     arr[NPOM_I3(c, i, j, k)] = val;
   }
-  if (!is_explicit(c)) return;
+  if (!explicit_bc(c)) return;
   if (c.k.obc_seamount) {
     // the seamount policy's bcond 6 (seamount_boundary.py:40-42): 1e-10 on
     // the east and west edges (B5 then applies uf * fsm + 1e-10)
@@ -566,7 +572,7 @@ NPOM_HD void phase_b5_filter(const Ctx &c, int i, int j, int k) {
   // bcond 6 mask (explicit adds 1e-10)
   float uf6 = F3(uf, i, j, k) * fsm;
   float vf6 = F3(vf, i, j, k) * fsm;
-  if (is_explicit(c)) {
+  if (explicit_bc(c)) {
     uf6 = uf6 + 1.0e-10f;
     vf6 = vf6 + 1.0e-10f;
   }
@@ -728,7 +734,7 @@ NPOM_HD void phase_b6_column(const Ctx &c, int i, int j) {
   q.fsurf = F2(ssurf, i, j);
   float dh = proft_column<KM>(q);
   P2(tps, i, j) = dh;
-  if (is_explicit(c) && !c.k.obc_seamount && (i == 0 || i == c.im - 1 || j == 0 || j == c.jm - 1))
+  if (explicit_bc(c) && !c.k.obc_seamount && (i == 0 || i == c.im - 1 || j == 0 || j == c.jm - 1))
     bcond4_explicit_edge(c, i, j, ufc, vfc);
 }
 
@@ -853,7 +859,7 @@ NPOM_HD void phase_b7_point(const Ctx &c, int i, int j, int k) {
   const float *vfa = c.F[NPOM_F_vf];
   float ufv, vfv;
   bool edge = (i == 0 || i == im - 1 || j == 0 || j == jm - 1);
-  if (is_explicit(c)) {
+  if (explicit_bc(c)) {
     ufv = F3(uf, i, j, k) * fsm;
     vfv = F3(vf, i, j, k) * fsm;
   } else {
@@ -1114,7 +1120,7 @@ NPOM_HD void phase_b8_column(const Ctx &c, int i, int j) {
   profuv_column(c, 1, i, j, fin, vo, wvb, tpsv);
   if (c.k.obc_jzb) {
     for (int k = 0; k < kb; ++k) jzb_bcond3_level(c, i, j, k, uo[k], vo[k]);
-  } else if (is_explicit(c) && !c.k.obc_seamount) {
+  } else if (explicit_bc(c) && !c.k.obc_seamount) {
     bcond3_explicit_edge(c, i, j, uo, vo);
   }
   for (int k = 0; k < kb; ++k) {
@@ -1145,7 +1151,7 @@ NPOM_HD void phase_b9_column(const Ctx &c, int i, int j) {
       float fnew[KMAX], term[KMAX];
       for (int k = 0; k < kb; ++k) {
         float x = ld(ff + NPOM_I3(c, i, j, k)) * mask;
-        if (!is_explicit(c) && ring) x = 0.0f;
+        if (!explicit_bc(c) && ring) x = 0.0f;
         fnew[k] = x;
       }
       float tps = 0.0f;

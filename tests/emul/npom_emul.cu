@@ -184,6 +184,74 @@ void pcg(const Ctx &c, int step, int with_rhs, int with_post) {
   });
 }
 
+// the tide policies' free-surface solve (k_cg_policy), sequentially
+void cg_policy(const Ctx &c, int step) {
+  const int im = c.im, jm = c.jm;
+  float *x = c.W[NPOM_W_x], *r = c.W[NPOM_W_r], *p = c.W[NPOM_W_p], *ap = c.W[NPOM_W_ap];
+  float *rhs = c.W[NPOM_W_rhs], *lift = c.W[NPOM_W_zv];
+  each_cell(c, [&](int i, int j) {
+    const size_t q = NPOM_I2(c, i, j);
+    rhs[q] = rhs_cell(c, i, j);
+    lift[q] = policy_lift(c, i, j);
+  });
+  each_cell(c, [&](int i, int j) {
+    P2(fluxua, i, j) = rhs_fluxua(c, i, j);
+    P2(fluxva, i, j) = rhs_fluxva(c, i, j);
+  });
+  auto wdot = [&](const float *a, const float *b) {
+    double s = 0.0;
+    for (int i = 0; i < im; ++i)
+      for (int j = 0; j < jm; ++j) {
+        const size_t q = NPOM_I2(c, i, j);
+        const float w = policy_fixed(c, i, j) ? 0.0f : F2(art, i, j);
+        s += (double)(w * a[q]) * (double)b[q];
+      }
+    return s;
+  };
+  each_cell(c, [&](int i, int j) {
+    const size_t q = NPOM_I2(c, i, j);
+    const float b = policy_fixed(c, i, j) ? 0.0f : rhs[q] - elliptic_apply_cell(c, lift, i, j);
+    x[q] = 0.0f;
+    r[q] = b;
+    p[q] = b;
+  });
+  double rr = wdot(r, r);
+  const double thr = std::max(1e-30, rr * 1e-24);
+  const int nmax = std::min(c.k.eta_max_iter, 500);
+  int its = nmax;
+  for (int it = 0; it < nmax; ++it) {
+    if (rr <= thr) {
+      its = it + 1;
+      break;
+    }
+    each_cell(c, [&](int i, int j) {
+      ap[NPOM_I2(c, i, j)] = policy_fixed(c, i, j) ? 0.0f : elliptic_apply_cell(c, p, i, j);
+    });
+    const float alpha = (float)(rr / (wdot(p, ap) + 1e-40));
+    each_cell(c, [&](int i, int j) {
+      const size_t q = NPOM_I2(c, i, j);
+      x[q] = x[q] + alpha * p[q];
+      r[q] = r[q] - alpha * ap[q];
+    });
+    const double nw = wdot(r, r);
+    const float beta = (float)(nw / (rr + 1e-40));
+    each_cell(c, [&](int i, int j) {
+      const size_t q = NPOM_I2(c, i, j);
+      p[q] = r[q] + beta * p[q];
+    });
+    rr = nw;
+  }
+  c.cg_iters[step] = its;
+  std::vector<float> e((size_t)im * jm);
+  each_cell(c, [&](int i, int j) { e[NPOM_I2(c, i, j)] = policy_elf(c, x, i, j); });
+  std::memcpy(c.F[NPOM_F_elf], e.data(), e.size() * sizeof(float));
+}
+
+void policy_lines(const Ctx &c, int which) {
+  if (!c.k.obc_coastal || c.k.obc_jzb) return;
+  for (int t = 0; t < c.jm + c.im; ++t) policy_bc2_line(c, t, which);
+}
+
 void subcycle(const Ctx &c) {
   for (int iext = 1; iext <= c.k.isplit; ++iext) {
     bool adv = (iext % c.k.ispadv) == 0;
@@ -199,19 +267,29 @@ void run_phase(const Ctx &c, const npom_params *p, int phase) {
   switch (phase) {
     case 0: a1(c); break;
     case 1: each_cell(c, [&](int i, int j) { phase_a2_column(c, i, j); }); break;
-    case 2: each_cell(c, [&](int i, int j) { phase_a3_cell(c, i, j); }); break;
+    case 2:
+      each_cell(c, [&](int i, int j) { phase_a3_cell(c, i, j); });
+      if (p->core == NPOM_CORE_IMPLICIT) policy_lines(c, 0);
+      break;
     case 3:
       if (p->core == NPOM_CORE_IMPLICIT) {
         each_cell(c, [&](int i, int j) { elliptic_coeff_cell(c, i, j); });
-        pcg(c, 0, 1, 1);
+        if (c.k.obc_coastal) cg_policy(c, 0);
+        else pcg(c, 0, 1, 1);
       } else {
         subcycle(c);
       }
       break;
     case 4:
+      if (c.k.obc_coastal && p->core == NPOM_CORE_IMPLICIT) {
+        each_cell(c, [&](int i, int j) { phase_i5a_cell(c, i, j); });
+        policy_lines(c, 1);
+      }
       each_cell(c, [&](int i, int j) {
         if (phase_i5_cell(c, i, j)) *c.status |= NPOM_DEV_VMAX;
       });
+      if (c.k.obc_coastal && p->core == NPOM_CORE_IMPLICIT)
+        each_cell(c, [&](int i, int j) { cbc_coastal_cell(c, i, j); });
       break;
     case 5: each_cell(c, [&](int i, int j) { phase_b1_column(c, i, j); }); break;
     case 6: each_cell(c, [&](int i, int j) { phase_b2a_column(c, i, j); }); break;
@@ -463,12 +541,13 @@ int emul_steps(const npom_params *p, float *const *fields, const npom_workspace 
     double time = p->dti * iint * 1.0 / 86400.0 + clk->time0;
     c.ramp = ramp_of(p, time);
     c.do_internal = ((iint != 1 || clk->time0 != 0.0) && p->mode != 2) ? 1 : 0;
-    c.tide_t0 = time * 86400.0 - p->dti;
+    c.tide_t0 = time * 86400.0 - (p->core == NPOM_CORE_IMPLICIT ? p->dte : p->dti);
     run_phase(c, p, 0);
     run_phase(c, p, 1);
     run_phase(c, p, 2);
     if (p->core == NPOM_CORE_IMPLICIT) {
-      pcg(c, n, 1, 1);
+      if (c.k.obc_coastal) cg_policy(c, n);
+      else pcg(c, n, 1, 1);
       wrap_x(c);
       run_phase(c, p, 4);
     } else {

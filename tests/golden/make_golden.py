@@ -420,32 +420,36 @@ def make_seamount_golden(im=24, jm=18, seed=71, steps=(1, 3)):
     make_step_golden("explicit", im, jm, seed, steps=steps, core=core, tag="seamount_explicit")
 
 
-def make_coastal_policy_golden(im=24, jm=18, steps=(1, 3)):
-    """The explicit core under the reference's coastal tide policy, set up
-    the way its registry does (cores/case_adapters/registry.py:136-146: the
-    policy's step copies bound as methods, coastal_boundary.install with a
-    tide table file, coastal_compat.install with the POM08-WAD closure) on
+def make_coastal_policy_golden(im=24, jm=18, steps=(1, 3), family="explicit"):
+    """The explicit (or semi-implicit) core under the reference's coastal
+    tide policy, set up the way its registry does (cores/case_adapters/
+    registry.py:136-146: alpha and smoth of the family, the policy's step
+    copies bound as methods, coastal_boundary.install with a tide table
+    file, coastal_compat.install with the POM08-WAD closure) on
     ``cases.tidal_inlet`` (kb = 16), clock at 0.25 day; one internal step
     per call with the tide substep counter reset, as the registry's
-    advancement does (registry.py:38-63); 1 and 3 steps."""
+    advancement does (registry.py:38-63); 1 and 3 steps.  The registry
+    would refuse a float32 state; the steps run in float32, the arithmetic
+    the B200 step restates."""
     import tempfile
     import torch
     from importlib import import_module
     sys.path.insert(0, ROOT)
     from neuralpom_b200 import cases
     from neuralpom.cores.case_adapters import coastal_boundary, coastal_compat, registry
-    A, Sc = cases.tidal_inlet(im, jm, kb=16)
+    name = "explicit" if family == "explicit" else "implicit_p0_fixed"
+    A, Sc = cases.tidal_inlet(im, jm, kb=16, core=name)
     Sc = dict(Sc, time=0.25, time0=0.25)
-    core = rh.build_reference_core("explicit", im, jm)
+    core = rh.build_reference_core(name, im, jm)
     rh.load_state(core, {k: v for k, v in A.items() if hasattr(core, k)}, Sc)
-    core.alpha, core.smoth = 0.225, 0.1
+    core.alpha, core.smoth = (0.225, 0.1) if family == "explicit" else (0.333, 0.15)
     for module, cls in (("momentum", "MomentumMixin"), ("tracers", "TracersMixin"), ("time_loop", "TimeLoopMixin")):
-        registry._bind_mixin(core, getattr(import_module(f"neuralpom.cores.case_adapters.kernels.coastal_explicit_{module}"),
-                                           cls))
+        registry._bind_mixin(core, getattr(import_module(
+            f"neuralpom.cores.case_adapters.kernels.coastal_{family}_{module}"), cls))
     with tempfile.TemporaryDirectory() as tmp:
         path = os.path.join(tmp, "tide.dat")
         np.savetxt(path, np.c_[A["tide_i"] + 1, A["tide_j"] + 1, A["tide_amp"], A["tide_phase"]])
-        coastal_boundary.install(core, "explicit", path)
+        coastal_boundary.install(core, family, path)
     coastal_compat.install(core)
     torch.set_default_dtype(torch.float32)
     core.profq_form, core.zsh, core.obc_form = "pom08", 0.01, "coastal"
@@ -458,22 +462,26 @@ def make_coastal_policy_golden(im=24, jm=18, steps=(1, 3)):
     for n in steps:
         while done < n:
             core._tide_substep = 0
-            rh.advance(core, "explicit", 1)
+            rh.advance(core, name, 1)
             done += 1
         a, _ = rh.extract_state(core)
         for f in OUTPUT_FIELDS:
             out[f"out{n}__{f}"] = a[f]
         out[f"out{n}__cbc"] = a["cbc"]
         out[f"out{n}__scalar_time"] = np.asarray(float(core.time))
-    path = os.path.join(HERE, f"step_coastal_policy_{im}x{jm}.npz")
+        if family != "explicit":
+            out[f"out{n}__scalar_cg_iterations"] = np.asarray(int(core._validation_eta_iterations))
+    tag = "coastal_policy" if family == "explicit" else "coastal_policy_implicit"
+    path = os.path.join(HERE, f"step_{tag}_{im}x{jm}.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path))
 
 
-def make_jzb_policy_golden(im=24, jm=18, steps=(1, 3)):
-    """The explicit core under the reference's Jiaozhou Bay tide policy, set
-    up the way its registry does (cores/case_adapters/registry.py:147-156:
-    the coastal step copies bound as methods, jzb_boundary.install with a
+def make_jzb_policy_golden(im=24, jm=18, steps=(1, 3), family="explicit"):
+    """The explicit (or semi-implicit) core under the reference's Jiaozhou
+    Bay tide policy, set up the way its registry does (cores/case_adapters/
+    registry.py:147-156: alpha and smoth of the family, the coastal step
+    copies of the family bound as methods, jzb_boundary.install with a
     tide table file, jzb_compat.install with the POM08-WAD closure) on
     ``cases.bay`` (kb = 16), clock at 0.25 day (ramp 0.083 of the bay's
     3-day ramp); one internal step per call with the tide substep counter
@@ -485,18 +493,19 @@ def make_jzb_policy_golden(im=24, jm=18, steps=(1, 3)):
     sys.path.insert(0, ROOT)
     from neuralpom_b200 import cases
     from neuralpom.cores.case_adapters import jzb_boundary, jzb_compat, registry
-    A, Sc = cases.bay(im, jm, kb=16)
+    name = "explicit" if family == "explicit" else "implicit_p0_fixed"
+    A, Sc = cases.bay(im, jm, kb=16, core=name)
     Sc = dict(Sc, time=0.25, time0=0.25)
-    core = rh.build_reference_core("explicit", im, jm)
+    core = rh.build_reference_core(name, im, jm)
     rh.load_state(core, {k: v for k, v in A.items() if hasattr(core, k) and k != "period"}, Sc)
-    core.alpha, core.smoth = 0.225, 0.1
+    core.alpha, core.smoth = (0.225, 0.1) if family == "explicit" else (0.333, 0.15)
     for module, cls in (("momentum", "MomentumMixin"), ("tracers", "TracersMixin"), ("time_loop", "TimeLoopMixin")):
-        registry._bind_mixin(core, getattr(import_module(f"neuralpom.cores.case_adapters.kernels.coastal_explicit_{module}"),
-                                           cls))
+        registry._bind_mixin(core, getattr(import_module(
+            f"neuralpom.cores.case_adapters.kernels.coastal_{family}_{module}"), cls))
     with tempfile.TemporaryDirectory() as tmp:
         path = os.path.join(tmp, "tide.dat")
         np.savetxt(path, np.c_[A["tide_i"] + 1, A["tide_j"] + 1, A["tide_amp"], A["tide_phase"]])
-        jzb_boundary.install(core, "explicit", path)
+        jzb_boundary.install(core, family, path)
     jzb_compat.install(core)
     torch.set_default_dtype(torch.float32)
     core.profq_form, core.zsh, core.obc_form = "pom08", 0.01, "jzb"
@@ -509,14 +518,17 @@ def make_jzb_policy_golden(im=24, jm=18, steps=(1, 3)):
     for n in steps:
         while done < n:
             core._tide_substep = 0
-            rh.advance(core, "explicit", 1)
+            rh.advance(core, name, 1)
             done += 1
         a, _ = rh.extract_state(core)
         for f in OUTPUT_FIELDS:
             out[f"out{n}__{f}"] = a[f]
         out[f"out{n}__cbc"] = a["cbc"]
         out[f"out{n}__scalar_time"] = np.asarray(float(core.time))
-    path = os.path.join(HERE, f"step_jzb_policy_{im}x{jm}.npz")
+        if family != "explicit":
+            out[f"out{n}__scalar_cg_iterations"] = np.asarray(int(core._validation_eta_iterations))
+    tag = "jzb_policy" if family == "explicit" else "jzb_policy_implicit"
+    path = os.path.join(HERE, f"step_{tag}_{im}x{jm}.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path))
 
@@ -550,7 +562,7 @@ def make_pom08_goldens():
 
 
 def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint", "coupling", "mpdata", "pom08", "seamount",
-                "shapiro", "jzb")):
+                "shapiro", "jzb", "coastal_implicit")):
     src = rh.default_reference_path()
     if src is None:
         raise SystemExit("reference sources not found; set NPOM_REFERENCE_SRC")
@@ -584,8 +596,11 @@ def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint", "couplin
         make_shapiro_golden()
     if "jzb" in which:
         make_jzb_policy_golden()
+    if "coastal_implicit" in which:
+        make_coastal_policy_golden(family="implicit")
+        make_jzb_policy_golden(family="implicit")
 
 
 if __name__ == "__main__":
     main(tuple(sys.argv[1:]) or ("proft", "steps", "adjoint", "coastal", "step_adjoint", "coupling", "mpdata",
-                                 "pom08", "seamount", "shapiro", "jzb"))
+                                 "pom08", "seamount", "shapiro", "jzb", "coastal_implicit"))

@@ -83,10 +83,12 @@ def test_boundary_policy_reaches_npom_params():
     with pytest.raises(ValueError):
         state.make_params(dict(state.default_scalars("implicit_p0_fixed"), obc_form="seamount"), 24, 18, 16,
                           "implicit_p0_fixed")
-    # the coastal and Jiaozhou Bay tide policies, explicit core only
+    # the coastal and Jiaozhou Bay tide policies on either core (the
+    # semi-implicit one with its Shapiro filter off)
     for form, code in (("coastal", _abi.OBC_COASTAL), ("jzb", _abi.OBC_JZB)):
-        assert state.make_params(dict(state.default_scalars("explicit"), obc_form=form), 24, 18, 16,
-                                 "explicit").obc_form == code
+        for core in ("explicit", "implicit_p0_fixed"):
+            assert state.make_params(dict(state.default_scalars(core), obc_form=form), 24, 18, 16,
+                                     core).obc_form == code
         with pytest.raises(ValueError):
-            state.make_params(dict(state.default_scalars("implicit_p0_fixed"), obc_form=form), 24, 18, 16,
-                              "implicit_p0_fixed")
+            state.make_params(dict(state.default_scalars("implicit_p0_fixed"), obc_form=form,
+                                   barotropic_shapiro=0.05), 24, 18, 16, "implicit_p0_fixed")

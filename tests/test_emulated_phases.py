@@ -24,6 +24,9 @@ STEP_FILES = [("step_explicit_12x10.npz", "explicit"), ("step_implicit_12x10.npz
               ("step_coastal_policy_24x18.npz", "explicit"),
               # the reference's Jiaozhou Bay tide policy (its boundary, the coastal step copies, closure)
               ("step_jzb_policy_24x18.npz", "explicit"),
+              # both tide policies on the semi-implicit core (their own area-weighted CG)
+              ("step_coastal_policy_implicit_24x18.npz", "implicit_p0_fixed"),
+              ("step_jzb_policy_implicit_24x18.npz", "implicit_p0_fixed"),
               ("step_implicit_shapiro_20x18.npz", "implicit_p0_fixed")]
 
 
@@ -42,6 +45,9 @@ def test_emulated_step_matches_reference(fname, core):
             assert err < bound, (fname, n, f, err)
         if "cg_iters" in OUT[n]:
             assert [int(v) for v in its] == [int(v) for v in OUT[n]["cg_iters"]]
+        if "scalar_cg_iterations" in OUT[n]:
+            # the tide policies' solve count of the last step
+            assert int(its[-1]) == int(OUT[n]["scalar_cg_iterations"])
 
 
 def _case(name):

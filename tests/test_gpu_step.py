@@ -20,6 +20,9 @@ STEP_FILES = [("step_explicit_12x10.npz", "explicit"), ("step_implicit_12x10.npz
               ("step_coastal_policy_24x18.npz", "explicit"),
               # the reference's Jiaozhou Bay tide policy
               ("step_jzb_policy_24x18.npz", "explicit"),
+              # both tide policies on the semi-implicit core
+              ("step_coastal_policy_implicit_24x18.npz", "implicit_p0_fixed"),
+              ("step_jzb_policy_implicit_24x18.npz", "implicit_p0_fixed"),
               # the semi-implicit core with its spatial Shapiro filters on (gamma 0.05)
               ("step_implicit_shapiro_20x18.npz", "implicit_p0_fixed")]
 
@@ -49,6 +52,9 @@ def test_gpu_step_matches_reference_golden(fname, core):
             assert err < bound, (fname, n, f, err)
         if "cg_iters" in OUT[n]:
             assert c._eta_solver_iteration_history == [int(v) for v in OUT[n]["cg_iters"]]
+        if "scalar_cg_iterations" in OUT[n]:
+            # the tide policies' own solve: the reference's count at the last step
+            assert c._eta_solver_iteration_history[-1] == int(OUT[n]["scalar_cg_iterations"])
         assert abs(c.time - float(OUT[n]["scalar_time"])) < 1e-9
 
 
@@ -270,7 +276,8 @@ def test_gpu_restart_continues_bitwise(tmp_path):
 
 
 @pytest.mark.parametrize("fname", ["step_pom08_explicit_12x10.npz", "step_seamount_explicit_24x18.npz",
-                                   "step_coastal_policy_24x18.npz", "step_jzb_policy_24x18.npz"])
+                                   "step_coastal_policy_24x18.npz", "step_jzb_policy_24x18.npz",
+                                   "step_coastal_policy_implicit_24x18.npz"])
 def test_gpu_case_policies_refuse_gradients(fname):
     """The case policies advance forward only, as the reference's registry
     requires (cores/case_adapters/registry.py:38-41)."""
