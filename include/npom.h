@@ -96,6 +96,9 @@ typedef struct npom_workspace {
   float *tide;             /* NPOM_OBC_COASTAL only (else may be null):    */
                            /* 3 planes of im*jm: 1 at tide cells, their   */
                            /* amplitude (m) and phase (degrees)           */
+  double *robin;           /* NPOM_OBC_SEAMOUNT on the semi-implicit core  */
+                           /* only (else may be null): 5 * im*jm doubles  */
+                           /* of the FP64 Robin solve                     */
 } npom_workspace;
 
 #define NPOM_MAX_COOP_BLOCKS 1024
@@ -168,6 +171,15 @@ enum { NPOM_PROFQ_PRODUCTION = 0, NPOM_PROFQ_POM08 = 1 };
  * edges; the north and south edges are walls.  Forward only (the reference
  * refuses gradients through its case policies). */
 enum { NPOM_OBC_NATIVE = 0, NPOM_OBC_SEAMOUNT = 1, NPOM_OBC_COASTAL = 2, NPOM_OBC_JZB = 3 };
+/* SEAMOUNT on the semi-implicit core (barotropic_shapiro 0; the Robin
+ * solve's FP64 planes in npom_workspace.robin): the policy's predictor
+ * (the incident transport on the east and west edges), its free-surface
+ * solve -- Picard iterations on the boundary depth around a CG with the
+ * characteristic (Robin) flux of the east and west edges in the operator,
+ * in FP64 (its 1e-11 m Picard test is a float64 criterion) -- its
+ * corrector with the old and new face depths and the edge radiation, the
+ * body continuity that rewrites utf, vtf and etf after the filter
+ * (seamount_boundary.py:45-147), and its bcond 1 and 3-6. */
 /* COASTAL and JZB on the semi-implicit core (barotropic_shapiro 0): the
  * policy's step copy (the old depth in the corrector's pressure-gradient
  * transport, cbc after the filter), its bcond 2 on u* and on the corrected

@@ -95,7 +95,7 @@ class NpomParams(ctypes.Structure):
 class NpomWorkspace(ctypes.Structure):
     _fields_ = [("buf", ctypes.c_void_p * len(WS_NAMES)), ("partials", ctypes.c_void_p),
                 ("sync", ctypes.c_void_p), ("status", ctypes.c_void_p), ("cg_iters", ctypes.c_void_p),
-                ("mp3d", ctypes.c_void_p), ("tide", ctypes.c_void_p)]
+                ("mp3d", ctypes.c_void_p), ("tide", ctypes.c_void_p), ("robin", ctypes.c_void_p)]
 
 
 class NpomClock(ctypes.Structure):

@@ -364,7 +364,7 @@ def coastal_tide(im=354, jm=322, kb=16, dte=2.0, isplit=30, dx=500.0, seed=4, la
     return finish_initialization(A, s, core)
 
 
-def seamount_policy(A, s):
+def seamount_policy(A, s, core="explicit"):
     """The seamount case policy's set-up on a state (cores/case_adapters/
     seamount_runtime.py:6-25): the exterior elevations, transports and T/S
     profiles taken from the current state's edge rows and columns, rf = 1,
@@ -378,20 +378,21 @@ def seamount_policy(A, s):
     for key, name, axis, index in (("tbe", "t", 0, -1), ("tbw", "t", 0, 0), ("sbe", "s", 0, -1), ("sbw", "s", 0, 0),
                                    ("tbn", "t", 1, -1), ("tbs", "t", 1, 0), ("sbn", "s", 1, -1), ("sbs", "s", 1, 0)):
         A[key] = np.ascontiguousarray(A[name][index, :, :] if axis == 0 else A[name][:, index, :]).copy()
-    s = dict(s, rfe=1.0, rfw=1.0, rfn=1.0, rfs=1.0, alpha=0.225, smoth=0.1, profq_form="pom08", zsh=0.01,
+    alpha, smoth = (0.225, 0.1) if core == "explicit" else (0.333, 0.15)
+    s = dict(s, rfe=1.0, rfw=1.0, rfn=1.0, rfs=1.0, alpha=alpha, smoth=smoth, profq_form="pom08", zsh=0.01,
              obc_form="seamount")
     return A, s
 
 
-def open_seamount(im=65, jm=49, kb=16, dte=5.0, isplit=30, dx=5.0e3, u0=0.1, lat=40.0):
+def open_seamount(im=65, jm=49, kb=16, dte=5.0, isplit=30, dx=5.0e3, u0=0.1, lat=40.0, core="explicit"):
     """Explicit seamount with open east and west edges, the geometry the
     seamount case policy serves (registered at 65x49x16 with dtE/dtI = 5/150
     s): flat 4500 m with a Gaussian seamount (height 4000 m, e-folding 25
     km) at the centre, dx = dy, walls on the north and south edges, water
     on the east and west edges, T = 10 + 10 exp(z/1000 m), S = 35, uniform
     inflow u0, f-plane at ``lat``, no wind; with ``seamount_policy``
-    applied."""
-    core = "explicit"
+    applied.  ``core`` "implicit_p0_fixed" gives the semi-implicit core's
+    scalars (dti = dte * isplit)."""
     s = state.default_scalars(core)
     s.update(dte=dte, isplit=isplit, hmax=4500.0)
     state.derived_time(s)
@@ -413,7 +414,7 @@ def open_seamount(im=65, jm=49, kb=16, dte=5.0, isplit=30, dx=5.0e3, u0=0.1, lat
     A["ub"][:, :, : kb - 1] = F32(u0) * A["dum"][:, :, None]
     A["uab"][:] = F32(u0) * A["dum"]
     A, s = finish_initialization(A, s, core)
-    return seamount_policy(A, s)
+    return seamount_policy(A, s, core=core)
 
 
 def coastal_policy(A, s, tide_i, tide_j, tide_amp, tide_phase, core="explicit"):

@@ -133,6 +133,11 @@ class B200Core:
                                                  for n in ("tide_i", "tide_j", "tide_amp", "tide_phase")))
             self._ws["tide"] = torch.from_numpy(planes).to(dev).contiguous()
             self._ws["struct"].tide = self._ws["tide"].data_ptr()
+        if (str(getattr(self, "obc_form", "native")).lower() == "seamount" and self.core_name != "explicit"
+                and "robin" not in self._ws):
+            # the semi-implicit seamount policy's FP64 Robin solve: 5 planes
+            self._ws["robin"] = torch.zeros(5 * im * jm, dtype=torch.float64, device=dev)
+            self._ws["struct"].robin = self._ws["robin"].data_ptr()
         if int(getattr(self, "nadv", 1)) == 2 and "mp3d" not in self._ws:
             # MPDATA scratch: mass fluxes and fluxes of T and S
             self._ws["mp3d"] = torch.zeros(12 * im * jm * self.kb, dtype=torch.float32, device=dev)

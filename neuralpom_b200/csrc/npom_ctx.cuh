@@ -48,8 +48,9 @@ struct Consts {
   int profq_pom08;     // PROFQ in the POM08-WAD form
   float kappa_zsh;     // POM08-WAD: kappa * zsh (folded in double)
   int obc_seamount;    // the seamount case policy's boundary (explicit core)
-  int obc_coastal;     // the coastal tide policy's machinery (explicit core; also set for JZB)
-  int obc_jzb;         // the Jiaozhou Bay tide policy (explicit core)
+  int obc_coastal;     // the coastal tide policy's machinery (also set for JZB)
+  int obc_jzb;         // the Jiaozhou Bay tide policy
+  int sea_implicit;    // the seamount policy on the semi-implicit core
   int periodic_x;      // periodic x: two halo columns each side, unique columns 2..im-3
   double tide_w;       // tide angular speed, rad/h, as the policy writes it
   double dte_d;        // dte in double (tide time of a substep)
@@ -67,6 +68,7 @@ struct Ctx {
   int *cg_iters;
   float *mp3d;  // MPDATA scratch (nadv 2)
   const float *tide;  // coastal policy: tide flag, amplitude, phase planes
+  double *robin;      // semi-implicit seamount policy: the FP64 Robin solve's planes
   double tide_t0;     // coastal policy: seconds at the start of the step
   Consts k;
   int coh;         // 1: loads bypass L1 (persistent cooperative kernels)

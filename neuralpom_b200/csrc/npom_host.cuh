@@ -55,6 +55,7 @@ inline Consts make_consts(const npom_params &p) {
   k.obc_seamount = p.obc_form == NPOM_OBC_SEAMOUNT ? 1 : 0;
   k.obc_coastal = (p.obc_form == NPOM_OBC_COASTAL || p.obc_form == NPOM_OBC_JZB) ? 1 : 0;
   k.obc_jzb = p.obc_form == NPOM_OBC_JZB ? 1 : 0;
+  k.sea_implicit = (p.obc_form == NPOM_OBC_SEAMOUNT && p.core == NPOM_CORE_IMPLICIT) ? 1 : 0;
   k.periodic_x = p.periodic_x ? 1 : 0;
   // coastal_boundary.py:9-10: (29.03225806451612*3.1416/180) in double
   // the policies' M2 angular speeds (rad/h) as they write them
@@ -117,10 +118,10 @@ inline bool check_args(const npom_params *p, float *const *fields, const npom_wo
   // installers set it)
   const bool tide_policy = p->obc_form == NPOM_OBC_COASTAL || p->obc_form == NPOM_OBC_JZB;
   if (p->obc_form != NPOM_OBC_NATIVE &&
-      ((p->obc_form != NPOM_OBC_SEAMOUNT && !tide_policy) ||
-       (p->obc_form == NPOM_OBC_SEAMOUNT && p->core != NPOM_CORE_EXPLICIT) || p->im < 6 || p->jm < 6 ||
+      ((p->obc_form != NPOM_OBC_SEAMOUNT && !tide_policy) || p->im < 6 || p->jm < 6 ||
        (tide_policy && !ws->tide) ||
-       (tide_policy && p->core == NPOM_CORE_IMPLICIT && p->barotropic_shapiro != 0.0)))
+       (p->obc_form == NPOM_OBC_SEAMOUNT && p->core == NPOM_CORE_IMPLICIT && !ws->robin) ||
+       (p->core == NPOM_CORE_IMPLICIT && p->barotropic_shapiro != 0.0)))
     return false;
   if (p->periodic_x &&
       (p->periodic_x != 1 || p->core != NPOM_CORE_IMPLICIT || p->obc_form != NPOM_OBC_NATIVE || p->nadv != 1 ||
@@ -145,6 +146,7 @@ inline Ctx make_ctx(const npom_params *p, float *const *fields, const npom_works
   c.cg_iters = ws->cg_iters;
   c.mp3d = ws->mp3d;
   c.tide = ws->tide;
+  c.robin = ws->robin;
   c.k = make_consts(*p);
   c.ramp = 1.0f;
   c.do_internal = 1;

@@ -759,6 +759,155 @@ __device__ __forceinline__ void cg_policy_body(const Ctx &c) {
 
 __global__ void __launch_bounds__(kThreads) k_cg_policy(Ctx c) { cg_policy_body(c); }
 
+// block-wide FP64 maximum of a non-negative value into partials[slot*G+b]
+__device__ void block_max(const Ctx &c, double a, int slot) {
+  __shared__ double red[kThreads / 32];
+  for (int off = 16; off > 0; off >>= 1) a = fmax(a, __shfl_down_sync(0xffffffffu, a, off));
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) red[w] = a;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t = fmax(t, red[q]);
+    c.partials[slot * vgrid(c) + vblock(c)] = t;
+  }
+  __syncthreads();
+}
+
+// maximum of one partial slot over blocks, identical in every block
+__device__ double grid_max(const Ctx &c, int slot) {
+  __shared__ double tot;
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (unsigned b = 0; b < vgrid(c); ++b) t = fmax(t, __ldcg(c.partials + slot * vgrid(c) + b));
+    tot = t;
+  }
+  __syncthreads();
+  const double r = tot;
+  __syncthreads();
+  return r;
+}
+
+// The seamount policy's free-surface solve on the semi-implicit core
+// (seamount_boundary.py:57-103), one cooperative launch in FP64 on the
+// robin planes (x, r, p, Ap, and the Picard guess G = ghost(x)): the step's
+// RHS and stored transports as the production solve sets them up; x0 = el
+// on the unknowns; up to 6 Picard iterations on the boundary depth, each a
+// CG (at most 300 iterations, stopping at the top of an iteration once
+// rr <= max(1e-28, 1e-22 rr0), rr0 = max(sum area b^2, 1e-40)) for the
+// Robin operator of that guess, warm-started from x; done when
+// max |ghost(x) - G| < 1e-11 m.  A non-positive or non-finite p.Ap sets
+// NPOM_DEV_NONFINITE and stops; Picard iterations that do not converge
+// set NPOM_DEV_PCG_MAXIT (the policy raises for both).  The CG iterations
+// of all Picard passes go to the iteration history.  Then elf (sea_elf);
+// the depth keeps its old value for the corrector.
+__device__ __forceinline__ void robin_picard_body(const Ctx &c) {
+  const int im = c.im, jm = c.jm;
+  const size_t ncell = (size_t)im * jm;
+  const size_t stride = (size_t)vgrid(c) * blockDim.x;
+  const size_t tid = (size_t)vblock(c) * blockDim.x + threadIdx.x;
+  double *X = c.robin, *R = c.robin + ncell, *P = c.robin + 2 * ncell, *AP = c.robin + 3 * ncell;
+  double *G = c.robin + 4 * ncell;
+  float *rhs = c.W[NPOM_W_rhs];
+  for (size_t q = tid; q < ncell; q += stride) {
+    const int i = (int)(q / jm), j = (int)(q % jm);
+    rhs[q] = rhs_cell(c, i, j);
+    P2(fluxua, i, j) = rhs_fluxua(c, i, j);
+    P2(fluxva, i, j) = rhs_fluxva(c, i, j);
+    X[q] = sea_free(c, i, j) ? (double)F2(el, i, j) : 0.0;
+  }
+  if (!grid_barrier(c)) return;
+  bool converged = false;
+  int total = 0;
+  for (int nl = 0; nl < 6 && !converged; ++nl) {
+    for (size_t q = tid; q < ncell; q += stride) G[q] = sea_ghost(c, X, (int)(q / jm), (int)(q % jm));
+    if (!grid_barrier(c)) return;
+    double rr = 0.0, bb = 0.0;
+    for (size_t q = tid; q < ncell; q += stride) {
+      const int i = (int)(q / jm), j = (int)(q % jm);
+      const double b = sea_rhs(c, rhs, G, i, j);
+      const double rv = b - sea_robin_op(c, X, G, i, j);
+      R[q] = rv;
+      P[q] = rv;
+      const double area = sea_free(c, i, j) ? (double)F2(art, i, j) : 0.0;
+      rr += area * rv * rv;
+      bb += area * b * b;
+    }
+    block_sum3(c, rr, bb, 0.0, 1, 2, -1);
+    if (!grid_barrier(c)) return;
+    rr = grid_total(c, 1);
+    const double rr0 = fmax(grid_total(c, 2), 1e-40);
+    const double thr = fmax(1e-28, rr0 * 1e-22);
+    for (int it = 0; it < 300; ++it) {
+      if (rr <= thr) break;
+      double den = 0.0;
+      for (size_t q = tid; q < ncell; q += stride) {
+        const int i = (int)(q / jm), j = (int)(q % jm);
+        const double a = sea_robin_op(c, P, G, i, j);
+        AP[q] = a;
+        const double area = sea_free(c, i, j) ? (double)F2(art, i, j) : 0.0;
+        den += area * __ldcg(P + q) * a;
+      }
+      block_sum3(c, den, 0.0, 0.0, 0, -1, -1);
+      if (!grid_barrier(c)) return;
+      den = grid_total(c, 0);
+      if (!(den > 0.0) || !(den < 1.0e308)) {
+        if (tid == 0) atomicOr(c.status, NPOM_DEV_NONFINITE);
+        return;
+      }
+      const double a = rr / den;
+      double nw = 0.0;
+      for (size_t q = tid; q < ncell; q += stride) {
+        const int i = (int)(q / jm), j = (int)(q % jm);
+        X[q] = __ldcg(X + q) + a * __ldcg(P + q);
+        const double rv = __ldcg(R + q) - a * __ldcg(AP + q);
+        R[q] = rv;
+        const double area = sea_free(c, i, j) ? (double)F2(art, i, j) : 0.0;
+        nw += area * rv * rv;
+      }
+      block_sum3(c, nw, 0.0, 0.0, 1, -1, -1);
+      if (!grid_barrier(c)) return;
+      nw = grid_total(c, 1);
+      const double beta = nw / fmax(rr, 1e-40);
+      for (size_t q = tid; q < ncell; q += stride) P[q] = __ldcg(R + q) + beta * __ldcg(P + q);
+      rr = nw;
+      ++total;
+      if (!grid_barrier(c)) return;
+    }
+    double change = 0.0;
+    for (size_t q = tid; q < ncell; q += stride) {
+      const int i = (int)(q / jm), j = (int)(q % jm);
+      change = fmax(change, fabs(sea_ghost(c, X, i, j) - __ldcg(G + q)));
+    }
+    block_max(c, change, 3);
+    if (!grid_barrier(c)) return;
+    converged = grid_max(c, 3) < 1e-11;
+  }
+  if (tid == 0) {
+    unsigned int slot = c.sync[2];
+    c.cg_iters[slot] = total;
+    c.sync[2] = slot + 1;
+    if (!converged) atomicOr(c.status, NPOM_DEV_PCG_MAXIT);
+  }
+  for (size_t q = tid; q < ncell; q += stride) {
+    const int i = (int)(q / jm), j = (int)(q % jm);
+    const float e = sea_elf(c, X, i, j);
+    if (!(fabsf(e) <= 3.0e38f)) atomicOr(c.status, NPOM_DEV_NONFINITE);
+    P2(elf, i, j) = e;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_robin_picard(Ctx c) { robin_picard_body(c); }
+
+// the seamount policy's body continuity: the transports, then etf
+__global__ void __launch_bounds__(kThreads) k_sea_continuity(Ctx c, int which) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= c.im * c.jm) return;
+  const int i = q / c.jm, j = q % c.jm;
+  if (which == 0) sea_transport_cell(c, i, j);
+  else P2(etf, i, j) = sea_etf_cell(c, i, j);
+}
+
 // The coastal policy's bcond 2 lines (policy_bc2_line): jm + im lines
 __global__ void __launch_bounds__(kThreads) k_policy_bc2(Ctx c, int which) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1128,6 +1277,11 @@ cudaError_t plan_pcg(const Ctx &c, PcgPlan *plan) {
     plan->cluster = false;
     return coop_blocks((const void *)k_cg_policy, (size_t)c.im * c.jm, &plan->coop_blocks);
   }
+  if (c.k.sea_implicit) {
+    // the seamount policy's Robin / Picard solve (k_robin_picard)
+    plan->cluster = false;
+    return coop_blocks((const void *)k_robin_picard, (size_t)c.im * c.jm, &plan->coop_blocks);
+  }
   plan->cluster = pcg_cluster_layout(c, &plan->L) && ensure_cluster_attrs(plan->L) &&
                   cluster_launchable(pcg_cluster_fn(plan->L), plan->L.nc, plan->L.bytes());
   if (plan->cluster) return cudaSuccess;
@@ -1135,11 +1289,12 @@ cudaError_t plan_pcg(const Ctx &c, PcgPlan *plan) {
 }
 
 cudaError_t run_pcg(Ctx c, const PcgPlan &plan, int with_rhs, int with_post, cudaStream_t s) {
-  if (c.k.obc_coastal) {
-    // the policy solve always sets up its RHS and applies its bcond 1
+  if (c.k.obc_coastal || c.k.sea_implicit) {
+    // the policy solves always set up their RHS and apply their bcond 1
     c.coh = 1;
     void *args[] = {&c};
-    return launch_coop((const void *)k_cg_policy, plan.coop_blocks, args, c.sync, s);
+    return launch_coop(c.k.sea_implicit ? (const void *)k_robin_picard : (const void *)k_cg_policy,
+                       plan.coop_blocks, args, c.sync, s);
   }
   if (plan.cluster) return run_pcg_cluster(c, plan.L, with_rhs, with_post, s);
   c.coh = 1;
@@ -1400,18 +1555,21 @@ cudaError_t enqueue_step(const Ctx &c, int core, const PcgPlan &plan, int sub_bl
     e = run_pcg(c, plan, 1, 1, s);
     if (e != cudaSuccess) return e;
     launch_wrap_x(c, s);
-    if (c.k.obc_coastal) {
-      // the tide policies: corrector with bcond 2 first, then the filter
-      // and shifts, then cbc from the new depth (coastal_implicit_time_loop
-      // .py:351-352)
+    if (c.k.obc_coastal || c.k.sea_implicit) {
+      // the policies: corrector with bcond 2 first, then the filter and
+      // shifts; then the tide policies' cbc from the new depth
+      // (coastal_implicit_time_loop.py:351-352), the seamount policy's body
+      // continuity (seamount_boundary.py:26-42)
       launch_cells<XP_I5A>(c, s);
       launch_policy_bc2(c, 1, s);
     }
     launch_cells<XP_I5>(c, s);
     launch_wrap_x(c, s);
-    if (c.k.obc_coastal) {
-      const int n = c.im * c.jm;
-      k_cbc_coastal<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(c);
+    const int n2 = c.im * c.jm;
+    if (c.k.obc_coastal) k_cbc_coastal<<<(n2 + kThreads - 1) / kThreads, kThreads, 0, s>>>(c);
+    if (c.k.sea_implicit) {
+      k_sea_continuity<<<(n2 + kThreads - 1) / kThreads, kThreads, 0, s>>>(c, 0);
+      k_sea_continuity<<<(n2 + kThreads - 1) / kThreads, kThreads, 0, s>>>(c, 1);
     }
   } else {
     e = run_subcycle(c, sub_blocks, s);
@@ -1891,17 +2049,21 @@ npom_status npom_run_phase(const npom_params *p, float *const *fields, const npo
         if (e == cudaSuccess) e = run_subcycle(c, blocks, s);
       }
       break;
-    case 4:
-      if (c.k.obc_coastal && p->core == NPOM_CORE_IMPLICIT) {
+    case 4: {
+      const bool pol = (c.k.obc_coastal || c.k.sea_implicit) && p->core == NPOM_CORE_IMPLICIT;
+      if (pol) {
         launch_cells<XP_I5A>(c, s);
         launch_policy_bc2(c, 1, s);
       }
       launch_cells<XP_I5>(c, s);
-      if (c.k.obc_coastal && p->core == NPOM_CORE_IMPLICIT) {
-        const int n = c.im * c.jm;
-        k_cbc_coastal<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(c);
+      const int n = c.im * c.jm;
+      if (pol && c.k.obc_coastal) k_cbc_coastal<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(c);
+      if (pol && c.k.sea_implicit) {
+        k_sea_continuity<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(c, 0);
+        k_sea_continuity<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(c, 1);
       }
       break;
+    }
     case 5: launch_cols<CP_B1>(c, s); break;
     case 6: launch_cols<CP_B2A>(c, s); break;
     case 7: launch_points<PP_B2B>(c, s); break;

@@ -73,7 +73,23 @@ NPOM_HD void phase_a3_cell(const Ctx &c, int i, int j) {
     vs = vs * F2(dvm, i, j);
   }
   const bool ring = i == 0 || i == im - 1 || j == 0 || j == jm - 1;
-  if (c.k.obc_coastal) {
+  if (c.k.obc_seamount) {
+    // the seamount policy's predictor (seamount_boundary.py:86-92): the
+    // ring keeps the raw values (ua, va); the incident transport on the
+    // west edge (column 1 and its ghost 0) and the east edge, no v through
+    // them; then the masks
+    if (ring) {
+      us = F2(ua, i, j);
+      vs = F2(va, i, j);
+    }
+    if (j >= 1 && j <= jm - 2) {
+      if (i == 1 || i == 0) us = c.ramp * F1(uabw, j);
+      if (i == im - 1) us = c.ramp * F1(uabe, j);
+    }
+    if (i == 0 || i == im - 1) vs = 0.0f;
+    us = us * F2(dum, i, j);
+    vs = vs * F2(dvm, i, j);
+  } else if (c.k.obc_coastal) {
     // the tide policies' bcond 2 on u*, v* (coastal_boundary.py:23-29,
     // jzb_boundary.py:51-86): the ring keeps the predictor's raw values (ua,
     // va); the bay's Sommerfeld edges read only ua, va and d; the coastal
@@ -286,12 +302,48 @@ NPOM_HD void i5_uvaf(const Ctx &c, int i, int j, float &uaf, float &vaf) {
   }
 }
 
-// Phase I5a of the tide policies: the corrector with bcond 2 into uaf/vaf
-// (the coastal radiation's edges follow in policy_bc2_line); I5 then reads
-// them.  Reads ua, va, d and uaf, none of which it writes elsewhere.
+// The seamount policy's corrector (seamount_boundary.py:120-134): the
+// transport of the predictor's u*, v* at the old face depth plus the
+// implicit pressure gradient, divided by the new face depth (h + elf); row
+// and column 0 zero; the west edge (column 1 and its ghost 0) and the east
+// edge from the characteristic radiation about the exterior elevation;
+// then the masks.  The old depth is d, which the solve leaves alone.
+NPOM_HD void sea_corrector(const Ctx &c, int i, int j, float &uaf, float &vaf) {
+  const int im = c.im, jm = c.jm;
+  const float k2 = (float)(2.0 * (double)c.k.dti * (double)c.k.grav * (double)c.k.alpha);
+  uaf = 0.0f;
+  vaf = 0.0f;
+  if (i >= 1) {
+    const float hu = 0.5f * (F2(d, i, j) + F2(d, i - 1, j));
+    const float hun = 0.5f * ((F2(h, i, j) + F2(elf, i, j)) + (F2(h, i - 1, j) + F2(elf, i - 1, j)));
+    const float dxu = 0.5f * (F2(dx, i, j) + F2(dx, i - 1, j));
+    uaf = (hu * W2(us, i, j) - k2 * hu * (F2(elf, i, j) - F2(elf, i - 1, j)) / dxu) / hun;
+  }
+  if (j >= 1) {
+    const float hv = 0.5f * (F2(d, i, j) + F2(d, i, j - 1));
+    const float hvn = 0.5f * ((F2(h, i, j) + F2(elf, i, j)) + (F2(h, i, j - 1) + F2(elf, i, j - 1)));
+    const float dyv = 0.5f * (F2(dy, i, j) + F2(dy, i, j - 1));
+    vaf = (hv * W2(vs, i, j) - k2 * hv * (F2(elf, i, j) - F2(elf, i, j - 1)) / dyv) / hvn;
+  }
+  if (j >= 1 && j <= jm - 2) {
+    const float g = c.k.grav;
+    if (i == 1 || i == 0)
+      uaf = c.ramp * F1(uabw, j) - sqrtf(g / F2(h, 1, j)) * (F2(elf, 1, j) - F1(elw, j));
+    if (i == im - 1)
+      uaf = c.ramp * F1(uabe, j) + sqrtf(g / F2(h, im - 2, j)) * (F2(elf, im - 2, j) - F1(ele, j));
+  }
+  uaf = uaf * F2(dum, i, j);
+  vaf = vaf * F2(dvm, i, j);
+}
+
+// Phase I5a of the policies on the semi-implicit core: the corrector with
+// bcond 2 into uaf/vaf (the coastal radiation's edges follow in
+// policy_bc2_line); I5 then reads them.  Reads ua, va, d and uaf, none of
+// which it writes elsewhere.
 NPOM_HD void phase_i5a_cell(const Ctx &c, int i, int j) {
   float uaf, vaf;
-  i5_uvaf(c, i, j, uaf, vaf);
+  if (c.k.obc_seamount) sea_corrector(c, i, j, uaf, vaf);
+  else i5_uvaf(c, i, j, uaf, vaf);
   P2(uaf, i, j) = uaf;
   P2(vaf, i, j) = vaf;
 }
@@ -300,7 +352,7 @@ NPOM_HD bool phase_i5_cell(const Ctx &c, int i, int j) {
   const int im = c.im, jm = c.jm;
   const float elf0 = F2(elf, i, j);
   float uaf, vaf;
-  if (c.k.obc_coastal) {
+  if (c.k.obc_coastal || c.k.obc_seamount) {
     uaf = F2(uaf, i, j);
     vaf = F2(vaf, i, j);
   } else {
@@ -755,6 +807,137 @@ NPOM_HD float policy_elf(const Ctx &c, const float *x, int i, int j) {
     return inner(si, sj) * F2(fsm, i, j);
   }
   return inner(i, j) * F2(fsm, i, j);
+}
+
+// ---------------------------------------------------------------------------
+// The seamount policy on the semi-implicit core (seamount_boundary.py:
+// 45-147).  Its solve runs in FP64 on the npom_workspace.robin planes.
+// ---------------------------------------------------------------------------
+
+// eta_ghost (seamount_boundary.py:9-11): the east and west edge columns
+// copy the adjacent column, then the mask
+NPOM_HD int sea_gi(const Ctx &c, int i) { return i == 0 ? 1 : (i == c.im - 1 ? c.im - 2 : i); }
+NPOM_HD double sea_ghost(const Ctx &c, const double *v, int i, int j) {
+  return v[NPOM_I2(c, sea_gi(c, i), j)] * (double)F2(fsm, i, j);
+}
+// the unknowns: interior sea cells
+NPOM_HD bool sea_free(const Ctx &c, int i, int j) { return interior(c, i, j) && F2(fsm, i, j) > 0.0f; }
+
+// The Robin terms of row j (1..jm-2) from the Picard guess G = ghost(x):
+// face depths of the new depth h + G at the west (columns 0, 1) and east
+// (im-2, im-1) edges, and the characteristic flux coefficients
+// 2 dti H dy sqrt(g / h) / art of columns 1 and im-2.
+struct SeaRobin {
+  double hw, he, dyw, dye, bw, be, rw, re;
+};
+NPOM_HD SeaRobin sea_robin(const Ctx &c, const double *G, int j) {
+  const int im = c.im;
+  const double dti = c.k.dti, g = c.k.grav;
+  SeaRobin r;
+  r.hw = 0.5 * (((double)F2(h, 1, j) + G[NPOM_I2(c, 1, j)]) + ((double)F2(h, 0, j) + G[NPOM_I2(c, 0, j)]));
+  r.he = 0.5 * (((double)F2(h, im - 1, j) + G[NPOM_I2(c, im - 1, j)]) +
+                ((double)F2(h, im - 2, j) + G[NPOM_I2(c, im - 2, j)]));
+  r.dyw = 0.5 * ((double)F2(dy, 1, j) + (double)F2(dy, 0, j));
+  r.dye = 0.5 * ((double)F2(dy, im - 1, j) + (double)F2(dy, im - 2, j));
+  r.bw = sqrt(g / (double)F2(h, 1, j));
+  r.be = sqrt(g / (double)F2(h, im - 2, j));
+  r.rw = 2.0 * dti * r.hw * r.dyw * r.bw / (double)F2(art, 1, j);
+  r.re = 2.0 * dti * r.he * r.dye * r.be / (double)F2(art, im - 2, j);
+  return r;
+}
+
+// op(v) = the elliptic operator (old depth d) on ghost(v), plus the Robin
+// terms on columns 1 and im-2, zero off the unknowns (seamount_boundary.py:
+// 73-76), in FP64
+NPOM_HD double sea_robin_op(const Ctx &c, const double *v, const double *G, int i, int j) {
+  if (!sea_free(c, i, j)) return 0.0;
+  auto z = [&](int ii, int jj) { return sea_ghost(c, v, ii, jj); };
+  const double e = z(i, j);
+  const double d0 = F2(d, i, j);
+  const double he = 0.5 * ((double)F2(d, i + 1, j) + d0), hw = 0.5 * (d0 + (double)F2(d, i - 1, j));
+  const double hn = 0.5 * ((double)F2(d, i, j + 1) + d0), hs = 0.5 * (d0 + (double)F2(d, i, j - 1));
+  const double fe = he * (z(i + 1, j) - e) * (double)W2(ce, i, j) * (double)F2(dum, i + 1, j);
+  const double fw = hw * (e - z(i - 1, j)) * (double)W2(cw, i, j) * (double)F2(dum, i, j);
+  const double fn = hn * (z(i, j + 1) - e) * (double)W2(cn, i, j) * (double)F2(dvm, i, j + 1);
+  const double fs = hs * (e - z(i, j - 1)) * (double)W2(cs, i, j) * (double)F2(dvm, i, j);
+  double out = e - (double)c.k.implicit_coeff * ((fe - fw + fn - fs) * (double)W2(inv_art, i, j));
+  if (j >= 1 && j <= c.jm - 2 && (i == 1 || i == c.im - 2)) {
+    const SeaRobin r = sea_robin(c, G, j);
+    if (i == 1) out += r.rw * e;
+    if (i == c.im - 2) out += r.re * e;
+  }
+  return out;
+}
+
+// The right-hand side b of one Picard iteration (seamount_boundary.py:
+// 77-86): the step's RHS on the unknowns, plus on columns 1 and im-2 the
+// new-depth incident and exterior-elevation fluxes, minus the old-depth
+// incident flux the predictor already holds
+NPOM_HD double sea_rhs(const Ctx &c, const float *rhs, const double *G, int i, int j) {
+  double b = sea_free(c, i, j) ? (double)rhs[NPOM_I2(c, i, j)] : 0.0;
+  if (j >= 1 && j <= c.jm - 2 && (i == 1 || i == c.im - 2)) {
+    const int im = c.im;
+    const SeaRobin r = sea_robin(c, G, j);
+    const double dti = c.k.dti, ramp = c.ramp;
+    if (i == 1) {
+      b += 2.0 * dti * r.hw * r.dyw * (ramp * (double)F1(uabw, j) + r.bw * (double)F1(elw, j)) / (double)F2(art, 1, j);
+      b -= 2.0 * dti * 0.5 * ((double)F2(d, 1, j) + (double)F2(d, 0, j)) * r.dyw * ramp * (double)F1(uabw, j) /
+           (double)F2(art, 1, j);
+    }
+    if (i == im - 2) {
+      b -= 2.0 * dti * r.he * r.dye * (ramp * (double)F1(uabe, j) - r.be * (double)F1(ele, j)) /
+           (double)F2(art, im - 2, j);
+      b += 2.0 * dti * 0.5 * ((double)F2(d, im - 1, j) + (double)F2(d, im - 2, j)) * r.dye * ramp *
+           (double)F1(uabe, j) / (double)F2(art, im - 2, j);
+    }
+  }
+  return b;
+}
+
+// elf after the solve (ghost(x)), the Shapiro filter at gamma 0 (the
+// interior masked) and bcond 1 (ghost again)
+NPOM_HD float sea_elf(const Ctx &c, const double *x, int i, int j) {
+  const int si = sea_gi(c, i);
+  double e = sea_ghost(c, x, si, j);
+  if (interior(c, si, j)) e = e * (double)F2(fsm, si, j);
+  return (float)(e * (double)F2(fsm, i, j));
+}
+
+// The body continuity after the filter (seamount_boundary.py:28-42): the
+// transports from the filtered and new velocities and depths (hb = h + elb,
+// hn = h + el, both after the filter and shift) ...
+NPOM_HD void sea_transport_cell(const Ctx &c, int i, int j) {
+  if (i >= 1) {
+    const float hb = (F2(h, i, j) + F2(elb, i, j)) + (F2(h, i - 1, j) + F2(elb, i - 1, j));
+    const float hn = (F2(h, i, j) + F2(el, i, j)) + (F2(h, i - 1, j) + F2(el, i - 1, j));
+    P2(utf, i, j) = 0.25f * (F2(uab, i, j) * hb + F2(ua, i, j) * hn);
+  }
+  if (j >= 1) {
+    const float hb = (F2(h, i, j) + F2(elb, i, j)) + (F2(h, i, j - 1) + F2(elb, i, j - 1));
+    const float hn = (F2(h, i, j) + F2(el, i, j)) + (F2(h, i, j - 1) + F2(el, i, j - 1));
+    P2(vtf, i, j) = 0.25f * (F2(vab, i, j) * hb + F2(va, i, j) * hn);
+  }
+}
+
+// ... then etf on the interior from the continuity of the interval-mean
+// transports, 0.5 (utb + utf) and 0.5 (vtb + vtf), and the mean surface
+// volume flux; the east and west edges copy the adjacent column, then the
+// mask.  A cell off the interior rows keeps the etf I5 stored.
+NPOM_HD float sea_etf_interior(const Ctx &c, int i, int j) {
+  auto fx = [&](int ii) {
+    return (0.5f * (F2(utb, ii, j) + F2(utf, ii, j))) * 0.5f * (F2(dy, ii, j) + F2(dy, ii - 1, j));
+  };
+  auto fy = [&](int jj) {
+    return (0.5f * (F2(vtb, i, jj) + F2(vtf, i, jj))) * 0.5f * (F2(dx, i, jj) + F2(dx, i, jj - 1));
+  };
+  const float div = (fx(i + 1) - fx(i) + fy(j + 1) - fy(j)) / (F2(dx, i, j) * F2(dy, i, j));
+  const float flux = 0.5f * (F2(vfluxb, i, j) + F2(vfluxf, i, j));
+  return F2(etb, i, j) - c.k.dti2 * (div + flux);
+}
+NPOM_HD float sea_etf_cell(const Ctx &c, int i, int j) {
+  const int si = sea_gi(c, i);
+  const float v = interior(c, si, j) ? sea_etf_interior(c, si, j) : F2(etf, si, j);
+  return v * F2(fsm, i, j);
 }
 
 // The coastal tide policy's drag coefficient (coastal_compat.py:4-11):

@@ -14,10 +14,11 @@ constexpr int KMAX = 64;  // largest kb the column bodies accept
 NPOM_HD bool is_explicit(const Ctx &c) { return c.k.core == NPOM_CORE_EXPLICIT; }
 
 // bcond 3-6 in the explicit core's form: the explicit core, and the
-// semi-implicit core under the coastal or Jiaozhou Bay tide policy, whose
-// boundary hands indices 3-6 to the explicit step copy's bcond
-// (case_adapters/coastal_boundary.py:29, jzb_boundary.py:142)
-NPOM_HD bool explicit_bc(const Ctx &c) { return is_explicit(c) || c.k.obc_coastal; }
+// semi-implicit core under a case policy -- the tide policies hand indices
+// 3-6 to the explicit step copy's bcond (case_adapters/coastal_boundary.py:
+// 29, jzb_boundary.py:142), the seamount policy applies its own
+// (seamount_boundary.py:20-43)
+NPOM_HD bool explicit_bc(const Ctx &c) { return is_explicit(c) || c.k.obc_coastal || c.k.obc_seamount; }
 
 // ---------------------------------------------------------------------------
 // B1 (column): u/v barotropic fix (explicit time_loop.py:440-477).

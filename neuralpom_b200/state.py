@@ -129,9 +129,7 @@ def make_params(s, im, jm, kb, core, device=0):
     obc = str(get("obc_form", "native") or "native").strip().lower()
     if obc not in ("native", "seamount", "coastal", "jzb"):
         raise ValueError(f"unknown boundary policy {obc!r} (native, seamount, coastal or jzb)")
-    if obc == "seamount" and implicit:
-        raise ValueError("the seamount boundary policy is built for the explicit core")
-    if obc in ("coastal", "jzb") and implicit and float(get("barotropic_shapiro", 0.0) or 0.0) != 0.0:
+    if obc != "native" and implicit and float(get("barotropic_shapiro", 0.0) or 0.0) != 0.0:
         raise ValueError(f"the {obc} policy runs the semi-implicit core with its Shapiro filter off")
     p.obc_form = {"native": _abi.OBC_NATIVE, "seamount": _abi.OBC_SEAMOUNT, "coastal": _abi.OBC_COASTAL,
                   "jzb": _abi.OBC_JZB}[obc]

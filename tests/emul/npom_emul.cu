@@ -247,6 +247,73 @@ void cg_policy(const Ctx &c, int step) {
   std::memcpy(c.F[NPOM_F_elf], e.data(), e.size() * sizeof(float));
 }
 
+// the seamount policy's Picard / Robin solve (k_robin_picard), sequentially
+void robin_picard(const Ctx &c, int step) {
+  const int im = c.im, jm = c.jm;
+  const size_t ncell = (size_t)im * jm;
+  double *X = c.robin, *R = c.robin + ncell, *P = c.robin + 2 * ncell, *AP = c.robin + 3 * ncell;
+  double *G = c.robin + 4 * ncell;
+  float *rhs = c.W[NPOM_W_rhs];
+  each_cell(c, [&](int i, int j) { rhs[NPOM_I2(c, i, j)] = rhs_cell(c, i, j); });
+  each_cell(c, [&](int i, int j) {
+    P2(fluxua, i, j) = rhs_fluxua(c, i, j);
+    P2(fluxva, i, j) = rhs_fluxva(c, i, j);
+    X[NPOM_I2(c, i, j)] = sea_free(c, i, j) ? (double)F2(el, i, j) : 0.0;
+  });
+  auto area = [&](int i, int j) { return sea_free(c, i, j) ? (double)F2(art, i, j) : 0.0; };
+  bool converged = false;
+  int total = 0;
+  for (int nl = 0; nl < 6 && !converged; ++nl) {
+    each_cell(c, [&](int i, int j) { G[NPOM_I2(c, i, j)] = sea_ghost(c, X, i, j); });
+    double rr = 0.0, bb = 0.0;
+    each_cell(c, [&](int i, int j) {
+      const size_t q = NPOM_I2(c, i, j);
+      const double b = sea_rhs(c, rhs, G, i, j);
+      R[q] = b - sea_robin_op(c, X, G, i, j);
+      P[q] = R[q];
+      rr += area(i, j) * R[q] * R[q];
+      bb += area(i, j) * b * b;
+    });
+    const double thr = std::max(1e-28, std::max(bb, 1e-40) * 1e-22);
+    for (int it = 0; it < 300; ++it) {
+      if (rr <= thr) break;
+      double den = 0.0;
+      each_cell(c, [&](int i, int j) {
+        const size_t q = NPOM_I2(c, i, j);
+        AP[q] = sea_robin_op(c, P, G, i, j);
+        den += area(i, j) * P[q] * AP[q];
+      });
+      if (!(den > 0.0) || !(den < 1.0e308)) {
+        *c.status |= NPOM_DEV_NONFINITE;
+        return;
+      }
+      const double a = rr / den;
+      double nw = 0.0;
+      each_cell(c, [&](int i, int j) {
+        const size_t q = NPOM_I2(c, i, j);
+        X[q] = X[q] + a * P[q];
+        R[q] = R[q] - a * AP[q];
+        nw += area(i, j) * R[q] * R[q];
+      });
+      const double beta = nw / std::max(rr, 1e-40);
+      each_cell(c, [&](int i, int j) {
+        const size_t q = NPOM_I2(c, i, j);
+        P[q] = R[q] + beta * P[q];
+      });
+      rr = nw;
+      ++total;
+    }
+    double change = 0.0;
+    each_cell(c, [&](int i, int j) {
+      change = std::max(change, std::fabs(sea_ghost(c, X, i, j) - G[NPOM_I2(c, i, j)]));
+    });
+    converged = change < 1e-11;
+  }
+  c.cg_iters[step] = total;
+  if (!converged) *c.status |= NPOM_DEV_PCG_MAXIT;
+  each_cell(c, [&](int i, int j) { P2(elf, i, j) = sea_elf(c, X, i, j); });
+}
+
 void policy_lines(const Ctx &c, int which) {
   if (!c.k.obc_coastal || c.k.obc_jzb) return;
   for (int t = 0; t < c.jm + c.im; ++t) policy_bc2_line(c, t, which);
@@ -275,22 +342,30 @@ void run_phase(const Ctx &c, const npom_params *p, int phase) {
       if (p->core == NPOM_CORE_IMPLICIT) {
         each_cell(c, [&](int i, int j) { elliptic_coeff_cell(c, i, j); });
         if (c.k.obc_coastal) cg_policy(c, 0);
+        else if (c.k.sea_implicit) robin_picard(c, 0);
         else pcg(c, 0, 1, 1);
       } else {
         subcycle(c);
       }
       break;
-    case 4:
-      if (c.k.obc_coastal && p->core == NPOM_CORE_IMPLICIT) {
+    case 4: {
+      const bool pol = (c.k.obc_coastal || c.k.sea_implicit) && p->core == NPOM_CORE_IMPLICIT;
+      if (pol) {
         each_cell(c, [&](int i, int j) { phase_i5a_cell(c, i, j); });
         policy_lines(c, 1);
       }
       each_cell(c, [&](int i, int j) {
         if (phase_i5_cell(c, i, j)) *c.status |= NPOM_DEV_VMAX;
       });
-      if (c.k.obc_coastal && p->core == NPOM_CORE_IMPLICIT)
-        each_cell(c, [&](int i, int j) { cbc_coastal_cell(c, i, j); });
+      if (pol && c.k.obc_coastal) each_cell(c, [&](int i, int j) { cbc_coastal_cell(c, i, j); });
+      if (pol && c.k.sea_implicit) {
+        each_cell(c, [&](int i, int j) { sea_transport_cell(c, i, j); });
+        std::vector<float> e((size_t)c.im * c.jm);
+        each_cell(c, [&](int i, int j) { e[NPOM_I2(c, i, j)] = sea_etf_cell(c, i, j); });
+        std::memcpy(c.F[NPOM_F_etf], e.data(), e.size() * sizeof(float));
+      }
       break;
+    }
     case 5: each_cell(c, [&](int i, int j) { phase_b1_column(c, i, j); }); break;
     case 6: each_cell(c, [&](int i, int j) { phase_b2a_column(c, i, j); }); break;
     case 7: each_point(c, [&](int i, int j, int k) { phase_b2b_point(c, i, j, k); }); break;
@@ -547,6 +622,7 @@ int emul_steps(const npom_params *p, float *const *fields, const npom_workspace 
     run_phase(c, p, 2);
     if (p->core == NPOM_CORE_IMPLICIT) {
       if (c.k.obc_coastal) cg_policy(c, n);
+      else if (c.k.sea_implicit) robin_picard(c, n);
       else pcg(c, n, 1, 1);
       wrap_x(c);
       run_phase(c, p, 4);

@@ -96,6 +96,8 @@ class EmulCore:
                                           arrays["tide_phase"])
             self.ws.tide = self.tide.ctypes.data
         self.ws.mp3d = self.mp3d.ctypes.data
+        self.robin = np.zeros(5 * im * jm, np.float64)
+        self.ws.robin = self.robin.ctypes.data
         self.time = float(s.get("time", 0.0))
 
     def steps(self, n):

@@ -98,7 +98,7 @@ def make_step_golden(name, im, jm, seed, steps=(1, 3), core=None, tag=None):
             out[f"out{n}__{f}"] = a[f]
         out[f"out{n}__scalar_time"] = np.asarray(float(core.time))
         hist = getattr(core, "_eta_solver_iteration_history", None)
-        if hist is not None:
+        if hist:  # (a case policy's own solve keeps no history)
             out[f"out{n}__cg_iters"] = np.asarray(hist, dtype=np.int32)
     tag = tag or ("explicit" if name == "explicit" else "implicit")
     path = os.path.join(HERE, f"step_{tag}_{im}x{jm}.npz")
@@ -420,6 +420,40 @@ def make_seamount_golden(im=24, jm=18, seed=71, steps=(1, 3)):
     make_step_golden("explicit", im, jm, seed, steps=steps, core=core, tag="seamount_explicit")
 
 
+def make_seamount_implicit_golden(im=24, jm=18, seed=72, steps=(1, 3)):
+    """The semi-implicit core under the reference's seamount case policy
+    (seamount_runtime.install(core, "implicit"): its predictor, Robin CG
+    with Picard iterations, corrector, body continuity and boundary, and
+    the POM08-WAD closure) on ``cases.open_seamount`` with seeded T and u
+    perturbations, clock at 0.25 day; 1 and 3 steps, in float64, the only
+    precision whose Picard test (1e-11 m) the policy can pass."""
+    import torch
+    sys.path.insert(0, ROOT)
+    from neuralpom_b200 import cases
+    from neuralpom.cores.case_adapters import seamount_runtime
+    name = "implicit_p0_fixed"
+    A, Sc = cases.open_seamount(im, jm, dte=5.0, isplit=30, core=name)
+    g = np.random.default_rng(seed)
+    fsm3, dum3 = A["fsm"][:, :, None], A["dum"][:, :, None]
+    for f, sd, m in (("t", 0.2, fsm3), ("u", 0.02, dum3), ("v", 0.02, A["dvm"][:, :, None])):
+        p = (sd * g.standard_normal(A[f].shape) * m).astype(np.float32)
+        p[:, :, -1] = 0.0
+        A[f] = A[f] + p
+        A[f[0] + "b"] = A[f[0] + "b"] + p
+    A, Sc = cases.seamount_policy(A, Sc, core=name)
+    Sc = dict(Sc, time=0.25, time0=0.25)
+    core = rh.build_reference_core(name, im, jm)
+    rh.load_state(core, {k: v for k, v in A.items() if hasattr(core, k)}, Sc)
+    for k, v in list(vars(core).items()):
+        if torch.is_tensor(v) and v.is_floating_point():
+            setattr(core, k, v.double())
+    torch.set_default_dtype(torch.float64)
+    seamount_runtime.install(core, "implicit")
+    core.profq_form, core.zsh, core.obc_form = "pom08", 0.01, "seamount"
+    make_step_golden(name, im, jm, seed, steps=steps, core=core, tag="seamount_implicit")
+    torch.set_default_dtype(torch.float32)
+
+
 def make_coastal_policy_golden(im=24, jm=18, steps=(1, 3), family="explicit"):
     """The explicit (or semi-implicit) core under the reference's coastal
     tide policy, set up the way its registry does (cores/case_adapters/
@@ -562,7 +596,7 @@ def make_pom08_goldens():
 
 
 def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint", "coupling", "mpdata", "pom08", "seamount",
-                "shapiro", "jzb", "coastal_implicit")):
+                "shapiro", "jzb", "coastal_implicit", "seamount_implicit")):
     src = rh.default_reference_path()
     if src is None:
         raise SystemExit("reference sources not found; set NPOM_REFERENCE_SRC")
@@ -599,8 +633,11 @@ def main(which=("proft", "steps", "adjoint", "coastal", "step_adjoint", "couplin
     if "coastal_implicit" in which:
         make_coastal_policy_golden(family="implicit")
         make_jzb_policy_golden(family="implicit")
+    if "seamount_implicit" in which:
+        make_seamount_implicit_golden()
 
 
 if __name__ == "__main__":
     main(tuple(sys.argv[1:]) or ("proft", "steps", "adjoint", "coastal", "step_adjoint", "coupling", "mpdata",
-                                 "pom08", "seamount", "shapiro", "jzb", "coastal_implicit"))
+                                 "pom08", "seamount", "shapiro", "jzb", "coastal_implicit",
+                                 "seamount_implicit"))

@@ -70,6 +70,14 @@ def step_field_error(got, ref, field, nsteps, golden):
     bound = 1e-5 if nsteps == 1 else 1e-4
     if golden.startswith("step_coastal") and field in ILL_CONDITIONED_COASTAL:
         bound = 2e-2
+    if golden.startswith("step_seamount_implicit"):
+        # a float64 golden (the policy's Picard test, 1e-11 m, cannot pass in
+        # float32): the float32 step against float64.  The production
+        # core's oracle on the same perturbed state differs from its own
+        # float64 run by up to 8.3e-4 after three steps (kh); the Orlanski
+        # T/S ratio at the open edges, a quotient of differences of nearly
+        # equal temperatures, puts 2e-5 on T after one step.
+        bound = 1e-4 if nsteps == 1 else 2e-3
     if field == "w":
         return rel_err(got[..., :-1], ref[..., :-1]), bound
     return rel_err(got, ref), bound

@@ -27,6 +27,8 @@ STEP_FILES = [("step_explicit_12x10.npz", "explicit"), ("step_implicit_12x10.npz
               # both tide policies on the semi-implicit core (their own area-weighted CG)
               ("step_coastal_policy_implicit_24x18.npz", "implicit_p0_fixed"),
               ("step_jzb_policy_implicit_24x18.npz", "implicit_p0_fixed"),
+              # the seamount policy on the semi-implicit core (Picard / Robin solve; a float64 golden)
+              ("step_seamount_implicit_24x18.npz", "implicit_p0_fixed"),
               ("step_implicit_shapiro_20x18.npz", "implicit_p0_fixed")]
 
 

@@ -23,6 +23,8 @@ STEP_FILES = [("step_explicit_12x10.npz", "explicit"), ("step_implicit_12x10.npz
               # both tide policies on the semi-implicit core
               ("step_coastal_policy_implicit_24x18.npz", "implicit_p0_fixed"),
               ("step_jzb_policy_implicit_24x18.npz", "implicit_p0_fixed"),
+              # the seamount policy on the semi-implicit core (Picard / Robin solve; a float64 golden)
+              ("step_seamount_implicit_24x18.npz", "implicit_p0_fixed"),
               # the semi-implicit core with its spatial Shapiro filters on (gamma 0.05)
               ("step_implicit_shapiro_20x18.npz", "implicit_p0_fixed")]
 
@@ -277,7 +279,7 @@ def test_gpu_restart_continues_bitwise(tmp_path):
 
 @pytest.mark.parametrize("fname", ["step_pom08_explicit_12x10.npz", "step_seamount_explicit_24x18.npz",
                                    "step_coastal_policy_24x18.npz", "step_jzb_policy_24x18.npz",
-                                   "step_coastal_policy_implicit_24x18.npz"])
+                                   "step_coastal_policy_implicit_24x18.npz", "step_seamount_implicit_24x18.npz"])
 def test_gpu_case_policies_refuse_gradients(fname):
     """The case policies advance forward only, as the reference's registry
     requires (cores/case_adapters/registry.py:38-41)."""
