@@ -73,19 +73,16 @@ def test_profq_form_reaches_npom_params():
 
 
 def test_boundary_policy_reaches_npom_params():
-    """obc_form: native by default, seamount for the explicit core only."""
+    """obc_form: native by default; the seamount, coastal and Jiaozhou Bay
+    policies on either core (the semi-implicit one with its Shapiro filter
+    off)."""
     s = dict(state.default_scalars("explicit"), obc_form="seamount")
     assert state.make_params(s, 24, 18, 16, "explicit").obc_form == _abi.OBC_SEAMOUNT
     assert state.make_params(dict(state.default_scalars("explicit")), 24, 18, 16, "explicit").obc_form == \
         _abi.OBC_NATIVE
     with pytest.raises(ValueError):
         state.make_params(dict(s, obc_form="orlanski"), 24, 18, 16, "explicit")
-    with pytest.raises(ValueError):
-        state.make_params(dict(state.default_scalars("implicit_p0_fixed"), obc_form="seamount"), 24, 18, 16,
-                          "implicit_p0_fixed")
-    # the coastal and Jiaozhou Bay tide policies on either core (the
-    # semi-implicit one with its Shapiro filter off)
-    for form, code in (("coastal", _abi.OBC_COASTAL), ("jzb", _abi.OBC_JZB)):
+    for form, code in (("seamount", _abi.OBC_SEAMOUNT), ("coastal", _abi.OBC_COASTAL), ("jzb", _abi.OBC_JZB)):
         for core in ("explicit", "implicit_p0_fixed"):
             assert state.make_params(dict(state.default_scalars(core), obc_form=form), 24, 18, 16,
                                      core).obc_form == code
