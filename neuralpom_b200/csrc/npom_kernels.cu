@@ -1118,13 +1118,17 @@ bool lanes_enabled(const Ctx &c) {
 // Columns from which PROFT runs one thread per column: its lane form issues
 // every step of the sequential sweeps for the whole segment (~70x the
 // instructions per column), which only pays while columns are too few to
-// fill the GPU.  Both forms compute bitwise the same values.
+// fill the GPU.  With 16 levels fixed at compile time (k_cols_b6_kb16) the
+// thread-per-column form is the faster one at every size measured (90x82:
+// 18.9 against 28.3 us; 354x322: 73 against 215 us).  Both forms compute
+// bitwise the same values.
 constexpr size_t kProftThreadColumns = 16384;
 
 template <int PH>
 void launch_cols(const Ctx &c, cudaStream_t s) {
   size_t n = (size_t)c.im * c.jm;
-  const bool proft_threads = PH == CP_B6 && n >= kProftThreadColumns && c.tune.column_form != 1;
+  const bool proft_threads =
+      PH == CP_B6 && (n >= kProftThreadColumns || c.kb == 16) && c.tune.column_form != 1;
   // the POM08-WAD PROFQ has only the thread-per-column body
   const bool pom08 = PH == CP_B3 && c.k.profq_pom08;
   if (lanes_enabled(c) && !proft_threads && !pom08) {
