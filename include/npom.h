@@ -304,7 +304,9 @@ npom_status npom_proft(int ncol, int kb, const float *f_in, const float *wfsurf,
 
 /* One PCG free-surface solve: fields[elf] holds the initial guess on entry
  * and the solution on exit (before the Shapiro filter / boundary); rhs is
- * read from ws->buf[NPOM_W_rhs].  Iterations go to ws->cg_iters[0]. */
+ * read from ws->buf[NPOM_W_rhs].  Iterations go to ws->cg_iters[0].  The
+ * native boundary only (obc_form 0; a case policy's solve is part of its
+ * step), as for npom_pcg_adjoint and npom_pcg_solve_static. */
 npom_status npom_pcg_solve(const npom_params *p, float *const *fields,
                            const npom_workspace *ws, void *stream);
 

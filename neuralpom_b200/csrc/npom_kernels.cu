@@ -2104,7 +2104,10 @@ npom_status npom_proft(int ncol, int kb, const float *f_in, const float *wfsurf,
 }
 
 npom_status npom_pcg_solve(const npom_params *p, float *const *fields, const npom_workspace *ws, void *stream) {
-  if (!check_args_dev(p, fields, ws) || p->core != NPOM_CORE_IMPLICIT) return NPOM_ERR_ARG;
+  // (the case policies' solves belong to their step: they build their RHS
+  // from its predictor)
+  if (!check_args_dev(p, fields, ws) || p->core != NPOM_CORE_IMPLICIT || p->obc_form != NPOM_OBC_NATIVE)
+    return NPOM_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   Ctx c = make_ctx(p, fields, ws);
   if (cudaMemsetAsync(ws->sync, 0, 4 * sizeof(unsigned int), s) != cudaSuccess) return NPOM_ERR_CUDA;
@@ -2120,8 +2123,8 @@ npom_status npom_pcg_solve(const npom_params *p, float *const *fields, const npo
 npom_status npom_pcg_adjoint(const npom_params *p, float *const *fields, const npom_workspace *ws,
                              const float *grad_x, const float *x, const float *d2d, float *grad_rhs, float *grad_d,
                              void *stream) {
-  if (!check_args_dev(p, fields, ws) || p->core != NPOM_CORE_IMPLICIT || !grad_x || !x || !d2d || !grad_rhs ||
-      !grad_d)
+  if (!check_args_dev(p, fields, ws) || p->core != NPOM_CORE_IMPLICIT || p->obc_form != NPOM_OBC_NATIVE || !grad_x ||
+      !x || !d2d || !grad_rhs || !grad_d)
     return NPOM_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   Ctx c = make_ctx(p, fields, ws);
@@ -2140,7 +2143,9 @@ npom_status npom_pcg_adjoint(const npom_params *p, float *const *fields, const n
 npom_status npom_pcg_solve_static(const npom_params *p, float *const *fields, const float *rhs, const float *sx,
                                   const float *sy, const float *inv_eigs, int *iters_out, unsigned int *status_out,
                                   void *stream) {
-  if (!p || !fields || !rhs || p->core != NPOM_CORE_IMPLICIT || p->im < 3 || p->jm < 3) return NPOM_ERR_ARG;
+  if (!p || !fields || !rhs || p->core != NPOM_CORE_IMPLICIT || p->obc_form != NPOM_OBC_NATIVE || p->im < 3 ||
+      p->jm < 3)
+    return NPOM_ERR_ARG;
   if (p->eta_precond == NPOM_PRECOND_SPECTRAL && (!sx || !sy || !inv_eigs)) return NPOM_ERR_ARG;
   const size_t ncell = (size_t)p->im * p->jm;
   if (ncell > kStaticCells) return NPOM_ERR_TOO_LARGE;

@@ -51,6 +51,14 @@ def test_argument_errors_need_no_gpu(lib):
     assert lib.npom_step_batch(0, None, None, None, None, None) == 1
     assert lib.npom_step_batch(65, None, None, None, None, None) == 1
     assert lib.npom_step_batch(2, None, None, None, None, None) == 1
+    # a case policy's free-surface solve is part of its step: the standalone
+    # solve refuses it before touching any pointer
+    p = _abi.NpomParams()
+    p.core, p.im, p.jm, p.kb, p.obc_form = _abi.CORE_IMPLICIT, 24, 20, 16, _abi.OBC_COASTAL
+    fa = _abi.FieldArray()
+    dummy = ctypes.c_float(0.0)
+    assert lib.npom_pcg_solve_static(ctypes.byref(p), ctypes.byref(fa), ctypes.byref(dummy), None, None, None,
+                                     None, None, None) == 1
 
 
 def test_library_is_sm100a(lib):
