@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(kThreads) kb_subcycle(const BatchTable *t, Bat
 __global__ void __launch_bounds__(kThreads) kb_pcg(const BatchTable *t, BatchStep v, int with_rhs, int with_post) {
   __shared__ Ctx sc;
   batch_enter<BS_PCG>(t, v, sc);
-  pcg_coop_body(sc, with_rhs, with_post);
+  pcg_coop_body<true>(sc, with_rhs, with_post);
 }
 
 // cluster group g of the table: consecutive clusters of clu_nc[g] CTAs,

@@ -409,11 +409,37 @@ __device__ double grid_total(const Ctx &c, int slot) {
 // tiles are dealt to the blocks of the context; epi(a, b, value) stores.
 constexpr int kDstRows = 8, kDstCols = 32, kDstChunk = 64;
 static_assert(kDstRows * kDstCols == kThreads, "one output per thread");
+// dst_row_pairs (below): rows per group, largest interior side
+constexpr int kDstBandRows = 4, kDstBandMax = 384;
+constexpr int kDstTileFloats = kDstRows * (kDstChunk + 1) + kDstChunk * (kDstCols + 1);
+constexpr int kDstSmemFloats =
+    kDstTileFloats > 2 * kDstBandRows * kDstBandMax ? kDstTileFloats : 2 * kDstBandRows * kDstBandMax;
 
-template <bool ALONG_I, class Epi>
+// The one shared-memory buffer of every DST stage instantiation of a kernel
+// (a function-local static array of a non-template function is one array
+// per kernel; arrays declared in the templates would be one per
+// instantiation).
+__device__ __forceinline__ float *dst_smem() {
+  __shared__ float buf[kDstSmemFloats];
+  return buf;
+}
+
+// SHARED: the staging arrays in dst_smem(), the buffer that dst_row_pairs
+// also uses (kernels that compile both forms); otherwise arrays of each
+// instantiation, as the one-member kernel has them.
+template <bool ALONG_I, bool SHARED, class Epi>
 __device__ __forceinline__ void dst_tiles(const Ctx &c, const float *src, bool src_is_grid, Epi &&epi) {
-  __shared__ float lt[kDstRows][kDstChunk + 1];
-  __shared__ float rt[kDstChunk][kDstCols + 1];
+  float(*lt)[kDstChunk + 1];
+  float(*rt)[kDstCols + 1];
+  if constexpr (SHARED) {
+    lt = reinterpret_cast<float(*)[kDstChunk + 1]>(dst_smem());
+    rt = reinterpret_cast<float(*)[kDstCols + 1]>(dst_smem() + kDstRows * (kDstChunk + 1));
+  } else {
+    __shared__ float lt_own[kDstRows][kDstChunk + 1];
+    __shared__ float rt_own[kDstChunk][kDstCols + 1];
+    lt = lt_own;
+    rt = rt_own;
+  }
   // rows: the solve's unknowns (with periodic x the unique columns, Sx the
   // Hartley matrix of the period)
   const int i0 = pcg_i0(c), ni = c.im - 2 * i0, nj = c.jm - 2;
@@ -453,8 +479,72 @@ __device__ __forceinline__ void dst_tiles(const Ctx &c, const float *src, bool s
   }
 }
 
+// The DST stages in pairs (i-stage then j-stage) over bands of whole rows:
+// the rows of the interior are split into one contiguous band per block of
+// the context, and a block takes its band kDstBandRows rows at a time.  For
+// each group it computes the i-stage row(s) mid[q][b] = sum_m Sx[a][m] src(m, b)
+// over every column b, keeps them in shared memory, and then the j-stage
+// sum_b mid[q][b] Sy[b][l] of the same rows, so no grid barrier separates
+// the two stages.  Every output sums its terms in FP64 in index order, as
+// dst_tiles does, so the values are the same bits.  src(m, b) gives the
+// i-stage operand, epi(a, l, value) stores the j-stage output.  Interiors up
+// to kDstBandMax in either direction (larger ones use dst_tiles).
+// Used by the batched solve only.  Each thread runs its FP64 sums over L2
+// loads, latency-bound when one member has the GPU (177x161 alone: 3.2 ms
+// per step with the tiles, 4.0 with the pairs); in a batch the other
+// members' blocks hide that latency and the two barriers saved per
+// iteration win (64 mixed members: 8.4 -> 8.8 member-days/s).
+template <class Src, class Epi>
+__device__ __forceinline__ void dst_row_pairs(const Ctx &c, Src &&src, Epi &&epi) {
+  float(*sxr)[kDstBandMax] = reinterpret_cast<float(*)[kDstBandMax]>(dst_smem());
+  float(*mid)[kDstBandMax] = reinterpret_cast<float(*)[kDstBandMax]>(dst_smem() + kDstBandRows * kDstBandMax);
+  const int i0 = pcg_i0(c), ni = c.im - 2 * i0, nj = c.jm - 2;
+  const float *sx = c.W[NPOM_W_sx], *sy = c.W[NPOM_W_sy];
+  const int G = (int)vgrid(c), band = (ni + G - 1) / G;
+  const int a_beg = (int)vblock(c) * band, a_end = min(ni, a_beg + band);
+  for (int a0 = a_beg; a0 < a_end; a0 += kDstBandRows) {
+    const int nr = min(kDstBandRows, a_end - a0);
+    __syncthreads();  // the previous group is consumed
+    for (int e = threadIdx.x; e < kDstBandRows * ni; e += blockDim.x) {
+      const int q = e / ni, m = e - q * ni;
+      sxr[q][m] = q < nr ? __ldcg(sx + (size_t)(a0 + q) * ni + m) : 0.0f;
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < nj; b += blockDim.x) {
+      double acc[kDstBandRows];
+#pragma unroll
+      for (int q = 0; q < kDstBandRows; ++q) acc[q] = 0.0;
+#pragma unroll 4
+      for (int m = 0; m < ni; ++m) {
+        const double v = (double)src(m, b);
+#pragma unroll
+        for (int q = 0; q < kDstBandRows; ++q) acc[q] += (double)sxr[q][m] * v;
+      }
+#pragma unroll
+      for (int q = 0; q < kDstBandRows; ++q) mid[q][b] = (float)acc[q];
+    }
+    __syncthreads();
+    for (int l = threadIdx.x; l < nj; l += blockDim.x) {
+      double acc[kDstBandRows];
+#pragma unroll
+      for (int q = 0; q < kDstBandRows; ++q) acc[q] = 0.0;
+#pragma unroll 4
+      for (int b = 0; b < nj; ++b) {
+        const double w = (double)__ldcg(sy + (size_t)b * nj + l);
+#pragma unroll
+        for (int q = 0; q < kDstBandRows; ++q) acc[q] += (double)mid[q][b] * w;
+      }
+#pragma unroll
+      for (int q = 0; q < kDstBandRows; ++q)
+        if (q < nr) epi(a0 + q, l, (float)acc[q]);
+    }
+  }
+}
+
 // z = M^-1 r over the interior; returns after its own trailing barrier.
-// Accumulates r.z into *rz of this thread.
+// Accumulates r.z into *rz of this thread.  ROWS: the DST stages in row
+// pairs (one grid barrier instead of three; the batched solve).
+template <bool ROWS>
 __device__ bool precondition(const Ctx &c, double &rz) {
   const int nj = c.jm - 2, i0 = pcg_i0(c);
   const size_t nint = (size_t)(c.im - 2 * i0) * nj;
@@ -466,17 +556,36 @@ __device__ bool precondition(const Ctx &c, double &rz) {
   if (c.k.eta_precond == NPOM_PRECOND_SPECTRAL) {
     float *t1 = c.W[NPOM_W_t1], *t2 = c.W[NPOM_W_t2];
     const float *ie = c.W[NPOM_W_inv_eigs];
-    dst_tiles<true>(c, r, true, [&](int a, int b, float v) { t1[(size_t)a * nj + b] = v; });
+    const float inv_scale = c.k.inverse_scale;
+    if (ROWS && c.im - 2 * i0 <= kDstBandMax && nj <= kDstBandMax) {
+      // two stages per pass: one grid barrier instead of three
+      dst_row_pairs(
+          c, [&](int m, int b) { return __ldcg(r + NPOM_I2(c, m + i0, b + 1)); },
+          [&](int a, int b, float v) {
+            const size_t q = (size_t)a * nj + b;
+            t2[q] = v * __ldcg(ie + q);
+          });
+      if (!grid_barrier(c)) return false;
+      dst_row_pairs(
+          c, [&](int m, int b) { return __ldcg(t2 + (size_t)m * nj + b); },
+          [&](int a, int b, float v) {
+            const float zval = v / inv_scale;
+            const size_t o = NPOM_I2(c, a + i0, b + 1);
+            zv[o] = zval;
+            rz += (double)__ldcg(r + o) * (double)zval;
+          });
+      return true;
+    }
+    dst_tiles<true, ROWS>(c, r, true, [&](int a, int b, float v) { t1[(size_t)a * nj + b] = v; });
     if (!grid_barrier(c)) return false;
-    dst_tiles<false>(c, t1, false, [&](int a, int b, float v) {
+    dst_tiles<false, ROWS>(c, t1, false, [&](int a, int b, float v) {
       const size_t q = (size_t)a * nj + b;
       t2[q] = v * __ldcg(ie + q);
     });
     if (!grid_barrier(c)) return false;
-    dst_tiles<true>(c, t2, false, [&](int a, int b, float v) { t1[(size_t)a * nj + b] = v; });
+    dst_tiles<true, ROWS>(c, t2, false, [&](int a, int b, float v) { t1[(size_t)a * nj + b] = v; });
     if (!grid_barrier(c)) return false;
-    const float inv_scale = c.k.inverse_scale;
-    dst_tiles<false>(c, t1, false, [&](int a, int b, float v) {
+    dst_tiles<false, ROWS>(c, t1, false, [&](int a, int b, float v) {
       const float zval = v / inv_scale;
       const size_t o = NPOM_I2(c, a + i0, b + 1);
       zv[o] = zval;
@@ -498,7 +607,8 @@ __device__ bool precondition(const Ctx &c, double &rz) {
 // Fused PCG free-surface solve (core.py:460-589, eager branch), followed by
 // the Shapiro filter and closed-basin bcond 1 (core.py:893-916) and
 // d = h + elf.  Iterations -> c.cg_iters[c.sync[2]++] (one slot per solve
-// of the call).
+// of the call).  ROWS as for precondition: the same values either way.
+template <bool ROWS>
 __device__ __forceinline__ void pcg_coop_body(const Ctx &c, int with_rhs, int with_post) {
   // unknowns: rows i0 .. im-1-i0 (the interior, or the unique columns of a
   // periodic-x basin)
@@ -550,7 +660,7 @@ __device__ __forceinline__ void pcg_coop_body(const Ctx &c, int with_rhs, int wi
   block_sum3(c, rr, 0.0, 0.0, 1, -1, -1);
   if (!grid_barrier(c)) return;
   double rz;
-  if (!precondition(c, rz)) return;
+  if (!precondition<ROWS>(c, rz)) return;
   block_sum3(c, rz, 0.0, 0.0, 2, -1, -1);
   if (!grid_barrier(c)) return;
   double rs0 = grid_total(c, 1);
@@ -608,7 +718,7 @@ __device__ __forceinline__ void pcg_coop_body(const Ctx &c, int with_rhs, int wi
       converged = true;
       break;
     }
-    if (!precondition(c, rz)) return;
+    if (!precondition<ROWS>(c, rz)) return;
     block_sum3(c, rz, 0.0, 0.0, 2, -1, -1);
     if (!grid_barrier(c)) return;
     double rho_new = grid_total(c, 2);
@@ -662,8 +772,9 @@ __device__ __forceinline__ void pcg_coop_body(const Ctx &c, int with_rhs, int wi
   }
 }
 
+template <bool ROWS>
 __global__ void __launch_bounds__(kThreads) k_pcg(Ctx c, int with_rhs, int with_post) {
-  pcg_coop_body(c, with_rhs, with_post);
+  pcg_coop_body<ROWS>(c, with_rhs, with_post);
 }
 
 // The tide policies' free-surface solve on the semi-implicit core
@@ -1264,6 +1375,13 @@ bool cluster_launchable(const void *fn, int nc, size_t smem) {
 // Work of the grid-barrier PCG in threads: one per interior cell, and at
 // least one block per DST tile (a block holding two tiles would double
 // every DST stage).
+// The one-member cooperative solve: DST stages as tiles; NPOM_PCG_DST=rows
+// selects the batched solve's row pairs (the same values), for comparisons.
+const void *pcg_coop_fn() {
+  const char *e = getenv("NPOM_PCG_DST");
+  return (e && std::strcmp(e, "rows") == 0) ? (const void *)k_pcg<true> : (const void *)k_pcg<false>;
+}
+
 size_t pcg_coop_work(const Ctx &c) {
   const size_t ni = (size_t)(c.im - 2), nj = (size_t)(c.jm - 2);
   size_t work = ni * nj;
@@ -1289,7 +1407,7 @@ cudaError_t plan_pcg(const Ctx &c, PcgPlan *plan) {
   plan->cluster = pcg_cluster_layout(c, &plan->L) && ensure_cluster_attrs(plan->L) &&
                   cluster_launchable(pcg_cluster_fn(plan->L), plan->L.nc, plan->L.bytes());
   if (plan->cluster) return cudaSuccess;
-  return coop_blocks((const void *)k_pcg, pcg_coop_work(c), &plan->coop_blocks);
+  return coop_blocks(pcg_coop_fn(), pcg_coop_work(c), &plan->coop_blocks);
 }
 
 cudaError_t run_pcg(Ctx c, const PcgPlan &plan, int with_rhs, int with_post, cudaStream_t s) {
@@ -1303,7 +1421,7 @@ cudaError_t run_pcg(Ctx c, const PcgPlan &plan, int with_rhs, int with_post, cud
   if (plan.cluster) return run_pcg_cluster(c, plan.L, with_rhs, with_post, s);
   c.coh = 1;
   void *args[] = {&c, &with_rhs, &with_post};
-  return launch_coop((const void *)k_pcg, plan.coop_blocks, args, c.sync, s);
+  return launch_coop(pcg_coop_fn(), plan.coop_blocks, args, c.sync, s);
 }
 
 // Launch shape of the explicit subcycle, decided outside any capture:

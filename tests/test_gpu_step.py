@@ -189,6 +189,29 @@ def test_gpu_cluster_and_grid_barrier_pcg_agree(monkeypatch, grid):
     assert not np.array_equal(outs[0]["el"], outs[1]["el"])
 
 
+@pytest.mark.parametrize("grid", [(177, 161), (90, 82)])
+def test_gpu_coop_pcg_row_pair_dsts_equal_tiles(monkeypatch, grid):
+    """The grid-barrier PCG's two forms of the DST stages -- tiles (the
+    one-member solve) and row pairs (the batched solve: each i-stage fused
+    with its j-stage over bands of whole rows, one grid barrier instead of
+    three per preconditioner) -- sum every output in FP64 in index order, so
+    both give the same bits: fields and PCG iteration counts compared
+    bitwise over three steps."""
+    from neuralpom_b200 import B200Physics, cases
+    A, Sc = cases.seamount(*grid)
+    monkeypatch.setenv("NPOM_PCG", "coop")
+    outs = []
+    for form in ("tiles", "rows"):
+        monkeypatch.setenv("NPOM_PCG_DST", form)
+        c = _core(A, Sc, "implicit_p0_fixed")
+        B200Physics(core_name="implicit_p0_fixed").advance(c, steps=3)
+        outs.append(({f: getattr(c, f).cpu().numpy() for f in ("el", "elf", "ua", "u", "t")},
+                     list(c._eta_solver_iteration_history)))
+    assert outs[0][1] == outs[1][1]
+    for f in outs[0][0]:
+        assert np.array_equal(outs[0][0][f], outs[1][0][f]), (f, rel_err(outs[1][0][f], outs[0][0][f]))
+
+
 @pytest.mark.parametrize("core", ["implicit_p0_fixed", "explicit"])
 def test_gpu_lane_columns_equal_thread_columns(monkeypatch, core):
     """The 16-lane column kernels (level per lane, shuffled recurrences)
