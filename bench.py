@@ -793,7 +793,7 @@ def seamount_fwd_adjoint(core, args, dev, nsteps=36, reps=3):
 
 
 def coastal_fwd_adjoint(args, dev, nsteps=360):
-    """BASELINE config 4's differentiation: the explicit core on the
+    """The coastal differentiation workload: the explicit core on the
     354x322x16 coastal basin, ``nsteps`` internal steps (6 h at dtI = 60 s)
     forward under autograd from the set-up state (tide elevation held at its
     start value inside the window), MSE(u, v, T, S) against a seeded
@@ -880,11 +880,11 @@ def fwd_adjoint_sample(args, dev, reps=3):
 
 
 def fwd_adjoint_midtrain_batch(args, dev, members=8, reps=3):
-    """BASELINE config 2 as stated: the Midtrain-shaped forward+adjoint for
-    a batch of ``members`` seeded members (``midtrain_case(m)``), each with
-    its own core, raw correction output and CUDA stream.  Every member's
-    three differentiable intervals are enqueued on its stream through
-    run_time_loop with ``status_deferred`` (no host synchronisation between
+    """The Midtrain-shaped forward+adjoint of an ensemble: ``members``
+    seeded members (``midtrain_case(m)``), each with its own core, raw
+    correction output and CUDA stream.  Every member's three differentiable
+    intervals are enqueued on its stream through run_time_loop with
+    ``status_deferred`` (no host synchronisation between
     intervals); the loss is the sum of the members' MSE(u, v, T, S) and one
     backward() reaches every member's state leaves and raw output.  Timed
     with CUDA events on the launching stream around forward+backward; the
