@@ -490,10 +490,11 @@ __device__ __forceinline__ void dst_tiles(const Ctx &c, const float *src, bool s
 // i-stage operand, epi(a, l, value) stores the j-stage output.  Interiors up
 // to kDstBandMax in either direction (larger ones use dst_tiles).
 // Used by the batched solve only.  Each thread runs its FP64 sums over L2
-// loads, latency-bound when one member has the GPU (177x161 alone: 3.2 ms
-// per step with the tiles, 4.0 with the pairs); in a batch the other
-// members' blocks hide that latency and the two barriers saved per
-// iteration win (64 mixed members: 8.4 -> 8.8 member-days/s).
+// loads with few in flight, which one member alone does not hide (by timing,
+// not profiled: 177x161 alone 3.2 ms per step with the tiles, 4.0 with the
+// pairs); in a batch the other members' blocks hide that latency and the
+// two barriers saved per iteration win (64 mixed members: 8.4 -> 8.8
+// member-days/s).
 template <class Src, class Epi>
 __device__ __forceinline__ void dst_row_pairs(const Ctx &c, Src &&src, Epi &&epi) {
   float(*sxr)[kDstBandMax] = reinterpret_cast<float(*)[kDstBandMax]>(dst_smem());
